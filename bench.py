@@ -1,0 +1,333 @@
+"""Benchmark: batched dUCCSD energy + adjoint-gradient evaluations on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): 256 parameter sets of the 16-qubit dUCCSD problem
+(8 spatial orbitals, 8 electrons, 360 SD parameters, seeded random integrals,
+5,793 Hamiltonian terms); each evaluation is the energy <U^dag H U> and its full
+adjoint gradient.  Metric: evaluations per second (whole job).
+
+* ``value``    device-timed (CUDA events, max over ranks): parameters already in
+               HBM, one graph-captured run per step.
+* ``e2e``      the same through the public API with host buffers: the step's
+               parameters copied from pinned host memory and its energies and
+               gradients read back, inside the timed region.
+* ``roofline`` the dominant kernel, timed stage by stage with CUDA events.
+* ``cpu_baseline`` the compiled reference (``oracle/_ref``) on a bounded sample
+               of the same workload, on this host's cores (rank 0, N = 1 only).
+
+N > 1 runs N independent replicas (one process per GPU, no collective on the
+data path): weak scaling.  ``--impl reference`` times the reference's own CPU
+path on the same workload and prints the same metric.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "UCC energy+grad evals/s"
+UNIT = "evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--norb", type=int, default=8)
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def problem(norb, seed):
+    import qforte_b200 as qb
+    mol = qb.random_molecule(norb, norb, seed)
+    pool = qb.SQOpPool()
+    pool.set_orb_spaces(mol.hf_reference)
+    pool.fill_pool("SD")
+    return mol, pool
+
+
+def workload_config(a, nterms, nparam):
+    return {"workload": f"batched dUCCSD energy + adjoint gradient, {2 * a.norb} qubits "
+                        f"({a.norb} orbitals, {a.norb} electrons), {nparam} SD parameters, "
+                        f"{nterms} Hamiltonian terms, {a.batch} parameter sets per step",
+            "nqubit": 2 * a.norb, "batch": a.batch, "nparam": nparam, "hamiltonian_terms": nterms,
+            "l2": f"inputs larger than L2: {2 * a.batch} states x {16 << (2 * a.norb)} B "
+                  "resident per step",
+            "parallelism": f"replicas x{a.gpus}"}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(a, mol, pool, amps_row, steps=2):
+    """The compiled reference on a bounded sample (seconds per evaluation)."""
+    from oracle import oracle as O
+    from qforte_b200.pauli import letters
+    qf = O.load_reference_engine()
+
+    def terms(qo):
+        return [(complex(c), letters(*circ._pauli_masks()[:2])) for c, circ in qo.terms()]
+
+    import qforte_b200 as qb
+    kf, kg = [], []
+    for _, op in pool:
+        s = qb.SQOperator()
+        s.add_op(op)
+        q = s.jw_transform()
+        kg.append(terms(q))
+        q.simplify()
+        q.order_terms()
+        kf.append(terms(q))
+    ht = terms(mol.hamiltonian)
+    h_sample = max(1, len(ht) // 10)
+    m_sample = 24
+    per = []
+    for _ in range(steps):
+        t, parts = O.ref_eval_sample(qf, 2 * a.norb, mol.hf_reference, kf, kg, list(amps_row), ht,
+                                     h_sample, m_sample)
+        per.append(t)
+    t = statistics.median(per)
+    return {"value": 1.0 / t, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"per evaluation: U(t) as gates in full, apply_operator(H) on {h_sample} of "
+                      f"{len(ht)} terms scaled x{len(ht) / h_sample:.1f} (twice: energy and "
+                      f"sigma), {m_sample} of {len(kf)} reverse-sweep steps scaled; median of "
+                      f"{steps}; serial shipped build (USE_OpenMP off)",
+            "seconds_per_eval": t, "parts": parts}
+
+
+def run_reference(a, rank, world):
+    """--impl reference: the reference's CPU path on the same workload."""
+    mol, pool = problem(a.norb, a.seed)
+    rng = np.random.default_rng(a.seed + 1)
+    P = rng.uniform(-0.1, 0.1, (a.batch, len(pool)))
+    if rank != 0:
+        return None
+    try:
+        from oracle import oracle as O
+        O.load_reference_engine()
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference module not built: {e}"}))
+        return None
+    cb = cpu_baseline(a, mol, pool, P[0], steps=max(1, a.steps))
+    v = cb["value"]
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1000.0 * a.batch / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": workload_config(a, len(mol.hamiltonian), len(pool)), "impl": "reference",
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "gpu_launches": 0}
+    print(json.dumps(line))
+    return line
+
+
+def main():
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    import qforte_b200 as qb
+    from qforte_b200 import _lib
+    from qforte_b200.ucc import DUCC
+
+    _lib.check(_lib.lib().qfb_set_stream(_lib.ctypes.c_void_p(
+        torch.cuda.current_stream().cuda_stream)))
+    mol, pool = problem(a.norb, a.seed)
+    tops = list(range(len(pool)))
+    M = len(tops)
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+    ev = eng.evaluator(a.batch)
+    rng = np.random.default_rng(a.seed + 1 + rank)
+    P = rng.uniform(-0.1, 0.1, (a.batch, M))
+    d_params, d_energy, d_grad = ev.tensors()
+    d_params.copy_(torch.from_numpy(P))
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident throughput ----------------------------------------
+    for _ in range(max(a.warmup, 3)):
+        ev.run(True)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = _lib.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        ev.run(True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = _lib.launch_count() - l0
+    ms = e0.elapsed_time(e1) / a.steps
+    barrier()
+    ck = clocks.stop()
+    ms_all = ms
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_all = float(t.item())
+    value = world * a.batch / (ms_all / 1000.0)
+
+    # ---- end to end through the public API with host buffers ---------------
+    hP = torch.from_numpy(P).pin_memory()
+    hE = torch.empty(a.batch, dtype=torch.float64).pin_memory()
+    hG = torch.empty((a.batch, M), dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        ev.eval(P, True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(a.steps):
+        d_params.copy_(hP, non_blocking=True)
+        ev.run(True)
+        hE.copy_(d_energy, non_blocking=True)
+        hG.copy_(d_grad, non_blocking=True)
+        stream.synchronize()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / a.steps
+    if world > 1:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = world * a.batch / (ms_e2e / 1000.0)
+    # the numbers coming back are the evaluator's
+    assert np.all(np.isfinite(hE.numpy())) and np.all(np.isfinite(hG.numpy()))
+
+    # ---- roofline of the dominant kernel -------------------------------------
+    import ctypes
+    st_ms = (ctypes.c_double * 4)()
+    st_n = (ctypes.c_int64 * 4)()
+    _lib.check(_lib.lib().qfb_ucc_profile(ev.h, 1, max(2, min(a.steps, 5)), st_ms, st_n))
+    stages = ["reference", "U(t) program", "H psi + energy", "gradient sweep"]
+    N = 1 << (2 * a.norb)
+    state_bytes = 16 * N * a.batch
+    # algorithmic bytes per launch of each stage's main kernel
+    per_launch_bytes = {1: 2 * state_bytes,          # exp pass: read + write psi
+                        2: 2 * state_bytes,          # H psi: read psi (gathered) + write sigma
+                        3: 4 * state_bytes}          # gradient step: RMW psi and sigma
+    dom = max((1, 2, 3), key=lambda k: st_ms[k])
+    # launches of each stage's main kernel (stage 2 also holds the two small
+    # energy-reduction kernels, stage 3 the gradient finalisation)
+    main_launches = {1: st_n[1], 2: 1, 3: max(1, st_n[3] - 1)}
+    nl = max(1, main_launches[dom])
+    avg_ms = st_ms[dom] / nl
+    hbm, src = peaks()
+    achieved = per_launch_bytes[dom] / (avg_ms / 1000.0) / 1e9
+    kernel = {1: "k_prog_step", 2: "k_sum_apply", 3: "k_grad_step"}[dom]
+    roof = {"bound": "hbm", "kernel": kernel, "stage": stages[dom], "achieved": achieved,
+            "peak": hbm, "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": None, "algorithmic_bytes_per_launch": per_launch_bytes[dom],
+            "avg_launch_ms": avg_ms,
+            "stages_ms": {stages[k]: st_ms[k] for k in range(4)},
+            "stages_launches": {stages[k]: int(st_n[k]) for k in range(4)}}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": max(a.warmup, 3), "ms_per_step": ms_all, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": workload_config(a, len(mol.hamiltonian), M),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(P.nbytes),
+                    "d2h_bytes_per_step": int(hE.numel() * 8 + hG.numel() * 8)},
+            "roofline": roof, "gpu_launches": int(launches), "clocks": ck}
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            cb = cpu_baseline(a, mol, pool, P[0])
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            line["cpu_baseline"]["parts_s"] = cb["parts"]
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    del ev, eng
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

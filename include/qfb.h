@@ -1,0 +1,185 @@
+/*
+ * qfb.h -- C ABI of the B200 state-vector engine (libqfb.so).
+ *
+ * Drop-in boundary for QForte's `Computer` (src/qforte/computer.h:22-185) and
+ * the pybind11 surface that exposes it (src/qforte/bindings.cc:149-191).  Every
+ * entry point takes plain pointers and sizes, returns an int status (QFB_OK = 0)
+ * and never throws; qfb_last_error() gives the message of the calling thread's
+ * last failure.  The reference maps std::invalid_argument to ValueError and
+ * std::runtime_error to RuntimeError; here QFB_EINVAL plays the first role and
+ * every other non-zero status the second.
+ *
+ * Memory: the library owns the device buffers of states and compiled tables;
+ * callers own host arrays, which are copied before the call returns.  All work
+ * is enqueued on the calling thread's stream (qfb_set_stream, default: the
+ * legacy default stream); results that come back to the host (energies, inner
+ * products, amplitudes) synchronise that stream.
+ *
+ * Layout: a state of n qubits is 2^n complex128 amplitudes, interleaved
+ * (re, im), basis index i <-> qubit k is bit k of i (qubit_basis.h:27-45).
+ */
+#ifndef QFB_H
+#define QFB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define QFB_API __attribute__((visibility("default")))
+#else
+#define QFB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    QFB_OK = 0,
+    QFB_EINVAL = 22,     /* bad argument (reference: std::invalid_argument)  */
+    QFB_ENOMEM = 12,     /* device allocation refused                          */
+    QFB_EDEVICE = 5,     /* CUDA error                                         */
+    QFB_ETIMEDOUT = 110, /* a bounded device wait gave up                      */
+    QFB_ENOSYS = 38      /* not supported in this build                        */
+};
+
+typedef struct { double re, im; } qfb_complex;
+
+/* Gate kinds. Matrices follow make_gate.cc:18-235; the kind is informational,
+ * the kernels act on the matrix exactly as Computer::apply_gate does. */
+typedef struct {
+    int32_t target;
+    int32_t control; /* == target for 1-qubit gates                          */
+    qfb_complex mat[4][4]; /* row/col index (control_bit << 1) | target_bit  */
+} qfb_gate;
+
+/* One Pauli string in mask form: X on bits of xmask & ~zmask, Z on zmask &
+ * ~xmask, Y where both are set.  P|j> = i^ny (-1)^popcount(j & zmask) |j ^ xmask>
+ * with ny = popcount(xmask & zmask). */
+typedef struct {
+    uint64_t xmask;
+    uint64_t zmask;
+} qfb_pauli;
+
+typedef struct qfb_state_s *qfb_state; /* one (or a batch of) state vector(s) */
+typedef struct qfb_sum_s *qfb_sum;     /* device-resident grouped Pauli sum   */
+typedef struct qfb_prog_s *qfb_prog;   /* device-resident Pauli-exponential program */
+
+/* ---- library ------------------------------------------------------------ */
+QFB_API int qfb_version(void);
+QFB_API int qfb_last_error(char *buf, size_t len);
+/* Make `stream` (a cudaStream_t) the calling thread's stream; NULL = default. */
+QFB_API int qfb_set_stream(void *stream);
+QFB_API int qfb_sync(void);
+/* Count of kernels this library launched in this process (evidence counter). */
+QFB_API int qfb_launch_count(uint64_t *out);
+
+/* ---- states: Computer::Computer / copy ctor / reset / null_state ----------
+ * computer.cc:28-54, computer.h:28.  nbatch > 1 holds nbatch independent
+ * states of the same size back to back (batched evaluation). */
+QFB_API int qfb_state_create(int nqubit, int nbatch, qfb_state *out);
+QFB_API int qfb_state_destroy(qfb_state s);
+QFB_API int qfb_state_info(qfb_state s, int *nqubit, int *nbatch);
+QFB_API void *qfb_state_device_ptr(qfb_state s);
+/* dst <- src (same shape).  Computer(const Computer&). */
+QFB_API int qfb_state_copy(qfb_state dst, qfb_state src);
+/* batch slot `dst_b` of dst <- slot `src_b` of src. */
+QFB_API int qfb_state_copy_slot(qfb_state dst, int dst_b, qfb_state src, int src_b);
+/* |0...0> in every slot (Computer::reset, computer.cc:51-54). */
+QFB_API int qfb_state_reset(qfb_state s);
+/* all zero (Computer::null_state, computer.cc:49). */
+QFB_API int qfb_state_null(qfb_state s);
+/* zero, then amplitude `value` at each listed basis index, slot b
+ * (Computer::set_state, computer.cc:42-47). */
+QFB_API int qfb_state_set_basis(qfb_state s, int b, const uint64_t *index, const qfb_complex *value,
+                        int64_t n);
+/* host <-> device copies of slot b (set_coeff_vec / get_coeff_vec,
+ * computer.h:112,132; bindings.cc:176-182). */
+QFB_API int qfb_state_upload(qfb_state s, int b, const qfb_complex *host, uint64_t n);
+QFB_API int qfb_state_download(qfb_state s, int b, qfb_complex *host, uint64_t n);
+QFB_API int qfb_state_get_amp(qfb_state s, int b, uint64_t index, qfb_complex *out);
+
+/* ---- gates: Computer::apply_circuit / apply_gate ---------------------------
+ * computer.cc:93-114, :340-751.  Gates are applied in list order. */
+QFB_API int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates);
+
+/* ---- scalars and inner products -------------------------------------------
+ * apply_constant computer.cc:130-133; dot computer.cc:975-980. */
+QFB_API int qfb_scale(qfb_state s, qfb_complex a);
+/* out[b] = <a_b | b_b> for every slot. */
+QFB_API int qfb_vdot(qfb_state a, qfb_state b, qfb_complex *out);
+/* y <- y + alpha * x (same shape). */
+QFB_API int qfb_axpy(qfb_state y, qfb_complex alpha, qfb_state x);
+
+/* ---- grouped Pauli sums (QubitOperator of Pauli circuits) ------------------
+ * Terms are grouped by xmask on the device so one read of the (j, j^x) pairs
+ * serves every term of a group.  `segment` gives, per term, the index of the
+ * result it contributes to (0 for a plain operator; the pool index for a
+ * pool of operators); nsegment results come back from qfb_sum_expval. */
+QFB_API int qfb_sum_create(const qfb_pauli *paulis, const qfb_complex *coeffs, const int32_t *segment,
+                   int64_t nterms, int32_t nsegment, qfb_sum *out);
+QFB_API int qfb_sum_destroy(qfb_sum h);
+QFB_API int qfb_sum_info(qfb_sum h, int64_t *nterms, int64_t *ngroups, int32_t *nsegment);
+/* out[b * nsegment + g] = <bra_b | O_g | ket_b>.  bra may equal ket
+ * (direct_op_exp_val computer.cc:753-771, direct_oppl_exp_val :773-782). */
+QFB_API int qfb_sum_expval(qfb_sum h, qfb_state bra, qfb_state ket, qfb_complex *out);
+/* dst <- O src, all segments summed (apply_operator computer.cc:80-91). */
+QFB_API int qfb_sum_apply(qfb_sum h, qfb_state dst, qfb_state src);
+
+/* ---- Pauli-exponential programs (dUCC / ADAPT ansatz) ----------------------
+ * The program is the ordered list of exp(i phi_k P_k); phi_k =
+ * scale[k] * params[param[k]] (so one compiled program serves every
+ * amplitude vector).  Consecutive strings sharing an xmask run in one pass.
+ * Replaces exponentiate_pauli_string + trotterize (utils/exponentiate.py:9-87,
+ * utils/trotterization.py:10-57) followed by Computer::apply_circuit. */
+QFB_API int qfb_prog_create(const qfb_pauli *paulis, const double *scale, const int32_t *param,
+                    int64_t nstrings, int32_t nparam, qfb_prog *out);
+QFB_API int qfb_prog_destroy(qfb_prog p);
+QFB_API int qfb_prog_info(qfb_prog p, int64_t *nstrings, int64_t *nsteps, int32_t *nparam);
+/* Apply the program to every slot; params is [nbatch][nparam] (a single row
+ * is broadcast when nrows == 1).  sign = +1 applies U, -1 applies U^dagger
+ * (the strings in reverse order with negated angles). */
+QFB_API int qfb_prog_apply(qfb_prog p, qfb_state s, const double *params, int32_t nrows, int32_t sign);
+
+/* ---- adjoint dUCC gradient (UCCVQE.measure_gradient, uccvqeabc.py:122-251) --
+ * psi holds U(t)|ref>, sigma holds H psi.  `kprog` lists, per parameter mu,
+ * the strings of K_mu with scale = the imaginary parts of K_mu's JW
+ * coefficients (param[k] = mu); grad[b][mu] = 2 Re <sigma|K_mu|psi_mu>.  psi
+ * and sigma are consumed (un-rotated back to the reference). */
+QFB_API int qfb_ucc_gradient(qfb_prog kprog, qfb_state psi, qfb_state sigma, const double *params,
+                     int32_t nrows, double *grad);
+
+/* ---- compiled dUCC evaluator (batched, CUDA-graph captured) ----------------
+ * One object per (ansatz, Hamiltonian, batch size): it owns nbatch psi and
+ * sigma states, a device parameter block [nbatch][nparam], device outputs
+ * energy[nbatch] and grad[nbatch][nparam], and every scratch buffer its
+ * reductions need, so a run allocates nothing and synchronises nothing and
+ * can be captured once into a CUDA graph and replayed.  A run computes, per
+ * slot b: psi_b = U(t_b)|ref>, sigma_b = H psi_b, energy[b] = <psi_b|sigma_b>
+ * and (with_grad) the adjoint gradient of UCCVQE.measure_gradient
+ * (uccvqeabc.py:122-251).  `gprog` may be NULL when no gradient is wanted. */
+typedef struct qfb_ucc_s *qfb_ucc;
+QFB_API int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_sum ham, int nqubit,
+                           uint64_t ref_index, int nbatch, qfb_ucc *out);
+QFB_API int qfb_ucc_destroy(qfb_ucc u);
+/* Device addresses of the parameter block and the outputs. */
+QFB_API int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_grad);
+/* Enqueue one evaluation on the calling thread's stream (replays the
+ * captured graph when one exists for this with_grad). */
+QFB_API int qfb_ucc_run(qfb_ucc u, int with_grad);
+/* Capture one evaluation into a CUDA graph (replayed by later runs). */
+QFB_API int qfb_ucc_capture(qfb_ucc u, int with_grad);
+/* Host convenience: params in, energies (and gradients) out, synchronous. */
+QFB_API int qfb_ucc_eval(qfb_ucc u, const double *params, double *energy, double *grad);
+/* Instrumented runs: `reps` evaluations enqueued stage by stage with CUDA
+ * events between the stages; returns the mean milliseconds and the kernel
+ * launches of each stage: [0] reference state, [1] U(t) program, [2] H psi and
+ * energy, [3] gradient sweep. */
+QFB_API int qfb_ucc_profile(qfb_ucc u, int with_grad, int reps, double *stage_ms,
+                            int64_t *stage_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QFB_H */

@@ -1,0 +1,532 @@
+// libqfb.so core: library plumbing, state lifecycle, gate application,
+// scale / axpy / inner products.
+//
+// Gate semantics follow Computer::apply_1qubit_gate (computer.cc:340-425) and
+// Computer::apply_2qubit_gate (computer.cc:458-751) case by case, including
+// the reference's quirks, so a circuit gives the reference's amplitudes:
+//   * a 2x2 block with only off-diagonal entries that compare equal is applied
+//     as X (`op_0_1 == op_1_0 == 1.0`, computer.cc:398, :548, :669);
+//   * a 2-qubit matrix with m00 == m11 == 1 and |m01| + |m10| < 1e-16 is
+//     applied as a controlled 2x2 block on the control = 1 half, ignoring any
+//     other entry outside that block (computer.cc:469-719);
+//   * any other 2-qubit matrix is applied in full, each output accumulated
+//     over the 4 inputs in column order, entries with |m| <= 1e-16 skipped
+//     (computer.cc:721-750).
+// The classification is made once per gate on the host; each kernel then
+// touches only the amplitudes its case changes (a diagonal gate with one
+// entry equal to 1 reads and writes half the state, a controlled gate a
+// quarter or half).
+#include <cstdarg>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "qfb_common.cuh"
+
+namespace qfb {
+
+thread_local std::string t_last_error;
+thread_local cudaStream_t t_stream = nullptr;
+std::atomic<uint64_t> g_launches{0};
+
+int fail(int code, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(e == cudaErrorMemoryAllocation ? QFB_ENOMEM : QFB_EDEVICE, "%s: %s (%s)", what,
+                cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+static std::mutex g_pool_mu;
+static bool g_pool_ready[64];
+
+static void pool_init(int dev) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (dev < 0 || dev >= 64 || g_pool_ready[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;  // keep freed blocks cached in this process
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    g_pool_ready[dev] = true;
+}
+
+int dev_alloc(void **p, size_t bytes) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    pool_init(dev);
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, t_stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(QFB_ENOMEM, "device allocation of %zu bytes failed: %s", bytes,
+                    cudaGetErrorString(e));
+    }
+    return QFB_OK;
+}
+
+void dev_free(void *p) {
+    if (p) cudaFreeAsync(p, t_stream);
+}
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && cached[dev]) return cached[dev];
+    int n = 148;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (dev >= 0 && dev < 64) cached[dev] = n;
+    return n;
+}
+
+}  // namespace qfb
+
+using namespace qfb;
+
+// ===========================================================================
+// kernels
+// ===========================================================================
+
+namespace {
+
+enum : int { K_DENSE = 0, K_DIAG = 1, K_SWAP = 2, K_ANTI = 3 };
+
+struct Gate2 {  // a 2x2 block acting on target bit t, optionally where bit c == 1
+    int kind;
+    int t;
+    int c;         // -1: no control
+    int diag_set;  // K_DIAG: bit0 -> a != 1, bit1 -> d != 1
+    double2 a, b, cc, d;
+};
+
+struct Gate4 {  // generic 2-qubit matrix
+    int t, c;
+    uint32_t nz;  // bit (4*i + j) set when |m[i][j]| > 1e-16
+    double2 m[16];
+};
+
+__global__ void k_gate2(double2 *__restrict__ psi, uint64_t nbasis, Gate2 g) {
+    double2 *s = psi + (uint64_t)blockIdx.y * nbasis;
+    const uint64_t tbit = 1ull << g.t;
+    const uint64_t npair = (g.c < 0) ? (nbasis >> 1) : (nbasis >> 2);
+    const int lo = (g.c < 0) ? g.t : min(g.t, g.c);
+    const int hi = (g.c < 0) ? -1 : max(g.t, g.c);
+    const uint64_t cbit = (g.c < 0) ? 0ull : (1ull << g.c);
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i0 = insert0(p, lo);
+        if (hi >= 0) i0 = insert0(i0, hi) | cbit;
+        const uint64_t i1 = i0 | tbit;
+        if (g.kind == K_DENSE) {
+            const double2 x0 = s[i0], x1 = s[i1];
+            s[i0] = c_add(c_mul(g.a, x0), c_mul(g.b, x1));
+            s[i1] = c_add(c_mul(g.cc, x0), c_mul(g.d, x1));
+        } else if (g.kind == K_DIAG) {
+            if (g.diag_set & 1) s[i0] = c_mul(g.a, s[i0]);
+            if (g.diag_set & 2) s[i1] = c_mul(g.d, s[i1]);
+        } else if (g.kind == K_SWAP) {
+            const double2 x0 = s[i0], x1 = s[i1];
+            s[i0] = x1;
+            s[i1] = x0;
+        } else {
+            const double2 x0 = s[i0], x1 = s[i1];
+            s[i0] = c_mul(g.b, x1);
+            s[i1] = c_mul(g.cc, x0);
+        }
+    }
+}
+
+__global__ void k_gate4(double2 *__restrict__ psi, uint64_t nbasis, Gate4 g) {
+    double2 *s = psi + (uint64_t)blockIdx.y * nbasis;
+    const uint64_t tbit = 1ull << g.t, cbit = 1ull << g.c;
+    const int lo = min(g.t, g.c), hi = max(g.t, g.c);
+    const uint64_t nquad = nbasis >> 2;
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nquad;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t base = insert0(insert0(p, lo), hi);
+        uint64_t idx[4];
+        idx[0] = base;
+        idx[1] = base | tbit;
+        idx[2] = base | cbit;
+        idx[3] = base | cbit | tbit;
+        double2 x[4], y[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[j] = s[idx[j]];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (g.nz & (1u << (4 * i + j))) acc = c_add(acc, c_mul(g.m[4 * i + j], x[j]));
+            y[i] = acc;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) s[idx[i]] = y[i];
+    }
+}
+
+__global__ void k_scale(double2 *__restrict__ psi, uint64_t n, double2 a) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        psi[i] = c_mul(psi[i], a);
+}
+
+__global__ void k_axpy(double2 *__restrict__ y, const double2 *__restrict__ x, uint64_t n,
+                       double2 a) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        y[i] = c_add(y[i], c_mul(a, x[i]));
+}
+
+__global__ void k_set_first(double2 *__restrict__ psi, uint64_t nbasis, int nbatch) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nbatch) psi[(uint64_t)b * nbasis] = make_double2(1.0, 0.0);
+}
+
+__global__ void k_scatter(double2 *__restrict__ psi, const uint64_t *__restrict__ idx,
+                          const double2 *__restrict__ val, int64_t n) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) psi[idx[k]] = val[k];
+}
+
+// partial[b * gridDim.x + blockIdx.x] = sum over this block's indices of conj(a) b
+__global__ void k_vdot_partial(const double2 *__restrict__ a, const double2 *__restrict__ b,
+                               uint64_t nbasis, double2 *__restrict__ partial) {
+    const uint64_t off = (uint64_t)blockIdx.y * nbasis;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nbasis;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        acc = c_add(acc, c_cjmul(a[off + i], b[off + i]));
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) partial[(uint64_t)blockIdx.y * gridDim.x + blockIdx.x] = acc;
+}
+
+// out[r] = sum_{k < n} partial[r * n + k]  (one block per row, fixed order)
+__global__ void k_rows_sum(const double2 *__restrict__ partial, int64_t n,
+                           double2 *__restrict__ out) {
+    const double2 *row = partial + (uint64_t)blockIdx.x * n;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int64_t k = threadIdx.x; k < n; k += blockDim.x) acc = c_add(acc, row[k]);
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) out[blockIdx.x] = acc;
+}
+
+inline double2 d2(const qfb_complex &c) { return make_double2(c.re, c.im); }
+inline bool is_one(const qfb_complex &c) { return c.re == 1.0 && c.im == 0.0; }
+inline bool ceq(const qfb_complex &a, const qfb_complex &b) {
+    return a.re == b.re && a.im == b.im;
+}
+inline double cabs_h(const qfb_complex &c) { return std::hypot(c.re, c.im); }
+
+constexpr double kThr = 1.0e-16;  // Computer::compute_threshold_ (computer.h:172)
+
+// Classify a 2x2 block as computer.cc:353-423 does.
+Gate2 classify2(const qfb_complex &a, const qfb_complex &b, const qfb_complex &c,
+                const qfb_complex &d, int t, int ctrl) {
+    Gate2 g;
+    g.t = t;
+    g.c = ctrl;
+    g.a = d2(a);
+    g.b = d2(b);
+    g.cc = d2(c);
+    g.d = d2(d);
+    g.diag_set = 0;
+    const bool has_diag = cabs_h(a) + cabs_h(d) > kThr;
+    const bool has_off = cabs_h(b) + cabs_h(c) > kThr;
+    if (has_diag && has_off) {
+        g.kind = K_DENSE;
+    } else if (has_diag) {
+        g.kind = K_DIAG;
+        g.diag_set = (is_one(a) ? 0 : 1) | (is_one(d) ? 0 : 2);
+    } else {
+        g.kind = ceq(b, c) ? K_SWAP : K_ANTI;
+    }
+    return g;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+int qfb_version(void) { return 10000; }
+
+int qfb_last_error(char *buf, size_t len) {
+    if (!buf || !len) return QFB_EINVAL;
+    std::strncpy(buf, t_last_error.c_str(), len - 1);
+    buf[len - 1] = '\0';
+    return QFB_OK;
+}
+
+int qfb_set_stream(void *stream) {
+    t_stream = (cudaStream_t)stream;
+    return QFB_OK;
+}
+
+int qfb_sync(void) {
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
+int qfb_launch_count(uint64_t *out) {
+    if (!out) return fail(QFB_EINVAL, "qfb_launch_count: null output");
+    *out = g_launches.load();
+    return QFB_OK;
+}
+
+int qfb_state_create(int nqubit, int nbatch, qfb_state *out) {
+    if (!out) return fail(QFB_EINVAL, "qfb_state_create: null output");
+    *out = nullptr;
+    if (nqubit < 1 || nqubit > 40)
+        return fail(QFB_EINVAL, "qfb_state_create: nqubit = %d outside [1, 40]", nqubit);
+    if (nbatch < 1) return fail(QFB_EINVAL, "qfb_state_create: nbatch = %d < 1", nbatch);
+    qfb_state s = new qfb_state_s;
+    s->nqubit = nqubit;
+    s->nbatch = nbatch;
+    s->nbasis = 1ull << nqubit;
+    s->d = nullptr;
+    int rc = dev_alloc((void **)&s->d, s->nbasis * (uint64_t)nbatch * sizeof(double2));
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    rc = qfb_state_reset(s);
+    if (rc) {
+        qfb_state_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return QFB_OK;
+}
+
+int qfb_state_destroy(qfb_state s) {
+    if (!s) return QFB_OK;
+    dev_free(s->d);
+    delete s;
+    return QFB_OK;
+}
+
+int qfb_state_info(qfb_state s, int *nqubit, int *nbatch) {
+    if (!s) return fail(QFB_EINVAL, "qfb_state_info: null state");
+    if (nqubit) *nqubit = s->nqubit;
+    if (nbatch) *nbatch = s->nbatch;
+    return QFB_OK;
+}
+
+void *qfb_state_device_ptr(qfb_state s) { return s ? (void *)s->d : nullptr; }
+
+int qfb_state_copy(qfb_state dst, qfb_state src) {
+    if (!dst || !src) return fail(QFB_EINVAL, "qfb_state_copy: null state");
+    if (dst->nqubit != src->nqubit || dst->nbatch != src->nbatch)
+        return fail(QFB_EINVAL, "qfb_state_copy: shape mismatch (%d q x %d vs %d q x %d)",
+                    dst->nqubit, dst->nbatch, src->nqubit, src->nbatch);
+    if (dst == src) return QFB_OK;
+    QFB_CUDA(cudaMemcpyAsync(dst->d, src->d, src->nbasis * src->nbatch * sizeof(double2),
+                             cudaMemcpyDeviceToDevice, t_stream));
+    return QFB_OK;
+}
+
+int qfb_state_copy_slot(qfb_state dst, int db, qfb_state src, int sb) {
+    if (!dst || !src) return fail(QFB_EINVAL, "qfb_state_copy_slot: null state");
+    if (dst->nqubit != src->nqubit)
+        return fail(QFB_EINVAL, "qfb_state_copy_slot: qubit counts differ (%d vs %d)",
+                    dst->nqubit, src->nqubit);
+    if (db < 0 || db >= dst->nbatch || sb < 0 || sb >= src->nbatch)
+        return fail(QFB_EINVAL, "qfb_state_copy_slot: slot out of range");
+    QFB_CUDA(cudaMemcpyAsync(dst->d + (uint64_t)db * dst->nbasis,
+                             src->d + (uint64_t)sb * src->nbasis, src->nbasis * sizeof(double2),
+                             cudaMemcpyDeviceToDevice, t_stream));
+    return QFB_OK;
+}
+
+int qfb_state_null(qfb_state s) {
+    if (!s) return fail(QFB_EINVAL, "qfb_state_null: null state");
+    QFB_CUDA(cudaMemsetAsync(s->d, 0, s->nbasis * s->nbatch * sizeof(double2), t_stream));
+    return QFB_OK;
+}
+
+int qfb_state_reset(qfb_state s) {
+    int rc = qfb_state_null(s);
+    if (rc) return rc;
+    k_set_first<<<(s->nbatch + 127) / 128, 128, 0, t_stream>>>(s->d, s->nbasis, s->nbatch);
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
+int qfb_state_set_basis(qfb_state s, int b, const uint64_t *index, const qfb_complex *value,
+                        int64_t n) {
+    if (!s) return fail(QFB_EINVAL, "qfb_state_set_basis: null state");
+    if (b < 0 || b >= s->nbatch) return fail(QFB_EINVAL, "qfb_state_set_basis: bad slot %d", b);
+    if (n < 0 || (n > 0 && (!index || !value)))
+        return fail(QFB_EINVAL, "qfb_state_set_basis: bad arrays");
+    for (int64_t k = 0; k < n; ++k)
+        if (index[k] >= s->nbasis)
+            return fail(QFB_EINVAL, "qfb_state_set_basis: index %llu outside the %d-qubit basis",
+                        (unsigned long long)index[k], s->nqubit);
+    double2 *slot = s->d + (uint64_t)b * s->nbasis;
+    QFB_CUDA(cudaMemsetAsync(slot, 0, s->nbasis * sizeof(double2), t_stream));
+    if (n == 0) return QFB_OK;
+    // a repeated index keeps its last value, as the reference's loop does
+    std::vector<uint64_t> uidx;
+    std::vector<double2> uval;
+    {
+        std::unordered_map<uint64_t, size_t> pos;
+        for (int64_t k = 0; k < n; ++k) {
+            auto it = pos.find(index[k]);
+            if (it == pos.end()) {
+                pos.emplace(index[k], uidx.size());
+                uidx.push_back(index[k]);
+                uval.push_back(d2(value[k]));
+            } else {
+                uval[it->second] = d2(value[k]);
+            }
+        }
+    }
+    const int64_t cnt = (int64_t)uidx.size();
+    void *buf = nullptr;
+    int rc = dev_alloc(&buf, (size_t)cnt * (sizeof(uint64_t) + sizeof(double2)));
+    if (rc) return rc;
+    uint64_t *d_idx = (uint64_t *)buf;
+    double2 *d_val = (double2 *)(d_idx + cnt);
+    QFB_CUDA(cudaMemcpyAsync(d_idx, uidx.data(), cnt * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                             t_stream));
+    QFB_CUDA(cudaMemcpyAsync(d_val, uval.data(), cnt * sizeof(double2), cudaMemcpyHostToDevice,
+                             t_stream));
+    k_scatter<<<(unsigned)((cnt + 255) / 256), 256, 0, t_stream>>>(slot, d_idx, d_val, cnt);
+    QFB_LAUNCHED();
+    dev_free(buf);
+    return QFB_OK;
+}
+
+int qfb_state_upload(qfb_state s, int b, const qfb_complex *host, uint64_t n) {
+    if (!s || !host) return fail(QFB_EINVAL, "qfb_state_upload: null argument");
+    if (b < 0 || b >= s->nbatch) return fail(QFB_EINVAL, "qfb_state_upload: bad slot %d", b);
+    if (n != s->nbasis)
+        return fail(QFB_EINVAL, "qfb_state_upload: %llu amplitudes given, state holds %llu",
+                    (unsigned long long)n, (unsigned long long)s->nbasis);
+    QFB_CUDA(cudaMemcpyAsync(s->d + (uint64_t)b * s->nbasis, host, n * sizeof(double2),
+                             cudaMemcpyHostToDevice, t_stream));
+    return QFB_OK;
+}
+
+int qfb_state_download(qfb_state s, int b, qfb_complex *host, uint64_t n) {
+    if (!s || !host) return fail(QFB_EINVAL, "qfb_state_download: null argument");
+    if (b < 0 || b >= s->nbatch) return fail(QFB_EINVAL, "qfb_state_download: bad slot %d", b);
+    if (n != s->nbasis)
+        return fail(QFB_EINVAL, "qfb_state_download: buffer of %llu for a state of %llu",
+                    (unsigned long long)n, (unsigned long long)s->nbasis);
+    QFB_CUDA(cudaMemcpyAsync(host, s->d + (uint64_t)b * s->nbasis, n * sizeof(double2),
+                             cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
+int qfb_state_get_amp(qfb_state s, int b, uint64_t index, qfb_complex *out) {
+    if (!s || !out) return fail(QFB_EINVAL, "qfb_state_get_amp: null argument");
+    if (b < 0 || b >= s->nbatch || index >= s->nbasis)
+        return fail(QFB_EINVAL, "qfb_state_get_amp: index out of range");
+    QFB_CUDA(cudaMemcpyAsync(out, s->d + (uint64_t)b * s->nbasis + index, sizeof(double2),
+                             cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
+int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates) {
+    if (!s) return fail(QFB_EINVAL, "qfb_apply_gates: null state");
+    if (ngates < 0 || (ngates > 0 && !gates))
+        return fail(QFB_EINVAL, "qfb_apply_gates: bad gate array");
+    for (int64_t k = 0; k < ngates; ++k) {
+        const qfb_gate &g = gates[k];
+        if (g.target < 0 || g.target >= s->nqubit || g.control < 0 || g.control >= s->nqubit)
+            return fail(QFB_EINVAL,
+                        "qfb_apply_gates: gate %lld acts on qubit (%d, %d) of a %d-qubit state",
+                        (long long)k, g.target, g.control, s->nqubit);
+    }
+    const dim3 block(256);
+    for (int64_t k = 0; k < ngates; ++k) {
+        const qfb_gate &g = gates[k];
+        const auto &m = g.mat;
+        if (g.target == g.control) {
+            Gate2 q = classify2(m[0][0], m[0][1], m[1][0], m[1][1], g.target, -1);
+            const dim3 grid(grid_for(s->nbasis >> 1, 256), s->nbatch);
+            k_gate2<<<grid, block, 0, t_stream>>>(s->d, s->nbasis, q);
+            QFB_LAUNCHED();
+            continue;
+        }
+        const bool controlled = (cabs_h(m[0][1]) + cabs_h(m[1][0]) < kThr) && is_one(m[0][0]) &&
+                                is_one(m[1][1]);
+        if (controlled) {
+            Gate2 q = classify2(m[2][2], m[2][3], m[3][2], m[3][3], g.target, g.control);
+            const dim3 grid(grid_for(s->nbasis >> 2, 256), s->nbatch);
+            k_gate2<<<grid, block, 0, t_stream>>>(s->d, s->nbasis, q);
+            QFB_LAUNCHED();
+            continue;
+        }
+        Gate4 q;
+        q.t = g.target;
+        q.c = g.control;
+        q.nz = 0;
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) {
+                q.m[4 * i + j] = d2(m[i][j]);
+                if (cabs_h(m[i][j]) > kThr) q.nz |= 1u << (4 * i + j);
+            }
+        const dim3 grid(grid_for(s->nbasis >> 2, 256), s->nbatch);
+        k_gate4<<<grid, block, 0, t_stream>>>(s->d, s->nbasis, q);
+        QFB_LAUNCHED();
+    }
+    return QFB_OK;
+}
+
+int qfb_scale(qfb_state s, qfb_complex a) {
+    if (!s) return fail(QFB_EINVAL, "qfb_scale: null state");
+    const uint64_t n = s->nbasis * s->nbatch;
+    k_scale<<<grid_for(n, 256), 256, 0, t_stream>>>(s->d, n, d2(a));
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
+int qfb_axpy(qfb_state y, qfb_complex alpha, qfb_state x) {
+    if (!y || !x) return fail(QFB_EINVAL, "qfb_axpy: null state");
+    if (y->nqubit != x->nqubit || y->nbatch != x->nbatch)
+        return fail(QFB_EINVAL, "qfb_axpy: shape mismatch");
+    const uint64_t n = y->nbasis * y->nbatch;
+    k_axpy<<<grid_for(n, 256), 256, 0, t_stream>>>(y->d, x->d, n, d2(alpha));
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
+int qfb_vdot(qfb_state a, qfb_state b, qfb_complex *out) {
+    if (!a || !b || !out) return fail(QFB_EINVAL, "qfb_vdot: null argument");
+    if (a->nqubit != b->nqubit || a->nbatch != b->nbatch)
+        return fail(QFB_EINVAL, "qfb_vdot: shape mismatch");
+    const unsigned nblk = grid_for(a->nbasis, 256, 2);
+    void *buf = nullptr;
+    int rc = dev_alloc(&buf, sizeof(double2) * ((size_t)nblk + 1) * a->nbatch);
+    if (rc) return rc;
+    double2 *partial = (double2 *)buf;
+    double2 *res = partial + (size_t)nblk * a->nbatch;
+    k_vdot_partial<<<dim3(nblk, a->nbatch), 256, 0, t_stream>>>(a->d, b->d, a->nbasis, partial);
+    QFB_LAUNCHED();
+    k_rows_sum<<<a->nbatch, 256, 0, t_stream>>>(partial, nblk, res);
+    QFB_LAUNCHED();
+    QFB_CUDA(cudaMemcpyAsync(out, res, sizeof(double2) * a->nbatch, cudaMemcpyDeviceToHost,
+                             t_stream));
+    dev_free(buf);
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1081 @@
+// libqfb.so: grouped Pauli sums and Pauli-exponential programs.
+//
+// Pauli algebra on basis states (mask form, qfb.h):
+//   P|j> = i^ny (-1)^popcount(j & z) |j ^ x>,   ny = popcount(x & z).
+//
+// Grouped sums (qfb_sum_*).  The reference evaluates sum_t c_t P_t one term at a
+// time: a state copy, the term's gates, a scale and an accumulation per term
+// (Computer::apply_operator, computer.cc:80-91; direct_op_exp_val :753-771).
+// Here the terms are grouped by x on the host; within a group all terms pair
+// amplitude j with j ^ x, so for each pair one read of the two amplitudes
+// serves every term of the group:
+//   f_x(j) = sum_{t in x} c_t i^ny_t (-1)^popcount(j & z_t)
+//   <bra|O|ket> = sum_x sum_j conj(bra[j ^ x]) f_x(j) ket[j]
+//   (O ket)[k]  = sum_x f_x(k ^ x) ket[k ^ x]
+// f_x(j ^ x) differs from f_x(j) only by (-1)^popcount(x & z_t) per term, so a
+// pair costs one parity per term.  Groups whose coefficients c_t i^ny_t are all
+// real (every Hamiltonian built from real integrals) take a real-arithmetic path.
+//
+// Programs (qfb_prog_*).  exp(i phi P) acts on each pair (j, j ^ x) as
+//   new_j     = cos(phi) psi_j     + i sin(phi) ph(j ^ x) psi_{j^x}
+//   new_{j^x} = cos(phi) psi_{j^x} + i sin(phi) ph(j)     psi_j
+// with ph(j) = i^ny (-1)^popcount(j & z) (a diagonal phase when x = 0).  This
+// is the unitary that utils/exponentiate.py:9-87 builds out of 2w + 1 gates
+// (basis change, CNOT ladder, Rz(-2 Im c), uncompute); here it is one pass.
+// Consecutive strings sharing x map the same pairs onto themselves, so a run
+// of them (all strings of one dUCC excitation) is applied in one pass with
+// the rotations chained in registers.
+//
+// Adjoint gradient (qfb_ucc_gradient) follows UCCVQE.measure_gradient
+// (uccvqeabc.py:122-251): g_mu = 2 Re <sigma_mu|K_mu|psi_mu>, then
+// psi_{mu-1} = U_mu^dagger psi_mu and sigma_{mu-1} = U_mu^dagger sigma_mu.  When
+// K_mu is one x-group the inner product and both un-rotations share one pass
+// over (psi, sigma); no intermediate state is stored.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "qfb_common.cuh"
+
+using namespace qfb;
+
+namespace {
+
+struct TermDev {  // one term of a grouped sum
+    uint64_t z;
+    double2 c;  // c_t * i^ny_t
+};
+
+struct GroupDev {
+    uint64_t x;
+    int32_t h;      // highest set bit of x, -1 when x == 0
+    int32_t begin;  // first term
+    int32_t end;    // one past the last term
+    int32_t real;   // all term coefficients real
+};
+
+struct StrDev {  // one Pauli string of a program
+    uint64_t z;
+    int32_t ny;     // popcount(x & z) mod 4
+    int32_t param;  // parameter index
+    double scale;   // phi = scale * params[param]
+};
+
+struct StepDev {  // run of consecutive strings sharing one x (and one parameter)
+    uint64_t x;
+    int32_t h;
+    int32_t s0;  // first string
+    int32_t ns;  // number of strings
+    int32_t param;
+};
+
+constexpr int kMaxStepStrings = 64;   // strings per fused step (longer runs are split)
+constexpr int kTermTile = 256;        // terms staged in shared memory at a time
+
+int highest_bit(uint64_t x) { return x ? 63 - __builtin_clzll(x) : -1; }
+
+// ---------------------------------------------------------------------------
+// grouped sums
+// ---------------------------------------------------------------------------
+
+// partial[((b * G) + g) * gridDim.x + blockIdx.x] = this block's share of
+// <bra_b | O_g | ket_b>.  grid = (chunks, G, nbatch).
+__global__ void __launch_bounds__(256) k_sum_expval(
+    const double2 *__restrict__ bra, const double2 *__restrict__ ket, uint64_t nbasis,
+    const GroupDev *__restrict__ groups, const TermDev *__restrict__ terms, int32_t ngroups,
+    double2 *__restrict__ partial) {
+    __shared__ TermDev s_t[kTermTile];
+    const int g = blockIdx.y;
+    const uint64_t off = (uint64_t)blockIdx.z * nbasis;
+    const GroupDev gr = groups[g];
+    const uint64_t npair = nbasis >> 1;
+    const uint64_t chunk = (npair + gridDim.x - 1) / gridDim.x;
+    const uint64_t p0 = (uint64_t)blockIdx.x * chunk;
+    const uint64_t p1 = min(npair, p0 + chunk);
+    double2 acc = make_double2(0.0, 0.0);
+    for (int tb = gr.begin; tb < gr.end; tb += kTermTile) {
+        const int nt = min(kTermTile, gr.end - tb);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nt; i += blockDim.x) s_t[i] = terms[tb + i];
+        __syncthreads();
+        for (uint64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+            uint64_t j0, j1;
+            if (gr.h >= 0) {
+                j0 = insert0(p, gr.h);
+                j1 = j0 ^ gr.x;
+            } else {
+                j0 = p << 1;
+                j1 = j0 | 1ull;
+            }
+            const double2 a0 = ket[off + j0], a1 = ket[off + j1];
+            const double2 b0 = bra[off + j0], b1 = bra[off + j1];
+            if (gr.real) {
+                double f0 = 0.0, f1 = 0.0;
+                for (int t = 0; t < nt; ++t) {
+                    const double c = s_t[t].c.x;
+                    f0 += parity64(j0 & s_t[t].z) ? -c : c;
+                    f1 += parity64(j1 & s_t[t].z) ? -c : c;
+                }
+                // x != 0: conj(b1) f0 a0 + conj(b0) f1 a1 ; x == 0: conj(b0) f0 a0 + conj(b1) f1 a1
+                const double2 u = (gr.h >= 0) ? c_cjmul(b1, a0) : c_cjmul(b0, a0);
+                const double2 v = (gr.h >= 0) ? c_cjmul(b0, a1) : c_cjmul(b1, a1);
+                acc.x += f0 * u.x + f1 * v.x;
+                acc.y += f0 * u.y + f1 * v.y;
+            } else {
+                double2 f0 = make_double2(0.0, 0.0), f1 = make_double2(0.0, 0.0);
+                for (int t = 0; t < nt; ++t) {
+                    const double2 c = s_t[t].c;
+                    if (parity64(j0 & s_t[t].z)) { f0.x -= c.x; f0.y -= c.y; }
+                    else { f0.x += c.x; f0.y += c.y; }
+                    if (parity64(j1 & s_t[t].z)) { f1.x -= c.x; f1.y -= c.y; }
+                    else { f1.x += c.x; f1.y += c.y; }
+                }
+                const double2 u = (gr.h >= 0) ? c_cjmul(b1, a0) : c_cjmul(b0, a0);
+                const double2 v = (gr.h >= 0) ? c_cjmul(b0, a1) : c_cjmul(b1, a1);
+                acc = c_add(acc, c_add(c_mul(f0, u), c_mul(f1, v)));
+            }
+        }
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0)
+        partial[((uint64_t)blockIdx.z * ngroups + g) * gridDim.x + blockIdx.x] = acc;
+}
+
+// out[b * nseg + s] = sum of partial rows [row0[s], row0[s+1]) of batch b, each
+// row `chunks` long.  grid = (nseg, nbatch).
+__global__ void k_seg_sum(const double2 *__restrict__ partial, const int32_t *__restrict__ seg_g0,
+                          int32_t ngroups, int32_t chunks, double2 *__restrict__ out) {
+    const int s = blockIdx.x, b = blockIdx.y;
+    const uint64_t r0 = ((uint64_t)b * ngroups + seg_g0[s]) * chunks;
+    const uint64_t r1 = ((uint64_t)b * ngroups + seg_g0[s + 1]) * chunks;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint64_t k = r0 + threadIdx.x; k < r1; k += blockDim.x) acc = c_add(acc, partial[k]);
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) out[(uint64_t)b * gridDim.x + s] = acc;
+}
+
+// dst[k] = sum_g f_g(k ^ x_g) src[k ^ x_g]; one output per thread, written once.
+__global__ void __launch_bounds__(256) k_sum_apply(
+    double2 *__restrict__ dst, const double2 *__restrict__ src, uint64_t nbasis,
+    const GroupDev *__restrict__ groups, const TermDev *__restrict__ terms, int32_t ngroups) {
+    const uint64_t off = (uint64_t)blockIdx.y * nbasis;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nbasis;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int g = 0; g < ngroups; ++g) {
+            const GroupDev gr = groups[g];
+            const uint64_t j = k ^ gr.x;
+            const double2 a = src[off + j];
+            if (gr.real) {
+                double f = 0.0;
+                for (int t = gr.begin; t < gr.end; ++t) {
+                    const double c = __ldg(&terms[t].c.x);
+                    f += parity64(j & __ldg(&terms[t].z)) ? -c : c;
+                }
+                acc.x += f * a.x;
+                acc.y += f * a.y;
+            } else {
+                double2 f = make_double2(0.0, 0.0);
+                for (int t = gr.begin; t < gr.end; ++t) {
+                    const double2 c = terms[t].c;
+                    if (parity64(j & terms[t].z)) { f.x -= c.x; f.y -= c.y; }
+                    else { f.x += c.x; f.y += c.y; }
+                }
+                acc = c_add(acc, c_mul(f, a));
+            }
+        }
+        dst[off + k] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// programs
+// ---------------------------------------------------------------------------
+
+struct StepParams {
+    const StrDev *strs;
+    const double *params;  // [nrows][nparam]
+    int32_t nparam;
+    int32_t bcast;  // single parameter row for every slot
+    int32_t sign;   // +1: U, -1: U^dagger (reverse order, negated angles)
+};
+
+// Stage this step's strings (in application order) with cos/sin of their
+// angles for slot b into shared memory.
+__device__ __forceinline__ void stage_step(const StepDev &st, const StepParams &sp, int b,
+                                           uint64_t *s_z, int *s_q, double2 *s_cs) {
+    for (int i = threadIdx.x; i < st.ns; i += blockDim.x) {
+        const int k = st.s0 + (sp.sign > 0 ? i : st.ns - 1 - i);
+        const StrDev sd = sp.strs[k];
+        const double phi =
+            (double)sp.sign * sd.scale * sp.params[(sp.bcast ? 0 : b) * sp.nparam + sd.param];
+        double s, c;
+        sincos(phi, &s, &c);
+        s_z[i] = sd.z;
+        s_q[i] = sd.ny;
+        s_cs[i] = make_double2(c, s);
+    }
+    __syncthreads();
+}
+
+// exp(i phi P) on the pair (v0 at j0, v1 at j1 = j0 ^ x); for x == 0 call with
+// j1 == j0 on each amplitude separately (v1 is then ignored).
+__device__ __forceinline__ void rotate_pair(double2 &v0, double2 &v1, uint64_t j0, uint64_t j1,
+                                            uint64_t z, int ny, double2 cs, bool diag) {
+    const int q0 = (ny + 1 + 2 * parity64(j0 & z)) & 3;  // i * ph(j0)
+    if (diag) {
+        const double2 r = c_ipow(v0, q0);
+        v0 = make_double2(cs.x * v0.x + cs.y * r.x, cs.x * v0.y + cs.y * r.y);
+        return;
+    }
+    const int q1 = (ny + 1 + 2 * parity64(j1 & z)) & 3;  // i * ph(j1)
+    const double2 r1 = c_ipow(v1, q1), r0 = c_ipow(v0, q0);
+    const double2 n0 = make_double2(cs.x * v0.x + cs.y * r1.x, cs.x * v0.y + cs.y * r1.y);
+    const double2 n1 = make_double2(cs.x * v1.x + cs.y * r0.x, cs.x * v1.y + cs.y * r0.y);
+    v0 = n0;
+    v1 = n1;
+}
+
+__global__ void __launch_bounds__(256) k_prog_step(double2 *__restrict__ psi, uint64_t nbasis,
+                                                   StepDev st, StepParams sp) {
+    __shared__ uint64_t s_z[kMaxStepStrings];
+    __shared__ int s_q[kMaxStepStrings];
+    __shared__ double2 s_cs[kMaxStepStrings];
+    const int b = blockIdx.y;
+    stage_step(st, sp, b, s_z, s_q, s_cs);
+    double2 *s = psi + (uint64_t)b * nbasis;
+    const uint64_t npair = nbasis >> 1;
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        if (st.h >= 0) {
+            const uint64_t j0 = insert0(p, st.h), j1 = j0 ^ st.x;
+            double2 v0 = s[j0], v1 = s[j1];
+            for (int i = 0; i < st.ns; ++i) rotate_pair(v0, v1, j0, j1, s_z[i], s_q[i], s_cs[i], false);
+            s[j0] = v0;
+            s[j1] = v1;
+        } else {
+            const uint64_t j0 = p << 1, j1 = j0 | 1ull;
+            double2 v0 = s[j0], v1 = s[j1], dummy;
+            for (int i = 0; i < st.ns; ++i) {
+                rotate_pair(v0, dummy, j0, j0, s_z[i], s_q[i], s_cs[i], true);
+                rotate_pair(v1, dummy, j1, j1, s_z[i], s_q[i], s_cs[i], true);
+            }
+            s[j0] = v0;
+            s[j1] = v1;
+        }
+    }
+}
+
+// One gradient step: accumulate <sigma|K|psi> for K = sum_i (i scale_i) P_i over
+// this step's strings, then (when `rotate`) apply the step's U^dagger to both
+// states.  partial[((row * nbatch) + b) * gridDim.x + blockIdx.x].
+__global__ void __launch_bounds__(256) k_grad_step(double2 *__restrict__ psi,
+                                                   double2 *__restrict__ sig, uint64_t nbasis,
+                                                   StepDev st, StepParams sp, int rotate, int row,
+                                                   double2 *__restrict__ partial) {
+    __shared__ uint64_t s_z[kMaxStepStrings];
+    __shared__ int s_q[kMaxStepStrings];
+    __shared__ double2 s_cs[kMaxStepStrings];
+    __shared__ double s_scale[kMaxStepStrings];
+    const int b = blockIdx.y;
+    // strings in reverse order with negated angles: the un-rotation U^dagger
+    stage_step(st, sp, b, s_z, s_q, s_cs);
+    for (int i = threadIdx.x; i < st.ns; i += blockDim.x)
+        s_scale[i] = sp.strs[st.s0 + st.ns - 1 - i].scale;
+    __syncthreads();
+    double2 *ps = psi + (uint64_t)b * nbasis;
+    double2 *sg = sig + (uint64_t)b * nbasis;
+    const uint64_t npair = nbasis >> 1;
+    const bool diag = st.h < 0;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t j0 = diag ? (p << 1) : insert0(p, st.h);
+        const uint64_t j1 = diag ? (j0 | 1ull) : (j0 ^ st.x);
+        double2 v0 = ps[j0], v1 = ps[j1], w0 = sg[j0], w1 = sg[j1];
+        // (K psi)_j = sum_i scale_i * (i ph_i(j ^ x)) psi_{j ^ x}
+        double2 k0 = make_double2(0.0, 0.0), k1 = make_double2(0.0, 0.0);
+        for (int i = 0; i < st.ns; ++i) {
+            const int qa = (s_q[i] + 1 + 2 * parity64(j0 & s_z[i])) & 3;
+            const int qb = (s_q[i] + 1 + 2 * parity64(j1 & s_z[i])) & 3;
+            const double sc = s_scale[i];
+            if (diag) {
+                const double2 r0 = c_ipow(v0, qa), r1 = c_ipow(v1, qb);
+                k0.x += sc * r0.x; k0.y += sc * r0.y;
+                k1.x += sc * r1.x; k1.y += sc * r1.y;
+            } else {
+                const double2 r1 = c_ipow(v1, qb), r0 = c_ipow(v0, qa);
+                k0.x += sc * r1.x; k0.y += sc * r1.y;
+                k1.x += sc * r0.x; k1.y += sc * r0.y;
+            }
+        }
+        acc = c_add(acc, c_add(c_cjmul(w0, k0), c_cjmul(w1, k1)));
+        if (rotate) {
+            double2 dummy;
+            for (int i = 0; i < st.ns; ++i) {
+                if (diag) {
+                    rotate_pair(v0, dummy, j0, j0, s_z[i], s_q[i], s_cs[i], true);
+                    rotate_pair(v1, dummy, j1, j1, s_z[i], s_q[i], s_cs[i], true);
+                    rotate_pair(w0, dummy, j0, j0, s_z[i], s_q[i], s_cs[i], true);
+                    rotate_pair(w1, dummy, j1, j1, s_z[i], s_q[i], s_cs[i], true);
+                } else {
+                    rotate_pair(v0, v1, j0, j1, s_z[i], s_q[i], s_cs[i], false);
+                    rotate_pair(w0, w1, j0, j1, s_z[i], s_q[i], s_cs[i], false);
+                }
+            }
+            ps[j0] = v0;
+            ps[j1] = v1;
+            sg[j0] = w0;
+            sg[j1] = w1;
+        }
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0)
+        partial[((uint64_t)row * gridDim.y + b) * gridDim.x + blockIdx.x] = acc;
+}
+
+// per-slot partial sums of conj(a) b: partial[b * gridDim.x + blockIdx.x]
+__global__ void k_vdot_rows(const double2 *__restrict__ a, const double2 *__restrict__ b,
+                            uint64_t nbasis, double2 *__restrict__ partial) {
+    const uint64_t off = (uint64_t)blockIdx.y * nbasis;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nbasis;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        acc = c_add(acc, c_cjmul(a[off + i], b[off + i]));
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) partial[(uint64_t)blockIdx.y * gridDim.x + blockIdx.x] = acc;
+}
+
+// energy[b] = Re sum_k partial[b * n + k]   (one block per slot)
+__global__ void k_energy_final(const double2 *__restrict__ partial, int n,
+                               double *__restrict__ energy) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+        acc = c_add(acc, partial[(uint64_t)blockIdx.x * n + k]);
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) energy[blockIdx.x] = acc.x;
+}
+
+// grad[b * M + mu] = 2 Re sum over mu's steps s and chunks c of
+// partial[((s * B) + b) * chunks + c].  grid = (M, B).
+__global__ void k_grad_final(const double2 *__restrict__ partial, const int2 *__restrict__ psteps,
+                             int chunks, double *__restrict__ grad) {
+    const int mu = blockIdx.x, b = blockIdx.y, B = gridDim.y, M = gridDim.x;
+    const int2 r = psteps[mu];
+    double2 acc = make_double2(0.0, 0.0);
+    for (int s = r.x; s < r.y; ++s)
+        for (int c = threadIdx.x; c < chunks; c += blockDim.x)
+            acc = c_add(acc, partial[((uint64_t)s * B + b) * chunks + c]);
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) grad[(uint64_t)b * M + mu] = 2.0 * acc.x;
+}
+
+__global__ void k_set_ref(double2 *__restrict__ psi, uint64_t nbasis, uint64_t ref, int nbatch) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nbatch) psi[(uint64_t)b * nbasis + ref] = make_double2(1.0, 0.0);
+}
+
+}  // namespace
+
+// ===========================================================================
+// host objects
+// ===========================================================================
+
+struct qfb_sum_s {
+    int64_t nterms = 0;
+    int32_t ngroups = 0;
+    int32_t nsegment = 0;
+    void *blob = nullptr;  // device: groups, terms, segment starts
+    GroupDev *d_groups = nullptr;
+    TermDev *d_terms = nullptr;
+    int32_t *d_seg_g0 = nullptr;
+    std::vector<GroupDev> h_groups;
+    std::vector<int32_t> h_seg_g0;
+};
+
+struct qfb_prog_s {
+    int64_t nstrings = 0;
+    int32_t nparam = 0;
+    void *blob = nullptr;
+    StrDev *d_strs = nullptr;
+    std::vector<StrDev> h_strs;
+    std::vector<StepDev> h_steps;
+    std::vector<int32_t> p_step0, p_step1;  // steps of each parameter (gradient)
+    bool params_contiguous = true;
+};
+
+namespace {
+
+int upload_params(const double *params, int32_t nrows, int32_t nparam, double **d_out) {
+    *d_out = nullptr;
+    const size_t n = (size_t)std::max(nrows, 1) * std::max(nparam, 1);
+    int rc = dev_alloc((void **)d_out, n * sizeof(double));
+    if (rc) return rc;
+    if (nparam > 0)
+        QFB_CUDA(cudaMemcpyAsync(*d_out, params, (size_t)nrows * nparam * sizeof(double),
+                                 cudaMemcpyHostToDevice, t_stream));
+    return QFB_OK;
+}
+
+unsigned chunks_for(uint64_t npair, int nbatch, int nrows_of_work) {
+    // enough blocks to fill every SM several times over, at least 1024 pairs each
+    const uint64_t target = (uint64_t)sm_count() * 8;
+    uint64_t per = (uint64_t)nbatch * std::max(nrows_of_work, 1);
+    uint64_t c = (target + per - 1) / per;
+    const uint64_t cap = std::max<uint64_t>(1, npair / 1024);
+    if (c > cap) c = cap;
+    if (c < 1) c = 1;
+    if (c > 65535) c = 65535;
+    return (unsigned)c;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qfb_sum_create(const qfb_pauli *paulis, const qfb_complex *coeffs, const int32_t *segment,
+                   int64_t nterms, int32_t nsegment, qfb_sum *out) {
+    if (!out) return fail(QFB_EINVAL, "qfb_sum_create: null output");
+    *out = nullptr;
+    if (nterms < 0 || (nterms > 0 && (!paulis || !coeffs)))
+        return fail(QFB_EINVAL, "qfb_sum_create: bad term arrays");
+    if (nsegment < 1) return fail(QFB_EINVAL, "qfb_sum_create: nsegment = %d < 1", nsegment);
+    if (nterms > INT32_MAX) return fail(QFB_EINVAL, "qfb_sum_create: too many terms");
+    for (int64_t t = 0; t < nterms; ++t) {
+        const int32_t sg = segment ? segment[t] : 0;
+        if (sg < 0 || sg >= nsegment)
+            return fail(QFB_EINVAL, "qfb_sum_create: term %lld has segment %d outside [0, %d)",
+                        (long long)t, sg, nsegment);
+    }
+    // group by (segment, x) in order of first appearance within each segment
+    std::vector<std::vector<int64_t>> seg_order(nsegment);
+    std::vector<std::unordered_map<uint64_t, size_t>> seg_map(nsegment);
+    std::vector<std::vector<std::vector<int64_t>>> seg_groups(nsegment);
+    for (int64_t t = 0; t < nterms; ++t) {
+        const int32_t sg = segment ? segment[t] : 0;
+        auto &m = seg_map[sg];
+        auto it = m.find(paulis[t].xmask);
+        if (it == m.end()) {
+            m.emplace(paulis[t].xmask, seg_groups[sg].size());
+            seg_groups[sg].push_back({t});
+        } else {
+            seg_groups[sg][it->second].push_back(t);
+        }
+    }
+    qfb_sum h = new qfb_sum_s;
+    h->nterms = nterms;
+    h->nsegment = nsegment;
+    std::vector<TermDev> terms;
+    terms.reserve(nterms);
+    h->h_seg_g0.push_back(0);
+    for (int32_t sg = 0; sg < nsegment; ++sg) {
+        for (auto &grp : seg_groups[sg]) {
+            GroupDev gd;
+            gd.x = paulis[grp[0]].xmask;
+            gd.h = highest_bit(gd.x);
+            gd.begin = (int32_t)terms.size();
+            bool real = true;
+            for (int64_t t : grp) {
+                const uint64_t x = paulis[t].xmask, z = paulis[t].zmask;
+                const int ny = __builtin_popcountll(x & z) & 3;
+                // c * i^ny (exact)
+                double re = coeffs[t].re, im = coeffs[t].im, r2, i2;
+                switch (ny) {
+                    case 0: r2 = re; i2 = im; break;
+                    case 1: r2 = -im; i2 = re; break;
+                    case 2: r2 = -re; i2 = -im; break;
+                    default: r2 = im; i2 = -re; break;
+                }
+                TermDev td;
+                td.z = z;
+                td.c = make_double2(r2, i2);
+                if (i2 != 0.0) real = false;
+                terms.push_back(td);
+            }
+            gd.end = (int32_t)terms.size();
+            gd.real = real ? 1 : 0;
+            h->h_groups.push_back(gd);
+        }
+        h->h_seg_g0.push_back((int32_t)h->h_groups.size());
+    }
+    h->ngroups = (int32_t)h->h_groups.size();
+    const size_t gbytes = sizeof(GroupDev) * std::max<size_t>(1, h->h_groups.size());
+    const size_t tbytes = sizeof(TermDev) * std::max<size_t>(1, terms.size());
+    const size_t sbytes = sizeof(int32_t) * h->h_seg_g0.size();
+    int rc = dev_alloc(&h->blob, gbytes + tbytes + sbytes);
+    if (rc) {
+        delete h;
+        return rc;
+    }
+    h->d_groups = (GroupDev *)h->blob;
+    h->d_terms = (TermDev *)((char *)h->blob + gbytes);
+    h->d_seg_g0 = (int32_t *)((char *)h->blob + gbytes + tbytes);
+    cudaError_t e = cudaSuccess;
+    if (!h->h_groups.empty())
+        e = cudaMemcpyAsync(h->d_groups, h->h_groups.data(), sizeof(GroupDev) * h->h_groups.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess && !terms.empty())
+        e = cudaMemcpyAsync(h->d_terms, terms.data(), sizeof(TermDev) * terms.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h->d_seg_g0, h->h_seg_g0.data(), sbytes, cudaMemcpyHostToDevice,
+                            t_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);  // host vectors may go away
+    if (e != cudaSuccess) {
+        dev_free(h->blob);
+        delete h;
+        return cuda_fail(e, "qfb_sum_create upload");
+    }
+    *out = h;
+    return QFB_OK;
+}
+
+int qfb_sum_destroy(qfb_sum h) {
+    if (!h) return QFB_OK;
+    dev_free(h->blob);
+    delete h;
+    return QFB_OK;
+}
+
+int qfb_sum_info(qfb_sum h, int64_t *nterms, int64_t *ngroups, int32_t *nsegment) {
+    if (!h) return fail(QFB_EINVAL, "qfb_sum_info: null sum");
+    if (nterms) *nterms = h->nterms;
+    if (ngroups) *ngroups = h->ngroups;
+    if (nsegment) *nsegment = h->nsegment;
+    return QFB_OK;
+}
+
+int qfb_sum_expval(qfb_sum h, qfb_state bra, qfb_state ket, qfb_complex *out) {
+    if (!h || !bra || !ket || !out) return fail(QFB_EINVAL, "qfb_sum_expval: null argument");
+    if (bra->nqubit != ket->nqubit || bra->nbatch != ket->nbatch)
+        return fail(QFB_EINVAL, "qfb_sum_expval: bra and ket shapes differ");
+    for (const auto &g : h->h_groups)
+        if (g.h >= bra->nqubit)
+            return fail(QFB_EINVAL, "qfb_sum_expval: operator acts on qubit %d of a %d-qubit state",
+                        g.h, bra->nqubit);
+    const int B = bra->nbatch;
+    const size_t nout = (size_t)B * h->nsegment;
+    if (h->ngroups == 0) {
+        for (size_t i = 0; i < nout; ++i) out[i] = qfb_complex{0.0, 0.0};
+        return QFB_OK;
+    }
+    const uint64_t npair = bra->nbasis >> 1;
+    const unsigned chunks = chunks_for(npair, B, h->ngroups);
+    const size_t nparts = (size_t)B * h->ngroups * chunks;
+    void *buf = nullptr;
+    int rc = dev_alloc(&buf, sizeof(double2) * (nparts + nout));
+    if (rc) return rc;
+    double2 *partial = (double2 *)buf;
+    double2 *res = partial + nparts;
+    for (int32_t g0 = 0; g0 < h->ngroups; g0 += 65535) {
+        // grid.y is limited to 65535 groups per launch
+        const int32_t ng = std::min<int32_t>(65535, h->ngroups - g0);
+        if (g0 == 0 && ng == h->ngroups) {
+            k_sum_expval<<<dim3(chunks, ng, B), 256, 0, t_stream>>>(
+                bra->d, ket->d, bra->nbasis, h->d_groups, h->d_terms, h->ngroups, partial);
+            QFB_LAUNCHED();
+        } else {
+            dev_free(buf);
+            return fail(QFB_ENOSYS, "qfb_sum_expval: more than 65535 x-groups");
+        }
+    }
+    k_seg_sum<<<dim3(h->nsegment, B), 256, 0, t_stream>>>(partial, h->d_seg_g0, h->ngroups,
+                                                          chunks, res);
+    QFB_LAUNCHED();
+    QFB_CUDA(cudaMemcpyAsync(out, res, sizeof(double2) * nout, cudaMemcpyDeviceToHost, t_stream));
+    dev_free(buf);
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
+int qfb_sum_apply(qfb_sum h, qfb_state dst, qfb_state src) {
+    if (!h || !dst || !src) return fail(QFB_EINVAL, "qfb_sum_apply: null argument");
+    if (dst == src) return fail(QFB_EINVAL, "qfb_sum_apply: dst and src must differ");
+    if (dst->nqubit != src->nqubit || dst->nbatch != src->nbatch)
+        return fail(QFB_EINVAL, "qfb_sum_apply: dst and src shapes differ");
+    for (const auto &g : h->h_groups)
+        if (g.h >= src->nqubit)
+            return fail(QFB_EINVAL, "qfb_sum_apply: operator acts on qubit %d of a %d-qubit state",
+                        g.h, src->nqubit);
+    const dim3 grid(grid_for(src->nbasis, 256), src->nbatch);
+    k_sum_apply<<<grid, 256, 0, t_stream>>>(dst->d, src->d, src->nbasis, h->d_groups, h->d_terms,
+                                            h->ngroups);
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
+int qfb_prog_create(const qfb_pauli *paulis, const double *scale, const int32_t *param,
+                    int64_t nstrings, int32_t nparam, qfb_prog *out) {
+    if (!out) return fail(QFB_EINVAL, "qfb_prog_create: null output");
+    *out = nullptr;
+    if (nstrings < 0 || (nstrings > 0 && (!paulis || !scale || !param)))
+        return fail(QFB_EINVAL, "qfb_prog_create: bad arrays");
+    if (nparam < 0) return fail(QFB_EINVAL, "qfb_prog_create: nparam < 0");
+    for (int64_t k = 0; k < nstrings; ++k)
+        if (param[k] < 0 || param[k] >= nparam)
+            return fail(QFB_EINVAL, "qfb_prog_create: string %lld uses parameter %d of %d",
+                        (long long)k, param[k], nparam);
+    qfb_prog p = new qfb_prog_s;
+    p->nstrings = nstrings;
+    p->nparam = nparam;
+    p->p_step0.assign(nparam, -1);
+    p->p_step1.assign(nparam, -1);
+    for (int64_t k = 0; k < nstrings; ++k) {
+        StrDev sd;
+        sd.z = paulis[k].zmask;
+        sd.ny = __builtin_popcountll(paulis[k].xmask & paulis[k].zmask) & 3;
+        sd.param = param[k];
+        sd.scale = scale[k];
+        p->h_strs.push_back(sd);
+        const bool extend = !p->h_steps.empty() && p->h_steps.back().x == paulis[k].xmask &&
+                            p->h_steps.back().param == param[k] &&
+                            p->h_steps.back().ns < kMaxStepStrings;
+        if (extend) {
+            p->h_steps.back().ns += 1;
+        } else {
+            StepDev st;
+            st.x = paulis[k].xmask;
+            st.h = highest_bit(st.x);
+            st.s0 = (int32_t)k;
+            st.ns = 1;
+            st.param = param[k];
+            p->h_steps.push_back(st);
+        }
+    }
+    // steps of each parameter must be contiguous for the reverse gradient sweep
+    for (size_t s = 0; s < p->h_steps.size(); ++s) {
+        const int32_t mu = p->h_steps[s].param;
+        if (p->p_step0[mu] < 0) {
+            p->p_step0[mu] = (int32_t)s;
+        } else if (p->p_step1[mu] != (int32_t)s) {
+            p->params_contiguous = false;
+        }
+        p->p_step1[mu] = (int32_t)s + 1;
+    }
+    int rc = dev_alloc(&p->blob, sizeof(StrDev) * std::max<size_t>(1, p->h_strs.size()));
+    if (rc) {
+        delete p;
+        return rc;
+    }
+    p->d_strs = (StrDev *)p->blob;
+    cudaError_t e = cudaSuccess;
+    if (!p->h_strs.empty())
+        e = cudaMemcpyAsync(p->d_strs, p->h_strs.data(), sizeof(StrDev) * p->h_strs.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);
+    if (e != cudaSuccess) {
+        dev_free(p->blob);
+        delete p;
+        return cuda_fail(e, "qfb_prog_create upload");
+    }
+    *out = p;
+    return QFB_OK;
+}
+
+int qfb_prog_destroy(qfb_prog p) {
+    if (!p) return QFB_OK;
+    dev_free(p->blob);
+    delete p;
+    return QFB_OK;
+}
+
+int qfb_prog_info(qfb_prog p, int64_t *nstrings, int64_t *nsteps, int32_t *nparam) {
+    if (!p) return fail(QFB_EINVAL, "qfb_prog_info: null program");
+    if (nstrings) *nstrings = p->nstrings;
+    if (nsteps) *nsteps = (int64_t)p->h_steps.size();
+    if (nparam) *nparam = p->nparam;
+    return QFB_OK;
+}
+
+static int check_prog_state(qfb_prog p, qfb_state s, int32_t nrows, const char *who) {
+    if (nrows != 1 && nrows != s->nbatch)
+        return fail(QFB_EINVAL, "%s: %d parameter rows for %d slots", who, nrows, s->nbatch);
+    for (const auto &st : p->h_steps)
+        if (st.h >= s->nqubit)
+            return fail(QFB_EINVAL, "%s: program acts on qubit %d of a %d-qubit state", who, st.h,
+                        s->nqubit);
+    for (const auto &sd : p->h_strs)
+        if (sd.z >> s->nqubit)
+            return fail(QFB_EINVAL, "%s: program acts on a qubit beyond %d", who, s->nqubit);
+    return QFB_OK;
+}
+
+// ---- enqueue helpers: kernels only, no allocation, no host synchronisation --
+
+static int enqueue_prog(const qfb_prog_s *p, double2 *psi, uint64_t nbasis, int B,
+                        const double *d_par, int bcast, int sign) {
+    StepParams sp{p->d_strs, d_par, p->nparam, bcast, sign};
+    const dim3 grid(grid_for(nbasis >> 1, 256, 4), B);
+    const int64_t ns = (int64_t)p->h_steps.size();
+    for (int64_t k = 0; k < ns; ++k) {
+        const StepDev &st = p->h_steps[sign > 0 ? k : ns - 1 - k];
+        k_prog_step<<<grid, 256, 0, t_stream>>>(psi, nbasis, st, sp);
+        QFB_LAUNCHED();
+    }
+    return QFB_OK;
+}
+
+static int enqueue_sum_apply(const qfb_sum_s *h, double2 *dst, const double2 *src,
+                             uint64_t nbasis, int B) {
+    const dim3 grid(grid_for(nbasis, 256), B);
+    k_sum_apply<<<grid, 256, 0, t_stream>>>(dst, src, nbasis, h->d_groups, h->d_terms,
+                                            h->ngroups);
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
+// Reverse sweep of the adjoint gradient.  partial holds nsteps * B * chunks
+// entries; row (s * B + b) receives step s's share of <sigma|K_mu|psi>.
+static int enqueue_gradient(const qfb_prog_s *kp, double2 *psi, double2 *sig, uint64_t nbasis,
+                            int B, const double *d_par, int bcast, double2 *partial,
+                            unsigned chunks) {
+    const int M = kp->nparam;
+    StepParams sp{kp->d_strs, d_par, M, bcast, -1};
+    const dim3 grid(chunks, B);
+    for (int mu = M - 1; mu >= 0; --mu) {
+        const int32_t s0 = kp->p_step0[mu], s1 = kp->p_step1[mu];
+        if (s0 < 0) continue;  // parameter without strings: gradient 0
+        const bool last = (mu == 0);
+        if (s1 - s0 == 1) {
+            k_grad_step<<<grid, 256, 0, t_stream>>>(psi, sig, nbasis, kp->h_steps[s0], sp,
+                                                    last ? 0 : 1, s0, partial);
+            QFB_LAUNCHED();
+            continue;
+        }
+        // several x-groups: first every inner product on (psi_mu, sigma_mu) ...
+        for (int32_t s = s0; s < s1; ++s) {
+            k_grad_step<<<grid, 256, 0, t_stream>>>(psi, sig, nbasis, kp->h_steps[s], sp, 0, s,
+                                                    partial);
+            QFB_LAUNCHED();
+        }
+        if (last) continue;
+        // ... then U_mu^dagger on both states, steps in reverse order
+        const dim3 g2(grid_for(nbasis >> 1, 256, 4), B);
+        for (int32_t s = s1 - 1; s >= s0; --s) {
+            k_prog_step<<<g2, 256, 0, t_stream>>>(psi, nbasis, kp->h_steps[s], sp);
+            QFB_LAUNCHED();
+            k_prog_step<<<g2, 256, 0, t_stream>>>(sig, nbasis, kp->h_steps[s], sp);
+            QFB_LAUNCHED();
+        }
+    }
+    return QFB_OK;
+}
+
+int qfb_prog_apply(qfb_prog p, qfb_state s, const double *params, int32_t nrows, int32_t sign) {
+    if (!p || !s) return fail(QFB_EINVAL, "qfb_prog_apply: null argument");
+    if (p->nparam > 0 && !params) return fail(QFB_EINVAL, "qfb_prog_apply: null parameters");
+    if (sign != 1 && sign != -1) return fail(QFB_EINVAL, "qfb_prog_apply: sign must be +1 or -1");
+    int rc = check_prog_state(p, s, nrows, "qfb_prog_apply");
+    if (rc) return rc;
+    if (p->h_steps.empty()) return QFB_OK;
+    double *d_par = nullptr;
+    rc = upload_params(params, nrows, p->nparam, &d_par);
+    if (rc) return rc;
+    rc = enqueue_prog(p, s->d, s->nbasis, s->nbatch, d_par, nrows == 1 ? 1 : 0, sign);
+    dev_free(d_par);
+    return rc;
+}
+
+int qfb_ucc_gradient(qfb_prog kp, qfb_state psi, qfb_state sig, const double *params,
+                     int32_t nrows, double *grad) {
+    if (!kp || !psi || !sig || !grad) return fail(QFB_EINVAL, "qfb_ucc_gradient: null argument");
+    if (kp->nparam > 0 && !params) return fail(QFB_EINVAL, "qfb_ucc_gradient: null parameters");
+    if (psi->nqubit != sig->nqubit || psi->nbatch != sig->nbatch)
+        return fail(QFB_EINVAL, "qfb_ucc_gradient: psi and sigma shapes differ");
+    if (psi == sig) return fail(QFB_EINVAL, "qfb_ucc_gradient: psi and sigma must differ");
+    if (!kp->params_contiguous)
+        return fail(QFB_EINVAL, "qfb_ucc_gradient: each parameter's strings must be contiguous");
+    int rc = check_prog_state(kp, psi, nrows, "qfb_ucc_gradient");
+    if (rc) return rc;
+    const int M = kp->nparam, B = psi->nbatch;
+    if (M == 0) return QFB_OK;
+    double *d_par = nullptr;
+    rc = upload_params(params, nrows, M, &d_par);
+    if (rc) return rc;
+    const unsigned chunks = chunks_for(psi->nbasis >> 1, B, 1);
+    const size_t nrow = (size_t)std::max<size_t>(kp->h_steps.size(), 1) * B;
+    void *buf = nullptr;
+    rc = dev_alloc(&buf, sizeof(double2) * nrow * chunks + sizeof(double) * (size_t)B * M +
+                             sizeof(int2) * M);
+    if (rc) {
+        dev_free(d_par);
+        return rc;
+    }
+    double2 *partial = (double2 *)buf;
+    double *d_grad = (double *)(partial + nrow * chunks);
+    int2 *d_ps = (int2 *)(d_grad + (size_t)B * M);
+    std::vector<int2> ps(M);
+    for (int mu = 0; mu < M; ++mu)
+        ps[mu] = make_int2(std::max(kp->p_step0[mu], 0), std::max(kp->p_step1[mu], 0));
+    QFB_CUDA(cudaMemcpyAsync(d_ps, ps.data(), sizeof(int2) * M, cudaMemcpyHostToDevice, t_stream));
+    rc = enqueue_gradient(kp, psi->d, sig->d, psi->nbasis, B, d_par, nrows == 1 ? 1 : 0, partial,
+                          chunks);
+    if (rc == QFB_OK) {
+        k_grad_final<<<dim3(M, B), 128, 0, t_stream>>>(partial, d_ps, chunks, d_grad);
+        QFB_LAUNCHED();
+        QFB_CUDA(cudaMemcpyAsync(grad, d_grad, sizeof(double) * (size_t)B * M,
+                                 cudaMemcpyDeviceToHost, t_stream));
+    }
+    dev_free(buf);
+    dev_free(d_par);
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return rc;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// compiled dUCC evaluator
+// ===========================================================================
+
+struct qfb_ucc_s {
+    const qfb_prog_s *fwd = nullptr;
+    const qfb_prog_s *grad = nullptr;
+    const qfb_sum_s *ham = nullptr;
+    int nqubit = 0, nbatch = 0, nparam = 0;
+    uint64_t nbasis = 0, ref = 0;
+    unsigned vchunks = 1, gchunks = 1;
+    void *blob = nullptr;
+    double2 *psi = nullptr, *sig = nullptr;
+    double *params = nullptr, *energy = nullptr, *gradv = nullptr;
+    double2 *vpart = nullptr, *gpart = nullptr;
+    int2 *psteps = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    uint64_t graph_kernels[2] = {0, 0};
+};
+
+static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
+    const int B = u->nbatch;
+    int rc = QFB_OK;
+    switch (stage) {
+        case 0:
+            QFB_CUDA(cudaMemsetAsync(u->psi, 0, sizeof(double2) * u->nbasis * B, t_stream));
+            k_set_ref<<<(B + 127) / 128, 128, 0, t_stream>>>(u->psi, u->nbasis, u->ref, B);
+            QFB_LAUNCHED();
+            break;
+        case 1:
+            rc = enqueue_prog(u->fwd, u->psi, u->nbasis, B, u->params, 0, 1);
+            break;
+        case 2:
+            rc = enqueue_sum_apply(u->ham, u->sig, u->psi, u->nbasis, B);
+            if (rc) return rc;
+            k_vdot_rows<<<dim3(u->vchunks, B), 256, 0, t_stream>>>(u->psi, u->sig, u->nbasis,
+                                                                 u->vpart);
+            QFB_LAUNCHED();
+            k_energy_final<<<B, 128, 0, t_stream>>>(u->vpart, u->vchunks, u->energy);
+            QFB_LAUNCHED();
+            break;
+        default:
+            if (with_grad && u->grad && u->nparam > 0) {
+                rc = enqueue_gradient(u->grad, u->psi, u->sig, u->nbasis, B, u->params, 0,
+                                      u->gpart, u->gchunks);
+                if (rc) return rc;
+                k_grad_final<<<dim3(u->nparam, B), 128, 0, t_stream>>>(u->gpart, u->psteps,
+                                                                     u->gchunks, u->gradv);
+                QFB_LAUNCHED();
+            }
+            break;
+    }
+    return rc;
+}
+
+static int ucc_enqueue(qfb_ucc u, int with_grad) {
+    for (int st = 0; st < 4; ++st) {
+        int rc = ucc_stage(u, st, with_grad);
+        if (rc) return rc;
+    }
+    return QFB_OK;
+}
+
+extern "C" {
+
+int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_sum ham, int nqubit, uint64_t ref_index,
+                   int nbatch, qfb_ucc *out) {
+    if (!out) return fail(QFB_EINVAL, "qfb_ucc_create: null output");
+    *out = nullptr;
+    if (!fprog || !ham) return fail(QFB_EINVAL, "qfb_ucc_create: null program or Hamiltonian");
+    if (nqubit < 1 || nqubit > 40 || nbatch < 1)
+        return fail(QFB_EINVAL, "qfb_ucc_create: nqubit = %d, nbatch = %d", nqubit, nbatch);
+    if (ref_index >> nqubit) return fail(QFB_EINVAL, "qfb_ucc_create: reference index too large");
+    if (gprog && (gprog->nparam != fprog->nparam || !gprog->params_contiguous))
+        return fail(QFB_EINVAL, "qfb_ucc_create: gradient program does not match the ansatz");
+    for (const auto &g : ham->h_groups)
+        if (g.h >= nqubit) return fail(QFB_EINVAL, "qfb_ucc_create: H acts beyond qubit %d", nqubit);
+    for (const qfb_prog_s *p : {static_cast<const qfb_prog_s *>(fprog),
+                                static_cast<const qfb_prog_s *>(gprog)}) {
+        if (!p) continue;
+        for (const auto &st : p->h_steps)
+            if (st.h >= nqubit) return fail(QFB_EINVAL, "qfb_ucc_create: program beyond qubit");
+        for (const auto &sd : p->h_strs)
+            if (sd.z >> nqubit) return fail(QFB_EINVAL, "qfb_ucc_create: program beyond qubit");
+    }
+    qfb_ucc u = new qfb_ucc_s;
+    u->fwd = fprog;
+    u->grad = gprog;
+    u->ham = ham;
+    u->nqubit = nqubit;
+    u->nbatch = nbatch;
+    u->nparam = fprog->nparam;
+    u->nbasis = 1ull << nqubit;
+    u->ref = ref_index;
+    u->vchunks = grid_for(u->nbasis, 256, 2);
+    if (u->vchunks * (unsigned)nbatch > 65535u) u->vchunks = std::max(1u, 65535u / nbatch);
+    u->gchunks = chunks_for(u->nbasis >> 1, nbatch, 1);
+    const size_t B = nbatch, M = std::max(u->nparam, 1);
+    const size_t nsteps = gprog ? std::max<size_t>(gprog->h_steps.size(), 1) : 1;
+    const size_t b_state = sizeof(double2) * u->nbasis * B;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += (bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_psi = take(b_state), o_sig = take(b_state);
+    const size_t o_par = take(sizeof(double) * B * M), o_en = take(sizeof(double) * B);
+    const size_t o_gr = take(sizeof(double) * B * M);
+    const size_t o_vp = take(sizeof(double2) * B * u->vchunks);
+    const size_t o_gp = take(gprog ? sizeof(double2) * nsteps * B * u->gchunks : 16);
+    const size_t o_ps = take(sizeof(int2) * M);
+    int rc = dev_alloc(&u->blob, off);
+    if (rc) {
+        delete u;
+        return rc;
+    }
+    char *base = (char *)u->blob;
+    u->psi = (double2 *)(base + o_psi);
+    u->sig = (double2 *)(base + o_sig);
+    u->params = (double *)(base + o_par);
+    u->energy = (double *)(base + o_en);
+    u->gradv = (double *)(base + o_gr);
+    u->vpart = (double2 *)(base + o_vp);
+    u->gpart = (double2 *)(base + o_gp);
+    u->psteps = (int2 *)(base + o_ps);
+    std::vector<int2> ps(M, make_int2(0, 0));
+    if (gprog)
+        for (int mu = 0; mu < gprog->nparam; ++mu)
+            ps[mu] = make_int2(std::max(gprog->p_step0[mu], 0), std::max(gprog->p_step1[mu], 0));
+    cudaError_t e = cudaMemsetAsync(u->blob, 0, off, t_stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(u->psteps, ps.data(), sizeof(int2) * M, cudaMemcpyHostToDevice,
+                            t_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&u->cap_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        dev_free(u->blob);
+        delete u;
+        return cuda_fail(e, "qfb_ucc_create");
+    }
+    *out = u;
+    return QFB_OK;
+}
+
+int qfb_ucc_destroy(qfb_ucc u) {
+    if (!u) return QFB_OK;
+    for (auto &x : u->exec)
+        if (x) cudaGraphExecDestroy(x);
+    if (u->cap_stream) cudaStreamDestroy(u->cap_stream);
+    dev_free(u->blob);
+    delete u;
+    return QFB_OK;
+}
+
+int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_grad) {
+    if (!u) return fail(QFB_EINVAL, "qfb_ucc_buffers: null evaluator");
+    if (d_params) *d_params = u->params;
+    if (d_energy) *d_energy = u->energy;
+    if (d_grad) *d_grad = u->gradv;
+    return QFB_OK;
+}
+
+int qfb_ucc_run(qfb_ucc u, int with_grad) {
+    if (!u) return fail(QFB_EINVAL, "qfb_ucc_run: null evaluator");
+    const int k = with_grad ? 1 : 0;
+    if (u->exec[k]) {
+        QFB_CUDA(cudaGraphLaunch(u->exec[k], t_stream));
+        g_launches.fetch_add(u->graph_kernels[k], std::memory_order_relaxed);
+        return QFB_OK;
+    }
+    return ucc_enqueue(u, with_grad);
+}
+
+int qfb_ucc_capture(qfb_ucc u, int with_grad) {
+    if (!u) return fail(QFB_EINVAL, "qfb_ucc_capture: null evaluator");
+    const int k = with_grad ? 1 : 0;
+    if (u->exec[k]) return QFB_OK;
+    cudaStream_t saved = t_stream;
+    t_stream = u->cap_stream;
+    const uint64_t n0 = g_launches.load();
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(u->cap_stream, cudaStreamCaptureModeThreadLocal);
+    int rc = (e == cudaSuccess) ? ucc_enqueue(u, with_grad) : cuda_fail(e, "begin capture");
+    cudaError_t e2 = cudaStreamEndCapture(u->cap_stream, &graph);
+    t_stream = saved;
+    const uint64_t nk = g_launches.load() - n0;
+    g_launches.fetch_sub(nk, std::memory_order_relaxed);  // counted when replayed
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e2 != cudaSuccess) return cuda_fail(e2, "end capture");
+    e = cudaGraphInstantiate(&u->exec[k], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        u->exec[k] = nullptr;
+        return cuda_fail(e, "graph instantiate");
+    }
+    u->graph_kernels[k] = nk;
+    return QFB_OK;
+}
+
+int qfb_ucc_eval(qfb_ucc u, const double *params, double *energy, double *grad) {
+    if (!u || !energy) return fail(QFB_EINVAL, "qfb_ucc_eval: null argument");
+    if (u->nparam > 0 && !params) return fail(QFB_EINVAL, "qfb_ucc_eval: null parameters");
+    const size_t np = (size_t)u->nbatch * u->nparam;
+    if (np) QFB_CUDA(cudaMemcpyAsync(u->params, params, sizeof(double) * np,
+                                     cudaMemcpyHostToDevice, t_stream));
+    int rc = qfb_ucc_run(u, grad ? 1 : 0);
+    if (rc) return rc;
+    QFB_CUDA(cudaMemcpyAsync(energy, u->energy, sizeof(double) * u->nbatch,
+                             cudaMemcpyDeviceToHost, t_stream));
+    if (grad && np)
+        QFB_CUDA(cudaMemcpyAsync(grad, u->gradv, sizeof(double) * np, cudaMemcpyDeviceToHost,
+                                 t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
+int qfb_ucc_profile(qfb_ucc u, int with_grad, int reps, double *stage_ms,
+                    int64_t *stage_launches) {
+    if (!u || !stage_ms || reps < 1) return fail(QFB_EINVAL, "qfb_ucc_profile: bad argument");
+    cudaEvent_t ev[5];
+    for (auto &e : ev) QFB_CUDA(cudaEventCreate(&e));
+    double acc[4] = {0, 0, 0, 0};
+    int64_t nl[4] = {0, 0, 0, 0};
+    int rc = QFB_OK;
+    for (int r = 0; r < reps && rc == QFB_OK; ++r) {
+        QFB_CUDA(cudaEventRecord(ev[0], t_stream));
+        for (int st = 0; st < 4 && rc == QFB_OK; ++st) {
+            const uint64_t l0 = g_launches.load();
+            rc = ucc_stage(u, st, with_grad);
+            nl[st] = (int64_t)(g_launches.load() - l0);
+            QFB_CUDA(cudaEventRecord(ev[st + 1], t_stream));
+        }
+        QFB_CUDA(cudaEventSynchronize(ev[4]));
+        for (int st = 0; st < 4; ++st) {
+            float ms = 0.f;
+            QFB_CUDA(cudaEventElapsedTime(&ms, ev[st], ev[st + 1]));
+            acc[st] += ms;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (int st = 0; st < 4; ++st) {
+        stage_ms[st] = acc[st] / reps;
+        if (stage_launches) stage_launches[st] = nl[st];
+    }
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,517 @@
+"""dUCC energies and gradients on the device.
+
+``DUCC`` compiles one problem -- Hamiltonian, operator pool, selected
+operators, reference determinant -- into two device programs and a grouped
+Hamiltonian, then evaluates, for one parameter vector or a batch of them:
+
+* ``energy``       <Phi|U(t)^dagger H U(t)|Phi>
+                   (AnsatzAlgorithm.energy_feval, abc/algorithm.py:458-474)
+* ``energy_grad``  the energy and the adjoint gradient
+                   (UCCVQE.measure_gradient, abc/uccvqeabc.py:122-251)
+* ``pool_gradients``  2 Re <H psi|K_k psi> for every pool operator
+                   (UCCVQE.measure_gradient3, abc/uccvqeabc.py:253-283)
+
+The forward program holds, per selected operator mu, the JW strings of
+t_mu * tau_mu in the order ``get_qubit_operator('commuting_grp_lex')``
+gives them (abc/ansatz.py:25-82, sq_op_pool.cc:97-104); the gradient program
+holds K_mu = c_mu * JW(tau_mu) in ``jw_transform`` order.  The strings of one
+excitation share their x-mask, so each excitation is one fused pass.
+
+``UCCNVQE`` and ``ADAPTVQE`` are thin drivers with the reference's
+energy/gradient entry points.  ``engine='percall'`` runs the same numbers
+through the public ``Computer`` API call for call as the reference's
+drivers do (state copies, apply_operator, vdot per parameter) -- the plain
+per-call path the fused engine is compared against.
+"""
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, ptr
+from .circuit import Circuit
+from .computer import Computer, _new_state, inner_product
+from .device import prog_from_strings, sum_from_terms
+from .sq_op_pool import SQOpPool
+from .sq_operator import SQOperator
+from .utils import build_refprep, ref_to_basis_idx, trotterize
+
+__all__ = ["DUCC", "Evaluator", "UCCNVQE", "ADAPTVQE", "ansatz_strings", "gradient_strings"]
+
+
+class Evaluator:
+    """A qfb_ucc evaluator: ``nbatch`` parameter rows per run, its own psi and
+    sigma states, device parameter/output blocks and reduction scratch; one
+    run is captured into a CUDA graph and replayed."""
+
+    def __init__(self, ducc, nbatch, capture=True):
+        self._ducc = ducc  # keeps the programs and the Hamiltonian alive
+        self.nbatch = int(nbatch)
+        self.nparam = ducc.nparam
+        h = ctypes.c_void_p()
+        check(lib().qfb_ucc_create(ducc.fwd.h, ducc.grad_prog.h, ducc.H.h, ducc.nqubit,
+                                   ducc.ref_index, self.nbatch, ctypes.byref(h)), "qfb_ucc_create")
+        self.h = h
+        dp, de, dg = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        check(lib().qfb_ucc_buffers(h, ctypes.byref(dp), ctypes.byref(de), ctypes.byref(dg)))
+        self.d_params, self.d_energy, self.d_grad = dp.value, de.value, dg.value
+        self.capture = capture
+        self._captured = set()
+
+    def _ensure_graph(self, with_grad):
+        if self.capture and with_grad not in self._captured:
+            check(lib().qfb_ucc_capture(self.h, int(with_grad)), "qfb_ucc_capture")
+            self._captured.add(with_grad)
+
+    def eval(self, P, with_grad=True):
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        if P.shape != (self.nbatch, self.nparam):
+            raise ValueError(f"parameters of shape {P.shape}, expected "
+                             f"{(self.nbatch, self.nparam)}")
+        self._ensure_graph(with_grad)
+        e = np.empty(self.nbatch)
+        g = np.empty((self.nbatch, self.nparam)) if with_grad else None
+        check(lib().qfb_ucc_eval(self.h, ptr(P), ptr(e), None if g is None else ptr(g)),
+              "qfb_ucc_eval")
+        return e, g
+
+    def run(self, with_grad=True):
+        """Enqueue one evaluation on the current stream (device buffers in and
+        out, no host synchronisation)."""
+        self._ensure_graph(with_grad)
+        check(lib().qfb_ucc_run(self.h, int(with_grad)), "qfb_ucc_run")
+
+    def tensors(self):
+        """(params, energy, grad) as torch float64 CUDA views of the device blocks."""
+        import torch
+
+        def view(addr, shape):
+            class _I:
+                __cuda_array_interface__ = {"shape": shape, "typestr": "<f8",
+                                            "data": (int(addr), False), "version": 2}
+            return torch.as_tensor(_I(), device="cuda")
+
+        return (view(self.d_params, (self.nbatch, self.nparam)),
+                view(self.d_energy, (self.nbatch,)),
+                view(self.d_grad, (self.nbatch, self.nparam)))
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().qfb_ucc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def _sa_components(op):
+    """sa_SD operator -> its component anti-Hermitian excitations
+    (abc/ansatz.py:38-55)."""
+    terms = op.terms()
+    half = len(terms) // 2
+    out = []
+    for coeff, cr, ann in terms[:half]:
+        s = SQOperator()
+        s.add_term(coeff, cr, ann)
+        s.add_term(-coeff, ann, cr)
+        out.append(s)
+    return out
+
+
+def _strings_of(qo, who):
+    xs, zs, sc = [], [], []
+    for c, circ in qo.terms():
+        m = circ._pauli_masks()
+        if m is None:
+            raise ValueError(f"{who}: non-Pauli term")
+        x, z, e = m
+        if e:
+            raise ValueError(f"{who}: non-canonical Pauli term")
+        c = complex(c)
+        if abs(c.real) > 1.0e-14:
+            raise ValueError(f"exponentiate_pauli_string() called with a real coefficient {c}")
+        xs.append(x)
+        zs.append(z)
+        sc.append(c.imag)
+    return xs, zs, sc
+
+
+def ansatz_strings(pool, tops, pool_type=None, qubit_excitations=False):
+    """(x, z, scale, param) of U(t) = prod_mu exp(t_mu K_mu) in application order."""
+    X, Z, S, P = [], [], [], []
+    for mu, top in enumerate(tops):
+        op = pool[top][1]
+        comps = _sa_components(op) if pool_type == "sa_SD" else [op]
+        for comp in comps:
+            child = SQOperator()
+            child.add_op(comp)
+            q = child.jw_transform(qubit_excitations)
+            q.simplify()
+            q.order_terms()
+            xs, zs, sc = _strings_of(q, "ansatz")
+            X += xs
+            Z += zs
+            S += sc
+            P += [mu] * len(sc)
+    return X, Z, S, P
+
+
+def gradient_strings(pool, tops, qubit_excitations=False):
+    """(x, z, scale, param) of K_mu = c_mu JW(tau_mu) (uccvqeabc.py:154-157, :176-179)."""
+    X, Z, S, P = [], [], [], []
+    for mu, top in enumerate(tops):
+        c, op = pool[top]
+        child = SQOperator()
+        child.add_op(op)
+        q = child.jw_transform(qubit_excitations)
+        q.mult_coeffs(c)
+        xs, zs, sc = _strings_of(q, "gradient")
+        X += xs
+        Z += zs
+        S += sc
+        P += [mu] * len(sc)
+    return X, Z, S, P
+
+
+class DUCC:
+    """A compiled dUCC problem; evaluations take [nparam] or [batch, nparam]."""
+
+    def __init__(self, hamiltonian, pool, tops, ref, pool_type=None, qubit_excitations=False,
+                 nqubit=None):
+        self.nqubit = int(nqubit if nqubit is not None else len(ref))
+        self.ref = list(ref)
+        self.ref_index = ref_to_basis_idx(ref)
+        self.tops = list(tops)
+        self.nparam = len(self.tops)
+        pt = hamiltonian._pauli_terms(applied=True)
+        if pt is None:
+            raise ValueError("DUCC: the Hamiltonian must be a sum of Pauli strings")
+        self.H = sum_from_terms(pt)
+        if self.H.maxbit > self.nqubit:
+            raise ValueError("Hamiltonian acts beyond the reference's qubits")
+        fx, fz, fs, fp = ansatz_strings(pool, self.tops, pool_type, qubit_excitations)
+        self.fwd = prog_from_strings(fx, fz, fs, fp, self.nparam)
+        gx, gz, gs, gp = gradient_strings(pool, self.tops, qubit_excitations)
+        self.grad_prog = prog_from_strings(gx, gz, gs, gp, self.nparam)
+        self._pool = pool
+        self._qe = qubit_excitations
+        self._pool_sum = None
+        self._evals = {}
+
+    def evaluator(self, nbatch, capture=True):
+        """The batched, graph-captured evaluator for ``nbatch`` parameter rows."""
+        ev = self._evals.get(nbatch)
+        if ev is None:
+            ev = Evaluator(self, nbatch, capture)
+            if len(self._evals) >= 4:
+                self._evals.pop(next(iter(self._evals)))
+            self._evals[nbatch] = ev
+        return ev
+
+    # ---- states ----------------------------------------------------------
+    def _prepare(self, params):
+        P = np.ascontiguousarray(np.atleast_2d(np.asarray(params, dtype=np.float64)))
+        if P.shape[1] != self.nparam:
+            raise ValueError(f"expected {self.nparam} parameters, got {P.shape[1]}")
+        B = P.shape[0]
+        psi = _new_state(self.nqubit, B)
+        try:
+            idx = np.array([self.ref_index], dtype=np.uint64)
+            one = np.array([1.0 + 0j])
+            for b in range(B):
+                check(lib().qfb_state_set_basis(psi, b, ptr(idx), ptr(one), 1))
+            if self.nparam:
+                check(lib().qfb_prog_apply(self.fwd.h, psi, ptr(P), B, 1), "ansatz")
+        except Exception:
+            lib().qfb_state_destroy(psi)
+            raise
+        return psi, P, B
+
+    def state(self, params):
+        """U(t)|ref> as a Computer (first parameter row)."""
+        psi, P, B = self._prepare(np.atleast_2d(params)[:1])
+        qc = Computer.__new__(Computer)
+        qc._h, qc._n, qc._thr, qc._timings = psi, self.nqubit, 1e-6, []
+        return qc
+
+    # ---- evaluations -----------------------------------------------------
+    def energy(self, params):
+        P = np.ascontiguousarray(np.atleast_2d(np.asarray(params, dtype=np.float64)))
+        if P.shape[1] != self.nparam:
+            raise ValueError(f"expected {self.nparam} parameters, got {P.shape[1]}")
+        e, _ = self.evaluator(P.shape[0]).eval(P, with_grad=False)
+        return float(e[0]) if np.ndim(params) == 1 else e
+
+    def energy_grad(self, params):
+        P = np.ascontiguousarray(np.atleast_2d(np.asarray(params, dtype=np.float64)))
+        if P.shape[1] != self.nparam:
+            raise ValueError(f"expected {self.nparam} parameters, got {P.shape[1]}")
+        e, g = self.evaluator(P.shape[0]).eval(P, with_grad=True)
+        if np.ndim(params) == 1:
+            return float(e[0]), g[0]
+        return e, g
+
+    def energy_grad_percall(self, params):
+        """The same numbers through the per-call C ABI (one call per stage)."""
+        psi, P, B = self._prepare(params)
+        sig = None
+        try:
+            sig = _new_state(self.nqubit, B)
+            check(lib().qfb_sum_apply(self.H.h, sig, psi), "H psi")
+            ev = np.zeros(B, dtype=np.complex128)
+            check(lib().qfb_vdot(psi, sig, ptr(ev)), "energy")
+            g = np.zeros((B, self.nparam))
+            if self.nparam:
+                check(lib().qfb_ucc_gradient(self.grad_prog.h, psi, sig, ptr(P), B, ptr(g)),
+                      "gradient")
+        finally:
+            lib().qfb_state_destroy(psi)
+            if sig is not None:
+                lib().qfb_state_destroy(sig)
+        if np.ndim(params) == 1:
+            return float(ev.real[0]), g[0]
+        return ev.real, g
+
+    def _pool_sum_handle(self):
+        if self._pool_sum is None:
+            terms, seg = [], []
+            for k, (c, op) in enumerate(self._pool):
+                child = SQOperator()
+                child.add_op(op)
+                q = child.jw_transform(self._qe)
+                q.mult_coeffs(c)
+                pt = q._pauli_terms(applied=True)
+                terms += pt
+                seg += [k] * len(pt)
+            self._pool_sum = sum_from_terms(terms, seg, len(self._pool))
+        return self._pool_sum
+
+    def pool_gradients(self, params):
+        """2 Re <H psi | K_k psi> for every operator of the pool, one launch."""
+        ps = self._pool_sum_handle()
+        psi, P, B = self._prepare(params)
+        sig = None
+        try:
+            sig = _new_state(self.nqubit, B)
+            check(lib().qfb_sum_apply(self.H.h, sig, psi), "H psi")
+            out = np.zeros(B * ps.nsegment, dtype=np.complex128)
+            check(lib().qfb_sum_expval(ps.h, sig, psi, ptr(out)), "pool gradients")
+        finally:
+            lib().qfb_state_destroy(psi)
+            if sig is not None:
+                lib().qfb_state_destroy(sig)
+        g = 2.0 * out.real.reshape(B, ps.nsegment)
+        return g[0] if np.ndim(params) == 1 else g
+
+
+# ---------------------------------------------------------------------------
+# drivers
+# ---------------------------------------------------------------------------
+
+
+class _UCCBase:
+    def __init__(self, system, reference=None, pool_type="SD", qubit_excitations=False,
+                 engine="fused", trotter_number=1):
+        self._sys = system
+        self._ref = list(system.hf_reference if reference is None else reference)
+        self._nqb = len(self._ref)
+        self._qb_ham = system.hamiltonian
+        self._pool_type = pool_type
+        self._qubit_excitations = qubit_excitations
+        self._engine = engine
+        self._trotter_number = trotter_number
+        self._refprep = build_refprep(self._ref)
+        self._Uprep = Circuit(self._refprep)
+        self._tops = []
+        self._tamps = []
+        self._pool_obj = SQOpPool()
+        self._ducc = None
+        self._ducc_key = None
+        self._curr_energy = 0.0
+
+    def fill_pool(self):
+        if isinstance(self._pool_type, SQOpPool):
+            self._pool_obj = self._pool_type
+            return
+        self._pool_obj = SQOpPool()
+        irr = getattr(self._sys, "orb_irreps_to_int", None)
+        self._pool_obj.set_orb_spaces(self._ref, irr or [])
+        self._pool_obj.fill_pool(self._pool_type)
+
+    def _engine_for_tops(self):
+        key = tuple(self._tops)
+        if self._ducc is None or self._ducc_key != key:
+            pt = self._pool_type if isinstance(self._pool_type, str) else None
+            self._ducc = DUCC(self._qb_ham, self._pool_obj, self._tops, self._ref, pt,
+                              self._qubit_excitations, self._nqb)
+            self._ducc_key = key
+        return self._ducc
+
+    # ---- the reference's circuit path (abc/ansatz.py:25-82) ----------------
+    def ansatz_circuit(self, amplitudes=None):
+        tamps = self._tamps if amplitudes is None else amplitudes
+        temp = SQOpPool()
+        if self._pool_type == "sa_SD":
+            for t, top in zip(tamps, self._tops):
+                for comp in _sa_components(self._pool_obj[top][1]):
+                    temp.add(t, comp)
+        else:
+            for t, top in zip(tamps, self._tops):
+                temp.add(t, self._pool_obj[top][1])
+        A = temp.get_qubit_operator("commuting_grp_lex", qubit_excitations=self._qubit_excitations)
+        U, phase = trotterize(A, trotter_number=self._trotter_number)
+        if phase != 1.0 + 0.0j:
+            raise ValueError("Encountered phase change, phase not equal to (1.0 + 0.0i)")
+        return U
+
+    def build_Uvqc(self, amplitudes=None):
+        U = self.ansatz_circuit(amplitudes)
+        Uvqc = Circuit()
+        Uvqc.add(self._Uprep)
+        Uvqc.add(U)
+        return Uvqc
+
+    def measure_energy(self, Ucirc, computer=None):
+        if computer is None:
+            computer = Computer(self._nqb)
+        computer.apply_circuit(Ucirc)
+        val = computer.direct_op_exp_val(self._qb_ham)
+        return float(np.real(val))
+
+    # ---- entry points ------------------------------------------------------
+    def energy_feval(self, params):
+        if self._engine == "fused":
+            e = self._engine_for_tops().energy(np.asarray(params, dtype=np.float64))
+        else:
+            e = self.measure_energy(self.build_Uvqc(amplitudes=list(params)))
+        self._curr_energy = e
+        return e
+
+    def measure_gradient(self, params=None):
+        p = np.asarray(self._tamps if params is None else params, dtype=np.float64)
+        if self._engine == "fused":
+            return self._engine_for_tops().energy_grad(p)[1]
+        return self._measure_gradient_percall(p)
+
+    def gradient_ary_feval(self, params):
+        return np.asarray(self.measure_gradient(params))
+
+    def measure_gradient3(self):
+        p = np.asarray(self._tamps, dtype=np.float64)
+        if self._engine == "fused":
+            return self._engine_for_tops().pool_gradients(p)
+        Utot = self.build_Uvqc()
+        qc_psi = Computer(self._nqb)
+        qc_psi.apply_circuit(Utot)
+        qc_sig = Computer(qc_psi)
+        qc_sig.apply_operator(self._qb_ham)
+        grads = np.zeros(len(self._pool_obj))
+        for mu, (coeff, operator) in enumerate(self._pool_obj):
+            qc_temp = Computer(qc_psi)
+            op = SQOperator()
+            op.add_op(operator)
+            K = op.jw_transform(self._qubit_excitations)
+            K.mult_coeffs(coeff)
+            qc_temp.apply_operator(K)
+            grads[mu] = 2.0 * np.real(np.vdot(qc_sig.get_coeff_vec(), qc_temp.get_coeff_vec()))
+        return grads
+
+    def _measure_gradient_percall(self, params):
+        """uccvqeabc.py:122-251 through the Computer API, call for call."""
+        M = len(self._tamps)
+        grads = np.zeros(M)
+        Utot = self.build_Uvqc(list(params))
+        qc_psi = Computer(self._nqb)
+        qc_psi.apply_circuit(Utot)
+        qc_sig = Computer(qc_psi)
+        qc_sig.apply_operator(self._qb_ham)
+        qc_temp = Computer(qc_psi)
+        mu = M - 1
+
+        def K(m):
+            c, op = self._pool_obj[self._tops[m]]
+            s = SQOperator()
+            s.add_op(op)
+            q = s.jw_transform(self._qubit_excitations)
+            q.mult_coeffs(c)
+            return q
+
+        Kmu_prev = K(mu)
+        qc_temp.apply_operator(Kmu_prev)
+        grads[mu] = 2.0 * np.real(np.vdot(qc_sig.get_coeff_vec(), qc_temp.get_coeff_vec()))
+        for mu in reversed(range(M - 1)):
+            tamp = params[mu + 1]
+            Kmu = K(mu)
+            if self._pool_type == "sa_SD":
+                Umu = Circuit()
+                for comp in _sa_components(self._pool_obj[self._tops[mu + 1]][1]):
+                    q = comp.jw_transform(self._qubit_excitations)
+                    U, p = trotterize(q, factor=-tamp, trotter_number=self._trotter_number)
+                    Umu.add(U)
+            else:
+                Umu, _ = trotterize(Kmu_prev, factor=-tamp, trotter_number=self._trotter_number)
+            qc_sig.apply_circuit(Umu)
+            qc_psi.apply_circuit(Umu)
+            qc_temp = Computer(qc_psi)
+            qc_temp.apply_operator(Kmu)
+            grads[mu] = 2.0 * np.real(np.vdot(qc_sig.get_coeff_vec(), qc_temp.get_coeff_vec()))
+            Kmu_prev = Kmu
+        return grads
+
+    def get_gs_energy(self):
+        return self._Egs
+
+
+class UCCNVQE(_UCCBase):
+    """dUCC-VQE with all pool operators (ucc/uccnvqe.py:42-271)."""
+
+    def run(self, opt_thresh=1.0e-5, opt_maxiter=200, pool_type=None, optimizer="BFGS",
+            use_analytic_grad=True):
+        from scipy.optimize import minimize
+        if pool_type is not None:
+            self._pool_type = pool_type
+        self.fill_pool()
+        self._tops = list(range(len(self._pool_obj)))
+        self._tamps = [0.0] * len(self._pool_obj)
+        x0 = np.array(self._tamps)
+        opts = {"maxiter": opt_maxiter}
+        if optimizer in ("BFGS", "CG", "L-BFGS-B", "TNC", "trust-constr"):
+            opts["gtol"] = opt_thresh
+        res = minimize(self.energy_feval, x0, method=optimizer,
+                       jac=self.gradient_ary_feval if use_analytic_grad else None, options=opts)
+        self._Egs = float(res.fun)
+        self._tamps = list(res.x)
+        self._final_result = res
+        return self._Egs
+
+
+class ADAPTVQE(_UCCBase):
+    """ADAPT-VQE (ucc/adaptvqe.py:81-458): grow the ansatz by the largest
+    pool gradient, re-optimise, repeat."""
+
+    def run(self, avqe_thresh=1.0e-2, pool_type=None, opt_thresh=1.0e-5, opt_maxiter=200,
+            adapt_maxiter=20, optimizer="BFGS"):
+        from scipy.optimize import minimize
+        if pool_type is not None:
+            self._pool_type = pool_type
+        self.fill_pool()
+        self._tops, self._tamps = [], []
+        self._energies, self._grad_norms = [], []
+        for _ in range(adapt_maxiter):
+            grads = self.measure_gradient3()
+            norm = float(np.sqrt(np.sum(grads ** 2)))
+            self._grad_norms.append(norm)
+            if norm < abs(avqe_thresh):
+                break
+            k = int(np.argmax(np.abs(grads)))
+            self._tops.append(k)
+            self._tamps.append(0.0)
+            res = minimize(self.energy_feval, np.array(self._tamps), method=optimizer,
+                           jac=self.gradient_ary_feval,
+                           options={"gtol": opt_thresh, "maxiter": opt_maxiter})
+            self._tamps = list(res.x)
+            self._energies.append(float(res.fun))
+        self._Egs = self._energies[-1] if self._energies else self.energy_feval([])
+        return self._Egs

@@ -1,0 +1,198 @@
+"""Compile helpers of the reference: Pauli exponentials, Trotter products,
+reference-state preparation and string builders.
+
+* ``exponentiate_pauli_string``  utils/exponentiate.py:9-87
+* ``trotterize`` / ``trotterize_w_cRz``  utils/trotterization.py:10-215
+* ``build_refprep`` / ``ref_string`` / ``integer_to_ref``  utils/state_prep.py
+* ``build_circuit`` / ``build_operator`` / ``smart_print``  helper/io_helper.py
+
+The circuits returned are the reference's gate for gate (basis change, CNOT
+ladder, Rz(-2 Im c), uncompute), so their size, CNOT count and printout
+match.  Each also records the exponential it implements, which lets
+``Computer.apply_circuit`` run it as one fused pass.
+"""
+
+import cmath
+import math
+
+import numpy as np
+
+from .circuit import Circuit
+from .gate import gate as _gate
+from .qubit_basis import QubitBasis
+from .qubit_operator import QubitOperator
+
+__all__ = ["exponentiate_pauli_string", "trotterize", "trotterize_w_cRz", "build_refprep",
+           "ref_string", "integer_to_ref", "build_circuit", "build_operator", "smart_print"]
+
+
+def exponentiate_pauli_string(coefficient, term, Use_cRz=False, ancilla_idx=None,
+                              Use_open_cRz=False):
+    """exp(coefficient * term) for an imaginary coefficient -> (Circuit, phase)."""
+    coefficient = complex(coefficient)
+    if abs(coefficient.real) > 1.0e-14:
+        raise ValueError(
+            f"exponentiate_pauli_string() called with a real coefficient {coefficient}")
+    if term.size() == 0:
+        return (Circuit(), cmath.exp(coefficient))
+    exponential = Circuit()
+    to_z = Circuit()
+    cx_circ = Circuit()
+    prev_target = None
+    max_target = None
+    letters = []
+    for g in term.gates():
+        gid = g.gate_id()
+        target = g.target()
+        control = g.control()
+        if gid == "X":
+            to_z.add(_gate("H", target, control))
+        elif gid == "Y":
+            to_z.add(_gate("Rx", target, control, np.pi / 2))
+        elif gid == "I":
+            continue
+        letters.append((gid, target))
+        if prev_target is not None:
+            cx_circ.add(_gate("cX", target, prev_target))
+        prev_target = target
+        max_target = target
+    if Use_cRz:
+        z_rot = _gate("cRz", max_target, ancilla_idx, -2.0 * coefficient.imag)
+    else:
+        z_rot = _gate("Rz", max_target, max_target, -2.0 * coefficient.imag)
+    exponential.add(to_z)
+    exponential.add(cx_circ)
+    if Use_open_cRz:
+        exponential.add(_gate("X", ancilla_idx, ancilla_idx))
+    exponential.add(z_rot)
+    if Use_open_cRz:
+        exponential.add(_gate("X", ancilla_idx, ancilla_idx))
+    exponential.add(cx_circ.adjoint())
+    exponential.add(to_z.adjoint())
+    if not Use_cRz and letters:
+        # record exp(i theta P): the whole circuit is this one exponential
+        x = z = 0
+        distinct = True
+        for l, q in letters:
+            b = 1 << q
+            if (x | z) & b:
+                distinct = False
+                break
+            if l in ("X", "Y"):
+                x |= b
+            if l in ("Y", "Z"):
+                z |= b
+        if distinct:
+            exponential._pexp = [(0, exponential.size(), x, z, coefficient.imag)]
+    return (exponential, 1.0)
+
+
+def trotterize(operator, factor=1.0, trotter_number=1, trotter_order=1):
+    """Circuit for exp(factor * operator) as a first-order Trotter product."""
+    total_phase = 1.0
+    circ = Circuit()
+    if trotter_number == 1 and trotter_order == 1:
+        for coeff, term in operator.terms():
+            gen, phase = exponentiate_pauli_string(factor * coeff, term)
+            circ.add_circuit(gen)
+            total_phase *= phase
+    else:
+        if trotter_order > 1:
+            raise NotImplementedError("Higher order trotterization is not yet implemented.")
+        ho = QubitOperator()
+        for _ in range(1, trotter_number + 1):
+            for coeff, term in operator.terms():
+                ho.add(factor * coeff / float(trotter_number), term)
+        for coeff, term in ho.terms():
+            gen, phase = exponentiate_pauli_string(coeff, term)
+            circ.add_circuit(gen)
+            total_phase *= phase
+    return (circ, total_phase)
+
+
+def trotterize_w_cRz(operator, ancilla_qubit_idx, factor=1.0, Use_open_cRz=False,
+                     trotter_number=1, trotter_order=1):
+    """Controlled Trotter product (utils/trotterization.py:147-215)."""
+    total_phase = 1.0
+    circ = Circuit()
+    if trotter_number == 1 and trotter_order == 1:
+        terms = [(factor * c, t) for c, t in operator.terms()]
+    else:
+        if trotter_order > 1:
+            raise NotImplementedError("Higher order trotterization is not yet implemented.")
+        terms = []
+        for _ in range(1, trotter_number + 1):
+            for c, t in operator.terms():
+                terms.append((factor * c / float(trotter_number), t))
+    for c, t in terms:
+        gen, phase = exponentiate_pauli_string(c, t, Use_cRz=True, ancilla_idx=ancilla_qubit_idx,
+                                               Use_open_cRz=Use_open_cRz)
+        circ.add_circuit(gen)
+        total_phase *= phase
+    return (circ, total_phase)
+
+
+def build_refprep(ref):
+    refprep = Circuit()
+    for j, occupied in enumerate(ref):
+        if occupied:
+            refprep.add(_gate("X", j, j))
+    return refprep
+
+
+def ref_string(ref, nqb):
+    temp = list(ref)
+    temp.reverse()
+    idx = int("".join(str(x) for x in temp), 2)
+    return QubitBasis(idx).str(nqb)
+
+
+def integer_to_ref(n, nqubits):
+    """Occupation list of basis index n (bit k -> qubit k)."""
+    return [(n >> k) & 1 for k in range(nqubits)]
+
+
+def ref_to_basis_idx(ref):
+    return sum(int(b) << k for k, b in enumerate(ref))
+
+
+def build_circuit(Inputstr):
+    """'X_0 cX_1_0 Rx_2_0.5' -> Circuit (helper/io_helper.py:52-75)."""
+    circ = Circuit()
+    for tok in Inputstr.split():
+        parts = tok.split("_")
+        if len(parts) == 2:
+            circ.add(_gate(parts[0], int(parts[1]), int(parts[1])))
+        elif "R" in parts[0]:
+            circ.add(_gate(parts[0], int(parts[1]), int(parts[1]), float(parts[2])))
+        else:
+            circ.add(_gate(parts[0], int(parts[1]), int(parts[2])))
+    return circ
+
+
+def build_operator(Inputstr):
+    """'c1, circ1; c2, circ2' -> QubitOperator (helper/io_helper.py:87-94)."""
+    ops = QubitOperator()
+    for term in Inputstr.split(";"):
+        c, circ = term.split(",")
+        ops.add(complex(c), build_circuit(circ))
+    return ops
+
+
+def smart_print(obj):
+    from .computer import Computer
+    if isinstance(obj, QubitOperator):
+        print("\n Quantum operator:")
+        first = True
+        for c, circ in obj.terms():
+            if not first:
+                print("+", end=" ")
+            first = False
+            print(c, end=" ")
+            print("(" + " ".join(circ.str()[1:-1].split(" ")) + ")", "|Ψ>")
+    if isinstance(obj, Circuit):
+        print("\n Quantum circuit:")
+        print("(" + " ".join(obj.str()[1:-1].split(" ")) + ")", "|Ψ>")
+    if isinstance(obj, Computer):
+        print("\n Quantum Computer:")
+        print(obj.str())

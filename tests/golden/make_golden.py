@@ -1,0 +1,242 @@
+"""Generate the golden fixtures of tests/golden from the reference itself.
+
+Run in a container that holds the reference sources (read where they lie) and
+its compiled module (``make -C oracle ref``):
+
+    python tests/golden/make_golden.py [--ref-src /root/reference/src/qforte]
+
+Every output comes from the reference's own code path -- its C++ ``Computer``,
+``SQOperator.jw_transform``, ``SQOpPool`` and its Python UCC drivers -- on
+seeded synthetic inputs.  Integral files of the reference's tests are read
+and stored as second-quantised term arrays (the test data the FCI pins in
+tests/test_gpu_drivers.py refer to).
+"""
+
+import argparse
+import json
+import math
+import os
+import sys
+import warnings
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+warnings.filterwarnings("ignore")
+
+from oracle import oracle as O  # noqa: E402
+from qforte_b200.systems import hf_reference, random_integrals  # noqa: E402
+
+
+def pauli_arrays(qo):
+    """(coeff, x, z) arrays of a reference QubitOperator, circuits read as
+    left-to-right products of single-qubit Paulis on distinct qubits."""
+    c, xs, zs = [], [], []
+    for coeff, circ in qo.terms():
+        x = z = 0
+        for g in circ.gates():
+            b = 1 << g.target()
+            lab = g.gate_id()
+            if lab in ("X", "Y"):
+                x |= b
+            if lab in ("Y", "Z"):
+                z |= b
+        c.append(complex(coeff))
+        xs.append(x)
+        zs.append(z)
+    return (np.array(c, dtype=np.complex128), np.array(xs, dtype=np.uint64),
+            np.array(zs, dtype=np.uint64))
+
+
+def sq_arrays(sqop):
+    """Flatten SQOperator terms: coeff, cre/ann index lists padded with -1."""
+    terms = sqop.terms()
+    n = len(terms)
+    coeff = np.array([complex(t[0]) for t in terms], dtype=np.complex128)
+    w = max([len(t[1]) for t in terms] + [len(t[2]) for t in terms] + [1])
+    cre = -np.ones((n, w), dtype=np.int32)
+    ann = -np.ones((n, w), dtype=np.int32)
+    for k, t in enumerate(terms):
+        cre[k, :len(t[1])] = t[1]
+        ann[k, :len(t[2])] = t[2]
+    return coeff, cre, ann
+
+
+def ref_sq_ham(qf, h, g):
+    norb = h.shape[0]
+    H = qf.SQOperator()
+    H.add(0.0, [], [])
+    for i in range(norb):
+        ia, ib = 2 * i, 2 * i + 1
+        for j in range(norb):
+            ja, jb = 2 * j, 2 * j + 1
+            H.add(h[i, j], [ia], [ja])
+            H.add(h[i, j], [ib], [jb])
+            for k in range(norb):
+                ka, kb = 2 * k, 2 * k + 1
+                for l in range(norb):
+                    la, lb = 2 * l, 2 * l + 1
+                    v = g[i, l, k, j] / 2
+                    if ia != jb and kb != la:
+                        H.add(v, [ia, jb], [kb, la])
+                    if ib != ja and ka != lb:
+                        H.add(v, [ib, ja], [ka, lb])
+                    if ia != ja and ka != la:
+                        H.add(v, [ia, ja], [ka, la])
+                    if ib != jb and kb != lb:
+                        H.add(v, [ib, jb], [kb, lb])
+    return H
+
+
+class _Sys:
+    pass
+
+
+def make_alg(qf, H, ref, pool_type):
+    s = _Sys()
+    s.hamiltonian = H
+    s.hf_reference = ref
+    s.hf_energy = 0.0
+    alg = qf.UCCNVQE(s)
+    alg._pool_type = pool_type
+    alg.fill_pool()
+    return alg
+
+
+def ucc_fixture(qf, norb, seed, out):
+    h, g = random_integrals(norb, seed)
+    H = ref_sq_ham(qf, h, g).jw_transform()
+    ref = hf_reference(norb, norb)
+    nq = 2 * norb
+    hc, hx, hz = pauli_arrays(H)
+    rng = np.random.default_rng(1000 + seed)
+    # dUCCSD: every SD operator, amplitudes U(-0.1, 0.1)
+    alg = make_alg(qf, H, ref, "SD")
+    M = len(alg._pool_obj)
+    amps = rng.uniform(-0.1, 0.1, M)
+    alg._tops = list(range(M))
+    alg._tamps = list(amps)
+    E = alg.energy_feval(list(amps))
+    qc = qf.Computer(nq)
+    qc.apply_circuit(alg.build_Uvqc(list(amps)))
+    psi = np.array(qc.get_coeff_vec())
+    grad = np.array(alg.measure_gradient(list(amps)))
+    # ADAPT pool gradients: GSD pool, 12 operators drawn from it
+    algg = make_alg(qf, H, ref, "GSD")
+    P = len(algg._pool_obj)
+    tops = [int(t) for t in rng.choice(P, 12, replace=False)]
+    gamps = rng.uniform(-0.1, 0.1, 12)
+    algg._tops = tops
+    algg._tamps = list(gamps)
+    pool_grads = np.array(algg.measure_gradient3())
+    np.savez_compressed(out, norb=norb, seed=seed, nqubit=nq, ref=np.array(ref),
+                        h=h, g=g, ham_c=hc, ham_x=hx, ham_z=hz, amps=amps, energy=E, psi=psi,
+                        grad=grad, gsd_tops=np.array(tops), gsd_amps=gamps,
+                        pool_grads=pool_grads)
+    print(f"{out}: {nq} q, {len(hc)} H terms, {M} SD params, {P} GSD ops, E = {E:.12f}")
+
+
+def pools_fixture(qf, norb, out):
+    ref = hf_reference(norb, norb)
+    arrs = {}
+    rng = np.random.default_rng(7)
+    for pt in ("SD", "GSD", "sa_SD", "SDTQ"):
+        pool = qf.SQOpPool()
+        pool.set_orb_spaces(ref)
+        pool.fill_pool(pt)
+        cs, cr, an, owner = [], [], [], []
+        for k, (c, op) in enumerate(pool):
+            a, b, d = sq_arrays(op)
+            cs.append(a)
+            cr.append(b)
+            an.append(d)
+            owner += [k] * len(a)
+        w = max(x.shape[1] for x in cr)
+        pad = lambda m: np.pad(m, ((0, 0), (0, w - m.shape[1])), constant_values=-1)
+        arrs[f"{pt}_coeff"] = np.concatenate(cs)
+        arrs[f"{pt}_cre"] = np.concatenate([pad(m) for m in cr])
+        arrs[f"{pt}_ann"] = np.concatenate([pad(m) for m in an])
+        arrs[f"{pt}_owner"] = np.array(owner, dtype=np.int32)
+        if pt != "sa_SD":
+            amps = rng.uniform(-0.1, 0.1, len(pool))
+            tmp = qf.SQOpPool()
+            for t, (c, op) in zip(amps, pool):
+                tmp.add(t, op)
+            A = tmp.get_qubit_operator("commuting_grp_lex")
+            ac, ax, az = pauli_arrays(A)
+            arrs[f"{pt}_amps"] = amps
+            arrs[f"{pt}_A_c"], arrs[f"{pt}_A_x"], arrs[f"{pt}_A_z"] = ac, ax, az
+    np.savez_compressed(out, norb=norb, **arrs)
+    print(f"{out}: pools {[k for k in arrs if k.endswith('_owner')]}")
+
+
+def gates_fixture(qf, out, n=6, ngates=300, seed=5):
+    rng = np.random.default_rng(seed)
+    one = ["X", "Y", "Z", "H", "R", "Rx", "Ry", "Rz", "V", "S", "T", "I"]
+    two = ["A", "cX", "acX", "cY", "cZ", "cR", "cV", "cRz", "SWAP", "CNOT", "aCNOT"]
+    kinds, tg, ct, pr = [], [], [], []
+    qc = qf.Computer(n)
+    circ = qf.Circuit()
+    for _ in range(ngates):
+        if rng.random() < 0.5:
+            k = one[rng.integers(len(one))]
+            t = int(rng.integers(n))
+            c = t
+        else:
+            k = two[rng.integers(len(two))]
+            t, c = (int(v) for v in rng.choice(n, 2, replace=False))
+        p = float(rng.uniform(0, 4 * math.pi))
+        circ.add(qf.gate(k, t, c, p))
+        kinds.append(k)
+        tg.append(t)
+        ct.append(c)
+        pr.append(p)
+    qc.apply_circuit(circ)
+    psi = np.array(qc.get_coeff_vec())
+    # an operator application and its expectation value on that state
+    op = qf.build_operator("0.5, X_0 Z_2; 0.3j, Y_1 X_3; -0.7, Z_0 Z_5; 0.2, X_1 X_1; "
+                           "0.1, Y_2 Z_2 X_4; -0.25j, Z_3")
+    qc2 = qf.Computer(qc)
+    qc2.apply_operator(op)
+    ev = qc.direct_op_exp_val(op)
+    pev = [qc.direct_pauli_circ_exp_val(qf.build_circuit(s))
+           for s in ("X_0 Y_1", "Y_2", "Y_1 Y_3 Z_0", "X_5 X_5 Y_4", "Z_1 X_1")]
+    pmc = qc.perfect_measure_circuit(qf.build_circuit("X_0 Y_2 Z_4"))
+    np.savez_compressed(out, n=n, kinds=np.array(kinds), target=np.array(tg),
+                        control=np.array(ct), param=np.array(pr), psi=psi,
+                        op_psi=np.array(qc2.get_coeff_vec()), op_expval=ev,
+                        pauli_expvals=np.array(pev), perfect_measure=pmc)
+    print(f"{out}: {ngates} gates on {n} qubits")
+
+
+def integrals_fixture(path, out):
+    with open(path) as f:
+        data = json.load(f)
+    oei = np.array(data["oei"]["data"], dtype=np.float64)
+    tei = np.array(data["tei"]["data"], dtype=np.float64)
+    np.savez_compressed(out, nso=data["nso"]["data"], na=data["na"]["data"],
+                        nb=data["nb"]["data"], scalar=data["scalar_energy"]["data"],
+                        oei=oei, tei=tei)
+    print(f"{out}: {len(oei)} one-body, {len(tei)} two-body integrals")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref-src", default="/root/reference/src/qforte")
+    a = ap.parse_args()
+    qf = O.load_reference(a.ref_src)
+    tests_dir = os.path.join(os.path.dirname(a.ref_src.rstrip("/")), "..", "tests")
+    ucc_fixture(qf, 4, 11, os.path.join(HERE, "ucc_norb4_seed11.npz"))
+    ucc_fixture(qf, 6, 11, os.path.join(HERE, "ucc_norb6_seed11.npz"))
+    pools_fixture(qf, 4, os.path.join(HERE, "pools_norb4.npz"))
+    gates_fixture(qf, os.path.join(HERE, "gates_n6.npz"))
+    integrals_fixture(os.path.join(tests_dir, "He-ccpvdz.json"),
+                      os.path.join(HERE, "he_ccpvdz_integrals.npz"))
+    integrals_fixture(os.path.join(tests_dir, "H4-sto6g-075a.json"),
+                      os.path.join(HERE, "h4_sto6g_integrals.npz"))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,232 @@
+"""GPU parity: the libqfb.so kernels against the oracle and the reference's
+golden vectors.  Tolerances: amplitudes 1e-12
+max-abs, energies 1e-10, gradients 1e-8; basis-index work bit-exact."""
+
+import math
+
+import numpy as np
+import pytest
+
+import qforte_b200 as qb
+from oracle import oracle as O
+from qforte_b200.ucc import DUCC
+from tests.conftest import golden
+from tests.helpers import (kops_forward, kops_gradient, oracle_terms, oracle_terms_from_arrays,
+                           qo_from_arrays, random_problem)
+
+pytestmark = pytest.mark.gpu
+
+AMP_TOL = 1e-12
+E_TOL = 1e-10
+G_TOL = 1e-8
+
+ONE = ["X", "Y", "Z", "H", "R", "Rx", "Ry", "Rz", "V", "S", "T", "I"]
+TWO = ["A", "cX", "acX", "cY", "cZ", "cR", "cV", "cRz", "SWAP", "CNOT", "aCNOT"]
+
+
+def _rand_circuit(n, ngates, seed):
+    rng = np.random.default_rng(seed)
+    circ, ora = qb.Circuit(), []
+    for _ in range(ngates):
+        if rng.random() < 0.5:
+            k, t = ONE[rng.integers(len(ONE))], int(rng.integers(n))
+            c = t
+        else:
+            k = TWO[rng.integers(len(TWO))]
+            t, c = (int(v) for v in rng.choice(n, 2, replace=False))
+        p = float(rng.uniform(0, 4 * math.pi))
+        circ.add(qb.gate(k, t, c, p))
+        ora.append(O.make_gate(k, t, c, p))
+    return circ, ora
+
+
+def test_gates_match_reference_golden(cuda):
+    z = golden("gates_n6.npz")
+    qc = qb.Computer(int(z["n"]))
+    circ = qb.Circuit()
+    for k, t, c, p in zip(z["kinds"], z["target"], z["control"], z["param"]):
+        circ.add(qb.gate(str(k), int(t), int(c), float(p)))
+    qc.apply_circuit(circ)
+    assert np.max(np.abs(qc.get_coeff_array() - z["psi"])) < AMP_TOL
+
+
+@pytest.mark.parametrize("n,ngates,seed", [(2, 60, 1), (5, 400, 2), (9, 300, 3), (13, 120, 4)])
+def test_gates_match_oracle(cuda, n, ngates, seed):
+    circ, ora = _rand_circuit(n, ngates, seed)
+    qc = qb.Computer(n)
+    qc.apply_circuit(circ)
+    st = O.State(n)
+    st.apply_gates(ora)
+    assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
+
+
+def test_every_gate_every_ordering(cuda):
+    """tests/test_comprehensive_gate.py:74-91 of the reference: every 2-qubit
+    gate on all (target, control) orderings of 5 qubits, from a random state."""
+    rng = np.random.default_rng(9)
+    psi0 = rng.normal(size=32) + 1j * rng.normal(size=32)
+    psi0 /= np.linalg.norm(psi0)
+    for k in ("cV", "cX", "acX", "cY", "cZ", "cR", "cRz", "SWAP", "A"):
+        for t in range(5):
+            for c in range(5):
+                if t == c:
+                    continue
+                qc = qb.Computer(5)
+                qc.set_coeff_vec(psi0)
+                qc.apply_gate(qb.gate(k, t, c, 0.37))
+                st = O.State(5, psi0)
+                st.apply_gates([O.make_gate(k, t, c, 0.37)])
+                assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < 1e-15, (k, t, c)
+
+
+def test_operator_application_and_expectations(cuda):
+    z = golden("gates_n6.npz")
+    qc = qb.Computer(int(z["n"]))
+    qc.set_coeff_vec(z["psi"])
+    op = qb.build_operator("0.5, X_0 Z_2; 0.3j, Y_1 X_3; -0.7, Z_0 Z_5; 0.2, X_1 X_1; "
+                           "0.1, Y_2 Z_2 X_4; -0.25j, Z_3")
+    ev = qc.direct_op_exp_val(op)
+    assert abs(ev - complex(z["op_expval"])) < E_TOL
+    pev = [qc.direct_pauli_circ_exp_val(qb.build_circuit(s))
+           for s in ("X_0 Y_1", "Y_2", "Y_1 Y_3 Z_0", "X_5 X_5 Y_4", "Z_1 X_1")]
+    assert np.max(np.abs(np.array(pev) - z["pauli_expvals"])) < E_TOL
+    pm = qc.perfect_measure_circuit(qb.build_circuit("X_0 Y_2 Z_4"))
+    assert abs(pm - float(z["perfect_measure"])) < E_TOL
+    qc2 = qb.Computer(qc)
+    qc2.apply_operator(op)
+    assert np.max(np.abs(qc2.get_coeff_array() - z["op_psi"])) < AMP_TOL
+    # a term with a non-Pauli gate takes the general path (copy, circuit, scale, sum)
+    opg = qb.build_operator("0.5, X_0 Z_2; 0.3, H_1 cX_3_1")
+    qc3 = qb.Computer(qc)
+    qc3.apply_operator(opg)
+    st = O.State(6, z["psi"])
+    st.apply_operator([(0.5, [O.make_gate("X", 0, 0), O.make_gate("Z", 2, 2)]),
+                       (0.3, [O.make_gate("H", 1, 1), O.make_gate("cX", 3, 1)])])
+    assert np.max(np.abs(qc3.get_coeff_array() - st.psi)) < AMP_TOL
+
+
+def test_trotterized_exponentials_fused_vs_gates(cuda):
+    """exp(c P) circuits run as one fused pass; the gates they stand for give
+    the same state (reference: utils/exponentiate.py)."""
+    rng = np.random.default_rng(4)
+    n = 7
+    A = qb.QubitOperator()
+    terms = []
+    for _ in range(25):
+        sup = sorted(rng.choice(n, rng.integers(1, 5), replace=False))
+        letters = [("X", "Y", "Z")[rng.integers(3)] for _ in sup]
+        circ = qb.Circuit()
+        for l, q in zip(letters, sup):
+            circ.add(qb.gate(l, int(q)))
+        c = 1j * rng.uniform(-1, 1)
+        A.add(c, circ)
+        terms.append((c, list(zip(letters, [int(q) for q in sup]))))
+    U, phase = qb.trotterize(A)
+    assert U._pexp is not None and len(U._pexp) == 25
+    qc = qb.Computer(n)
+    qc.apply_circuit(qb.build_circuit("H_0 H_3 X_5 Ry_2_0.7"))
+    qc.apply_circuit(U)
+    st = O.State(n)
+    st.apply_gates([O.make_gate("H", 0, 0), O.make_gate("H", 3, 3), O.make_gate("X", 5, 5),
+                    O.make_gate("Ry", 2, 2, 0.7)])
+    g, _ = O.trotterize(terms)
+    st.apply_gates(g)
+    assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
+    # the adjoint circuit undoes it
+    qc.apply_circuit(U.adjoint())
+    st2 = O.State(n)
+    st2.apply_gates([O.make_gate("H", 0, 0), O.make_gate("H", 3, 3), O.make_gate("X", 5, 5),
+                     O.make_gate("Ry", 2, 2, 0.7)])
+    assert np.max(np.abs(qc.get_coeff_array() - st2.psi)) < AMP_TOL
+
+
+@pytest.mark.parametrize("name", ["ucc_norb4_seed11.npz", "ucc_norb6_seed11.npz"])
+def test_ducc_energy_state_gradient_vs_reference(cuda, name):
+    z = golden(name)
+    mol, pool = random_problem(int(z["norb"]), int(z["seed"]))
+    tops = list(range(len(pool)))
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+    amps = z["amps"]
+    E = eng.energy(amps)
+    assert abs(E - float(z["energy"])) < E_TOL
+    psi = eng.state(amps).get_coeff_array()
+    assert np.max(np.abs(psi - z["psi"])) < AMP_TOL
+    E2, g = eng.energy_grad(amps)
+    assert abs(E2 - float(z["energy"])) < E_TOL
+    assert np.max(np.abs(g - z["grad"])) < G_TOL
+    # a batch gives each row's single-call result
+    rng = np.random.default_rng(5)
+    P = np.vstack([amps, rng.uniform(-0.1, 0.1, (3, len(amps)))])
+    EB, GB = eng.energy_grad(P)
+    for b in range(P.shape[0]):
+        e1, g1 = eng.energy_grad(P[b])
+        assert abs(EB[b] - e1) < 1e-12 and np.max(np.abs(GB[b] - g1)) < 1e-12
+    assert np.max(np.abs(eng.energy(P) - EB)) < 1e-12
+
+
+def test_ducc_pool_gradients_vs_reference(cuda):
+    z = golden("ucc_norb4_seed11.npz")
+    mol, gsd = random_problem(4, int(z["seed"]), "GSD")
+    tops = [int(t) for t in z["gsd_tops"]]
+    eng = DUCC(mol.hamiltonian, gsd, tops, mol.hf_reference)
+    g = eng.pool_gradients(z["gsd_amps"])
+    assert np.max(np.abs(g - z["pool_grads"])) < G_TOL
+
+
+def test_ducc_vs_oracle_14_qubits(cuda):
+    mol, pool = random_problem(7, 3)
+    tops = list(range(len(pool)))
+    rng = np.random.default_rng(8)
+    amps = rng.uniform(-0.1, 0.1, len(tops))
+    hterms = oracle_terms(mol.hamiltonian)
+    E_o, st = O.energy(14, mol.hf_reference, kops_forward(pool, tops), amps, hterms)
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+    E, g = eng.energy_grad(amps)
+    assert abs(E - E_o) < E_TOL
+    assert np.max(np.abs(eng.state(amps).get_coeff_array() - st.psi)) < AMP_TOL
+
+
+def test_gradient_vs_central_differences(cuda):
+    mol, pool = random_problem(5, 21)
+    tops = list(range(len(pool)))
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+    rng = np.random.default_rng(2)
+    t = rng.uniform(-0.1, 0.1, len(tops))
+    _, g = eng.energy_grad(t)
+    h = 1e-5
+    P = np.repeat(t[None, :], 2 * len(t), axis=0)
+    for k in range(len(t)):
+        P[2 * k, k] += h
+        P[2 * k + 1, k] -= h
+    E = eng.energy(P)
+    fd = (E[0::2] - E[1::2]) / (2 * h)
+    assert np.max(np.abs(fd - g)) < G_TOL
+
+
+def test_computer_api_and_errors(cuda):
+    qc = qb.Computer(3)
+    assert qc.get_coeff_vec()[0] == 1.0 and qc.get_nqubit() == 3
+    qc.set_state([(qb.QubitBasis(5), 0.6), (qb.QubitBasis(2), 0.8j)])
+    a = qc.get_coeff_array()
+    assert a[5] == 0.6 and a[2] == 0.8j and np.count_nonzero(a) == 2
+    assert qc.coeff(qb.QubitBasis(2)) == 0.8j
+    cp = qb.Computer(qc)
+    assert cp == qc
+    cp.apply_constant(2.0)
+    assert abs(qb.inner_product(qc, cp) - 2.0) < 1e-15
+    cp.null_state()
+    assert not np.any(cp.get_coeff_array())
+    cp.reset()
+    assert cp.get_coeff_array()[0] == 1.0
+    assert qc.direct_gate_exp_val(qb.gate("X", 0)) == 0  # computer.cc:937-954 behaviour
+    assert qc.get_coeff_array()[4] == 0.6  # ... with the gate left applied
+    with pytest.raises(ValueError):
+        qc.apply_gate(qb.gate("X", 3))
+    with pytest.raises(ValueError):
+        qc.apply_operator(qb.build_operator("1.0, Z_7"))
+    with pytest.raises(ValueError):
+        qc.set_coeff_vec(np.zeros(4))
+    assert "Computer(" in qc.str()
+    big = qb.Computer(1)
+    big.apply_gate(qb.gate("H", 0))
+    assert abs(big.get_coeff_array()[1] - 1 / math.sqrt(2)) < 1e-16

@@ -1,0 +1,81 @@
+"""The oracle is pinned before it is trusted: its CPU restatement of the
+reference's algorithms must reproduce golden vectors that the compiled
+reference produced (tests/golden/make_golden.py) and the known answers of the
+reference's own tests."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.conftest import golden
+from tests.helpers import kops_forward, kops_gradient, oracle_terms_from_arrays, random_problem
+
+
+def _ucc_inputs(z, pool_type="SD"):
+    norb = int(z["norb"])
+    mol, pool = random_problem(norb, int(z["seed"]), pool_type)
+    hterms = oracle_terms_from_arrays(z["ham_c"], z["ham_x"], z["ham_z"])
+    return mol, pool, hterms
+
+
+@pytest.mark.parametrize("name", ["ucc_norb4_seed11.npz", "ucc_norb6_seed11.npz"])
+def test_oracle_energy_state_gradient(name):
+    z = golden(name)
+    mol, pool, hterms = _ucc_inputs(z)
+    nq = int(z["nqubit"])
+    tops = list(range(len(pool)))
+    amps = z["amps"]
+    E, st = O.energy(nq, list(z["ref"]), kops_forward(pool, tops), amps, hterms)
+    assert abs(E - float(z["energy"])) < 1e-12
+    assert np.max(np.abs(st.psi - z["psi"])) < 1e-13
+    g = O.measure_gradient(nq, list(z["ref"]), kops_forward(pool, tops), amps, hterms,
+                           kops_grad=kops_gradient(pool, tops))
+    assert np.max(np.abs(g - z["grad"])) < 1e-11
+
+
+def test_oracle_pool_gradients_norb4():
+    z = golden("ucc_norb4_seed11.npz")
+    mol, gsd, hterms = _ucc_inputs(z, "GSD")
+    nq = int(z["nqubit"])
+    tops = [int(t) for t in z["gsd_tops"]]
+    g = O.measure_gradient3(nq, list(z["ref"]), kops_forward(gsd, tops), z["gsd_amps"], hterms,
+                            kops_gradient(gsd, range(len(gsd))))
+    assert np.max(np.abs(g - z["pool_grads"])) < 1e-11
+
+
+def test_oracle_gates_bitexact():
+    z = golden("gates_n6.npz")
+    st = O.State(int(z["n"]))
+    gates = [O.make_gate(str(k), int(t), int(c), float(p))
+             for k, t, c, p in zip(z["kinds"], z["target"], z["control"], z["param"])]
+    st.apply_gates(gates)
+    # same algorithm, same operation order: bit-identical amplitudes
+    assert np.array_equal(st.psi, z["psi"])
+
+
+def test_oracle_trotter_known_answer():
+    """tests/test_trotter.py:15-47 of the reference (tolerance 1e-15)."""
+    terms = [(-1.0j * 0.5, []), (-1.0j * -0.04544288414432624, [("Z", 0)])]
+    gates, phase = O.trotterize(terms)
+    st = O.State(4)
+    st.psi[:] = 0
+    st.psi[3] = np.sqrt(2 / 3)
+    st.psi[12] = -np.sqrt(1 / 3)
+    st.apply_gates(gates)
+    st.apply_constant(phase)
+    c = st.psi
+    assert abs(c[3].real - 0.6980209737879599) < 1e-15
+    assert abs(c[3].imag - -0.423595782342996) < 1e-15
+    assert abs(c[12].real - -0.5187235657531178) < 1e-15
+    assert abs(c[12].imag - 0.25349397560041553) < 1e-15
+
+
+def test_oracle_operator_expval():
+    z = golden("gates_n6.npz")
+    st = O.State(int(z["n"]), z["psi"])
+    op = [(0.5, [("X", 0), ("Z", 2)]), (0.3j, [("Y", 1), ("X", 3)]), (-0.7, [("Z", 0), ("Z", 5)]),
+          (0.2, [("X", 1), ("X", 1)]), (0.1, [("Y", 2), ("Z", 2), ("X", 4)]), (-0.25j, [("Z", 3)])]
+    s2 = st.copy()
+    s2.apply_pauli_operator(op)
+    assert np.array_equal(s2.psi, z["op_psi"])
+    assert st.direct_op_exp_val(op) == complex(z["op_expval"])
