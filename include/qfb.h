@@ -144,10 +144,14 @@ QFB_API int qfb_prog_apply(qfb_prog p, qfb_state s, const double *params, int32_
 /* ---- adjoint dUCC gradient (UCCVQE.measure_gradient, uccvqeabc.py:122-251) --
  * psi holds U(t)|ref>, sigma holds H psi.  `kprog` lists, per parameter mu,
  * the strings of K_mu with scale = the imaginary parts of K_mu's JW
- * coefficients (param[k] = mu); grad[b][mu] = 2 Re <sigma|K_mu|psi_mu>.  psi
- * and sigma are consumed (un-rotated back to the reference). */
-QFB_API int qfb_ucc_gradient(qfb_prog kprog, qfb_state psi, qfb_state sigma, const double *params,
-                     int32_t nrows, double *grad);
+ * coefficients (param[k] = mu); grad[b][mu] = 2 Re <sigma|K_mu|psi_mu>.
+ * `uprog` is the program whose parameter-mu strings, reversed with negated
+ * angles, un-apply U_mu between steps: K itself for particle-hole pools
+ * (uccvqeabc.py:228-230), the forward ansatz program for spin-adapted ones,
+ * whose U_mu is the product of its component excitations (:208-224).  psi
+ * and sigma are consumed (un-rotated back towards the reference). */
+QFB_API int qfb_ucc_gradient(qfb_prog kprog, qfb_prog uprog, qfb_state psi, qfb_state sigma,
+                             const double *params, int32_t nrows, double *grad);
 
 /* ---- compiled dUCC evaluator (batched, CUDA-graph captured) ----------------
  * One object per (ansatz, Hamiltonian, batch size): it owns nbatch psi and
@@ -157,10 +161,11 @@ QFB_API int qfb_ucc_gradient(qfb_prog kprog, qfb_state psi, qfb_state sigma, con
  * can be captured once into a CUDA graph and replayed.  A run computes, per
  * slot b: psi_b = U(t_b)|ref>, sigma_b = H psi_b, energy[b] = <psi_b|sigma_b>
  * and (with_grad) the adjoint gradient of UCCVQE.measure_gradient
- * (uccvqeabc.py:122-251).  `gprog` may be NULL when no gradient is wanted. */
+ * (uccvqeabc.py:122-251) with kprog / uprog as for qfb_ucc_gradient.  kprog
+ * and uprog may be NULL when no gradient is wanted. */
 typedef struct qfb_ucc_s *qfb_ucc;
-QFB_API int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_sum ham, int nqubit,
-                           uint64_t ref_index, int nbatch, qfb_ucc *out);
+QFB_API int qfb_ucc_create(qfb_prog fprog, qfb_prog kprog, qfb_prog uprog, qfb_sum ham,
+                           int nqubit, uint64_t ref_index, int nbatch, qfb_ucc *out);
 QFB_API int qfb_ucc_destroy(qfb_ucc u);
 /* Device addresses of the parameter block and the outputs. */
 QFB_API int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_grad);

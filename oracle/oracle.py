@@ -328,13 +328,17 @@ def energy(nqubit, ref, kops, amps, hterms):
     return st.direct_op_exp_val(hterms).real, st
 
 
-def measure_gradient(nqubit, ref, kops, amps, hterms, kops_grad=None):
+def measure_gradient(nqubit, ref, kops, amps, hterms, kops_grad=None, kops_unrot=None):
     """Adjoint dUCC gradient, abc/uccvqeabc.py:122-251 (non-compact, trotter_number 1).
 
     ``kops_grad[mu]`` is K_mu as ``jw_transform`` returns it times the pool
     coefficient (term order of the gradient loop); defaults to ``kops``.
+    ``kops_unrot[mu]`` are the strings whose Trotter product un-applies U_mu:
+    K_mu itself for particle-hole pools (:228-230, the default), the ansatz's
+    component excitations for spin-adapted pools (:208-224).
     """
     kg = kops if kops_grad is None else kops_grad
+    ku = kg if kops_unrot is None else kops_unrot
     M = len(amps)
     grads = np.zeros(M)
     psi = prepare_state(nqubit, ref, kops, amps)
@@ -344,7 +348,7 @@ def measure_gradient(nqubit, ref, kops, amps, hterms, kops_grad=None):
     tmp.apply_pauli_operator(kg[M - 1])
     grads[M - 1] = 2.0 * sig.dot(tmp).real
     for mu in reversed(range(M - 1)):
-        umu, pmu = trotterize(kg[mu + 1], factor=-amps[mu + 1])
+        umu, pmu = trotterize(ku[mu + 1], factor=-amps[mu + 1])
         sig.apply_gates(umu)
         psi.apply_gates(umu)
         tmp = psi.copy()

@@ -69,9 +69,9 @@ SIGNATURES = {
     "qfb_prog_destroy": (ctypes.c_int, [c_prog]),
     "qfb_prog_info": (ctypes.c_int, [c_prog, _vp, _vp, _vp]),
     "qfb_prog_apply": (ctypes.c_int, [c_prog, c_state, _vp, _i32, _i32]),
-    "qfb_ucc_gradient": (ctypes.c_int, [c_prog, c_state, c_state, _vp, _i32, _vp]),
-    "qfb_ucc_create": (ctypes.c_int, [c_prog, c_prog, c_sum, ctypes.c_int, _u64, ctypes.c_int,
-                                      _vp]),
+    "qfb_ucc_gradient": (ctypes.c_int, [c_prog, c_prog, c_state, c_state, _vp, _i32, _vp]),
+    "qfb_ucc_create": (ctypes.c_int, [c_prog, c_prog, c_prog, c_sum, ctypes.c_int, _u64,
+                                      ctypes.c_int, _vp]),
     "qfb_ucc_destroy": (ctypes.c_int, [_vp]),
     "qfb_ucc_buffers": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "qfb_ucc_run": (ctypes.c_int, [_vp, ctypes.c_int]),

@@ -396,10 +396,12 @@ int qfb_state_set_basis(qfb_state s, int b, const uint64_t *index, const qfb_com
     }
     const int64_t cnt = (int64_t)uidx.size();
     void *buf = nullptr;
-    int rc = dev_alloc(&buf, (size_t)cnt * (sizeof(uint64_t) + sizeof(double2)));
+    // the value array starts on a 256-byte boundary (double2 needs 16)
+    const size_t ibytes = ((size_t)cnt * sizeof(uint64_t) + 255) & ~(size_t)255;
+    int rc = dev_alloc(&buf, ibytes + (size_t)cnt * sizeof(double2));
     if (rc) return rc;
     uint64_t *d_idx = (uint64_t *)buf;
-    double2 *d_val = (double2 *)(d_idx + cnt);
+    double2 *d_val = (double2 *)((char *)buf + ibytes);
     QFB_CUDA(cudaMemcpyAsync(d_idx, uidx.data(), cnt * sizeof(uint64_t), cudaMemcpyHostToDevice,
                              t_stream));
     QFB_CUDA(cudaMemcpyAsync(d_val, uval.data(), cnt * sizeof(double2), cudaMemcpyHostToDevice,

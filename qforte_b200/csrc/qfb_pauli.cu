@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "qfb_common.cuh"
+#include "qfb_window.cuh"
 
 using namespace qfb;
 
@@ -187,6 +188,78 @@ __global__ void __launch_bounds__(256) k_sum_apply(
             }
         }
         dst[off + k] = acc;
+    }
+}
+
+// dst = O src with four outputs per thread: k = k0 | d, d = 0..3.  For a
+// group x the four inputs j_d = (k0 ^ x) ^ d form one aligned quad, and
+// popcount(j_d & z) = popcount((k0 ^ x) & z) + popcount(d & z): one parity per
+// term serves all four outputs.  Terms are read in the real form (z, Re c)
+// when the group is real.
+__global__ void __launch_bounds__(256) k_sum_apply4(
+    double2 *__restrict__ dst, const double2 *__restrict__ src, uint64_t nbasis,
+    const GroupDev *__restrict__ groups, const TermDev *__restrict__ terms,
+    const double2 *__restrict__ rterms, int32_t ngroups) {
+    const uint64_t off = (uint64_t)blockIdx.y * nbasis;
+    const uint64_t nquad = nbasis >> 2;
+    for (uint64_t qd = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qd < nquad;
+         qd += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k0 = qd << 2;
+        double2 acc0 = make_double2(0.0, 0.0), acc1 = acc0, acc2 = acc0, acc3 = acc0;
+        for (int g = 0; g < ngroups; ++g) {
+            const uint64_t x = __ldg(&groups[g].x);
+            const int tb = __ldg(&groups[g].begin), te = __ldg(&groups[g].end);
+            const int real = __ldg(&groups[g].real);
+            const uint64_t base = k0 ^ x;
+            const uint64_t qb = base & ~3ull;
+            // a[e] = src[qb | e]; input of output d is a[d ^ (x & 3)]
+            double2 a0 = src[off + qb], a1 = src[off + qb + 1];
+            double2 a2 = src[off + qb + 2], a3 = src[off + qb + 3];
+            if (x & 1) {
+                double2 t = a0; a0 = a1; a1 = t;
+                t = a2; a2 = a3; a3 = t;
+            }
+            if (x & 2) {
+                double2 t = a0; a0 = a2; a2 = t;
+                t = a1; a1 = a3; a3 = t;
+            }
+            if (real) {
+                double f0 = 0.0, f1 = 0.0, f2 = 0.0, f3 = 0.0;
+                for (int t = tb; t < te; ++t) {
+                    const double2 zc = __ldg(&rterms[t]);  // (z bits, Re c)
+                    const uint64_t z = (uint64_t)__double_as_longlong(zc.x);
+                    const double c = parity64(base & z) ? -zc.y : zc.y;
+                    const double c1 = (z & 1) ? -c : c;
+                    f0 += c;
+                    f1 += c1;
+                    f2 += (z & 2) ? -c : c;
+                    f3 += (z & 2) ? -c1 : c1;
+                }
+                acc0.x += f0 * a0.x; acc0.y += f0 * a0.y;
+                acc1.x += f1 * a1.x; acc1.y += f1 * a1.y;
+                acc2.x += f2 * a2.x; acc2.y += f2 * a2.y;
+                acc3.x += f3 * a3.x; acc3.y += f3 * a3.y;
+            } else {
+                double2 f0 = make_double2(0.0, 0.0), f1 = f0, f2 = f0, f3 = f0;
+                for (int t = tb; t < te; ++t) {
+                    const uint64_t z = __ldg(&terms[t].z);
+                    double2 c = terms[t].c;
+                    if (parity64(base & z)) c = make_double2(-c.x, -c.y);
+                    const double2 c1 = (z & 1) ? make_double2(-c.x, -c.y) : c;
+                    const double2 c2 = (z & 2) ? make_double2(-c.x, -c.y) : c;
+                    const double2 c3 = (z & 2) ? make_double2(-c1.x, -c1.y) : c1;
+                    f0 = c_add(f0, c); f1 = c_add(f1, c1); f2 = c_add(f2, c2); f3 = c_add(f3, c3);
+                }
+                acc0 = c_add(acc0, c_mul(f0, a0));
+                acc1 = c_add(acc1, c_mul(f1, a1));
+                acc2 = c_add(acc2, c_mul(f2, a2));
+                acc3 = c_add(acc3, c_mul(f3, a3));
+            }
+        }
+        dst[off + k0] = acc0;
+        dst[off + k0 + 1] = acc1;
+        dst[off + k0 + 2] = acc2;
+        dst[off + k0 + 3] = acc3;
     }
 }
 
@@ -390,9 +463,23 @@ struct qfb_sum_s {
     void *blob = nullptr;  // device: groups, terms, segment starts
     GroupDev *d_groups = nullptr;
     TermDev *d_terms = nullptr;
+    double2 *d_rterms = nullptr;  // (z bits, Re c) per term, for real groups
     int32_t *d_seg_g0 = nullptr;
     std::vector<GroupDev> h_groups;
     std::vector<int32_t> h_seg_g0;
+};
+
+// A window plan of a program for one qubit count (qfb_window.cuh).
+struct WinPlan {
+    int b = 0, L = 0, nqubit = 0, nt = 1;
+    std::vector<qfbw::Window> wins;
+    std::vector<qfbw::WStep> steps;
+    std::vector<qfbw::WStr> strs;
+    void *blob = nullptr;
+    qfbw::WStep *d_steps = nullptr;
+    qfbw::WStr *d_strs = nullptr;
+    size_t smem_max = 0;
+    int ntiles() const { return 1 << (nqubit - b); }
 };
 
 struct qfb_prog_s {
@@ -404,9 +491,303 @@ struct qfb_prog_s {
     std::vector<StepDev> h_steps;
     std::vector<int32_t> p_step0, p_step1;  // steps of each parameter (gradient)
     bool params_contiguous = true;
+    WinPlan *fwd_plan[41] = {nullptr};   // by qubit count
+    WinPlan *grad_plan[41] = {nullptr};  // gradient sweep with K = this program ...
+    const qfb_prog_s *grad_plan_u[41] = {nullptr};  // ... and U_mu from this one
+    ~qfb_prog_s() {
+        for (auto *v : {&fwd_plan, &grad_plan})
+            for (auto *pl : *v)
+                if (pl) {
+                    dev_free(pl->blob);
+                    delete pl;
+                }
+    }
 };
 
 namespace {
+
+// Tile size (qubits) of the forward and gradient windows: a forward tile of
+// 2^12 amplitudes is 64 KB; a gradient window holds psi and sigma, 2 x 32 KB.
+constexpr int kFwdTileBits = 12;
+constexpr int kGradTileBits = 11;
+constexpr int kLowBits = 3;
+
+static qfbw::Window make_window(uint64_t U, int n, int b, int L) {
+    qfbw::Window w{};
+    const uint64_t all = (n >= 64) ? ~0ull : ((1ull << n) - 1ull);
+    uint64_t q = U | ((1ull << L) - 1ull);
+    for (int k = 0; k < n && __builtin_popcountll(q) < b; ++k) q |= 1ull << k;
+    w.qmask = q & all;
+    w.cmask = all & ~w.qmask;
+    w.b = b;
+    w.global_step = -1;
+    w.global_mu = -1;
+    return w;
+}
+
+static void push_strings(WinPlan *pl, const qfb_prog_s *p, const StepDev &st, uint64_t qmask,
+                         int sign, bool reversed) {
+    for (int i = 0; i < st.ns; ++i) {
+        const int k = st.s0 + (reversed ? st.ns - 1 - i : i);
+        const StrDev &sd = p->h_strs[k];
+        qfbw::WStr w;
+        w.zl = qfbw::pext_h(sd.z, qmask);
+        w.zc = sd.z & ~qmask;
+        w.ny = sd.ny;
+        w.param = sd.param;
+        w.rscale = sign * sd.scale;
+        w.scale = sd.scale;
+        pl->strs.push_back(w);
+    }
+}
+
+static void push_step(WinPlan *pl, const qfbw::Window &win, const StepDev &st, int rotate,
+                      int ip_row) {
+    qfbw::WStep w{};
+    w.xl = qfbw::pext_h(st.x, win.qmask);
+    w.hl = w.xl ? 63 - __builtin_clzll(w.xl) : -1;
+    w.s0 = (int32_t)pl->strs.size() - win.sr0;
+    w.ns = st.ns;
+    w.rotate = rotate;
+    w.ip_row = ip_row;
+    pl->steps.push_back(w);
+}
+
+static int upload_plan(WinPlan *pl) {
+    const size_t sb = sizeof(qfbw::WStep) * std::max<size_t>(1, pl->steps.size());
+    const size_t sbal = (sb + 255) & ~(size_t)255;
+    const size_t rb = sizeof(qfbw::WStr) * std::max<size_t>(1, pl->strs.size());
+    int rc = dev_alloc(&pl->blob, sbal + rb);
+    if (rc) return rc;
+    pl->d_steps = (qfbw::WStep *)pl->blob;
+    pl->d_strs = (qfbw::WStr *)((char *)pl->blob + sbal);
+    if (!pl->steps.empty())
+        QFB_CUDA(cudaMemcpyAsync(pl->d_steps, pl->steps.data(), sb, cudaMemcpyHostToDevice,
+                                 t_stream));
+    if (!pl->strs.empty())
+        QFB_CUDA(cudaMemcpyAsync(pl->d_strs, pl->strs.data(), rb, cudaMemcpyHostToDevice,
+                                 t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    for (const auto &w : pl->wins)
+        pl->smem_max = std::max(pl->smem_max,
+                                qfbw::win_smem_bytes(w.b, pl->L, w.sr1 - w.sr0, pl->nt));
+    return QFB_OK;
+}
+
+// Forward windows: consecutive steps whose x-supports fit in the tile.
+static int build_fwd_plan(qfb_prog_s *p, int n, WinPlan **out) {
+    WinPlan *pl = new WinPlan;
+    pl->nqubit = n;
+    pl->b = std::min(kFwdTileBits, n);
+    pl->L = std::min(kLowBits, pl->b);
+    pl->nt = 1;
+    const uint64_t low = (1ull << pl->L) - 1ull;
+    const int room = pl->b - pl->L;
+    const size_t K = p->h_steps.size();
+    size_t i = 0;
+    while (i < K) {
+        const StepDev &s0 = p->h_steps[i];
+        if (__builtin_popcountll(s0.x & ~low) > room || s0.ns > qfbw::kWinMaxStr) {
+            qfbw::Window w{};
+            w.global_step = (int32_t)i;
+            w.global_mu = -1;
+            pl->wins.push_back(w);
+            ++i;
+            continue;
+        }
+        uint64_t U = s0.x;
+        size_t j = i + 1;
+        int nstr = s0.ns;
+        while (j < K) {
+            const StepDev &sj = p->h_steps[j];
+            const uint64_t U2 = U | sj.x;
+            if (__builtin_popcountll(U2 & ~low) > room || nstr + sj.ns > qfbw::kWinMaxStr) break;
+            U = U2;
+            nstr += sj.ns;
+            ++j;
+        }
+        qfbw::Window w = make_window(U & ~low, n, pl->b, pl->L);
+        w.st0 = (int32_t)pl->steps.size();
+        w.sr0 = (int32_t)pl->strs.size();
+        for (size_t k = i; k < j; ++k) {
+            push_step(pl, w, p->h_steps[k], 1, -1);
+            push_strings(pl, p, p->h_steps[k], w.qmask, +1, false);
+        }
+        w.st1 = (int32_t)pl->steps.size();
+        w.sr1 = (int32_t)pl->strs.size();
+        pl->wins.push_back(w);
+        i = j;
+    }
+    int rc = upload_plan(pl);
+    if (rc) {
+        delete pl;
+        return rc;
+    }
+    *out = pl;
+    return QFB_OK;
+}
+
+// Gradient windows: the reverse sweep over parameters; per parameter the
+// inner product(s) <sigma|K_mu|psi> on kp's strings, then (except for the
+// first parameter) U_mu^dagger from up's strings in reverse.  When kp and up
+// are one program and the parameter is one x-group, both share one pass.
+static int build_grad_plan(qfb_prog_s *kp, const qfb_prog_s *up, int n, WinPlan **out) {
+    WinPlan *pl = new WinPlan;
+    pl->nqubit = n;
+    pl->b = std::min(kGradTileBits, n);
+    pl->L = std::min(kLowBits, pl->b);
+    pl->nt = 2;
+    const uint64_t low = (1ull << pl->L) - 1ull;
+    const int room = pl->b - pl->L;
+    const int M = kp->nparam;
+    auto steps_of = [](const qfb_prog_s *p, int m, int32_t &a0, int32_t &a1) {
+        a0 = p->p_step0[m];
+        a1 = p->p_step1[m];
+        if (a0 < 0) a0 = a1 = 0;
+    };
+    auto supp = [&](int m) {
+        uint64_t u = 0;
+        int32_t a0, a1;
+        steps_of(kp, m, a0, a1);
+        for (int32_t s = a0; s < a1; ++s) u |= kp->h_steps[s].x;
+        steps_of(up, m, a0, a1);
+        for (int32_t s = a0; s < a1; ++s) u |= up->h_steps[s].x;
+        return u;
+    };
+    auto nstr_of = [&](int m) {
+        int c = 0;
+        int32_t a0, a1;
+        steps_of(kp, m, a0, a1);
+        for (int32_t s = a0; s < a1; ++s) c += kp->h_steps[s].ns;
+        steps_of(up, m, a0, a1);
+        for (int32_t s = a0; s < a1; ++s) c += up->h_steps[s].ns;
+        return c;
+    };
+    auto empty = [&](int m) { return kp->p_step0[m] < 0 && up->p_step0[m] < 0; };
+    int mu = M - 1;
+    while (mu >= 0) {
+        if (empty(mu)) {
+            --mu;
+            continue;
+        }
+        if (__builtin_popcountll(supp(mu) & ~low) > room || nstr_of(mu) > qfbw::kWinMaxStr) {
+            qfbw::Window w{};
+            w.global_step = -1;
+            w.global_mu = mu;
+            pl->wins.push_back(w);
+            --mu;
+            continue;
+        }
+        uint64_t U = supp(mu);
+        int nstr = nstr_of(mu);
+        int lo = mu;
+        while (lo - 1 >= 0) {
+            const int m = lo - 1;
+            if (empty(m)) {
+                --lo;
+                continue;
+            }
+            const uint64_t U2 = U | supp(m);
+            if (__builtin_popcountll(U2 & ~low) > room || nstr + nstr_of(m) > qfbw::kWinMaxStr)
+                break;
+            U = U2;
+            nstr += nstr_of(m);
+            --lo;
+        }
+        qfbw::Window w = make_window(U & ~low, n, pl->b, pl->L);
+        w.st0 = (int32_t)pl->steps.size();
+        w.sr0 = (int32_t)pl->strs.size();
+        for (int m = mu; m >= lo; --m) {
+            const int rot = (m > 0) ? 1 : 0;
+            int32_t k0, k1, u0, u1;
+            steps_of(kp, m, k0, k1);
+            steps_of(up, m, u0, u1);
+            if (kp == up && k1 - k0 == 1) {
+                push_step(pl, w, kp->h_steps[k0], rot, k0);
+                push_strings(pl, kp, kp->h_steps[k0], w.qmask, -1, true);
+                continue;
+            }
+            for (int32_t s = k0; s < k1; ++s) {
+                push_step(pl, w, kp->h_steps[s], 0, s);
+                push_strings(pl, kp, kp->h_steps[s], w.qmask, -1, true);
+            }
+            if (rot)
+                for (int32_t s = u1 - 1; s >= u0; --s) {
+                    push_step(pl, w, up->h_steps[s], 1, -1);
+                    push_strings(pl, up, up->h_steps[s], w.qmask, -1, true);
+                }
+        }
+        w.st1 = (int32_t)pl->steps.size();
+        w.sr1 = (int32_t)pl->strs.size();
+        pl->wins.push_back(w);
+        mu = lo - 1;
+    }
+    int rc = upload_plan(pl);
+    if (rc) {
+        delete pl;
+        return rc;
+    }
+    *out = pl;
+    return QFB_OK;
+}
+
+static int ensure_plans(qfb_prog_s *p, int n, bool fwd, const qfb_prog_s *up = nullptr) {
+    if (n < 1 || n > 40) return fail(QFB_EINVAL, "window plan: bad qubit count %d", n);
+    int rc = QFB_OK;
+    if (fwd && !p->fwd_plan[n]) rc = build_fwd_plan(p, n, &p->fwd_plan[n]);
+    if (rc == QFB_OK && up && p->grad_plan_u[n] != up) {
+        if (p->grad_plan[n]) {
+            dev_free(p->grad_plan[n]->blob);
+            delete p->grad_plan[n];
+            p->grad_plan[n] = nullptr;
+        }
+        rc = build_grad_plan(p, up, n, &p->grad_plan[n]);
+        p->grad_plan_u[n] = (rc == QFB_OK) ? up : nullptr;
+    }
+    return rc;
+}
+
+static int set_win_smem(size_t bytes, int nt) {
+    static size_t done[3] = {0, 0, 0};
+    if (bytes <= done[nt]) return QFB_OK;
+    if (bytes > 227 * 1024)
+        return fail(QFB_ENOSYS, "window of %zu bytes of shared memory", bytes);
+    if (nt == 1)
+        QFB_CUDA(cudaFuncSetAttribute(qfbw::k_window<1>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    else
+        QFB_CUDA(cudaFuncSetAttribute(qfbw::k_window<2>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done[nt] = bytes;
+    return QFB_OK;
+}
+
+static int launch_window(const WinPlan *pl, const qfbw::Window &w, double2 *psi, double2 *sig,
+                         uint64_t nbasis, int B, const double *d_par, int nparam, int bcast,
+                         double2 *partial) {
+    qfbw::WinLaunch a;
+    a.qmask = w.qmask;
+    a.cmask = w.cmask;
+    a.b = w.b;
+    a.L = pl->L;
+    a.nsteps = w.st1 - w.st0;
+    a.nstr = w.sr1 - w.sr0;
+    a.steps = pl->d_steps + w.st0;
+    a.strs = pl->d_strs + w.sr0;
+    a.params = d_par;
+    a.nparam = nparam;
+    a.bcast = bcast;
+    a.partial = partial;
+    a.ntiles = pl->ntiles();
+    const size_t smem = qfbw::win_smem_bytes(w.b, pl->L, a.nstr, pl->nt);
+    const dim3 grid((unsigned)a.ntiles, (unsigned)B);
+    if (pl->nt == 1)
+        qfbw::k_window<1><<<grid, qfbw::kWinThreads, smem, t_stream>>>(psi, nullptr, nbasis, a);
+    else
+        qfbw::k_window<2><<<grid, qfbw::kWinThreads, smem, t_stream>>>(psi, sig, nbasis, a);
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
 
 int upload_params(const double *params, int32_t nrows, int32_t nparam, double **d_out) {
     *d_out = nullptr;
@@ -434,6 +815,9 @@ unsigned chunks_for(uint64_t npair, int nbatch, int nrows_of_work) {
 }  // namespace
 
 extern "C" {
+
+static int enqueue_sum_apply(const qfb_sum_s *h, double2 *dst, const double2 *src,
+                             uint64_t nbasis, int B);
 
 int qfb_sum_create(const qfb_pauli *paulis, const qfb_complex *coeffs, const int32_t *segment,
                    int64_t nterms, int32_t nsegment, qfb_sum *out) {
@@ -501,23 +885,36 @@ int qfb_sum_create(const qfb_pauli *paulis, const qfb_complex *coeffs, const int
         h->h_seg_g0.push_back((int32_t)h->h_groups.size());
     }
     h->ngroups = (int32_t)h->h_groups.size();
-    const size_t gbytes = sizeof(GroupDev) * std::max<size_t>(1, h->h_groups.size());
-    const size_t tbytes = sizeof(TermDev) * std::max<size_t>(1, terms.size());
+    // each sub-array starts on a 256-byte boundary (TermDev holds a double2)
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t gbytes = al(sizeof(GroupDev) * std::max<size_t>(1, h->h_groups.size()));
+    const size_t tbytes = al(sizeof(TermDev) * std::max<size_t>(1, terms.size()));
+    const size_t rbytes = al(sizeof(double2) * std::max<size_t>(1, terms.size()));
     const size_t sbytes = sizeof(int32_t) * h->h_seg_g0.size();
-    int rc = dev_alloc(&h->blob, gbytes + tbytes + sbytes);
+    std::vector<double2> rterms(terms.size());
+    for (size_t t = 0; t < terms.size(); ++t) {
+        double zb;
+        std::memcpy(&zb, &terms[t].z, sizeof(double));
+        rterms[t] = make_double2(zb, terms[t].c.x);
+    }
+    int rc = dev_alloc(&h->blob, gbytes + tbytes + rbytes + sbytes);
     if (rc) {
         delete h;
         return rc;
     }
     h->d_groups = (GroupDev *)h->blob;
     h->d_terms = (TermDev *)((char *)h->blob + gbytes);
-    h->d_seg_g0 = (int32_t *)((char *)h->blob + gbytes + tbytes);
+    h->d_rterms = (double2 *)((char *)h->blob + gbytes + tbytes);
+    h->d_seg_g0 = (int32_t *)((char *)h->blob + gbytes + tbytes + rbytes);
     cudaError_t e = cudaSuccess;
     if (!h->h_groups.empty())
         e = cudaMemcpyAsync(h->d_groups, h->h_groups.data(), sizeof(GroupDev) * h->h_groups.size(),
                             cudaMemcpyHostToDevice, t_stream);
     if (e == cudaSuccess && !terms.empty())
         e = cudaMemcpyAsync(h->d_terms, terms.data(), sizeof(TermDev) * terms.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess && !rterms.empty())
+        e = cudaMemcpyAsync(h->d_rterms, rterms.data(), sizeof(double2) * rterms.size(),
                             cudaMemcpyHostToDevice, t_stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(h->d_seg_g0, h->h_seg_g0.data(), sbytes, cudaMemcpyHostToDevice,
@@ -599,11 +996,7 @@ int qfb_sum_apply(qfb_sum h, qfb_state dst, qfb_state src) {
         if (g.h >= src->nqubit)
             return fail(QFB_EINVAL, "qfb_sum_apply: operator acts on qubit %d of a %d-qubit state",
                         g.h, src->nqubit);
-    const dim3 grid(grid_for(src->nbasis, 256), src->nbatch);
-    k_sum_apply<<<grid, 256, 0, t_stream>>>(dst->d, src->d, src->nbasis, h->d_groups, h->d_terms,
-                                            h->ngroups);
-    QFB_LAUNCHED();
-    return QFB_OK;
+    return enqueue_sum_apply(h, dst->d, src->d, src->nbasis, src->nbatch);
 }
 
 int qfb_prog_create(const qfb_pauli *paulis, const double *scale, const int32_t *param,
@@ -704,61 +1097,123 @@ static int check_prog_state(qfb_prog p, qfb_state s, int32_t nrows, const char *
 
 // ---- enqueue helpers: kernels only, no allocation, no host synchronisation --
 
-static int enqueue_prog(const qfb_prog_s *p, double2 *psi, uint64_t nbasis, int B,
-                        const double *d_par, int bcast, int sign) {
+static int enqueue_step(const qfb_prog_s *p, const StepDev &st, double2 *psi, uint64_t nbasis,
+                        int B, const double *d_par, int bcast, int sign) {
     StepParams sp{p->d_strs, d_par, p->nparam, bcast, sign};
     const dim3 grid(grid_for(nbasis >> 1, 256, 4), B);
+    k_prog_step<<<grid, 256, 0, t_stream>>>(psi, nbasis, st, sp);
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
+// U (sign +1) or U^dagger (sign -1).  Forward application runs the window
+// plan of this qubit count when one has been built (ensure_plans).
+static int enqueue_prog(const qfb_prog_s *p, double2 *psi, int nqubit, int B,
+                        const double *d_par, int bcast, int sign) {
+    const uint64_t nbasis = 1ull << nqubit;
+    const WinPlan *pl = (sign > 0) ? p->fwd_plan[nqubit] : nullptr;
+    if (pl) {
+        int rc = set_win_smem(pl->smem_max, 1);
+        if (rc) return rc;
+        for (const auto &w : pl->wins) {
+            rc = (w.global_step >= 0)
+                     ? enqueue_step(p, p->h_steps[w.global_step], psi, nbasis, B, d_par, bcast, 1)
+                     : launch_window(pl, w, psi, nullptr, nbasis, B, d_par, p->nparam, bcast,
+                                     nullptr);
+            if (rc) return rc;
+        }
+        return QFB_OK;
+    }
     const int64_t ns = (int64_t)p->h_steps.size();
     for (int64_t k = 0; k < ns; ++k) {
-        const StepDev &st = p->h_steps[sign > 0 ? k : ns - 1 - k];
-        k_prog_step<<<grid, 256, 0, t_stream>>>(psi, nbasis, st, sp);
-        QFB_LAUNCHED();
+        int rc = enqueue_step(p, p->h_steps[sign > 0 ? k : ns - 1 - k], psi, nbasis, B, d_par,
+                              bcast, sign);
+        if (rc) return rc;
     }
     return QFB_OK;
 }
 
 static int enqueue_sum_apply(const qfb_sum_s *h, double2 *dst, const double2 *src,
                              uint64_t nbasis, int B) {
-    const dim3 grid(grid_for(nbasis, 256), B);
-    k_sum_apply<<<grid, 256, 0, t_stream>>>(dst, src, nbasis, h->d_groups, h->d_terms,
-                                            h->ngroups);
+    if (nbasis >= 4) {
+        const dim3 grid(grid_for(nbasis >> 2, 256), B);
+        k_sum_apply4<<<grid, 256, 0, t_stream>>>(dst, src, nbasis, h->d_groups, h->d_terms,
+                                                 h->d_rterms, h->ngroups);
+    } else {
+        const dim3 grid(grid_for(nbasis, 256), B);
+        k_sum_apply<<<grid, 256, 0, t_stream>>>(dst, src, nbasis, h->d_groups, h->d_terms,
+                                                h->ngroups);
+    }
     QFB_LAUNCHED();
     return QFB_OK;
 }
 
-// Reverse sweep of the adjoint gradient.  partial holds nsteps * B * chunks
-// entries; row (s * B + b) receives step s's share of <sigma|K_mu|psi>.
-static int enqueue_gradient(const qfb_prog_s *kp, double2 *psi, double2 *sig, uint64_t nbasis,
-                            int B, const double *d_par, int bcast, double2 *partial,
-                            unsigned chunks) {
-    const int M = kp->nparam;
-    StepParams sp{kp->d_strs, d_par, M, bcast, -1};
+// The reverse sweep of one parameter with the per-step kernels; partial
+// rows are laid out [step][slot][chunks].
+static int enqueue_grad_mu(const qfb_prog_s *kp, const qfb_prog_s *up, int mu, double2 *psi,
+                           double2 *sig, uint64_t nbasis, int B, const double *d_par, int bcast,
+                           double2 *partial, unsigned chunks) {
+    StepParams kpar{kp->d_strs, d_par, kp->nparam, bcast, -1};
+    StepParams upar{up->d_strs, d_par, up->nparam, bcast, -1};
     const dim3 grid(chunks, B);
-    for (int mu = M - 1; mu >= 0; --mu) {
-        const int32_t s0 = kp->p_step0[mu], s1 = kp->p_step1[mu];
-        if (s0 < 0) continue;  // parameter without strings: gradient 0
-        const bool last = (mu == 0);
-        if (s1 - s0 == 1) {
-            k_grad_step<<<grid, 256, 0, t_stream>>>(psi, sig, nbasis, kp->h_steps[s0], sp,
-                                                    last ? 0 : 1, s0, partial);
-            QFB_LAUNCHED();
-            continue;
+    const int32_t s0 = kp->p_step0[mu], s1 = kp->p_step1[mu];
+    const bool last = (mu == 0);
+    if (kp == up && s0 >= 0 && s1 - s0 == 1) {
+        k_grad_step<<<grid, 256, 0, t_stream>>>(psi, sig, nbasis, kp->h_steps[s0], kpar,
+                                                last ? 0 : 1, s0, partial);
+        QFB_LAUNCHED();
+        return QFB_OK;
+    }
+    // first every inner product on (psi_mu, sigma_mu) ...
+    for (int32_t s = s0; s >= 0 && s < s1; ++s) {
+        k_grad_step<<<grid, 256, 0, t_stream>>>(psi, sig, nbasis, kp->h_steps[s], kpar, 0, s,
+                                                partial);
+        QFB_LAUNCHED();
+    }
+    if (last) return QFB_OK;
+    // ... then U_mu^dagger on both states, steps in reverse order
+    const dim3 g2(grid_for(nbasis >> 1, 256, 4), B);
+    const int32_t u0 = up->p_step0[mu], u1 = up->p_step1[mu];
+    for (int32_t s = u1 - 1; u0 >= 0 && s >= u0; --s) {
+        k_prog_step<<<g2, 256, 0, t_stream>>>(psi, nbasis, up->h_steps[s], upar);
+        QFB_LAUNCHED();
+        k_prog_step<<<g2, 256, 0, t_stream>>>(sig, nbasis, up->h_steps[s], upar);
+        QFB_LAUNCHED();
+    }
+    return QFB_OK;
+}
+
+// Partial-row chunks of the gradient sweep for this program and qubit count.
+static unsigned grad_chunks(const qfb_prog_s *kp, int nqubit, int B) {
+    const WinPlan *pl = kp->grad_plan[nqubit];
+    return pl ? (unsigned)pl->ntiles() : chunks_for((1ull << nqubit) >> 1, B, 1);
+}
+
+// Reverse sweep of the adjoint gradient.  partial holds nsteps(kp) * B *
+// chunks entries (chunks = grad_chunks); row (s * B + b) receives step s's
+// share of <sigma|K_mu|psi>.
+static int enqueue_gradient(const qfb_prog_s *kp, const qfb_prog_s *up, double2 *psi,
+                            double2 *sig, int nqubit, int B, const double *d_par, int bcast,
+                            double2 *partial) {
+    const uint64_t nbasis = 1ull << nqubit;
+    const unsigned chunks = grad_chunks(kp, nqubit, B);
+    const WinPlan *pl = (kp->grad_plan_u[nqubit] == up) ? kp->grad_plan[nqubit] : nullptr;
+    if (pl) {
+        int rc = set_win_smem(pl->smem_max, 2);
+        if (rc) return rc;
+        for (const auto &w : pl->wins) {
+            rc = (w.global_mu >= 0)
+                     ? enqueue_grad_mu(kp, up, w.global_mu, psi, sig, nbasis, B, d_par, bcast,
+                                       partial, chunks)
+                     : launch_window(pl, w, psi, sig, nbasis, B, d_par, kp->nparam, bcast,
+                                     partial);
+            if (rc) return rc;
         }
-        // several x-groups: first every inner product on (psi_mu, sigma_mu) ...
-        for (int32_t s = s0; s < s1; ++s) {
-            k_grad_step<<<grid, 256, 0, t_stream>>>(psi, sig, nbasis, kp->h_steps[s], sp, 0, s,
-                                                    partial);
-            QFB_LAUNCHED();
-        }
-        if (last) continue;
-        // ... then U_mu^dagger on both states, steps in reverse order
-        const dim3 g2(grid_for(nbasis >> 1, 256, 4), B);
-        for (int32_t s = s1 - 1; s >= s0; --s) {
-            k_prog_step<<<g2, 256, 0, t_stream>>>(psi, nbasis, kp->h_steps[s], sp);
-            QFB_LAUNCHED();
-            k_prog_step<<<g2, 256, 0, t_stream>>>(sig, nbasis, kp->h_steps[s], sp);
-            QFB_LAUNCHED();
-        }
+        return QFB_OK;
+    }
+    for (int mu = kp->nparam - 1; mu >= 0; --mu) {
+        int rc = enqueue_grad_mu(kp, up, mu, psi, sig, nbasis, B, d_par, bcast, partial, chunks);
+        if (rc) return rc;
     }
     return QFB_OK;
 }
@@ -770,31 +1225,42 @@ int qfb_prog_apply(qfb_prog p, qfb_state s, const double *params, int32_t nrows,
     int rc = check_prog_state(p, s, nrows, "qfb_prog_apply");
     if (rc) return rc;
     if (p->h_steps.empty()) return QFB_OK;
+    if (sign > 0) {
+        rc = ensure_plans(p, s->nqubit, true);
+        if (rc) return rc;
+    }
     double *d_par = nullptr;
     rc = upload_params(params, nrows, p->nparam, &d_par);
     if (rc) return rc;
-    rc = enqueue_prog(p, s->d, s->nbasis, s->nbatch, d_par, nrows == 1 ? 1 : 0, sign);
+    rc = enqueue_prog(p, s->d, s->nqubit, s->nbatch, d_par, nrows == 1 ? 1 : 0, sign);
     dev_free(d_par);
     return rc;
 }
 
-int qfb_ucc_gradient(qfb_prog kp, qfb_state psi, qfb_state sig, const double *params,
-                     int32_t nrows, double *grad) {
-    if (!kp || !psi || !sig || !grad) return fail(QFB_EINVAL, "qfb_ucc_gradient: null argument");
+int qfb_ucc_gradient(qfb_prog kp, qfb_prog up, qfb_state psi, qfb_state sig,
+                     const double *params, int32_t nrows, double *grad) {
+    if (!kp || !up || !psi || !sig || !grad)
+        return fail(QFB_EINVAL, "qfb_ucc_gradient: null argument");
     if (kp->nparam > 0 && !params) return fail(QFB_EINVAL, "qfb_ucc_gradient: null parameters");
     if (psi->nqubit != sig->nqubit || psi->nbatch != sig->nbatch)
         return fail(QFB_EINVAL, "qfb_ucc_gradient: psi and sigma shapes differ");
     if (psi == sig) return fail(QFB_EINVAL, "qfb_ucc_gradient: psi and sigma must differ");
-    if (!kp->params_contiguous)
+    if (up->nparam != kp->nparam)
+        return fail(QFB_EINVAL, "qfb_ucc_gradient: K and U programs have %d and %d parameters",
+                    kp->nparam, up->nparam);
+    if (!kp->params_contiguous || !up->params_contiguous)
         return fail(QFB_EINVAL, "qfb_ucc_gradient: each parameter's strings must be contiguous");
     int rc = check_prog_state(kp, psi, nrows, "qfb_ucc_gradient");
+    if (rc == QFB_OK) rc = check_prog_state(up, psi, nrows, "qfb_ucc_gradient");
     if (rc) return rc;
     const int M = kp->nparam, B = psi->nbatch;
     if (M == 0) return QFB_OK;
+    rc = ensure_plans(kp, psi->nqubit, false, up);
+    if (rc) return rc;
     double *d_par = nullptr;
     rc = upload_params(params, nrows, M, &d_par);
     if (rc) return rc;
-    const unsigned chunks = chunks_for(psi->nbasis >> 1, B, 1);
+    const unsigned chunks = grad_chunks(kp, psi->nqubit, B);
     const size_t nrow = (size_t)std::max<size_t>(kp->h_steps.size(), 1) * B;
     void *buf = nullptr;
     rc = dev_alloc(&buf, sizeof(double2) * nrow * chunks + sizeof(double) * (size_t)B * M +
@@ -810,8 +1276,8 @@ int qfb_ucc_gradient(qfb_prog kp, qfb_state psi, qfb_state sig, const double *pa
     for (int mu = 0; mu < M; ++mu)
         ps[mu] = make_int2(std::max(kp->p_step0[mu], 0), std::max(kp->p_step1[mu], 0));
     QFB_CUDA(cudaMemcpyAsync(d_ps, ps.data(), sizeof(int2) * M, cudaMemcpyHostToDevice, t_stream));
-    rc = enqueue_gradient(kp, psi->d, sig->d, psi->nbasis, B, d_par, nrows == 1 ? 1 : 0, partial,
-                          chunks);
+    rc = enqueue_gradient(kp, up, psi->d, sig->d, psi->nqubit, B, d_par, nrows == 1 ? 1 : 0,
+                          partial);
     if (rc == QFB_OK) {
         k_grad_final<<<dim3(M, B), 128, 0, t_stream>>>(partial, d_ps, chunks, d_grad);
         QFB_LAUNCHED();
@@ -831,8 +1297,9 @@ int qfb_ucc_gradient(qfb_prog kp, qfb_state psi, qfb_state sig, const double *pa
 // ===========================================================================
 
 struct qfb_ucc_s {
-    const qfb_prog_s *fwd = nullptr;
-    const qfb_prog_s *grad = nullptr;
+    qfb_prog_s *fwd = nullptr;
+    qfb_prog_s *grad = nullptr;   // K_mu (inner products)
+    qfb_prog_s *unrot = nullptr;  // U_mu (un-rotation)
     const qfb_sum_s *ham = nullptr;
     int nqubit = 0, nbatch = 0, nparam = 0;
     uint64_t nbasis = 0, ref = 0;
@@ -857,7 +1324,7 @@ static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
             QFB_LAUNCHED();
             break;
         case 1:
-            rc = enqueue_prog(u->fwd, u->psi, u->nbasis, B, u->params, 0, 1);
+            rc = enqueue_prog(u->fwd, u->psi, u->nqubit, B, u->params, 0, 1);
             break;
         case 2:
             rc = enqueue_sum_apply(u->ham, u->sig, u->psi, u->nbasis, B);
@@ -870,8 +1337,8 @@ static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
             break;
         default:
             if (with_grad && u->grad && u->nparam > 0) {
-                rc = enqueue_gradient(u->grad, u->psi, u->sig, u->nbasis, B, u->params, 0,
-                                      u->gpart, u->gchunks);
+                rc = enqueue_gradient(u->grad, u->unrot, u->psi, u->sig, u->nqubit, B,
+                                      u->params, 0, u->gpart);
                 if (rc) return rc;
                 k_grad_final<<<dim3(u->nparam, B), 128, 0, t_stream>>>(u->gpart, u->psteps,
                                                                      u->gchunks, u->gradv);
@@ -892,29 +1359,37 @@ static int ucc_enqueue(qfb_ucc u, int with_grad) {
 
 extern "C" {
 
-int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_sum ham, int nqubit, uint64_t ref_index,
-                   int nbatch, qfb_ucc *out) {
+int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, int nqubit,
+                   uint64_t ref_index, int nbatch, qfb_ucc *out) {
     if (!out) return fail(QFB_EINVAL, "qfb_ucc_create: null output");
     *out = nullptr;
     if (!fprog || !ham) return fail(QFB_EINVAL, "qfb_ucc_create: null program or Hamiltonian");
     if (nqubit < 1 || nqubit > 40 || nbatch < 1)
         return fail(QFB_EINVAL, "qfb_ucc_create: nqubit = %d, nbatch = %d", nqubit, nbatch);
     if (ref_index >> nqubit) return fail(QFB_EINVAL, "qfb_ucc_create: reference index too large");
-    if (gprog && (gprog->nparam != fprog->nparam || !gprog->params_contiguous))
-        return fail(QFB_EINVAL, "qfb_ucc_create: gradient program does not match the ansatz");
+    if ((gprog == nullptr) != (uprog == nullptr))
+        return fail(QFB_EINVAL, "qfb_ucc_create: give both gradient programs or neither");
+    if (gprog && (gprog->nparam != fprog->nparam || !gprog->params_contiguous ||
+                  uprog->nparam != fprog->nparam || !uprog->params_contiguous))
+        return fail(QFB_EINVAL, "qfb_ucc_create: gradient programs do not match the ansatz");
     for (const auto &g : ham->h_groups)
         if (g.h >= nqubit) return fail(QFB_EINVAL, "qfb_ucc_create: H acts beyond qubit %d", nqubit);
     for (const qfb_prog_s *p : {static_cast<const qfb_prog_s *>(fprog),
-                                static_cast<const qfb_prog_s *>(gprog)}) {
+                                static_cast<const qfb_prog_s *>(gprog),
+                                static_cast<const qfb_prog_s *>(uprog)}) {
         if (!p) continue;
         for (const auto &st : p->h_steps)
             if (st.h >= nqubit) return fail(QFB_EINVAL, "qfb_ucc_create: program beyond qubit");
         for (const auto &sd : p->h_strs)
             if (sd.z >> nqubit) return fail(QFB_EINVAL, "qfb_ucc_create: program beyond qubit");
     }
+    int prc = ensure_plans(fprog, nqubit, true);
+    if (prc == QFB_OK && gprog) prc = ensure_plans(gprog, nqubit, false, uprog);
+    if (prc) return prc;
     qfb_ucc u = new qfb_ucc_s;
     u->fwd = fprog;
     u->grad = gprog;
+    u->unrot = uprog;
     u->ham = ham;
     u->nqubit = nqubit;
     u->nbatch = nbatch;
@@ -923,7 +1398,7 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_sum ham, int nqubit, uint
     u->ref = ref_index;
     u->vchunks = grid_for(u->nbasis, 256, 2);
     if (u->vchunks * (unsigned)nbatch > 65535u) u->vchunks = std::max(1u, 65535u / nbatch);
-    u->gchunks = chunks_for(u->nbasis >> 1, nbatch, 1);
+    u->gchunks = gprog ? grad_chunks(gprog, nqubit, nbatch) : 1;
     const size_t B = nbatch, M = std::max(u->nparam, 1);
     const size_t nsteps = gprog ? std::max<size_t>(gprog->h_steps.size(), 1) : 1;
     const size_t b_state = sizeof(double2) * u->nbasis * B;

@@ -1,0 +1,243 @@
+// Windowed Pauli-exponential passes over shared-memory tiles.
+//
+// exp(i phi P) couples amplitude j only with j ^ x (x = P's X/Y support), and
+// its phase (-1)^popcount(j & z) splits into the bits of j inside any qubit
+// set Q and a sign that is constant over the rest.  So if every step of a
+// run of consecutive exponentials has its x inside one set Q of b qubits, the
+// state splits into 2^(n-b) independent tiles (the indices that agree outside
+// Q), and the whole run can be applied to each tile in shared memory: one
+// read and one write of the state per run instead of per exponential.
+//
+// The planner walks a program (forward: strings in order; gradient: the
+// reverse sweep of UCCVQE.measure_gradient, uccvqeabc.py:122-251) and cuts it
+// into windows whose x-supports fit in b qubits.  Q always holds the lowest L
+// qubits, so a tile is gathered in contiguous runs of 2^L amplitudes (128 B
+// for L = 3), and is padded with the lowest unused qubits up to b.  Each
+// window is one launch over (tile, slot); in gradient windows a step can
+// also accumulate its share of <sigma|K_mu|psi> (one partial per tile).
+//
+// The arithmetic per pair is the per-step kernel's, step for step, so a
+// windowed program produces the same amplitudes as the unwindowed one.
+#pragma once
+
+#include <vector>
+
+namespace qfbw {
+
+struct WStep {       // one step of a window, masks in tile coordinates
+    uint64_t xl;     // x compressed into the tile's bits
+    int32_t hl;      // highest bit of xl, -1 when xl == 0 (diagonal)
+    int32_t s0;      // first string (window-relative)
+    int32_t ns;      // strings
+    int32_t rotate;  // apply the rotation
+    int32_t ip_row;  // >= 0: add this step's <sigma|K|psi> share to that row
+    int32_t pad;
+};
+
+struct WStr {
+    uint64_t zl;    // z compressed into the tile's bits
+    uint64_t zc;    // z outside the tile (per-tile constant sign)
+    int32_t ny;     // popcount(x & z) mod 4
+    int32_t param;  // parameter index
+    double rscale;  // rotation angle = rscale * params[param] (sign included)
+    double scale;   // K coefficient is i * scale (inner products)
+};
+
+struct Window {
+    uint64_t qmask, cmask;
+    int32_t b;
+    int32_t st0, st1;        // steps [st0, st1) of the plan
+    int32_t sr0, sr1;        // strings [sr0, sr1) of the plan
+    int32_t global_step;     // >= 0: not windowed, run this program step globally
+    int32_t global_mu;       // >= 0: not windowed, run parameter mu's gradient globally
+};
+
+constexpr int kWinMaxStr = 512;
+constexpr int kWinThreads = 512;
+
+inline uint64_t pext_h(uint64_t v, uint64_t m) {
+    uint64_t r = 0;
+    int k = 0;
+    while (m) {
+        const uint64_t low = m & (~m + 1);
+        if (v & low) r |= 1ull << k;
+        ++k;
+        m &= m - 1;
+    }
+    return r;
+}
+
+__device__ __forceinline__ uint64_t pdep_d(uint64_t v, uint64_t m) {
+    uint64_t r = 0;
+    while (m) {
+        const uint64_t low = m & (~m + 1);
+        if (v & 1ull) r |= low;
+        v >>= 1;
+        m &= m - 1;
+    }
+    return r;
+}
+
+struct WinLaunch {
+    uint64_t qmask, cmask;
+    int b, L;
+    int nsteps, nstr;
+    const WStep *steps;  // this window's steps
+    const WStr *strs;    // this window's strings
+    const double *params;
+    int nparam, bcast;
+    double2 *partial;  // [rows][nbatch][ntiles]
+    int ntiles;
+};
+
+__host__ __device__ inline size_t win_smem_bytes(int b, int L, int nstr, int nt) {
+    const size_t T = (size_t)1 << b;
+    size_t o = nt * T * sizeof(double2);
+    o += (size_t)nstr * (sizeof(double2) + sizeof(double) + sizeof(uint64_t) + sizeof(int));
+    o = (o + 15) & ~(size_t)15;
+    o += ((size_t)1 << (b - L)) * sizeof(uint64_t);
+    return o;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ psi,
+                                                        double2 *__restrict__ sig,
+                                                        uint64_t nbasis, WinLaunch a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = 1 << a.b;
+    double2 *t0 = reinterpret_cast<double2 *>(smem);
+    double2 *t1 = t0 + T;
+    double2 *s_cs = t0 + (size_t)NT * T;
+    double *s_sc = reinterpret_cast<double *>(s_cs + a.nstr);
+    uint64_t *s_zl = reinterpret_cast<uint64_t *>(s_sc + a.nstr);
+    int *s_q = reinterpret_cast<int *>(s_zl + a.nstr);
+    size_t o = (size_t)NT * T * sizeof(double2) +
+               (size_t)a.nstr * (sizeof(double2) + sizeof(double) + sizeof(uint64_t) + sizeof(int));
+    o = (o + 15) & ~(size_t)15;
+    uint64_t *s_tab = reinterpret_cast<uint64_t *>(smem + o);
+
+    const int slot = blockIdx.y, tile = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    const uint64_t base = pdep_d((uint64_t)tile, a.cmask);
+    for (int h = tid; h < (T >> a.L); h += nth) s_tab[h] = pdep_d((uint64_t)h << a.L, a.qmask);
+    const double *par = a.params + (a.bcast ? 0 : (size_t)slot * a.nparam);
+    for (int i = tid; i < a.nstr; i += nth) {
+        const WStr w = a.strs[i];
+        double s, c;
+        sincos(w.rscale * par[w.param], &s, &c);
+        s_cs[i] = make_double2(c, s);
+        s_sc[i] = w.scale;
+        s_zl[i] = w.zl;
+        s_q[i] = (w.ny + 1 + 2 * parity64(base & w.zc)) & 3;
+    }
+    __syncthreads();
+    const uint64_t lowm = (1ull << a.L) - 1ull;
+    double2 *P = psi + (uint64_t)slot * nbasis;
+    double2 *S = (NT == 2) ? sig + (uint64_t)slot * nbasis : nullptr;
+    for (int l = tid; l < T; l += nth) {
+        const uint64_t g = base | s_tab[l >> a.L] | ((uint64_t)l & lowm);
+        t0[l] = P[g];
+        if (NT == 2) t1[l] = S[g];
+    }
+    __syncthreads();
+
+    for (int st = 0; st < a.nsteps; ++st) {
+        const WStep w = a.steps[st];
+        double2 ip = make_double2(0.0, 0.0);
+        const bool want_ip = (NT == 2) && (w.ip_row >= 0);
+        if (w.hl >= 0) {
+            for (int p = tid; p < (T >> 1); p += nth) {
+                const uint64_t l0 = insert0((uint64_t)p, w.hl), l1 = l0 ^ w.xl;
+                double2 v0 = t0[l0], v1 = t0[l1];
+                double2 w0 = make_double2(0.0, 0.0), w1 = w0;
+                if (NT == 2) {
+                    w0 = t1[l0];
+                    w1 = t1[l1];
+                }
+                if (want_ip) {
+                    double2 k0 = make_double2(0.0, 0.0), k1 = k0;
+                    for (int i = w.s0; i < w.s0 + w.ns; ++i) {
+                        const int qa = (s_q[i] + 2 * parity64(l0 & s_zl[i])) & 3;
+                        const int qb = (s_q[i] + 2 * parity64(l1 & s_zl[i])) & 3;
+                        const double sc = s_sc[i];
+                        const double2 r1 = c_ipow(v1, qb), r0 = c_ipow(v0, qa);
+                        k0.x += sc * r1.x;
+                        k0.y += sc * r1.y;
+                        k1.x += sc * r0.x;
+                        k1.y += sc * r0.y;
+                    }
+                    ip = c_add(ip, c_add(c_cjmul(w0, k0), c_cjmul(w1, k1)));
+                }
+                if (w.rotate) {
+                    for (int i = w.s0; i < w.s0 + w.ns; ++i) {
+                        const int q0 = (s_q[i] + 2 * parity64(l0 & s_zl[i])) & 3;
+                        const int q1 = (s_q[i] + 2 * parity64(l1 & s_zl[i])) & 3;
+                        const double2 cs = s_cs[i];
+                        {
+                            const double2 r1 = c_ipow(v1, q1), r0 = c_ipow(v0, q0);
+                            const double2 n0 = make_double2(cs.x * v0.x + cs.y * r1.x,
+                                                            cs.x * v0.y + cs.y * r1.y);
+                            v1 = make_double2(cs.x * v1.x + cs.y * r0.x, cs.x * v1.y + cs.y * r0.y);
+                            v0 = n0;
+                        }
+                        if (NT == 2) {
+                            const double2 r1 = c_ipow(w1, q1), r0 = c_ipow(w0, q0);
+                            const double2 n0 = make_double2(cs.x * w0.x + cs.y * r1.x,
+                                                            cs.x * w0.y + cs.y * r1.y);
+                            w1 = make_double2(cs.x * w1.x + cs.y * r0.x, cs.x * w1.y + cs.y * r0.y);
+                            w0 = n0;
+                        }
+                    }
+                    t0[l0] = v0;
+                    t0[l1] = v1;
+                    if (NT == 2) {
+                        t1[l0] = w0;
+                        t1[l1] = w1;
+                    }
+                }
+            }
+        } else {
+            for (int l = tid; l < T; l += nth) {
+                double2 v = t0[l];
+                double2 wv = (NT == 2) ? t1[l] : make_double2(0.0, 0.0);
+                if (want_ip) {
+                    double2 k = make_double2(0.0, 0.0);
+                    for (int i = w.s0; i < w.s0 + w.ns; ++i) {
+                        const int q = (s_q[i] + 2 * parity64((uint64_t)l & s_zl[i])) & 3;
+                        const double2 r = c_ipow(v, q);
+                        k.x += s_sc[i] * r.x;
+                        k.y += s_sc[i] * r.y;
+                    }
+                    ip = c_add(ip, c_cjmul(wv, k));
+                }
+                if (w.rotate) {
+                    for (int i = w.s0; i < w.s0 + w.ns; ++i) {
+                        const int q = (s_q[i] + 2 * parity64((uint64_t)l & s_zl[i])) & 3;
+                        const double2 cs = s_cs[i];
+                        const double2 r = c_ipow(v, q);
+                        v = make_double2(cs.x * v.x + cs.y * r.x, cs.x * v.y + cs.y * r.y);
+                        if (NT == 2) {
+                            const double2 rw = c_ipow(wv, q);
+                            wv = make_double2(cs.x * wv.x + cs.y * rw.x, cs.x * wv.y + cs.y * rw.y);
+                        }
+                    }
+                    t0[l] = v;
+                    if (NT == 2) t1[l] = wv;
+                }
+            }
+        }
+        if (want_ip) {
+            ip = block_sum(ip);
+            if (tid == 0)
+                a.partial[((uint64_t)w.ip_row * gridDim.y + slot) * a.ntiles + tile] = ip;
+        }
+        __syncthreads();
+    }
+
+    for (int l = tid; l < T; l += nth) {
+        const uint64_t g = base | s_tab[l >> a.L] | ((uint64_t)l & lowm);
+        P[g] = t0[l];
+        if (NT == 2) S[g] = t1[l];
+    }
+}
+
+}  // namespace qfbw

@@ -51,8 +51,9 @@ class Evaluator:
         self.nbatch = int(nbatch)
         self.nparam = ducc.nparam
         h = ctypes.c_void_p()
-        check(lib().qfb_ucc_create(ducc.fwd.h, ducc.grad_prog.h, ducc.H.h, ducc.nqubit,
-                                   ducc.ref_index, self.nbatch, ctypes.byref(h)), "qfb_ucc_create")
+        check(lib().qfb_ucc_create(ducc.fwd.h, ducc.grad_prog.h, ducc.unrot_prog.h, ducc.H.h,
+                                   ducc.nqubit, ducc.ref_index, self.nbatch, ctypes.byref(h)),
+              "qfb_ucc_create")
         self.h = h
         dp, de, dg = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
         check(lib().qfb_ucc_buffers(h, ctypes.byref(dp), ctypes.byref(de), ctypes.byref(dg)))
@@ -195,6 +196,10 @@ class DUCC:
         self.fwd = prog_from_strings(fx, fz, fs, fp, self.nparam)
         gx, gz, gs, gp = gradient_strings(pool, self.tops, qubit_excitations)
         self.grad_prog = prog_from_strings(gx, gz, gs, gp, self.nparam)
+        # U_mu is un-applied from K_mu itself for particle-hole pools
+        # (uccvqeabc.py:228-230) and from the component excitations of the
+        # ansatz for spin-adapted ones (uccvqeabc.py:208-224)
+        self.unrot_prog = self.fwd if pool_type == "sa_SD" else self.grad_prog
         self._pool = pool
         self._qe = qubit_excitations
         self._pool_sum = None
@@ -264,8 +269,8 @@ class DUCC:
             check(lib().qfb_vdot(psi, sig, ptr(ev)), "energy")
             g = np.zeros((B, self.nparam))
             if self.nparam:
-                check(lib().qfb_ucc_gradient(self.grad_prog.h, psi, sig, ptr(P), B, ptr(g)),
-                      "gradient")
+                check(lib().qfb_ucc_gradient(self.grad_prog.h, self.unrot_prog.h, psi, sig,
+                                             ptr(P), B, ptr(g)), "gradient")
         finally:
             lib().qfb_state_destroy(psi)
             if sig is not None:

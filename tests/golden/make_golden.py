@@ -131,10 +131,19 @@ def ucc_fixture(qf, norb, seed, out):
     algg._tops = tops
     algg._tamps = list(gamps)
     pool_grads = np.array(algg.measure_gradient3())
+    # spin-adapted pool: multi-excitation operators (abc/ansatz.py:38-55)
+    alsa = make_alg(qf, H, ref, "sa_SD")
+    S = len(alsa._pool_obj)
+    sa_amps = rng.uniform(-0.1, 0.1, S)
+    alsa._tops = list(range(S))
+    alsa._tamps = list(sa_amps)
+    sa_E = alsa.energy_feval(list(sa_amps))
+    sa_grad = np.array(alsa.measure_gradient(list(sa_amps)))
     np.savez_compressed(out, norb=norb, seed=seed, nqubit=nq, ref=np.array(ref),
                         h=h, g=g, ham_c=hc, ham_x=hx, ham_z=hz, amps=amps, energy=E, psi=psi,
                         grad=grad, gsd_tops=np.array(tops), gsd_amps=gamps,
-                        pool_grads=pool_grads)
+                        pool_grads=pool_grads, sa_amps=sa_amps, sa_energy=sa_E,
+                        sa_grad=sa_grad)
     print(f"{out}: {nq} q, {len(hc)} H terms, {M} SD params, {P} GSD ops, E = {E:.12f}")
 
 

@@ -30,16 +30,23 @@ def oracle_terms_from_arrays(c, x, z):
     return [(complex(cc), letters(int(xx), int(zz))) for cc, xx, zz in zip(c, x, z)]
 
 
-def kops_forward(pool, tops):
-    """Per-operator ordered JW term lists of the ansatz (oracle input)."""
+def kops_forward(pool, tops, pool_type=None):
+    """Per-operator ordered JW term lists of the ansatz (oracle input); an
+    sa_SD operator contributes its component excitations in turn
+    (abc/ansatz.py:38-55)."""
+    from qforte_b200.ucc import _sa_components
     out = []
     for top in tops:
-        s = qb.SQOperator()
-        s.add_op(pool[top][1])
-        q = s.jw_transform()
-        q.simplify()
-        q.order_terms()
-        out.append(oracle_terms(q))
+        comps = _sa_components(pool[top][1]) if pool_type == "sa_SD" else [pool[top][1]]
+        terms = []
+        for comp in comps:
+            s = qb.SQOperator()
+            s.add_op(comp)
+            q = s.jw_transform()
+            q.simplify()
+            q.order_terms()
+            terms += oracle_terms(q)
+        out.append(terms)
     return out
 
 

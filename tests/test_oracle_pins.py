@@ -43,6 +43,21 @@ def test_oracle_pool_gradients_norb4():
     assert np.max(np.abs(g - z["pool_grads"])) < 1e-11
 
 
+@pytest.mark.parametrize("name", ["ucc_norb4_seed11.npz", "ucc_norb6_seed11.npz"])
+def test_oracle_spin_adapted_pool(name):
+    z = golden(name)
+    mol, pool, hterms = _ucc_inputs(z, "sa_SD")
+    nq = int(z["nqubit"])
+    tops = list(range(len(pool)))
+    amps = z["sa_amps"]
+    kf = kops_forward(pool, tops, "sa_SD")
+    E, _ = O.energy(nq, list(z["ref"]), kf, amps, hterms)
+    assert abs(E - float(z["sa_energy"])) < 1e-12
+    g = O.measure_gradient(nq, list(z["ref"]), kf, amps, hterms,
+                           kops_grad=kops_gradient(pool, tops), kops_unrot=kf)
+    assert np.max(np.abs(g - z["sa_grad"])) < 1e-11
+
+
 def test_oracle_gates_bitexact():
     z = golden("gates_n6.npz")
     st = O.State(int(z["n"]))
