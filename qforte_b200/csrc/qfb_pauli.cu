@@ -33,6 +33,7 @@
 // over (psi, sigma); no intermediate state is stored.
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <unordered_map>
 #include <vector>
@@ -70,6 +71,16 @@ struct StepDev {  // run of consecutive strings sharing one x (and one parameter
     int32_t s0;  // first string
     int32_t ns;  // number of strings
     int32_t param;
+    // Givens form (tab >= 0): the strings commute and their sum K restricted
+    // to each pair (j, j ^ x) is sigma(j) * [[0, gamma hn], [gamma gn, 0]]
+    // with sigma(j) = (-1)^popcount(j & zbase) and (gn, hn) read from the
+    // table at the pattern of j's bits at the nd positions in dpos (6 bits
+    // each); exp(t K) is then a rotation by t * gamma on every active pair.
+    int32_t tab;   // offset of the (gn, hn) table, in double2 entries; -1: none
+    int32_t nd;
+    uint64_t dpos;
+    uint64_t zbase;
+    double gamma;
 };
 
 constexpr int kMaxStepStrings = 64;   // strings per fused step (longer runs are split)
@@ -270,25 +281,39 @@ __global__ void __launch_bounds__(256) k_sum_apply4(
 struct StepParams {
     const StrDev *strs;
     const double *params;  // [nrows][nparam]
+    const double2 *tab;    // Givens tables of the program
     int32_t nparam;
-    int32_t bcast;  // single parameter row for every slot
-    int32_t sign;   // +1: U, -1: U^dagger (reverse order, negated angles)
+    int32_t bcast;    // single parameter row for every slot
+    int32_t sign;     // +1: U, -1: negated angles
+    int32_t reverse;  // strings of a step in reverse order (exact U^dagger)
 };
+
+__device__ __forceinline__ double step_param(const StepParams &sp, int b, int param) {
+    return sp.params[(sp.bcast ? 0 : (size_t)b) * sp.nparam + param];
+}
+
+// Pattern of j's bits at the step's table positions.
+__device__ __forceinline__ int step_pattern(uint64_t j, int nd, uint64_t dpos) {
+    int pat = 0;
+    for (int i = 0; i < nd; ++i) pat |= (int)((j >> ((dpos >> (6 * i)) & 63)) & 1ull) << i;
+    return pat;
+}
 
 // Stage this step's strings (in application order) with cos/sin of their
 // angles for slot b into shared memory.
 __device__ __forceinline__ void stage_step(const StepDev &st, const StepParams &sp, int b,
-                                           uint64_t *s_z, int *s_q, double2 *s_cs) {
+                                           uint64_t *s_z, int *s_q, double2 *s_cs,
+                                           double *s_scale) {
     for (int i = threadIdx.x; i < st.ns; i += blockDim.x) {
-        const int k = st.s0 + (sp.sign > 0 ? i : st.ns - 1 - i);
+        const int k = st.s0 + (sp.reverse ? st.ns - 1 - i : i);
         const StrDev sd = sp.strs[k];
-        const double phi =
-            (double)sp.sign * sd.scale * sp.params[(sp.bcast ? 0 : b) * sp.nparam + sd.param];
+        const double phi = (double)sp.sign * sd.scale * step_param(sp, b, sd.param);
         double s, c;
         sincos(phi, &s, &c);
         s_z[i] = sd.z;
         s_q[i] = sd.ny;
         s_cs[i] = make_double2(c, s);
+        if (s_scale) s_scale[i] = sd.scale;
     }
     __syncthreads();
 }
@@ -311,15 +336,44 @@ __device__ __forceinline__ void rotate_pair(double2 &v0, double2 &v1, uint64_t j
     v1 = n1;
 }
 
+// Givens rotation of one active pair: new0 = c v0 + s hn v1, new1 = c v1 + s gn v0
+// (s already carries sigma(j)).
+__device__ __forceinline__ void givens_pair(double2 &v0, double2 &v1, double c, double s,
+                                            double2 gn, double2 hn) {
+    const double2 a = c_mul(hn, v1), b = c_mul(gn, v0);
+    const double2 n0 = make_double2(c * v0.x + s * a.x, c * v0.y + s * a.y);
+    v1 = make_double2(c * v1.x + s * b.x, c * v1.y + s * b.y);
+    v0 = n0;
+}
+
 __global__ void __launch_bounds__(256) k_prog_step(double2 *__restrict__ psi, uint64_t nbasis,
                                                    StepDev st, StepParams sp) {
     __shared__ uint64_t s_z[kMaxStepStrings];
     __shared__ int s_q[kMaxStepStrings];
     __shared__ double2 s_cs[kMaxStepStrings];
     const int b = blockIdx.y;
-    stage_step(st, sp, b, s_z, s_q, s_cs);
     double2 *s = psi + (uint64_t)b * nbasis;
     const uint64_t npair = nbasis >> 1;
+    if (st.tab >= 0) {
+        double sn, cs;
+        sincos((double)sp.sign * st.gamma * step_param(sp, b, st.param), &sn, &cs);
+        const double2 *tab = sp.tab + st.tab;
+        for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
+             p += (uint64_t)gridDim.x * blockDim.x) {
+            const uint64_t j0 = insert0(p, st.h);
+            const int pat = step_pattern(j0, st.nd, st.dpos);
+            const double2 gn = __ldg(&tab[2 * pat]), hn = __ldg(&tab[2 * pat + 1]);
+            if (gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
+            const uint64_t j1 = j0 ^ st.x;
+            const double ss = parity64(j0 & st.zbase) ? -sn : sn;
+            double2 v0 = s[j0], v1 = s[j1];
+            givens_pair(v0, v1, cs, ss, gn, hn);
+            s[j0] = v0;
+            s[j1] = v1;
+        }
+        return;
+    }
+    stage_step(st, sp, b, s_z, s_q, s_cs, nullptr);
     for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
          p += (uint64_t)gridDim.x * blockDim.x) {
         if (st.h >= 0) {
@@ -342,8 +396,9 @@ __global__ void __launch_bounds__(256) k_prog_step(double2 *__restrict__ psi, ui
 }
 
 // One gradient step: accumulate <sigma|K|psi> for K = sum_i (i scale_i) P_i over
-// this step's strings, then (when `rotate`) apply the step's U^dagger to both
-// states.  partial[((row * nbatch) + b) * gridDim.x + blockIdx.x].
+// this step's strings, then (when `rotate`) apply the step's rotation with the
+// angles of `sp` (negated: U^dagger) to both states.
+// partial[((row * nbatch) + b) * gridDim.x + blockIdx.x].
 __global__ void __launch_bounds__(256) k_grad_step(double2 *__restrict__ psi,
                                                    double2 *__restrict__ sig, uint64_t nbasis,
                                                    StepDev st, StepParams sp, int rotate, int row,
@@ -353,55 +408,81 @@ __global__ void __launch_bounds__(256) k_grad_step(double2 *__restrict__ psi,
     __shared__ double2 s_cs[kMaxStepStrings];
     __shared__ double s_scale[kMaxStepStrings];
     const int b = blockIdx.y;
-    // strings in reverse order with negated angles: the un-rotation U^dagger
-    stage_step(st, sp, b, s_z, s_q, s_cs);
-    for (int i = threadIdx.x; i < st.ns; i += blockDim.x)
-        s_scale[i] = sp.strs[st.s0 + st.ns - 1 - i].scale;
-    __syncthreads();
     double2 *ps = psi + (uint64_t)b * nbasis;
     double2 *sg = sig + (uint64_t)b * nbasis;
     const uint64_t npair = nbasis >> 1;
-    const bool diag = st.h < 0;
     double2 acc = make_double2(0.0, 0.0);
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
-         p += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t j0 = diag ? (p << 1) : insert0(p, st.h);
-        const uint64_t j1 = diag ? (j0 | 1ull) : (j0 ^ st.x);
-        double2 v0 = ps[j0], v1 = ps[j1], w0 = sg[j0], w1 = sg[j1];
-        // (K psi)_j = sum_i scale_i * (i ph_i(j ^ x)) psi_{j ^ x}
-        double2 k0 = make_double2(0.0, 0.0), k1 = make_double2(0.0, 0.0);
-        for (int i = 0; i < st.ns; ++i) {
-            const int qa = (s_q[i] + 1 + 2 * parity64(j0 & s_z[i])) & 3;
-            const int qb = (s_q[i] + 1 + 2 * parity64(j1 & s_z[i])) & 3;
-            const double sc = s_scale[i];
-            if (diag) {
-                const double2 r0 = c_ipow(v0, qa), r1 = c_ipow(v1, qb);
-                k0.x += sc * r0.x; k0.y += sc * r0.y;
-                k1.x += sc * r1.x; k1.y += sc * r1.y;
-            } else {
-                const double2 r1 = c_ipow(v1, qb), r0 = c_ipow(v0, qa);
-                k0.x += sc * r1.x; k0.y += sc * r1.y;
-                k1.x += sc * r0.x; k1.y += sc * r0.y;
+    if (st.tab >= 0) {
+        double sn, cs;
+        sincos((double)sp.sign * st.gamma * step_param(sp, b, st.param), &sn, &cs);
+        const double2 *tab = sp.tab + st.tab;
+        for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
+             p += (uint64_t)gridDim.x * blockDim.x) {
+            const uint64_t j0 = insert0(p, st.h);
+            const int pat = step_pattern(j0, st.nd, st.dpos);
+            const double2 gn = __ldg(&tab[2 * pat]), hn = __ldg(&tab[2 * pat + 1]);
+            if (gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
+            const uint64_t j1 = j0 ^ st.x;
+            const bool neg = parity64(j0 & st.zbase);
+            double2 v0 = ps[j0], v1 = ps[j1], w0 = sg[j0], w1 = sg[j1];
+            // <sigma|K|psi> on the pair: sigma(j) gamma (conj(w0) hn v1 + conj(w1) gn v0)
+            const double2 t = c_add(c_cjmul(w0, c_mul(hn, v1)), c_cjmul(w1, c_mul(gn, v0)));
+            const double gs = neg ? -st.gamma : st.gamma;
+            acc.x += gs * t.x;
+            acc.y += gs * t.y;
+            if (rotate) {
+                const double ss = neg ? -sn : sn;
+                givens_pair(v0, v1, cs, ss, gn, hn);
+                givens_pair(w0, w1, cs, ss, gn, hn);
+                ps[j0] = v0;
+                ps[j1] = v1;
+                sg[j0] = w0;
+                sg[j1] = w1;
             }
         }
-        acc = c_add(acc, c_add(c_cjmul(w0, k0), c_cjmul(w1, k1)));
-        if (rotate) {
-            double2 dummy;
+    } else {
+        stage_step(st, sp, b, s_z, s_q, s_cs, s_scale);
+        const bool diag = st.h < 0;
+        for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
+             p += (uint64_t)gridDim.x * blockDim.x) {
+            const uint64_t j0 = diag ? (p << 1) : insert0(p, st.h);
+            const uint64_t j1 = diag ? (j0 | 1ull) : (j0 ^ st.x);
+            double2 v0 = ps[j0], v1 = ps[j1], w0 = sg[j0], w1 = sg[j1];
+            // (K psi)_j = sum_i scale_i * (i ph_i(j ^ x)) psi_{j ^ x}
+            double2 k0 = make_double2(0.0, 0.0), k1 = make_double2(0.0, 0.0);
             for (int i = 0; i < st.ns; ++i) {
+                const int qa = (s_q[i] + 1 + 2 * parity64(j0 & s_z[i])) & 3;
+                const int qb = (s_q[i] + 1 + 2 * parity64(j1 & s_z[i])) & 3;
+                const double sc = s_scale[i];
                 if (diag) {
-                    rotate_pair(v0, dummy, j0, j0, s_z[i], s_q[i], s_cs[i], true);
-                    rotate_pair(v1, dummy, j1, j1, s_z[i], s_q[i], s_cs[i], true);
-                    rotate_pair(w0, dummy, j0, j0, s_z[i], s_q[i], s_cs[i], true);
-                    rotate_pair(w1, dummy, j1, j1, s_z[i], s_q[i], s_cs[i], true);
+                    const double2 r0 = c_ipow(v0, qa), r1 = c_ipow(v1, qb);
+                    k0.x += sc * r0.x; k0.y += sc * r0.y;
+                    k1.x += sc * r1.x; k1.y += sc * r1.y;
                 } else {
-                    rotate_pair(v0, v1, j0, j1, s_z[i], s_q[i], s_cs[i], false);
-                    rotate_pair(w0, w1, j0, j1, s_z[i], s_q[i], s_cs[i], false);
+                    const double2 r1 = c_ipow(v1, qb), r0 = c_ipow(v0, qa);
+                    k0.x += sc * r1.x; k0.y += sc * r1.y;
+                    k1.x += sc * r0.x; k1.y += sc * r0.y;
                 }
             }
-            ps[j0] = v0;
-            ps[j1] = v1;
-            sg[j0] = w0;
-            sg[j1] = w1;
+            acc = c_add(acc, c_add(c_cjmul(w0, k0), c_cjmul(w1, k1)));
+            if (rotate) {
+                double2 dummy;
+                for (int i = 0; i < st.ns; ++i) {
+                    if (diag) {
+                        rotate_pair(v0, dummy, j0, j0, s_z[i], s_q[i], s_cs[i], true);
+                        rotate_pair(v1, dummy, j1, j1, s_z[i], s_q[i], s_cs[i], true);
+                        rotate_pair(w0, dummy, j0, j0, s_z[i], s_q[i], s_cs[i], true);
+                        rotate_pair(w1, dummy, j1, j1, s_z[i], s_q[i], s_cs[i], true);
+                    } else {
+                        rotate_pair(v0, v1, j0, j1, s_z[i], s_q[i], s_cs[i], false);
+                        rotate_pair(w0, w1, j0, j1, s_z[i], s_q[i], s_cs[i], false);
+                    }
+                }
+                ps[j0] = v0;
+                ps[j1] = v1;
+                sg[j0] = w0;
+                sg[j1] = w1;
+            }
         }
     }
     acc = block_sum(acc);
@@ -475,9 +556,11 @@ struct WinPlan {
     std::vector<qfbw::Window> wins;
     std::vector<qfbw::WStep> steps;
     std::vector<qfbw::WStr> strs;
+    std::vector<double2> tabs;
     void *blob = nullptr;
     qfbw::WStep *d_steps = nullptr;
     qfbw::WStr *d_strs = nullptr;
+    double2 *d_tabs = nullptr;
     size_t smem_max = 0;
     int ntiles() const { return 1 << (nqubit - b); }
 };
@@ -487,6 +570,8 @@ struct qfb_prog_s {
     int32_t nparam = 0;
     void *blob = nullptr;
     StrDev *d_strs = nullptr;
+    double2 *d_tab = nullptr;       // Givens tables (StepDev::tab)
+    std::vector<double2> h_tab;
     std::vector<StrDev> h_strs;
     std::vector<StepDev> h_steps;
     std::vector<int32_t> p_step0, p_step1;  // steps of each parameter (gradient)
@@ -541,8 +626,8 @@ static void push_strings(WinPlan *pl, const qfb_prog_s *p, const StepDev &st, ui
     }
 }
 
-static void push_step(WinPlan *pl, const qfbw::Window &win, const StepDev &st, int rotate,
-                      int ip_row) {
+static void push_step(WinPlan *pl, const qfbw::Window &win, const qfb_prog_s *p,
+                      const StepDev &st, int rotate, int ip_row, int sign) {
     qfbw::WStep w{};
     w.xl = qfbw::pext_h(st.x, win.qmask);
     w.hl = w.xl ? 63 - __builtin_clzll(w.xl) : -1;
@@ -550,6 +635,28 @@ static void push_step(WinPlan *pl, const qfbw::Window &win, const StepDev &st, i
     w.ns = st.ns;
     w.rotate = rotate;
     w.ip_row = ip_row;
+    w.tab = -1;
+    w.param = st.param;
+    w.sign = sign;
+    bool inside = st.tab >= 0;
+    for (int i = 0; inside && i < st.nd; ++i)
+        inside = (win.qmask >> ((st.dpos >> (6 * i)) & 63)) & 1ull;
+    if (inside) {
+        // pattern positions in tile coordinates
+        w.nd = st.nd;
+        w.dpos = 0;
+        for (int i = 0; i < st.nd; ++i) {
+            const int q = (int)((st.dpos >> (6 * i)) & 63);
+            const int lp = __builtin_popcountll(win.qmask & ((1ull << q) - 1ull));
+            w.dpos |= (uint64_t)lp << (6 * i);
+        }
+        w.zb_l = qfbw::pext_h(st.zbase, win.qmask);
+        w.zb_c = st.zbase & ~win.qmask;
+        w.gamma = st.gamma;
+        w.tab = (int32_t)pl->tabs.size();
+        const int n = 2 << st.nd;
+        pl->tabs.insert(pl->tabs.end(), p->h_tab.begin() + st.tab, p->h_tab.begin() + st.tab + n);
+    }
     pl->steps.push_back(w);
 }
 
@@ -557,10 +664,16 @@ static int upload_plan(WinPlan *pl) {
     const size_t sb = sizeof(qfbw::WStep) * std::max<size_t>(1, pl->steps.size());
     const size_t sbal = (sb + 255) & ~(size_t)255;
     const size_t rb = sizeof(qfbw::WStr) * std::max<size_t>(1, pl->strs.size());
-    int rc = dev_alloc(&pl->blob, sbal + rb);
+    const size_t rbal = (rb + 255) & ~(size_t)255;
+    const size_t tb = sizeof(double2) * std::max<size_t>(1, pl->tabs.size());
+    int rc = dev_alloc(&pl->blob, sbal + rbal + tb);
     if (rc) return rc;
     pl->d_steps = (qfbw::WStep *)pl->blob;
     pl->d_strs = (qfbw::WStr *)((char *)pl->blob + sbal);
+    pl->d_tabs = (double2 *)((char *)pl->blob + sbal + rbal);
+    if (!pl->tabs.empty())
+        QFB_CUDA(cudaMemcpyAsync(pl->d_tabs, pl->tabs.data(), sizeof(double2) * pl->tabs.size(),
+                                 cudaMemcpyHostToDevice, t_stream));
     if (!pl->steps.empty())
         QFB_CUDA(cudaMemcpyAsync(pl->d_steps, pl->steps.data(), sb, cudaMemcpyHostToDevice,
                                  t_stream));
@@ -569,8 +682,9 @@ static int upload_plan(WinPlan *pl) {
                                  t_stream));
     QFB_CUDA(cudaStreamSynchronize(t_stream));
     for (const auto &w : pl->wins)
-        pl->smem_max = std::max(pl->smem_max,
-                                qfbw::win_smem_bytes(w.b, pl->L, w.sr1 - w.sr0, pl->nt));
+        if (w.global_step < 0 && w.global_mu < 0)
+            pl->smem_max = std::max(pl->smem_max, qfbw::win_smem_bytes(w.b, pl->L, w.sr1 - w.sr0,
+                                                                       w.st1 - w.st0, pl->nt));
     return QFB_OK;
 }
 
@@ -610,7 +724,7 @@ static int build_fwd_plan(qfb_prog_s *p, int n, WinPlan **out) {
         w.st0 = (int32_t)pl->steps.size();
         w.sr0 = (int32_t)pl->strs.size();
         for (size_t k = i; k < j; ++k) {
-            push_step(pl, w, p->h_steps[k], 1, -1);
+            push_step(pl, w, p, p->h_steps[k], 1, -1, +1);
             push_strings(pl, p, p->h_steps[k], w.qmask, +1, false);
         }
         w.st1 = (int32_t)pl->steps.size();
@@ -703,18 +817,21 @@ static int build_grad_plan(qfb_prog_s *kp, const qfb_prog_s *up, int n, WinPlan 
             steps_of(kp, m, k0, k1);
             steps_of(up, m, u0, u1);
             if (kp == up && k1 - k0 == 1) {
-                push_step(pl, w, kp->h_steps[k0], rot, k0);
+                // U^dagger exactly: strings reversed, angles negated
+                push_step(pl, w, kp, kp->h_steps[k0], rot, k0, -1);
                 push_strings(pl, kp, kp->h_steps[k0], w.qmask, -1, true);
                 continue;
             }
             for (int32_t s = k0; s < k1; ++s) {
-                push_step(pl, w, kp->h_steps[s], 0, s);
+                push_step(pl, w, kp, kp->h_steps[s], 0, s, -1);
                 push_strings(pl, kp, kp->h_steps[s], w.qmask, -1, true);
             }
+            // up's strings in forward order with negated angles, as the
+            // reference's Trotter product of -t K_mu (uccvqeabc.py:208-238)
             if (rot)
-                for (int32_t s = u1 - 1; s >= u0; --s) {
-                    push_step(pl, w, up->h_steps[s], 1, -1);
-                    push_strings(pl, up, up->h_steps[s], w.qmask, -1, true);
+                for (int32_t s = u0; s < u1; ++s) {
+                    push_step(pl, w, up, up->h_steps[s], 1, -1, -1);
+                    push_strings(pl, up, up->h_steps[s], w.qmask, -1, false);
                 }
         }
         w.st1 = (int32_t)pl->steps.size();
@@ -774,12 +891,13 @@ static int launch_window(const WinPlan *pl, const qfbw::Window &w, double2 *psi,
     a.nstr = w.sr1 - w.sr0;
     a.steps = pl->d_steps + w.st0;
     a.strs = pl->d_strs + w.sr0;
+    a.tab = pl->d_tabs;
     a.params = d_par;
     a.nparam = nparam;
     a.bcast = bcast;
     a.partial = partial;
     a.ntiles = pl->ntiles();
-    const size_t smem = qfbw::win_smem_bytes(w.b, pl->L, a.nstr, pl->nt);
+    const size_t smem = qfbw::win_smem_bytes(w.b, pl->L, a.nstr, a.nsteps, pl->nt);
     const dim3 grid((unsigned)a.ntiles, (unsigned)B);
     if (pl->nt == 1)
         qfbw::k_window<1><<<grid, qfbw::kWinThreads, smem, t_stream>>>(psi, nullptr, nbasis, a);
@@ -813,6 +931,81 @@ unsigned chunks_for(uint64_t npair, int nbatch, int nrows_of_work) {
 }
 
 }  // namespace
+
+// Givens form of a step (StepDev): the strings must commute, their z-masks
+// may differ from the first one's only at <= 6 positions (other than h), and
+// -(k01 k10) on every active pattern must be one real gamma^2.
+static void make_table(qfb_prog_s *p, StepDev &st) {
+    st.tab = -1;
+    st.nd = 0;
+    st.dpos = 0;
+    st.zbase = 0;
+    st.gamma = 0.0;
+    if (st.x == 0 || st.ns < 1) return;
+    const StrDev *S = &p->h_strs[st.s0];
+    for (int a = 0; a < st.ns; ++a)
+        for (int b = a + 1; b < st.ns; ++b)
+            if (__builtin_popcountll(st.x & (S[a].z ^ S[b].z)) & 1) return;  // not commuting
+    const uint64_t zb = S[0].z;
+    uint64_t D = 0;
+    for (int a = 0; a < st.ns; ++a) D |= S[a].z ^ zb;
+    D &= ~(1ull << st.h);
+    const int nd = __builtin_popcountll(D);
+    if (nd > 6) return;
+    int dp[6];
+    {
+        uint64_t m = D;
+        for (int i = 0; i < nd; ++i) {
+            dp[i] = __builtin_ctzll(m);
+            m &= m - 1;
+        }
+    }
+    const int npat = 1 << nd;
+    std::vector<std::complex<double>> g(npat), hh(npat);
+    double scale_norm = 0.0;
+    for (int a = 0; a < st.ns; ++a) scale_norm += std::fabs(S[a].scale);
+    static const std::complex<double> ipow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+    for (int pat = 0; pat < npat; ++pat) {
+        uint64_t jd = 0;
+        for (int i = 0; i < nd; ++i)
+            if (pat >> i & 1) jd |= 1ull << dp[i];
+        std::complex<double> gg = 0.0, hv = 0.0;
+        for (int a = 0; a < st.ns; ++a) {
+            const int par = __builtin_popcountll(jd & (S[a].z ^ zb)) & 1;
+            const std::complex<double> term = S[a].scale * ipow[(S[a].ny + 1) & 3] * (par ? -1.0 : 1.0);
+            gg += term;
+            hv += (S[a].ny & 1) ? -term : term;
+        }
+        g[pat] = gg;
+        hh[pat] = hv;
+    }
+    const double tol = 1e-12 * std::max(scale_norm, 1e-300);
+    double gamma2 = -1.0;
+    for (int pat = 0; pat < npat; ++pat) {
+        const bool active = std::abs(g[pat]) > tol || std::abs(hh[pat]) > tol;
+        if (!active) {
+            g[pat] = hh[pat] = 0.0;
+            continue;
+        }
+        const std::complex<double> pr = -(g[pat] * hh[pat]);
+        if (std::fabs(pr.imag()) > tol * scale_norm || pr.real() <= 0.0) return;
+        if (gamma2 < 0.0)
+            gamma2 = pr.real();
+        else if (std::fabs(pr.real() - gamma2) > 1e-12 * gamma2)
+            return;
+    }
+    const double gamma = gamma2 > 0.0 ? std::sqrt(gamma2) : 1.0;
+    st.tab = (int32_t)p->h_tab.size();
+    st.nd = nd;
+    for (int i = 0; i < nd; ++i) st.dpos |= (uint64_t)dp[i] << (6 * i);
+    st.zbase = zb;
+    st.gamma = gamma2 > 0.0 ? gamma : 0.0;
+    for (int pat = 0; pat < npat; ++pat) {
+        const std::complex<double> gn = g[pat] / gamma, hn = hh[pat] / gamma;
+        p->h_tab.push_back(make_double2(gn.real(), gn.imag()));
+        p->h_tab.push_back(make_double2(hn.real(), hn.imag()));
+    }
+}
 
 extern "C" {
 
@@ -1034,6 +1227,11 @@ int qfb_prog_create(const qfb_pauli *paulis, const double *scale, const int32_t 
             st.s0 = (int32_t)k;
             st.ns = 1;
             st.param = param[k];
+            st.tab = -1;
+            st.nd = 0;
+            st.dpos = 0;
+            st.zbase = 0;
+            st.gamma = 0.0;
             p->h_steps.push_back(st);
         }
     }
@@ -1047,15 +1245,22 @@ int qfb_prog_create(const qfb_pauli *paulis, const double *scale, const int32_t 
         }
         p->p_step1[mu] = (int32_t)s + 1;
     }
-    int rc = dev_alloc(&p->blob, sizeof(StrDev) * std::max<size_t>(1, p->h_strs.size()));
+    for (auto &st : p->h_steps) make_table(p, st);
+    const size_t sb = (sizeof(StrDev) * std::max<size_t>(1, p->h_strs.size()) + 255) & ~(size_t)255;
+    const size_t tb = sizeof(double2) * std::max<size_t>(1, p->h_tab.size());
+    int rc = dev_alloc(&p->blob, sb + tb);
     if (rc) {
         delete p;
         return rc;
     }
     p->d_strs = (StrDev *)p->blob;
+    p->d_tab = (double2 *)((char *)p->blob + sb);
     cudaError_t e = cudaSuccess;
     if (!p->h_strs.empty())
         e = cudaMemcpyAsync(p->d_strs, p->h_strs.data(), sizeof(StrDev) * p->h_strs.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess && !p->h_tab.empty())
+        e = cudaMemcpyAsync(p->d_tab, p->h_tab.data(), sizeof(double2) * p->h_tab.size(),
                             cudaMemcpyHostToDevice, t_stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);
     if (e != cudaSuccess) {
@@ -1098,8 +1303,8 @@ static int check_prog_state(qfb_prog p, qfb_state s, int32_t nrows, const char *
 // ---- enqueue helpers: kernels only, no allocation, no host synchronisation --
 
 static int enqueue_step(const qfb_prog_s *p, const StepDev &st, double2 *psi, uint64_t nbasis,
-                        int B, const double *d_par, int bcast, int sign) {
-    StepParams sp{p->d_strs, d_par, p->nparam, bcast, sign};
+                        int B, const double *d_par, int bcast, int sign, int reverse) {
+    StepParams sp{p->d_strs, d_par, p->d_tab, p->nparam, bcast, sign, reverse};
     const dim3 grid(grid_for(nbasis >> 1, 256, 4), B);
     k_prog_step<<<grid, 256, 0, t_stream>>>(psi, nbasis, st, sp);
     QFB_LAUNCHED();
@@ -1117,7 +1322,8 @@ static int enqueue_prog(const qfb_prog_s *p, double2 *psi, int nqubit, int B,
         if (rc) return rc;
         for (const auto &w : pl->wins) {
             rc = (w.global_step >= 0)
-                     ? enqueue_step(p, p->h_steps[w.global_step], psi, nbasis, B, d_par, bcast, 1)
+                     ? enqueue_step(p, p->h_steps[w.global_step], psi, nbasis, B, d_par, bcast, 1,
+                                    0)
                      : launch_window(pl, w, psi, nullptr, nbasis, B, d_par, p->nparam, bcast,
                                      nullptr);
             if (rc) return rc;
@@ -1127,7 +1333,7 @@ static int enqueue_prog(const qfb_prog_s *p, double2 *psi, int nqubit, int B,
     const int64_t ns = (int64_t)p->h_steps.size();
     for (int64_t k = 0; k < ns; ++k) {
         int rc = enqueue_step(p, p->h_steps[sign > 0 ? k : ns - 1 - k], psi, nbasis, B, d_par,
-                              bcast, sign);
+                              bcast, sign, sign > 0 ? 0 : 1);
         if (rc) return rc;
     }
     return QFB_OK;
@@ -1153,8 +1359,11 @@ static int enqueue_sum_apply(const qfb_sum_s *h, double2 *dst, const double2 *sr
 static int enqueue_grad_mu(const qfb_prog_s *kp, const qfb_prog_s *up, int mu, double2 *psi,
                            double2 *sig, uint64_t nbasis, int B, const double *d_par, int bcast,
                            double2 *partial, unsigned chunks) {
-    StepParams kpar{kp->d_strs, d_par, kp->nparam, bcast, -1};
-    StepParams upar{up->d_strs, d_par, up->nparam, bcast, -1};
+    // fused step: U^dagger exactly (strings reversed, angles negated); separate
+    // un-rotation: up's strings in forward order with negated angles, as the
+    // reference's Trotter product of -t K does (uccvqeabc.py:208-238)
+    StepParams kpar{kp->d_strs, d_par, kp->d_tab, kp->nparam, bcast, -1, 1};
+    StepParams upar{up->d_strs, d_par, up->d_tab, up->nparam, bcast, -1, 0};
     const dim3 grid(chunks, B);
     const int32_t s0 = kp->p_step0[mu], s1 = kp->p_step1[mu];
     const bool last = (mu == 0);
@@ -1174,7 +1383,7 @@ static int enqueue_grad_mu(const qfb_prog_s *kp, const qfb_prog_s *up, int mu, d
     // ... then U_mu^dagger on both states, steps in reverse order
     const dim3 g2(grid_for(nbasis >> 1, 256, 4), B);
     const int32_t u0 = up->p_step0[mu], u1 = up->p_step1[mu];
-    for (int32_t s = u1 - 1; u0 >= 0 && s >= u0; --s) {
+    for (int32_t s = u0; u0 >= 0 && s < u1; ++s) {
         k_prog_step<<<g2, 256, 0, t_stream>>>(psi, nbasis, up->h_steps[s], upar);
         QFB_LAUNCHED();
         k_prog_step<<<g2, 256, 0, t_stream>>>(sig, nbasis, up->h_steps[s], upar);

@@ -31,7 +31,16 @@ struct WStep {       // one step of a window, masks in tile coordinates
     int32_t ns;      // strings
     int32_t rotate;  // apply the rotation
     int32_t ip_row;  // >= 0: add this step's <sigma|K|psi> share to that row
+    // Givens form (StepDev of qfb_pauli.cu) in tile coordinates; tab < 0: none
+    int32_t tab;     // offset into the plan's tables (double2 entries)
+    int32_t nd;
+    int32_t param;
+    int32_t sign;    // angle sign of the rotation
     int32_t pad;
+    uint64_t dpos;   // 6-bit tile positions of the pattern bits
+    uint64_t zb_l;   // zbase inside the tile ...
+    uint64_t zb_c;   // ... and outside it (a per-tile sign)
+    double gamma;
 };
 
 struct WStr {
@@ -84,19 +93,27 @@ struct WinLaunch {
     int nsteps, nstr;
     const WStep *steps;  // this window's steps
     const WStr *strs;    // this window's strings
+    const double2 *tab;  // the plan's Givens tables
     const double *params;
     int nparam, bcast;
     double2 *partial;  // [rows][nbatch][ntiles]
     int ntiles;
 };
 
-__host__ __device__ inline size_t win_smem_bytes(int b, int L, int nstr, int nt) {
+__host__ __device__ inline size_t win_smem_bytes(int b, int L, int nstr, int nsteps, int nt) {
     const size_t T = (size_t)1 << b;
     size_t o = nt * T * sizeof(double2);
+    o += (size_t)nsteps * (sizeof(double2) + sizeof(double));
     o += (size_t)nstr * (sizeof(double2) + sizeof(double) + sizeof(uint64_t) + sizeof(int));
     o = (o + 15) & ~(size_t)15;
     o += ((size_t)1 << (b - L)) * sizeof(uint64_t);
     return o;
+}
+
+__device__ __forceinline__ int tile_pattern(uint32_t l, int nd, uint64_t dpos) {
+    int pat = 0;
+    for (int i = 0; i < nd; ++i) pat |= (int)((l >> ((dpos >> (6 * i)) & 63)) & 1u) << i;
+    return pat;
 }
 
 template <int NT>
@@ -107,11 +124,14 @@ __global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ ps
     const int T = 1 << a.b;
     double2 *t0 = reinterpret_cast<double2 *>(smem);
     double2 *t1 = t0 + T;
-    double2 *s_cs = t0 + (size_t)NT * T;
+    double2 *s_stcs = t0 + (size_t)NT * T;  // per step: (cos, sin * tile sign)
+    double *s_stg = reinterpret_cast<double *>(s_stcs + a.nsteps);  // gamma * tile sign
+    double2 *s_cs = reinterpret_cast<double2 *>(s_stg + a.nsteps);
     double *s_sc = reinterpret_cast<double *>(s_cs + a.nstr);
     uint64_t *s_zl = reinterpret_cast<uint64_t *>(s_sc + a.nstr);
     int *s_q = reinterpret_cast<int *>(s_zl + a.nstr);
     size_t o = (size_t)NT * T * sizeof(double2) +
+               (size_t)a.nsteps * (sizeof(double2) + sizeof(double)) +
                (size_t)a.nstr * (sizeof(double2) + sizeof(double) + sizeof(uint64_t) + sizeof(int));
     o = (o + 15) & ~(size_t)15;
     uint64_t *s_tab = reinterpret_cast<uint64_t *>(smem + o);
@@ -129,6 +149,15 @@ __global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ ps
         s_zl[i] = w.zl;
         s_q[i] = (w.ny + 1 + 2 * parity64(base & w.zc)) & 3;
     }
+    for (int st = tid; st < a.nsteps; st += nth) {
+        const WStep w = a.steps[st];
+        if (w.tab < 0) continue;
+        const double ts = parity64(base & w.zb_c) ? -1.0 : 1.0;
+        double s, c;
+        sincos((double)w.sign * w.gamma * par[w.param], &s, &c);
+        s_stcs[st] = make_double2(c, s * ts);
+        s_stg[st] = w.gamma * ts;
+    }
     __syncthreads();
     const uint64_t lowm = (1ull << a.L) - 1ull;
     double2 *P = psi + (uint64_t)slot * nbasis;
@@ -144,7 +173,50 @@ __global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ ps
         const WStep w = a.steps[st];
         double2 ip = make_double2(0.0, 0.0);
         const bool want_ip = (NT == 2) && (w.ip_row >= 0);
-        if (w.hl >= 0) {
+        if (w.tab >= 0) {
+            const double c = s_stcs[st].x, sn = s_stcs[st].y, gam = s_stg[st];
+            const double2 *tb = a.tab + w.tab;
+            const uint32_t xl = (uint32_t)w.xl, zb = (uint32_t)w.zb_l;
+            for (int p = tid; p < (T >> 1); p += nth) {
+                const uint32_t l0 = (uint32_t)insert0((uint64_t)p, w.hl);
+                const int pat = tile_pattern(l0, w.nd, w.dpos);
+                const double2 gn = __ldg(&tb[2 * pat]), hn = __ldg(&tb[2 * pat + 1]);
+                if (gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
+                const uint32_t l1 = l0 ^ xl;
+                const bool neg = __popc(l0 & zb) & 1;
+                double2 v0 = t0[l0], v1 = t0[l1];
+                double2 w0 = make_double2(0.0, 0.0), w1 = w0;
+                if (NT == 2) {
+                    w0 = t1[l0];
+                    w1 = t1[l1];
+                }
+                if (want_ip) {
+                    const double2 t = c_add(c_cjmul(w0, c_mul(hn, v1)), c_cjmul(w1, c_mul(gn, v0)));
+                    const double g = neg ? -gam : gam;
+                    ip.x += g * t.x;
+                    ip.y += g * t.y;
+                }
+                if (w.rotate) {
+                    const double ss = neg ? -sn : sn;
+                    {
+                        const double2 ra = c_mul(hn, v1), rb = c_mul(gn, v0);
+                        const double2 n0 = make_double2(c * v0.x + ss * ra.x, c * v0.y + ss * ra.y);
+                        v1 = make_double2(c * v1.x + ss * rb.x, c * v1.y + ss * rb.y);
+                        v0 = n0;
+                    }
+                    t0[l0] = v0;
+                    t0[l1] = v1;
+                    if (NT == 2) {
+                        const double2 ra = c_mul(hn, w1), rb = c_mul(gn, w0);
+                        const double2 n0 = make_double2(c * w0.x + ss * ra.x, c * w0.y + ss * ra.y);
+                        w1 = make_double2(c * w1.x + ss * rb.x, c * w1.y + ss * rb.y);
+                        w0 = n0;
+                        t1[l0] = w0;
+                        t1[l1] = w1;
+                    }
+                }
+            }
+        } else if (w.hl >= 0) {
             for (int p = tid; p < (T >> 1); p += nth) {
                 const uint64_t l0 = insert0((uint64_t)p, w.hl), l1 = l0 ^ w.xl;
                 double2 v0 = t0[l0], v1 = t0[l1];
