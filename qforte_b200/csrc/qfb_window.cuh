@@ -100,14 +100,38 @@ struct WinLaunch {
     int ntiles;
 };
 
-__host__ __device__ inline size_t win_smem_bytes(int b, int L, int nstr, int nsteps, int nt) {
+// Shared-memory layout of a window, ordered by alignment: the 16-byte
+// arrays (tiles, per-step and per-string cos/sin) first, then the 8-byte
+// ones, then the ints; the spread table starts on a 16-byte boundary.
+struct WinSmem {
+    size_t cs_step, cs_str, g_step, sc_str, zl_str, q_str, tab, total;
+};
+
+__host__ __device__ inline WinSmem win_smem_layout(int b, int L, int nstr, int nsteps, int nt) {
+    WinSmem m;
     const size_t T = (size_t)1 << b;
-    size_t o = nt * T * sizeof(double2);
-    o += (size_t)nsteps * (sizeof(double2) + sizeof(double));
-    o += (size_t)nstr * (sizeof(double2) + sizeof(double) + sizeof(uint64_t) + sizeof(int));
+    size_t o = (size_t)nt * T * 16;
+    m.cs_step = o;
+    o += (size_t)nsteps * 16;
+    m.cs_str = o;
+    o += (size_t)nstr * 16;
+    m.g_step = o;
+    o += (size_t)nsteps * 8;
+    m.sc_str = o;
+    o += (size_t)nstr * 8;
+    m.zl_str = o;
+    o += (size_t)nstr * 8;
+    m.q_str = o;
+    o += (size_t)nstr * 4;
     o = (o + 15) & ~(size_t)15;
-    o += ((size_t)1 << (b - L)) * sizeof(uint64_t);
-    return o;
+    m.tab = o;
+    o += ((size_t)1 << (b - L)) * 8;
+    m.total = o;
+    return m;
+}
+
+__host__ __device__ inline size_t win_smem_bytes(int b, int L, int nstr, int nsteps, int nt) {
+    return win_smem_layout(b, L, nstr, nsteps, nt).total;
 }
 
 __device__ __forceinline__ int tile_pattern(uint32_t l, int nd, uint64_t dpos) {
@@ -122,19 +146,16 @@ __global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ ps
                                                         uint64_t nbasis, WinLaunch a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = 1 << a.b;
+    const WinSmem lay = win_smem_layout(a.b, a.L, a.nstr, a.nsteps, NT);
     double2 *t0 = reinterpret_cast<double2 *>(smem);
     double2 *t1 = t0 + T;
-    double2 *s_stcs = t0 + (size_t)NT * T;  // per step: (cos, sin * tile sign)
-    double *s_stg = reinterpret_cast<double *>(s_stcs + a.nsteps);  // gamma * tile sign
-    double2 *s_cs = reinterpret_cast<double2 *>(s_stg + a.nsteps);
-    double *s_sc = reinterpret_cast<double *>(s_cs + a.nstr);
-    uint64_t *s_zl = reinterpret_cast<uint64_t *>(s_sc + a.nstr);
-    int *s_q = reinterpret_cast<int *>(s_zl + a.nstr);
-    size_t o = (size_t)NT * T * sizeof(double2) +
-               (size_t)a.nsteps * (sizeof(double2) + sizeof(double)) +
-               (size_t)a.nstr * (sizeof(double2) + sizeof(double) + sizeof(uint64_t) + sizeof(int));
-    o = (o + 15) & ~(size_t)15;
-    uint64_t *s_tab = reinterpret_cast<uint64_t *>(smem + o);
+    double2 *s_stcs = reinterpret_cast<double2 *>(smem + lay.cs_step);  // (cos, sin * tile sign)
+    double2 *s_cs = reinterpret_cast<double2 *>(smem + lay.cs_str);
+    double *s_stg = reinterpret_cast<double *>(smem + lay.g_step);  // gamma * tile sign
+    double *s_sc = reinterpret_cast<double *>(smem + lay.sc_str);
+    uint64_t *s_zl = reinterpret_cast<uint64_t *>(smem + lay.zl_str);
+    int *s_q = reinterpret_cast<int *>(smem + lay.q_str);
+    uint64_t *s_tab = reinterpret_cast<uint64_t *>(smem + lay.tab);
 
     const int slot = blockIdx.y, tile = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
     const uint64_t base = pdep_d((uint64_t)tile, a.cmask);
