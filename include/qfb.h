@@ -123,6 +123,21 @@ QFB_API int qfb_sum_info(qfb_sum h, int64_t *nterms, int64_t *ngroups, int32_t *
 /* out[b * nsegment + g] = <bra_b | O_g | ket_b>.  bra may equal ket
  * (direct_op_exp_val computer.cc:753-771, direct_oppl_exp_val :773-782). */
 QFB_API int qfb_sum_expval(qfb_sum h, qfb_state bra, qfb_state ket, qfb_complex *out);
+/* The same expectation values as qfb_sum_expval, computed without allocating
+ * any device memory.  No counterpart in the reference.  It serves callers that
+ * must not allocate on the device while they run: a request loop that admits
+ * work against a fixed HBM budget and has to keep its footprint constant from
+ * call to call, or code running where every free byte may be held by other
+ * work, so that an allocation could fail or stall.  Its reduction scratch is a
+ * fixed 65,536-entry complex128 array (1 MiB) inside the library, held by every
+ * GPU that loads the library until the process exits; the first call on each
+ * device looks up that array's device address.  Limit: nbatch * (number of
+ * x-groups) + nbatch * nsegment <= 65,536, otherwise QFB_EINVAL.  All calls
+ * share the array, so calls whose kernels overlap on the GPU (different
+ * streams or host threads at the same time) race on it; the caller orders
+ * them.  Results are copied to `out` and the calling thread's stream is
+ * synchronised. */
+QFB_API int qfb_sum_expval_noalloc(qfb_sum h, qfb_state bra, qfb_state ket, qfb_complex *out);
 /* dst <- O src, all segments summed (apply_operator computer.cc:80-91). */
 QFB_API int qfb_sum_apply(qfb_sum h, qfb_state dst, qfb_state src);
 

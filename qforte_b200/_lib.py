@@ -65,6 +65,7 @@ SIGNATURES = {
     "qfb_sum_info": (ctypes.c_int, [c_sum, _vp, _vp, _vp]),
     "qfb_sum_expval": (ctypes.c_int, [c_sum, c_state, c_state, _vp]),
     "qfb_sum_apply": (ctypes.c_int, [c_sum, c_state, c_state]),
+    "qfb_sum_expval_noalloc": (ctypes.c_int, [c_sum, c_state, c_state, _vp]),
     "qfb_prog_create": (ctypes.c_int, [_vp, _vp, _vp, _i64, _i32, _vp]),
     "qfb_prog_destroy": (ctypes.c_int, [c_prog]),
     "qfb_prog_info": (ctypes.c_int, [c_prog, _vp, _vp, _vp]),

@@ -35,6 +35,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <mutex>
 #include <unordered_map>
 #include <vector>
 
@@ -1763,3 +1764,81 @@ int qfb_ucc_profile(qfb_ucc u, int with_grad, int reps, double *stage_ms,
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// expectation values without device allocation
+// ===========================================================================
+
+// Scratch of qfb_sum_expval_noalloc: the per-block partial sums and the
+// per-segment results live in this fixed array of the library's device image
+// instead of a fresh allocation.  Every GPU that loads the library holds it
+// (1 MiB) until the process exits.
+constexpr size_t kNoAllocEntries = 65536;  // double2 entries
+static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocEntries];
+
+static std::mutex g_noalloc_mu;
+static double2 *g_noalloc_addr[64];  // device address of the array, per device
+
+// The array's device address on the current device, looked up once per
+// device (with that device current) on the first call that needs it.
+static int noalloc_scratch(double2 **out) {
+    int dev = 0;
+    QFB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(QFB_ENOSYS, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_addr[dev] = (double2 *)p;
+    }
+    *out = g_noalloc_addr[dev];
+    return QFB_OK;
+}
+
+extern "C" int qfb_sum_expval_noalloc(qfb_sum h, qfb_state bra, qfb_state ket,
+                                      qfb_complex *out) {
+    if (!h || !bra || !ket || !out)
+        return fail(QFB_EINVAL, "qfb_sum_expval_noalloc: null argument");
+    if (bra->nqubit != ket->nqubit || bra->nbatch != ket->nbatch)
+        return fail(QFB_EINVAL, "qfb_sum_expval_noalloc: bra and ket shapes differ");
+    for (const auto &g : h->h_groups)
+        if (g.h >= bra->nqubit)
+            return fail(QFB_EINVAL,
+                        "qfb_sum_expval_noalloc: operator acts on qubit %d of a %d-qubit state",
+                        g.h, bra->nqubit);
+    const int B = bra->nbatch;
+    const size_t nout = (size_t)B * h->nsegment;
+    if (h->ngroups == 0) {
+        for (size_t i = 0; i < nout; ++i) out[i] = qfb_complex{0.0, 0.0};
+        return QFB_OK;
+    }
+    if (h->ngroups > 65535)
+        return fail(QFB_ENOSYS, "qfb_sum_expval_noalloc: more than 65535 x-groups");
+    // one partial per (slot, group, chunk) plus one result per (slot, segment)
+    const size_t rows = (size_t)B * h->ngroups;
+    if (rows + nout > kNoAllocEntries)
+        return fail(QFB_EINVAL,
+                    "qfb_sum_expval_noalloc: %d states x %d x-groups + %zu results need more than "
+                    "the %zu entries of the fixed scratch; use qfb_sum_expval",
+                    B, h->ngroups, nout, kNoAllocEntries);
+    unsigned chunks = chunks_for(bra->nbasis >> 1, B, h->ngroups);
+    const size_t fit = (kNoAllocEntries - nout) / rows;
+    if (chunks > fit) chunks = (unsigned)fit;
+    double2 *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    // every partial is written by exactly one block before it is read, so
+    // the previous call's contents need no clearing
+    double2 *partial = scratch;
+    double2 *res = scratch + rows * chunks;
+    k_sum_expval<<<dim3(chunks, h->ngroups, B), 256, 0, t_stream>>>(
+        bra->d, ket->d, bra->nbasis, h->d_groups, h->d_terms, h->ngroups, partial);
+    QFB_LAUNCHED();
+    k_seg_sum<<<dim3(h->nsegment, B), 256, 0, t_stream>>>(partial, h->d_seg_g0, h->ngroups,
+                                                          chunks, res);
+    QFB_LAUNCHED();
+    QFB_CUDA(cudaMemcpyAsync(out, res, sizeof(double2) * nout, cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
