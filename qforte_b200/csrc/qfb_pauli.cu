@@ -275,6 +275,76 @@ __global__ void __launch_bounds__(256) k_sum_apply4(
     }
 }
 
+// dst = O src over output tiles in shared memory, several states per block.
+// Block (t, c) owns outputs k = t * 2^m + tid (one per thread) of states
+// c * NB .. c * NB + NB - 1.  Groups are visited ordered by their high part
+// x >> m: for each distinct high part the block stages the partner tile
+// (the 2^m inputs k ^ x of its outputs for every x with that high part) of
+// its NB states once, then every group of that high part reads its inputs
+// from shared memory.  f_x(k ^ x) depends on k and x only, so it is computed
+// once and applied to all NB states.
+constexpr int kApplyTileBits = 8;
+constexpr int kApplyStates = 8;
+
+__global__ void __launch_bounds__(1 << kApplyTileBits) k_sum_apply_tiled(
+    double2 *__restrict__ dst, const double2 *__restrict__ src, uint64_t nbasis, int nbatch,
+    int m, const GroupDev *__restrict__ groups, const int32_t *__restrict__ hi_g0,
+    const uint64_t *__restrict__ hi_val, int nhi, const TermDev *__restrict__ terms,
+    const double2 *__restrict__ rterms) {
+    __shared__ double2 tile[kApplyStates][1 << kApplyTileBits];
+    const int T = 1 << m;
+    const int tid = threadIdx.x;
+    const uint64_t kbase = (uint64_t)blockIdx.x << m;
+    const int s0 = blockIdx.y * kApplyStates;
+    const int ns = min(kApplyStates, nbatch - s0);
+    const uint64_t k = kbase + tid;
+    double2 acc[kApplyStates];
+#pragma unroll
+    for (int s = 0; s < kApplyStates; ++s) acc[s] = make_double2(0.0, 0.0);
+    for (int r = 0; r < nhi; ++r) {
+        const uint64_t jbase = kbase ^ (hi_val[r] << m);
+        __syncthreads();
+        for (int s = 0; s < ns; ++s)
+            for (int l = tid; l < T; l += blockDim.x)
+                tile[s][l] = src[(uint64_t)(s0 + s) * nbasis + jbase + l];
+        __syncthreads();
+        if (tid >= T) continue;
+        for (int g = hi_g0[r]; g < hi_g0[r + 1]; ++g) {
+            const GroupDev gr = groups[g];
+            const uint64_t j = k ^ gr.x;
+            const int lj = (int)(j & (uint64_t)(T - 1));
+            if (gr.real) {
+                double f = 0.0;
+                for (int t = gr.begin; t < gr.end; ++t) {
+                    const double2 zc = __ldg(&rterms[t]);
+                    const uint64_t z = (uint64_t)__double_as_longlong(zc.x);
+                    f += parity64(j & z) ? -zc.y : zc.y;
+                }
+#pragma unroll
+                for (int s = 0; s < kApplyStates; ++s) {
+                    if (s < ns) {
+                        const double2 a = tile[s][lj];
+                        acc[s].x += f * a.x;
+                        acc[s].y += f * a.y;
+                    }
+                }
+            } else {
+                double2 f = make_double2(0.0, 0.0);
+                for (int t = gr.begin; t < gr.end; ++t) {
+                    const double2 c = terms[t].c;
+                    if (parity64(j & __ldg(&terms[t].z))) { f.x -= c.x; f.y -= c.y; }
+                    else { f.x += c.x; f.y += c.y; }
+                }
+#pragma unroll
+                for (int s = 0; s < kApplyStates; ++s)
+                    if (s < ns) acc[s] = c_add(acc[s], c_mul(f, tile[s][lj]));
+            }
+        }
+    }
+    if (tid < T)
+        for (int s = 0; s < ns; ++s) dst[(uint64_t)(s0 + s) * nbasis + k] = acc[s];
+}
+
 // ---------------------------------------------------------------------------
 // programs
 // ---------------------------------------------------------------------------
@@ -538,10 +608,27 @@ __global__ void k_set_ref(double2 *__restrict__ psi, uint64_t nbasis, uint64_t r
 // host objects
 // ===========================================================================
 
+// Groups ordered by their high part x >> m, for k_sum_apply_tiled.
+struct TiledView {
+    int m = 0, nhi = 0;
+    void *blob = nullptr;
+    GroupDev *d_groups = nullptr;
+    int32_t *d_hi0 = nullptr;
+    uint64_t *d_hival = nullptr;
+};
+
 struct qfb_sum_s {
     int64_t nterms = 0;
     int32_t ngroups = 0;
     int32_t nsegment = 0;
+    TiledView *tiled[kApplyTileBits + 1] = {nullptr};
+    ~qfb_sum_s() {
+        for (auto *t : tiled)
+            if (t) {
+                dev_free(t->blob);
+                delete t;
+            }
+    }
     void *blob = nullptr;  // device: groups, terms, segment starts
     GroupDev *d_groups = nullptr;
     TermDev *d_terms = nullptr;
@@ -654,7 +741,7 @@ static void push_step(WinPlan *pl, const qfbw::Window &win, const qfb_prog_s *p,
         w.zb_l = qfbw::pext_h(st.zbase, win.qmask);
         w.zb_c = st.zbase & ~win.qmask;
         w.gamma = st.gamma;
-        w.tab = (int32_t)pl->tabs.size();
+        w.tab = (int32_t)pl->tabs.size() - win.tr0;
         const int n = 2 << st.nd;
         pl->tabs.insert(pl->tabs.end(), p->h_tab.begin() + st.tab, p->h_tab.begin() + st.tab + n);
     }
@@ -684,8 +771,9 @@ static int upload_plan(WinPlan *pl) {
     QFB_CUDA(cudaStreamSynchronize(t_stream));
     for (const auto &w : pl->wins)
         if (w.global_step < 0 && w.global_mu < 0)
-            pl->smem_max = std::max(pl->smem_max, qfbw::win_smem_bytes(w.b, pl->L, w.sr1 - w.sr0,
-                                                                       w.st1 - w.st0, pl->nt));
+            pl->smem_max = std::max(pl->smem_max,
+                                    qfbw::win_smem_bytes(w.b, pl->L, w.sr1 - w.sr0, w.st1 - w.st0,
+                                                         pl->nt, w.tr1 - w.tr0));
     return QFB_OK;
 }
 
@@ -710,26 +798,32 @@ static int build_fwd_plan(qfb_prog_s *p, int n, WinPlan **out) {
             ++i;
             continue;
         }
+        auto ntab = [](const StepDev &st) { return st.tab >= 0 ? (2 << st.nd) : 0; };
         uint64_t U = s0.x;
         size_t j = i + 1;
-        int nstr = s0.ns;
+        int nstr = s0.ns, nt = ntab(s0);
         while (j < K) {
             const StepDev &sj = p->h_steps[j];
             const uint64_t U2 = U | sj.x;
-            if (__builtin_popcountll(U2 & ~low) > room || nstr + sj.ns > qfbw::kWinMaxStr) break;
+            if (__builtin_popcountll(U2 & ~low) > room || nstr + sj.ns > qfbw::kWinMaxStr ||
+                (int)(j - i) + 1 > qfbw::kWinMaxSteps || nt + ntab(sj) > qfbw::kWinMaxTab)
+                break;
             U = U2;
             nstr += sj.ns;
+            nt += ntab(sj);
             ++j;
         }
         qfbw::Window w = make_window(U & ~low, n, pl->b, pl->L);
         w.st0 = (int32_t)pl->steps.size();
         w.sr0 = (int32_t)pl->strs.size();
+        w.tr0 = (int32_t)pl->tabs.size();
         for (size_t k = i; k < j; ++k) {
             push_step(pl, w, p, p->h_steps[k], 1, -1, +1);
             push_strings(pl, p, p->h_steps[k], w.qmask, +1, false);
         }
         w.st1 = (int32_t)pl->steps.size();
         w.sr1 = (int32_t)pl->strs.size();
+        w.tr1 = (int32_t)pl->tabs.size();
         pl->wins.push_back(w);
         i = j;
     }
@@ -779,13 +873,32 @@ static int build_grad_plan(qfb_prog_s *kp, const qfb_prog_s *up, int n, WinPlan 
         return c;
     };
     auto empty = [&](int m) { return kp->p_step0[m] < 0 && up->p_step0[m] < 0; };
+    // steps and table entries a parameter adds to a window (upper bounds)
+    auto nst_of = [&](int m) {
+        int32_t a0, a1, b0, b1;
+        steps_of(kp, m, a0, a1);
+        steps_of(up, m, b0, b1);
+        return (a1 - a0) + (b1 - b0);
+    };
+    auto ntab_of = [&](int m) {
+        int c = 0;
+        int32_t a0, a1;
+        steps_of(kp, m, a0, a1);
+        for (int32_t s = a0; s < a1; ++s)
+            if (kp->h_steps[s].tab >= 0) c += 2 << kp->h_steps[s].nd;
+        steps_of(up, m, a0, a1);
+        for (int32_t s = a0; s < a1; ++s)
+            if (up->h_steps[s].tab >= 0) c += 2 << up->h_steps[s].nd;
+        return c;
+    };
     int mu = M - 1;
     while (mu >= 0) {
         if (empty(mu)) {
             --mu;
             continue;
         }
-        if (__builtin_popcountll(supp(mu) & ~low) > room || nstr_of(mu) > qfbw::kWinMaxStr) {
+        if (__builtin_popcountll(supp(mu) & ~low) > room || nstr_of(mu) > qfbw::kWinMaxStr ||
+            nst_of(mu) > qfbw::kWinMaxSteps || ntab_of(mu) > qfbw::kWinMaxTab) {
             qfbw::Window w{};
             w.global_step = -1;
             w.global_mu = mu;
@@ -794,7 +907,7 @@ static int build_grad_plan(qfb_prog_s *kp, const qfb_prog_s *up, int n, WinPlan 
             continue;
         }
         uint64_t U = supp(mu);
-        int nstr = nstr_of(mu);
+        int nstr = nstr_of(mu), nst = nst_of(mu), ntb = ntab_of(mu);
         int lo = mu;
         while (lo - 1 >= 0) {
             const int m = lo - 1;
@@ -803,15 +916,19 @@ static int build_grad_plan(qfb_prog_s *kp, const qfb_prog_s *up, int n, WinPlan 
                 continue;
             }
             const uint64_t U2 = U | supp(m);
-            if (__builtin_popcountll(U2 & ~low) > room || nstr + nstr_of(m) > qfbw::kWinMaxStr)
+            if (__builtin_popcountll(U2 & ~low) > room || nstr + nstr_of(m) > qfbw::kWinMaxStr ||
+                nst + nst_of(m) > qfbw::kWinMaxSteps || ntb + ntab_of(m) > qfbw::kWinMaxTab)
                 break;
             U = U2;
             nstr += nstr_of(m);
+            nst += nst_of(m);
+            ntb += ntab_of(m);
             --lo;
         }
         qfbw::Window w = make_window(U & ~low, n, pl->b, pl->L);
         w.st0 = (int32_t)pl->steps.size();
         w.sr0 = (int32_t)pl->strs.size();
+        w.tr0 = (int32_t)pl->tabs.size();
         for (int m = mu; m >= lo; --m) {
             const int rot = (m > 0) ? 1 : 0;
             int32_t k0, k1, u0, u1;
@@ -837,6 +954,7 @@ static int build_grad_plan(qfb_prog_s *kp, const qfb_prog_s *up, int n, WinPlan 
         }
         w.st1 = (int32_t)pl->steps.size();
         w.sr1 = (int32_t)pl->strs.size();
+        w.tr1 = (int32_t)pl->tabs.size();
         pl->wins.push_back(w);
         mu = lo - 1;
     }
@@ -892,13 +1010,14 @@ static int launch_window(const WinPlan *pl, const qfbw::Window &w, double2 *psi,
     a.nstr = w.sr1 - w.sr0;
     a.steps = pl->d_steps + w.st0;
     a.strs = pl->d_strs + w.sr0;
-    a.tab = pl->d_tabs;
+    a.tab = pl->d_tabs + w.tr0;
+    a.ntab = w.tr1 - w.tr0;
     a.params = d_par;
     a.nparam = nparam;
     a.bcast = bcast;
     a.partial = partial;
     a.ntiles = pl->ntiles();
-    const size_t smem = qfbw::win_smem_bytes(w.b, pl->L, a.nstr, a.nsteps, pl->nt);
+    const size_t smem = qfbw::win_smem_bytes(w.b, pl->L, a.nstr, a.nsteps, pl->nt, a.ntab);
     const dim3 grid((unsigned)a.ntiles, (unsigned)B);
     if (pl->nt == 1)
         qfbw::k_window<1><<<grid, qfbw::kWinThreads, smem, t_stream>>>(psi, nullptr, nbasis, a);
@@ -1012,6 +1131,7 @@ extern "C" {
 
 static int enqueue_sum_apply(const qfb_sum_s *h, double2 *dst, const double2 *src,
                              uint64_t nbasis, int B);
+static int ensure_tiled(qfb_sum_s *h, int nqubit);
 
 int qfb_sum_create(const qfb_pauli *paulis, const qfb_complex *coeffs, const int32_t *segment,
                    int64_t nterms, int32_t nsegment, qfb_sum *out) {
@@ -1190,6 +1310,8 @@ int qfb_sum_apply(qfb_sum h, qfb_state dst, qfb_state src) {
         if (g.h >= src->nqubit)
             return fail(QFB_EINVAL, "qfb_sum_apply: operator acts on qubit %d of a %d-qubit state",
                         g.h, src->nqubit);
+    int rc = ensure_tiled(h, src->nqubit);
+    if (rc) return rc;
     return enqueue_sum_apply(h, dst->d, src->d, src->nbasis, src->nbatch);
 }
 
@@ -1340,8 +1462,76 @@ static int enqueue_prog(const qfb_prog_s *p, double2 *psi, int nqubit, int B,
     return QFB_OK;
 }
 
+static int tile_bits_for(int nqubit) { return std::min(kApplyTileBits, nqubit); }
+
+static int ensure_tiled(qfb_sum_s *h, int nqubit) {
+    const int m = tile_bits_for(nqubit);
+    if (h->tiled[m]) return QFB_OK;
+    std::vector<int32_t> order(h->h_groups.size());
+    for (size_t g = 0; g < order.size(); ++g) order[g] = (int32_t)g;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        return (h->h_groups[a].x >> m) < (h->h_groups[b].x >> m);
+    });
+    std::vector<GroupDev> gs;
+    std::vector<int32_t> hi0;
+    std::vector<uint64_t> hiv;
+    for (size_t i = 0; i < order.size(); ++i) {
+        const GroupDev &g = h->h_groups[order[i]];
+        const uint64_t hi = g.x >> m;
+        if (hiv.empty() || hiv.back() != hi) {
+            hiv.push_back(hi);
+            hi0.push_back((int32_t)i);
+        }
+        gs.push_back(g);
+    }
+    hi0.push_back((int32_t)gs.size());
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t gb = al(sizeof(GroupDev) * std::max<size_t>(1, gs.size()));
+    const size_t hb = al(sizeof(int32_t) * hi0.size());
+    const size_t vb = sizeof(uint64_t) * std::max<size_t>(1, hiv.size());
+    TiledView *tv = new TiledView;
+    tv->m = m;
+    tv->nhi = (int)hiv.size();
+    int rc = dev_alloc(&tv->blob, gb + hb + vb);
+    if (rc) {
+        delete tv;
+        return rc;
+    }
+    tv->d_groups = (GroupDev *)tv->blob;
+    tv->d_hi0 = (int32_t *)((char *)tv->blob + gb);
+    tv->d_hival = (uint64_t *)((char *)tv->blob + gb + hb);
+    cudaError_t e = cudaSuccess;
+    if (!gs.empty())
+        e = cudaMemcpyAsync(tv->d_groups, gs.data(), sizeof(GroupDev) * gs.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(tv->d_hi0, hi0.data(), sizeof(int32_t) * hi0.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess && !hiv.empty())
+        e = cudaMemcpyAsync(tv->d_hival, hiv.data(), sizeof(uint64_t) * hiv.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);
+    if (e != cudaSuccess) {
+        dev_free(tv->blob);
+        delete tv;
+        return cuda_fail(e, "tiled group view upload");
+    }
+    h->tiled[m] = tv;
+    return QFB_OK;
+}
+
 static int enqueue_sum_apply(const qfb_sum_s *h, double2 *dst, const double2 *src,
                              uint64_t nbasis, int B) {
+    const int nq = 63 - __builtin_clzll(nbasis);
+    const TiledView *tv = h->tiled[tile_bits_for(nq)];
+    if (tv && h->ngroups > 0) {
+        const dim3 grid((unsigned)(nbasis >> tv->m), (unsigned)((B + kApplyStates - 1) / kApplyStates));
+        k_sum_apply_tiled<<<grid, 1 << kApplyTileBits, 0, t_stream>>>(
+            dst, src, nbasis, B, tv->m, tv->d_groups, tv->d_hi0, tv->d_hival, tv->nhi, h->d_terms,
+            h->d_rterms);
+        QFB_LAUNCHED();
+        return QFB_OK;
+    }
     if (nbasis >= 4) {
         const dim3 grid(grid_for(nbasis >> 2, 256), B);
         k_sum_apply4<<<grid, 256, 0, t_stream>>>(dst, src, nbasis, h->d_groups, h->d_terms,
@@ -1593,7 +1783,8 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
         for (const auto &sd : p->h_strs)
             if (sd.z >> nqubit) return fail(QFB_EINVAL, "qfb_ucc_create: program beyond qubit");
     }
-    int prc = ensure_plans(fprog, nqubit, true);
+    int prc = ensure_tiled(ham, nqubit);
+    if (prc == QFB_OK) prc = ensure_plans(fprog, nqubit, true);
     if (prc == QFB_OK && gprog) prc = ensure_plans(gprog, nqubit, false, uprog);
     if (prc) return prc;
     qfb_ucc u = new qfb_ucc_s;

@@ -57,12 +57,16 @@ struct Window {
     int32_t b;
     int32_t st0, st1;        // steps [st0, st1) of the plan
     int32_t sr0, sr1;        // strings [sr0, sr1) of the plan
+    int32_t tr0, tr1;        // Givens table entries [tr0, tr1) of the plan
     int32_t global_step;     // >= 0: not windowed, run this program step globally
     int32_t global_mu;       // >= 0: not windowed, run parameter mu's gradient globally
 };
 
 constexpr int kWinMaxStr = 512;
+constexpr int kWinMaxSteps = 128;
+constexpr int kWinMaxTab = 1024;  // double2 table entries staged per window
 constexpr int kWinThreads = 512;
+constexpr int kWinWarps = kWinThreads / 32;
 
 inline uint64_t pext_h(uint64_t v, uint64_t m) {
     uint64_t r = 0;
@@ -93,7 +97,8 @@ struct WinLaunch {
     int nsteps, nstr;
     const WStep *steps;  // this window's steps
     const WStr *strs;    // this window's strings
-    const double2 *tab;  // the plan's Givens tables
+    const double2 *tab;  // this window's Givens tables (WStep::tab is relative)
+    int ntab;
     const double *params;
     int nparam, bcast;
     double2 *partial;  // [rows][nbatch][ntiles]
@@ -104,10 +109,11 @@ struct WinLaunch {
 // arrays (tiles, per-step and per-string cos/sin) first, then the 8-byte
 // ones, then the ints; the spread table starts on a 16-byte boundary.
 struct WinSmem {
-    size_t cs_step, cs_str, g_step, sc_str, zl_str, q_str, tab, total;
+    size_t cs_step, cs_str, gtab, ipw, steps, g_step, sc_str, zl_str, q_str, tab, total;
 };
 
-__host__ __device__ inline WinSmem win_smem_layout(int b, int L, int nstr, int nsteps, int nt) {
+__host__ __device__ inline WinSmem win_smem_layout(int b, int L, int nstr, int nsteps, int nt,
+                                                   int ntab) {
     WinSmem m;
     const size_t T = (size_t)1 << b;
     size_t o = (size_t)nt * T * 16;
@@ -115,6 +121,12 @@ __host__ __device__ inline WinSmem win_smem_layout(int b, int L, int nstr, int n
     o += (size_t)nsteps * 16;
     m.cs_str = o;
     o += (size_t)nstr * 16;
+    m.gtab = o;
+    o += (size_t)ntab * 16;
+    m.ipw = o;
+    o += (size_t)2 * kWinWarps * 16;
+    m.steps = o;
+    o += (size_t)nsteps * sizeof(WStep);
     m.g_step = o;
     o += (size_t)nsteps * 8;
     m.sc_str = o;
@@ -130,8 +142,9 @@ __host__ __device__ inline WinSmem win_smem_layout(int b, int L, int nstr, int n
     return m;
 }
 
-__host__ __device__ inline size_t win_smem_bytes(int b, int L, int nstr, int nsteps, int nt) {
-    return win_smem_layout(b, L, nstr, nsteps, nt).total;
+__host__ __device__ inline size_t win_smem_bytes(int b, int L, int nstr, int nsteps, int nt,
+                                                 int ntab) {
+    return win_smem_layout(b, L, nstr, nsteps, nt, ntab).total;
 }
 
 __device__ __forceinline__ int tile_pattern(uint32_t l, int nd, uint64_t dpos) {
@@ -141,12 +154,12 @@ __device__ __forceinline__ int tile_pattern(uint32_t l, int nd, uint64_t dpos) {
 }
 
 template <int NT>
-__global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ psi,
+__global__ void __launch_bounds__(kWinThreads, 2) k_window(double2 *__restrict__ psi,
                                                         double2 *__restrict__ sig,
                                                         uint64_t nbasis, WinLaunch a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int T = 1 << a.b;
-    const WinSmem lay = win_smem_layout(a.b, a.L, a.nstr, a.nsteps, NT);
+    const WinSmem lay = win_smem_layout(a.b, a.L, a.nstr, a.nsteps, NT, a.ntab);
     double2 *t0 = reinterpret_cast<double2 *>(smem);
     double2 *t1 = t0 + T;
     double2 *s_stcs = reinterpret_cast<double2 *>(smem + lay.cs_step);  // (cos, sin * tile sign)
@@ -156,6 +169,9 @@ __global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ ps
     uint64_t *s_zl = reinterpret_cast<uint64_t *>(smem + lay.zl_str);
     int *s_q = reinterpret_cast<int *>(smem + lay.q_str);
     uint64_t *s_tab = reinterpret_cast<uint64_t *>(smem + lay.tab);
+    double2 *s_gtab = reinterpret_cast<double2 *>(smem + lay.gtab);
+    double2 *s_ipw = reinterpret_cast<double2 *>(smem + lay.ipw);  // [2][warps]
+    WStep *s_steps = reinterpret_cast<WStep *>(smem + lay.steps);
 
     const int slot = blockIdx.y, tile = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
     const uint64_t base = pdep_d((uint64_t)tile, a.cmask);
@@ -170,8 +186,10 @@ __global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ ps
         s_zl[i] = w.zl;
         s_q[i] = (w.ny + 1 + 2 * parity64(base & w.zc)) & 3;
     }
+    for (int i = tid; i < a.ntab; i += nth) s_gtab[i] = a.tab[i];
     for (int st = tid; st < a.nsteps; st += nth) {
         const WStep w = a.steps[st];
+        s_steps[st] = w;
         if (w.tab < 0) continue;
         const double ts = parity64(base & w.zb_c) ? -1.0 : 1.0;
         double s, c;
@@ -190,18 +208,31 @@ __global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ ps
     }
     __syncthreads();
 
+    // Inner products: each warp reduces its share and publishes it in one of
+    // two buffers; after the step's barrier, warp 0 of the next step adds the
+    // warps' shares and writes the tile's partial.  One barrier per step.
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
+    int pend_row = -1;
     for (int st = 0; st < a.nsteps; ++st) {
-        const WStep w = a.steps[st];
+        const WStep w = s_steps[st];
+        if (pend_row >= 0 && warp == 0) {
+            double2 v = (lane < nwarps) ? s_ipw[((st - 1) & 1) * kWinWarps + lane]
+                                        : make_double2(0.0, 0.0);
+            v = warp_sum(v);
+            if (lane == 0)
+                a.partial[((uint64_t)pend_row * gridDim.y + slot) * a.ntiles + tile] = v;
+        }
+        pend_row = -1;
         double2 ip = make_double2(0.0, 0.0);
         const bool want_ip = (NT == 2) && (w.ip_row >= 0);
         if (w.tab >= 0) {
             const double c = s_stcs[st].x, sn = s_stcs[st].y, gam = s_stg[st];
-            const double2 *tb = a.tab + w.tab;
+            const double2 *tb = s_gtab + w.tab;
             const uint32_t xl = (uint32_t)w.xl, zb = (uint32_t)w.zb_l;
             for (int p = tid; p < (T >> 1); p += nth) {
                 const uint32_t l0 = (uint32_t)insert0((uint64_t)p, w.hl);
                 const int pat = tile_pattern(l0, w.nd, w.dpos);
-                const double2 gn = __ldg(&tb[2 * pat]), hn = __ldg(&tb[2 * pat + 1]);
+                const double2 gn = tb[2 * pat], hn = tb[2 * pat + 1];
                 if (gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
                 const uint32_t l1 = l0 ^ xl;
                 const bool neg = __popc(l0 & zb) & 1;
@@ -319,11 +350,17 @@ __global__ void __launch_bounds__(kWinThreads) k_window(double2 *__restrict__ ps
             }
         }
         if (want_ip) {
-            ip = block_sum(ip);
-            if (tid == 0)
-                a.partial[((uint64_t)w.ip_row * gridDim.y + slot) * a.ntiles + tile] = ip;
+            ip = warp_sum(ip);
+            if (lane == 0) s_ipw[(st & 1) * kWinWarps + warp] = ip;
+            pend_row = w.ip_row;
         }
         __syncthreads();
+    }
+    if (pend_row >= 0 && warp == 0) {
+        double2 v = (lane < nwarps) ? s_ipw[((a.nsteps - 1) & 1) * kWinWarps + lane]
+                                    : make_double2(0.0, 0.0);
+        v = warp_sum(v);
+        if (lane == 0) a.partial[((uint64_t)pend_row * gridDim.y + slot) * a.ntiles + tile] = v;
     }
 
     for (int l = tid; l < T; l += nth) {

@@ -22,13 +22,18 @@ int main() {
     for (int nt = 1; nt <= 2; ++nt)
       for (int b = 1; b <= 12; ++b)
         for (int L = 0; L <= 3 && L <= b; ++L)
-          for (int nstr = 0; nstr <= qfbw::kWinMaxStr; ++nstr)
-            for (int nsteps = 0; nsteps <= nstr; nsteps += (nsteps < 8 ? 1 : 37)) {
-              qfbw::WinSmem m = qfbw::win_smem_layout(b, L, nstr, nsteps, nt);
-              bad += (m.cs_step % 16) + (m.cs_str % 16) + (m.g_step % 8) + (m.sc_str % 8) +
-                     (m.zl_str % 8) + (m.q_str % 4) + (m.tab % 16);
-              bad += m.total > 227u * 1024u && b <= 12 && nstr <= 512 && nt * (16u << b) <= 131072u
-                     && (b < 12 || nt == 1);
+          for (int nstr = 0; nstr <= qfbw::kWinMaxStr; nstr += (nstr < 20 ? 1 : 7))
+            for (int nsteps = 0; nsteps <= nstr && nsteps <= 2 * qfbw::kWinMaxSteps;
+                 nsteps += (nsteps < 8 ? 1 : 37)) {
+              for (int ntab = 0; ntab <= qfbw::kWinMaxTab; ntab += 1 + ntab / 3) {
+                qfbw::WinSmem m = qfbw::win_smem_layout(b, L, nstr, nsteps, nt, ntab);
+                bad += (m.cs_step % 16) + (m.cs_str % 16) + (m.gtab % 16) + (m.ipw % 16) +
+                       (m.steps % 8) + (m.g_step % 8) + (m.sc_str % 8) + (m.zl_str % 8) +
+                       (m.q_str % 4) + (m.tab % 16);
+                // the planner's largest windows fit the 227 KB a block may use
+                if (nsteps <= qfbw::kWinMaxSteps && ((b <= 12 && nt == 1) || (b <= 11 && nt == 2)))
+                    bad += m.total > 227u * 1024u;
+              }
             }
     printf("%d\n", bad);
     return bad != 0;
