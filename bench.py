@@ -300,7 +300,7 @@ def main():
     avg_ms = st_ms[dom] / nl
     hbm, src = peaks()
     achieved = per_launch_bytes[dom] / (avg_ms / 1000.0) / 1e9
-    kernel = {1: "k_prog_step", 2: "k_sum_apply", 3: "k_grad_step"}[dom]
+    kernel = {1: "k_window<1>", 2: "k_sum_apply_tiled", 3: "k_window<2>"}[dom]
     roof = {"bound": "hbm", "kernel": kernel, "stage": stages[dom], "achieved": achieved,
             "peak": hbm, "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
             "traffic": None, "algorithmic_bytes_per_launch": per_launch_bytes[dom],

@@ -82,7 +82,15 @@ struct StepDev {  // run of consecutive strings sharing one x (and one parameter
     uint64_t dpos;
     uint64_t zbase;
     double gamma;
+    // Active pairs only: the na <= kMaxActive patterns with a non-zero entry,
+    // as table index and bit mask; j0 = (free-bit counter with zeros inserted
+    // at the nd + 1 sorted positions in zpos, 6 bits each) | patbits[a].
+    int32_t na;    // -1: enumerate every pair and test the pattern
+    uint8_t patidx[8];
+    uint64_t zpos;
+    uint64_t patbits[8];
 };
+constexpr int kMaxActive = 8;
 
 constexpr int kMaxStepStrings = 64;   // strings per fused step (longer runs are split)
 constexpr int kTermTile = 256;        // terms staged in shared memory at a time
@@ -370,6 +378,13 @@ __device__ __forceinline__ int step_pattern(uint64_t j, int nd, uint64_t dpos) {
     return pat;
 }
 
+// Free-bit counter f with zeros inserted at the step's nd + 1 sorted
+// positions (the pattern bits and h): the f-th pair of one active pattern.
+__device__ __forceinline__ uint64_t active_pair(uint64_t f, const StepDev &st) {
+    for (int i = 0; i <= st.nd; ++i) f = insert0(f, (int)((st.zpos >> (6 * i)) & 63));
+    return f;
+}
+
 // Stage this step's strings (in application order) with cos/sin of their
 // angles for slot b into shared memory.
 __device__ __forceinline__ void stage_step(const StepDev &st, const StepParams &sp, int b,
@@ -429,12 +444,23 @@ __global__ void __launch_bounds__(256) k_prog_step(double2 *__restrict__ psi, ui
         double sn, cs;
         sincos((double)sp.sign * st.gamma * step_param(sp, b, st.param), &sn, &cs);
         const double2 *tab = sp.tab + st.tab;
-        for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
-             p += (uint64_t)gridDim.x * blockDim.x) {
-            const uint64_t j0 = insert0(p, st.h);
-            const int pat = step_pattern(j0, st.nd, st.dpos);
+        const bool act = st.na > 0;
+        const int fb = act ? (63 - __clzll(nbasis) - 1 - st.nd) : 0;
+        const uint64_t total = act ? ((uint64_t)st.na << fb) : npair;
+        for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+             q += (uint64_t)gridDim.x * blockDim.x) {
+            uint64_t j0;
+            int pat;
+            if (act) {
+                const int ai = (int)(q >> fb);
+                j0 = active_pair(q & ((1ull << fb) - 1ull), st) | st.patbits[ai];
+                pat = st.patidx[ai];
+            } else {
+                j0 = insert0(q, st.h);
+                pat = step_pattern(j0, st.nd, st.dpos);
+            }
             const double2 gn = __ldg(&tab[2 * pat]), hn = __ldg(&tab[2 * pat + 1]);
-            if (gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
+            if (!act && gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
             const uint64_t j1 = j0 ^ st.x;
             const double ss = parity64(j0 & st.zbase) ? -sn : sn;
             double2 v0 = s[j0], v1 = s[j1];
@@ -487,12 +513,23 @@ __global__ void __launch_bounds__(256) k_grad_step(double2 *__restrict__ psi,
         double sn, cs;
         sincos((double)sp.sign * st.gamma * step_param(sp, b, st.param), &sn, &cs);
         const double2 *tab = sp.tab + st.tab;
-        for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair;
-             p += (uint64_t)gridDim.x * blockDim.x) {
-            const uint64_t j0 = insert0(p, st.h);
-            const int pat = step_pattern(j0, st.nd, st.dpos);
+        const bool act = st.na > 0;
+        const int fb = act ? (63 - __clzll(nbasis) - 1 - st.nd) : 0;
+        const uint64_t total = act ? ((uint64_t)st.na << fb) : npair;
+        for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+             q += (uint64_t)gridDim.x * blockDim.x) {
+            uint64_t j0;
+            int pat;
+            if (act) {
+                const int ai = (int)(q >> fb);
+                j0 = active_pair(q & ((1ull << fb) - 1ull), st) | st.patbits[ai];
+                pat = st.patidx[ai];
+            } else {
+                j0 = insert0(q, st.h);
+                pat = step_pattern(j0, st.nd, st.dpos);
+            }
             const double2 gn = __ldg(&tab[2 * pat]), hn = __ldg(&tab[2 * pat + 1]);
-            if (gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
+            if (!act && gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
             const uint64_t j1 = j0 ^ st.x;
             const bool neg = parity64(j0 & st.zbase);
             double2 v0 = ps[j0], v1 = ps[j1], w0 = sg[j0], w1 = sg[j1];
@@ -741,6 +778,19 @@ static void push_step(WinPlan *pl, const qfbw::Window &win, const qfb_prog_s *p,
         w.zb_l = qfbw::pext_h(st.zbase, win.qmask);
         w.zb_c = st.zbase & ~win.qmask;
         w.gamma = st.gamma;
+        w.na = st.na;
+        if (st.na > 0) {
+            for (int a = 0; a < st.na; ++a) {
+                w.patidx[a] = st.patidx[a];
+                w.patbits[a] = (uint32_t)qfbw::pext_h(st.patbits[a], win.qmask);
+            }
+            int zp[7], nz = 0;
+            for (int i = 0; i < st.nd; ++i) zp[nz++] = (int)((w.dpos >> (6 * i)) & 63);
+            zp[nz++] = w.hl;
+            std::sort(zp, zp + nz);
+            w.zpos = 0;
+            for (int i = 0; i < nz; ++i) w.zpos |= (uint32_t)zp[i] << (4 * i);
+        }
         w.tab = (int32_t)pl->tabs.size() - win.tr0;
         const int n = 2 << st.nd;
         pl->tabs.insert(pl->tabs.end(), p->h_tab.begin() + st.tab, p->h_tab.begin() + st.tab + n);
@@ -1061,6 +1111,7 @@ static void make_table(qfb_prog_s *p, StepDev &st) {
     st.dpos = 0;
     st.zbase = 0;
     st.gamma = 0.0;
+    st.na = -1;
     if (st.x == 0 || st.ns < 1) return;
     const StrDev *S = &p->h_strs[st.s0];
     for (int a = 0; a < st.ns; ++a)
@@ -1118,6 +1169,28 @@ static void make_table(qfb_prog_s *p, StepDev &st) {
     st.tab = (int32_t)p->h_tab.size();
     st.nd = nd;
     for (int i = 0; i < nd; ++i) st.dpos |= (uint64_t)dp[i] << (6 * i);
+    {
+        int na = 0;
+        for (int pat = 0; pat < npat; ++pat)
+            if (g[pat] != 0.0 || hh[pat] != 0.0) {
+                if (na < kMaxActive) {
+                    st.patidx[na] = (uint8_t)pat;
+                    uint64_t bits = 0;
+                    for (int i = 0; i < nd; ++i)
+                        if (pat >> i & 1) bits |= 1ull << dp[i];
+                    st.patbits[na] = bits;
+                }
+                ++na;
+            }
+        st.na = (na <= kMaxActive) ? na : -1;
+        // sorted positions of the pattern bits and h
+        int zp[7], nz = 0;
+        for (int i = 0; i < nd; ++i) zp[nz++] = dp[i];
+        zp[nz++] = st.h;
+        std::sort(zp, zp + nz);
+        st.zpos = 0;
+        for (int i = 0; i < nz; ++i) st.zpos |= (uint64_t)zp[i] << (6 * i);
+    }
     st.zbase = zb;
     st.gamma = gamma2 > 0.0 ? gamma : 0.0;
     for (int pat = 0; pat < npat; ++pat) {
@@ -1355,6 +1428,12 @@ int qfb_prog_create(const qfb_pauli *paulis, const double *scale, const int32_t 
             st.dpos = 0;
             st.zbase = 0;
             st.gamma = 0.0;
+            st.na = -1;
+            st.zpos = 0;
+            for (int a = 0; a < kMaxActive; ++a) {
+                st.patidx[a] = 0;
+                st.patbits[a] = 0;
+            }
             p->h_steps.push_back(st);
         }
     }

@@ -41,6 +41,12 @@ struct WStep {       // one step of a window, masks in tile coordinates
     uint64_t zb_l;   // zbase inside the tile ...
     uint64_t zb_c;   // ... and outside it (a per-tile sign)
     double gamma;
+    // active pairs only (na > 0): zeros inserted at the nd + 1 sorted tile
+    // positions in zpos (4 bits each), then patbits[a] or-ed in
+    int32_t na;
+    uint32_t zpos;
+    uint32_t patbits[8];
+    uint8_t patidx[8];
 };
 
 struct WStr {
@@ -214,7 +220,7 @@ __global__ void __launch_bounds__(kWinThreads, 2) k_window(double2 *__restrict__
     const int lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     int pend_row = -1;
     for (int st = 0; st < a.nsteps; ++st) {
-        const WStep w = s_steps[st];
+        const WStep &w = s_steps[st];
         if (pend_row >= 0 && warp == 0) {
             double2 v = (lane < nwarps) ? s_ipw[((st - 1) & 1) * kWinWarps + lane]
                                         : make_double2(0.0, 0.0);
@@ -229,11 +235,30 @@ __global__ void __launch_bounds__(kWinThreads, 2) k_window(double2 *__restrict__
             const double c = s_stcs[st].x, sn = s_stcs[st].y, gam = s_stg[st];
             const double2 *tb = s_gtab + w.tab;
             const uint32_t xl = (uint32_t)w.xl, zb = (uint32_t)w.zb_l;
-            for (int p = tid; p < (T >> 1); p += nth) {
-                const uint32_t l0 = (uint32_t)insert0((uint64_t)p, w.hl);
-                const int pat = tile_pattern(l0, w.nd, w.dpos);
+            const int nd = w.nd, hl = w.hl;
+            const bool act = w.na > 0;
+            const int fb = act ? (a.b - 1 - nd) : 0;
+            const int total = act ? (w.na << fb) : (T >> 1);
+            const uint32_t zpos = w.zpos;
+            for (int q = tid; q < total; q += nth) {
+                uint32_t l0;
+                int pat;
+                if (act) {
+                    // the q-th active pair: free bits with zeros at D and h
+                    const int ai = q >> fb;
+                    uint32_t f = (uint32_t)q & ((1u << fb) - 1u);
+                    for (int i = 0; i <= nd; ++i) {
+                        const int ps = (int)((zpos >> (4 * i)) & 15u);
+                        f = ((f >> ps) << (ps + 1)) | (f & ((1u << ps) - 1u));
+                    }
+                    l0 = f | w.patbits[ai];
+                    pat = w.patidx[ai];
+                } else {
+                    l0 = (uint32_t)insert0((uint64_t)q, hl);
+                    pat = tile_pattern(l0, nd, w.dpos);
+                }
                 const double2 gn = tb[2 * pat], hn = tb[2 * pat + 1];
-                if (gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
+                if (!act && gn.x == 0.0 && gn.y == 0.0 && hn.x == 0.0 && hn.y == 0.0) continue;
                 const uint32_t l1 = l0 ^ xl;
                 const bool neg = __popc(l0 & zb) & 1;
                 double2 v0 = t0[l0], v1 = t0[l1];
