@@ -292,20 +292,23 @@ __global__ void __launch_bounds__(256) k_sum_apply4(
 // from shared memory.  f_x(k ^ x) depends on k and x only, so it is computed
 // once and applied to all NB states.
 constexpr int kApplyTileBits = 8;
-constexpr int kApplyStates = 8;
+constexpr int kApplyStates = 16;
 
-__global__ void __launch_bounds__(1 << kApplyTileBits) k_sum_apply_tiled(
+// IDX = uint32_t when the state has at most 32 qubits (one popcount per term).
+template <typename IDX>
+__global__ void __launch_bounds__(1 << kApplyTileBits, 2) k_sum_apply_tiled(
     double2 *__restrict__ dst, const double2 *__restrict__ src, uint64_t nbasis, int nbatch,
     int m, const GroupDev *__restrict__ groups, const int32_t *__restrict__ hi_g0,
     const uint64_t *__restrict__ hi_val, int nhi, const TermDev *__restrict__ terms,
     const double2 *__restrict__ rterms) {
-    __shared__ double2 tile[kApplyStates][1 << kApplyTileBits];
+    extern __shared__ double2 apply_smem[];
+    double2(*tile)[1 << kApplyTileBits] = reinterpret_cast<double2(*)[1 << kApplyTileBits]>(apply_smem);
     const int T = 1 << m;
     const int tid = threadIdx.x;
     const uint64_t kbase = (uint64_t)blockIdx.x << m;
     const int s0 = blockIdx.y * kApplyStates;
     const int ns = min(kApplyStates, nbatch - s0);
-    const uint64_t k = kbase + tid;
+    const IDX k = (IDX)(kbase + tid);
     double2 acc[kApplyStates];
 #pragma unroll
     for (int s = 0; s < kApplyStates; ++s) acc[s] = make_double2(0.0, 0.0);
@@ -319,14 +322,17 @@ __global__ void __launch_bounds__(1 << kApplyTileBits) k_sum_apply_tiled(
         if (tid >= T) continue;
         for (int g = hi_g0[r]; g < hi_g0[r + 1]; ++g) {
             const GroupDev gr = groups[g];
-            const uint64_t j = k ^ gr.x;
-            const int lj = (int)(j & (uint64_t)(T - 1));
+            const IDX j = k ^ (IDX)gr.x;
+            const int lj = (int)(j & (IDX)(T - 1));
             if (gr.real) {
                 double f = 0.0;
+#pragma unroll 4
                 for (int t = gr.begin; t < gr.end; ++t) {
                     const double2 zc = __ldg(&rterms[t]);
-                    const uint64_t z = (uint64_t)__double_as_longlong(zc.x);
-                    f += parity64(j & z) ? -zc.y : zc.y;
+                    const IDX z = (IDX)__double_as_longlong(zc.x);
+                    const int odd = (sizeof(IDX) == 4) ? (__popc((uint32_t)(j & z)) & 1)
+                                                       : parity64((uint64_t)(j & z));
+                    f += odd ? -zc.y : zc.y;
                 }
 #pragma unroll
                 for (int s = 0; s < kApplyStates; ++s) {
@@ -340,7 +346,7 @@ __global__ void __launch_bounds__(1 << kApplyTileBits) k_sum_apply_tiled(
                 double2 f = make_double2(0.0, 0.0);
                 for (int t = gr.begin; t < gr.end; ++t) {
                     const double2 c = terms[t].c;
-                    if (parity64(j & __ldg(&terms[t].z))) { f.x -= c.x; f.y -= c.y; }
+                    if (parity64((uint64_t)j & __ldg(&terms[t].z))) { f.x -= c.x; f.y -= c.y; }
                     else { f.x += c.x; f.y += c.y; }
                 }
 #pragma unroll
@@ -349,9 +355,14 @@ __global__ void __launch_bounds__(1 << kApplyTileBits) k_sum_apply_tiled(
             }
         }
     }
-    if (tid < T)
-        for (int s = 0; s < ns; ++s) dst[(uint64_t)(s0 + s) * nbasis + k] = acc[s];
+    if (tid < T) {
+#pragma unroll
+        for (int s = 0; s < kApplyStates; ++s)
+            if (s < ns) dst[(uint64_t)(s0 + s) * nbasis + (uint64_t)k] = acc[s];
+    }
 }
+
+constexpr size_t kApplySmem = sizeof(double2) * kApplyStates * (1 << kApplyTileBits);
 
 // ---------------------------------------------------------------------------
 // programs
@@ -819,11 +830,15 @@ static int upload_plan(WinPlan *pl) {
         QFB_CUDA(cudaMemcpyAsync(pl->d_strs, pl->strs.data(), rb, cudaMemcpyHostToDevice,
                                  t_stream));
     QFB_CUDA(cudaStreamSynchronize(t_stream));
-    for (const auto &w : pl->wins)
-        if (w.global_step < 0 && w.global_mu < 0)
-            pl->smem_max = std::max(pl->smem_max,
-                                    qfbw::win_smem_bytes(w.b, pl->L, w.sr1 - w.sr0, w.st1 - w.st0,
-                                                         pl->nt, w.tr1 - w.tr0));
+    for (auto &w : pl->wins) {
+        if (w.global_step >= 0 || w.global_mu >= 0) continue;
+        w.needs_strings = 0;
+        for (int32_t k = w.st0; k < w.st1; ++k)
+            if (pl->steps[k].tab < 0) w.needs_strings = 1;
+        pl->smem_max = std::max(
+            pl->smem_max, qfbw::win_smem_bytes(w.b, pl->L, w.needs_strings ? w.sr1 - w.sr0 : 0,
+                                               w.st1 - w.st0, pl->nt, w.tr1 - w.tr0));
+    }
     return QFB_OK;
 }
 
@@ -1060,6 +1075,7 @@ static int launch_window(const WinPlan *pl, const qfbw::Window &w, double2 *psi,
     a.nstr = w.sr1 - w.sr0;
     a.steps = pl->d_steps + w.st0;
     a.strs = pl->d_strs + w.sr0;
+    if (!w.needs_strings) a.nstr = 0;  // every step has its Givens table
     a.tab = pl->d_tabs + w.tr0;
     a.ntab = w.tr1 - w.tr0;
     a.params = d_par;
@@ -1068,6 +1084,7 @@ static int launch_window(const WinPlan *pl, const qfbw::Window &w, double2 *psi,
     a.partial = partial;
     a.ntiles = pl->ntiles();
     const size_t smem = qfbw::win_smem_bytes(w.b, pl->L, a.nstr, a.nsteps, pl->nt, a.ntab);
+    if (smem > pl->smem_max) return fail(QFB_EDEVICE, "window shared memory %zu > %zu", smem, pl->smem_max);
     const dim3 grid((unsigned)a.ntiles, (unsigned)B);
     if (pl->nt == 1)
         qfbw::k_window<1><<<grid, qfbw::kWinThreads, smem, t_stream>>>(psi, nullptr, nbasis, a);
@@ -1546,6 +1563,17 @@ static int tile_bits_for(int nqubit) { return std::min(kApplyTileBits, nqubit); 
 static int ensure_tiled(qfb_sum_s *h, int nqubit) {
     const int m = tile_bits_for(nqubit);
     if (h->tiled[m]) return QFB_OK;
+    static std::once_flag smem_once;
+    static cudaError_t smem_err = cudaSuccess;
+    std::call_once(smem_once, [] {
+        smem_err = cudaFuncSetAttribute(k_sum_apply_tiled<uint32_t>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplySmem);
+        if (smem_err == cudaSuccess)
+            smem_err = cudaFuncSetAttribute(k_sum_apply_tiled<uint64_t>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kApplySmem);
+    });
+    if (smem_err != cudaSuccess) return cuda_fail(smem_err, "tiled apply shared memory");
     std::vector<int32_t> order(h->h_groups.size());
     for (size_t g = 0; g < order.size(); ++g) order[g] = (int32_t)g;
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
@@ -1605,9 +1633,14 @@ static int enqueue_sum_apply(const qfb_sum_s *h, double2 *dst, const double2 *sr
     const TiledView *tv = h->tiled[tile_bits_for(nq)];
     if (tv && h->ngroups > 0) {
         const dim3 grid((unsigned)(nbasis >> tv->m), (unsigned)((B + kApplyStates - 1) / kApplyStates));
-        k_sum_apply_tiled<<<grid, 1 << kApplyTileBits, 0, t_stream>>>(
-            dst, src, nbasis, B, tv->m, tv->d_groups, tv->d_hi0, tv->d_hival, tv->nhi, h->d_terms,
-            h->d_rterms);
+        if (nq <= 32)
+            k_sum_apply_tiled<uint32_t><<<grid, 1 << kApplyTileBits, kApplySmem, t_stream>>>(
+                dst, src, nbasis, B, tv->m, tv->d_groups, tv->d_hi0, tv->d_hival, tv->nhi,
+                h->d_terms, h->d_rterms);
+        else
+            k_sum_apply_tiled<uint64_t><<<grid, 1 << kApplyTileBits, kApplySmem, t_stream>>>(
+                dst, src, nbasis, B, tv->m, tv->d_groups, tv->d_hi0, tv->d_hival, tv->nhi,
+                h->d_terms, h->d_rterms);
         QFB_LAUNCHED();
         return QFB_OK;
     }

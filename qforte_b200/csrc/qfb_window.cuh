@@ -66,12 +66,13 @@ struct Window {
     int32_t tr0, tr1;        // Givens table entries [tr0, tr1) of the plan
     int32_t global_step;     // >= 0: not windowed, run this program step globally
     int32_t global_mu;       // >= 0: not windowed, run parameter mu's gradient globally
+    int32_t needs_strings;   // a step without a Givens table: stage the strings
 };
 
 constexpr int kWinMaxStr = 512;
 constexpr int kWinMaxSteps = 128;
 constexpr int kWinMaxTab = 1024;  // double2 table entries staged per window
-constexpr int kWinThreads = 512;
+constexpr int kWinThreads = 256;
 constexpr int kWinWarps = kWinThreads / 32;
 
 inline uint64_t pext_h(uint64_t v, uint64_t m) {
@@ -160,7 +161,7 @@ __device__ __forceinline__ int tile_pattern(uint32_t l, int nd, uint64_t dpos) {
 }
 
 template <int NT>
-__global__ void __launch_bounds__(kWinThreads, 2) k_window(double2 *__restrict__ psi,
+__global__ void __launch_bounds__(kWinThreads, 3) k_window(double2 *__restrict__ psi,
                                                         double2 *__restrict__ sig,
                                                         uint64_t nbasis, WinLaunch a) {
     extern __shared__ __align__(16) unsigned char smem[];
