@@ -182,6 +182,14 @@ typedef struct qfb_ucc_s *qfb_ucc;
 QFB_API int qfb_ucc_create(qfb_prog fprog, qfb_prog kprog, qfb_prog uprog, qfb_sum ham,
                            int nqubit, uint64_t ref_index, int nbatch, qfb_ucc *out);
 QFB_API int qfb_ucc_destroy(qfb_ucc u);
+/* Size of the particle-number sector the evaluator works in (0: the full
+ * space).  When every step of every program keeps the reference's numbers of
+ * alpha (even) and beta (odd) bits, psi stays in that sector and sigma = H psi
+ * is formed on its indices only (sigma is zero elsewhere); the energy and
+ * gradient equal the full-space ones.  No counterpart in the reference, whose
+ * Computer::apply_operator (computer.cc:80-91) always runs over all 2^n
+ * amplitudes. */
+QFB_API int qfb_ucc_sector(qfb_ucc u, int64_t *nsec);
 /* Device addresses of the parameter block and the outputs. */
 QFB_API int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_grad);
 /* Enqueue one evaluation on the calling thread's stream (replays the

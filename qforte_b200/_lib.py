@@ -74,6 +74,7 @@ SIGNATURES = {
     "qfb_ucc_create": (ctypes.c_int, [c_prog, c_prog, c_prog, c_sum, ctypes.c_int, _u64,
                                       ctypes.c_int, _vp]),
     "qfb_ucc_destroy": (ctypes.c_int, [_vp]),
+    "qfb_ucc_sector": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_buffers": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "qfb_ucc_run": (ctypes.c_int, [_vp, ctypes.c_int]),
     "qfb_ucc_capture": (ctypes.c_int, [_vp, ctypes.c_int]),

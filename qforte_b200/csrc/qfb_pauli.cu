@@ -364,6 +364,70 @@ __global__ void __launch_bounds__(1 << kApplyTileBits, 2) k_sum_apply_tiled(
 
 constexpr size_t kApplySmem = sizeof(double2) * kApplyStates * (1 << kApplyTileBits);
 
+// One x-group of a Hamiltonian restricted to a particle-number sector: an
+// output index k of the sector reaches k ^ x inside the sector exactly when k
+// holds half of x's alpha (even) bits and half of its beta (odd) bits.
+struct SecGroup {
+    uint64_t x;
+    int32_t begin, end, real;
+    int32_t halves;  // popcount(x & alpha) / 2 | (popcount(x & beta) / 2) << 8
+};
+
+template <typename IDX>
+__device__ __forceinline__ int popc_t(IDX v) {
+    return (sizeof(IDX) == 4) ? __popc((uint32_t)v) : __popcll((uint64_t)v);
+}
+
+// sigma = H psi on the amplitudes of one sector (states whose amplitudes lie
+// in that sector; the caller zeroes sigma elsewhere).  One warp per output
+// index k of the sector and one lane per state: the group scan and the
+// coefficient sums f_x(k ^ x) are uniform across the warp, and each lane
+// gathers psi[state][k ^ x] once per group that connects k inside the sector.
+template <typename IDX>
+__global__ void __launch_bounds__(256) k_sum_apply_sector(
+    double2 *__restrict__ dst, const double2 *__restrict__ src, uint64_t nbasis, int nbatch,
+    const IDX *__restrict__ sec, int64_t nsec, const SecGroup *__restrict__ groups, int ngroups,
+    const TermDev *__restrict__ terms, const double2 *__restrict__ rterms) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (i >= nsec) return;
+    const int s = blockIdx.y * 32 + lane;
+    const bool live = s < nbatch;
+    const IDX k = sec[i];
+    const double2 *row = src + (uint64_t)(live ? s : 0) * nbasis;
+    const IDX A = (IDX)0x5555555555555555ull;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int g = 0; g < ngroups; ++g) {
+        const uint64_t gx = __ldg(&groups[g].x);
+        const IDX x = (IDX)gx;
+        const IDX kx = k & x;
+        if ((popc_t<IDX>(kx & A) | popc_t<IDX>(kx & ~A) << 8) != __ldg(&groups[g].halves)) continue;
+        const IDX j = k ^ x;
+        const double2 v = live ? __ldg(&row[j]) : make_double2(0.0, 0.0);
+        const int t0 = __ldg(&groups[g].begin), t1 = __ldg(&groups[g].end);
+        if (__ldg(&groups[g].real)) {
+            double f = 0.0;
+#pragma unroll 4
+            for (int t = t0; t < t1; ++t) {
+                const double2 zc = __ldg(&rterms[t]);
+                const IDX z = (IDX)__double_as_longlong(zc.x);
+                f += (popc_t<IDX>(j & z) & 1) ? -zc.y : zc.y;
+            }
+            acc.x += f * v.x;
+            acc.y += f * v.y;
+        } else {
+            double2 f = make_double2(0.0, 0.0);
+            for (int t = t0; t < t1; ++t) {
+                const double2 c = terms[t].c;
+                if (parity64((uint64_t)j & __ldg(&terms[t].z))) { f.x -= c.x; f.y -= c.y; }
+                else { f.x += c.x; f.y += c.y; }
+            }
+            acc = c_add(acc, c_mul(f, v));
+        }
+    }
+    if (live) dst[(uint64_t)s * nbasis + (uint64_t)k] = acc;
+}
+
 // ---------------------------------------------------------------------------
 // programs
 // ---------------------------------------------------------------------------
@@ -1808,6 +1872,127 @@ int qfb_ucc_gradient(qfb_prog kp, qfb_prog up, qfb_state psi, qfb_state sig,
 // compiled dUCC evaluator
 // ===========================================================================
 
+// True when K = sum_a scale_a P_a over strings sharing the x-mask x maps |j>
+// to |j ^ x> only where j and j ^ x hold equal numbers of alpha (even) and of
+// beta (odd) bits.  Patterns run over the bits where K's coefficient can
+// change (the strings' differing z bits and x); more than 16 such bits report
+// false.
+static bool strings_conserve(const StrDev *S, int ns, uint64_t x) {
+    if (x == 0 || ns == 0) return true;
+    const uint64_t A = 0x5555555555555555ull;
+    const int hxa = __builtin_popcountll(x & A), hxb = __builtin_popcountll(x & ~A);
+    if ((hxa | hxb) & 1) return false;
+    uint64_t P = x;
+    for (int a = 0; a < ns; ++a) P |= S[a].z ^ S[0].z;
+    const int np = __builtin_popcountll(P);
+    if (np > 16) return false;
+    int pos[16];
+    for (int i = 0; i < np; ++i) {
+        pos[i] = __builtin_ctzll(P);
+        P &= P - 1;
+    }
+    double norm = 0.0;
+    for (int a = 0; a < ns; ++a) norm += std::fabs(S[a].scale);
+    const double tol = 1e-13 * norm;
+    static const std::complex<double> ipow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+    for (int pat = 0; pat < (1 << np); ++pat) {
+        uint64_t j = 0;
+        for (int i = 0; i < np; ++i)
+            if (pat >> i & 1) j |= 1ull << pos[i];
+        std::complex<double> c = 0.0;
+        for (int a = 0; a < ns; ++a) {
+            const int par = __builtin_popcountll(j & (S[a].z ^ S[0].z)) & 1;
+            c += S[a].scale * ipow[S[a].ny & 3] * (par ? -1.0 : 1.0);
+        }
+        if (std::abs(c) <= tol) continue;
+        if (2 * __builtin_popcountll(j & x & A) != hxa || 2 * __builtin_popcountll(j & x & ~A) != hxb)
+            return false;
+    }
+    return true;
+}
+
+// A step is exponentiated as a whole: its strings must commute (the product
+// of their exponentials is then exp(theta K)) and K must keep every sector.
+static bool step_conserves(const qfb_prog_s *p, const StepDev &st) {
+    if (st.x == 0) return true;
+    const StrDev *S = &p->h_strs[st.s0];
+    for (int a = 0; a < st.ns; ++a)
+        for (int b = a + 1; b < st.ns; ++b)
+            if (__builtin_popcountll(st.x & (S[a].z ^ S[b].z)) & 1) return false;
+    return strings_conserve(S, st.ns, st.x);
+}
+
+// A program used only for inner products <sigma|K_mu|psi> needs each
+// parameter's whole operator K_mu to keep every sector: its strings are
+// checked x-mask by x-mask, wherever they sit in the program.
+static bool prog_sum_conserves(const qfb_prog_s *p) {
+    std::unordered_map<uint64_t, std::vector<StrDev>> by_x;
+    int cur = -1;
+    auto flush = [&]() {
+        for (auto &kv : by_x)
+            if (!strings_conserve(kv.second.data(), (int)kv.second.size(), kv.first)) return false;
+        by_x.clear();
+        return true;
+    };
+    std::vector<const StepDev *> order;
+    for (const auto &st : p->h_steps) order.push_back(&st);
+    std::stable_sort(order.begin(), order.end(),
+                     [](const StepDev *a, const StepDev *b) { return a->param < b->param; });
+    for (const StepDev *st : order) {
+        if (st->param != cur) {
+            if (!flush()) return false;
+            cur = st->param;
+        }
+        auto &v = by_x[st->x];
+        v.insert(v.end(), p->h_strs.begin() + st->s0, p->h_strs.begin() + st->s0 + st->ns);
+    }
+    return flush();
+}
+
+static bool prog_conserves(const qfb_prog_s *p) {
+    for (const auto &st : p->h_steps)
+        if (!step_conserves(p, st)) return false;
+    return true;
+}
+
+// Every index of n qubits with the reference's numbers of alpha (even) and
+// beta (odd) bits, ascending; empty when the sector has 2^31 or more entries.
+static std::vector<uint64_t> sector_indices(int n, uint64_t ref) {
+    const uint64_t A = 0x5555555555555555ull;
+    const uint64_t all = (n >= 64) ? ~0ull : (1ull << n) - 1ull;
+    const int na = (n + 1) / 2, nb = n / 2;
+    const int ka = __builtin_popcountll(ref & A & all), kb = __builtin_popcountll(ref & ~A & all);
+    auto combos = [](int m, int k, int offset) {
+        std::vector<uint64_t> out;
+        if (k > m) return out;
+        if (k == 0) {
+            out.push_back(0);
+            return out;
+        }
+        uint64_t c = (1ull << k) - 1ull;
+        while (c < (1ull << m)) {
+            uint64_t d = 0, w = c;
+            while (w) {
+                const int b = __builtin_ctzll(w);
+                d |= 1ull << (2 * b + offset);
+                w &= w - 1;
+            }
+            out.push_back(d);
+            const uint64_t t = c | (c - 1);  // next combination (Gosper)
+            c = (t + 1) | (((~t & -~t) - 1) >> (__builtin_ctzll(c) + 1));
+        }
+        return out;
+    };
+    const std::vector<uint64_t> ca = combos(na, ka, 0), cb = combos(nb, kb, 1);
+    std::vector<uint64_t> sec;
+    if ((double)ca.size() * (double)cb.size() >= 2147483648.0) return sec;
+    sec.reserve(ca.size() * cb.size());
+    for (uint64_t b : cb)
+        for (uint64_t a : ca) sec.push_back(a | b);
+    std::sort(sec.begin(), sec.end());
+    return sec;
+}
+
 struct qfb_ucc_s {
     qfb_prog_s *fwd = nullptr;
     qfb_prog_s *grad = nullptr;   // K_mu (inner products)
@@ -1824,6 +2009,12 @@ struct qfb_ucc_s {
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     uint64_t graph_kernels[2] = {0, 0};
+    // particle-number sector of the state (every program conserves it):
+    // H psi is formed on these indices only; nsec == 0 means the full space
+    int64_t nsec = 0;
+    void *sec = nullptr;  // uint32_t (nqubit <= 32) or uint64_t indices
+    SecGroup *sgroups = nullptr;
+    int nsgroups = 0;
 };
 
 static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
@@ -1839,7 +2030,21 @@ static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
             rc = enqueue_prog(u->fwd, u->psi, u->nqubit, B, u->params, 0, 1);
             break;
         case 2:
-            rc = enqueue_sum_apply(u->ham, u->sig, u->psi, u->nbasis, B);
+            if (u->nsec > 0) {
+                QFB_CUDA(cudaMemsetAsync(u->sig, 0, sizeof(double2) * u->nbasis * B, t_stream));
+                const dim3 grid((unsigned)((u->nsec + 7) / 8), (unsigned)((B + 31) / 32));
+                if (u->nqubit <= 32)
+                    k_sum_apply_sector<uint32_t><<<grid, 256, 0, t_stream>>>(
+                        u->sig, u->psi, u->nbasis, B, (const uint32_t *)u->sec, u->nsec,
+                        u->sgroups, u->nsgroups, u->ham->d_terms, u->ham->d_rterms);
+                else
+                    k_sum_apply_sector<uint64_t><<<grid, 256, 0, t_stream>>>(
+                        u->sig, u->psi, u->nbasis, B, (const uint64_t *)u->sec, u->nsec,
+                        u->sgroups, u->nsgroups, u->ham->d_terms, u->ham->d_rterms);
+                QFB_LAUNCHED();
+            } else {
+                rc = enqueue_sum_apply(u->ham, u->sig, u->psi, u->nbasis, B);
+            }
             if (rc) return rc;
             k_vdot_rows<<<dim3(u->vchunks, B), 256, 0, t_stream>>>(u->psi, u->sig, u->nbasis,
                                                                  u->vpart);
@@ -1899,6 +2104,18 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     if (prc == QFB_OK) prc = ensure_plans(fprog, nqubit, true);
     if (prc == QFB_OK && gprog) prc = ensure_plans(gprog, nqubit, false, uprog);
     if (prc) return prc;
+    std::vector<uint64_t> sector;
+    std::vector<SecGroup> sgroups;
+    if (prog_conserves(fprog) && (!gprog || (prog_sum_conserves(gprog) && prog_conserves(uprog)))) {
+        sector = sector_indices(nqubit, ref_index);
+        const uint64_t A = 0x5555555555555555ull;
+        for (const auto &g : ham->h_groups) {
+            const int ha = __builtin_popcountll(g.x & A), hb = __builtin_popcountll(g.x & ~A);
+            if ((ha | hb) & 1) continue;  // never connects two indices of one sector
+            sgroups.push_back(SecGroup{g.x, g.begin, g.end, g.real, ha / 2 | (hb / 2) << 8});
+        }
+        if (sgroups.empty()) sector.clear();
+    }
     qfb_ucc u = new qfb_ucc_s;
     u->fwd = fprog;
     u->grad = gprog;
@@ -1927,6 +2144,9 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     const size_t o_vp = take(sizeof(double2) * B * u->vchunks);
     const size_t o_gp = take(gprog ? sizeof(double2) * nsteps * B * u->gchunks : 16);
     const size_t o_ps = take(sizeof(int2) * M);
+    const size_t idx_bytes = nqubit <= 32 ? sizeof(uint32_t) : sizeof(uint64_t);
+    const size_t o_sec = take(idx_bytes * std::max<size_t>(sector.size(), 1));
+    const size_t o_sg = take(sizeof(SecGroup) * std::max<size_t>(sgroups.size(), 1));
     int rc = dev_alloc(&u->blob, off);
     if (rc) {
         delete u;
@@ -1941,6 +2161,12 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     u->vpart = (double2 *)(base + o_vp);
     u->gpart = (double2 *)(base + o_gp);
     u->psteps = (int2 *)(base + o_ps);
+    u->nsec = (int64_t)sector.size();
+    u->sec = base + o_sec;
+    u->sgroups = (SecGroup *)(base + o_sg);
+    u->nsgroups = (int)sgroups.size();
+    std::vector<uint32_t> sec32;
+    if (nqubit <= 32) sec32.assign(sector.begin(), sector.end());
     std::vector<int2> ps(M, make_int2(0, 0));
     if (gprog)
         for (int mu = 0; mu < gprog->nparam; ++mu)
@@ -1949,6 +2175,12 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(u->psteps, ps.data(), sizeof(int2) * M, cudaMemcpyHostToDevice,
                             t_stream);
+    if (e == cudaSuccess && !sector.empty())
+        e = cudaMemcpyAsync(u->sec, nqubit <= 32 ? (const void *)sec32.data() : (const void *)sector.data(),
+                            idx_bytes * sector.size(), cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess && !sgroups.empty())
+        e = cudaMemcpyAsync(u->sgroups, sgroups.data(), sizeof(SecGroup) * sgroups.size(),
+                            cudaMemcpyHostToDevice, t_stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&u->cap_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -1957,6 +2189,12 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
         return cuda_fail(e, "qfb_ucc_create");
     }
     *out = u;
+    return QFB_OK;
+}
+
+int qfb_ucc_sector(qfb_ucc u, int64_t *nsec) {
+    if (!u || !nsec) return fail(QFB_EINVAL, "qfb_ucc_sector: null argument");
+    *nsec = u->nsec;
     return QFB_OK;
 }
 

@@ -61,6 +61,13 @@ class Evaluator:
         self.capture = capture
         self._captured = set()
 
+    @property
+    def sector_size(self):
+        """Indices of the particle-number sector H psi is formed on (0: all)."""
+        n = ctypes.c_int64()
+        check(lib().qfb_ucc_sector(self.h, ctypes.byref(n)), "qfb_ucc_sector")
+        return n.value
+
     def _ensure_graph(self, with_grad):
         if self.capture and with_grad not in self._captured:
             check(lib().qfb_ucc_capture(self.h, int(with_grad)), "qfb_ucc_capture")

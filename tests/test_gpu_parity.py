@@ -267,3 +267,57 @@ def test_computer_api_and_errors(cuda):
     big = qb.Computer(1)
     big.apply_gate(qb.gate("H", 0))
     assert abs(big.get_coeff_array()[1] - 1 / math.sqrt(2)) < 1e-16
+
+
+def test_sector_restricted_h_apply(cuda):
+    """Programs that keep the reference's numbers of alpha and beta electrons
+    form sigma = H psi on that sector only; a program with a spin flip keeps
+    the full space.  Both match the oracle."""
+    from math import comb
+    mol, pool = random_problem(4, 11)
+    tops = list(range(len(pool)))
+    rng = np.random.default_rng(4)
+    amps = rng.uniform(-0.1, 0.1, len(tops))
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+    assert eng.evaluator(1).sector_size == comb(4, 2) ** 2
+    hterms = oracle_terms(mol.hamiltonian)
+    E_o, _ = O.energy(8, mol.hf_reference, kops_forward(pool, tops), amps, hterms)
+    g_o = O.measure_gradient(8, mol.hf_reference, kops_forward(pool, tops), amps, hterms,
+                             kops_grad=kops_gradient(pool, tops))
+    E, g = eng.energy_grad(amps)
+    assert abs(E - E_o) < E_TOL and np.max(np.abs(g - g_o)) < G_TOL
+
+    # append a spin flip (alpha orbital 1 <- beta orbital 0) to the pool
+    flip = qb.SQOperator()
+    flip.add(1.0, [2], [1])
+    flip.add(-1.0, [1], [2])
+    pool.add_term(1.0, flip)
+    tops2 = tops + [len(pool) - 1]
+    amps2 = np.append(amps, 0.07)
+    eng2 = DUCC(mol.hamiltonian, pool, tops2, mol.hf_reference)
+    assert eng2.evaluator(1).sector_size == 0
+    E_o2, _ = O.energy(8, mol.hf_reference, kops_forward(pool, tops2), amps2, hterms)
+    g_o2 = O.measure_gradient(8, mol.hf_reference, kops_forward(pool, tops2), amps2, hterms,
+                              kops_grad=kops_gradient(pool, tops2))
+    E2, g2 = eng2.energy_grad(amps2)
+    assert abs(E2 - E_o2) < E_TOL and np.max(np.abs(g2 - g_o2)) < G_TOL
+    assert abs(E2 - E) > 1e-6  # the flip changes the state
+
+
+@pytest.mark.parametrize("pool_type", ["GSD", "sa_SD"])
+def test_sector_for_generalized_and_spin_adapted_pools(cuda, pool_type):
+    from math import comb
+    mol, pool = random_problem(4, 9, pool_type)
+    tops = list(range(0, len(pool), 3))
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference, pool_type=pool_type)
+    assert eng.evaluator(2).sector_size == comb(4, 2) ** 2
+    rng = np.random.default_rng(1)
+    amps = rng.uniform(-0.1, 0.1, len(tops))
+    hterms = oracle_terms(mol.hamiltonian)
+    kf = kops_forward(pool, tops, pool_type)
+    E_o, _ = O.energy(8, mol.hf_reference, kf, amps, hterms)
+    g_o = O.measure_gradient(8, mol.hf_reference, kf, amps, hterms,
+                             kops_grad=kops_gradient(pool, tops),
+                             kops_unrot=kf if pool_type == "sa_SD" else None)
+    E, g = eng.energy_grad(np.vstack([amps, amps]))
+    assert np.max(np.abs(E - E_o)) < E_TOL and np.max(np.abs(g - g_o[None, :])) < G_TOL
