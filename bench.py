@@ -48,6 +48,13 @@ def parse():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="ucc", choices=["ucc", "gates"],
+                    help="ucc: batched dUCCSD energy+gradient (default); gates: the gate sweep")
+    ap.add_argument("--nqubits", default="20,24,28",
+                    help="gate sweep: comma-separated qubit counts")
+    ap.add_argument("--layers", type=int, default=100, help="gate sweep: layers per circuit")
+    ap.add_argument("--tile", type=int, default=0,
+                    help="gate sweep: tile bits of gate runs (0 default, -1 one pass per gate)")
     return ap.parse_args()
 
 
@@ -189,6 +196,91 @@ def run_reference(a, rank, world):
     return line
 
 
+GATE_METRIC = "gate-sweep pass GB/s"
+
+
+def gate_cpu_baseline(n, spec, seconds=12.0):
+    """The compiled reference's apply_circuit on the first gates of the sweep
+    circuit: seconds per gate, GB/s at the reference's own bytes per gate."""
+    from oracle import oracle as O
+    qf = O.load_reference_engine()
+    t1 = O.ref_gate_sample(qf, n, spec, 4)
+    ngates = int(max(4, min(len(spec), seconds / max(t1, 1e-9))))
+    t = O.ref_gate_sample(qf, n, spec, ngates)
+    return t, ngates
+
+
+def run_gates(a, rank, world, local):
+    """Gate sweep: layered random circuits applied with Computer.apply_circuit."""
+    import torch
+    import qforte_b200 as qb
+    from qforte_b200._lib import launch_count
+    from qforte_b200.device import gate_plan, gates_config
+    from qforte_b200.workloads import layered_random_circuit
+    torch.cuda.set_device(local)
+    gates_config(a.tile, 4)
+    peak, src = peaks()
+    ns = [int(v) for v in a.nqubits.split(",") if v]
+    rows = []
+    clocks = Clocks(local)
+    for n in ns:
+        circ, spec = layered_random_circuit(n, a.layers, a.seed + n)
+        nw, nsingle, pass_bytes = gate_plan(circ.gates(), n)
+        qc = qb.Computer(n)
+        for _ in range(max(a.warmup, 3) if n < 28 else 1):
+            qc.apply_circuit(circ)
+        steps = a.steps if n < 28 else 1
+        torch.cuda.synchronize()
+        if n == ns[-1]:
+            clocks.start()
+        l0 = launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            qc.apply_circuit(circ)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        launches = (launch_count() - l0) // steps
+        ck = clocks.stop() if n == ns[-1] else None
+        gbs = pass_bytes / (ms * 1e-3) / 1e9
+        rows.append({"nqubit": n, "gates": len(spec), "passes": nw + nsingle, "tile_runs": nw,
+                     "one_gate_passes": nsingle, "ms_per_circuit": ms, "pass_gbs": gbs,
+                     "frac_of_hbm": gbs / peak,
+                     "effective_gate_gbs": len(spec) * 32.0 * 2 ** n / (ms * 1e-3) / 1e9,
+                     "gpu_launches": launches})
+        del qc
+    last = rows[-1]
+    line = {"metric": GATE_METRIC, "value": last["pass_gbs"], "unit": "GB/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": last["ms_per_circuit"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic",
+            "config": {"workload": f"layered random circuits, {a.layers} layers, "
+                                   f"{','.join(map(str, ns))} qubits, from |0...0>",
+                       "tile_bits": a.tile, "l2": "state larger than L2 from 23 qubits"},
+            "sweep": rows,
+            "roofline": {"bound": "hbm", "kernel": "k_gate_window", "achieved": last["pass_gbs"],
+                         "peak": peak, "peak_source": src, "unit": "GB/s",
+                         "frac": last["pass_gbs"] / peak, "traffic": None},
+            "gpu_launches": last["gpu_launches"], "clocks": ck}
+    if not a.no_cpu_baseline:
+        try:
+            n0 = min(ns)
+            _, spec0 = layered_random_circuit(n0, a.layers, a.seed + n0)
+            t, ng = gate_cpu_baseline(n0, spec0)
+            bpg = 32.0 * 2 ** n0
+            line["cpu_baseline"] = {"value": bpg / t / 1e9, "unit": "GB/s", "cores": 1,
+                                    "kind": "reference",
+                                    "sample": f"apply_circuit of the first {ng} gates of the "
+                                              f"{n0}-qubit sweep circuit, 32 * 2^n bytes per gate, "
+                                              "serial shipped build",
+                                    "seconds_per_gate": t}
+        except Exception as e:
+            line["cpu_baseline"] = {"unavailable": str(e)}
+    print(json.dumps(line))
+    return line
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -196,6 +288,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         run_reference(a, rank, world)
+        return
+    if a.workload == "gates":
+        if rank == 0:
+            run_gates(a, rank, world, local)
         return
 
     import torch

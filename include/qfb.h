@@ -100,8 +100,23 @@ QFB_API int qfb_state_download(qfb_state s, int b, qfb_complex *host, uint64_t n
 QFB_API int qfb_state_get_amp(qfb_state s, int b, uint64_t index, qfb_complex *out);
 
 /* ---- gates: Computer::apply_circuit / apply_gate ---------------------------
- * computer.cc:93-114, :340-751.  Gates are applied in list order. */
+ * computer.cc:93-114, :340-751.  The result is that of applying the gates one
+ * by one in list order.  Runs of gates whose qubits fit in one set of
+ * tile_bits qubits are applied together to shared-memory tiles of the state
+ * (one read and one write of the state per run); gates on disjoint qubits may
+ * move between runs, which reorders only commuting operations. */
 QFB_API int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates);
+/* Tile shape of the gate runs, process-wide: tile_bits qubits per tile (0: the
+ * default of 11; -1: one full-state pass per gate, as the reference does),
+ * always including the lowest low_bits qubits (default 4).  No counterpart in
+ * the reference; set by the autotuner. */
+QFB_API int qfb_gates_config(int tile_bits, int low_bits);
+/* Host only: how qfb_apply_gates would apply these gates to one nqubit state
+ * under the current tile shape: the number of tile runs, of one-gate passes,
+ * and the bytes those passes read and write (a run 32 * 2^n; a one-gate pass
+ * only the amplitudes its case touches).  No counterpart in the reference. */
+QFB_API int qfb_gates_plan(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t *windows,
+                           int64_t *single_passes, double *pass_bytes);
 
 /* ---- scalars and inner products -------------------------------------------
  * apply_constant computer.cc:130-133; dot computer.cc:975-980. */

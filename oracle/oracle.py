@@ -511,3 +511,19 @@ def ref_eval_sample(qf, nqubit, ref, kops_fwd, kops_grad, amps, hterms, h_sample
         np.vdot(sig.get_coeff_vec(), tmp.get_coeff_vec())
     t_sweep = (time.perf_counter() - t0) * M / m_s
     return t_u + 2.0 * t_h + t_sweep, {"t_U": t_u, "t_H": t_h, "t_sweep": t_sweep}
+
+
+def ref_gate_sample(qf, nqubit, spec, ngates):
+    """Seconds per gate of the compiled reference's Computer.apply_circuit
+    (computer.cc:93-114) on the first ``ngates`` gates of ``spec`` [(kind,
+    target, control, parameter)], from |0...0> (the first gates of the sweep
+    act on a fresh state, as in the reference's own use)."""
+    import time
+
+    circ = qf.Circuit()
+    for k, t, c, p in spec[:ngates]:
+        circ.add(qf.gate(k, int(t), int(c), float(p)))
+    qc = qf.Computer(nqubit)
+    t0 = time.perf_counter()
+    qc.apply_circuit(circ)
+    return (time.perf_counter() - t0) / ngates

@@ -16,6 +16,7 @@
 // touches only the amplitudes its case changes (a diagonal gate with one
 // entry equal to 1 reads and writes half the state, a controlled gate a
 // quarter or half).
+#include <algorithm>
 #include <cstdarg>
 #include <cmath>
 #include <cstring>
@@ -174,6 +175,111 @@ __global__ void k_gate4(double2 *__restrict__ psi, uint64_t nbasis, Gate4 g) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Gate windows: a run of gates whose qubits all lie in one set Q of b qubits
+// (always holding the lowest L qubits, so each tile row is 2^L contiguous
+// amplitudes) is applied to 2^b-amplitude tiles held in shared memory: one
+// read and one write of the state for the whole run.  Each gate performs the
+// per-pair arithmetic of k_gate2 / k_gate4, so a window gives the amplitudes
+// of the same gates applied one pass at a time.
+// ---------------------------------------------------------------------------
+enum : int { K_GEN = 4 };
+
+struct WGate {
+    int32_t kind;  // K_DENSE..K_ANTI: 2x2 block on t (where bit c is set, c >= 0); K_GEN: 4x4
+    int32_t t, c;  // bit positions inside the tile
+    int32_t diag_set;
+    uint32_t nz;
+    int32_t pad;
+    double2 m[16];  // 2x2 kinds: a, b, c, d in m[0..3]
+};
+
+struct GWin {
+    uint64_t qmask, cmask;
+    int b, L, g0, ng;
+};
+
+__device__ __forceinline__ uint64_t gw_pdep(uint64_t v, uint64_t m) {
+    uint64_t r = 0;
+    while (m) {
+        const uint64_t low = m & (~m + 1);
+        if (v & 1ull) r |= low;
+        v >>= 1;
+        m &= m - 1;
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_gate_window(double2 *__restrict__ psi, uint64_t nbasis,
+                                                    GWin w, const WGate *__restrict__ gates) {
+    extern __shared__ double2 gw_smem[];
+    const int T = 1 << w.b;
+    double2 *tile = gw_smem;
+    uint64_t *hitab = reinterpret_cast<uint64_t *>(gw_smem + T);
+    const int tid = threadIdx.x, nth = blockDim.x;
+    double2 *s = psi + (uint64_t)blockIdx.y * nbasis;
+    const uint64_t base = gw_pdep((uint64_t)blockIdx.x, w.cmask);
+    for (int h = tid; h < (T >> w.L); h += nth) hitab[h] = gw_pdep((uint64_t)h << w.L, w.qmask);
+    __syncthreads();
+    const int lmask = (1 << w.L) - 1;
+    for (int l = tid; l < T; l += nth) tile[l] = s[base | hitab[l >> w.L] | (uint64_t)(l & lmask)];
+    __syncthreads();
+    for (int gi = 0; gi < w.ng; ++gi) {
+        const WGate *g = gates + w.g0 + gi;
+        const int kind = __ldg(&g->kind), t = __ldg(&g->t), c = __ldg(&g->c);
+        if (kind == K_GEN) {
+            const uint32_t nz = __ldg(&g->nz);
+            const int lo = min(t, c), hi = max(t, c);
+            for (int p = tid; p < (T >> 2); p += nth) {
+                const int b0 = (int)insert0(insert0((uint64_t)p, lo), hi);
+                const int idx[4] = {b0, b0 | (1 << t), b0 | (1 << c), b0 | (1 << t) | (1 << c)};
+                double2 x[4], y[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) x[j] = tile[idx[j]];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (nz & (1u << (4 * i + j))) acc = c_add(acc, c_mul(__ldg(&g->m[4 * i + j]), x[j]));
+                    y[i] = acc;
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) tile[idx[i]] = y[i];
+            }
+        } else {
+            const double2 a = __ldg(&g->m[0]), bb = __ldg(&g->m[1]), cc = __ldg(&g->m[2]),
+                          d = __ldg(&g->m[3]);
+            const int dset = __ldg(&g->diag_set);
+            const int npair = (c < 0) ? (T >> 1) : (T >> 2);
+            const int lo = (c < 0) ? t : min(t, c), hi = (c < 0) ? -1 : max(t, c);
+            for (int p = tid; p < npair; p += nth) {
+                int i0 = (int)insert0((uint64_t)p, lo);
+                if (hi >= 0) i0 = (int)insert0((uint64_t)i0, hi) | (1 << c);
+                const int i1 = i0 | (1 << t);
+                if (kind == K_DENSE) {
+                    const double2 x0 = tile[i0], x1 = tile[i1];
+                    tile[i0] = c_add(c_mul(a, x0), c_mul(bb, x1));
+                    tile[i1] = c_add(c_mul(cc, x0), c_mul(d, x1));
+                } else if (kind == K_DIAG) {
+                    if (dset & 1) tile[i0] = c_mul(a, tile[i0]);
+                    if (dset & 2) tile[i1] = c_mul(d, tile[i1]);
+                } else if (kind == K_SWAP) {
+                    const double2 x0 = tile[i0], x1 = tile[i1];
+                    tile[i0] = x1;
+                    tile[i1] = x0;
+                } else {
+                    const double2 x0 = tile[i0], x1 = tile[i1];
+                    tile[i0] = c_mul(bb, x1);
+                    tile[i1] = c_mul(cc, x0);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    for (int l = tid; l < T; l += nth) s[base | hitab[l >> w.L] | (uint64_t)(l & lmask)] = tile[l];
+}
+
 __global__ void k_scale(double2 *__restrict__ psi, uint64_t n, double2 a) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x)
@@ -251,6 +357,152 @@ Gate2 classify2(const qfb_complex &a, const qfb_complex &b, const qfb_complex &c
         g.kind = ceq(b, c) ? K_SWAP : K_ANTI;
     }
     return g;
+}
+
+// One gate as the kernels apply it (classified once on the host).
+struct HGate {
+    int form;  // 0: Gate2 (1-qubit or controlled), 1: Gate4
+    Gate2 g2;
+    Gate4 g4;
+    uint64_t qubits;
+};
+
+HGate classify_gate(const qfb_gate &g) {
+    HGate h{};
+    const auto &m = g.mat;
+    h.qubits = (1ull << g.target) | (1ull << g.control);
+    if (g.target == g.control) {
+        h.form = 0;
+        h.g2 = classify2(m[0][0], m[0][1], m[1][0], m[1][1], g.target, -1);
+        return h;
+    }
+    const bool controlled =
+        (cabs_h(m[0][1]) + cabs_h(m[1][0]) < kThr) && is_one(m[0][0]) && is_one(m[1][1]);
+    if (controlled) {
+        h.form = 0;
+        h.g2 = classify2(m[2][2], m[2][3], m[3][2], m[3][3], g.target, g.control);
+        return h;
+    }
+    h.form = 1;
+    h.g4.t = g.target;
+    h.g4.c = g.control;
+    h.g4.nz = 0;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            h.g4.m[4 * i + j] = d2(m[i][j]);
+            if (cabs_h(m[i][j]) > kThr) h.g4.nz |= 1u << (4 * i + j);
+        }
+    return h;
+}
+
+// One full-state pass for one gate.
+int launch_single(qfb_state s, const HGate &h) {
+    const dim3 block(256);
+    if (h.form == 0) {
+        const uint64_t n = (h.g2.c < 0) ? (s->nbasis >> 1) : (s->nbasis >> 2);
+        k_gate2<<<dim3(grid_for(n, 256), s->nbatch), block, 0, t_stream>>>(s->d, s->nbasis, h.g2);
+    } else {
+        k_gate4<<<dim3(grid_for(s->nbasis >> 2, 256), s->nbatch), block, 0, t_stream>>>(
+            s->d, s->nbasis, h.g4);
+    }
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
+constexpr int kGateTileDefault = 11;  // 2^11 amplitudes = 32 KB of shared memory per tile
+constexpr int kGateTileMax = 13;
+int g_gate_tile_bits = 0;  // 0: kGateTileDefault; -1: one pass per gate
+int g_gate_low_bits = 4;
+
+int gate_window_smem() {
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        const int bytes = (int)(sizeof(double2) << kGateTileMax) + (int)(sizeof(uint64_t) << kGateTileMax);
+        err = cudaFuncSetAttribute(k_gate_window, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    });
+    return err == cudaSuccess ? QFB_OK : cuda_fail(err, "gate window shared memory");
+}
+
+struct GatePlanWin {
+    GWin w;
+    int64_t single;  // >= 0: a window of one gate, applied by its own pass
+};
+
+// Greedy windows: scanning the unapplied gates in order, a gate joins the
+// current window when no earlier unapplied gate shares one of its qubits
+// (gates on disjoint qubits commute) and its qubits fit in the window's b
+// qubits together with those already chosen; a gate that cannot join blocks
+// its qubits for the rest of the scan.  The window's qubits always include
+// the lowest L, and are filled up to b with the lowest unused ones.
+void plan_gate_windows(const std::vector<HGate> &hg, int n, int b, int L,
+                       std::vector<GatePlanWin> &wins, std::vector<WGate> &wg) {
+    const int64_t N = (int64_t)hg.size();
+    const uint64_t all = (n >= 64) ? ~0ull : (1ull << n) - 1ull;
+    const uint64_t low = (1ull << L) - 1ull;
+    std::vector<char> done((size_t)N, 0);
+    int64_t first = 0;
+    std::vector<int64_t> sel;
+    while (first < N) {
+        uint64_t Q = low, blocked = 0;
+        sel.clear();
+        int64_t scanned = 0;
+        for (int64_t i = first; i < N && blocked != all && scanned < 16384; ++i) {
+            if (done[i]) continue;
+            ++scanned;
+            const uint64_t gm = hg[i].qubits;
+            if (gm & blocked) {
+                blocked |= gm;
+                continue;
+            }
+            const uint64_t nq = Q | gm;
+            if (__builtin_popcountll(nq) <= b) {
+                Q = nq;
+                sel.push_back(i);
+                done[i] = 1;
+            } else {
+                blocked |= gm;
+            }
+        }
+        while (first < N && done[first]) ++first;
+        GatePlanWin pw{};
+        if (sel.size() == 1) {
+            pw.single = sel[0];
+            wins.push_back(pw);
+            continue;
+        }
+        for (int q = 0; q < n && __builtin_popcountll(Q) < b; ++q) Q |= 1ull << q;
+        auto loc = [&](int q) { return __builtin_popcountll(Q & ((1ull << q) - 1ull)); };
+        pw.single = -1;
+        pw.w.qmask = Q;
+        pw.w.cmask = all & ~Q;
+        pw.w.b = b;
+        pw.w.L = L;
+        pw.w.g0 = (int)wg.size();
+        pw.w.ng = (int)sel.size();
+        for (int64_t i : sel) {
+            const HGate &h = hg[i];
+            WGate w{};
+            if (h.form == 0) {
+                w.kind = h.g2.kind;
+                w.t = loc(h.g2.t);
+                w.c = h.g2.c < 0 ? -1 : loc(h.g2.c);
+                w.diag_set = h.g2.diag_set;
+                w.m[0] = h.g2.a;
+                w.m[1] = h.g2.b;
+                w.m[2] = h.g2.cc;
+                w.m[3] = h.g2.d;
+            } else {
+                w.kind = K_GEN;
+                w.t = loc(h.g4.t);
+                w.c = loc(h.g4.c);
+                w.nz = h.g4.nz;
+                for (int k = 0; k < 16; ++k) w.m[k] = h.g4.m[k];
+            }
+            wg.push_back(w);
+        }
+        wins.push_back(pw);
+    }
 }
 
 }  // namespace
@@ -445,6 +697,63 @@ int qfb_state_get_amp(qfb_state s, int b, uint64_t index, qfb_complex *out) {
     return QFB_OK;
 }
 
+int qfb_gates_config(int tile_bits, int low_bits) {
+    if (low_bits < 0 || low_bits > 6)
+        return fail(QFB_EINVAL, "qfb_gates_config: low_bits = %d outside [0, 6]", low_bits);
+    if (tile_bits != -1 && tile_bits != 0 && (tile_bits < low_bits + 2 || tile_bits > kGateTileMax))
+        return fail(QFB_EINVAL, "qfb_gates_config: tile_bits = %d outside [%d, %d]", tile_bits,
+                    low_bits + 2, kGateTileMax);
+    g_gate_tile_bits = tile_bits;
+    g_gate_low_bits = low_bits;
+    return QFB_OK;
+}
+
+int qfb_gates_plan(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t *windows,
+                   int64_t *single_passes, double *pass_bytes) {
+    if (ngates < 0 || (ngates > 0 && !gates) || nqubit < 1 || nqubit > 40)
+        return fail(QFB_EINVAL, "qfb_gates_plan: bad arguments");
+    std::vector<HGate> hg((size_t)ngates);
+    for (int64_t k = 0; k < ngates; ++k) {
+        const qfb_gate &g = gates[k];
+        if (g.target < 0 || g.target >= nqubit || g.control < 0 || g.control >= nqubit)
+            return fail(QFB_EINVAL, "qfb_gates_plan: gate %lld acts beyond qubit %d",
+                        (long long)k, nqubit);
+        hg[k] = classify_gate(g);
+    }
+    const double full = 32.0 * (double)(1ull << nqubit);
+    // amplitudes a one-gate pass reads and writes (16 bytes each way)
+    auto single_bytes = [&](const HGate &h) {
+        if (h.form == 1) return full;
+        double f = (h.g2.c < 0) ? 1.0 : 0.5;
+        if (h.g2.kind == K_DIAG && h.g2.diag_set != 3) f *= (h.g2.diag_set == 0) ? 0.0 : 0.5;
+        return f * full;
+    };
+    int64_t nw = 0, ns = 0;
+    double bytes = 0.0;
+    int b = g_gate_tile_bits == 0 ? kGateTileDefault : g_gate_tile_bits;
+    if (b < 0 || ngates == 1) {
+        for (const HGate &h : hg) bytes += single_bytes(h);
+        ns = ngates;
+    } else {
+        std::vector<GatePlanWin> wins;
+        std::vector<WGate> wg;
+        plan_gate_windows(hg, nqubit, std::min(b, nqubit), std::min(g_gate_low_bits, nqubit), wins, wg);
+        for (const GatePlanWin &pw : wins) {
+            if (pw.single >= 0) {
+                ++ns;
+                bytes += single_bytes(hg[pw.single]);
+            } else {
+                ++nw;
+                bytes += full;
+            }
+        }
+    }
+    if (windows) *windows = nw;
+    if (single_passes) *single_passes = ns;
+    if (pass_bytes) *pass_bytes = bytes;
+    return QFB_OK;
+}
+
 int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates) {
     if (!s) return fail(QFB_EINVAL, "qfb_apply_gates: null state");
     if (ngates < 0 || (ngates > 0 && !gates))
@@ -456,40 +765,45 @@ int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates) {
                         "qfb_apply_gates: gate %lld acts on qubit (%d, %d) of a %d-qubit state",
                         (long long)k, g.target, g.control, s->nqubit);
     }
-    const dim3 block(256);
-    for (int64_t k = 0; k < ngates; ++k) {
-        const qfb_gate &g = gates[k];
-        const auto &m = g.mat;
-        if (g.target == g.control) {
-            Gate2 q = classify2(m[0][0], m[0][1], m[1][0], m[1][1], g.target, -1);
-            const dim3 grid(grid_for(s->nbasis >> 1, 256), s->nbatch);
-            k_gate2<<<grid, block, 0, t_stream>>>(s->d, s->nbasis, q);
-            QFB_LAUNCHED();
-            continue;
+    if (ngates == 0) return QFB_OK;
+    std::vector<HGate> hg((size_t)ngates);
+    for (int64_t k = 0; k < ngates; ++k) hg[k] = classify_gate(gates[k]);
+    const int n = s->nqubit;
+    int b = g_gate_tile_bits == 0 ? kGateTileDefault : g_gate_tile_bits;
+    if (b < 0 || ngates == 1) {
+        for (const HGate &h : hg) {
+            const int rc = launch_single(s, h);
+            if (rc) return rc;
         }
-        const bool controlled = (cabs_h(m[0][1]) + cabs_h(m[1][0]) < kThr) && is_one(m[0][0]) &&
-                                is_one(m[1][1]);
-        if (controlled) {
-            Gate2 q = classify2(m[2][2], m[2][3], m[3][2], m[3][3], g.target, g.control);
-            const dim3 grid(grid_for(s->nbasis >> 2, 256), s->nbatch);
-            k_gate2<<<grid, block, 0, t_stream>>>(s->d, s->nbasis, q);
-            QFB_LAUNCHED();
-            continue;
-        }
-        Gate4 q;
-        q.t = g.target;
-        q.c = g.control;
-        q.nz = 0;
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) {
-                q.m[4 * i + j] = d2(m[i][j]);
-                if (cabs_h(m[i][j]) > kThr) q.nz |= 1u << (4 * i + j);
-            }
-        const dim3 grid(grid_for(s->nbasis >> 2, 256), s->nbatch);
-        k_gate4<<<grid, block, 0, t_stream>>>(s->d, s->nbasis, q);
-        QFB_LAUNCHED();
+        return QFB_OK;
     }
-    return QFB_OK;
+    int L = std::min(g_gate_low_bits, n);
+    b = std::min(b, n);
+    std::vector<GatePlanWin> wins;
+    std::vector<WGate> wg;
+    plan_gate_windows(hg, n, b, L, wins, wg);
+    void *buf = nullptr;
+    if (!wg.empty()) {
+        int rc = dev_alloc(&buf, sizeof(WGate) * wg.size());
+        if (rc) return rc;
+        QFB_CUDA(cudaMemcpyAsync(buf, wg.data(), sizeof(WGate) * wg.size(), cudaMemcpyHostToDevice,
+                                 t_stream));
+    }
+    int rc = gate_window_smem();
+    for (const GatePlanWin &pw : wins) {
+        if (rc) break;
+        if (pw.single >= 0) {
+            rc = launch_single(s, hg[pw.single]);
+            continue;
+        }
+        const size_t smem = sizeof(double2) * ((size_t)1 << pw.w.b) +
+                            sizeof(uint64_t) * ((size_t)1 << (pw.w.b - pw.w.L));
+        const dim3 grid((unsigned)(s->nbasis >> pw.w.b), s->nbatch);
+        k_gate_window<<<grid, 256, smem, t_stream>>>(s->d, s->nbasis, pw.w, (const WGate *)buf);
+        rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
+    }
+    dev_free(buf);
+    return rc;
 }
 
 int qfb_scale(qfb_state s, qfb_complex a) {

@@ -161,3 +161,21 @@ def pack_gates(gates):
         arr[k]["control"] = g.control()
         arr[k]["mat"] = g.matrix()
     return arr
+
+
+def gate_plan(gates, nqubit):
+    """(tile runs, one-gate passes, bytes read and written) of applying
+    ``gates`` (Gate objects) to one ``nqubit`` state under the current tile
+    shape; host only."""
+    arr = pack_gates(gates)
+    w, s, b = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()
+    check(lib().qfb_gates_plan(arr.ctypes.data if len(arr) else None, len(arr), int(nqubit),
+                               ctypes.byref(w), ctypes.byref(s), ctypes.byref(b)),
+          "qfb_gates_plan")
+    return w.value, s.value, b.value
+
+
+def gates_config(tile_bits=0, low_bits=4):
+    """Process-wide tile shape of gate runs (tile_bits 0: default, -1: one
+    pass per gate)."""
+    check(lib().qfb_gates_config(int(tile_bits), int(low_bits)), "qfb_gates_config")

@@ -1,0 +1,49 @@
+"""Host-side planning of gate runs (no GPU): how many shared-memory tile runs
+and one-gate passes a circuit becomes, and the bytes those passes move."""
+
+import pytest
+
+import qforte_b200 as qb
+from qforte_b200.device import gate_plan, gates_config
+from qforte_b200.workloads import layered_random_circuit
+
+
+@pytest.fixture(autouse=True)
+def _default_tiles():
+    yield
+    gates_config(0, 4)
+
+
+def test_small_state_is_one_run():
+    circ, _ = layered_random_circuit(8, 10, 1)
+    w, s, b = gate_plan(circ.gates(), 8)
+    assert (w, s, b) == (1, 0, 32.0 * 2 ** 8)
+
+
+def test_one_pass_per_gate_counts_touched_amplitudes():
+    gates_config(-1, 4)
+    g = [qb.gate("H", 0, 0), qb.gate("T", 1, 1), qb.gate("Z", 2, 2), qb.gate("cX", 0, 3),
+         qb.gate("cZ", 1, 2), qb.gate("SWAP", 0, 1), qb.gate("I", 3, 3)]
+    w, s, b = gate_plan(g, 4)
+    full = 32.0 * 16
+    # H full; T and Z one diagonal entry != 1: half; cX controlled: half;
+    # cZ controlled diagonal with one entry != 1: a quarter; SWAP generic: full;
+    # identity: nothing
+    assert (w, s) == (0, 7)
+    assert b == full * (1 + 0.5 + 0.5 + 0.5 + 0.25 + 1 + 0)
+
+
+def test_sweep_runs_fuse_layers():
+    circ, spec = layered_random_circuit(24, 20, 2)
+    w, s, b = gate_plan(circ.gates(), 24)
+    assert 0 < w + s < len(spec) / 4
+    gates_config(13, 4)
+    w13, s13, _ = gate_plan(circ.gates(), 24)
+    assert w13 + s13 <= w + s
+
+
+def test_plan_rejects_gates_beyond_the_state():
+    with pytest.raises(ValueError):
+        gate_plan([qb.gate("X", 5, 5)], 4)
+    with pytest.raises(ValueError):
+        gates_config(20, 4)

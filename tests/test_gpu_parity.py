@@ -321,3 +321,39 @@ def test_sector_for_generalized_and_spin_adapted_pools(cuda, pool_type):
                              kops_unrot=kf if pool_type == "sa_SD" else None)
     E, g = eng.energy_grad(np.vstack([amps, amps]))
     assert np.max(np.abs(E - E_o)) < E_TOL and np.max(np.abs(g - g_o[None, :])) < G_TOL
+
+
+@pytest.fixture
+def gate_tiles():
+    """Restores the default gate tile shape after a test changes it."""
+    from qforte_b200._lib import check, lib
+    yield lambda b, L: check(lib().qfb_gates_config(b, L), "qfb_gates_config")
+    check(lib().qfb_gates_config(0, 4), "qfb_gates_config")
+
+
+@pytest.mark.parametrize("tile,low", [(-1, 4), (0, 4), (2, 0), (4, 1), (6, 3), (9, 4), (13, 6)])
+@pytest.mark.parametrize("n,ngates,seed", [(3, 80, 5), (8, 300, 6), (14, 200, 7)])
+def test_gate_windows_match_oracle(cuda, gate_tiles, tile, low, n, ngates, seed):
+    """Gate runs applied to shared-memory tiles of every shape (and one pass
+    per gate, tile -1) against the oracle's gate-by-gate application."""
+    gate_tiles(tile, low)
+    circ, ora = _rand_circuit(n, ngates, seed)
+    qc = qb.Computer(n)
+    qc.apply_circuit(circ)
+    st = O.State(n)
+    st.apply_gates(ora)
+    assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
+
+
+@pytest.mark.parametrize("n", [7, 16])
+def test_layered_sweep_circuit_matches_oracle(cuda, gate_tiles, n):
+    """The gate-sweep workload (random layers of 1-qubit gates and pairings)."""
+    from qforte_b200.workloads import layered_random_circuit
+    circ, spec = layered_random_circuit(n, 12, 3)
+    st = O.State(n)
+    st.apply_gates([O.make_gate(k, t, c, p) for k, t, c, p in spec])
+    for tile in (0, -1):
+        gate_tiles(tile, 4)
+        qc = qb.Computer(n)
+        qc.apply_circuit(circ)
+        assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
