@@ -48,8 +48,12 @@ def parse():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="ucc", choices=["ucc", "gates"],
-                    help="ucc: batched dUCCSD energy+gradient (default); gates: the gate sweep")
+    ap.add_argument("--workload", default="ucc", choices=["ucc", "gates", "grad", "adapt"],
+                    help="ucc: batched dUCCSD energy+gradient (default); gates: the gate sweep; "
+                         "grad: differentiable energy, forward+backward against forward alone; "
+                         "adapt: every ADAPT pool gradient of a 12-operator state in one launch")
+    ap.add_argument("--adapt-norb", type=int, default=10, help="adapt workload: orbitals")
+    ap.add_argument("--norbs", default="8,10", help="grad workload: orbital counts")
     ap.add_argument("--nqubits", default="20,24,28",
                     help="gate sweep: comma-separated qubit counts")
     ap.add_argument("--layers", type=int, default=100, help="gate sweep: layers per circuit")
@@ -281,6 +285,148 @@ def run_gates(a, rank, world, local):
     return line
 
 
+def run_grad(a, local):
+    """Differentiable dUCCSD energy: forward (energy) and forward+backward
+    (energy and the adjoint gradient through torch.autograd) per parameter
+    set, at each orbital count (half filling, SD pool)."""
+    import torch
+    from qforte_b200.autograd import ucc_energy
+    from qforte_b200.ucc import DUCC
+    torch.cuda.set_device(local)
+    rows = []
+    for norb in [int(v) for v in a.norbs.split(",") if v]:
+        mol, pool = problem(norb, a.seed)
+        eng = DUCC(mol.hamiltonian, pool, list(range(len(pool))), mol.hf_reference)
+        M = len(pool)
+        rng = np.random.default_rng(a.seed + norb)
+        res = {"nqubit": 2 * norb, "nparam": M, "hamiltonian_terms": len(mol.hamiltonian)}
+        for B in (1, a.batch):
+            t = torch.tensor(rng.uniform(-0.1, 0.1, (B, M)), device="cuda", requires_grad=True)
+            for _ in range(max(a.warmup, 3)):
+                ucc_energy(t, eng).sum().backward()
+                with torch.no_grad():
+                    ucc_energy(t, eng)
+            times = {}
+            for mode in ("forward", "forward+backward"):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                for _ in range(a.steps):
+                    if mode == "forward":
+                        with torch.no_grad():
+                            ucc_energy(t, eng)
+                    else:
+                        t.grad = None
+                        ucc_energy(t, eng).sum().backward()
+                e1.record()
+                torch.cuda.synchronize()
+                times[mode] = e0.elapsed_time(e1) / a.steps
+            res[f"batch{B}"] = {"forward_ms": times["forward"],
+                                "forward_backward_ms": times["forward+backward"],
+                                "ratio": times["forward+backward"] / times["forward"]}
+        rows.append(res)
+        del eng
+    big = rows[-1][f"batch{a.batch}"]
+    line = {"metric": "dUCCSD energy+gradient evals/s (autograd)",
+            "value": 1000.0 * a.batch / big["forward_backward_ms"], "unit": "evals/s",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": big["forward_backward_ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "torch.autograd over the adjoint sweep, SD pool, half filling, "
+                                   f"orbitals {a.norbs}, batches 1 and {a.batch}"},
+            "sizes": rows}
+    print(json.dumps(line))
+    return line
+
+
+def run_adapt(a, local):
+    """ADAPT pool gradients 2 Re <H psi|A_k psi> of every generalized
+    spin-conserving single and double (GSD pool) at a 12-operator dUCC state,
+    against the plain per-call path (UCCVQE.measure_gradient3 through the
+    Computer API, call for call, timed on a sample of operators)."""
+    import time
+    import torch
+    import qforte_b200 as qb
+    from qforte_b200._lib import launch_count
+    from qforte_b200.ucc import ADAPTVQE, DUCC
+    torch.cuda.set_device(local)
+    norb = a.adapt_norb
+    mol = qb.random_molecule(norb, norb, a.seed)
+    pool = qb.SQOpPool()
+    pool.set_orb_spaces(mol.hf_reference)
+    pool.fill_pool("GSD")
+    rng = np.random.default_rng(a.seed + 7)
+    tops = [int(v) for v in rng.choice(len(pool), 12, replace=False)]
+    amps = rng.uniform(-0.1, 0.1, 12)
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+    t0 = time.perf_counter()
+    eng._pool_sum_handle()
+    compile_s = time.perf_counter() - t0
+    for _ in range(max(a.warmup, 3)):
+        g = eng.pool_gradients(amps)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = launch_count()
+    e0.record()
+    for _ in range(a.steps):
+        g = eng.pool_gradients(amps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    launches = (launch_count() - l0) // a.steps
+    # plain per-call path (measure_gradient3, call for call) on a sample of operators
+    drv = ADAPTVQE(mol, engine="percall")
+    drv._pool_obj = pool
+    drv._tops, drv._tamps = tops, list(amps)
+    # the sample: the 20 largest gradients and 20 operators drawn at random
+    top = [int(v) for v in np.argsort(-np.abs(g))[:20]]
+    rest = [int(v) for v in rng.choice(len(pool), 40, replace=False) if int(v) not in top]
+    idx = top + rest[:20]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    qc_psi = qb.Computer(2 * norb)
+    qc_psi.apply_circuit(drv.build_Uvqc())
+    qc_sig = qb.Computer(qc_psi)
+    qc_sig.apply_operator(mol.hamiltonian)
+    torch.cuda.synchronize()
+    t_state = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    g_plain = []
+    for k in idx:
+        coeff, operator = pool[k]
+        qc_temp = qb.Computer(qc_psi)
+        op = qb.SQOperator()
+        op.add_op(operator)
+        K = op.jw_transform()
+        K.mult_coeffs(coeff)
+        qc_temp.apply_operator(K)
+        g_plain.append(2.0 * np.real(np.vdot(qc_sig.get_coeff_vec(), qc_temp.get_coeff_vec())))
+    t_ops = (time.perf_counter() - t1) / len(idx)
+    plain_s = t_state + t_ops * len(pool)
+    err = float(np.max(np.abs(np.array(g_plain) - g[idx])))
+    line = {"metric": "ADAPT pool gradients per second", "value": len(pool) / (ms * 1e-3),
+            "unit": "gradients/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic",
+            "config": {"workload": f"GSD pool gradients, {2 * norb} qubits ({norb} orbitals, "
+                                   f"{norb} electrons), 12-operator dUCC state",
+                       "pool_ops": len(pool), "pool_strings": int(eng._pool_sum.nterms),
+                       "hamiltonian_terms": len(mol.hamiltonian)},
+            "gpu_launches": launches, "pool_compile_s": compile_s,
+            "max_abs_gradient": float(np.max(np.abs(g))),
+            "gradients_above_1e-10": int(np.sum(np.abs(g) > 1e-10)),
+            "plain_per_call": {"seconds": plain_s, "unit": "s per full pool",
+                               "sample": f"state + H psi once, then {len(idx)} of {len(pool)} "
+                                         "operators (the 20 largest gradients and 20 at random) "
+                                         "through Computer copies, apply_operator and "
+                                         "get_coeff_vec, scaled",
+                               "max_abs_diff_vs_batched": err},
+            "batched_vs_plain": plain_s / (ms * 1e-3)}
+    print(json.dumps(line))
+    return line
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -292,6 +438,14 @@ def main():
     if a.workload == "gates":
         if rank == 0:
             run_gates(a, rank, world, local)
+        return
+    if a.workload == "grad":
+        if rank == 0:
+            run_grad(a, local)
+        return
+    if a.workload == "adapt":
+        if rank == 0:
+            run_adapt(a, local)
         return
 
     import torch
@@ -376,6 +530,31 @@ def main():
     # the numbers coming back are the evaluator's
     assert np.all(np.isfinite(hE.numpy())) and np.all(np.isfinite(hG.numpy()))
 
+    # ---- the plain per-call GPU path: the reference's drivers call for call --
+    plain = None
+    if rank == 0 and not a.no_cpu_baseline:
+        import time
+        from qforte_b200.ucc import UCCNVQE
+        drv = UCCNVQE(mol, engine="percall")
+        drv._pool_obj = pool
+        drv._tops, drv._tamps = tops, list(P[0])
+        drv.energy_feval(P[0])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        E_p = drv.energy_feval(P[0])
+        g_p = drv.measure_gradient(P[0])
+        torch.cuda.synchronize()
+        t_p = time.perf_counter() - t0
+        e_b, g_b = ev.eval(P, True)
+        plain = {"value": 1.0 / t_p, "unit": UNIT,
+                 "sample": "one energy + gradient of parameter row 0 through the Computer API "
+                           "call for call (UCCNVQE engine='percall': the ansatz circuit built and "
+                           "applied, direct_op_exp_val, then the reverse sweep of "
+                           "measure_gradient with Computer copies, apply_operator and "
+                           "get_coeff_vec readbacks)",
+                 "energy_abs_diff": abs(E_p - float(e_b[0])),
+                 "gradient_max_abs_diff": float(np.max(np.abs(np.asarray(g_p) - g_b[0])))}
+
     # ---- roofline of the dominant kernel -------------------------------------
     import ctypes
     st_ms = (ctypes.c_double * 4)()
@@ -396,7 +575,8 @@ def main():
     avg_ms = st_ms[dom] / nl
     hbm, src = peaks()
     achieved = per_launch_bytes[dom] / (avg_ms / 1000.0) / 1e9
-    kernel = {1: "k_window<1>", 2: "k_sum_apply_tiled", 3: "k_window<2>"}[dom]
+    kernel = {1: "k_window<1>", 2: "k_sum_apply_sector" if ev.sector_size else "k_sum_apply_tiled",
+              3: "k_window<2>"}[dom]
     roof = {"bound": "hbm", "kernel": kernel, "stage": stages[dom], "achieved": achieved,
             "peak": hbm, "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
             "traffic": None, "algorithmic_bytes_per_launch": per_launch_bytes[dom],
@@ -411,6 +591,9 @@ def main():
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(P.nbytes),
                     "d2h_bytes_per_step": int(hE.numel() * 8 + hG.numel() * 8)},
             "roofline": roof, "gpu_launches": int(launches), "clocks": ck}
+    if plain is not None:
+        line["plain_per_call"] = plain
+        line["batched_vs_plain"] = value / plain["value"]
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             cb = cpu_baseline(a, mol, pool, P[0])

@@ -208,9 +208,13 @@ QFB_API int qfb_ucc_sector(qfb_ucc u, int64_t *nsec);
 /* Device addresses of the parameter block and the outputs. */
 QFB_API int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_grad);
 /* Enqueue one evaluation on the calling thread's stream (replays the
- * captured graph when one exists for this with_grad). */
+ * captured graph when one exists for this mode).  with_grad: 0 energy only;
+ * 1 energy and gradient; 2 the gradient sweep alone, on the psi and sigma a
+ * preceding with_grad = 0 run left (the sweep un-rotates them in place, so a
+ * second mode-2 run needs a new mode-0 run first). */
 QFB_API int qfb_ucc_run(qfb_ucc u, int with_grad);
-/* Capture one evaluation into a CUDA graph (replayed by later runs). */
+/* Capture one evaluation of the given mode into a CUDA graph (replayed by
+ * later runs). */
 QFB_API int qfb_ucc_capture(qfb_ucc u, int with_grad);
 /* Host convenience: params in, energies (and gradients) out, synchronous. */
 QFB_API int qfb_ucc_eval(qfb_ucc u, const double *params, double *energy, double *grad);

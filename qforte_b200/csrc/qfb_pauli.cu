@@ -428,6 +428,77 @@ __global__ void __launch_bounds__(256) k_sum_apply_sector(
     if (live) dst[(uint64_t)s * nbasis + (uint64_t)k] = acc;
 }
 
+// The same for small batches: one thread per output index k of the sector and
+// NS states per thread, so a warp's lanes are 32 different outputs (each
+// lane skips the groups that do not connect its k inside the sector).
+template <typename IDX, int NS>
+__global__ void __launch_bounds__(256) k_sum_apply_sector_k(
+    double2 *__restrict__ dst, const double2 *__restrict__ src, uint64_t nbasis, int nbatch,
+    const IDX *__restrict__ sec, int64_t nsec, const SecGroup *__restrict__ groups, int ngroups,
+    const TermDev *__restrict__ terms, const double2 *__restrict__ rterms) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsec) return;
+    const int s0 = blockIdx.y * NS;
+    const IDX k = sec[i];
+    const IDX A = (IDX)0x5555555555555555ull;
+    double2 acc[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) acc[s] = make_double2(0.0, 0.0);
+    for (int g = 0; g < ngroups; ++g) {
+        const IDX x = (IDX)__ldg(&groups[g].x);
+        const IDX kx = k & x;
+        if ((popc_t<IDX>(kx & A) | popc_t<IDX>(kx & ~A) << 8) != __ldg(&groups[g].halves)) continue;
+        const IDX j = k ^ x;
+        const int t0 = __ldg(&groups[g].begin), t1 = __ldg(&groups[g].end);
+        double2 f = make_double2(0.0, 0.0);
+        if (__ldg(&groups[g].real)) {
+            for (int t = t0; t < t1; ++t) {
+                const double2 zc = __ldg(&rterms[t]);
+                const IDX z = (IDX)__double_as_longlong(zc.x);
+                f.x += (popc_t<IDX>(j & z) & 1) ? -zc.y : zc.y;
+            }
+        } else {
+            for (int t = t0; t < t1; ++t) {
+                const double2 c = terms[t].c;
+                if (parity64((uint64_t)j & __ldg(&terms[t].z))) { f.x -= c.x; f.y -= c.y; }
+                else { f.x += c.x; f.y += c.y; }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            if (s0 + s < nbatch) {
+                const double2 v = __ldg(&src[(uint64_t)(s0 + s) * nbasis + j]);
+                acc[s] = c_add(acc[s], c_mul(f, v));
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+        if (s0 + s < nbatch) dst[(uint64_t)(s0 + s) * nbasis + (uint64_t)k] = acc[s];
+}
+
+template <typename IDX>
+static void launch_sector_apply(double2 *dst, const double2 *src, uint64_t nbasis, int B,
+                                const IDX *sec, int64_t nsec, const SecGroup *groups, int ngroups,
+                                const TermDev *terms, const double2 *rterms) {
+    if (B >= 24) {
+        const dim3 grid((unsigned)((nsec + 7) / 8), (unsigned)((B + 31) / 32));
+        k_sum_apply_sector<IDX><<<grid, 256, 0, t_stream>>>(dst, src, nbasis, B, sec, nsec, groups,
+                                                           ngroups, terms, rterms);
+        return;
+    }
+    const unsigned gx = (unsigned)((nsec + 255) / 256);
+#define QFB_SECTOR_K(NS)                                                                        \
+    k_sum_apply_sector_k<IDX, NS><<<dim3(gx, (unsigned)((B + NS - 1) / NS)), 256, 0, t_stream>>>( \
+        dst, src, nbasis, B, sec, nsec, groups, ngroups, terms, rterms)
+    if (B == 1) QFB_SECTOR_K(1);
+    else if (B == 2) QFB_SECTOR_K(2);
+    else if (B <= 4) QFB_SECTOR_K(4);
+    else if (B <= 8) QFB_SECTOR_K(8);
+    else QFB_SECTOR_K(12);
+#undef QFB_SECTOR_K
+}
+
 // ---------------------------------------------------------------------------
 // programs
 // ---------------------------------------------------------------------------
@@ -2007,8 +2078,8 @@ struct qfb_ucc_s {
     double2 *vpart = nullptr, *gpart = nullptr;
     int2 *psteps = nullptr;
     cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
-    uint64_t graph_kernels[2] = {0, 0};
+    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};  // by run mode
+    uint64_t graph_kernels[3] = {0, 0, 0};
     // particle-number sector of the state (every program conserves it):
     // H psi is formed on these indices only; nsec == 0 means the full space
     int64_t nsec = 0;
@@ -2032,15 +2103,14 @@ static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
         case 2:
             if (u->nsec > 0) {
                 QFB_CUDA(cudaMemsetAsync(u->sig, 0, sizeof(double2) * u->nbasis * B, t_stream));
-                const dim3 grid((unsigned)((u->nsec + 7) / 8), (unsigned)((B + 31) / 32));
                 if (u->nqubit <= 32)
-                    k_sum_apply_sector<uint32_t><<<grid, 256, 0, t_stream>>>(
-                        u->sig, u->psi, u->nbasis, B, (const uint32_t *)u->sec, u->nsec,
-                        u->sgroups, u->nsgroups, u->ham->d_terms, u->ham->d_rterms);
+                    launch_sector_apply(u->sig, u->psi, u->nbasis, B, (const uint32_t *)u->sec,
+                                        u->nsec, u->sgroups, u->nsgroups, u->ham->d_terms,
+                                        u->ham->d_rterms);
                 else
-                    k_sum_apply_sector<uint64_t><<<grid, 256, 0, t_stream>>>(
-                        u->sig, u->psi, u->nbasis, B, (const uint64_t *)u->sec, u->nsec,
-                        u->sgroups, u->nsgroups, u->ham->d_terms, u->ham->d_rterms);
+                    launch_sector_apply(u->sig, u->psi, u->nbasis, B, (const uint64_t *)u->sec,
+                                        u->nsec, u->sgroups, u->nsgroups, u->ham->d_terms,
+                                        u->ham->d_rterms);
                 QFB_LAUNCHED();
             } else {
                 rc = enqueue_sum_apply(u->ham, u->sig, u->psi, u->nbasis, B);
@@ -2066,9 +2136,11 @@ static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
     return rc;
 }
 
-static int ucc_enqueue(qfb_ucc u, int with_grad) {
-    for (int st = 0; st < 4; ++st) {
-        int rc = ucc_stage(u, st, with_grad);
+// mode 0: energy (stages 0-2); 1: energy and gradient (0-3); 2: the gradient
+// sweep alone (stage 3) on psi and sigma as a mode-0 run left them.
+static int ucc_enqueue(qfb_ucc u, int mode) {
+    for (int st = (mode == 2 ? 3 : 0); st < 4; ++st) {
+        int rc = ucc_stage(u, st, mode != 0);
         if (rc) return rc;
     }
     return QFB_OK;
@@ -2218,7 +2290,8 @@ int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_
 
 int qfb_ucc_run(qfb_ucc u, int with_grad) {
     if (!u) return fail(QFB_EINVAL, "qfb_ucc_run: null evaluator");
-    const int k = with_grad ? 1 : 0;
+    if (with_grad < 0 || with_grad > 2) return fail(QFB_EINVAL, "qfb_ucc_run: mode %d", with_grad);
+    const int k = with_grad;
     if (u->exec[k]) {
         QFB_CUDA(cudaGraphLaunch(u->exec[k], t_stream));
         g_launches.fetch_add(u->graph_kernels[k], std::memory_order_relaxed);
@@ -2229,7 +2302,9 @@ int qfb_ucc_run(qfb_ucc u, int with_grad) {
 
 int qfb_ucc_capture(qfb_ucc u, int with_grad) {
     if (!u) return fail(QFB_EINVAL, "qfb_ucc_capture: null evaluator");
-    const int k = with_grad ? 1 : 0;
+    if (with_grad < 0 || with_grad > 2)
+        return fail(QFB_EINVAL, "qfb_ucc_capture: mode %d", with_grad);
+    const int k = with_grad;
     if (u->exec[k]) return QFB_OK;
     cudaStream_t saved = t_stream;
     t_stream = u->cap_stream;

@@ -60,6 +60,7 @@ class Evaluator:
         self.d_params, self.d_energy, self.d_grad = dp.value, de.value, dg.value
         self.capture = capture
         self._captured = set()
+        self.generation = 0  # bumped whenever a run overwrites psi and sigma
 
     @property
     def sector_size(self):
@@ -83,13 +84,18 @@ class Evaluator:
         g = np.empty((self.nbatch, self.nparam)) if with_grad else None
         check(lib().qfb_ucc_eval(self.h, ptr(P), ptr(e), None if g is None else ptr(g)),
               "qfb_ucc_eval")
+        self.generation += 1
         return e, g
 
     def run(self, with_grad=True):
-        """Enqueue one evaluation on the current stream (device buffers in and
-        out, no host synchronisation)."""
-        self._ensure_graph(with_grad)
-        check(lib().qfb_ucc_run(self.h, int(with_grad)), "qfb_ucc_run")
+        """Enqueue one evaluation on the library's stream (device buffers in and
+        out, no host synchronisation).  ``with_grad`` 0/False: energies; 1/True:
+        energies and gradients; 2: the gradient sweep alone on the states the
+        last energy-only run left."""
+        mode = int(with_grad)
+        self._ensure_graph(mode)
+        check(lib().qfb_ucc_run(self.h, mode), "qfb_ucc_run")
+        self.generation += 1
 
     def tensors(self):
         """(params, energy, grad) as torch float64 CUDA views of the device blocks."""

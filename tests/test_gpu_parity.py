@@ -357,3 +357,21 @@ def test_layered_sweep_circuit_matches_oracle(cuda, gate_tiles, n):
         qc = qb.Computer(n)
         qc.apply_circuit(circ)
         assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
+
+
+@pytest.mark.parametrize("B", [3, 9, 13, 40])
+def test_sector_apply_every_batch_width(cuda, B):
+    """Small batches take the one-output-per-thread sector kernel, large ones
+    the one-output-per-warp kernel; each row equals its single-row result."""
+    mol, pool = random_problem(5, 23)
+    tops = list(range(len(pool)))
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+    rng = np.random.default_rng(B)
+    P = rng.uniform(-0.1, 0.1, (B, len(tops)))
+    EB, GB = eng.energy_grad(P)
+    for b in (0, B // 2, B - 1):
+        e1, g1 = eng.energy_grad(P[b])
+        assert abs(EB[b] - e1) < 1e-12 and np.max(np.abs(GB[b] - g1)) < 1e-12
+    hterms = oracle_terms(mol.hamiltonian)
+    E_o, _ = O.energy(10, mol.hf_reference, kops_forward(pool, tops), P[B - 1], hterms)
+    assert abs(EB[B - 1] - E_o) < E_TOL
