@@ -48,11 +48,16 @@ def parse():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="ucc", choices=["ucc", "gates", "grad", "adapt"],
+    ap.add_argument("--workload", default="ucc",
+                    choices=["ucc", "gates", "grad", "adapt", "serve"],
                     help="ucc: batched dUCCSD energy+gradient (default); gates: the gate sweep; "
                          "grad: differentiable energy, forward+backward against forward alone; "
                          "adapt: every ADAPT pool gradient of a 12-operator state in one launch")
     ap.add_argument("--adapt-norb", type=int, default=10, help="adapt workload: orbitals")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: mean requests per second")
+    ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
+    ap.add_argument("--norb-range", default="5,13", help="serve: orbital counts lo,hi")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM budget")
     ap.add_argument("--norbs", default="8,10", help="grad workload: orbital counts")
     ap.add_argument("--nqubits", default="20,24,28",
                     help="gate sweep: comma-separated qubit counts")
@@ -427,6 +432,89 @@ def run_adapt(a, local):
     return line
 
 
+def serve_trace(a, problems):
+    """Poisson arrivals over ``duration`` seconds: (t, key, params, with_grad)."""
+    rng = np.random.default_rng(a.seed + 99)
+    keys = sorted(problems)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / a.rate)
+        if t > a.duration:
+            return out
+        k = keys[rng.integers(len(keys))]
+        out.append((t, k, rng.uniform(-0.1, 0.1, problems[k].nparam), bool(rng.integers(2))))
+
+
+def replay(server, trace):
+    """Submit the trace at its arrival times (open loop); wait for every result."""
+    import time
+    t0 = time.perf_counter()
+    futs = []
+    for t, k, p, wg in trace:
+        dt = t - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        futs.append((k, server.submit(k, p, wg), time.perf_counter()))
+    res = [(k, f.result(), ts) for k, f, ts in futs]
+    return res, time.perf_counter() - t0
+
+
+def run_serve(a, local):
+    """Serving: Poisson stream of mixed energy / energy+gradient requests of
+    random-integral dUCCSD problems, orbital counts U{lo..hi}, half filling."""
+    import torch
+    import qforte_b200 as qb
+    from qforte_b200.serving import Server
+    from qforte_b200.ucc import DUCC
+    torch.cuda.set_device(local)
+    lo, hi = (int(v) for v in a.norb_range.split(","))
+    problems = {}
+    for norb in range(lo, hi + 1):
+        mol, pool = problem(norb, a.seed + norb)
+        problems[f"norb{norb}"] = DUCC(mol.hamiltonian, pool, list(range(len(pool))),
+                                       mol.hf_reference)
+    trace = serve_trace(a, problems)
+    budget = a.budget_gb * 1e9
+
+    def served(max_batch, streams, tr):
+        srv = Server(hbm_budget=budget, max_batch=max_batch, streams=streams, device=local)
+        for k, d in problems.items():
+            srv.register(k, d)
+        with srv:
+            # warm: one request of each problem and kind (captures the graphs)
+            for k, d in problems.items():
+                for wg in (False, True):
+                    srv.submit(k, np.zeros(d.nparam), wg).result()
+            srv.reset_stats()
+            res, wall = replay(srv, tr)
+            st = srv.stats()
+        return st, res, wall
+
+    st, res, wall = served(256, 4, trace)
+    by = {}
+    for k, (e, g), ts in res:
+        by.setdefault(k, 0)
+        by[k] += 1
+    # sequential baseline: the same requests one at a time (batch 1, one stream)
+    nseq = min(len(trace), max(8, len(trace) // 4))
+    st1, _, wall1 = served(1, 1, trace[:nseq])
+    line = {"metric": "served dUCC requests/s", "value": len(res) / wall, "unit": "requests/s",
+            "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": 1000.0 * wall,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic",
+            "config": {"workload": f"Poisson arrivals at {a.rate}/s for {a.duration} s, "
+                                   f"dUCCSD problems of {lo}..{hi} orbitals (half filling, SD "
+                                   "pool), half energy and half energy+gradient requests",
+                       "requests": len(trace), "per_problem": by, "hbm_budget_gb": a.budget_gb},
+            "latency_ms": st.get("latency_ms"), "server": st,
+            "sequential": {"requests": nseq, "requests_per_s": nseq / wall1,
+                           "latency_ms": st1.get("latency_ms"),
+                           "sample": "the first requests of the same trace served one at a time "
+                                     "(batch 1, one stream, same evaluator kernels)"}}
+    print(json.dumps(line))
+    return line
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -446,6 +534,10 @@ def main():
     if a.workload == "adapt":
         if rank == 0:
             run_adapt(a, local)
+        return
+    if a.workload == "serve":
+        if rank == 0:
+            run_serve(a, local)
         return
 
     import torch

@@ -205,6 +205,10 @@ QFB_API int qfb_ucc_destroy(qfb_ucc u);
  * Computer::apply_operator (computer.cc:80-91) always runs over all 2^n
  * amplitudes. */
 QFB_API int qfb_ucc_sector(qfb_ucc u, int64_t *nsec);
+/* Device bytes the evaluator holds (states, parameter and output blocks,
+ * scratch); a request loop admits work against its HBM budget with this.  No
+ * counterpart in the reference. */
+QFB_API int qfb_ucc_memory(qfb_ucc u, uint64_t *bytes);
 /* Device addresses of the parameter block and the outputs. */
 QFB_API int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_grad);
 /* Enqueue one evaluation on the calling thread's stream (replays the

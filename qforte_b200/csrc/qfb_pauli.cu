@@ -2083,6 +2083,7 @@ struct qfb_ucc_s {
     // particle-number sector of the state (every program conserves it):
     // H psi is formed on these indices only; nsec == 0 means the full space
     int64_t nsec = 0;
+    size_t bytes = 0;     // device bytes held (blob)
     void *sec = nullptr;  // uint32_t (nqubit <= 32) or uint64_t indices
     SecGroup *sgroups = nullptr;
     int nsgroups = 0;
@@ -2224,6 +2225,7 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
         delete u;
         return rc;
     }
+    u->bytes = off;
     char *base = (char *)u->blob;
     u->psi = (double2 *)(base + o_psi);
     u->sig = (double2 *)(base + o_sig);
@@ -2277,6 +2279,12 @@ int qfb_ucc_destroy(qfb_ucc u) {
     if (u->cap_stream) cudaStreamDestroy(u->cap_stream);
     dev_free(u->blob);
     delete u;
+    return QFB_OK;
+}
+
+int qfb_ucc_memory(qfb_ucc u, uint64_t *bytes) {
+    if (!u || !bytes) return fail(QFB_EINVAL, "qfb_ucc_memory: null argument");
+    *bytes = u->bytes;
     return QFB_OK;
 }
 

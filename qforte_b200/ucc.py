@@ -63,6 +63,13 @@ class Evaluator:
         self.generation = 0  # bumped whenever a run overwrites psi and sigma
 
     @property
+    def device_bytes(self):
+        """Device memory this evaluator holds."""
+        n = ctypes.c_uint64()
+        check(lib().qfb_ucc_memory(self.h, ctypes.byref(n)), "qfb_ucc_memory")
+        return n.value
+
+    @property
     def sector_size(self):
         """Indices of the particle-number sector H psi is formed on (0: all)."""
         n = ctypes.c_int64()
