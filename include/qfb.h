@@ -205,6 +205,14 @@ QFB_API int qfb_ucc_destroy(qfb_ucc u);
  * Computer::apply_operator (computer.cc:80-91) always runs over all 2^n
  * amplitudes. */
 QFB_API int qfb_ucc_sector(qfb_ucc u, int64_t *nsec);
+/* How the evaluator runs: 0 full space; 1 full-space states with sigma formed
+ * on the sector; 2 compact sector states, one CTA per parameter set holding
+ * psi and sigma in shared memory (sectors up to 6,400 amplitudes whose
+ * program steps are all in Givens form).  No counterpart in the reference. */
+QFB_API int qfb_ucc_path(qfb_ucc u, int32_t *path);
+/* Process-wide: whether evaluators created from now on may use the compact
+ * sector path (1, the default) or not (0).  No counterpart in the reference. */
+QFB_API int qfb_ucc_config(int compact);
 /* Device bytes the evaluator holds (states, parameter and output blocks,
  * scratch); a request loop admits work against its HBM budget with this.  No
  * counterpart in the reference. */

@@ -35,11 +35,14 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
 #include "qfb_common.cuh"
+#include "qfb_sector.cuh"
 #include "qfb_window.cuh"
 
 using namespace qfb;
@@ -2064,6 +2067,206 @@ static std::vector<uint64_t> sector_indices(int n, uint64_t ref) {
     return sec;
 }
 
+// ---------------------------------------------------------------------------
+// compact sector evaluator (qfb_sector.cuh): host plan
+// ---------------------------------------------------------------------------
+
+constexpr size_t kSectorSmemMax = 200 * 1024;  // psi + sigma of one parameter set
+constexpr int kSectorThreads = 512;
+static int g_ucc_compact = 1;  // process-wide: use the compact evaluator when it applies
+
+// Rows of H on the compact sector: row i (the sector index of det[i]) holds,
+// for every group x connecting det[i] to j = det[i] ^ x inside the sector,
+// the column of j and f_x(j) = sum_t c_t (-1)^popcount(j & z_t).  Pass 1
+// (col == nullptr) counts the entries of each row.
+__global__ void k_sector_rows(const uint64_t *__restrict__ det, int nsec,
+                              const SecGroup *__restrict__ groups, int ngroups,
+                              const TermDev *__restrict__ terms, const double2 *__restrict__ rterms,
+                              const int32_t *__restrict__ arank, const int32_t *__restrict__ brank,
+                              int nbeta, int nqubit, const int32_t *__restrict__ rowptr,
+                              int32_t *__restrict__ count, uint32_t *__restrict__ col,
+                              double *__restrict__ val_r, double2 *__restrict__ val_c) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsec) return;
+    const uint64_t k = det[i];
+    const uint64_t A = 0x5555555555555555ull;
+    int e = rowptr ? rowptr[i] : 0, c = 0;
+    for (int g = 0; g < ngroups; ++g) {
+        const SecGroup gr = groups[g];
+        const uint64_t kx = k & gr.x;
+        if ((__popcll(kx & A) | __popcll(kx & ~A) << 8) != gr.halves) continue;
+        if (!col) {
+            ++c;
+            continue;
+        }
+        const uint64_t j = k ^ gr.x;
+        double2 f = make_double2(0.0, 0.0);
+        if (gr.real) {
+            for (int t = gr.begin; t < gr.end; ++t) {
+                const double2 zc = rterms[t];
+                f.x += parity64(j & (uint64_t)__double_as_longlong(zc.x)) ? -zc.y : zc.y;
+            }
+        } else {
+            for (int t = gr.begin; t < gr.end; ++t) {
+                const double2 cc = terms[t].c;
+                if (parity64(j & terms[t].z)) { f.x -= cc.x; f.y -= cc.y; }
+                else { f.x += cc.x; f.y += cc.y; }
+            }
+        }
+        uint32_t ca = 0, cb = 0;
+        for (int q = 0, ia = 0, ib = 0; q < nqubit; ++q) {
+            if (q & 1) cb |= (uint32_t)((j >> q) & 1ull) << ib++;
+            else ca |= (uint32_t)((j >> q) & 1ull) << ia++;
+        }
+        col[e] = (uint32_t)(arank[ca] * nbeta + brank[cb]);
+        if (val_c) val_c[e] = f;
+        else val_r[e] = f.x;
+        ++e;
+    }
+    if (!col) count[i] = c;
+}
+
+struct SectorPlan {
+    int na_orb = 0, nb_orb = 0, nalpha = 0, nbeta = 0, nsec = 0, ref_i = 0;
+    std::vector<uint64_t> adet, bdet;
+    std::vector<int32_t> arank, brank;
+    std::vector<qfbs::SEntry> ents;
+    std::vector<qfbs::SPat> pats;
+    std::vector<qfbs::SStep> steps;  // forward, then K, then U programs
+    int f0 = 0, nf = 0, k0 = 0, nk = 0, u0 = 0, nu = 0;
+    std::vector<int2> kmu, umu;
+    int fused = 0;
+    std::map<std::tuple<int, uint64_t, uint64_t, uint64_t, uint64_t>, int2> lists;
+};
+
+static uint32_t pext_parity_bits(uint64_t v, int odd, int n) {
+    uint32_t r = 0;
+    for (int q = odd, k = 0; q < n; q += 2, ++k) r |= (uint32_t)((v >> q) & 1ull) << k;
+    return r;
+}
+
+// Strings of one spin (odd = 0 alpha on even qubits, 1 beta on odd qubits)
+// whose bits on P equal want's, with their partner ranks and sign bits; the
+// list is shared by every step with the same key.  false: a partner leaves
+// the sector.
+static bool sector_list(SectorPlan &sp, int odd, int n, uint64_t P, uint64_t want, uint64_t x,
+                        uint64_t zb, int2 *out) {
+    const uint64_t M = odd ? 0xAAAAAAAAAAAAAAAAull : 0x5555555555555555ull;
+    const auto key = std::make_tuple(odd, P & M, want & P & M, x & M, zb & M);
+    auto it = sp.lists.find(key);
+    if (it != sp.lists.end()) {
+        *out = it->second;
+        return true;
+    }
+    const std::vector<uint64_t> &det = odd ? sp.bdet : sp.adet;
+    const std::vector<int32_t> &rank = odd ? sp.brank : sp.arank;
+    const int a0 = (int)sp.ents.size();
+    for (size_t r = 0; r < det.size(); ++r) {
+        if ((det[r] & P & M) != (want & P & M)) continue;
+        const uint64_t partner = det[r] ^ (x & M);
+        const int32_t pr = rank[pext_parity_bits(partner, odd, n)];
+        if (pr < 0) return false;
+        qfbs::SEntry e;
+        e.r0 = (uint16_t)r;
+        e.r1 = (uint16_t)pr;
+        e.s = (uint32_t)(__builtin_popcountll(det[r] & zb & M) & 1);
+        sp.ents.push_back(e);
+    }
+    *out = make_int2(a0, (int)sp.ents.size() - a0);
+    sp.lists[key] = *out;
+    return true;
+}
+
+static bool sector_steps(SectorPlan &sp, const qfb_prog_s *p, int n) {
+    for (const StepDev &st : p->h_steps) {
+        if (st.tab < 0 || st.na <= 0 || st.x == 0) return false;
+        uint64_t P = 1ull << st.h;
+        for (int i = 0; i < st.nd; ++i) P |= 1ull << ((st.dpos >> (6 * i)) & 63);
+        qfbs::SStep ss{};
+        ss.p0 = (int)sp.pats.size();
+        ss.param = st.param;
+        ss.gamma = st.gamma;
+        for (int a = 0; a < st.na; ++a) {
+            int2 la, lb;
+            if (!sector_list(sp, 0, n, P, st.patbits[a], st.x, st.zbase, &la)) return false;
+            if (!sector_list(sp, 1, n, P, st.patbits[a], st.x, st.zbase, &lb)) return false;
+            if (la.y == 0 || lb.y == 0) continue;
+            qfbs::SPat pt{};
+            pt.a0 = la.x;
+            pt.na = la.y;
+            pt.b0 = lb.x;
+            pt.nb = lb.y;
+            pt.gn = p->h_tab[st.tab + 2 * st.patidx[a]];
+            pt.hn = p->h_tab[st.tab + 2 * st.patidx[a] + 1];
+            sp.pats.push_back(pt);
+        }
+        ss.np = (int)sp.pats.size() - ss.p0;
+        sp.steps.push_back(ss);
+    }
+    return true;
+}
+
+// The compact plan of an evaluator, or false when it does not apply (a step
+// outside the Givens form, a sector too large for shared memory, ranks that
+// do not fit 16 bits).
+static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_prog_s *kp,
+                              const qfb_prog_s *up, int n, uint64_t ref) {
+    const uint64_t A = 0x5555555555555555ull;
+    const uint64_t all = (1ull << n) - 1ull;
+    sp.na_orb = (n + 1) / 2;
+    sp.nb_orb = n / 2;
+    if (sp.na_orb > 20) return false;
+    const int ka = __builtin_popcountll(ref & A & all), kb = __builtin_popcountll(ref & ~A & all);
+    auto strings = [&](int m, int k, int odd, std::vector<uint64_t> &det, std::vector<int32_t> &rank) {
+        rank.assign((size_t)1 << m, -1);
+        if (k > m) return;
+        uint64_t c = (k == 0) ? 0 : ((1ull << k) - 1ull);
+        while (true) {
+            uint64_t d = 0;
+            for (int b = 0; b < m; ++b)
+                if (c >> b & 1ull) d |= 1ull << (2 * b + odd);
+            rank[c] = (int32_t)det.size();
+            det.push_back(d);
+            if (k == 0) break;
+            const uint64_t t = c | (c - 1);
+            c = (t + 1) | (((~t & -~t) - 1) >> (__builtin_ctzll(c) + 1));
+            if (c >= (1ull << m)) break;
+        }
+    };
+    strings(sp.na_orb, ka, 0, sp.adet, sp.arank);
+    strings(sp.nb_orb, kb, 1, sp.bdet, sp.brank);
+    sp.nalpha = (int)sp.adet.size();
+    sp.nbeta = (int)sp.bdet.size();
+    if (sp.nalpha == 0 || sp.nbeta == 0 || sp.nalpha > 65535 || sp.nbeta > 65535) return false;
+    const size_t nsec = (size_t)sp.nalpha * sp.nbeta;
+    if (nsec * 2 * sizeof(double2) > kSectorSmemMax) return false;
+    sp.nsec = (int)nsec;
+    sp.ref_i = sp.arank[pext_parity_bits(ref, 0, n)] * sp.nbeta + sp.brank[pext_parity_bits(ref, 1, n)];
+    sp.f0 = 0;
+    if (!sector_steps(sp, fp, n)) return false;
+    sp.nf = (int)sp.steps.size();
+    sp.k0 = (int)sp.steps.size();
+    if (kp) {
+        if (!sector_steps(sp, kp, n)) return false;
+        sp.nk = (int)sp.steps.size() - sp.k0;
+        sp.u0 = (int)sp.steps.size();
+        if (!sector_steps(sp, up, n)) return false;
+        sp.nu = (int)sp.steps.size() - sp.u0;
+        const int M = kp->nparam;
+        sp.kmu.resize(M);
+        sp.umu.resize(M);
+        sp.fused = (kp == up) ? 1 : 0;
+        for (int mu = 0; mu < M; ++mu) {
+            const int s0 = kp->p_step0[mu], s1 = kp->p_step1[mu];
+            sp.kmu[mu] = (s0 >= 0) ? make_int2(s0, s1) : make_int2(0, 0);
+            const int t0 = up->p_step0[mu], t1 = up->p_step1[mu];
+            sp.umu[mu] = (t0 >= 0) ? make_int2(t0, t1) : make_int2(0, 0);
+            if (s0 < 0 || s1 - s0 != 1) sp.fused = 0;
+        }
+    }
+    return true;
+}
+
 struct qfb_ucc_s {
     qfb_prog_s *fwd = nullptr;
     qfb_prog_s *grad = nullptr;   // K_mu (inner products)
@@ -2083,13 +2286,157 @@ struct qfb_ucc_s {
     // particle-number sector of the state (every program conserves it):
     // H psi is formed on these indices only; nsec == 0 means the full space
     int64_t nsec = 0;
-    size_t bytes = 0;     // device bytes held (blob)
+    size_t bytes = 0;     // device bytes held (blobs)
+    int compact = 0;      // compact sector evaluator (qfb_sector.cuh)
+    void *sblob = nullptr, *csr = nullptr;
+    qfbs::SLaunch SL{};
     void *sec = nullptr;  // uint32_t (nqubit <= 32) or uint64_t indices
     SecGroup *sgroups = nullptr;
     int nsgroups = 0;
 };
 
+// Device copies of a compact plan and the H rows on its sector.
+static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> &sg) {
+    const int nsec = sp.nsec;
+    std::vector<uint64_t> det((size_t)nsec);
+    for (int ra = 0; ra < sp.nalpha; ++ra)
+        for (int rb = 0; rb < sp.nbeta; ++rb) det[(size_t)ra * sp.nbeta + rb] = sp.adet[ra] | sp.bdet[rb];
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_st = take(sizeof(qfbs::SStep) * sp.steps.size());
+    const size_t o_pt = take(sizeof(qfbs::SPat) * sp.pats.size());
+    const size_t o_en = take(sizeof(qfbs::SEntry) * sp.ents.size());
+    const size_t o_km = take(sizeof(int2) * sp.kmu.size());
+    const size_t o_um = take(sizeof(int2) * sp.umu.size());
+    const size_t o_det = take(sizeof(uint64_t) * det.size());
+    const size_t o_ar = take(sizeof(int32_t) * sp.arank.size());
+    const size_t o_br = take(sizeof(int32_t) * sp.brank.size());
+    const size_t o_g = take(sizeof(SecGroup) * sg.size());
+    const size_t o_cnt = take(sizeof(int32_t) * (size_t)(nsec + 1));
+    int rc = dev_alloc(&u->sblob, off);
+    if (rc) return rc;
+    u->bytes += off;
+    char *base = (char *)u->sblob;
+    struct Up { size_t o; const void *p; size_t n; };
+    const Up ups[] = {{o_st, sp.steps.data(), sizeof(qfbs::SStep) * sp.steps.size()},
+                      {o_pt, sp.pats.data(), sizeof(qfbs::SPat) * sp.pats.size()},
+                      {o_en, sp.ents.data(), sizeof(qfbs::SEntry) * sp.ents.size()},
+                      {o_km, sp.kmu.data(), sizeof(int2) * sp.kmu.size()},
+                      {o_um, sp.umu.data(), sizeof(int2) * sp.umu.size()},
+                      {o_det, det.data(), sizeof(uint64_t) * det.size()},
+                      {o_ar, sp.arank.data(), sizeof(int32_t) * sp.arank.size()},
+                      {o_br, sp.brank.data(), sizeof(int32_t) * sp.brank.size()},
+                      {o_g, sg.data(), sizeof(SecGroup) * sg.size()}};
+    for (const Up &x : ups)
+        if (x.n) QFB_CUDA(cudaMemcpyAsync(base + x.o, x.p, x.n, cudaMemcpyHostToDevice, t_stream));
+    int32_t *d_cnt = (int32_t *)(base + o_cnt);
+    const SecGroup *d_g = (const SecGroup *)(base + o_g);
+    const uint64_t *d_det = (const uint64_t *)(base + o_det);
+    const int32_t *d_ar = (const int32_t *)(base + o_ar), *d_br = (const int32_t *)(base + o_br);
+    const unsigned nb = (unsigned)((nsec + 127) / 128);
+    k_sector_rows<<<nb, 128, 0, t_stream>>>(d_det, nsec, d_g, (int)sg.size(), u->ham->d_terms,
+                                            u->ham->d_rterms, d_ar, d_br, sp.nbeta, u->nqubit,
+                                            nullptr, d_cnt, nullptr, nullptr, nullptr);
+    QFB_LAUNCHED();
+    std::vector<int32_t> cnt((size_t)nsec);
+    QFB_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int32_t) * nsec, cudaMemcpyDeviceToHost,
+                             t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    std::vector<int32_t> rowptr((size_t)nsec + 1, 0);
+    int64_t nnz = 0;
+    for (int i = 0; i < nsec; ++i) {
+        rowptr[i] = (int32_t)nnz;
+        nnz += cnt[i];
+        if (nnz >= ((int64_t)1 << 31)) return fail(QFB_ENOMEM, "sector H rows: too many entries");
+    }
+    rowptr[nsec] = (int32_t)nnz;
+    bool real = true;
+    for (const SecGroup &g : sg) real = real && g.real;
+    const size_t o_rp = 0;
+    size_t coff = ((sizeof(int32_t) * (nsec + 1)) + 255) & ~(size_t)255;
+    const size_t o_col = coff;
+    coff += ((sizeof(uint32_t) * std::max<int64_t>(nnz, 1)) + 255) & ~(size_t)255;
+    const size_t o_val = coff;
+    coff += (real ? sizeof(double) : sizeof(double2)) * std::max<int64_t>(nnz, 1);
+    rc = dev_alloc(&u->csr, coff);
+    if (rc) return rc;
+    u->bytes += coff;
+    char *cb = (char *)u->csr;
+    QFB_CUDA(cudaMemcpyAsync(cb + o_rp, rowptr.data(), sizeof(int32_t) * (nsec + 1),
+                             cudaMemcpyHostToDevice, t_stream));
+    int32_t *d_rp = (int32_t *)(cb + o_rp);
+    uint32_t *d_col = (uint32_t *)(cb + o_col);
+    double *d_vr = real ? (double *)(cb + o_val) : nullptr;
+    double2 *d_vc = real ? nullptr : (double2 *)(cb + o_val);
+    k_sector_rows<<<nb, 128, 0, t_stream>>>(d_det, nsec, d_g, (int)sg.size(), u->ham->d_terms,
+                                            u->ham->d_rterms, d_ar, d_br, sp.nbeta, u->nqubit, d_rp,
+                                            nullptr, d_col, d_vr, d_vc);
+    QFB_LAUNCHED();
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    qfbs::SLaunch &L = u->SL;
+    L.nsec = nsec;
+    L.nbeta = sp.nbeta;
+    L.ref_i = sp.ref_i;
+    L.nparam = u->nparam;
+    L.nf = sp.nf;
+    L.fused = sp.fused;
+    L.nmu = sp.kmu.empty() ? 0 : (int)sp.kmu.size();
+    const qfbs::SStep *d_st = (const qfbs::SStep *)(base + o_st);
+    L.fsteps = d_st + sp.f0;
+    L.ksteps = d_st + sp.k0;
+    L.usteps = d_st + sp.u0;
+    L.kmu = (const int2 *)(base + o_km);
+    L.umu = (const int2 *)(base + o_um);
+    L.pats = (const qfbs::SPat *)(base + o_pt);
+    L.ents = (const qfbs::SEntry *)(base + o_en);
+    L.rowptr = d_rp;
+    L.col = d_col;
+    L.val_r = d_vr;
+    L.val_c = d_vc;
+    L.params = u->params;
+    L.energy = u->energy;
+    L.partial = u->gpart;
+    return QFB_OK;
+}
+
+static int sector_smem_attr() {
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        err = cudaFuncSetAttribute(qfbs::k_sector_eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kSectorSmemMax);
+    });
+    return err == cudaSuccess ? QFB_OK : cuda_fail(err, "sector evaluator shared memory");
+}
+
+// Compact evaluator: stage 2 runs the forward program, H psi and the energy
+// (saving psi and sigma), stage 3 the reverse sweep from the saved states.
+static int ucc_stage_compact(qfb_ucc u, int stage, int with_grad) {
+    if (stage < 2) return QFB_OK;
+    qfbs::SLaunch L = u->SL;
+    const size_t smem = sizeof(double2) * 2 * (size_t)L.nsec;
+    if (stage == 2) {
+        L.mode = 1 | 4;
+    } else {
+        if (!(with_grad && u->grad && u->nparam > 0)) return QFB_OK;
+        L.mode = 2;
+    }
+    qfbs::k_sector_eval<<<u->nbatch, kSectorThreads, smem, t_stream>>>(L);
+    QFB_LAUNCHED();
+    if (stage == 3) {
+        k_grad_final<<<dim3(u->nparam, u->nbatch), 128, 0, t_stream>>>(u->gpart, u->psteps,
+                                                                     u->gchunks, u->gradv);
+        QFB_LAUNCHED();
+    }
+    return QFB_OK;
+}
+
 static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
+    if (u->compact) return ucc_stage_compact(u, stage, with_grad);
     const int B = u->nbatch;
     int rc = QFB_OK;
     switch (stage) {
@@ -2189,7 +2536,16 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
         }
         if (sgroups.empty()) sector.clear();
     }
+    SectorPlan splan;
+    const bool compact = g_ucc_compact && !sector.empty() &&
+                         build_sector_plan(splan, fprog, gprog, uprog, nqubit, ref_index);
+    if (compact) {
+        int src = sector_smem_attr();
+        if (src) return src;
+        sector.clear();
+    }
     qfb_ucc u = new qfb_ucc_s;
+    u->compact = compact ? 1 : 0;
     u->fwd = fprog;
     u->grad = gprog;
     u->unrot = uprog;
@@ -2201,10 +2557,10 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     u->ref = ref_index;
     u->vchunks = grid_for(u->nbasis, 256, 2);
     if (u->vchunks * (unsigned)nbatch > 65535u) u->vchunks = std::max(1u, 65535u / nbatch);
-    u->gchunks = gprog ? grad_chunks(gprog, nqubit, nbatch) : 1;
+    u->gchunks = compact ? kSectorThreads / 32 : (gprog ? grad_chunks(gprog, nqubit, nbatch) : 1);
     const size_t B = nbatch, M = std::max(u->nparam, 1);
     const size_t nsteps = gprog ? std::max<size_t>(gprog->h_steps.size(), 1) : 1;
-    const size_t b_state = sizeof(double2) * u->nbasis * B;
+    const size_t b_state = compact ? 16 : sizeof(double2) * u->nbasis * B;
     size_t off = 0;
     auto take = [&](size_t bytes) {
         size_t o = off;
@@ -2220,6 +2576,7 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     const size_t idx_bytes = nqubit <= 32 ? sizeof(uint32_t) : sizeof(uint64_t);
     const size_t o_sec = take(idx_bytes * std::max<size_t>(sector.size(), 1));
     const size_t o_sg = take(sizeof(SecGroup) * std::max<size_t>(sgroups.size(), 1));
+    const size_t o_save = take(compact ? sizeof(double2) * 2 * (size_t)splan.nsec * B : 16);
     int rc = dev_alloc(&u->blob, off);
     if (rc) {
         delete u;
@@ -2235,7 +2592,8 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     u->vpart = (double2 *)(base + o_vp);
     u->gpart = (double2 *)(base + o_gp);
     u->psteps = (int2 *)(base + o_ps);
-    u->nsec = (int64_t)sector.size();
+    u->nsec = compact ? (int64_t)splan.nsec : (int64_t)sector.size();
+    u->SL.save = (double2 *)(base + o_save);
     u->sec = base + o_sec;
     u->sgroups = (SecGroup *)(base + o_sg);
     u->nsgroups = (int)sgroups.size();
@@ -2262,7 +2620,26 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
         delete u;
         return cuda_fail(e, "qfb_ucc_create");
     }
+    if (compact) {
+        rc = sector_upload(u, splan, sgroups);
+        if (rc) {
+            qfb_ucc_destroy(u);
+            return rc;
+        }
+    }
     *out = u;
+    return QFB_OK;
+}
+
+int qfb_ucc_config(int compact) {
+    if (compact != 0 && compact != 1) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
+    g_ucc_compact = compact;
+    return QFB_OK;
+}
+
+int qfb_ucc_path(qfb_ucc u, int32_t *path) {
+    if (!u || !path) return fail(QFB_EINVAL, "qfb_ucc_path: null argument");
+    *path = u->compact ? 2 : (u->nsec > 0 ? 1 : 0);
     return QFB_OK;
 }
 
@@ -2274,6 +2651,8 @@ int qfb_ucc_sector(qfb_ucc u, int64_t *nsec) {
 
 int qfb_ucc_destroy(qfb_ucc u) {
     if (!u) return QFB_OK;
+    dev_free(u->sblob);
+    dev_free(u->csr);
     for (auto &x : u->exec)
         if (x) cudaGraphExecDestroy(x);
     if (u->cap_stream) cudaStreamDestroy(u->cap_stream);

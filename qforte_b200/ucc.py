@@ -38,7 +38,13 @@ from .sq_op_pool import SQOpPool
 from .sq_operator import SQOperator
 from .utils import build_refprep, ref_to_basis_idx, trotterize
 
-__all__ = ["DUCC", "Evaluator", "UCCNVQE", "ADAPTVQE", "ansatz_strings", "gradient_strings"]
+__all__ = ["DUCC", "Evaluator", "evaluator_config", "UCCNVQE", "ADAPTVQE", "ansatz_strings", "gradient_strings"]
+
+
+def evaluator_config(compact=True):
+    """Process-wide: let evaluators created from now on use the compact
+    sector path (the default) or keep full-space states."""
+    check(lib().qfb_ucc_config(1 if compact else 0), "qfb_ucc_config")
 
 
 class Evaluator:
@@ -67,6 +73,13 @@ class Evaluator:
         """Device memory this evaluator holds."""
         n = ctypes.c_uint64()
         check(lib().qfb_ucc_memory(self.h, ctypes.byref(n)), "qfb_ucc_memory")
+        return n.value
+
+    @property
+    def path(self):
+        """0: full space; 1: sigma on the sector; 2: compact sector states."""
+        n = ctypes.c_int32()
+        check(lib().qfb_ucc_path(self.h, ctypes.byref(n)), "qfb_ucc_path")
         return n.value
 
     @property

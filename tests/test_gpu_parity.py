@@ -375,3 +375,65 @@ def test_sector_apply_every_batch_width(cuda, B):
     hterms = oracle_terms(mol.hamiltonian)
     E_o, _ = O.energy(10, mol.hf_reference, kops_forward(pool, tops), P[B - 1], hterms)
     assert abs(EB[B - 1] - E_o) < E_TOL
+
+
+@pytest.fixture
+def compact_off():
+    from qforte_b200.ucc import evaluator_config
+    evaluator_config(False)
+    yield
+    evaluator_config(True)
+
+
+@pytest.mark.parametrize("norb,seed,pool_type", [(4, 11, "SD"), (6, 3, "SD"), (5, 9, "GSD"),
+                                                 (6, 17, "sa_SD"), (7, 5, "SD"), (8, 2, "SD")])
+def test_compact_sector_path_matches_full_space(cuda, norb, seed, pool_type):
+    """The compact sector evaluator (psi and sigma of one parameter set in a
+    CTA's shared memory) against the full-space evaluator and the oracle."""
+    from qforte_b200.ucc import evaluator_config
+    mol, pool = random_problem(norb, seed, pool_type)
+    tops = list(range(0, len(pool), 1 if len(pool) < 400 else 3))
+    rng = np.random.default_rng(norb + seed)
+    P = rng.uniform(-0.1, 0.1, (5, len(tops)))
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference, pool_type=pool_type)
+    ev = eng.evaluator(5)
+    E, G = eng.energy_grad(P)
+    evaluator_config(False)
+    try:
+        eng2 = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference, pool_type=pool_type)
+        assert eng2.evaluator(5).path != 2
+        E2, G2 = eng2.energy_grad(P)
+    finally:
+        evaluator_config(True)
+    assert np.max(np.abs(E - E2)) < 1e-12 and np.max(np.abs(G - G2)) < 1e-11
+    if pool_type in ("SD", "GSD"):
+        assert ev.path == 2
+    if norb <= 6:
+        hterms = oracle_terms(mol.hamiltonian)
+        kf = kops_forward(pool, tops, pool_type)
+        E_o, _ = O.energy(2 * norb, mol.hf_reference, kf, P[0], hterms)
+        g_o = O.measure_gradient(2 * norb, mol.hf_reference, kf, P[0], hterms,
+                                 kops_grad=kops_gradient(pool, tops),
+                                 kops_unrot=kf if pool_type == "sa_SD" else None)
+        assert abs(E[0] - E_o) < E_TOL and np.max(np.abs(G[0] - g_o)) < G_TOL
+
+
+def test_compact_energy_only_then_gradient_sweep(cuda):
+    """Mode 0 (energy) saves the compact states; mode 2 sweeps from them."""
+    import torch
+    mol, pool = random_problem(6, 4)
+    tops = list(range(len(pool)))
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+    ev = eng.evaluator(3)
+    assert ev.path == 2
+    rng = np.random.default_rng(6)
+    P = rng.uniform(-0.1, 0.1, (3, len(tops)))
+    E, G = eng.energy_grad(P)
+    d_par, d_en, d_gr = ev.tensors()
+    d_par.copy_(torch.from_numpy(P))
+    d_gr.zero_()
+    ev.run(0)
+    ev.run(2)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(d_en.cpu().numpy() - E)) < 1e-13
+    assert np.max(np.abs(d_gr.cpu().numpy() - G)) < 1e-13
