@@ -210,6 +210,9 @@ QFB_API int qfb_ucc_sector(qfb_ucc u, int64_t *nsec);
  * psi and sigma in shared memory (sectors up to 6,400 amplitudes whose
  * program steps are all in Givens form).  No counterpart in the reference. */
 QFB_API int qfb_ucc_path(qfb_ucc u, int32_t *path);
+/* Entries of the H rows the compact path streams for each parameter set (0
+ * on the other paths).  No counterpart in the reference. */
+QFB_API int qfb_ucc_rows(qfb_ucc u, int64_t *nnz);
 /* Process-wide: whether evaluators created from now on may use the compact
  * sector path (1, the default) or not (0).  No counterpart in the reference. */
 QFB_API int qfb_ucc_config(int compact);

@@ -2126,17 +2126,34 @@ __global__ void k_sector_rows(const uint64_t *__restrict__ det, int nsec,
     if (!col) count[i] = c;
 }
 
+// One kernel's records (qfbs::SStream) on the host.
+struct StreamHost {
+    std::vector<uint4> rec;
+    std::vector<int2> span;
+    std::vector<int32_t> param;
+    int maxw = 0;
+};
+
+// A step of a program in compact form: its patterns with their alpha and
+// beta lists (entries of the lists follow in `ents`).
+struct CStep {
+    int32_t param = 0;
+    double gamma = 0.0;
+    struct Pat {
+        std::vector<qfbs::SEntry> a, b;
+        double2 gn, hn;
+    };
+    std::vector<Pat> pats;
+};
+
 struct SectorPlan {
     int na_orb = 0, nb_orb = 0, nalpha = 0, nbeta = 0, nsec = 0, ref_i = 0;
     std::vector<uint64_t> adet, bdet;
     std::vector<int32_t> arank, brank;
-    std::vector<qfbs::SEntry> ents;
-    std::vector<qfbs::SPat> pats;
-    std::vector<qfbs::SStep> steps;  // forward, then K, then U programs
-    int f0 = 0, nf = 0, k0 = 0, nk = 0, u0 = 0, nu = 0;
+    std::vector<CStep> fsteps, ksteps, usteps;
     std::vector<int2> kmu, umu;
     int fused = 0;
-    std::map<std::tuple<int, uint64_t, uint64_t, uint64_t, uint64_t>, int2> lists;
+    StreamHost fwd, sweep;
 };
 
 static uint32_t pext_parity_bits(uint64_t v, int odd, int n) {
@@ -2146,69 +2163,96 @@ static uint32_t pext_parity_bits(uint64_t v, int odd, int n) {
 }
 
 // Strings of one spin (odd = 0 alpha on even qubits, 1 beta on odd qubits)
-// whose bits on P equal want's, with their partner ranks and sign bits; the
-// list is shared by every step with the same key.  false: a partner leaves
-// the sector.
-static bool sector_list(SectorPlan &sp, int odd, int n, uint64_t P, uint64_t want, uint64_t x,
-                        uint64_t zb, int2 *out) {
+// whose bits on P equal want's, with their partner ranks and sign bits.
+// false: a partner leaves the sector.
+static bool sector_list(const SectorPlan &sp, int odd, int n, uint64_t P, uint64_t want,
+                        uint64_t x, uint64_t zb, std::vector<qfbs::SEntry> &out) {
     const uint64_t M = odd ? 0xAAAAAAAAAAAAAAAAull : 0x5555555555555555ull;
-    const auto key = std::make_tuple(odd, P & M, want & P & M, x & M, zb & M);
-    auto it = sp.lists.find(key);
-    if (it != sp.lists.end()) {
-        *out = it->second;
-        return true;
-    }
     const std::vector<uint64_t> &det = odd ? sp.bdet : sp.adet;
     const std::vector<int32_t> &rank = odd ? sp.brank : sp.arank;
-    const int a0 = (int)sp.ents.size();
+    out.clear();
     for (size_t r = 0; r < det.size(); ++r) {
         if ((det[r] & P & M) != (want & P & M)) continue;
-        const uint64_t partner = det[r] ^ (x & M);
-        const int32_t pr = rank[pext_parity_bits(partner, odd, n)];
+        const int32_t pr = rank[pext_parity_bits(det[r] ^ (x & M), odd, n)];
         if (pr < 0) return false;
         qfbs::SEntry e;
         e.r0 = (uint16_t)r;
         e.r1 = (uint16_t)pr;
         e.s = (uint32_t)(__builtin_popcountll(det[r] & zb & M) & 1);
-        sp.ents.push_back(e);
+        out.push_back(e);
     }
-    *out = make_int2(a0, (int)sp.ents.size() - a0);
-    sp.lists[key] = *out;
     return true;
 }
 
-static bool sector_steps(SectorPlan &sp, const qfb_prog_s *p, int n) {
+static bool sector_steps(const SectorPlan &sp, const qfb_prog_s *p, int n,
+                         std::vector<CStep> &out) {
     for (const StepDev &st : p->h_steps) {
         if (st.tab < 0 || st.na <= 0 || st.x == 0) return false;
         uint64_t P = 1ull << st.h;
         for (int i = 0; i < st.nd; ++i) P |= 1ull << ((st.dpos >> (6 * i)) & 63);
-        qfbs::SStep ss{};
-        ss.p0 = (int)sp.pats.size();
-        ss.param = st.param;
-        ss.gamma = st.gamma;
+        CStep cs;
+        cs.param = st.param;
+        cs.gamma = st.gamma;
         for (int a = 0; a < st.na; ++a) {
-            int2 la, lb;
-            if (!sector_list(sp, 0, n, P, st.patbits[a], st.x, st.zbase, &la)) return false;
-            if (!sector_list(sp, 1, n, P, st.patbits[a], st.x, st.zbase, &lb)) return false;
-            if (la.y == 0 || lb.y == 0) continue;
-            qfbs::SPat pt{};
-            pt.a0 = la.x;
-            pt.na = la.y;
-            pt.b0 = lb.x;
-            pt.nb = lb.y;
+            CStep::Pat pt;
+            if (!sector_list(sp, 0, n, P, st.patbits[a], st.x, st.zbase, pt.a)) return false;
+            if (!sector_list(sp, 1, n, P, st.patbits[a], st.x, st.zbase, pt.b)) return false;
+            if (pt.a.empty() || pt.b.empty()) continue;
             pt.gn = p->h_tab[st.tab + 2 * st.patidx[a]];
             pt.hn = p->h_tab[st.tab + 2 * st.patidx[a] + 1];
-            sp.pats.push_back(pt);
+            cs.pats.push_back(std::move(pt));
         }
-        ss.np = (int)sp.pats.size() - ss.p0;
-        sp.steps.push_back(ss);
+        out.push_back(std::move(cs));
     }
+    return true;
+}
+
+// Append one record (header, patterns, their lists) to a stream; false when
+// it outgrows one 16-byte word per thread or 16-bit list offsets.
+static bool push_record(StreamHost &S, const CStep &cs, int flags, int row) {
+    const int np = (int)cs.pats.size();
+    if (np > 255) return false;
+    size_t nent = 0;
+    for (const auto &pt : cs.pats) nent += pt.a.size() + pt.b.size();
+    const size_t bytes = sizeof(qfbs::RHead) + np * sizeof(qfbs::RPat) + nent * sizeof(qfbs::SEntry);
+    const int words = (int)((bytes + 15) / 16);
+    if (words > kSectorThreads) return false;
+    std::vector<uint4> w((size_t)words, make_uint4(0, 0, 0, 0));
+    char *base = (char *)w.data();
+    qfbs::RHead hd;
+    hd.npf = np | (flags << 8);
+    hd.row = row;
+    hd.gamma = cs.gamma;
+    std::memcpy(base, &hd, sizeof(hd));
+    size_t e = (sizeof(qfbs::RHead) + np * sizeof(qfbs::RPat)) / sizeof(qfbs::SEntry);
+    for (int k = 0; k < np; ++k) {
+        const auto &pt = cs.pats[k];
+        qfbs::RPat rp{};
+        rp.a0 = (uint16_t)e;
+        rp.na = (uint16_t)pt.a.size();
+        std::memcpy(base + e * sizeof(qfbs::SEntry), pt.a.data(), pt.a.size() * sizeof(qfbs::SEntry));
+        e += pt.a.size();
+        rp.b0 = (uint16_t)e;
+        rp.nb = (uint16_t)pt.b.size();
+        std::memcpy(base + e * sizeof(qfbs::SEntry), pt.b.data(), pt.b.size() * sizeof(qfbs::SEntry));
+        e += pt.b.size();
+        if (e > 65535) return false;
+        rp.inv = (pt.b.size() == 1) ? 0u
+                                    : (uint32_t)(((1ull << 32) + pt.b.size() - 1) / pt.b.size());
+        rp.gn = pt.gn;
+        rp.hn = pt.hn;
+        std::memcpy(base + sizeof(qfbs::RHead) + k * sizeof(qfbs::RPat), &rp, sizeof(rp));
+    }
+    S.span.push_back(make_int2((int)S.rec.size(), words));
+    S.param.push_back(cs.param);
+    S.rec.insert(S.rec.end(), w.begin(), w.end());
+    S.maxw = std::max(S.maxw, words);
     return true;
 }
 
 // The compact plan of an evaluator, or false when it does not apply (a step
 // outside the Givens form, a sector too large for shared memory, ranks that
-// do not fit 16 bits).
+// do not fit 16 bits, a step record larger than the block).
 static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_prog_s *kp,
                               const qfb_prog_s *up, int n, uint64_t ref) {
     const uint64_t A = 0x5555555555555555ull;
@@ -2242,28 +2286,38 @@ static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_pr
     if (nsec * 2 * sizeof(double2) > kSectorSmemMax) return false;
     sp.nsec = (int)nsec;
     sp.ref_i = sp.arank[pext_parity_bits(ref, 0, n)] * sp.nbeta + sp.brank[pext_parity_bits(ref, 1, n)];
-    sp.f0 = 0;
-    if (!sector_steps(sp, fp, n)) return false;
-    sp.nf = (int)sp.steps.size();
-    sp.k0 = (int)sp.steps.size();
+    if (!sector_steps(sp, fp, n, sp.fsteps)) return false;
+    for (const CStep &cs : sp.fsteps)
+        if (!push_record(sp.fwd, cs, qfbs::R_ROT, -1)) return false;
     if (kp) {
-        if (!sector_steps(sp, kp, n)) return false;
-        sp.nk = (int)sp.steps.size() - sp.k0;
-        sp.u0 = (int)sp.steps.size();
-        if (!sector_steps(sp, up, n)) return false;
-        sp.nu = (int)sp.steps.size() - sp.u0;
+        if (!sector_steps(sp, kp, n, sp.ksteps)) return false;
+        if (!sector_steps(sp, up, n, sp.usteps)) return false;
         const int M = kp->nparam;
-        sp.kmu.resize(M);
-        sp.umu.resize(M);
         sp.fused = (kp == up) ? 1 : 0;
-        for (int mu = 0; mu < M; ++mu) {
+        for (int mu = 0; mu < M; ++mu)
+            if (kp->p_step0[mu] < 0 || kp->p_step1[mu] - kp->p_step0[mu] != 1) sp.fused = 0;
+        // the reverse sweep in execution order (uccvqeabc.py:122-251): for mu
+        // from last to first, <sigma|K_mu|psi> on each K step, then (mu > 0)
+        // U_mu^dagger on both states; a single step that is both K and U does
+        // the two at once
+        for (int mu = M - 1; mu >= 0; --mu) {
             const int s0 = kp->p_step0[mu], s1 = kp->p_step1[mu];
-            sp.kmu[mu] = (s0 >= 0) ? make_int2(s0, s1) : make_int2(0, 0);
-            const int t0 = up->p_step0[mu], t1 = up->p_step1[mu];
-            sp.umu[mu] = (t0 >= 0) ? make_int2(t0, t1) : make_int2(0, 0);
-            if (s0 < 0 || s1 - s0 != 1) sp.fused = 0;
+            if (sp.fused) {
+                const int fl = mu > 0 ? (qfbs::R_ROT | qfbs::R_IP | qfbs::R_TWO) : qfbs::R_IP;
+                if (!push_record(sp.sweep, sp.ksteps[s0], fl, s0)) return false;
+                continue;
+            }
+            for (int s = s0; s >= 0 && s < s1; ++s)
+                if (!push_record(sp.sweep, sp.ksteps[s], qfbs::R_IP, s)) return false;
+            if (mu == 0) break;
+            const int u0 = up->p_step0[mu], u1 = up->p_step1[mu];
+            for (int s = u0; u0 >= 0 && s < u1; ++s)
+                if (!push_record(sp.sweep, sp.usteps[s], qfbs::R_ROT | qfbs::R_TWO, -1)) return false;
         }
     }
+    const size_t ring = 3 * (size_t)std::max(sp.fwd.maxw, sp.sweep.maxw) * 16;
+    const size_t ang = sizeof(double2) * std::max(sp.fwd.span.size(), sp.sweep.span.size());
+    if (nsec * 2 * sizeof(double2) + ang + ring > kSectorSmemMax) return false;
     return true;
 }
 
@@ -2288,6 +2342,7 @@ struct qfb_ucc_s {
     int64_t nsec = 0;
     size_t bytes = 0;     // device bytes held (blobs)
     int compact = 0;      // compact sector evaluator (qfb_sector.cuh)
+    int64_t nnz = 0;      // entries of the H rows on the compact sector
     void *sblob = nullptr, *csr = nullptr;
     qfbs::SLaunch SL{};
     void *sec = nullptr;  // uint32_t (nqubit <= 32) or uint64_t indices
@@ -2307,11 +2362,12 @@ static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> 
         off += (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
         return o;
     };
-    const size_t o_st = take(sizeof(qfbs::SStep) * sp.steps.size());
-    const size_t o_pt = take(sizeof(qfbs::SPat) * sp.pats.size());
-    const size_t o_en = take(sizeof(qfbs::SEntry) * sp.ents.size());
-    const size_t o_km = take(sizeof(int2) * sp.kmu.size());
-    const size_t o_um = take(sizeof(int2) * sp.umu.size());
+    const size_t o_fr = take(sizeof(uint4) * sp.fwd.rec.size());
+    const size_t o_fs = take(sizeof(int2) * sp.fwd.span.size());
+    const size_t o_fp = take(sizeof(int32_t) * sp.fwd.param.size());
+    const size_t o_sr = take(sizeof(uint4) * sp.sweep.rec.size());
+    const size_t o_ss = take(sizeof(int2) * sp.sweep.span.size());
+    const size_t o_sp = take(sizeof(int32_t) * sp.sweep.param.size());
     const size_t o_det = take(sizeof(uint64_t) * det.size());
     const size_t o_ar = take(sizeof(int32_t) * sp.arank.size());
     const size_t o_br = take(sizeof(int32_t) * sp.brank.size());
@@ -2322,11 +2378,12 @@ static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> 
     u->bytes += off;
     char *base = (char *)u->sblob;
     struct Up { size_t o; const void *p; size_t n; };
-    const Up ups[] = {{o_st, sp.steps.data(), sizeof(qfbs::SStep) * sp.steps.size()},
-                      {o_pt, sp.pats.data(), sizeof(qfbs::SPat) * sp.pats.size()},
-                      {o_en, sp.ents.data(), sizeof(qfbs::SEntry) * sp.ents.size()},
-                      {o_km, sp.kmu.data(), sizeof(int2) * sp.kmu.size()},
-                      {o_um, sp.umu.data(), sizeof(int2) * sp.umu.size()},
+    const Up ups[] = {{o_fr, sp.fwd.rec.data(), sizeof(uint4) * sp.fwd.rec.size()},
+                      {o_fs, sp.fwd.span.data(), sizeof(int2) * sp.fwd.span.size()},
+                      {o_fp, sp.fwd.param.data(), sizeof(int32_t) * sp.fwd.param.size()},
+                      {o_sr, sp.sweep.rec.data(), sizeof(uint4) * sp.sweep.rec.size()},
+                      {o_ss, sp.sweep.span.data(), sizeof(int2) * sp.sweep.span.size()},
+                      {o_sp, sp.sweep.param.data(), sizeof(int32_t) * sp.sweep.param.size()},
                       {o_det, det.data(), sizeof(uint64_t) * det.size()},
                       {o_ar, sp.arank.data(), sizeof(int32_t) * sp.arank.size()},
                       {o_br, sp.brank.data(), sizeof(int32_t) * sp.brank.size()},
@@ -2354,6 +2411,7 @@ static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> 
         if (nnz >= ((int64_t)1 << 31)) return fail(QFB_ENOMEM, "sector H rows: too many entries");
     }
     rowptr[nsec] = (int32_t)nnz;
+    u->nnz = nnz;
     bool real = true;
     for (const SecGroup &g : sg) real = real && g.real;
     const size_t o_rp = 0;
@@ -2382,17 +2440,16 @@ static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> 
     L.nbeta = sp.nbeta;
     L.ref_i = sp.ref_i;
     L.nparam = u->nparam;
-    L.nf = sp.nf;
-    L.fused = sp.fused;
-    L.nmu = sp.kmu.empty() ? 0 : (int)sp.kmu.size();
-    const qfbs::SStep *d_st = (const qfbs::SStep *)(base + o_st);
-    L.fsteps = d_st + sp.f0;
-    L.ksteps = d_st + sp.k0;
-    L.usteps = d_st + sp.u0;
-    L.kmu = (const int2 *)(base + o_km);
-    L.umu = (const int2 *)(base + o_um);
-    L.pats = (const qfbs::SPat *)(base + o_pt);
-    L.ents = (const qfbs::SEntry *)(base + o_en);
+    L.fwd.rec = (const uint4 *)(base + o_fr);
+    L.fwd.span = (const int2 *)(base + o_fs);
+    L.fwd.param = (const int32_t *)(base + o_fp);
+    L.fwd.n = (int)sp.fwd.span.size();
+    L.fwd.maxw = std::max(sp.fwd.maxw, 1);
+    L.sweep.rec = (const uint4 *)(base + o_sr);
+    L.sweep.span = (const int2 *)(base + o_ss);
+    L.sweep.param = (const int32_t *)(base + o_sp);
+    L.sweep.n = (int)sp.sweep.span.size();
+    L.sweep.maxw = std::max(sp.sweep.maxw, 1);
     L.rowptr = d_rp;
     L.col = d_col;
     L.val_r = d_vr;
@@ -2407,30 +2464,55 @@ static int sector_smem_attr() {
     static std::once_flag once;
     static cudaError_t err = cudaSuccess;
     std::call_once(once, [] {
-        err = cudaFuncSetAttribute(qfbs::k_sector_eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kSectorSmemMax);
+        err = cudaFuncSetAttribute(qfbs::k_sector_forward,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(qfbs::k_sector_h<true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(qfbs::k_sector_h<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(qfbs::k_sector_sweep,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
     });
     return err == cudaSuccess ? QFB_OK : cuda_fail(err, "sector evaluator shared memory");
 }
 
-// Compact evaluator: stage 2 runs the forward program, H psi and the energy
-// (saving psi and sigma), stage 3 the reverse sweep from the saved states.
+// Compact evaluator: stage 1 the forward program, stage 2 sigma = H psi and
+// the energy, stage 3 the reverse sweep (psi and sigma pass through the save
+// buffer between them).
 static int ucc_stage_compact(qfb_ucc u, int stage, int with_grad) {
-    if (stage < 2) return QFB_OK;
-    qfbs::SLaunch L = u->SL;
-    const size_t smem = sizeof(double2) * 2 * (size_t)L.nsec;
-    if (stage == 2) {
-        L.mode = 1 | 4;
-    } else {
-        if (!(with_grad && u->grad && u->nparam > 0)) return QFB_OK;
-        L.mode = 2;
-    }
-    qfbs::k_sector_eval<<<u->nbatch, kSectorThreads, smem, t_stream>>>(L);
-    QFB_LAUNCHED();
-    if (stage == 3) {
-        k_grad_final<<<dim3(u->nparam, u->nbatch), 128, 0, t_stream>>>(u->gpart, u->psteps,
-                                                                     u->gchunks, u->gradv);
-        QFB_LAUNCHED();
+    const qfbs::SLaunch &L = u->SL;
+    const size_t n = (size_t)L.nsec;
+    switch (stage) {
+        case 1:
+            qfbs::k_sector_forward<<<u->nbatch, kSectorThreads,
+                                     sizeof(double2) * (n + (size_t)L.fwd.n) +
+                                         sizeof(uint4) * 3 * (size_t)L.fwd.maxw,
+                                     t_stream>>>(L);
+            QFB_LAUNCHED();
+            break;
+        case 2:
+            if (L.val_c)
+                qfbs::k_sector_h<false><<<u->nbatch, kSectorThreads, sizeof(double2) * n, t_stream>>>(L);
+            else
+                qfbs::k_sector_h<true><<<u->nbatch, kSectorThreads, sizeof(double2) * n, t_stream>>>(L);
+            QFB_LAUNCHED();
+            break;
+        case 3:
+            if (!(with_grad && u->grad && u->nparam > 0)) break;
+            qfbs::k_sector_sweep<<<u->nbatch, kSectorThreads,
+                                   sizeof(double2) * (2 * n + (size_t)L.sweep.n) +
+                                       sizeof(uint4) * 3 * (size_t)L.sweep.maxw,
+                                   t_stream>>>(L);
+            QFB_LAUNCHED();
+            k_grad_final<<<dim3(u->nparam, u->nbatch), 128, 0, t_stream>>>(u->gpart, u->psteps,
+                                                                         u->gchunks, u->gradv);
+            QFB_LAUNCHED();
+            break;
+        default:
+            break;
     }
     return QFB_OK;
 }
@@ -2634,6 +2716,12 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
 int qfb_ucc_config(int compact) {
     if (compact != 0 && compact != 1) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
     g_ucc_compact = compact;
+    return QFB_OK;
+}
+
+int qfb_ucc_rows(qfb_ucc u, int64_t *nnz) {
+    if (!u || !nnz) return fail(QFB_EINVAL, "qfb_ucc_rows: null argument");
+    *nnz = u->nnz;
     return QFB_OK;
 }
 

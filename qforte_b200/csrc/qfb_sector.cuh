@@ -9,7 +9,8 @@
 // sigma of one parameter set in shared memory and runs the whole evaluation
 // there: the forward program, sigma = H psi from a sparse row list of H built
 // once per evaluator, the energy, and the adjoint reverse sweep, with one
-// barrier per program step and no global traffic besides the H rows.
+// barrier per program step and no global traffic besides the H rows and one
+// save of psi and sigma between the kernels.
 //
 // Each step is one of the Givens-form steps of the full-space program: the
 // pairs (j0, j1 = j0 ^ x) with j0's bits on the step's pattern positions equal
@@ -31,28 +32,33 @@ struct SEntry {  // one string of an alpha or beta list
     uint32_t s;       // parity of string & zbase
 };
 
-struct SPat {  // the pairs of one active pattern of a step
-    int32_t a0, na;  // alpha list entries [a0, a0 + na)
-    int32_t b0, nb;  // beta list entries [b0, b0 + nb)
+// A step record: the 16-byte header, the patterns, then the entries of their
+// lists, contiguous so that one cooperative copy brings a whole step into
+// shared memory.  Records run in the order a kernel executes them.
+struct RHead {
+    int32_t npf;   // patterns | flags << 8
+    int32_t row;   // partial row of an inner product
+    double gamma;
+};
+struct RPat {
+    uint16_t a0, na, b0, nb;  // lists: entries [a0, a0 + na) and [b0, b0 + nb) of the record
+    uint32_t inv;             // ceil(2^32 / nb), 0 when nb == 1
+    uint32_t pad;
     double2 gn, hn;
 };
+enum : int { R_ROT = 1, R_IP = 2, R_TWO = 4 };
 
-struct SStep {
-    int32_t p0, np;  // patterns [p0, p0 + np)
-    int32_t param;
-    int32_t pad;
-    double gamma;
+struct SStream {          // one kernel's records
+    const uint4 *rec;     // records, 16-byte words
+    const int2 *span;     // per record: first word, words
+    const int32_t *param; // per record: parameter of its angle
+    int n;
+    int maxw;             // longest record (words), <= block size
 };
 
 struct SLaunch {
     int nsec, nbeta, ref_i, nparam;
-    int nf, fused, nmu, mode;  // mode bit 0: forward + H (else load), bit 1: sweep, bit 2: save
-    const SStep *fsteps;       // forward program
-    const SStep *ksteps;       // K program (inner products); partial row = K step index
-    const SStep *usteps;       // U program (un-rotation)
-    const int2 *kmu, *umu;     // steps of each parameter in the K and U programs
-    const SPat *pats;
-    const SEntry *ents;
+    SStream fwd, sweep;
     const int32_t *rowptr;     // H rows
     const uint32_t *col;
     const double *val_r;       // real H (val_c == nullptr) ...
@@ -60,7 +66,7 @@ struct SLaunch {
     const double *params;      // [B][nparam]
     double *energy;            // [B]
     double2 *partial;          // [K steps][B][warps]
-    double2 *save;             // [B][2][nsec]: psi, sigma after H
+    double2 *save;             // [B][2][nsec]: psi after the forward program, sigma
 };
 
 __device__ __forceinline__ double2 s_cadd(double2 a, double2 b) {
@@ -82,27 +88,31 @@ __device__ __forceinline__ void s_givens(double2 &v0, double2 &v1, double c, dou
     v0 = n0;
 }
 
-// One step on the compact states: rotation by sign * gamma * theta (rot),
-// and / or the inner product <w|K|v> of the step's generator (acc).
+// One record on the compact states: rotation of v (and w when TWO) by the
+// angle whose cos / sin is csn, and / or the inner product <w|K|v> of the
+// step's generator into acc.  rec is the record in shared memory.
 template <bool ROT, bool IP, bool TWO>
-__device__ __forceinline__ void s_step(const SLaunch &L, const SStep &st, double theta, int sign,
-                                       double2 *v, double2 *w, double2 &acc) {
-    double sn = 0.0, cs = 1.0;
-    if (ROT) sincos((double)sign * st.gamma * theta, &sn, &cs);
-    const int nb = L.nbeta;
-    for (int p = st.p0; p < st.p0 + st.np; ++p) {
-        const SPat pt = L.pats[p];
-        const int total = pt.na * pt.nb;
+__device__ __forceinline__ void s_record(const uint4 *rec, int nbeta, double2 csn, double2 *v,
+                                         double2 *w, double2 &acc) {
+    const RHead hd = *reinterpret_cast<const RHead *>(rec);
+    const RPat *pats = reinterpret_cast<const RPat *>(rec + 1);
+    const SEntry *ents = reinterpret_cast<const SEntry *>(rec);
+    const int np = hd.npf & 255;
+    const double cs = csn.x, sn = csn.y;
+    for (int p = 0; p < np; ++p) {
+        const RPat pt = pats[p];
+        const int total = (int)pt.na * (int)pt.nb;
         for (int q = threadIdx.x; q < total; q += blockDim.x) {
-            const int ai = q / pt.nb, bi = q - ai * pt.nb;
-            const SEntry ea = L.ents[pt.a0 + ai], eb = L.ents[pt.b0 + bi];
-            const int i0 = (int)ea.r0 * nb + (int)eb.r0, i1 = (int)ea.r1 * nb + (int)eb.r1;
+            const int ai = pt.inv ? (int)__umulhi((uint32_t)q, pt.inv) : q;
+            const int bi = q - ai * (int)pt.nb;
+            const SEntry ea = ents[pt.a0 + ai], eb = ents[pt.b0 + bi];
+            const int i0 = (int)ea.r0 * nbeta + (int)eb.r0, i1 = (int)ea.r1 * nbeta + (int)eb.r1;
             const bool neg = (ea.s ^ eb.s) & 1u;
             double2 v0 = v[i0], v1 = v[i1];
             if (IP) {
                 const double2 w0 = w[i0], w1 = w[i1];
                 const double2 t = s_cadd(s_cjmul(w0, s_cmul(pt.hn, v1)), s_cjmul(w1, s_cmul(pt.gn, v0)));
-                const double gs = neg ? -st.gamma : st.gamma;
+                const double gs = neg ? -hd.gamma : hd.gamma;
                 acc.x += gs * t.x;
                 acc.y += gs * t.y;
             }
@@ -131,98 +141,148 @@ __device__ __forceinline__ double2 s_warp_sum(double2 v) {
     return v;
 }
 
-// Per-warp share of an inner product, written to partial[row][b][warp].
-__device__ __forceinline__ void s_flush(const SLaunch &L, int row, double2 acc) {
-    acc = s_warp_sum(acc);
-    const int nw = blockDim.x >> 5;
-    if ((threadIdx.x & 31) == 0)
-        L.partial[((size_t)row * gridDim.x + blockIdx.x) * nw + (threadIdx.x >> 5)] = acc;
+// cos and sin of sign * gamma * theta of every record of a stream, into s_cs
+__device__ __forceinline__ void s_angles(const SStream &S, const double *par, int sign,
+                                         double2 *s_cs) {
+    for (int r = threadIdx.x; r < S.n; r += blockDim.x) {
+        const RHead hd = *reinterpret_cast<const RHead *>(S.rec + S.span[r].x);
+        double sn, cs;
+        sincos((double)sign * hd.gamma * par[S.param[r]], &sn, &cs);
+        s_cs[r] = make_double2(cs, sn);
+    }
 }
 
-// One CTA per parameter set (blockIdx.x); psi and sigma in shared memory.
-__global__ void __launch_bounds__(512) k_sector_eval(SLaunch L) {
-    extern __shared__ double2 s_mem[];
-    __shared__ double2 s_red[32];
-    double2 *psi = s_mem, *sig = s_mem + L.nsec;
-    const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
-    const double *par = L.params + (size_t)b * L.nparam;
-    double2 *sv = L.save + (size_t)b * 2 * L.nsec;
-    double2 dummy = make_double2(0.0, 0.0);
-    if (L.mode & 1) {
-        for (int i = tid; i < L.nsec; i += nth) psi[i] = make_double2(0.0, 0.0);
-        __syncthreads();
-        if (tid == 0) psi[L.ref_i] = make_double2(1.0, 0.0);
-        __syncthreads();
-        for (int s = 0; s < L.nf; ++s) {
-            const SStep st = L.fsteps[s];
-            s_step<true, false, false>(L, st, par[st.param], 1, psi, nullptr, dummy);
-            __syncthreads();
-        }
-        // sigma = H psi: one warp per row
-        const int lane = tid & 31, nw = nth >> 5;
-        for (int i = tid >> 5; i < L.nsec; i += nw) {
-            double2 acc = make_double2(0.0, 0.0);
-            const int e1 = L.rowptr[i + 1];
-            if (L.val_c) {
-                for (int e = L.rowptr[i] + lane; e < e1; e += 32)
-                    acc = s_cadd(acc, s_cmul(__ldg(&L.val_c[e]), psi[__ldg(&L.col[e])]));
-            } else {
-                for (int e = L.rowptr[i] + lane; e < e1; e += 32) {
-                    const double f = __ldg(&L.val_r[e]);
-                    const double2 x = psi[__ldg(&L.col[e])];
-                    acc.x += f * x.x;
-                    acc.y += f * x.y;
-                }
-            }
-            acc = s_warp_sum(acc);
-            if (lane == 0) sig[i] = acc;
-        }
-        __syncthreads();
-        double2 e = make_double2(0.0, 0.0);
-        for (int i = tid; i < L.nsec; i += nth) e = s_cadd(e, s_cjmul(psi[i], sig[i]));
-        e = s_warp_sum(e);
-        if ((tid & 31) == 0) s_red[tid >> 5] = e;
-        __syncthreads();
-        if (tid == 0) {
-            double2 t = make_double2(0.0, 0.0);
-            for (int k = 0; k < (nth >> 5); ++k) t = s_cadd(t, s_red[k]);
-            L.energy[b] = t.x;
-        }
-        if (L.mode & 4)
-            for (int i = tid; i < 2 * L.nsec; i += nth) sv[i] = s_mem[i];
-    } else {
-        for (int i = tid; i < 2 * L.nsec; i += nth) s_mem[i] = sv[i];
+// Run a stream: record r + 2 is copied from global memory into registers
+// while record r is applied from shared memory (three buffers of maxw words
+// at s_rec), and stored after it; one barrier per record.
+template <bool SWEEP>
+__device__ __forceinline__ void s_run(const SLaunch &L, const SStream &S, const double2 *s_cs,
+                                      uint4 *s_rec, double2 *v, double2 *w) {
+    const int tid = threadIdx.x, nw = blockDim.x >> 5;
+    for (int r = 0; r < 2 && r < S.n; ++r) {
+        const int2 sp = S.span[r];
+        if (tid < sp.y) s_rec[r * S.maxw + tid] = S.rec[sp.x + tid];
     }
     __syncthreads();
-    if (!(L.mode & 2)) return;
-    for (int mu = L.nmu - 1; mu >= 0; --mu) {
-        const double th = par[mu];
-        const int2 kr = L.kmu[mu];
-        if (L.fused) {
-            double2 acc = make_double2(0.0, 0.0);
-            const SStep st = L.ksteps[kr.x];
-            if (mu > 0)
-                s_step<true, true, true>(L, st, th, -1, psi, sig, acc);
-            else
-                s_step<false, true, false>(L, st, th, -1, psi, sig, acc);
-            s_flush(L, kr.x, acc);
-            __syncthreads();
-            continue;
+    for (int r = 0; r < S.n; ++r) {
+        uint4 nxt = make_uint4(0, 0, 0, 0);
+        bool have = false;
+        if (r + 2 < S.n) {
+            const int2 sp = S.span[r + 2];
+            have = tid < sp.y;
+            if (have) nxt = S.rec[sp.x + tid];
         }
-        for (int s = kr.x; s < kr.y; ++s) {
-            double2 acc = make_double2(0.0, 0.0);
-            s_step<false, true, false>(L, L.ksteps[s], th, -1, psi, sig, acc);
-            s_flush(L, s, acc);
+        const uint4 *rec = s_rec + (r % 3) * S.maxw;
+        const int npf = reinterpret_cast<const RHead *>(rec)->npf;
+        const int fl = npf >> 8;
+        double2 acc = make_double2(0.0, 0.0);
+        if (!SWEEP) {
+            s_record<true, false, false>(rec, L.nbeta, s_cs[r], v, nullptr, acc);
+        } else if (fl == (R_ROT | R_IP | R_TWO)) {
+            s_record<true, true, true>(rec, L.nbeta, s_cs[r], v, w, acc);
+        } else if (fl == R_IP) {
+            s_record<false, true, false>(rec, L.nbeta, s_cs[r], v, w, acc);
+        } else {
+            s_record<true, false, true>(rec, L.nbeta, s_cs[r], v, w, acc);
         }
+        if (SWEEP && (fl & R_IP)) {
+            acc = s_warp_sum(acc);
+            const int row = reinterpret_cast<const RHead *>(rec)->row;
+            if ((tid & 31) == 0)
+                L.partial[((size_t)row * gridDim.x + blockIdx.x) * nw + (tid >> 5)] = acc;
+        }
+        if (have) s_rec[((r + 2) % 3) * S.maxw + tid] = nxt;
         __syncthreads();
-        if (mu == 0) break;
-        const int2 ur = L.umu[mu];
-        for (int s = ur.x; s < ur.y; ++s) {
-            const SStep st = L.usteps[s];
-            s_step<true, false, true>(L, st, par[st.param], -1, psi, sig, dummy);
-            __syncthreads();
+    }
+}
+
+constexpr int kRowUnroll = 8;  // H row entries in flight per lane
+
+// The evaluation runs as three kernels, one CTA per parameter set
+// (blockIdx.x) each: the forward program (psi in shared memory), sigma = H psi
+// with the energy (psi in shared memory, sigma rows straight to the save
+// buffer), and the reverse sweep (psi and sigma in shared memory).  The
+// first two hold one state and fit two CTAs per SM.  Shared memory: the
+// states, then the cos / sin of every record's angle, then the record ring.
+
+__global__ void __launch_bounds__(512, 2) k_sector_forward(SLaunch L) {
+    extern __shared__ double2 s_mem[];
+    double2 *psi = s_mem, *s_cs = s_mem + L.nsec;
+    uint4 *s_rec = reinterpret_cast<uint4 *>(s_cs + L.fwd.n);
+    const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    const double *par = L.params + (size_t)b * L.nparam;
+    for (int i = tid; i < L.nsec; i += nth) psi[i] = make_double2(0.0, 0.0);
+    s_angles(L.fwd, par, 1, s_cs);
+    __syncthreads();
+    if (tid == 0) psi[L.ref_i] = make_double2(1.0, 0.0);
+    s_run<false>(L, L.fwd, s_cs, s_rec, psi, nullptr);
+    double2 *sv = L.save + (size_t)b * 2 * L.nsec;
+    for (int i = tid; i < L.nsec; i += nth) sv[i] = psi[i];
+}
+
+template <bool REAL>
+__global__ void __launch_bounds__(512, 2) k_sector_h(SLaunch L) {
+    extern __shared__ double2 s_mem[];
+    __shared__ double2 s_red[32];
+    double2 *psi = s_mem;
+    const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    double2 *sv = L.save + (size_t)b * 2 * L.nsec;
+    for (int i = tid; i < L.nsec; i += nth) psi[i] = sv[i];
+    __syncthreads();
+    // one warp per row, kRowUnroll entries in flight per lane
+    const int lane = tid & 31, nw = nth >> 5;
+    double2 en = make_double2(0.0, 0.0);
+    for (int i = tid >> 5; i < L.nsec; i += nw) {
+        double2 acc = make_double2(0.0, 0.0);
+        const int e1 = L.rowptr[i + 1];
+        for (int e0 = L.rowptr[i] + lane; e0 < e1; e0 += 32 * kRowUnroll) {
+            uint32_t c[kRowUnroll];
+            double fr[REAL ? kRowUnroll : 1];
+            double2 fc[REAL ? 1 : kRowUnroll];
+#pragma unroll
+            for (int u = 0; u < kRowUnroll; ++u) {
+                const int e = e0 + 32 * u;
+                c[u] = (e < e1) ? __ldg(&L.col[e]) : 0u;
+                if (REAL) fr[u] = (e < e1) ? __ldg(&L.val_r[e]) : 0.0;
+                else fc[REAL ? 0 : u] = (e < e1) ? __ldg(&L.val_c[e]) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < kRowUnroll; ++u) {
+                const double2 x = psi[c[u]];
+                if (REAL) {
+                    acc.x += fr[u] * x.x;
+                    acc.y += fr[u] * x.y;
+                } else {
+                    acc = s_cadd(acc, s_cmul(fc[REAL ? 0 : u], x));
+                }
+            }
+        }
+        acc = s_warp_sum(acc);
+        if (lane == 0) {
+            sv[L.nsec + i] = acc;
+            en = s_cadd(en, s_cjmul(psi[i], acc));
         }
     }
+    if (lane == 0) s_red[tid >> 5] = en;
+    __syncthreads();
+    if (tid == 0) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int k = 0; k < nw; ++k) t = s_cadd(t, s_red[k]);
+        L.energy[b] = t.x;
+    }
+}
+
+__global__ void __launch_bounds__(512) k_sector_sweep(SLaunch L) {
+    extern __shared__ double2 s_mem[];
+    double2 *psi = s_mem, *sig = s_mem + L.nsec, *s_cs = s_mem + 2 * L.nsec;
+    uint4 *s_rec = reinterpret_cast<uint4 *>(s_cs + L.sweep.n);
+    const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    const double *par = L.params + (size_t)b * L.nparam;
+    const double2 *sv = L.save + (size_t)b * 2 * L.nsec;
+    for (int i = tid; i < 2 * L.nsec; i += nth) s_mem[i] = sv[i];
+    s_angles(L.sweep, par, -1, s_cs);
+    __syncthreads();
+    s_run<true>(L, L.sweep, s_cs, s_rec, psi, sig);
 }
 
 }  // namespace qfbs

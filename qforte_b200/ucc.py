@@ -83,6 +83,13 @@ class Evaluator:
         return n.value
 
     @property
+    def h_rows(self):
+        """Entries of H on the compact sector (0 unless path == 2)."""
+        n = ctypes.c_int64()
+        check(lib().qfb_ucc_rows(self.h, ctypes.byref(n)), "qfb_ucc_rows")
+        return n.value
+
+    @property
     def sector_size(self):
         """Indices of the particle-number sector H psi is formed on (0: all)."""
         n = ctypes.c_int64()
