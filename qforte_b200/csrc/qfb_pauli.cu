@@ -2350,6 +2350,60 @@ struct qfb_ucc_s {
     int nsgroups = 0;
 };
 
+// Reorder the entries of every H row so that each run of 8 consecutive
+// entries (the 8 lanes of a quarter warp in k_sector_h) gathers psi from 8
+// different 16-byte bank slots (column mod 8) as far as the row allows:
+// entries are bucketed by column mod 8 and dealt out one bucket after the
+// other, fullest bucket first.  Only the order of the row's sum changes.
+static int sector_rows_interleave(const std::vector<int32_t> &rowptr, int64_t nnz, uint32_t *d_col,
+                                  void *d_val, size_t vbytes) {
+    if (nnz == 0) return QFB_OK;
+    std::vector<uint32_t> col((size_t)nnz), col2((size_t)nnz);
+    std::vector<char> val((size_t)nnz * vbytes), val2((size_t)nnz * vbytes);
+    QFB_CUDA(cudaMemcpyAsync(col.data(), d_col, sizeof(uint32_t) * nnz, cudaMemcpyDeviceToHost,
+                             t_stream));
+    QFB_CUDA(cudaMemcpyAsync(val.data(), d_val, vbytes * nnz, cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    std::vector<int64_t> bucket[8];
+    const size_t nrow = rowptr.size() - 1;
+    for (size_t i = 0; i < nrow; ++i) {
+        for (auto &b : bucket) b.clear();
+        for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) bucket[col[e] & 7u].push_back(e);
+        size_t next[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int64_t out = rowptr[i];
+        auto left = [&](int r) { return bucket[r].size() - next[r]; };
+        auto emit = [&](int r) {
+            const int64_t e = bucket[r][next[r]++];
+            col2[out] = col[e];
+            std::memcpy(&val2[(size_t)out * vbytes], &val[(size_t)e * vbytes], vbytes);
+            ++out;
+        };
+        while (out < rowptr[i + 1]) {  // one group of (up to) 8 positions
+            const int64_t n = std::min<int64_t>(8, rowptr[i + 1] - out);
+            int order[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+            std::sort(order, order + 8, [&](int a, int b) { return left(a) > left(b); });
+            int64_t taken = 0;
+            for (int k = 0; k < 8 && taken < n; ++k)
+                if (left(order[k]) > 0) {
+                    emit(order[k]);
+                    ++taken;
+                }
+            while (taken < n) {  // fewer distinct residues than positions left
+                int best = 0;
+                for (int r = 1; r < 8; ++r)
+                    if (left(r) > left(best)) best = r;
+                emit(best);
+                ++taken;
+            }
+        }
+    }
+    QFB_CUDA(cudaMemcpyAsync(d_col, col2.data(), sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice,
+                             t_stream));
+    QFB_CUDA(cudaMemcpyAsync(d_val, val2.data(), vbytes * nnz, cudaMemcpyHostToDevice, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
 // Device copies of a compact plan and the H rows on its sector.
 static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> &sg) {
     const int nsec = sp.nsec;
@@ -2435,6 +2489,9 @@ static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> 
                                             nullptr, d_col, d_vr, d_vc);
     QFB_LAUNCHED();
     QFB_CUDA(cudaStreamSynchronize(t_stream));
+    rc = sector_rows_interleave(rowptr, nnz, d_col, real ? (void *)d_vr : (void *)d_vc,
+                                real ? sizeof(double) : sizeof(double2));
+    if (rc) return rc;
     qfbs::SLaunch &L = u->SL;
     L.nsec = nsec;
     L.nbeta = sp.nbeta;
