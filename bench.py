@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--full-space", action="store_true",
+                    help="keep full-space states (no compact sector evaluator)")
     ap.add_argument("--workload", default="ucc",
                     choices=["ucc", "gates", "grad", "adapt", "serve"],
                     help="ucc: batched dUCCSD energy+gradient (default); gates: the gate sweep; "
@@ -558,6 +560,9 @@ def main():
     mol, pool = problem(a.norb, a.seed)
     tops = list(range(len(pool)))
     M = len(tops)
+    if a.full_space:
+        from qforte_b200.ucc import evaluator_config
+        evaluator_config(False)
     eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
     ev = eng.evaluator(a.batch)
     rng = np.random.default_rng(a.seed + 1 + rank)
