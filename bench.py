@@ -368,7 +368,7 @@ def run_adapt(a, local):
     amps = rng.uniform(-0.1, 0.1, 12)
     eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
     t0 = time.perf_counter()
-    eng._pool_sum_handle()
+    eng._pool_program()
     compile_s = time.perf_counter() - t0
     for _ in range(max(a.warmup, 3)):
         g = eng.pool_gradients(amps)

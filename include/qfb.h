@@ -220,13 +220,24 @@ QFB_API int qfb_ucc_config(int compact);
  * scratch); a request loop admits work against its HBM budget with this.  No
  * counterpart in the reference. */
 QFB_API int qfb_ucc_memory(qfb_ucc u, uint64_t *bytes);
+/* ADAPT pool gradients (UCCVQE.measure_gradient3, uccvqeabc.py:253-283): give
+ * the evaluator a pool program (the pool operators' K strings, one parameter
+ * per operator, as for kprog); a run of mode 3 then computes psi, sigma, the
+ * energy and 2 Re <sigma|K_k|psi> for every pool operator k of every slot into
+ * a device block [nbatch][npool] (qfb_ucc_pool_buffer), in one graph launch
+ * when captured.  The pool's steps must be in Givens form. */
+QFB_API int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool);
+QFB_API int qfb_ucc_pool_buffer(qfb_ucc u, double **d_pool_grad);
+/* Host convenience: params in, energies and pool gradients out, synchronous. */
+QFB_API int qfb_ucc_eval_pool(qfb_ucc u, const double *params, double *energy, double *pool_grad);
 /* Device addresses of the parameter block and the outputs. */
 QFB_API int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_grad);
 /* Enqueue one evaluation on the calling thread's stream (replays the
  * captured graph when one exists for this mode).  with_grad: 0 energy only;
  * 1 energy and gradient; 2 the gradient sweep alone, on the psi and sigma a
  * preceding with_grad = 0 run left (the sweep un-rotates them in place, so a
- * second mode-2 run needs a new mode-0 run first). */
+ * second mode-2 run needs a new mode-0 run first); 3 energy and the pool
+ * gradients (qfb_ucc_set_pool). */
 QFB_API int qfb_ucc_run(qfb_ucc u, int with_grad);
 /* Capture one evaluation of the given mode into a CUDA graph (replayed by
  * later runs). */

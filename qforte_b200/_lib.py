@@ -78,6 +78,9 @@ SIGNATURES = {
     "qfb_ucc_destroy": (ctypes.c_int, [_vp]),
     "qfb_ucc_sector": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_memory": (ctypes.c_int, [_vp, _vp]),
+    "qfb_ucc_set_pool": (ctypes.c_int, [_vp, c_prog]),
+    "qfb_ucc_pool_buffer": (ctypes.c_int, [_vp, _vp]),
+    "qfb_ucc_eval_pool": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "qfb_ucc_path": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_rows": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_config": (ctypes.c_int, [ctypes.c_int]),

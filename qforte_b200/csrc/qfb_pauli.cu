@@ -36,6 +36,7 @@
 #include <complex>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <tuple>
 #include <unordered_map>
@@ -767,6 +768,40 @@ __global__ void k_energy_final(const double2 *__restrict__ partial, int n,
         acc = c_add(acc, partial[(uint64_t)blockIdx.x * n + k]);
     acc = block_sum(acc);
     if (threadIdx.x == 0) energy[blockIdx.x] = acc.x;
+}
+
+// Pool inner products <sigma|K_s|psi> of Givens-form steps read from a device
+// array (one step per blockIdx.y, slot blockIdx.z, chunk blockIdx.x), states
+// untouched: every ADAPT pool operator in one launch.
+// partial[((s * B) + b) * chunks + c].
+__global__ void __launch_bounds__(256) k_pool_ip(const double2 *__restrict__ psi,
+                                                 const double2 *__restrict__ sig, uint64_t nbasis,
+                                                 const StepDev *__restrict__ steps,
+                                                 const double2 *__restrict__ tab,
+                                                 double2 *__restrict__ partial) {
+    const int s = blockIdx.y, b = blockIdx.z, B = gridDim.z;
+    const StepDev &st = steps[s];
+    const double2 *ps = psi + (uint64_t)b * nbasis;
+    const double2 *sg = sig + (uint64_t)b * nbasis;
+    const double2 *tb = tab + st.tab;
+    const int fb = 63 - __clzll(nbasis) - 1 - st.nd;
+    const uint64_t total = (uint64_t)st.na << fb;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (uint64_t)gridDim.x * blockDim.x) {
+        const int ai = (int)(q >> fb);
+        const uint64_t j0 = active_pair(q & ((1ull << fb) - 1ull), st) | st.patbits[ai];
+        const int pat = st.patidx[ai];
+        const double2 gn = __ldg(&tb[2 * pat]), hn = __ldg(&tb[2 * pat + 1]);
+        const uint64_t j1 = j0 ^ st.x;
+        const double2 v0 = ps[j0], v1 = ps[j1], w0 = sg[j0], w1 = sg[j1];
+        const double2 t = c_add(c_cjmul(w0, c_mul(hn, v1)), c_cjmul(w1, c_mul(gn, v0)));
+        const double gs = parity64(j0 & st.zbase) ? -st.gamma : st.gamma;
+        acc.x += gs * t.x;
+        acc.y += gs * t.y;
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) partial[((uint64_t)s * B + b) * gridDim.x + blockIdx.x] = acc;
 }
 
 // grad[b * M + mu] = 2 Re sum over mu's steps s and chunks c of
@@ -2335,8 +2370,8 @@ struct qfb_ucc_s {
     double2 *vpart = nullptr, *gpart = nullptr;
     int2 *psteps = nullptr;
     cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};  // by run mode
-    uint64_t graph_kernels[3] = {0, 0, 0};
+    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};  // by run mode
+    uint64_t graph_kernels[4] = {0, 0, 0, 0};
     // particle-number sector of the state (every program conserves it):
     // H psi is formed on these indices only; nsec == 0 means the full space
     int64_t nsec = 0;
@@ -2348,6 +2383,17 @@ struct qfb_ucc_s {
     void *sec = nullptr;  // uint32_t (nqubit <= 32) or uint64_t indices
     SecGroup *sgroups = nullptr;
     int nsgroups = 0;
+    std::shared_ptr<SectorPlan> splan;  // compact path: strings and ranks of the sector
+    // ADAPT pool (qfb_ucc_set_pool): 2 Re <sigma|K_k|psi> for every pool operator k
+    const qfb_prog_s *pool = nullptr;
+    int npool = 0;
+    void *pblob = nullptr;
+    double *pgrad = nullptr;   // [B][npool]
+    double2 *ppart = nullptr;  // [pool steps][B][pchunks]
+    int2 *pranges = nullptr;   // pool steps of each operator
+    StepDev *pool_steps = nullptr;  // full space: the pool's steps on the device
+    unsigned pchunks = 1;
+    qfbs::SStream pstream{};   // compact: the pool's inner-product records
 };
 
 // Reorder the entries of every H row so that each run of 8 consecutive
@@ -2623,14 +2669,41 @@ static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
     return rc;
 }
 
+// Stage 4: the pool's inner products on psi and sigma (qfb_ucc_set_pool).
+static int ucc_pool_stage(qfb_ucc u) {
+    if (!u->pool) return fail(QFB_EINVAL, "qfb_ucc_run: no pool set (qfb_ucc_set_pool)");
+    const int B = u->nbatch;
+    unsigned chunks = u->pchunks;
+    if (u->compact) {
+        qfbs::SLaunch L = u->SL;
+        L.partial = u->ppart;
+        const int sm = sm_count();
+        const int G = std::max(1, std::min(u->pstream.n, (2 * sm + B - 1) / B));
+        const size_t smem = sizeof(double2) * 2 * (size_t)L.nsec + sizeof(uint4) * u->pstream.maxw;
+        qfbs::k_sector_pool<<<dim3(G, B), kSectorThreads, smem, t_stream>>>(L, u->pstream);
+        QFB_LAUNCHED();
+        chunks = kSectorThreads / 32;
+    } else {
+        const dim3 grid(u->pchunks, (unsigned)u->pool->h_steps.size(), B);
+        k_pool_ip<<<grid, 256, 0, t_stream>>>(u->psi, u->sig, u->nbasis, u->pool_steps,
+                                              u->pool->d_tab, u->ppart);
+        QFB_LAUNCHED();
+    }
+    k_grad_final<<<dim3(u->npool, B), 128, 0, t_stream>>>(u->ppart, u->pranges, chunks, u->pgrad);
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
 // mode 0: energy (stages 0-2); 1: energy and gradient (0-3); 2: the gradient
-// sweep alone (stage 3) on psi and sigma as a mode-0 run left them.
+// sweep alone (stage 3) on psi and sigma as a mode-0 run left them; 3: energy
+// and the pool's gradients (stages 0-2, then the pool stage).
 static int ucc_enqueue(qfb_ucc u, int mode) {
-    for (int st = (mode == 2 ? 3 : 0); st < 4; ++st) {
-        int rc = ucc_stage(u, st, mode != 0);
+    const int last = (mode == 3) ? 2 : 3;
+    for (int st = (mode == 2 ? 3 : 0); st <= last; ++st) {
+        int rc = ucc_stage(u, st, mode == 1 || mode == 2);
         if (rc) return rc;
     }
-    return QFB_OK;
+    return mode == 3 ? ucc_pool_stage(u) : QFB_OK;
 }
 
 extern "C" {
@@ -2765,6 +2838,7 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
             qfb_ucc_destroy(u);
             return rc;
         }
+        u->splan = std::make_shared<SectorPlan>(std::move(splan));
     }
     *out = u;
     return QFB_OK;
@@ -2798,11 +2872,125 @@ int qfb_ucc_destroy(qfb_ucc u) {
     if (!u) return QFB_OK;
     dev_free(u->sblob);
     dev_free(u->csr);
+    dev_free(u->pblob);
     for (auto &x : u->exec)
         if (x) cudaGraphExecDestroy(x);
     if (u->cap_stream) cudaStreamDestroy(u->cap_stream);
     dev_free(u->blob);
     delete u;
+    return QFB_OK;
+}
+
+int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
+    if (!u || !pool) return fail(QFB_EINVAL, "qfb_ucc_set_pool: null argument");
+    if (!pool->params_contiguous || pool->nparam < 1)
+        return fail(QFB_EINVAL, "qfb_ucc_set_pool: the pool program needs one parameter per operator");
+    for (const auto &st : pool->h_steps)
+        if (st.h >= u->nqubit) return fail(QFB_EINVAL, "qfb_ucc_set_pool: pool acts beyond qubit");
+    const int B = u->nbatch, M = pool->nparam;
+    const size_t nst = pool->h_steps.size();
+    if (nst == 0 || nst > 65535) return fail(QFB_ENOSYS, "qfb_ucc_set_pool: %zu pool steps", nst);
+    qfbs::SStream ps{};
+    StreamHost sh;
+    unsigned chunks = 1;
+    if (u->compact) {
+        std::vector<CStep> cs;
+        if (!sector_steps(*u->splan, pool, u->nqubit, cs))
+            return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool outside the Givens form on the sector");
+        for (size_t k = 0; k < cs.size(); ++k)
+            if (!push_record(sh, cs[k], qfbs::R_IP, (int)k))
+                return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool step too large");
+        chunks = kSectorThreads / 32;
+    } else {
+        uint64_t most = 1;
+        for (const auto &st : pool->h_steps) {
+            if (st.tab < 0 || st.na <= 0 || st.x == 0)
+                return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool step outside the Givens form");
+            const int fb = u->nqubit - 1 - st.nd;
+            if (fb < 0) return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool step wider than the state");
+            most = std::max<uint64_t>(most, (uint64_t)st.na << fb);
+        }
+        chunks = (unsigned)std::min<uint64_t>(256, std::max<uint64_t>(1, most / (256 * 8)));
+    }
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_pg = take(sizeof(double) * (size_t)B * M);
+    const size_t o_pp = take(sizeof(double2) * nst * B * chunks);
+    const size_t o_pr = take(sizeof(int2) * M);
+    const size_t o_ps = take(u->compact ? 16 : sizeof(StepDev) * nst);
+    const size_t o_rec = take(sizeof(uint4) * sh.rec.size());
+    const size_t o_sp = take(sizeof(int2) * sh.span.size());
+    void *blob = nullptr;
+    int rc = dev_alloc(&blob, off);
+    if (rc) return rc;
+    char *base = (char *)blob;
+    std::vector<int2> pr(M);
+    for (int k = 0; k < M; ++k)
+        pr[k] = pool->p_step0[k] >= 0 ? make_int2(pool->p_step0[k], pool->p_step1[k]) : make_int2(0, 0);
+    cudaError_t e = cudaMemsetAsync(blob, 0, off, t_stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(base + o_pr, pr.data(), sizeof(int2) * M, cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess && !u->compact)
+        e = cudaMemcpyAsync(base + o_ps, pool->h_steps.data(), sizeof(StepDev) * nst,
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess && !sh.rec.empty())
+        e = cudaMemcpyAsync(base + o_rec, sh.rec.data(), sizeof(uint4) * sh.rec.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess && !sh.span.empty())
+        e = cudaMemcpyAsync(base + o_sp, sh.span.data(), sizeof(int2) * sh.span.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);
+    if (e != cudaSuccess) {
+        dev_free(blob);
+        return cuda_fail(e, "qfb_ucc_set_pool");
+    }
+    dev_free(u->pblob);
+    if (u->exec[3]) {
+        cudaGraphExecDestroy(u->exec[3]);
+        u->exec[3] = nullptr;
+    }
+    u->pblob = blob;
+    u->pool = pool;
+    u->npool = M;
+    u->pgrad = (double *)(base + o_pg);
+    u->ppart = (double2 *)(base + o_pp);
+    u->pranges = (int2 *)(base + o_pr);
+    u->pool_steps = (StepDev *)(base + o_ps);
+    u->pchunks = chunks;
+    ps.rec = (const uint4 *)(base + o_rec);
+    ps.span = (const int2 *)(base + o_sp);
+    ps.param = nullptr;
+    ps.n = (int)sh.span.size();
+    ps.maxw = std::max(sh.maxw, 1);
+    u->pstream = ps;
+    return QFB_OK;
+}
+
+int qfb_ucc_eval_pool(qfb_ucc u, const double *params, double *energy, double *pool_grad) {
+    if (!u || !energy || !pool_grad) return fail(QFB_EINVAL, "qfb_ucc_eval_pool: null argument");
+    if (!u->pool) return fail(QFB_EINVAL, "qfb_ucc_eval_pool: no pool set");
+    if (u->nparam > 0 && !params) return fail(QFB_EINVAL, "qfb_ucc_eval_pool: null parameters");
+    const size_t np = (size_t)u->nbatch * u->nparam;
+    if (np) QFB_CUDA(cudaMemcpyAsync(u->params, params, sizeof(double) * np,
+                                     cudaMemcpyHostToDevice, t_stream));
+    int rc = qfb_ucc_run(u, 3);
+    if (rc) return rc;
+    QFB_CUDA(cudaMemcpyAsync(energy, u->energy, sizeof(double) * u->nbatch,
+                             cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaMemcpyAsync(pool_grad, u->pgrad, sizeof(double) * u->nbatch * u->npool,
+                             cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
+int qfb_ucc_pool_buffer(qfb_ucc u, double **d_pool_grad) {
+    if (!u || !d_pool_grad) return fail(QFB_EINVAL, "qfb_ucc_pool_buffer: null argument");
+    if (!u->pool) return fail(QFB_EINVAL, "qfb_ucc_pool_buffer: no pool set");
+    *d_pool_grad = u->pgrad;
     return QFB_OK;
 }
 
@@ -2822,7 +3010,7 @@ int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_
 
 int qfb_ucc_run(qfb_ucc u, int with_grad) {
     if (!u) return fail(QFB_EINVAL, "qfb_ucc_run: null evaluator");
-    if (with_grad < 0 || with_grad > 2) return fail(QFB_EINVAL, "qfb_ucc_run: mode %d", with_grad);
+    if (with_grad < 0 || with_grad > 3) return fail(QFB_EINVAL, "qfb_ucc_run: mode %d", with_grad);
     const int k = with_grad;
     if (u->exec[k]) {
         QFB_CUDA(cudaGraphLaunch(u->exec[k], t_stream));
@@ -2834,7 +3022,7 @@ int qfb_ucc_run(qfb_ucc u, int with_grad) {
 
 int qfb_ucc_capture(qfb_ucc u, int with_grad) {
     if (!u) return fail(QFB_EINVAL, "qfb_ucc_capture: null evaluator");
-    if (with_grad < 0 || with_grad > 2)
+    if (with_grad < 0 || with_grad > 3)
         return fail(QFB_EINVAL, "qfb_ucc_capture: mode %d", with_grad);
     const int k = with_grad;
     if (u->exec[k]) return QFB_OK;

@@ -285,4 +285,29 @@ __global__ void __launch_bounds__(512) k_sector_sweep(SLaunch L) {
     s_run<true>(L, L.sweep, s_cs, s_rec, psi, sig);
 }
 
+// Pool inner products on the compact states: each CTA loads psi and sigma of
+// slot blockIdx.y and runs the inner-product records r = blockIdx.x,
+// blockIdx.x + gridDim.x, ... of the pool stream (records leave the states
+// unchanged, so CTAs share none).
+__global__ void __launch_bounds__(512) k_sector_pool(SLaunch L, SStream P) {
+    extern __shared__ double2 s_mem[];
+    double2 *psi = s_mem, *sig = s_mem + L.nsec;
+    uint4 *s_rec = reinterpret_cast<uint4 *>(s_mem + 2 * L.nsec);
+    const int b = blockIdx.y, tid = threadIdx.x, nth = blockDim.x, nw = nth >> 5;
+    const double2 *sv = L.save + (size_t)b * 2 * L.nsec;
+    for (int i = tid; i < 2 * L.nsec; i += nth) s_mem[i] = sv[i];
+    for (int r = blockIdx.x; r < P.n; r += gridDim.x) {
+        const int2 sp = P.span[r];
+        if (tid < sp.y) s_rec[tid] = P.rec[sp.x + tid];
+        __syncthreads();
+        double2 acc = make_double2(0.0, 0.0);
+        s_record<false, true, false>(s_rec, L.nbeta, make_double2(1.0, 0.0), psi, sig, acc);
+        acc = s_warp_sum(acc);
+        const int row = reinterpret_cast<const RHead *>(s_rec)->row;
+        if ((tid & 31) == 0)
+            L.partial[((size_t)row * gridDim.y + b) * nw + (tid >> 5)] = acc;
+        __syncthreads();
+    }
+}
+
 }  // namespace qfbs

@@ -114,6 +114,28 @@ class Evaluator:
         self.generation += 1
         return e, g
 
+    def set_pool(self, prog):
+        """Give the evaluator an ADAPT pool program (one parameter per operator)."""
+        check(lib().qfb_ucc_set_pool(self.h, prog.h), "qfb_ucc_set_pool")
+        self._pool_prog = prog  # keeps it alive
+        self.npool = prog.nparam
+        d = ctypes.c_void_p()
+        check(lib().qfb_ucc_pool_buffer(self.h, ctypes.byref(d)), "qfb_ucc_pool_buffer")
+        self.d_pool = d.value
+
+    def eval_pool(self, P):
+        """Energies and every pool operator's gradient 2 Re <H psi|K_k psi> per row."""
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        if P.shape != (self.nbatch, self.nparam):
+            raise ValueError(f"parameters of shape {P.shape}, expected "
+                             f"{(self.nbatch, self.nparam)}")
+        self._ensure_graph(3)
+        e = np.empty(self.nbatch)
+        g = np.empty((self.nbatch, self.npool))
+        check(lib().qfb_ucc_eval_pool(self.h, ptr(P), ptr(e), ptr(g)), "qfb_ucc_eval_pool")
+        self.generation += 1
+        return e, g
+
     def run(self, with_grad=True):
         """Enqueue one evaluation on the library's stream (device buffers in and
         out, no host synchronisation).  ``with_grad`` 0/False: energies; 1/True:
@@ -333,8 +355,29 @@ class DUCC:
             self._pool_sum = sum_from_terms(terms, seg, len(self._pool))
         return self._pool_sum
 
+    def _pool_program(self):
+        if getattr(self, "_pool_prog", None) is None:
+            gx, gz, gs, gp = gradient_strings(self._pool, range(len(self._pool)), self._qe)
+            self._pool_prog = prog_from_strings(gx, gz, gs, gp, len(self._pool))
+        return self._pool_prog
+
     def pool_gradients(self, params):
-        """2 Re <H psi | K_k psi> for every operator of the pool, one launch."""
+        """2 Re <H psi | K_k psi> for every operator of the pool
+        (measure_gradient3): the evaluator's graph-captured run of mode 3 (psi,
+        sigma, then every operator's inner product in one launch)."""
+        P = np.ascontiguousarray(np.atleast_2d(np.asarray(params, dtype=np.float64)))
+        ev = self.evaluator(P.shape[0])
+        if getattr(ev, "_pool_prog", None) is None:
+            try:
+                ev.set_pool(self._pool_program())
+            except RuntimeError:  # a pool outside the Givens form
+                return self.pool_gradients_grouped(params)
+        _, g = ev.eval_pool(P)
+        return g[0] if np.ndim(params) == 1 else g
+
+    def pool_gradients_grouped(self, params):
+        """The same through the grouped Pauli-sum expectation values of the
+        pool (one x-group per operator, qfb_sum_expval)."""
         ps = self._pool_sum_handle()
         psi, P, B = self._prepare(params)
         sig = None

@@ -437,3 +437,34 @@ def test_compact_energy_only_then_gradient_sweep(cuda):
     torch.cuda.synchronize()
     assert np.max(np.abs(d_en.cpu().numpy() - E)) < 1e-13
     assert np.max(np.abs(d_gr.cpu().numpy() - G)) < 1e-13
+
+
+@pytest.mark.parametrize("compact", [True, False])
+def test_pool_gradients_one_launch_vs_grouped_and_oracle(cuda, compact):
+    """Every ADAPT pool gradient from the evaluator's pool stage (mode 3)
+    against the grouped Pauli-sum path and the oracle's measure_gradient3."""
+    from qforte_b200.ucc import evaluator_config
+    mol, gsd = random_problem(5, 31, "GSD")
+    rng = np.random.default_rng(3)
+    tops = [int(t) for t in rng.choice(len(gsd), 6, replace=False)]
+    amps = rng.uniform(-0.1, 0.1, 6)
+    evaluator_config(compact)
+    try:
+        eng = DUCC(mol.hamiltonian, gsd, tops, mol.hf_reference)
+        g = eng.pool_gradients(amps)
+        ev = eng.evaluator(1)
+        assert (ev.path == 2) == compact and getattr(ev, "_pool_prog", None) is not None
+        g2 = eng.pool_gradients_grouped(amps)
+        P = np.vstack([amps, rng.uniform(-0.1, 0.1, 6)])
+        GB = eng.pool_gradients(P)
+    finally:
+        evaluator_config(True)
+    assert np.max(np.abs(g - g2)) < 1e-12
+    assert np.max(np.abs(GB[0] - g)) < 1e-12
+    hterms = oracle_terms(mol.hamiltonian)
+    g_o = O.measure_gradient3(10, mol.hf_reference, kops_forward(gsd, tops), amps, hterms,
+                              kops_gradient(gsd, range(len(gsd))))
+    assert np.max(np.abs(g - g_o)) < G_TOL
+    g_o1 = O.measure_gradient3(10, mol.hf_reference, kops_forward(gsd, tops), P[1], hterms,
+                               kops_gradient(gsd, range(len(gsd))))
+    assert np.max(np.abs(GB[1] - g_o1)) < G_TOL
