@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--layers", type=int, default=100, help="gate sweep: layers per circuit")
     ap.add_argument("--tile", type=int, default=0,
                     help="gate sweep: tile bits of gate runs (0 default, -1 one pass per gate)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="gate sweep: pick the tile shape per qubit count with the autotuner")
     return ap.parse_args()
 
 
@@ -236,6 +238,10 @@ def run_gates(a, rank, world, local):
     clocks = Clocks(local)
     for n in ns:
         circ, spec = layered_random_circuit(n, a.layers, a.seed + n)
+        tuned = None
+        if a.autotune:
+            from qforte_b200.autotune import tune_gates
+            tuned, _ = tune_gates(circ, n, reps=1, store=False)
         nw, nsingle, pass_bytes = gate_plan(circ.gates(), n)
         qc = qb.Computer(n)
         for _ in range(max(a.warmup, 3) if n < 28 else 1):
@@ -259,7 +265,8 @@ def run_gates(a, rank, world, local):
                      "one_gate_passes": nsingle, "ms_per_circuit": ms, "pass_gbs": gbs,
                      "frac_of_hbm": gbs / peak,
                      "effective_gate_gbs": len(spec) * 32.0 * 2 ** n / (ms * 1e-3) / 1e9,
-                     "gpu_launches": launches})
+                     "gpu_launches": launches,
+                     "tile": list(tuned) if tuned else a.tile})
         del qc
     last = rows[-1]
     line = {"metric": GATE_METRIC, "value": last["pass_gbs"], "unit": "GB/s", "n_gpus": 1,

@@ -216,6 +216,12 @@ QFB_API int qfb_ucc_rows(qfb_ucc u, int64_t *nnz);
 /* Process-wide: whether evaluators created from now on may use the compact
  * sector path (1, the default) or not (0).  No counterpart in the reference. */
 QFB_API int qfb_ucc_config(int compact);
+/* Process-wide tile shape of the full-space windows of evaluators created
+ * from now on: fwd_bits qubits per forward tile (default 12, at most 13),
+ * grad_bits per two-state gradient tile (default 11, at most 12), always
+ * including the lowest low_bits qubits (default 3).  Set by the autotuner.
+ * No counterpart in the reference. */
+QFB_API int qfb_ucc_tiles(int fwd_bits, int grad_bits, int low_bits);
 /* Device bytes the evaluator holds (states, parameter and output blocks,
  * scratch); a request loop admits work against its HBM budget with this.  No
  * counterpart in the reference. */

@@ -84,6 +84,7 @@ SIGNATURES = {
     "qfb_ucc_path": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_rows": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_config": (ctypes.c_int, [ctypes.c_int]),
+    "qfb_ucc_tiles": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "qfb_ucc_buffers": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "qfb_ucc_run": (ctypes.c_int, [_vp, ctypes.c_int]),
     "qfb_ucc_capture": (ctypes.c_int, [_vp, ctypes.c_int]),

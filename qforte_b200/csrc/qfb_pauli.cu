@@ -888,6 +888,9 @@ struct qfb_prog_s {
     WinPlan *fwd_plan[41] = {nullptr};   // by qubit count
     WinPlan *grad_plan[41] = {nullptr};  // gradient sweep with K = this program ...
     const qfb_prog_s *grad_plan_u[41] = {nullptr};  // ... and U_mu from this one
+    // plans replaced while the program lives (a new tile shape or U program):
+    // captured evaluator graphs may still read them, so they go with the program
+    std::vector<WinPlan *> retired;
     ~qfb_prog_s() {
         for (auto *v : {&fwd_plan, &grad_plan})
             for (auto *pl : *v)
@@ -895,6 +898,10 @@ struct qfb_prog_s {
                     dev_free(pl->blob);
                     delete pl;
                 }
+        for (auto *pl : retired) {
+            dev_free(pl->blob);
+            delete pl;
+        }
     }
 };
 
@@ -905,6 +912,8 @@ namespace {
 constexpr int kFwdTileBits = 12;
 constexpr int kGradTileBits = 11;
 constexpr int kLowBits = 3;
+// process-wide tile shape of new window plans (qfb_ucc_tiles)
+int g_win_fwd = kFwdTileBits, g_win_grad = kGradTileBits, g_win_low = kLowBits;
 
 static qfbw::Window make_window(uint64_t U, int n, int b, int L) {
     qfbw::Window w{};
@@ -1019,8 +1028,8 @@ static int upload_plan(WinPlan *pl) {
 static int build_fwd_plan(qfb_prog_s *p, int n, WinPlan **out) {
     WinPlan *pl = new WinPlan;
     pl->nqubit = n;
-    pl->b = std::min(kFwdTileBits, n);
-    pl->L = std::min(kLowBits, pl->b);
+    pl->b = std::min(g_win_fwd, n);
+    pl->L = std::min(g_win_low, pl->b);
     pl->nt = 1;
     const uint64_t low = (1ull << pl->L) - 1ull;
     const int room = pl->b - pl->L;
@@ -1081,8 +1090,8 @@ static int build_fwd_plan(qfb_prog_s *p, int n, WinPlan **out) {
 static int build_grad_plan(qfb_prog_s *kp, const qfb_prog_s *up, int n, WinPlan **out) {
     WinPlan *pl = new WinPlan;
     pl->nqubit = n;
-    pl->b = std::min(kGradTileBits, n);
-    pl->L = std::min(kLowBits, pl->b);
+    pl->b = std::min(g_win_grad, n);
+    pl->L = std::min(g_win_low, pl->b);
     pl->nt = 2;
     const uint64_t low = (1ull << pl->L) - 1ull;
     const int room = pl->b - pl->L;
@@ -1205,14 +1214,24 @@ static int build_grad_plan(qfb_prog_s *kp, const qfb_prog_s *up, int n, WinPlan 
     return QFB_OK;
 }
 
+static bool plan_shape_is(const WinPlan *pl, int bits, int n) {
+    const int b = std::min(bits, n);
+    return pl->b == b && pl->L == std::min(g_win_low, b);
+}
+
 static int ensure_plans(qfb_prog_s *p, int n, bool fwd, const qfb_prog_s *up = nullptr) {
     if (n < 1 || n > 40) return fail(QFB_EINVAL, "window plan: bad qubit count %d", n);
     int rc = QFB_OK;
+    if (fwd && p->fwd_plan[n] && !plan_shape_is(p->fwd_plan[n], g_win_fwd, n)) {
+        p->retired.push_back(p->fwd_plan[n]);
+        p->fwd_plan[n] = nullptr;
+    }
     if (fwd && !p->fwd_plan[n]) rc = build_fwd_plan(p, n, &p->fwd_plan[n]);
-    if (rc == QFB_OK && up && p->grad_plan_u[n] != up) {
+    if (rc == QFB_OK && up &&
+        (p->grad_plan_u[n] != up ||
+         (p->grad_plan[n] && !plan_shape_is(p->grad_plan[n], g_win_grad, n)))) {
         if (p->grad_plan[n]) {
-            dev_free(p->grad_plan[n]->blob);
-            delete p->grad_plan[n];
+            p->retired.push_back(p->grad_plan[n]);
             p->grad_plan[n] = nullptr;
         }
         rc = build_grad_plan(p, up, n, &p->grad_plan[n]);
@@ -2841,6 +2860,17 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
         u->splan = std::make_shared<SectorPlan>(std::move(splan));
     }
     *out = u;
+    return QFB_OK;
+}
+
+int qfb_ucc_tiles(int fwd_bits, int grad_bits, int low_bits) {
+    if (low_bits < 0 || low_bits > 6 || fwd_bits < low_bits + 2 || fwd_bits > 13 ||
+        grad_bits < low_bits + 2 || grad_bits > 12)
+        return fail(QFB_EINVAL, "qfb_ucc_tiles: (%d, %d, %d) outside fwd in [low+2, 13], "
+                    "grad in [low+2, 12], low in [0, 6]", fwd_bits, grad_bits, low_bits);
+    g_win_fwd = fwd_bits;
+    g_win_grad = grad_bits;
+    g_win_low = low_bits;
     return QFB_OK;
 }
 
