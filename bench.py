@@ -425,7 +425,8 @@ def run_adapt(a, local):
             "dtype": "c128", "data": "synthetic",
             "config": {"workload": f"GSD pool gradients, {2 * norb} qubits ({norb} orbitals, "
                                    f"{norb} electrons), 12-operator dUCC state",
-                       "pool_ops": len(pool), "pool_strings": int(eng._pool_sum.nterms),
+                       "pool_ops": len(pool), "pool_strings": int(eng._pool_program().nstrings),
+                       "evaluator_path": eng.evaluator(1).path,
                        "hamiltonian_terms": len(mol.hamiltonian)},
             "gpu_launches": launches, "pool_compile_s": compile_s,
             "max_abs_gradient": float(np.max(np.abs(g))),
@@ -676,7 +677,14 @@ def main():
     stages = ["reference", "U(t) program", "H psi + energy", "gradient sweep"]
     N = 1 << (2 * a.norb)
     compact = ev.path == 2
-    if compact:
+    if ev.path == 3:
+        # slot-minor compact states in global memory: a step record reads and
+        # writes the pairs it touches; stage totals are reported, per launch
+        # the mean over the stage's launches
+        nsec, nnz = ev.sector_size, ev.h_rows
+        per_launch_bytes = {1: 32 * nsec * a.batch, 2: (12 * nnz / max(1, a.batch) + 32 * nsec) * a.batch,
+                            3: 64 * nsec * a.batch}
+    elif compact:
         # one CTA per parameter set, states in shared memory: the bytes each
         # kernel must move per launch are the save buffer it writes / reads
         # and (H) the H rows, streamed once per parameter set
@@ -698,7 +706,9 @@ def main():
     avg_ms = st_ms[dom] / nl
     hbm, src = peaks()
     achieved = per_launch_bytes[dom] / (avg_ms / 1000.0) / 1e9
-    if compact:
+    if ev.path == 3:
+        kernel = {1: "k_cg_step (forward)", 2: "k_cg_h_rows", 3: "k_cg_step (sweep)"}[dom]
+    elif compact:
         kernel = {1: "k_sector_forward", 2: "k_sector_h", 3: "k_sector_sweep"}[dom]
     else:
         kernel = {1: "k_window<1>", 2: "k_sum_apply_sector" if ev.sector_size else "k_sum_apply_tiled",
@@ -710,8 +720,9 @@ def main():
             "stages_ms": {stages[k]: st_ms[k] for k in range(4)},
             "stages_launches": {stages[k]: int(st_n[k]) for k in range(4)},
             "evaluator_path": {0: "full space", 1: "full space, sigma on the sector",
-                               2: "compact sector in shared memory"}[ev.path]}
-    if compact:
+                               2: "compact sector in shared memory",
+                               3: "compact sector in global memory"}[ev.path]}
+    if ev.path in (2, 3):
         roof["sector_amplitudes"] = ev.sector_size
         roof["h_row_entries"] = ev.h_rows
 

@@ -1,0 +1,231 @@
+// Compact particle-number sector evaluator with the states in global memory.
+//
+// For sectors too large for one CTA's shared memory (18-26 qubits at half
+// filling: 15,876 to 2.9 M amplitudes) psi and sigma of all B parameter sets
+// are stored state-minor, amplitude i of slot s at [i * B + s], so the B
+// slots of one amplitude are contiguous and every access below is coalesced
+// across slots.  A program step is one launch over (pair, slot): the pairs
+// are the alpha-list x beta-list products of the step's record (the same
+// records as the shared-memory path, qfb_sector.cuh), read from global
+// memory.  sigma = H psi runs one warp per output amplitude with the lanes
+// over slots, from the sector's H rows (an evaluator whose rows would exceed
+// their memory budget keeps full-space states instead).
+#pragma once
+
+#include <cstdint>
+
+#include "qfb_sector.cuh"
+
+namespace qfbg {
+
+using qfbs::RHead;
+using qfbs::RPat;
+using qfbs::SEntry;
+
+struct GLaunch {
+    int nsec, nbeta, B;
+    int spw;                   // slots per warp: min(32, B rounded up to a power of two)
+    double2 *psi, *sig;        // [nsec][B]
+    const double *params;      // [B][nparam]
+    int nparam;
+};
+
+__device__ __forceinline__ double2 g_cadd(double2 a, double2 b) {
+    return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 g_cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 g_cjmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+
+// One step record over (pair, slot): lane l of a warp takes slot
+// group * spw + l % spw and pair sub-index l / spw.  ROT rotates psi (and
+// sigma when TWO) by sign * gamma * theta_slot; IP accumulates <sigma|K|psi>
+// per slot into partial[(row * B + s) * gridDim.x + blockIdx.x].
+template <bool ROT, bool IP, bool TWO>
+__global__ void __launch_bounds__(256) k_cg_step(GLaunch L, const uint4 *__restrict__ rec,
+                                                 int param, int sign, int row,
+                                                 double2 *__restrict__ partial) {
+    __shared__ double2 s_acc[8][32];
+    const RHead hd = *reinterpret_cast<const RHead *>(rec);
+    const RPat *pats = reinterpret_cast<const RPat *>(rec + 1);
+    const SEntry *ents = reinterpret_cast<const SEntry *>(rec);
+    const int np = hd.npf & 255;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int per = 32 / L.spw;  // pairs per warp at a time
+    const int s = blockIdx.y * L.spw + (lane % L.spw);
+    const bool live = s < L.B;
+    double cs = 1.0, sn = 0.0;
+    if (ROT && live) sincos((double)sign * hd.gamma * L.params[(size_t)s * L.nparam + param], &sn, &cs);
+    double2 acc = make_double2(0.0, 0.0);
+    const int sub = lane / L.spw;
+    const int stride = gridDim.x * nwarp * per;
+    for (int p = 0; p < np; ++p) {
+        const RPat pt = pats[p];
+        const int total = (int)pt.na * (int)pt.nb;
+        for (int q = (blockIdx.x * nwarp + warp) * per + sub; q < total; q += stride) {
+            const int ai = pt.inv ? (int)__umulhi((uint32_t)q, pt.inv) : q;
+            const int bi = q - ai * (int)pt.nb;
+            const SEntry ea = ents[pt.a0 + ai], eb = ents[pt.b0 + bi];
+            if (!live) continue;
+            const size_t i0 = ((size_t)ea.r0 * L.nbeta + eb.r0) * L.B + s;
+            const size_t i1 = ((size_t)ea.r1 * L.nbeta + eb.r1) * L.B + s;
+            const bool neg = (ea.s ^ eb.s) & 1u;
+            double2 v0 = L.psi[i0], v1 = L.psi[i1];
+            if (IP) {
+                const double2 w0 = L.sig[i0], w1 = L.sig[i1];
+                const double2 t = g_cadd(g_cjmul(w0, g_cmul(pt.hn, v1)), g_cjmul(w1, g_cmul(pt.gn, v0)));
+                const double gs = neg ? -hd.gamma : hd.gamma;
+                acc.x += gs * t.x;
+                acc.y += gs * t.y;
+            }
+            if (ROT) {
+                const double ss = neg ? -sn : sn;
+                const double2 a = g_cmul(pt.hn, v1), b = g_cmul(pt.gn, v0);
+                L.psi[i0] = make_double2(cs * v0.x + ss * a.x, cs * v0.y + ss * a.y);
+                L.psi[i1] = make_double2(cs * v1.x + ss * b.x, cs * v1.y + ss * b.y);
+                if (TWO) {
+                    const double2 w0 = L.sig[i0], w1 = L.sig[i1];
+                    const double2 c = g_cmul(pt.hn, w1), d = g_cmul(pt.gn, w0);
+                    L.sig[i0] = make_double2(cs * w0.x + ss * c.x, cs * w0.y + ss * c.y);
+                    L.sig[i1] = make_double2(cs * w1.x + ss * d.x, cs * w1.y + ss * d.y);
+                }
+            }
+        }
+    }
+    if (!IP) return;
+    // lanes of one slot: l % spw equal; sum over the pair sub-index, then warps
+    for (int o = L.spw; o < 32; o <<= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+    }
+    if (lane < L.spw) s_acc[warp][lane] = acc;
+    __syncthreads();
+    if (threadIdx.x < L.spw) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < nwarp; ++w) t = g_cadd(t, s_acc[w][threadIdx.x]);
+        const int ss = blockIdx.y * L.spw + threadIdx.x;
+        if (ss < L.B) partial[((size_t)row * L.B + ss) * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// Inner products of many independent records in one launch (blockIdx.z =
+// record; ADAPT pool operators): partial[(row * B + s) * gridDim.x + blockIdx.x].
+__global__ void __launch_bounds__(256) k_cg_ip_many(GLaunch L, const uint4 *__restrict__ recs,
+                                                    const int2 *__restrict__ span,
+                                                    double2 *__restrict__ partial) {
+    __shared__ double2 s_acc[8][32];
+    const uint4 *rec = recs + span[blockIdx.z].x;
+    const RHead hd = *reinterpret_cast<const RHead *>(rec);
+    const RPat *pats = reinterpret_cast<const RPat *>(rec + 1);
+    const SEntry *ents = reinterpret_cast<const SEntry *>(rec);
+    const int np = hd.npf & 255;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int per = 32 / L.spw, sub = lane / L.spw;
+    const int s = blockIdx.y * L.spw + (lane % L.spw);
+    const bool live = s < L.B;
+    const int stride = gridDim.x * nwarp * per;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int p = 0; p < np; ++p) {
+        const RPat pt = pats[p];
+        const int total = (int)pt.na * (int)pt.nb;
+        for (int q = (blockIdx.x * nwarp + warp) * per + sub; q < total; q += stride) {
+            const int ai = pt.inv ? (int)__umulhi((uint32_t)q, pt.inv) : q;
+            const int bi = q - ai * (int)pt.nb;
+            const SEntry ea = ents[pt.a0 + ai], eb = ents[pt.b0 + bi];
+            if (!live) continue;
+            const size_t i0 = ((size_t)ea.r0 * L.nbeta + eb.r0) * L.B + s;
+            const size_t i1 = ((size_t)ea.r1 * L.nbeta + eb.r1) * L.B + s;
+            const double2 v0 = L.psi[i0], v1 = L.psi[i1], w0 = L.sig[i0], w1 = L.sig[i1];
+            const double2 t = g_cadd(g_cjmul(w0, g_cmul(pt.hn, v1)), g_cjmul(w1, g_cmul(pt.gn, v0)));
+            const double gs = ((ea.s ^ eb.s) & 1u) ? -hd.gamma : hd.gamma;
+            acc.x += gs * t.x;
+            acc.y += gs * t.y;
+        }
+    }
+    for (int o = L.spw; o < 32; o <<= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+    }
+    if (lane < L.spw) s_acc[warp][lane] = acc;
+    __syncthreads();
+    if (threadIdx.x < L.spw) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < nwarp; ++w) t = g_cadd(t, s_acc[w][threadIdx.x]);
+        const int ss = blockIdx.y * L.spw + threadIdx.x;
+        if (ss < L.B) partial[((size_t)hd.row * L.B + ss) * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// psi = |ref> in every slot (psi zeroed beforehand).
+__global__ void k_cg_ref(GLaunch L, int ref_i) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < L.B) L.psi[(size_t)ref_i * L.B + s] = make_double2(1.0, 0.0);
+}
+
+// sigma = H psi from the sector's H rows: one warp per output row i, lanes
+// over (slot, entry sub-index) as in k_cg_step; energy partials per slot.
+// epart[s * gridDim.x + blockIdx.x] = sum over this block's rows of conj(psi) sigma.
+template <bool REAL>
+__global__ void __launch_bounds__(256) k_cg_h_rows(GLaunch L, const int32_t *__restrict__ rowptr,
+                                                   const uint32_t *__restrict__ col,
+                                                   const double *__restrict__ val_r,
+                                                   const double2 *__restrict__ val_c,
+                                                   double2 *__restrict__ epart) {
+    __shared__ double2 s_e[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int per = 32 / L.spw, sub = lane / L.spw;
+    const int s = blockIdx.y * L.spw + (lane % L.spw);
+    const bool live = s < L.B;
+    double2 en = make_double2(0.0, 0.0);
+    for (int i = blockIdx.x * nwarp + warp; i < L.nsec; i += gridDim.x * nwarp) {
+        double2 acc = make_double2(0.0, 0.0);
+        const int e1 = rowptr[i + 1];
+        for (int e = rowptr[i] + sub; e < e1; e += per) {
+            const uint32_t c = __ldg(&col[e]);
+            const double2 x = live ? L.psi[(size_t)c * L.B + s] : make_double2(0.0, 0.0);
+            if (REAL) {
+                const double f = __ldg(&val_r[e]);
+                acc.x += f * x.x;
+                acc.y += f * x.y;
+            } else {
+                acc = g_cadd(acc, g_cmul(__ldg(&val_c[e]), x));
+            }
+        }
+        for (int o = L.spw; o < 32; o <<= 1) {
+            acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+        }
+        if (sub == 0 && live) {
+            L.sig[(size_t)i * L.B + s] = acc;
+            en = g_cadd(en, g_cjmul(L.psi[(size_t)i * L.B + s], acc));
+        }
+    }
+    if (lane < L.spw) s_e[warp][lane] = en;
+    __syncthreads();
+    if (threadIdx.x < L.spw) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < nwarp; ++w) t = g_cadd(t, s_e[w][threadIdx.x]);
+        const int ss = blockIdx.y * L.spw + threadIdx.x;
+        if (ss < L.B) epart[(size_t)ss * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// energy[s] = Re sum_k epart[s * n + k]  (one warp per slot, fixed order)
+__global__ void k_cg_energy(const double2 *__restrict__ epart, int n, int B,
+                            double *__restrict__ energy) {
+    const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (s >= B) return;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int k = lane; k < n; k += 32) acc = g_cadd(acc, epart[(size_t)s * n + k]);
+    for (int o = 16; o > 0; o >>= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+    }
+    if (lane == 0) energy[s] = acc.x;
+}
+
+}  // namespace qfbg

@@ -43,6 +43,7 @@
 #include <vector>
 
 #include "qfb_common.cuh"
+#include "qfb_csec.cuh"
 #include "qfb_sector.cuh"
 #include "qfb_window.cuh"
 
@@ -2263,14 +2264,15 @@ static bool sector_steps(const SectorPlan &sp, const qfb_prog_s *p, int n,
 
 // Append one record (header, patterns, their lists) to a stream; false when
 // it outgrows one 16-byte word per thread or 16-bit list offsets.
-static bool push_record(StreamHost &S, const CStep &cs, int flags, int row) {
+static bool push_record(StreamHost &S, const CStep &cs, int flags, int row,
+                        int max_words = kSectorThreads) {
     const int np = (int)cs.pats.size();
     if (np > 255) return false;
     size_t nent = 0;
     for (const auto &pt : cs.pats) nent += pt.a.size() + pt.b.size();
     const size_t bytes = sizeof(qfbs::RHead) + np * sizeof(qfbs::RPat) + nent * sizeof(qfbs::SEntry);
     const int words = (int)((bytes + 15) / 16);
-    if (words > kSectorThreads) return false;
+    if (words > max_words) return false;
     std::vector<uint4> w((size_t)words, make_uint4(0, 0, 0, 0));
     char *base = (char *)w.data();
     qfbs::RHead hd;
@@ -2308,7 +2310,8 @@ static bool push_record(StreamHost &S, const CStep &cs, int flags, int row) {
 // outside the Givens form, a sector too large for shared memory, ranks that
 // do not fit 16 bits, a step record larger than the block).
 static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_prog_s *kp,
-                              const qfb_prog_s *up, int n, uint64_t ref) {
+                              const qfb_prog_s *up, int n, uint64_t ref, bool shared = true) {
+    const int mw = shared ? kSectorThreads : (1 << 30);
     const uint64_t A = 0x5555555555555555ull;
     const uint64_t all = (1ull << n) - 1ull;
     sp.na_orb = (n + 1) / 2;
@@ -2337,12 +2340,13 @@ static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_pr
     sp.nbeta = (int)sp.bdet.size();
     if (sp.nalpha == 0 || sp.nbeta == 0 || sp.nalpha > 65535 || sp.nbeta > 65535) return false;
     const size_t nsec = (size_t)sp.nalpha * sp.nbeta;
-    if (nsec * 2 * sizeof(double2) > kSectorSmemMax) return false;
+    if (shared && nsec * 2 * sizeof(double2) > kSectorSmemMax) return false;
+    if (nsec >= (1ull << 31)) return false;
     sp.nsec = (int)nsec;
     sp.ref_i = sp.arank[pext_parity_bits(ref, 0, n)] * sp.nbeta + sp.brank[pext_parity_bits(ref, 1, n)];
     if (!sector_steps(sp, fp, n, sp.fsteps)) return false;
     for (const CStep &cs : sp.fsteps)
-        if (!push_record(sp.fwd, cs, qfbs::R_ROT, -1)) return false;
+        if (!push_record(sp.fwd, cs, qfbs::R_ROT, -1, mw)) return false;
     if (kp) {
         if (!sector_steps(sp, kp, n, sp.ksteps)) return false;
         if (!sector_steps(sp, up, n, sp.usteps)) return false;
@@ -2358,17 +2362,19 @@ static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_pr
             const int s0 = kp->p_step0[mu], s1 = kp->p_step1[mu];
             if (sp.fused) {
                 const int fl = mu > 0 ? (qfbs::R_ROT | qfbs::R_IP | qfbs::R_TWO) : qfbs::R_IP;
-                if (!push_record(sp.sweep, sp.ksteps[s0], fl, s0)) return false;
+                if (!push_record(sp.sweep, sp.ksteps[s0], fl, s0, mw)) return false;
                 continue;
             }
             for (int s = s0; s >= 0 && s < s1; ++s)
-                if (!push_record(sp.sweep, sp.ksteps[s], qfbs::R_IP, s)) return false;
+                if (!push_record(sp.sweep, sp.ksteps[s], qfbs::R_IP, s, mw)) return false;
             if (mu == 0) break;
             const int u0 = up->p_step0[mu], u1 = up->p_step1[mu];
             for (int s = u0; u0 >= 0 && s < u1; ++s)
-                if (!push_record(sp.sweep, sp.usteps[s], qfbs::R_ROT | qfbs::R_TWO, -1)) return false;
+                if (!push_record(sp.sweep, sp.usteps[s], qfbs::R_ROT | qfbs::R_TWO, -1, mw))
+                    return false;
         }
     }
+    if (!shared) return true;
     const size_t ring = 3 * (size_t)std::max(sp.fwd.maxw, sp.sweep.maxw) * 16;
     const size_t ang = sizeof(double2) * std::max(sp.fwd.span.size(), sp.sweep.span.size());
     if (nsec * 2 * sizeof(double2) + ang + ring > kSectorSmemMax) return false;
@@ -2402,7 +2408,17 @@ struct qfb_ucc_s {
     void *sec = nullptr;  // uint32_t (nqubit <= 32) or uint64_t indices
     SecGroup *sgroups = nullptr;
     int nsgroups = 0;
-    std::shared_ptr<SectorPlan> splan;  // compact path: strings and ranks of the sector
+    std::shared_ptr<SectorPlan> splan;  // compact paths: strings, ranks and step records
+    // compact sector in global memory (qfb_csec.cuh)
+    int gsec = 0;
+    qfbg::GLaunch GL{};
+    const uint4 *g_frec = nullptr, *g_srec = nullptr;  // device copies of the record streams
+    unsigned g_sgrid = 1, g_hgrid = 1, g_ygrid = 1;
+    double2 *g_epart = nullptr;
+    const int32_t *g_rowptr = nullptr;
+    const uint32_t *g_col = nullptr;
+    const double *g_vr = nullptr;
+    const double2 *g_vc = nullptr;
     // ADAPT pool (qfb_ucc_set_pool): 2 Re <sigma|K_k|psi> for every pool operator k
     const qfb_prog_s *pool = nullptr;
     int npool = 0;
@@ -2469,8 +2485,13 @@ static int sector_rows_interleave(const std::vector<int32_t> &rowptr, int64_t nn
     return QFB_OK;
 }
 
-// Device copies of a compact plan and the H rows on its sector.
-static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> &sg) {
+constexpr double kRowsBudget = 8e9;  // bytes of H rows a global-memory sector path may hold
+
+// Device copies of a compact plan and the H rows on its sector (global:
+// the states live in global memory; QFB_ENOMEM when the rows exceed their
+// budget).
+static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> &sg,
+                         bool global = false) {
     const int nsec = sp.nsec;
     std::vector<uint64_t> det((size_t)nsec);
     for (int ra = 0; ra < sp.nalpha; ++ra)
@@ -2533,6 +2554,8 @@ static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> 
     u->nnz = nnz;
     bool real = true;
     for (const SecGroup &g : sg) real = real && g.real;
+    if (global && (double)nnz * (real ? 12.0 : 20.0) > kRowsBudget)
+        return fail(QFB_ENOMEM, "sector H rows: %lld entries exceed the budget", (long long)nnz);
     const size_t o_rp = 0;
     size_t coff = ((sizeof(int32_t) * (nsec + 1)) + 255) & ~(size_t)255;
     const size_t o_col = coff;
@@ -2554,9 +2577,20 @@ static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> 
                                             nullptr, d_col, d_vr, d_vc);
     QFB_LAUNCHED();
     QFB_CUDA(cudaStreamSynchronize(t_stream));
-    rc = sector_rows_interleave(rowptr, nnz, d_col, real ? (void *)d_vr : (void *)d_vc,
-                                real ? sizeof(double) : sizeof(double2));
-    if (rc) return rc;
+    if (!global) {
+        rc = sector_rows_interleave(rowptr, nnz, d_col, real ? (void *)d_vr : (void *)d_vc,
+                                    real ? sizeof(double) : sizeof(double2));
+        if (rc) return rc;
+    }
+    if (global) {
+        u->g_frec = (const uint4 *)(base + o_fr);
+        u->g_srec = (const uint4 *)(base + o_sr);
+        u->g_rowptr = d_rp;
+        u->g_col = d_col;
+        u->g_vr = d_vr;
+        u->g_vc = d_vc;
+        return QFB_OK;
+    }
     qfbs::SLaunch &L = u->SL;
     L.nsec = nsec;
     L.nbeta = sp.nbeta;
@@ -2639,8 +2673,94 @@ static int ucc_stage_compact(qfb_ucc u, int stage, int with_grad) {
     return QFB_OK;
 }
 
+// Pairs of the largest record of a stream (grid sizing of the global path).
+static int64_t stream_max_pairs(const StreamHost &S) {
+    int64_t most = 1;
+    for (const int2 &sp : S.span) {
+        const char *rec = (const char *)&S.rec[sp.x];
+        qfbs::RHead hd;
+        std::memcpy(&hd, rec, sizeof(hd));
+        int64_t pairs = 0;
+        for (int p = 0; p < (hd.npf & 255); ++p) {
+            qfbs::RPat pt;
+            std::memcpy(&pt, rec + sizeof(qfbs::RHead) + p * sizeof(qfbs::RPat), sizeof(pt));
+            pairs += (int64_t)pt.na * pt.nb;
+        }
+        most = std::max(most, pairs);
+    }
+    return most;
+}
+
+static unsigned global_grid(int64_t pairs, int spw) {
+    const int64_t per_block = 8 * (32 / spw);  // pairs one block covers per sweep of its warps
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(2048, (pairs + 2 * per_block - 1) /
+                                                                     (2 * per_block)));
+}
+
+// Compact sector in global memory: stage 0 the reference, 1 the forward
+// records, 2 sigma = H psi and the energy, 3 the sweep records.
+static int ucc_stage_global(qfb_ucc u, int stage, int with_grad) {
+    const qfbg::GLaunch &L = u->GL;
+    const SectorPlan &sp = *u->splan;
+    const dim3 grid(u->g_sgrid, u->g_ygrid);
+    switch (stage) {
+        case 0:
+            QFB_CUDA(cudaMemsetAsync(L.psi, 0, sizeof(double2) * (size_t)L.nsec * L.B, t_stream));
+            qfbg::k_cg_ref<<<(L.B + 127) / 128, 128, 0, t_stream>>>(L, sp.ref_i);
+            QFB_LAUNCHED();
+            break;
+        case 1:
+            for (size_t r = 0; r < sp.fwd.span.size(); ++r) {
+                qfbg::k_cg_step<true, false, false><<<grid, 256, 0, t_stream>>>(
+                    L, u->g_frec + sp.fwd.span[r].x, sp.fwd.param[r], 1, -1, nullptr);
+                QFB_LAUNCHED();
+            }
+            break;
+        case 2: {
+            const dim3 hg(u->g_hgrid, u->g_ygrid);
+            if (u->g_vc)
+                qfbg::k_cg_h_rows<false><<<hg, 256, 0, t_stream>>>(L, u->g_rowptr, u->g_col, nullptr,
+                                                                  u->g_vc, u->g_epart);
+            else
+                qfbg::k_cg_h_rows<true><<<hg, 256, 0, t_stream>>>(L, u->g_rowptr, u->g_col, u->g_vr,
+                                                                 nullptr, u->g_epart);
+            QFB_LAUNCHED();
+            qfbg::k_cg_energy<<<(L.B + 7) / 8, 256, 0, t_stream>>>(u->g_epart, (int)u->g_hgrid, L.B,
+                                                                  u->energy);
+            QFB_LAUNCHED();
+            break;
+        }
+        default: {
+            if (!(with_grad && u->grad && u->nparam > 0)) break;
+            for (size_t r = 0; r < sp.sweep.span.size(); ++r) {
+                qfbs::RHead hd;
+                std::memcpy(&hd, &sp.sweep.rec[sp.sweep.span[r].x], sizeof(hd));
+                const int fl = hd.npf >> 8;
+                const uint4 *rec = u->g_srec + sp.sweep.span[r].x;
+                const int par = sp.sweep.param[r];
+                if (fl == (qfbs::R_ROT | qfbs::R_IP | qfbs::R_TWO))
+                    qfbg::k_cg_step<true, true, true><<<grid, 256, 0, t_stream>>>(L, rec, par, -1, hd.row,
+                                                                                 u->gpart);
+                else if (fl == qfbs::R_IP)
+                    qfbg::k_cg_step<false, true, false><<<grid, 256, 0, t_stream>>>(L, rec, par, -1,
+                                                                                   hd.row, u->gpart);
+                else
+                    qfbg::k_cg_step<true, false, true><<<grid, 256, 0, t_stream>>>(L, rec, par, -1, -1,
+                                                                                  nullptr);
+                QFB_LAUNCHED();
+            }
+            k_grad_final<<<dim3(u->nparam, L.B), 128, 0, t_stream>>>(u->gpart, u->psteps, u->gchunks,
+                                                                   u->gradv);
+            QFB_LAUNCHED();
+            break;
+        }
+    }
+    return QFB_OK;
+}
+
 static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
     if (u->compact) return ucc_stage_compact(u, stage, with_grad);
+    if (u->gsec) return ucc_stage_global(u, stage, with_grad);
     const int B = u->nbatch;
     int rc = QFB_OK;
     switch (stage) {
@@ -2693,7 +2813,12 @@ static int ucc_pool_stage(qfb_ucc u) {
     if (!u->pool) return fail(QFB_EINVAL, "qfb_ucc_run: no pool set (qfb_ucc_set_pool)");
     const int B = u->nbatch;
     unsigned chunks = u->pchunks;
-    if (u->compact) {
+    if (u->gsec) {
+        const dim3 grid(u->pchunks, u->g_ygrid, (unsigned)u->pstream.n);
+        qfbg::k_cg_ip_many<<<grid, 256, 0, t_stream>>>(u->GL, u->pstream.rec, u->pstream.span,
+                                                       u->ppart);
+        QFB_LAUNCHED();
+    } else if (u->compact) {
         qfbs::SLaunch L = u->SL;
         L.partial = u->ppart;
         const int sm = sm_count();
@@ -2727,8 +2852,21 @@ static int ucc_enqueue(qfb_ucc u, int mode) {
 
 extern "C" {
 
+static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham,
+                           int nqubit, uint64_t ref_index, int nbatch, qfb_ucc *out,
+                           bool allow_global);
+
 int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, int nqubit,
                    uint64_t ref_index, int nbatch, qfb_ucc *out) {
+    int rc = ucc_create_impl(fprog, gprog, uprog, ham, nqubit, ref_index, nbatch, out, true);
+    if (rc == QFB_ENOMEM && out && !*out)  // sector rows over budget (or no room): full space
+        rc = ucc_create_impl(fprog, gprog, uprog, ham, nqubit, ref_index, nbatch, out, false);
+    return rc;
+}
+
+static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham,
+                           int nqubit, uint64_t ref_index, int nbatch, qfb_ucc *out,
+                           bool allow_global) {
     if (!out) return fail(QFB_EINVAL, "qfb_ucc_create: null output");
     *out = nullptr;
     if (!fprog || !ham) return fail(QFB_EINVAL, "qfb_ucc_create: null program or Hamiltonian");
@@ -2768,15 +2906,31 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
         if (sgroups.empty()) sector.clear();
     }
     SectorPlan splan;
-    const bool compact = g_ucc_compact && !sector.empty() &&
-                         build_sector_plan(splan, fprog, gprog, uprog, nqubit, ref_index);
+    bool compact = false, gsec = false;
+    if (g_ucc_compact && !sector.empty()) {
+        if (g_ucc_compact == 1)
+            compact = build_sector_plan(splan, fprog, gprog, uprog, nqubit, ref_index, true);
+        if (!compact && allow_global) {
+            SectorPlan gp;
+            if (build_sector_plan(gp, fprog, gprog, uprog, nqubit, ref_index, false)) {
+                splan = std::move(gp);
+                gsec = true;
+            }
+        }
+    }
     if (compact) {
         int src = sector_smem_attr();
         if (src) return src;
-        sector.clear();
     }
+    if (compact || gsec) sector.clear();
+    const int spw = gsec ? (int)std::min<int64_t>(32, 1ll << (int)std::ceil(std::log2((double)nbatch))) : 32;
+    const unsigned sgrid = gsec ? global_grid(std::max(stream_max_pairs(splan.fwd),
+                                                       stream_max_pairs(splan.sweep)), spw)
+                                : 1;
+    const unsigned hgrid = gsec ? (unsigned)std::min<int64_t>(1024, (splan.nsec + 7) / 8) : 1;
     qfb_ucc u = new qfb_ucc_s;
     u->compact = compact ? 1 : 0;
+    u->gsec = gsec ? 1 : 0;
     u->fwd = fprog;
     u->grad = gprog;
     u->unrot = uprog;
@@ -2788,10 +2942,11 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     u->ref = ref_index;
     u->vchunks = grid_for(u->nbasis, 256, 2);
     if (u->vchunks * (unsigned)nbatch > 65535u) u->vchunks = std::max(1u, 65535u / nbatch);
-    u->gchunks = compact ? kSectorThreads / 32 : (gprog ? grad_chunks(gprog, nqubit, nbatch) : 1);
+    u->gchunks = compact ? kSectorThreads / 32
+                         : gsec ? sgrid : (gprog ? grad_chunks(gprog, nqubit, nbatch) : 1);
     const size_t B = nbatch, M = std::max(u->nparam, 1);
     const size_t nsteps = gprog ? std::max<size_t>(gprog->h_steps.size(), 1) : 1;
-    const size_t b_state = compact ? 16 : sizeof(double2) * u->nbasis * B;
+    const size_t b_state = (compact || gsec) ? 16 : sizeof(double2) * u->nbasis * B;
     size_t off = 0;
     auto take = [&](size_t bytes) {
         size_t o = off;
@@ -2808,6 +2963,9 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     const size_t o_sec = take(idx_bytes * std::max<size_t>(sector.size(), 1));
     const size_t o_sg = take(sizeof(SecGroup) * std::max<size_t>(sgroups.size(), 1));
     const size_t o_save = take(compact ? sizeof(double2) * 2 * (size_t)splan.nsec * B : 16);
+    const size_t b_cstate = gsec ? sizeof(double2) * (size_t)splan.nsec * B : 16;
+    const size_t o_cpsi = take(b_cstate), o_csig = take(b_cstate);
+    const size_t o_epart = take(gsec ? sizeof(double2) * B * hgrid : 16);
     int rc = dev_alloc(&u->blob, off);
     if (rc) {
         delete u;
@@ -2825,6 +2983,21 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
     u->psteps = (int2 *)(base + o_ps);
     u->nsec = compact ? (int64_t)splan.nsec : (int64_t)sector.size();
     u->SL.save = (double2 *)(base + o_save);
+    if (gsec) {
+        u->nsec = splan.nsec;
+        u->GL.nsec = splan.nsec;
+        u->GL.nbeta = splan.nbeta;
+        u->GL.B = nbatch;
+        u->GL.spw = spw;
+        u->GL.psi = (double2 *)(base + o_cpsi);
+        u->GL.sig = (double2 *)(base + o_csig);
+        u->GL.params = u->params;
+        u->GL.nparam = u->nparam;
+        u->g_sgrid = sgrid;
+        u->g_hgrid = hgrid;
+        u->g_ygrid = (unsigned)((nbatch + spw - 1) / spw);
+        u->g_epart = (double2 *)(base + o_epart);
+    }
     u->sec = base + o_sec;
     u->sgroups = (SecGroup *)(base + o_sg);
     u->nsgroups = (int)sgroups.size();
@@ -2851,8 +3024,8 @@ int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, 
         delete u;
         return cuda_fail(e, "qfb_ucc_create");
     }
-    if (compact) {
-        rc = sector_upload(u, splan, sgroups);
+    if (compact || gsec) {
+        rc = sector_upload(u, splan, sgroups, gsec);
         if (rc) {
             qfb_ucc_destroy(u);
             return rc;
@@ -2875,7 +3048,7 @@ int qfb_ucc_tiles(int fwd_bits, int grad_bits, int low_bits) {
 }
 
 int qfb_ucc_config(int compact) {
-    if (compact != 0 && compact != 1) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
+    if (compact < 0 || compact > 2) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
     g_ucc_compact = compact;
     return QFB_OK;
 }
@@ -2888,7 +3061,7 @@ int qfb_ucc_rows(qfb_ucc u, int64_t *nnz) {
 
 int qfb_ucc_path(qfb_ucc u, int32_t *path) {
     if (!u || !path) return fail(QFB_EINVAL, "qfb_ucc_path: null argument");
-    *path = u->compact ? 2 : (u->nsec > 0 ? 1 : 0);
+    *path = u->gsec ? 3 : u->compact ? 2 : (u->nsec > 0 ? 1 : 0);
     return QFB_OK;
 }
 
@@ -2923,14 +3096,14 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
     qfbs::SStream ps{};
     StreamHost sh;
     unsigned chunks = 1;
-    if (u->compact) {
+    if (u->compact || u->gsec) {
         std::vector<CStep> cs;
         if (!sector_steps(*u->splan, pool, u->nqubit, cs))
             return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool outside the Givens form on the sector");
         for (size_t k = 0; k < cs.size(); ++k)
-            if (!push_record(sh, cs[k], qfbs::R_IP, (int)k))
+            if (!push_record(sh, cs[k], qfbs::R_IP, (int)k, u->gsec ? (1 << 30) : kSectorThreads))
                 return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool step too large");
-        chunks = kSectorThreads / 32;
+        chunks = u->compact ? kSectorThreads / 32 : global_grid(stream_max_pairs(sh), u->GL.spw);
     } else {
         uint64_t most = 1;
         for (const auto &st : pool->h_steps) {
@@ -2951,7 +3124,7 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
     const size_t o_pg = take(sizeof(double) * (size_t)B * M);
     const size_t o_pp = take(sizeof(double2) * nst * B * chunks);
     const size_t o_pr = take(sizeof(int2) * M);
-    const size_t o_ps = take(u->compact ? 16 : sizeof(StepDev) * nst);
+    const size_t o_ps = take((u->compact || u->gsec) ? 16 : sizeof(StepDev) * nst);
     const size_t o_rec = take(sizeof(uint4) * sh.rec.size());
     const size_t o_sp = take(sizeof(int2) * sh.span.size());
     void *blob = nullptr;
@@ -2964,7 +3137,7 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
     cudaError_t e = cudaMemsetAsync(blob, 0, off, t_stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(base + o_pr, pr.data(), sizeof(int2) * M, cudaMemcpyHostToDevice, t_stream);
-    if (e == cudaSuccess && !u->compact)
+    if (e == cudaSuccess && !u->compact && !u->gsec)
         e = cudaMemcpyAsync(base + o_ps, pool->h_steps.data(), sizeof(StepDev) * nst,
                             cudaMemcpyHostToDevice, t_stream);
     if (e == cudaSuccess && !sh.rec.empty())

@@ -43,8 +43,10 @@ __all__ = ["DUCC", "Evaluator", "evaluator_config", "UCCNVQE", "ADAPTVQE", "ansa
 
 def evaluator_config(compact=True):
     """Process-wide: let evaluators created from now on use the compact
-    sector path (the default) or keep full-space states."""
-    check(lib().qfb_ucc_config(1 if compact else 0), "qfb_ucc_config")
+    sector paths (True, the default), only the global-memory one ("global"),
+    or keep full-space states (False)."""
+    mode = 2 if compact == "global" else (1 if compact else 0)
+    check(lib().qfb_ucc_config(mode), "qfb_ucc_config")
 
 
 class Evaluator:
@@ -77,7 +79,8 @@ class Evaluator:
 
     @property
     def path(self):
-        """0: full space; 1: sigma on the sector; 2: compact sector states."""
+        """0: full space; 1: sigma on the sector; 2: compact sector states in
+        shared memory; 3: compact sector states in global memory."""
         n = ctypes.c_int32()
         check(lib().qfb_ucc_path(self.h, ctypes.byref(n)), "qfb_ucc_path")
         return n.value

@@ -468,3 +468,53 @@ def test_pool_gradients_one_launch_vs_grouped_and_oracle(cuda, compact):
     g_o1 = O.measure_gradient3(10, mol.hf_reference, kops_forward(gsd, tops), P[1], hterms,
                                kops_gradient(gsd, range(len(gsd))))
     assert np.max(np.abs(GB[1] - g_o1)) < G_TOL
+
+
+@pytest.mark.parametrize("B", [1, 3, 40])
+@pytest.mark.parametrize("norb,seed,pool_type", [(4, 11, "SD"), (6, 3, "SD"), (5, 9, "GSD"),
+                                                 (6, 17, "sa_SD")])
+def test_global_sector_path_matches_shared_and_full(cuda, norb, seed, pool_type, B):
+    """Compact sector states in global memory (slot-minor, one launch per
+    step record) against the shared-memory path, the full-space path and the
+    oracle, for slot groups of 1, 4 and 32 lanes."""
+    from qforte_b200.ucc import evaluator_config
+    mol, pool = random_problem(norb, seed, pool_type)
+    tops = list(range(0, len(pool), 1 if len(pool) < 400 else 3))
+    rng = np.random.default_rng(B + norb)
+    P = rng.uniform(-0.1, 0.1, (B, len(tops)))
+    res = {}
+    for mode in (True, "global", False):
+        evaluator_config(mode)
+        try:
+            eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference, pool_type=pool_type)
+            res[mode] = eng.energy_grad(P) + (eng.evaluator(B).path,)
+        finally:
+            evaluator_config(True)
+    E3, G3, path3 = res["global"]
+    E1, G1, path1 = res[False]
+    E2, G2, path2 = res[True]
+    assert path1 in (0, 1) and (pool_type == "sa_SD" or path3 == 3)
+    assert np.max(np.abs(E3 - E1)) < 1e-12 and np.max(np.abs(G3 - G1)) < 1e-11
+    assert np.max(np.abs(E3 - E2)) < 1e-12 and np.max(np.abs(G3 - G2)) < 1e-11
+    if B == 3:
+        hterms = oracle_terms(mol.hamiltonian)
+        kf = kops_forward(pool, tops, pool_type)
+        E_o, _ = O.energy(2 * norb, mol.hf_reference, kf, P[2], hterms)
+        assert abs(E3[2] - E_o) < E_TOL
+
+
+def test_global_sector_pool_gradients(cuda):
+    from qforte_b200.ucc import evaluator_config
+    mol, gsd = random_problem(5, 31, "GSD")
+    rng = np.random.default_rng(3)
+    tops = [int(t) for t in rng.choice(len(gsd), 6, replace=False)]
+    P = rng.uniform(-0.1, 0.1, (2, 6))
+    evaluator_config("global")
+    try:
+        eng = DUCC(mol.hamiltonian, gsd, tops, mol.hf_reference)
+        g = eng.pool_gradients(P)
+        assert eng.evaluator(2).path == 3 and getattr(eng.evaluator(2), "_pool_prog", None) is not None
+    finally:
+        evaluator_config(True)
+    g2 = np.vstack([eng.pool_gradients_grouped(P[b]) for b in range(2)])
+    assert np.max(np.abs(g - g2)) < 1e-12
