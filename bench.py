@@ -505,6 +505,9 @@ def run_serve(a, local):
     for k, (e, g), ts in res:
         by.setdefault(k, 0)
         by[k] += 1
+    # per-problem latency: the client-side submit time to the future's completion
+    # is not kept per request by the server, so report the server's overall
+    # percentiles and the requests per problem
     # sequential baseline: the same requests one at a time (batch 1, one stream)
     nseq = min(len(trace), max(8, len(trace) // 4))
     st1, _, wall1 = served(1, 1, trace[:nseq])

@@ -208,17 +208,20 @@ QFB_API int qfb_ucc_sector(qfb_ucc u, int64_t *nsec);
 /* How the evaluator runs: 0 full space; 1 full-space states with sigma formed
  * on the sector; 2 compact sector states, one CTA per parameter set holding
  * psi and sigma in shared memory (sectors up to 6,400 amplitudes); 3 compact
- * sector states in global memory, slot-minor (larger sectors whose H rows fit
- * 8 GB).  Paths 2 and 3 need every program step in Givens form.  No
- * counterpart in the reference. */
+ * sector states in global memory, slot-minor (larger sectors; sigma from
+ * stored H rows up to 24 GB of them, else from the grouped terms).  Paths 2
+ * and 3 need every program step in Givens form.  No counterpart in the
+ * reference. */
 QFB_API int qfb_ucc_path(qfb_ucc u, int32_t *path);
 /* Entries of the H rows the compact path streams for each parameter set (0
  * on the other paths).  No counterpart in the reference. */
 QFB_API int qfb_ucc_rows(qfb_ucc u, int64_t *nnz);
 /* Process-wide: whether evaluators created from now on may use the compact
  * sector paths (1, the default: shared memory when the sector fits, else
- * global memory), only the global-memory one (2), or neither (0).  No
- * counterpart in the reference. */
+ * global memory), only the global-memory one (2), only the global-memory one
+ * with sigma formed from the grouped terms instead of stored H rows (3; the
+ * rows are over 24 GB beyond ~24 qubits, where this happens by itself), or
+ * neither (0).  No counterpart in the reference. */
 QFB_API int qfb_ucc_config(int compact);
 /* Process-wide tile shape of the full-space windows of evaluators created
  * from now on: fwd_bits qubits per forward tile (default 12, at most 13),

@@ -213,6 +213,92 @@ __global__ void __launch_bounds__(256) k_cg_h_rows(GLaunch L, const int32_t *__r
     }
 }
 
+// Bits 0, 2, 4, ... (odd = 0) or 1, 3, 5, ... (odd = 1) of v, packed.
+__device__ __forceinline__ uint32_t g_pext_parity(uint64_t v, int odd) {
+    uint64_t x = (v >> odd) & 0x5555555555555555ull;
+    x = (x | (x >> 1)) & 0x3333333333333333ull;
+    x = (x | (x >> 2)) & 0x0f0f0f0f0f0f0f0full;
+    x = (x | (x >> 4)) & 0x00ff00ff00ff00ffull;
+    x = (x | (x >> 8)) & 0x0000ffff0000ffffull;
+    x = (x | (x >> 16)) & 0x00000000ffffffffull;
+    return (uint32_t)x;
+}
+
+struct GGroup {  // one x-group of H restricted to the sector (layout of SecGroup)
+    uint64_t x;
+    int32_t begin, end, real;
+    int32_t halves;
+};
+
+struct GTerm {  // one term of a grouped sum (layout of TermDev)
+    uint64_t z;
+    double2 c;
+};
+
+// sigma = H psi without stored rows (sectors whose rows would exceed their
+// budget): one warp per output row i, lanes over (slot, group sub-index);
+// each lane scans its share of the groups, forms f_x(j) for the groups that
+// connect det[i] to j = det[i] ^ x inside the sector and gathers psi at j's
+// sector index (alpha rank * nbeta + beta rank).
+__global__ void __launch_bounds__(256) k_cg_h_groups(GLaunch L, const uint64_t *__restrict__ det,
+                                                     const GGroup *__restrict__ groups, int ngroups,
+                                                     const GTerm *__restrict__ terms,
+                                                     const double2 *__restrict__ rterms,
+                                                     const int32_t *__restrict__ arank,
+                                                     const int32_t *__restrict__ brank,
+                                                     double2 *__restrict__ epart) {
+    __shared__ double2 s_e[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int per = 32 / L.spw, sub = lane / L.spw;
+    const int s = blockIdx.y * L.spw + (lane % L.spw);
+    const bool live = s < L.B;
+    const uint64_t A = 0x5555555555555555ull;
+    double2 en = make_double2(0.0, 0.0);
+    for (int i = blockIdx.x * nwarp + warp; i < L.nsec; i += gridDim.x * nwarp) {
+        const uint64_t k = det[i];
+        double2 acc = make_double2(0.0, 0.0);
+        for (int g = sub; g < ngroups; g += per) {
+            const uint64_t x = __ldg(&groups[g].x);
+            const uint64_t kx = k & x;
+            if ((__popcll(kx & A) | __popcll(kx & ~A) << 8) != __ldg(&groups[g].halves)) continue;
+            const uint64_t j = k ^ x;
+            const int t0 = __ldg(&groups[g].begin), t1 = __ldg(&groups[g].end);
+            double2 f = make_double2(0.0, 0.0);
+            if (__ldg(&groups[g].real)) {
+                for (int t = t0; t < t1; ++t) {
+                    const double2 zc = __ldg(&rterms[t]);
+                    f.x += (__popcll(j & (uint64_t)__double_as_longlong(zc.x)) & 1) ? -zc.y : zc.y;
+                }
+            } else {
+                for (int t = t0; t < t1; ++t) {
+                    const double2 c = __ldg(&terms[t].c);
+                    if (__popcll(j & __ldg(&terms[t].z)) & 1) { f.x -= c.x; f.y -= c.y; }
+                    else { f.x += c.x; f.y += c.y; }
+                }
+            }
+            if (!live) continue;
+            const size_t col = (size_t)arank[g_pext_parity(j, 0)] * L.nbeta + brank[g_pext_parity(j, 1)];
+            acc = g_cadd(acc, g_cmul(f, L.psi[col * L.B + s]));
+        }
+        for (int o = L.spw; o < 32; o <<= 1) {
+            acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+        }
+        if (sub == 0 && live) {
+            L.sig[(size_t)i * L.B + s] = acc;
+            en = g_cadd(en, g_cjmul(L.psi[(size_t)i * L.B + s], acc));
+        }
+    }
+    if (lane < L.spw) s_e[warp][lane] = en;
+    __syncthreads();
+    if (threadIdx.x < L.spw) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < nwarp; ++w) t = g_cadd(t, s_e[w][threadIdx.x]);
+        const int ss = blockIdx.y * L.spw + threadIdx.x;
+        if (ss < L.B) epart[(size_t)ss * gridDim.x + blockIdx.x] = t;
+    }
+}
+
 // energy[s] = Re sum_k epart[s * n + k]  (one warp per slot, fixed order)
 __global__ void k_cg_energy(const double2 *__restrict__ epart, int n, int B,
                             double *__restrict__ energy) {

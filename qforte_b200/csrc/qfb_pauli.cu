@@ -32,6 +32,7 @@
 // K_mu is one x-group the inner product and both un-rotations share one pass
 // over (psi, sigma); no intermediate state is stored.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -839,6 +840,13 @@ struct TiledView {
     uint64_t *d_hival = nullptr;
 };
 
+// H rows on a particle-number sector and compact plans (defined with the
+// compact evaluator below); cached on the Hamiltonian and on the forward
+// program so that every evaluator of one problem shares them.
+struct SectorRows;
+struct SectorPlan;
+static std::atomic<uint64_t> g_prog_uid{1};
+
 struct qfb_sum_s {
     int64_t nterms = 0;
     int32_t ngroups = 0;
@@ -858,6 +866,8 @@ struct qfb_sum_s {
     int32_t *d_seg_g0 = nullptr;
     std::vector<GroupDev> h_groups;
     std::vector<int32_t> h_seg_g0;
+    // (nqubit, alpha count, beta count, bank-interleaved) -> rows
+    std::map<std::tuple<int, int, int, int>, std::shared_ptr<SectorRows>> rows_cache;
 };
 
 // A window plan of a program for one qubit count (qfb_window.cuh).
@@ -876,6 +886,10 @@ struct WinPlan {
 };
 
 struct qfb_prog_s {
+    uint64_t uid = g_prog_uid.fetch_add(1);  // identity for caches keyed on other programs
+    // (K uid, U uid, nqubit, alpha count, beta count, shared) -> plan (null: none)
+    std::map<std::tuple<uint64_t, uint64_t, int, int, int, int>, std::shared_ptr<SectorPlan>>
+        sector_plans;
     int64_t nstrings = 0;
     int32_t nparam = 0;
     void *blob = nullptr;
@@ -2201,8 +2215,20 @@ struct CStep {
     std::vector<Pat> pats;
 };
 
+// Device copies of a plan's record streams (shared by its evaluators).
+struct SectorPlanDev {
+    void *blob = nullptr;
+    size_t bytes = 0;
+    const uint4 *frec = nullptr, *srec = nullptr;
+    const int2 *fspan = nullptr, *sspan = nullptr;
+    const int32_t *fparam = nullptr, *sparam = nullptr;
+    ~SectorPlanDev() { dev_free(blob); }
+};
+
 struct SectorPlan {
     int na_orb = 0, nb_orb = 0, nalpha = 0, nbeta = 0, nsec = 0, ref_i = 0;
+    int ka = 0, kb = 0;  // alpha and beta electrons of the sector
+    std::shared_ptr<SectorPlanDev> dev;
     std::vector<uint64_t> adet, bdet;
     std::vector<int32_t> arank, brank;
     std::vector<CStep> fsteps, ksteps, usteps;
@@ -2318,6 +2344,8 @@ static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_pr
     sp.nb_orb = n / 2;
     if (sp.na_orb > 20) return false;
     const int ka = __builtin_popcountll(ref & A & all), kb = __builtin_popcountll(ref & ~A & all);
+    sp.ka = ka;
+    sp.kb = kb;
     auto strings = [&](int m, int k, int odd, std::vector<uint64_t> &det, std::vector<int32_t> &rank) {
         rank.assign((size_t)1 << m, -1);
         if (k > m) return;
@@ -2403,7 +2431,7 @@ struct qfb_ucc_s {
     size_t bytes = 0;     // device bytes held (blobs)
     int compact = 0;      // compact sector evaluator (qfb_sector.cuh)
     int64_t nnz = 0;      // entries of the H rows on the compact sector
-    void *sblob = nullptr, *csr = nullptr;
+    std::shared_ptr<SectorRows> rows;  // compact paths: H rows on the sector
     qfbs::SLaunch SL{};
     void *sec = nullptr;  // uint32_t (nqubit <= 32) or uint64_t indices
     SecGroup *sgroups = nullptr;
@@ -2485,17 +2513,38 @@ static int sector_rows_interleave(const std::vector<int32_t> &rowptr, int64_t nn
     return QFB_OK;
 }
 
-constexpr double kRowsBudget = 8e9;  // bytes of H rows a global-memory sector path may hold
+constexpr double kRowsBudget = 24e9;  // bytes of H rows a global-memory sector path may hold
 
-// Device copies of a compact plan and the H rows on its sector (global:
-// the states live in global memory; QFB_ENOMEM when the rows exceed their
-// budget).
-static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> &sg,
-                         bool global = false) {
-    const int nsec = sp.nsec;
-    std::vector<uint64_t> det((size_t)nsec);
-    for (int ra = 0; ra < sp.nalpha; ++ra)
-        for (int rb = 0; rb < sp.nbeta; ++rb) det[(size_t)ra * sp.nbeta + rb] = sp.adet[ra] | sp.bdet[rb];
+static_assert(sizeof(qfbg::GGroup) == sizeof(SecGroup), "GGroup mirrors SecGroup");
+static_assert(sizeof(qfbg::GTerm) == sizeof(TermDev), "GTerm mirrors TermDev");
+
+struct SectorRows {
+    void *blob = nullptr;
+    size_t bytes = 0;
+    // the sector's dets in compact order, the rank tables and the groups
+    // (kept for sigma without rows when the rows are over budget)
+    void *tblob = nullptr;
+    size_t tbytes = 0;
+    const uint64_t *det = nullptr;
+    const int32_t *arank = nullptr, *brank = nullptr;
+    const SecGroup *groups = nullptr;
+    int ngroups = 0;
+    const int32_t *rowptr = nullptr;
+    const uint32_t *col = nullptr;
+    const double *vr = nullptr;    // real H ...
+    const double2 *vc = nullptr;   // ... or complex
+    int64_t nnz = 0;
+    bool too_big = false;          // over kRowsBudget: no rows held
+    ~SectorRows() {
+        dev_free(blob);
+        dev_free(tblob);
+    }
+};
+
+// The device copies of a plan's record streams, uploaded once.
+static int plan_upload(SectorPlan &sp) {
+    if (sp.dev) return QFB_OK;
+    auto d = std::make_shared<SectorPlanDev>();
     size_t off = 0;
     auto take = [&](size_t bytes) {
         size_t o = off;
@@ -2508,36 +2557,107 @@ static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> 
     const size_t o_sr = take(sizeof(uint4) * sp.sweep.rec.size());
     const size_t o_ss = take(sizeof(int2) * sp.sweep.span.size());
     const size_t o_sp = take(sizeof(int32_t) * sp.sweep.param.size());
-    const size_t o_det = take(sizeof(uint64_t) * det.size());
-    const size_t o_ar = take(sizeof(int32_t) * sp.arank.size());
-    const size_t o_br = take(sizeof(int32_t) * sp.brank.size());
-    const size_t o_g = take(sizeof(SecGroup) * sg.size());
-    const size_t o_cnt = take(sizeof(int32_t) * (size_t)(nsec + 1));
-    int rc = dev_alloc(&u->sblob, off);
+    int rc = dev_alloc(&d->blob, off);
     if (rc) return rc;
-    u->bytes += off;
-    char *base = (char *)u->sblob;
+    d->bytes = off;
+    char *base = (char *)d->blob;
     struct Up { size_t o; const void *p; size_t n; };
     const Up ups[] = {{o_fr, sp.fwd.rec.data(), sizeof(uint4) * sp.fwd.rec.size()},
                       {o_fs, sp.fwd.span.data(), sizeof(int2) * sp.fwd.span.size()},
                       {o_fp, sp.fwd.param.data(), sizeof(int32_t) * sp.fwd.param.size()},
                       {o_sr, sp.sweep.rec.data(), sizeof(uint4) * sp.sweep.rec.size()},
                       {o_ss, sp.sweep.span.data(), sizeof(int2) * sp.sweep.span.size()},
-                      {o_sp, sp.sweep.param.data(), sizeof(int32_t) * sp.sweep.param.size()},
-                      {o_det, det.data(), sizeof(uint64_t) * det.size()},
-                      {o_ar, sp.arank.data(), sizeof(int32_t) * sp.arank.size()},
-                      {o_br, sp.brank.data(), sizeof(int32_t) * sp.brank.size()},
-                      {o_g, sg.data(), sizeof(SecGroup) * sg.size()}};
+                      {o_sp, sp.sweep.param.data(), sizeof(int32_t) * sp.sweep.param.size()}};
     for (const Up &x : ups)
         if (x.n) QFB_CUDA(cudaMemcpyAsync(base + x.o, x.p, x.n, cudaMemcpyHostToDevice, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    d->frec = (const uint4 *)(base + o_fr);
+    d->fspan = (const int2 *)(base + o_fs);
+    d->fparam = (const int32_t *)(base + o_fp);
+    d->srec = (const uint4 *)(base + o_sr);
+    d->sspan = (const int2 *)(base + o_ss);
+    d->sparam = (const int32_t *)(base + o_sp);
+    sp.dev = d;
+    return QFB_OK;
+}
+
+// H rows of `ham` on the plan's sector (compact order), built on the device
+// once per (qubits, electrons, layout) and cached on the Hamiltonian.  With
+// `global`, rows over kRowsBudget are refused (QFB_ENOMEM) and the refusal
+// is cached too; `interleave` orders each row's entries for k_sector_h.
+static int get_sector_rows(qfb_sum_s *ham, const SectorPlan &sp, const std::vector<SecGroup> &sg,
+                           int n, bool interleave, bool global, std::shared_ptr<SectorRows> *out) {
+    const int layout = interleave ? 1 : (global && g_ucc_compact == 3) ? 2 : 0;
+    const auto key = std::make_tuple(n, sp.ka, sp.kb, layout);
+    auto it = ham->rows_cache.find(key);
+    if (it != ham->rows_cache.end()) {
+        if (!global && it->second->too_big)
+            return fail(QFB_ENOMEM, "sector H rows exceed their budget");
+        *out = it->second;
+        return QFB_OK;
+    }
+    const int nsec = sp.nsec;
+    bool real = true;
+    for (const SecGroup &g : sg) real = real && g.real;
+    const double entry_bytes = real ? 12.0 : 20.0;
+    auto rows = std::make_shared<SectorRows>();
+    // persistent tables: dets in compact order, ranks, groups, row counts
+    std::vector<uint64_t> det((size_t)nsec);
+    for (int ra = 0; ra < sp.nalpha; ++ra)
+        for (int rb = 0; rb < sp.nbeta; ++rb) det[(size_t)ra * sp.nbeta + rb] = sp.adet[ra] | sp.bdet[rb];
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_det = take(sizeof(uint64_t) * det.size());
+    const size_t o_ar = take(sizeof(int32_t) * sp.arank.size());
+    const size_t o_br = take(sizeof(int32_t) * sp.brank.size());
+    const size_t o_g = take(sizeof(SecGroup) * sg.size());
+    const size_t o_cnt = take(sizeof(int32_t) * (size_t)(nsec + 1));
+    int rc = dev_alloc(&rows->tblob, off);
+    if (rc) return rc;
+    rows->tbytes = off;
+    char *base = (char *)rows->tblob;
+    QFB_CUDA(cudaMemcpyAsync(base + o_det, det.data(), sizeof(uint64_t) * det.size(),
+                             cudaMemcpyHostToDevice, t_stream));
+    QFB_CUDA(cudaMemcpyAsync(base + o_ar, sp.arank.data(), sizeof(int32_t) * sp.arank.size(),
+                             cudaMemcpyHostToDevice, t_stream));
+    QFB_CUDA(cudaMemcpyAsync(base + o_br, sp.brank.data(), sizeof(int32_t) * sp.brank.size(),
+                             cudaMemcpyHostToDevice, t_stream));
+    if (!sg.empty())
+        QFB_CUDA(cudaMemcpyAsync(base + o_g, sg.data(), sizeof(SecGroup) * sg.size(),
+                                 cudaMemcpyHostToDevice, t_stream));
     int32_t *d_cnt = (int32_t *)(base + o_cnt);
-    const SecGroup *d_g = (const SecGroup *)(base + o_g);
-    const uint64_t *d_det = (const uint64_t *)(base + o_det);
-    const int32_t *d_ar = (const int32_t *)(base + o_ar), *d_br = (const int32_t *)(base + o_br);
+    rows->det = (const uint64_t *)(base + o_det);
+    rows->arank = (const int32_t *)(base + o_ar);
+    rows->brank = (const int32_t *)(base + o_br);
+    rows->groups = (const SecGroup *)(base + o_g);
+    rows->ngroups = (int)sg.size();
+    auto over_budget = [&]() -> int {  // rows kept without entries: sigma from the groups
+        rows->too_big = true;
+        QFB_CUDA(cudaStreamSynchronize(t_stream));
+        ham->rows_cache[key] = rows;
+        if (!global) return fail(QFB_ENOMEM, "sector H rows exceed their budget");
+        *out = rows;
+        return QFB_OK;
+    };
+    if (global && g_ucc_compact == 3) return over_budget();  // rows switched off
+    {   // estimate from the reference row before counting every row
+        const uint64_t A = 0x5555555555555555ull;
+        const uint64_t k = sp.adet[sp.ref_i / sp.nbeta] | sp.bdet[sp.ref_i % sp.nbeta];
+        int64_t c = 0;
+        for (const SecGroup &g : sg) {
+            const uint64_t kx = k & g.x;
+            if ((__builtin_popcountll(kx & A) | __builtin_popcountll(kx & ~A) << 8) == g.halves) ++c;
+        }
+        if ((double)c * nsec * entry_bytes > 1.5 * kRowsBudget) return over_budget();
+    }
     const unsigned nb = (unsigned)((nsec + 127) / 128);
-    k_sector_rows<<<nb, 128, 0, t_stream>>>(d_det, nsec, d_g, (int)sg.size(), u->ham->d_terms,
-                                            u->ham->d_rterms, d_ar, d_br, sp.nbeta, u->nqubit,
-                                            nullptr, d_cnt, nullptr, nullptr, nullptr);
+    k_sector_rows<<<nb, 128, 0, t_stream>>>(rows->det, nsec, rows->groups, (int)sg.size(),
+                                            ham->d_terms, ham->d_rterms, rows->arank, rows->brank,
+                                            sp.nbeta, n, nullptr, d_cnt, nullptr, nullptr, nullptr);
     QFB_LAUNCHED();
     std::vector<int32_t> cnt((size_t)nsec);
     QFB_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int32_t) * nsec, cudaMemcpyDeviceToHost,
@@ -2548,68 +2668,88 @@ static int sector_upload(qfb_ucc u, SectorPlan &sp, const std::vector<SecGroup> 
     for (int i = 0; i < nsec; ++i) {
         rowptr[i] = (int32_t)nnz;
         nnz += cnt[i];
-        if (nnz >= ((int64_t)1 << 31)) return fail(QFB_ENOMEM, "sector H rows: too many entries");
+        if (nnz >= ((int64_t)1 << 31)) return over_budget();
     }
     rowptr[nsec] = (int32_t)nnz;
-    u->nnz = nnz;
-    bool real = true;
-    for (const SecGroup &g : sg) real = real && g.real;
-    if (global && (double)nnz * (real ? 12.0 : 20.0) > kRowsBudget)
-        return fail(QFB_ENOMEM, "sector H rows: %lld entries exceed the budget", (long long)nnz);
-    const size_t o_rp = 0;
+    if ((double)nnz * entry_bytes > kRowsBudget) return over_budget();
     size_t coff = ((sizeof(int32_t) * (nsec + 1)) + 255) & ~(size_t)255;
     const size_t o_col = coff;
     coff += ((sizeof(uint32_t) * std::max<int64_t>(nnz, 1)) + 255) & ~(size_t)255;
     const size_t o_val = coff;
     coff += (real ? sizeof(double) : sizeof(double2)) * std::max<int64_t>(nnz, 1);
-    rc = dev_alloc(&u->csr, coff);
+    rc = dev_alloc(&rows->blob, coff);
     if (rc) return rc;
-    u->bytes += coff;
-    char *cb = (char *)u->csr;
-    QFB_CUDA(cudaMemcpyAsync(cb + o_rp, rowptr.data(), sizeof(int32_t) * (nsec + 1),
-                             cudaMemcpyHostToDevice, t_stream));
-    int32_t *d_rp = (int32_t *)(cb + o_rp);
+    rows->bytes = coff;
+    rows->nnz = nnz;
+    char *cb = (char *)rows->blob;
+    QFB_CUDA(cudaMemcpyAsync(cb, rowptr.data(), sizeof(int32_t) * (nsec + 1), cudaMemcpyHostToDevice,
+                             t_stream));
+    int32_t *d_rp = (int32_t *)cb;
     uint32_t *d_col = (uint32_t *)(cb + o_col);
     double *d_vr = real ? (double *)(cb + o_val) : nullptr;
     double2 *d_vc = real ? nullptr : (double2 *)(cb + o_val);
-    k_sector_rows<<<nb, 128, 0, t_stream>>>(d_det, nsec, d_g, (int)sg.size(), u->ham->d_terms,
-                                            u->ham->d_rterms, d_ar, d_br, sp.nbeta, u->nqubit, d_rp,
-                                            nullptr, d_col, d_vr, d_vc);
+    k_sector_rows<<<nb, 128, 0, t_stream>>>(rows->det, nsec, rows->groups, (int)sg.size(),
+                                            ham->d_terms, ham->d_rterms, rows->arank, rows->brank,
+                                            sp.nbeta, n, d_rp, nullptr, d_col, d_vr, d_vc);
     QFB_LAUNCHED();
     QFB_CUDA(cudaStreamSynchronize(t_stream));
-    if (!global) {
+    if (interleave) {
         rc = sector_rows_interleave(rowptr, nnz, d_col, real ? (void *)d_vr : (void *)d_vc,
                                     real ? sizeof(double) : sizeof(double2));
         if (rc) return rc;
     }
+    rows->rowptr = d_rp;
+    rows->col = d_col;
+    rows->vr = d_vr;
+    rows->vc = d_vc;
+    ham->rows_cache[key] = rows;
+    *out = rows;
+    return QFB_OK;
+}
+
+// Attach a compact plan and its H rows to an evaluator (shared memory or,
+// with `global`, global memory states).
+static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<SectorPlan> &plan,
+                         const std::vector<SecGroup> &sg, bool global) {
+    SectorPlan &sp = *plan;
+    int rc = plan_upload(sp);
+    if (rc) return rc;
+    std::shared_ptr<SectorRows> rows;
+    rc = get_sector_rows(ham, sp, sg, u->nqubit, !global, global, &rows);
+    if (rc) return rc;
+    u->splan = plan;
+    u->rows = rows;
+    u->nnz = rows->nnz;
+    u->bytes += sp.dev->bytes + rows->bytes + rows->tbytes;
+    const SectorPlanDev &d = *sp.dev;
     if (global) {
-        u->g_frec = (const uint4 *)(base + o_fr);
-        u->g_srec = (const uint4 *)(base + o_sr);
-        u->g_rowptr = d_rp;
-        u->g_col = d_col;
-        u->g_vr = d_vr;
-        u->g_vc = d_vc;
+        u->g_frec = d.frec;
+        u->g_srec = d.srec;
+        u->g_rowptr = rows->rowptr;
+        u->g_col = rows->col;
+        u->g_vr = rows->vr;
+        u->g_vc = rows->vc;
         return QFB_OK;
     }
     qfbs::SLaunch &L = u->SL;
-    L.nsec = nsec;
+    L.nsec = sp.nsec;
     L.nbeta = sp.nbeta;
     L.ref_i = sp.ref_i;
     L.nparam = u->nparam;
-    L.fwd.rec = (const uint4 *)(base + o_fr);
-    L.fwd.span = (const int2 *)(base + o_fs);
-    L.fwd.param = (const int32_t *)(base + o_fp);
+    L.fwd.rec = d.frec;
+    L.fwd.span = d.fspan;
+    L.fwd.param = d.fparam;
     L.fwd.n = (int)sp.fwd.span.size();
     L.fwd.maxw = std::max(sp.fwd.maxw, 1);
-    L.sweep.rec = (const uint4 *)(base + o_sr);
-    L.sweep.span = (const int2 *)(base + o_ss);
-    L.sweep.param = (const int32_t *)(base + o_sp);
+    L.sweep.rec = d.srec;
+    L.sweep.span = d.sspan;
+    L.sweep.param = d.sparam;
     L.sweep.n = (int)sp.sweep.span.size();
     L.sweep.maxw = std::max(sp.sweep.maxw, 1);
-    L.rowptr = d_rp;
-    L.col = d_col;
-    L.val_r = d_vr;
-    L.val_c = d_vc;
+    L.rowptr = rows->rowptr;
+    L.col = rows->col;
+    L.val_r = rows->vr;
+    L.val_c = rows->vc;
     L.params = u->params;
     L.energy = u->energy;
     L.partial = u->gpart;
@@ -2718,7 +2858,12 @@ static int ucc_stage_global(qfb_ucc u, int stage, int with_grad) {
             break;
         case 2: {
             const dim3 hg(u->g_hgrid, u->g_ygrid);
-            if (u->g_vc)
+            if (u->rows->too_big)
+                qfbg::k_cg_h_groups<<<hg, 256, 0, t_stream>>>(
+                    L, u->rows->det, (const qfbg::GGroup *)u->rows->groups, u->rows->ngroups,
+                    (const qfbg::GTerm *)u->ham->d_terms, u->ham->d_rterms, u->rows->arank,
+                    u->rows->brank, u->g_epart);
+            else if (u->g_vc)
                 qfbg::k_cg_h_rows<false><<<hg, 256, 0, t_stream>>>(L, u->g_rowptr, u->g_col, nullptr,
                                                                   u->g_vc, u->g_epart);
             else
@@ -2854,19 +2999,23 @@ extern "C" {
 
 static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham,
                            int nqubit, uint64_t ref_index, int nbatch, qfb_ucc *out,
-                           bool allow_global);
+                           bool allow_sector);
 
 int qfb_ucc_create(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham, int nqubit,
                    uint64_t ref_index, int nbatch, qfb_ucc *out) {
+    // plans, window plans and sector rows are cached on the shared program and
+    // Hamiltonian objects: one creation at a time
+    static std::mutex create_mu;
+    std::lock_guard<std::mutex> lk(create_mu);
     int rc = ucc_create_impl(fprog, gprog, uprog, ham, nqubit, ref_index, nbatch, out, true);
-    if (rc == QFB_ENOMEM && out && !*out)  // sector rows over budget (or no room): full space
+    if (rc == QFB_ENOMEM && out && !*out)  // no room for the sector's tables: full space
         rc = ucc_create_impl(fprog, gprog, uprog, ham, nqubit, ref_index, nbatch, out, false);
     return rc;
 }
 
 static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_sum ham,
                            int nqubit, uint64_t ref_index, int nbatch, qfb_ucc *out,
-                           bool allow_global) {
+                           bool allow_sector) {
     if (!out) return fail(QFB_EINVAL, "qfb_ucc_create: null output");
     *out = nullptr;
     if (!fprog || !ham) return fail(QFB_EINVAL, "qfb_ucc_create: null program or Hamiltonian");
@@ -2905,19 +3054,34 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
         }
         if (sgroups.empty()) sector.clear();
     }
-    SectorPlan splan;
+    std::shared_ptr<SectorPlan> plan;
     bool compact = false, gsec = false;
-    if (g_ucc_compact && !sector.empty()) {
-        if (g_ucc_compact == 1)
-            compact = build_sector_plan(splan, fprog, gprog, uprog, nqubit, ref_index, true);
-        if (!compact && allow_global) {
-            SectorPlan gp;
-            if (build_sector_plan(gp, fprog, gprog, uprog, nqubit, ref_index, false)) {
-                splan = std::move(gp);
-                gsec = true;
-            }
+    if (g_ucc_compact && allow_sector && !sector.empty()) {
+        const uint64_t A = 0x5555555555555555ull, all = (1ull << nqubit) - 1ull;
+        const int ka = __builtin_popcountll(ref_index & A & all);
+        const int kb = __builtin_popcountll(ref_index & ~A & all);
+        auto get_plan = [&](bool shared) {
+            const auto key = std::make_tuple(gprog ? gprog->uid : 0, uprog ? uprog->uid : 0, nqubit,
+                                             ka, kb, shared ? 1 : 0);
+            auto it = fprog->sector_plans.find(key);
+            if (it != fprog->sector_plans.end()) return it->second;
+            auto sp = std::make_shared<SectorPlan>();
+            std::shared_ptr<SectorPlan> r;
+            if (build_sector_plan(*sp, fprog, gprog, uprog, nqubit, ref_index, shared)) r = sp;
+            fprog->sector_plans[key] = r;
+            return r;
+        };
+        if (g_ucc_compact == 1) {  // 2, 3: global memory only (3: sigma without stored rows)
+            plan = get_plan(true);
+            compact = plan != nullptr;
+        }
+        if (!compact) {
+            plan = get_plan(false);
+            gsec = plan != nullptr;
         }
     }
+    static const SectorPlan no_plan;
+    const SectorPlan &splan = plan ? *plan : no_plan;
     if (compact) {
         int src = sector_smem_attr();
         if (src) return src;
@@ -3025,12 +3189,11 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
         return cuda_fail(e, "qfb_ucc_create");
     }
     if (compact || gsec) {
-        rc = sector_upload(u, splan, sgroups, gsec);
+        rc = sector_attach(u, ham, plan, sgroups, gsec);
         if (rc) {
             qfb_ucc_destroy(u);
             return rc;
         }
-        u->splan = std::make_shared<SectorPlan>(std::move(splan));
     }
     *out = u;
     return QFB_OK;
@@ -3048,7 +3211,7 @@ int qfb_ucc_tiles(int fwd_bits, int grad_bits, int low_bits) {
 }
 
 int qfb_ucc_config(int compact) {
-    if (compact < 0 || compact > 2) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
+    if (compact < 0 || compact > 3) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
     g_ucc_compact = compact;
     return QFB_OK;
 }
@@ -3073,8 +3236,6 @@ int qfb_ucc_sector(qfb_ucc u, int64_t *nsec) {
 
 int qfb_ucc_destroy(qfb_ucc u) {
     if (!u) return QFB_OK;
-    dev_free(u->sblob);
-    dev_free(u->csr);
     dev_free(u->pblob);
     for (auto &x : u->exec)
         if (x) cudaGraphExecDestroy(x);

@@ -45,7 +45,7 @@ def evaluator_config(compact=True):
     """Process-wide: let evaluators created from now on use the compact
     sector paths (True, the default), only the global-memory one ("global"),
     or keep full-space states (False)."""
-    mode = 2 if compact == "global" else (1 if compact else 0)
+    mode = {"global": 2, "global-no-rows": 3}.get(compact, 1 if compact else 0)
     check(lib().qfb_ucc_config(mode), "qfb_ucc_config")
 
 

@@ -483,7 +483,7 @@ def test_global_sector_path_matches_shared_and_full(cuda, norb, seed, pool_type,
     rng = np.random.default_rng(B + norb)
     P = rng.uniform(-0.1, 0.1, (B, len(tops)))
     res = {}
-    for mode in (True, "global", False):
+    for mode in (True, "global", "global-no-rows", False):
         evaluator_config(mode)
         try:
             eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference, pool_type=pool_type)
@@ -491,11 +491,13 @@ def test_global_sector_path_matches_shared_and_full(cuda, norb, seed, pool_type,
         finally:
             evaluator_config(True)
     E3, G3, path3 = res["global"]
+    E4, G4, path4 = res["global-no-rows"]
     E1, G1, path1 = res[False]
     E2, G2, path2 = res[True]
-    assert path1 in (0, 1) and (pool_type == "sa_SD" or path3 == 3)
+    assert path1 in (0, 1) and (pool_type == "sa_SD" or path3 == path4 == 3)
     assert np.max(np.abs(E3 - E1)) < 1e-12 and np.max(np.abs(G3 - G1)) < 1e-11
     assert np.max(np.abs(E3 - E2)) < 1e-12 and np.max(np.abs(G3 - G2)) < 1e-11
+    assert np.max(np.abs(E4 - E1)) < 1e-12 and np.max(np.abs(G4 - G1)) < 1e-11
     if B == 3:
         hterms = oracle_terms(mol.hamiltonian)
         kf = kops_forward(pool, tops, pool_type)
