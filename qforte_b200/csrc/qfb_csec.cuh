@@ -299,6 +299,108 @@ __global__ void __launch_bounds__(256) k_cg_h_groups(GLaunch L, const uint64_t *
     }
 }
 
+constexpr int kRowCap = 224;  // entries of one row staged per warp before they are consumed
+
+// The same without scanning the groups slot by slot: each warp takes one
+// output row, its 32 lanes test 32 groups at a time, and the groups that
+// connect the row inside the sector are compacted (column, f) into a
+// shared-memory list with a ballot; the list is then consumed with the lanes
+// over (slot, entry), kRowUnrollG entries in flight per lane.
+constexpr int kRowUnrollG = 4;
+
+__global__ void __launch_bounds__(256) k_cg_h_list(GLaunch L, const uint64_t *__restrict__ det,
+                                                   const GGroup *__restrict__ groups, int ngroups,
+                                                   const GTerm *__restrict__ terms,
+                                                   const double2 *__restrict__ rterms,
+                                                   const int32_t *__restrict__ arank,
+                                                   const int32_t *__restrict__ brank,
+                                                   double2 *__restrict__ epart) {
+    __shared__ double2 s_f[8][kRowCap];
+    __shared__ uint32_t s_c[8][kRowCap];
+    __shared__ double2 s_e[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int per = 32 / L.spw, sub = lane / L.spw;
+    const int s = blockIdx.y * L.spw + (lane % L.spw);
+    const bool live = s < L.B;
+    const uint64_t A = 0x5555555555555555ull;
+    double2 *lf = s_f[warp];
+    uint32_t *lc = s_c[warp];
+    double2 en = make_double2(0.0, 0.0);
+    for (int i = blockIdx.x * nwarp + warp; i < L.nsec; i += gridDim.x * nwarp) {
+        const uint64_t k = det[i];
+        double2 acc = make_double2(0.0, 0.0);
+        int cnt = 0;
+        for (int g0 = 0; g0 < ngroups; g0 += 32) {
+            const int g = g0 + lane;
+            bool valid = false;
+            double2 f = make_double2(0.0, 0.0);
+            uint32_t col = 0;
+            if (g < ngroups) {
+                const GGroup gr = groups[g];
+                const uint64_t kx = k & gr.x;
+                valid = (__popcll(kx & A) | __popcll(kx & ~A) << 8) == gr.halves;
+                if (valid) {
+                    const uint64_t j = k ^ gr.x;
+                    if (gr.real) {
+                        for (int t = gr.begin; t < gr.end; ++t) {
+                            const double2 zc = __ldg(&rterms[t]);
+                            f.x += (__popcll(j & (uint64_t)__double_as_longlong(zc.x)) & 1) ? -zc.y : zc.y;
+                        }
+                    } else {
+                        for (int t = gr.begin; t < gr.end; ++t) {
+                            const double2 c = __ldg(&terms[t].c);
+                            if (__popcll(j & __ldg(&terms[t].z)) & 1) { f.x -= c.x; f.y -= c.y; }
+                            else { f.x += c.x; f.y += c.y; }
+                        }
+                    }
+                    col = (uint32_t)(arank[g_pext_parity(j, 0)] * L.nbeta + brank[g_pext_parity(j, 1)]);
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, valid);
+            if (valid) {
+                const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+                lf[pos] = f;
+                lc[pos] = col;
+            }
+            cnt += __popc(m);
+            if (cnt > kRowCap - 32 || g0 + 32 >= ngroups) {  // consume the list
+                __syncwarp();
+                for (int e0 = sub; e0 < cnt; e0 += per * kRowUnrollG) {
+                    double2 x[kRowUnrollG];
+#pragma unroll
+                    for (int u = 0; u < kRowUnrollG; ++u) {
+                        const int e = e0 + per * u;
+                        x[u] = (live && e < cnt) ? L.psi[(size_t)lc[e] * L.B + s] : make_double2(0.0, 0.0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < kRowUnrollG; ++u) {
+                        const int e = e0 + per * u;
+                        if (e < cnt) acc = g_cadd(acc, g_cmul(lf[e], x[u]));
+                    }
+                }
+                __syncwarp();
+                cnt = 0;
+            }
+        }
+        for (int o = L.spw; o < 32; o <<= 1) {
+            acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+        }
+        if (sub == 0 && live) {
+            L.sig[(size_t)i * L.B + s] = acc;
+            en = g_cadd(en, g_cjmul(L.psi[(size_t)i * L.B + s], acc));
+        }
+    }
+    if (lane < L.spw) s_e[warp][lane] = en;
+    __syncthreads();
+    if (threadIdx.x < L.spw) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < nwarp; ++w) t = g_cadd(t, s_e[w][threadIdx.x]);
+        const int ss = blockIdx.y * L.spw + threadIdx.x;
+        if (ss < L.B) epart[(size_t)ss * gridDim.x + blockIdx.x] = t;
+    }
+}
+
 // energy[s] = Re sum_k epart[s * n + k]  (one warp per slot, fixed order)
 __global__ void k_cg_energy(const double2 *__restrict__ epart, int n, int B,
                             double *__restrict__ energy) {

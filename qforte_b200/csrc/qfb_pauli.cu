@@ -2859,7 +2859,7 @@ static int ucc_stage_global(qfb_ucc u, int stage, int with_grad) {
         case 2: {
             const dim3 hg(u->g_hgrid, u->g_ygrid);
             if (u->rows->too_big)
-                qfbg::k_cg_h_groups<<<hg, 256, 0, t_stream>>>(
+                qfbg::k_cg_h_list<<<hg, 256, 0, t_stream>>>(
                     L, u->rows->det, (const qfbg::GGroup *)u->rows->groups, u->rows->ngroups,
                     (const qfbg::GTerm *)u->ham->d_terms, u->ham->d_rterms, u->rows->arank,
                     u->rows->brank, u->g_epart);
