@@ -51,10 +51,14 @@ def parse():
     ap.add_argument("--full-space", action="store_true",
                     help="keep full-space states (no compact sector evaluator)")
     ap.add_argument("--workload", default="ucc",
-                    choices=["ucc", "gates", "grad", "adapt", "serve"],
+                    choices=["ucc", "gates", "grad", "adapt", "serve", "pexp"],
                     help="ucc: batched dUCCSD energy+gradient (default); gates: the gate sweep; "
                          "grad: differentiable energy, forward+backward against forward alone; "
-                         "adapt: every ADAPT pool gradient of a 12-operator state in one launch")
+                         "adapt: every ADAPT pool gradient of a 12-operator state in one launch; "
+                         "pexp: Pauli-exponential passes on one large state")
+    ap.add_argument("--pexp-n", type=int, default=28, help="pexp: qubits")
+    ap.add_argument("--pexp-strings", type=int, default=64,
+                    help="pexp: random Pauli strings, and dUCC operators, per program")
     ap.add_argument("--adapt-norb", type=int, default=10, help="adapt workload: orbitals")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: mean requests per second")
     ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
@@ -66,6 +70,10 @@ def parse():
     ap.add_argument("--layers", type=int, default=100, help="gate sweep: layers per circuit")
     ap.add_argument("--tile", type=int, default=0,
                     help="gate sweep: tile bits of gate runs (0 default, -1 one pass per gate)")
+    ap.add_argument("--low-bits", type=int, default=3,
+                    help="gate sweep: lowest qubits every tile keeps")
+    ap.add_argument("--reg-bits", type=int, default=0,
+                    help="gate sweep: register bits per thread of a tile (0: default)")
     ap.add_argument("--autotune", action="store_true",
                     help="gate sweep: pick the tile shape per qubit count with the autotuner")
     return ap.parse_args()
@@ -228,10 +236,10 @@ def run_gates(a, rank, world, local):
     import torch
     import qforte_b200 as qb
     from qforte_b200._lib import launch_count
-    from qforte_b200.device import gate_plan, gates_config
+    from qforte_b200.device import gate_phases, gate_plan, gates_config
     from qforte_b200.workloads import layered_random_circuit
     torch.cuda.set_device(local)
-    gates_config(a.tile, 4)
+    gates_config(a.tile, a.low_bits, a.reg_bits)
     peak, src = peaks()
     ns = [int(v) for v in a.nqubits.split(",") if v]
     rows = []
@@ -243,6 +251,7 @@ def run_gates(a, rank, world, local):
             from qforte_b200.autotune import tune_gates
             tuned, _ = tune_gates(circ, n, reps=1, store=False)
         nw, nsingle, pass_bytes = gate_plan(circ.gates(), n)
+        nphase, _ = gate_phases(circ.gates(), n)
         qc = qb.Computer(n)
         for _ in range(max(a.warmup, 3) if n < 28 else 1):
             qc.apply_circuit(circ)
@@ -262,7 +271,8 @@ def run_gates(a, rank, world, local):
         ck = clocks.stop() if n == ns[-1] else None
         gbs = pass_bytes / (ms * 1e-3) / 1e9
         rows.append({"nqubit": n, "gates": len(spec), "passes": nw + nsingle, "tile_runs": nw,
-                     "one_gate_passes": nsingle, "ms_per_circuit": ms, "pass_gbs": gbs,
+                     "register_phases": nphase, "one_gate_passes": nsingle,
+                     "ms_per_circuit": ms, "pass_gbs": gbs,
                      "frac_of_hbm": gbs / peak,
                      "effective_gate_gbs": len(spec) * 32.0 * 2 ** n / (ms * 1e-3) / 1e9,
                      "gpu_launches": launches,
@@ -275,9 +285,10 @@ def run_gates(a, rank, world, local):
             "data": "synthetic",
             "config": {"workload": f"layered random circuits, {a.layers} layers, "
                                    f"{','.join(map(str, ns))} qubits, from |0...0>",
-                       "tile_bits": a.tile, "l2": "state larger than L2 from 23 qubits"},
+                       "tile_bits": a.tile, "low_bits": a.low_bits, "reg_bits": a.reg_bits,
+                       "l2": "state larger than L2 from 23 qubits"},
             "sweep": rows,
-            "roofline": {"bound": "hbm", "kernel": "k_gate_window", "achieved": last["pass_gbs"],
+            "roofline": {"bound": "hbm", "kernel": "k_gate_tile", "achieved": last["pass_gbs"],
                          "peak": peak, "peak_source": src, "unit": "GB/s",
                          "frac": last["pass_gbs"] / peak, "traffic": None},
             "gpu_launches": last["gpu_launches"], "clocks": ck}
@@ -295,6 +306,117 @@ def run_gates(a, rank, world, local):
                                     "seconds_per_gate": t}
         except Exception as e:
             line["cpu_baseline"] = {"unavailable": str(e)}
+    print(json.dumps(line))
+    return line
+
+
+PEXP_METRIC = "Pauli-exponential pass GB/s"
+
+
+def run_pexp(a, local):
+    """Pauli-exponential passes on one n-qubit state (default 28 qubits, 4 GiB).
+
+    * ``strings``: exp(i phi P) for random Pauli strings with distinct x-masks,
+      one streaming pass each (pairs j, j ^ x; phase from popcount(j & z)),
+      32 * 2^n bytes per pass.  Applied as U^dagger (one pass per string),
+      then U, and the state must come back to |0...0>.
+    * ``ducc``: the ansatz strings of seeded SD operators of the half-filled
+      (n/2)-orbital problem; U applied with windows (several exponentials per
+      pass over the state) and U^dagger one Givens step per pass (each step
+      touches only its active pairs)."""
+    import ctypes
+    import torch
+    import qforte_b200 as qb
+    from qforte_b200._lib import check, launch_count, lib
+    from qforte_b200.device import DeviceProg
+    from qforte_b200.ucc import ansatz_strings
+    torch.cuda.set_device(local)
+    n, K = a.pexp_n, a.pexp_strings
+    N = 1 << n
+    peak, src = peaks()
+    rng = np.random.default_rng(a.seed + n)
+    xs, seen = [], set()
+    while len(xs) < K:
+        x = int(rng.integers(1, N))
+        if x not in seen:
+            seen.add(x)
+            xs.append(x)
+    zs = [int(rng.integers(0, N)) for _ in range(K)]
+    prog = DeviceProg(np.array(xs, dtype=np.uint64), np.array(zs, dtype=np.uint64),
+                      np.ones(K), np.arange(K, dtype=np.int32), K)
+    params = rng.uniform(-np.pi, np.pi, K)
+    h = ctypes.c_void_p()
+    check(lib().qfb_state_create(n, 1, ctypes.byref(h)), "qfb_state_create")
+    L = lib()
+    P = params.ctypes.data_as(ctypes.c_void_p)
+
+    def apply(pr, par, sign):
+        check(L.qfb_prog_apply(pr.h, h, par, 1, sign), "qfb_prog_apply")
+
+    def timed(fn, reps):
+        for _ in range(max(a.warmup, 3) if n < 28 else 1):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = launch_count()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, (launch_count() - l0) // reps
+
+    clocks = Clocks(local)
+    clocks.start()
+    ms_s, launches = timed(lambda: apply(prog, P, -1), max(1, a.steps))
+    ck = clocks.stop()
+    # round trip: U (one pass per string) after U^dagger gives |0...0> back
+    check(L.qfb_state_reset(h), "reset")
+    apply(prog, P, 1)
+    apply(prog, P, -1)
+    out = (ctypes.c_double * 2)()
+    check(L.qfb_state_get_amp(h, 0, 0, out), "qfb_state_get_amp")
+    roundtrip_err = abs(complex(out[0], out[1]) - 1.0)
+    gbs = K * 32.0 * N / (ms_s * 1e-3) / 1e9
+
+    # dUCC ansatz program of the (n/2)-orbital half-filled problem
+    norb = n // 2
+    pool = qb.SQOpPool()
+    pool.set_orb_spaces([1] * norb + [0] * norb)
+    pool.fill_pool("SD")
+    tops = sorted(int(t) for t in rng.choice(len(pool), min(K, len(pool)), replace=False))
+    X, Z, S, PP = ansatz_strings(pool, tops)
+    dp = DeviceProg(np.array(X, dtype=np.uint64), np.array(Z, dtype=np.uint64), np.array(S),
+                    np.array(PP, dtype=np.int32), len(tops))
+    amps = rng.uniform(-0.1, 0.1, len(tops))
+    PA = amps.ctypes.data_as(ctypes.c_void_p)
+    check(L.qfb_state_reset(h), "reset")
+    ms_w, l_w = timed(lambda: apply(dp, PA, 1), max(1, a.steps))
+    ms_g, l_g = timed(lambda: apply(dp, PA, -1), max(1, a.steps))
+    check(L.qfb_state_reset(h), "reset")
+    apply(dp, PA, 1)
+    apply(dp, PA, -1)
+    check(L.qfb_state_get_amp(h, 0, 0, out), "qfb_state_get_amp")
+    ducc_err = abs(complex(out[0], out[1]) - 1.0)
+    check(L.qfb_state_destroy(h), "destroy")
+    ducc = {"operators": len(tops), "strings": len(X), "steps": int(dp.nsteps),
+            "windowed_ms": ms_w, "windowed_launches": int(l_w),
+            "windowed_pass_gbs": l_w * 32.0 * N / (ms_w * 1e-3) / 1e9,
+            "per_step_ms": ms_g, "per_step_launches": int(l_g),
+            "effective_step_gbs": int(dp.nsteps) * 32.0 * N / (ms_g * 1e-3) / 1e9,
+            "roundtrip_abs_err": ducc_err}
+    line = {"metric": PEXP_METRIC, "value": gbs, "unit": "GB/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_s, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": f"{K} exponentials of random Pauli strings (distinct x-masks) "
+                                   f"on one {n}-qubit state, one streaming pass each",
+                       "nqubit": n, "l2": f"state {16 * N} B, larger than L2"},
+            "roofline": {"bound": "hbm", "kernel": "k_prog_step", "achieved": gbs, "peak": peak,
+                         "peak_source": src, "unit": "GB/s", "frac": gbs / peak,
+                         "algorithmic_bytes_per_launch": 32.0 * N,
+                         "avg_launch_ms": ms_s / max(1, launches), "traffic": None},
+            "roundtrip_abs_err": roundtrip_err, "ducc": ducc,
+            "gpu_launches": int(launches), "clocks": ck}
     print(json.dumps(line))
     return line
 
@@ -551,6 +673,10 @@ def main():
     if a.workload == "serve":
         if rank == 0:
             run_serve(a, local)
+        return
+    if a.workload == "pexp":
+        if rank == 0:
+            run_pexp(a, local)
         return
 
     import torch

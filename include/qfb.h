@@ -107,16 +107,28 @@ QFB_API int qfb_state_get_amp(qfb_state s, int b, uint64_t index, qfb_complex *o
  * move between runs, which reorders only commuting operations. */
 QFB_API int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates);
 /* Tile shape of the gate runs, process-wide: tile_bits qubits per tile (0: the
- * default of 11; -1: one full-state pass per gate, as the reference does),
- * always including the lowest low_bits qubits (default 4).  No counterpart in
- * the reference; set by the autotuner. */
+ * default of 10; at most 12; -1: one full-state pass per gate, as the
+ * reference does), always including the lowest max(low_bits, 3) qubits
+ * (default 3).  Within a tile, each thread holds 2^R amplitudes in registers
+ * (R between 2 and 4, qfb_gates_regs) and the run is applied in phases that
+ * each fix R mixing qubits.  No counterpart in the reference; set by the
+ * autotuner. */
 QFB_API int qfb_gates_config(int tile_bits, int low_bits);
+/* Register bits R per thread of the gate tiles, process-wide (0: the default
+ * of 3; always clamped so a tile has at most 256 threads and at least 4).  No
+ * counterpart in the reference; set by the autotuner. */
+QFB_API int qfb_gates_regs(int reg_bits);
 /* Host only: how qfb_apply_gates would apply these gates to one nqubit state
  * under the current tile shape: the number of tile runs, of one-gate passes,
  * and the bytes those passes read and write (a run 32 * 2^n; a one-gate pass
  * only the amplitudes its case touches).  No counterpart in the reference. */
 QFB_API int qfb_gates_plan(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t *windows,
                            int64_t *single_passes, double *pass_bytes);
+/* Host only: the register phases of those tile runs (shared-memory round
+ * trips of the tile) and the gate operations they hold.  No counterpart in
+ * the reference. */
+QFB_API int qfb_gates_phases(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t *phases,
+                             int64_t *ops);
 
 /* ---- scalars and inner products -------------------------------------------
  * apply_constant computer.cc:130-133; dot computer.cc:975-980. */

@@ -1,9 +1,10 @@
 """Autotuning of the tile shapes that decide how many operations one pass
 over the state fuses.
 
-* Gate runs (``tune_gates``): ``tile_bits`` qubits per shared-memory tile and
-  the ``low_bits`` lowest qubits every tile keeps (contiguous rows), for a
-  circuit on a given qubit count.
+* Gate runs (``tune_gates``): ``tile_bits`` qubits per shared-memory tile, the
+  ``low_bits`` lowest qubits every tile keeps (contiguous rows) and the
+  ``reg_bits`` register bits each thread holds, for a circuit on a given
+  qubit count.
 * Full-space evaluator windows (``tune_evaluator``): the forward and gradient
   tile sizes and the low bits, for a dUCC problem and batch width.  (The
   compact sector path holds whole states in shared memory and has no tile.)
@@ -24,7 +25,7 @@ from .device import gate_plan, gates_config
 __all__ = ["tune_gates", "tune_evaluator", "apply_cached", "cache_path",
            "GATE_CANDIDATES", "WINDOW_CANDIDATES"]
 
-GATE_CANDIDATES = ((10, 4), (11, 3), (11, 4), (12, 4), (12, 5), (13, 4), (13, 5))
+GATE_CANDIDATES = ((10, 3, 3), (10, 4, 3), (11, 3, 3), (11, 4, 3), (9, 3, 3), (12, 3, 4))
 WINDOW_CANDIDATES = ((12, 11, 3), (11, 11, 3), (13, 11, 3), (12, 10, 3), (12, 12, 3),
                      (12, 11, 4))
 
@@ -74,23 +75,23 @@ def gate_key(nqubit):
 
 def tune_gates(circuit, nqubit, candidates=GATE_CANDIDATES, reps=2, store=True):
     """Time ``circuit`` on a fresh ``nqubit`` state under each (tile_bits,
-    low_bits); set and return the fastest with every timing (ms)."""
+    low_bits, reg_bits); set and return the fastest with every timing (ms)."""
     from .computer import Computer
     qc = Computer(int(nqubit))
     timings = {}
-    for tile, low in candidates:
-        if tile > nqubit and (tile, low) != candidates[0]:
+    for tile, low, regs in candidates:
+        if tile > nqubit and (tile, low, regs) != tuple(candidates[0]):
             continue
-        gates_config(tile, low)
+        gates_config(tile, low, regs)
         runs, singles, _ = gate_plan(circuit.gates(), nqubit)
         ms = _time(lambda: qc.apply_circuit(circuit), reps)
-        timings[f"{tile},{low}"] = {"ms": ms, "passes": runs + singles}
+        timings[f"{tile},{low},{regs}"] = {"ms": ms, "passes": runs + singles}
     best = min(timings, key=lambda k: timings[k]["ms"])
-    tile, low = (int(v) for v in best.split(","))
-    gates_config(tile, low)
+    shape = tuple(int(v) for v in best.split(","))
+    gates_config(*shape)
     if store:
-        _store(gate_key(nqubit), [tile, low])
-    return (tile, low), timings
+        _store(gate_key(nqubit), list(shape))
+    return shape, timings
 
 
 def evaluator_key(ducc, nbatch):
@@ -137,9 +138,9 @@ def apply_cached(nqubit=None, ducc=None, nbatch=None):
     d = _load()
     out = {}
     if nqubit is not None and gate_key(nqubit) in d:
-        tile, low = d[gate_key(nqubit)]
-        gates_config(tile, low)
-        out["gates"] = (tile, low)
+        shape = tuple(d[gate_key(nqubit)])
+        gates_config(*shape)
+        out["gates"] = shape
     if ducc is not None and nbatch is not None and evaluator_key(ducc, nbatch) in d:
         shape = tuple(d[evaluator_key(ducc, nbatch)])
         _ucc_tiles(*shape)

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "qfb_common.cuh"
+#include "qfb_gatetile.cuh"
 
 namespace qfb {
 
@@ -176,12 +177,11 @@ __global__ void k_gate4(double2 *__restrict__ psi, uint64_t nbasis, Gate4 g) {
 }
 
 // ---------------------------------------------------------------------------
-// Gate windows: a run of gates whose qubits all lie in one set Q of b qubits
-// (always holding the lowest L qubits, so each tile row is 2^L contiguous
-// amplitudes) is applied to 2^b-amplitude tiles held in shared memory: one
-// read and one write of the state for the whole run.  Each gate performs the
-// per-pair arithmetic of k_gate2 / k_gate4, so a window gives the amplitudes
-// of the same gates applied one pass at a time.
+// Gate runs: a run of gates whose qubits all lie in one set Q of b qubits
+// (always holding the lowest L >= 3 qubits) is applied to 2^b-amplitude tiles
+// by k_gate_tile (qfb_gatetile.cuh): one read and one write of the state for
+// the whole run.  WGate is a run's gate in tile coordinates, as the planner
+// hands it to the phase planner.
 // ---------------------------------------------------------------------------
 enum : int { K_GEN = 4 };
 
@@ -198,87 +198,6 @@ struct GWin {
     uint64_t qmask, cmask;
     int b, L, g0, ng;
 };
-
-__device__ __forceinline__ uint64_t gw_pdep(uint64_t v, uint64_t m) {
-    uint64_t r = 0;
-    while (m) {
-        const uint64_t low = m & (~m + 1);
-        if (v & 1ull) r |= low;
-        v >>= 1;
-        m &= m - 1;
-    }
-    return r;
-}
-
-__global__ void __launch_bounds__(256) k_gate_window(double2 *__restrict__ psi, uint64_t nbasis,
-                                                    GWin w, const WGate *__restrict__ gates) {
-    extern __shared__ double2 gw_smem[];
-    const int T = 1 << w.b;
-    double2 *tile = gw_smem;
-    uint64_t *hitab = reinterpret_cast<uint64_t *>(gw_smem + T);
-    const int tid = threadIdx.x, nth = blockDim.x;
-    double2 *s = psi + (uint64_t)blockIdx.y * nbasis;
-    const uint64_t base = gw_pdep((uint64_t)blockIdx.x, w.cmask);
-    for (int h = tid; h < (T >> w.L); h += nth) hitab[h] = gw_pdep((uint64_t)h << w.L, w.qmask);
-    __syncthreads();
-    const int lmask = (1 << w.L) - 1;
-    for (int l = tid; l < T; l += nth) tile[l] = s[base | hitab[l >> w.L] | (uint64_t)(l & lmask)];
-    __syncthreads();
-    for (int gi = 0; gi < w.ng; ++gi) {
-        const WGate *g = gates + w.g0 + gi;
-        const int kind = __ldg(&g->kind), t = __ldg(&g->t), c = __ldg(&g->c);
-        if (kind == K_GEN) {
-            const uint32_t nz = __ldg(&g->nz);
-            const int lo = min(t, c), hi = max(t, c);
-            for (int p = tid; p < (T >> 2); p += nth) {
-                const int b0 = (int)insert0(insert0((uint64_t)p, lo), hi);
-                const int idx[4] = {b0, b0 | (1 << t), b0 | (1 << c), b0 | (1 << t) | (1 << c)};
-                double2 x[4], y[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) x[j] = tile[idx[j]];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    double2 acc = make_double2(0.0, 0.0);
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        if (nz & (1u << (4 * i + j))) acc = c_add(acc, c_mul(__ldg(&g->m[4 * i + j]), x[j]));
-                    y[i] = acc;
-                }
-#pragma unroll
-                for (int i = 0; i < 4; ++i) tile[idx[i]] = y[i];
-            }
-        } else {
-            const double2 a = __ldg(&g->m[0]), bb = __ldg(&g->m[1]), cc = __ldg(&g->m[2]),
-                          d = __ldg(&g->m[3]);
-            const int dset = __ldg(&g->diag_set);
-            const int npair = (c < 0) ? (T >> 1) : (T >> 2);
-            const int lo = (c < 0) ? t : min(t, c), hi = (c < 0) ? -1 : max(t, c);
-            for (int p = tid; p < npair; p += nth) {
-                int i0 = (int)insert0((uint64_t)p, lo);
-                if (hi >= 0) i0 = (int)insert0((uint64_t)i0, hi) | (1 << c);
-                const int i1 = i0 | (1 << t);
-                if (kind == K_DENSE) {
-                    const double2 x0 = tile[i0], x1 = tile[i1];
-                    tile[i0] = c_add(c_mul(a, x0), c_mul(bb, x1));
-                    tile[i1] = c_add(c_mul(cc, x0), c_mul(d, x1));
-                } else if (kind == K_DIAG) {
-                    if (dset & 1) tile[i0] = c_mul(a, tile[i0]);
-                    if (dset & 2) tile[i1] = c_mul(d, tile[i1]);
-                } else if (kind == K_SWAP) {
-                    const double2 x0 = tile[i0], x1 = tile[i1];
-                    tile[i0] = x1;
-                    tile[i1] = x0;
-                } else {
-                    const double2 x0 = tile[i0], x1 = tile[i1];
-                    tile[i0] = c_mul(bb, x1);
-                    tile[i1] = c_mul(cc, x0);
-                }
-            }
-        }
-        __syncthreads();
-    }
-    for (int l = tid; l < T; l += nth) s[base | hitab[l >> w.L] | (uint64_t)(l & lmask)] = tile[l];
-}
 
 __global__ void k_scale(double2 *__restrict__ psi, uint64_t n, double2 a) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -409,19 +328,49 @@ int launch_single(qfb_state s, const HGate &h) {
     return QFB_OK;
 }
 
-constexpr int kGateTileDefault = 11;  // 2^11 amplitudes = 32 KB of shared memory per tile
-constexpr int kGateTileMax = 13;
+constexpr int kGateTileDefault = 10;  // 2^10 amplitudes = 18 KB of shared memory per tile
+constexpr int kGateTileMax = 12;
 int g_gate_tile_bits = 0;  // 0: kGateTileDefault; -1: one pass per gate
-int g_gate_low_bits = 4;
+int g_gate_low_bits = 3;
 
-int gate_window_smem() {
+int g_gate_reg_bits = 0;  // 0: default
+
+// Register bits R of a tile of b qubits: 2^(b-R) threads (<= 256) hold 2^R
+// amplitudes each.  Default 3 (8 amplitudes, 80 registers a thread, three
+// CTAs an SM); qfb_gates_regs may ask for another value, clamped to the tile.
+inline int tile_reg_bits(int b) {
+    const int lo = std::max(2, b - 8), hi = std::min(qfbt::kMaxRegBits, std::max(2, b - 2));
+    const int want = g_gate_reg_bits > 0 ? g_gate_reg_bits : 3;
+    return std::min(hi, std::max(lo, want));
+}
+
+// Tile shape for an n-qubit state: false when every gate takes its own pass
+// (tile_bits -1, or a state smaller than two 128-byte chunks).
+bool gate_tile_shape(int n, int &b, int &L) {
+    b = g_gate_tile_bits == 0 ? kGateTileDefault : g_gate_tile_bits;
+    if (b < 0 || n < 4) return false;
+    L = std::max(3, std::min(g_gate_low_bits, n));
+    b = std::max(4, std::min(b, n));
+    b = std::max(b, std::min(n, L + 2));  // room for any 2-qubit gate beside the low qubits
+    return true;
+}
+
+int gate_tile_smem() {
     static std::once_flag once;
     static cudaError_t err = cudaSuccess;
     std::call_once(once, [] {
-        const int bytes = (int)(sizeof(double2) << kGateTileMax) + (int)(sizeof(uint64_t) << kGateTileMax);
-        err = cudaFuncSetAttribute(k_gate_window, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        auto bytes = [](int b) { return (int)(sizeof(double2) * qfbt::tpad_size(b) + 16); };
+        err = cudaFuncSetAttribute(qfbt::k_gate_tile<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   bytes(10));
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(qfbt::k_gate_tile<3>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes(11));
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(qfbt::k_gate_tile<4>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       bytes(kGateTileMax));
     });
-    return err == cudaSuccess ? QFB_OK : cuda_fail(err, "gate window shared memory");
+    return err == cudaSuccess ? QFB_OK : cuda_fail(err, "gate tile shared memory");
 }
 
 struct GatePlanWin {
@@ -464,6 +413,11 @@ void plan_gate_windows(const std::vector<HGate> &hg, int n, int b, int L,
                 blocked |= gm;
             }
         }
+        if (sel.empty()) {
+            // the first unapplied gate fits no tile of this shape: its own pass
+            sel.push_back(first);
+            done[first] = 1;
+        }
         while (first < N && done[first]) ++first;
         GatePlanWin pw{};
         if (sel.size() == 1) {
@@ -505,6 +459,233 @@ void plan_gate_windows(const std::vector<HGate> &hg, int n, int b, int L,
     }
 }
 
+struct TilePlan {
+    std::vector<qfbt::TPhase> ph;
+    std::vector<qfbt::TOp> ops;
+    std::vector<double2> m4;
+    std::vector<uint64_t> chunks;   // per run: global offset of each 8-amplitude chunk
+    std::vector<uint32_t> threads;  // per phase: tl | tpad(tl) << 16 of each thread
+};
+
+// The bits of v, lowest first, placed on the set bits of m.
+uint64_t deposit_host(uint64_t v, uint64_t m) {
+    uint64_t r = 0;
+    for (; m; m &= m - 1, v >>= 1)
+        if (v & 1ull) r |= m & (~m + 1);
+    return r;
+}
+
+// The 4x4 matrix of SWAP exactly (unit entries at (0,0), (1,2), (2,1), (3,3)).
+bool is_swap4(const WGate &g) {
+    const uint32_t want = (1u << 0) | (1u << 6) | (1u << 9) | (1u << 15);
+    if (g.nz != want) return false;
+    for (int e : {0, 6, 9, 15})
+        if (g.m[e].x != 1.0 || g.m[e].y != 0.0) return false;
+    return true;
+}
+
+// Split a run's gates (tile coordinates) into phases of R register bits.
+// Scanning the unplaced gates in order, a gate joins the current phase when
+// no earlier unplaced gate shares one of its tile bits and its mixing bits
+// fit in the phase's R register bits together with those already chosen; a
+// gate that cannot join blocks its bits for the rest of the scan, so only
+// gates on disjoint qubits change order.
+void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, TilePlan &tp) {
+    std::vector<uint32_t> mix((size_t)ng), qm((size_t)ng);
+    for (int i = 0; i < ng; ++i) {
+        const WGate &w = g[i];
+        if (w.kind == K_GEN) {
+            qm[i] = mix[i] = (1u << w.t) | (1u << w.c);
+        } else {
+            qm[i] = (1u << w.t) | (w.c >= 0 ? 1u << w.c : 0u);
+            mix[i] = (w.kind == K_DIAG) ? 0u : (1u << w.t);
+        }
+    }
+    const uint32_t all = (1u << b) - 1u;
+    std::vector<char> done((size_t)ng, 0);
+    std::vector<int> sel;
+    int first = 0;
+    run.p0 = (int)tp.ph.size();
+    while (first < ng) {
+        uint32_t S = 0, blocked = 0;
+        sel.clear();
+        for (int i = first; i < ng; ++i) {
+            if (done[i]) continue;
+            if (qm[i] & blocked) {
+                blocked |= qm[i];
+                continue;
+            }
+            if (__builtin_popcount(S | mix[i]) <= R) {
+                S |= mix[i];
+                sel.push_back(i);
+                done[i] = 1;
+            } else {
+                blocked |= qm[i];
+            }
+        }
+        while (first < ng && done[first]) ++first;
+        // complete S to R bits, each filler from the residue class (tile bit
+        // mod 3) that keeps the most bits among the thread bits
+        while (__builtin_popcount(S) < R) {
+            int best = -1, bestn = -1;
+            for (int p = b - 1; p >= 0; --p) {
+                if (S >> p & 1u) continue;
+                int cnt = 0;
+                for (int q = 0; q < b; ++q)
+                    if (!(S >> q & 1u) && q % 3 == p % 3) ++cnt;
+                if (cnt > bestn) {
+                    bestn = cnt;
+                    best = p;
+                }
+            }
+            S |= 1u << best;
+        }
+        // thread bits; the three lowest (a quarter warp) from distinct classes
+        const uint32_t T = all & ~S;
+        std::vector<int> tb;
+        for (int cls = 0; cls < 3; ++cls)
+            for (int p = 0; p < b; ++p)
+                if ((T >> p & 1u) && p % 3 == cls) {
+                    tb.push_back(p);
+                    break;
+                }
+        for (int p = 0; p < b; ++p)
+            if ((T >> p & 1u) && std::find(tb.begin(), tb.end(), p) == tb.end()) tb.push_back(p);
+        qfbt::TPhase ph{};
+        // physical register position of each tile bit in S, and whether its
+        // register bit holds the complement of the tile bit: uncontrolled
+        // exchanges on a register bit (X) and SWAPs of two register bits are
+        // relabelings, applied here instead of on the device
+        int pos[32], flip[32];
+        for (int p = 0, k = 0; p < b; ++p) {
+            pos[p] = (S >> p & 1u) ? k++ : -1;
+            flip[p] = 0;
+        }
+        for (int k = 0; k < (1 << R); ++k) {
+            uint32_t l = 0;
+            for (int p = 0; p < b; ++p)
+                if (pos[p] >= 0 && (k >> pos[p] & 1)) l |= 1u << p;
+            ph.roff[k] = qfbt::tpad(l);
+        }
+        ph.th0 = (int)tp.threads.size();
+        for (uint32_t tid = 0; tid < (1u << (b - R)); ++tid) {
+            uint32_t tl = 0;
+            for (size_t j = 0; j < tb.size(); ++j)
+                if (tid >> j & 1u) tl |= 1u << tb[j];
+            tp.threads.push_back(tl | (qfbt::tpad(tl) << 16));
+        }
+        ph.o0 = (int)tp.ops.size();
+        auto swap2 = [](double2 &x, double2 &y) {
+            const double2 t = x;
+            x = y;
+            y = t;
+        };
+        for (int i : sel) {
+            const WGate &w = g[i];
+            if (w.kind == K_GEN && is_swap4(w)) {
+                std::swap(pos[w.t], pos[w.c]);
+                std::swap(flip[w.t], flip[w.c]);
+                continue;
+            }
+            if (w.kind == K_SWAP && w.c < 0) {
+                flip[w.t] ^= 1;
+                continue;
+            }
+            qfbt::TOp o{};
+            uint32_t opc = 0;
+            if (w.kind == K_GEN) {
+                opc = qfbt::OPC_GEN4 + (uint32_t)(4 * pos[w.t] + pos[w.c]);
+                const int fm = flip[w.t] | (flip[w.c] << 1);
+                o.aux = (uint32_t)tp.m4.size();
+                for (int r = 0; r < 4; ++r)
+                    for (int c = 0; c < 4; ++c) {
+                        const int k = 4 * (r ^ fm) + (c ^ fm);
+                        tp.m4.push_back((w.nz >> k & 1u) ? w.m[k] : make_double2(0.0, 0.0));
+                    }
+            } else {
+                uint32_t cm = 0, cv = 0;
+                if (w.c >= 0) {
+                    if (S >> w.c & 1u) {  // control on a register bit
+                        cm = 1u << pos[w.c];
+                        cv = flip[w.c] ? 0u : cm;
+                    } else {  // control on one of the thread's bits
+                        o.tctl = 1u << w.c;
+                    }
+                }
+                double2 a = w.m[0], bb = w.m[1], cc = w.m[2], d = w.m[3];
+                const bool fl = (S >> w.t & 1u) && flip[w.t];
+                if (fl) {  // the register bit holds the complement: conjugate by X
+                    swap2(a, d);
+                    swap2(bb, cc);
+                }
+                o.m[0] = a;
+                o.m[1] = bb;
+                o.m[2] = cc;
+                o.m[3] = d;
+                if (w.kind == K_DIAG) {
+                    uint32_t dset = (uint32_t)w.diag_set;
+                    if (fl) dset = ((dset & 1u) << 1) | ((dset >> 1) & 1u);
+                    if (dset == 0) continue;  // identity: no arithmetic
+                    if (S >> w.t & 1u) {
+                        opc = qfbt::OPC_DIAG + 4u * (dset - 1u) + (uint32_t)pos[w.t];
+                        o.aux = cm | (cv << 16);
+                    } else {
+                        opc = qfbt::OPC_DIAG_THREAD;
+                        o.tbit = 1u << w.t;
+                        o.aux = cm | (dset << 8) | (cv << 16);
+                    }
+                } else {
+                    uint32_t kind;
+                    if (w.kind == K_SWAP)
+                        kind = qfbt::OP_PSWAP;
+                    else if (w.kind == K_ANTI)
+                        kind = qfbt::OP_ANTI;
+                    else if (a.y == 0.0 && bb.y == 0.0 && cc.y == 0.0 && d.y == 0.0)
+                        kind = qfbt::OP_REAL;
+                    else if (a.y == 0.0 && d.y == 0.0 && bb.x == 0.0 && cc.x == 0.0)
+                        kind = qfbt::OP_RXI;
+                    else
+                        kind = qfbt::OP_DENSE;
+                    opc = 4u * kind + (uint32_t)pos[w.t];
+                    o.aux = cm | (cv << 16);
+                }
+            }
+            o.opc = opc;
+            tp.ops.push_back(o);
+        }
+        // store offsets: physical register k holds, for each tile bit p of S,
+        // the value (bit pos[p] of k) ^ flip[p]
+        for (int k = 0; k < (1 << R); ++k) {
+            uint32_t l = 0;
+            for (int p = 0; p < b; ++p)
+                if (pos[p] >= 0 && (((k >> pos[p]) & 1) ^ flip[p])) l |= 1u << p;
+            ph.soff[k] = qfbt::tpad(l);
+        }
+        ph.no = (int)tp.ops.size() - ph.o0;
+        tp.ph.push_back(ph);
+    }
+    run.np = (int)tp.ph.size() - run.p0;
+    run.b = b;
+}
+
+// Runs of a gate list and the phases of each run.
+void plan_gate_tiles(const std::vector<HGate> &hg, int n, int b, int L,
+                     std::vector<GatePlanWin> &wins, TilePlan &tp, std::vector<qfbt::TRun> &runs) {
+    std::vector<WGate> wg;
+    plan_gate_windows(hg, n, b, L, wins, wg);
+    runs.assign(wins.size(), qfbt::TRun{});
+    for (size_t i = 0; i < wins.size(); ++i) {
+        const GatePlanWin &pw = wins[i];
+        if (pw.single >= 0) continue;
+        qfbt::TRun &r = runs[i];
+        r.qmask = pw.w.qmask;
+        r.ch0 = (int)tp.chunks.size();
+        for (uint64_t c = 0; c < (1ull << (pw.w.b - 3)); ++c)
+            tp.chunks.push_back(deposit_host(c, pw.w.qmask & ~7ull));
+        plan_tile_phases(wg.data() + pw.w.g0, pw.w.ng, pw.w.b, tile_reg_bits(pw.w.b), r, tp);
+    }
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -527,9 +708,25 @@ int qfb_set_stream(void *stream) {
     return QFB_OK;
 }
 
+// After a stream synchronisation: report (and clear) a bounded device wait
+// that gave up since the last check.
+static int check_device_waits() {
+    int v = 0;
+    QFB_CUDA(cudaMemcpyFromSymbolAsync(&v, qfbt::g_tile_wait_err, sizeof(int), 0,
+                                       cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    if (v == 0) return QFB_OK;
+    const int zero = 0;
+    QFB_CUDA(cudaMemcpyToSymbolAsync(qfbt::g_tile_wait_err, &zero, sizeof(int), 0,
+                                     cudaMemcpyHostToDevice, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return fail(QFB_ETIMEDOUT, "a gate tile's bulk copies did not complete within 2 s; "
+                               "the state is not valid");
+}
+
 int qfb_sync(void) {
     QFB_CUDA(cudaStreamSynchronize(t_stream));
-    return QFB_OK;
+    return check_device_waits();
 }
 
 int qfb_launch_count(uint64_t *out) {
@@ -684,7 +881,7 @@ int qfb_state_download(qfb_state s, int b, qfb_complex *host, uint64_t n) {
     QFB_CUDA(cudaMemcpyAsync(host, s->d + (uint64_t)b * s->nbasis, n * sizeof(double2),
                              cudaMemcpyDeviceToHost, t_stream));
     QFB_CUDA(cudaStreamSynchronize(t_stream));
-    return QFB_OK;
+    return check_device_waits();
 }
 
 int qfb_state_get_amp(qfb_state s, int b, uint64_t index, qfb_complex *out) {
@@ -705,6 +902,14 @@ int qfb_gates_config(int tile_bits, int low_bits) {
                     low_bits + 2, kGateTileMax);
     g_gate_tile_bits = tile_bits;
     g_gate_low_bits = low_bits;
+    return QFB_OK;
+}
+
+int qfb_gates_regs(int reg_bits) {
+    if (reg_bits < 0 || reg_bits > qfbt::kMaxRegBits)
+        return fail(QFB_EINVAL, "qfb_gates_regs: reg_bits = %d outside [0, %d]", reg_bits,
+                    qfbt::kMaxRegBits);
+    g_gate_reg_bits = reg_bits;
     return QFB_OK;
 }
 
@@ -730,14 +935,14 @@ int qfb_gates_plan(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t *w
     };
     int64_t nw = 0, ns = 0;
     double bytes = 0.0;
-    int b = g_gate_tile_bits == 0 ? kGateTileDefault : g_gate_tile_bits;
-    if (b < 0 || ngates == 1) {
+    int b = 0, L = 0;
+    if (!gate_tile_shape(nqubit, b, L) || ngates == 1) {
         for (const HGate &h : hg) bytes += single_bytes(h);
         ns = ngates;
     } else {
         std::vector<GatePlanWin> wins;
         std::vector<WGate> wg;
-        plan_gate_windows(hg, nqubit, std::min(b, nqubit), std::min(g_gate_low_bits, nqubit), wins, wg);
+        plan_gate_windows(hg, nqubit, b, L, wins, wg);
         for (const GatePlanWin &pw : wins) {
             if (pw.single >= 0) {
                 ++ns;
@@ -751,6 +956,33 @@ int qfb_gates_plan(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t *w
     if (windows) *windows = nw;
     if (single_passes) *single_passes = ns;
     if (pass_bytes) *pass_bytes = bytes;
+    return QFB_OK;
+}
+
+int qfb_gates_phases(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t *phases,
+                     int64_t *ops) {
+    if (ngates < 0 || (ngates > 0 && !gates) || nqubit < 1 || nqubit > 40)
+        return fail(QFB_EINVAL, "qfb_gates_phases: bad arguments");
+    std::vector<HGate> hg((size_t)ngates);
+    for (int64_t k = 0; k < ngates; ++k) {
+        const qfb_gate &g = gates[k];
+        if (g.target < 0 || g.target >= nqubit || g.control < 0 || g.control >= nqubit)
+            return fail(QFB_EINVAL, "qfb_gates_phases: gate %lld acts beyond qubit %d",
+                        (long long)k, nqubit);
+        hg[k] = classify_gate(g);
+    }
+    int b = 0, L = 0;
+    int64_t np = 0, no = 0;
+    if (gate_tile_shape(nqubit, b, L) && ngates > 1) {
+        std::vector<GatePlanWin> wins;
+        TilePlan tp;
+        std::vector<qfbt::TRun> runs;
+        plan_gate_tiles(hg, nqubit, b, L, wins, tp, runs);
+        np = (int64_t)tp.ph.size();
+        no = (int64_t)tp.ops.size();
+    }
+    if (phases) *phases = np;
+    if (ops) *ops = no;
     return QFB_OK;
 }
 
@@ -769,37 +1001,65 @@ int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates) {
     std::vector<HGate> hg((size_t)ngates);
     for (int64_t k = 0; k < ngates; ++k) hg[k] = classify_gate(gates[k]);
     const int n = s->nqubit;
-    int b = g_gate_tile_bits == 0 ? kGateTileDefault : g_gate_tile_bits;
-    if (b < 0 || ngates == 1) {
+    int b = 0, L = 0;
+    if (!gate_tile_shape(n, b, L) || ngates == 1) {
         for (const HGate &h : hg) {
             const int rc = launch_single(s, h);
             if (rc) return rc;
         }
         return QFB_OK;
     }
-    int L = std::min(g_gate_low_bits, n);
-    b = std::min(b, n);
     std::vector<GatePlanWin> wins;
-    std::vector<WGate> wg;
-    plan_gate_windows(hg, n, b, L, wins, wg);
+    TilePlan tp;
+    std::vector<qfbt::TRun> runs;
+    plan_gate_tiles(hg, n, b, L, wins, tp, runs);
+    // one upload of phases, ops and 4x4 matrices
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t bp = al(sizeof(qfbt::TPhase) * tp.ph.size());
+    const size_t bo = al(sizeof(qfbt::TOp) * tp.ops.size());
+    const size_t bm = al(sizeof(double2) * tp.m4.size());
+    const size_t bc = al(sizeof(uint64_t) * tp.chunks.size());
+    const size_t bt = sizeof(uint32_t) * tp.threads.size();
     void *buf = nullptr;
-    if (!wg.empty()) {
-        int rc = dev_alloc(&buf, sizeof(WGate) * wg.size());
+    if (!tp.ph.empty()) {
+        std::vector<unsigned char> host(bp + bo + bm + bc + bt);
+        auto put = [&](size_t off, const void *src, size_t n) {
+            if (n) std::memcpy(host.data() + off, src, n);
+        };
+        put(0, tp.ph.data(), sizeof(qfbt::TPhase) * tp.ph.size());
+        put(bp, tp.ops.data(), sizeof(qfbt::TOp) * tp.ops.size());
+        put(bp + bo, tp.m4.data(), sizeof(double2) * tp.m4.size());
+        put(bp + bo + bm, tp.chunks.data(), sizeof(uint64_t) * tp.chunks.size());
+        put(bp + bo + bm + bc, tp.threads.data(), bt);
+        int rc = dev_alloc(&buf, host.size());
         if (rc) return rc;
-        QFB_CUDA(cudaMemcpyAsync(buf, wg.data(), sizeof(WGate) * wg.size(), cudaMemcpyHostToDevice,
-                                 t_stream));
+        QFB_CUDA(cudaMemcpyAsync(buf, host.data(), host.size(), cudaMemcpyHostToDevice, t_stream));
     }
-    int rc = gate_window_smem();
-    for (const GatePlanWin &pw : wins) {
-        if (rc) break;
+    unsigned char *ub = (unsigned char *)buf;
+    const qfbt::TPhase *d_ph = (const qfbt::TPhase *)ub;
+    const qfbt::TOp *d_ops = (const qfbt::TOp *)(ub + bp);
+    const double2 *d_m4 = (const double2 *)(ub + bp + bo);
+    const uint64_t *d_ch = (const uint64_t *)(ub + bp + bo + bm);
+    const uint32_t *d_th = (const uint32_t *)(ub + bp + bo + bm + bc);
+    int rc = gate_tile_smem();
+    for (size_t i = 0; i < wins.size() && rc == QFB_OK; ++i) {
+        const GatePlanWin &pw = wins[i];
         if (pw.single >= 0) {
             rc = launch_single(s, hg[pw.single]);
             continue;
         }
-        const size_t smem = sizeof(double2) * ((size_t)1 << pw.w.b) +
-                            sizeof(uint64_t) * ((size_t)1 << (pw.w.b - pw.w.L));
-        const dim3 grid((unsigned)(s->nbasis >> pw.w.b), s->nbatch);
-        k_gate_window<<<grid, 256, smem, t_stream>>>(s->d, s->nbasis, pw.w, (const WGate *)buf);
+        const int tb = pw.w.b, R = tile_reg_bits(tb);
+        const size_t smem = sizeof(double2) * qfbt::tpad_size(tb) + 16;
+        const dim3 grid((unsigned)(s->nbasis >> tb), s->nbatch), block(1u << (tb - R));
+        if (R == 2)
+            qfbt::k_gate_tile<2><<<grid, block, smem, t_stream>>>(s->d, s->nbasis, runs[i], d_ph,
+                                                                  d_ops, d_m4, d_ch, d_th);
+        else if (R == 3)
+            qfbt::k_gate_tile<3><<<grid, block, smem, t_stream>>>(s->d, s->nbasis, runs[i], d_ph,
+                                                                  d_ops, d_m4, d_ch, d_th);
+        else
+            qfbt::k_gate_tile<4><<<grid, block, smem, t_stream>>>(s->d, s->nbasis, runs[i], d_ph,
+                                                                  d_ops, d_m4, d_ch, d_th);
         rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
     }
     dev_free(buf);

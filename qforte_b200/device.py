@@ -175,7 +175,18 @@ def gate_plan(gates, nqubit):
     return w.value, s.value, b.value
 
 
-def gates_config(tile_bits=0, low_bits=4):
+def gate_phases(gates, nqubit):
+    """(register phases, gate operations) of the tile runs of ``gates`` on one
+    ``nqubit`` state under the current tile shape; host only."""
+    arr = pack_gates(gates)
+    p, o = ctypes.c_int64(), ctypes.c_int64()
+    check(lib().qfb_gates_phases(arr.ctypes.data if len(arr) else None, len(arr), int(nqubit),
+                                 ctypes.byref(p), ctypes.byref(o)), "qfb_gates_phases")
+    return p.value, o.value
+
+
+def gates_config(tile_bits=0, low_bits=3, reg_bits=0):
     """Process-wide tile shape of gate runs (tile_bits 0: default, -1: one
-    pass per gate)."""
+    pass per gate; reg_bits 0: default register bits per thread)."""
     check(lib().qfb_gates_config(int(tile_bits), int(low_bits)), "qfb_gates_config")
+    check(lib().qfb_gates_regs(int(reg_bits)), "qfb_gates_regs")

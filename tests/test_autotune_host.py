@@ -12,14 +12,14 @@ from qforte_b200.device import gates_config
 
 def test_cache_round_trip(tmp_path, monkeypatch):
     monkeypatch.setenv("QFB_TUNE_CACHE", str(tmp_path / "t.json"))
-    autotune._store(autotune.gate_key(28), [12, 4])
+    autotune._store(autotune.gate_key(28), [11, 4, 3])
     autotune._store("ucc:n=20:nparam=875:batch=64", [12, 11, 3])
     d = json.loads((tmp_path / "t.json").read_text())
-    assert d["gates:n=28"] == [12, 4] and d["ucc:n=20:nparam=875:batch=64"] == [12, 11, 3]
+    assert d["gates:n=28"] == [11, 4, 3] and d["ucc:n=20:nparam=875:batch=64"] == [12, 11, 3]
     try:
-        assert autotune.apply_cached(nqubit=28) == {"gates": (12, 4)}
+        assert autotune.apply_cached(nqubit=28) == {"gates": (11, 4, 3)}
     finally:
-        gates_config(0, 4)
+        gates_config(0, 3)
     assert autotune.apply_cached(nqubit=30) == {}
 
 

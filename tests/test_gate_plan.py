@@ -1,6 +1,7 @@
 """Host-side planning of gate runs (no GPU): how many shared-memory tile runs
 and one-gate passes a circuit becomes, and the bytes those passes move."""
 
+import numpy as np
 import pytest
 
 import qforte_b200 as qb
@@ -11,7 +12,7 @@ from qforte_b200.workloads import layered_random_circuit
 @pytest.fixture(autouse=True)
 def _default_tiles():
     yield
-    gates_config(0, 4)
+    gates_config(0, 3)
 
 
 def test_small_state_is_one_run():
@@ -37,9 +38,9 @@ def test_sweep_runs_fuse_layers():
     circ, spec = layered_random_circuit(24, 20, 2)
     w, s, b = gate_plan(circ.gates(), 24)
     assert 0 < w + s < len(spec) / 4
-    gates_config(13, 4)
-    w13, s13, _ = gate_plan(circ.gates(), 24)
-    assert w13 + s13 <= w + s
+    gates_config(12, 4)
+    w12, s12, _ = gate_plan(circ.gates(), 24)
+    assert w12 + s12 <= w + s
 
 
 def test_plan_rejects_gates_beyond_the_state():
@@ -47,3 +48,29 @@ def test_plan_rejects_gates_beyond_the_state():
         gate_plan([qb.gate("X", 5, 5)], 4)
     with pytest.raises(ValueError):
         gates_config(20, 4)
+
+
+@pytest.mark.parametrize("tile,low", [(2, 0), (4, 1), (6, 3), (9, 4), (10, 3), (11, 3), (12, 3),
+                                      (12, 6)])
+@pytest.mark.parametrize("n", [3, 4, 5, 8, 14])
+def test_every_gate_is_planned_once(tile, low, n):
+    """Planning ends for every tile shape (including tiles too narrow for some
+    2-qubit gates); tile runs carry at most the gates not given their own pass
+    (exchanges and SWAPs on register bits become relabelings, identities
+    nothing)."""
+    from qforte_b200.device import gate_phases
+    rng = np.random.default_rng(n * 100 + tile)
+    gates = []
+    for _ in range(150):
+        if rng.random() < 0.5:
+            t = int(rng.integers(n))
+            gates.append(qb.gate(["H", "T", "Rx", "Y"][int(rng.integers(4))], t, t, 0.3))
+        elif n > 1:
+            t, c = (int(v) for v in rng.choice(n, 2, replace=False))
+            gates.append(qb.gate(["cX", "cZ", "SWAP", "A"][int(rng.integers(4))], t, c, 0.7))
+    gates_config(tile, low)
+    w, s, _ = gate_plan(gates, n)
+    phases, ops = gate_phases(gates, n)
+    assert ops + s <= len(gates)
+    assert (w == 0) == (phases == 0)
+    assert w <= phases

@@ -18,16 +18,16 @@ def test_tune_gates_and_results_unchanged(cuda, tmp_path, monkeypatch):
     monkeypatch.setenv("QFB_TUNE_CACHE", str(tmp_path / "t.json"))
     circ, spec = layered_random_circuit(15, 6, 2)
     try:
-        (tile, low), timings = autotune.tune_gates(circ, 15, reps=1)
-        assert len(timings) >= 5 and f"{tile},{low}" in timings
+        shape, timings = autotune.tune_gates(circ, 15, reps=1)
+        assert len(timings) >= 5 and ",".join(map(str, shape)) in timings
         qc = qb.Computer(15)
         qc.apply_circuit(circ)
         st = O.State(15)
         st.apply_gates([O.make_gate(k, t, c, p) for k, t, c, p in spec])
         assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < 1e-12
-        assert autotune.apply_cached(nqubit=15)["gates"] == (tile, low)
+        assert autotune.apply_cached(nqubit=15)["gates"] == shape
     finally:
-        gates_config(0, 4)
+        gates_config(0, 3)
 
 
 def test_tune_evaluator_full_space_windows(cuda, tmp_path, monkeypatch):

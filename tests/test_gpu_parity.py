@@ -328,10 +328,11 @@ def gate_tiles():
     """Restores the default gate tile shape after a test changes it."""
     from qforte_b200._lib import check, lib
     yield lambda b, L: check(lib().qfb_gates_config(b, L), "qfb_gates_config")
-    check(lib().qfb_gates_config(0, 4), "qfb_gates_config")
+    check(lib().qfb_gates_config(0, 3), "qfb_gates_config")
 
 
-@pytest.mark.parametrize("tile,low", [(-1, 4), (0, 4), (2, 0), (4, 1), (6, 3), (9, 4), (13, 6)])
+@pytest.mark.parametrize("tile,low", [(-1, 4), (0, 4), (2, 0), (4, 1), (6, 3), (9, 4), (10, 3),
+                                      (11, 3), (12, 3), (12, 6)])
 @pytest.mark.parametrize("n,ngates,seed", [(3, 80, 5), (8, 300, 6), (14, 200, 7)])
 def test_gate_windows_match_oracle(cuda, gate_tiles, tile, low, n, ngates, seed):
     """Gate runs applied to shared-memory tiles of every shape (and one pass
