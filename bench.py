@@ -51,11 +51,12 @@ def parse():
     ap.add_argument("--full-space", action="store_true",
                     help="keep full-space states (no compact sector evaluator)")
     ap.add_argument("--workload", default="ucc",
-                    choices=["ucc", "gates", "grad", "adapt", "serve", "pexp"],
+                    choices=["ucc", "gates", "grad", "adapt", "serve", "pexp", "pqe"],
                     help="ucc: batched dUCCSD energy+gradient (default); gates: the gate sweep; "
                          "grad: differentiable energy, forward+backward against forward alone; "
                          "adapt: every ADAPT pool gradient of a 12-operator state in one launch; "
-                         "pexp: Pauli-exponential passes on one large state")
+                         "pexp: Pauli-exponential passes on one large state; "
+                         "pqe: batched PQE residual vectors")
     ap.add_argument("--pexp-n", type=int, default=28, help="pexp: qubits")
     ap.add_argument("--pexp-strings", type=int, default=64,
                     help="pexp: random Pauli strings, and dUCC operators, per program")
@@ -421,6 +422,127 @@ def run_pexp(a, local):
     return line
 
 
+def run_pqe(a, local):
+    """PQE residual vectors (UCCNPQE.get_residual_vector) for a batch of
+    parameter sets of the dUCCSD problem: psi, H psi, U^dagger on sigma and
+    the projections on the excited determinants in one graph launch, against
+    the reference's recipe through the Computer API call for call and the
+    compiled reference on the host."""
+    import time
+    import torch
+    from qforte_b200._lib import launch_count
+    from qforte_b200.ucc import DUCC, UCCNPQE, excited_determinants
+    torch.cuda.set_device(local)
+    mol, pool = problem(a.norb, a.seed)
+    tops = list(range(len(pool)))
+    M = len(tops)
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+    rng = np.random.default_rng(a.seed + 3)
+    P = rng.uniform(-0.1, 0.1, (a.batch, M))
+    dets = excited_determinants(pool, tops, mol.hf_reference)
+    E, R = eng.residuals(P, dets)
+    ev = eng.evaluator(a.batch)
+    d_params = ev.tensors()[0]
+    d_params.copy_(torch.from_numpy(P))
+    for _ in range(max(a.warmup, 3)):
+        ev.run(4)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        ev.run(4)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    launches = (launch_count() - l0) // a.steps
+    t_end = time.perf_counter() + max(0.0, 0.8 - a.steps * ms / 1000.0)
+    while time.perf_counter() < t_end:
+        ev.run(4)
+        torch.cuda.synchronize()
+    ck = clocks.stop()
+    # end to end: host parameters in, residuals out, every step
+    hP = torch.from_numpy(P).pin_memory()
+    hR = torch.empty((a.batch, len(dets)), dtype=torch.float64).pin_memory()
+
+    def view(addr, shape):
+        class _I:
+            __cuda_array_interface__ = {"shape": shape, "typestr": "<f8",
+                                        "data": (int(addr), False), "version": 2}
+        return torch.as_tensor(_I(), device="cuda")
+
+    d_res = view(ev.d_res, (a.batch, len(dets)))
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(a.steps):
+        d_params.copy_(hP, non_blocking=True)
+        ev.run(4)
+        hR.copy_(d_res, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / a.steps
+    assert np.max(np.abs(hR.numpy() - R)) < 1e-12
+    # plain per-call path: the reference's recipe through the Computer API
+    drv = UCCNPQE(mol, engine="percall")
+    drv._pool_obj = pool
+    drv._tops, drv._tamps = tops, list(P[0])
+    drv._excited_dets = dets
+    drv._noise_factor = 0.0
+    drv._res_vec_evals = drv._res_m_evals = 0
+    drv.get_residual_vector(P[0])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r_plain = np.array(drv.get_residual_vector(P[0]))
+    t_plain = time.perf_counter() - t0
+    line = {"metric": "PQE residual vectors/s", "value": 1000.0 * a.batch / ms, "unit": "vectors/s",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic",
+            "config": {"workload": f"PQE residuals of the dUCCSD problem, {2 * a.norb} qubits "
+                                   f"({a.norb} orbitals), {M} residuals, {a.batch} parameter "
+                                   "sets per step"},
+            "e2e": {"value": 1000.0 * a.batch / ms_e2e, "unit": "vectors/s",
+                    "h2d_bytes_per_step": int(P.nbytes), "d2h_bytes_per_step": int(hR.numel() * 8)},
+            "evaluator_path": ev.path, "gpu_launches": int(launches), "clocks": ck,
+            "plain_per_call": {"value": 1.0 / t_plain, "unit": "vectors/s",
+                               "max_abs_diff_vs_batched": float(np.max(np.abs(r_plain - R[0])))},
+            "batched_vs_plain": (1000.0 * a.batch / ms) * t_plain}
+    if not a.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            from qforte_b200.pauli import letters
+            import qforte_b200 as qb
+
+            def terms(qo):
+                return [(complex(c), letters(*circ._pauli_masks()[:2])) for c, circ in qo.terms()]
+
+            qf = O.load_reference_engine()
+            kf = []
+            for _, op in pool:
+                sq = qb.SQOperator()
+                sq.add_op(op)
+                q = sq.jw_transform()
+                q.simplify()
+                q.order_terms()
+                kf.append(terms(q))
+            ht = terms(mol.hamiltonian)
+            hs = max(1, len(ht) // 10)
+            t, parts = O.ref_pqe_sample(qf, 2 * a.norb, mol.hf_reference, kf, list(P[0]), ht, hs)
+            line["cpu_baseline"] = {"value": 1.0 / t, "unit": "vectors/s", "cores": 1,
+                                    "kind": "reference",
+                                    "sample": f"one get_residual_vector: U and U^dagger as gates in "
+                                              f"full, apply_operator(H) on {hs} of {len(ht)} "
+                                              "terms scaled; serial shipped build",
+                                    "parts_s": parts}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    print(json.dumps(line))
+    return line
+
+
 def run_grad(a, local):
     """Differentiable dUCCSD energy: forward (energy) and forward+backward
     (energy and the adjoint gradient through torch.autograd) per parameter
@@ -677,6 +799,10 @@ def main():
     if a.workload == "pexp":
         if rank == 0:
             run_pexp(a, local)
+        return
+    if a.workload == "pqe":
+        if rank == 0:
+            run_pqe(a, local)
         return
 
     import torch

@@ -255,6 +255,18 @@ QFB_API int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool);
 QFB_API int qfb_ucc_pool_buffer(qfb_ucc u, double **d_pool_grad);
 /* Host convenience: params in, energies and pool gradients out, synchronous. */
 QFB_API int qfb_ucc_eval_pool(qfb_ucc u, const double *params, double *energy, double *pool_grad);
+/* PQE residuals (UCCNPQE.get_residual_vector, uccnpqe.py:249-292): give the
+ * evaluator n excited determinants I_k (full-space basis indices) and their
+ * phase factors (uccnpqe.py:193-247); a run of mode 4 then computes psi,
+ * sigma = H psi, the energy and res[b][k] = Re(<I_k|U^dagger H U|ref> *
+ * phase_k) into a device block [nbatch][n] (qfb_ucc_residual_buffer), in one
+ * graph launch when captured.  U^dagger is the ansatz program in reverse with
+ * negated angles, applied to sigma (which the run consumes). */
+QFB_API int qfb_ucc_set_residuals(qfb_ucc u, const uint64_t *dets, const qfb_complex *phases,
+                                  int32_t n);
+QFB_API int qfb_ucc_residual_buffer(qfb_ucc u, double **d_res);
+/* Host convenience: params in, energies and residuals out, synchronous. */
+QFB_API int qfb_ucc_eval_residuals(qfb_ucc u, const double *params, double *energy, double *res);
 /* Device addresses of the parameter block and the outputs. */
 QFB_API int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_grad);
 /* Enqueue one evaluation on the calling thread's stream (replays the
@@ -262,7 +274,8 @@ QFB_API int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, dou
  * 1 energy and gradient; 2 the gradient sweep alone, on the psi and sigma a
  * preceding with_grad = 0 run left (the sweep un-rotates them in place, so a
  * second mode-2 run needs a new mode-0 run first); 3 energy and the pool
- * gradients (qfb_ucc_set_pool). */
+ * gradients (qfb_ucc_set_pool); 4 energy and the PQE residuals
+ * (qfb_ucc_set_residuals). */
 QFB_API int qfb_ucc_run(qfb_ucc u, int with_grad);
 /* Capture one evaluation of the given mode into a CUDA graph (replayed by
  * later runs). */

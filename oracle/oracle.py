@@ -357,6 +357,27 @@ def measure_gradient(nqubit, ref, kops, amps, hterms, kops_grad=None, kops_unrot
     return grads
 
 
+def pqe_residuals(nqubit, ref, kops, amps, hterms, excited_dets):
+    """UCCNPQE.get_residual_vector (ucc/uccnpqe.py:249-292): Uprep, U(t), H,
+    U(t)^dagger (the adjoint circuit), then coeff[I] * phase for each excited
+    determinant (I, phase)."""
+    st = State(nqubit)
+    st.apply_gates(refprep(ref))
+    gates, phase = trotterize(ansatz_terms(kops, amps))
+    if phase != 1.0:
+        raise ValueError("Encountered phase change")
+    st.apply_gates(gates)
+    st.apply_pauli_operator(hterms)
+    st.apply_gates(circuit_adjoint(gates))
+    out = []
+    for I, ph in excited_dets:
+        r = st.psi[int(I)] * ph
+        if abs(r.imag) > 1.0e-12:
+            raise ValueError("residual has imaginary component")
+        out.append(r.real)
+    return np.array(out)
+
+
 def measure_gradient3(nqubit, ref, kops, amps, hterms, pool_kops):
     """ADAPT pool gradients 2 Re <H psi| K_mu psi>, abc/uccvqeabc.py:253-283."""
     psi = prepare_state(nqubit, ref, kops, amps)
@@ -468,6 +489,35 @@ def ref_trotter(qf, terms, factor=1.0):
     for c, term in terms:
         circ.add(ref_exponential(qf, factor * complex(c), term))
     return circ
+
+
+def ref_pqe_sample(qf, nqubit, ref, kops_fwd, amps, hterms, h_sample):
+    """Time one UCCNPQE.get_residual_vector of the compiled reference
+    (uccnpqe.py:249-292) on a bounded sample: refprep and U(t) as gates, then
+    apply_operator on ``h_sample`` of the H terms scaled to all of them, then
+    U(t)^dagger as gates and the coefficient read-back.  Returns seconds per
+    residual vector."""
+    import time
+
+    t0 = time.perf_counter()
+    qc = qf.Computer(nqubit)
+    prep = qf.Circuit()
+    for j, occ in enumerate(ref):
+        if occ:
+            prep.add(qf.gate("X", j, j))
+    qc.apply_circuit(prep)
+    U = ref_trotter(qf, ansatz_terms(kops_fwd, amps))
+    qc.apply_circuit(U)
+    t_u = time.perf_counter() - t0
+    hs = ref_operator(qf, hterms[:h_sample])
+    t0 = time.perf_counter()
+    qc.apply_operator(hs)
+    t_h = (time.perf_counter() - t0) * len(hterms) / max(1, min(h_sample, len(hterms)))
+    t0 = time.perf_counter()
+    qc.apply_circuit(U.adjoint())
+    qc.get_coeff_vec()
+    t_ud = time.perf_counter() - t0
+    return t_u + t_h + t_ud, {"t_U": t_u, "t_H": t_h, "t_Udagger": t_ud}
 
 
 def ref_eval_sample(qf, nqubit, ref, kops_fwd, kops_grad, amps, hterms, h_sample, m_sample):

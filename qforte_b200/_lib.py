@@ -81,6 +81,9 @@ SIGNATURES = {
     "qfb_ucc_sector": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_memory": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_set_pool": (ctypes.c_int, [_vp, c_prog]),
+    "qfb_ucc_set_residuals": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
+    "qfb_ucc_residual_buffer": (ctypes.c_int, [_vp, _vp]),
+    "qfb_ucc_eval_residuals": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "qfb_ucc_pool_buffer": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_eval_pool": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "qfb_ucc_path": (ctypes.c_int, [_vp, _vp]),

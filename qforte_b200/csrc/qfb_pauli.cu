@@ -808,6 +808,22 @@ __global__ void __launch_bounds__(256) k_pool_ip(const double2 *__restrict__ psi
 
 // grad[b * M + mu] = 2 Re sum over mu's steps s and chunks c of
 // partial[((s * B) + b) * chunks + c].  grid = (M, B).
+// res[b][k] = Re(st[idx[k] * s_i + b * s_b] * phase[k]) (0 where idx[k] < 0)
+__global__ void k_resid_gather(const double2 *__restrict__ st, const int64_t *__restrict__ idx,
+                               uint64_t s_i, uint64_t s_b, const double2 *__restrict__ phase,
+                               int nres, int B, double *__restrict__ res) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nres * B) return;
+    const int b = (int)(t / nres), k = (int)(t % nres);
+    const int64_t i = idx[k];
+    double r = 0.0;
+    if (i >= 0) {
+        const double2 v = st[(uint64_t)i * s_i + (uint64_t)b * s_b], ph = phase[k];
+        r = v.x * ph.x - v.y * ph.y;
+    }
+    res[(size_t)b * nres + k] = r;
+}
+
 __global__ void k_grad_final(const double2 *__restrict__ partial, const int2 *__restrict__ psteps,
                              int chunks, double *__restrict__ grad) {
     const int mu = blockIdx.x, b = blockIdx.y, B = gridDim.y, M = gridDim.x;
@@ -2423,8 +2439,8 @@ struct qfb_ucc_s {
     double2 *vpart = nullptr, *gpart = nullptr;
     int2 *psteps = nullptr;
     cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};  // by run mode
-    uint64_t graph_kernels[4] = {0, 0, 0, 0};
+    cudaGraphExec_t exec[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // by run mode
+    uint64_t graph_kernels[5] = {0, 0, 0, 0, 0};
     // particle-number sector of the state (every program conserves it):
     // H psi is formed on these indices only; nsec == 0 means the full space
     int64_t nsec = 0;
@@ -2457,6 +2473,14 @@ struct qfb_ucc_s {
     StepDev *pool_steps = nullptr;  // full space: the pool's steps on the device
     unsigned pchunks = 1;
     qfbs::SStream pstream{};   // compact: the pool's inner-product records
+    // PQE residuals (qfb_ucc_set_residuals): Re(<I_k|U^dagger H U|ref> phase_k)
+    int nres = 0;
+    void *rblob = nullptr;
+    size_t rbytes = 0;
+    double *res = nullptr;            // [B][nres]
+    const int64_t *ridx = nullptr;    // full-space index, or compact index (-1: outside)
+    const double2 *rphase = nullptr;  // [nres]
+    qfbs::SStream rstream{};          // compact: forward records in reverse order
 };
 
 // Reorder the entries of every H row so that each run of 8 consecutive
@@ -2771,6 +2795,9 @@ static int sector_smem_attr() {
         if (err == cudaSuccess)
             err = cudaFuncSetAttribute(qfbs::k_sector_sweep,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(qfbs::k_sector_resid,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
     });
     return err == cudaSuccess ? QFB_OK : cuda_fail(err, "sector evaluator shared memory");
 }
@@ -2983,16 +3010,57 @@ static int ucc_pool_stage(qfb_ucc u) {
     return QFB_OK;
 }
 
+// Residual stage (qfb_ucc_set_residuals): U^dagger on sigma, then the
+// residual entries.  Sigma is consumed.
+static int ucc_resid_stage(qfb_ucc u) {
+    if (!u->rblob) return fail(QFB_EINVAL, "qfb_ucc_run: no residuals set (qfb_ucc_set_residuals)");
+    const int B = u->nbatch;
+    const unsigned gg = (unsigned)(((int64_t)u->nres * B + 255) / 256);
+    if (u->compact) {
+        const qfbs::SLaunch &L = u->SL;
+        const size_t smem = sizeof(double2) * ((size_t)L.nsec + (size_t)u->rstream.n) +
+                            sizeof(uint4) * 3 * (size_t)u->rstream.maxw;
+        qfbs::k_sector_resid<<<B, kSectorThreads, smem, t_stream>>>(L, u->rstream, u->ridx,
+                                                                   u->rphase, u->nres, u->res);
+        QFB_LAUNCHED();
+        return QFB_OK;
+    }
+    if (u->gsec) {
+        qfbg::GLaunch Ls = u->GL;  // rotate sigma: the step kernel rotates L.psi
+        Ls.psi = u->GL.sig;
+        const SectorPlan &sp = *u->splan;
+        const dim3 grid(u->g_sgrid, u->g_ygrid);
+        for (size_t r = sp.fwd.span.size(); r-- > 0;) {
+            qfbg::k_cg_step<true, false, false><<<grid, 256, 0, t_stream>>>(
+                Ls, u->g_frec + sp.fwd.span[r].x, sp.fwd.param[r], -1, -1, nullptr);
+            QFB_LAUNCHED();
+        }
+        k_resid_gather<<<gg, 256, 0, t_stream>>>(u->GL.sig, u->ridx, (uint64_t)B, 1, u->rphase,
+                                                 u->nres, B, u->res);
+        QFB_LAUNCHED();
+        return QFB_OK;
+    }
+    int rc = enqueue_prog(u->fwd, u->sig, u->nqubit, B, u->params, 0, -1);
+    if (rc) return rc;
+    k_resid_gather<<<gg, 256, 0, t_stream>>>(u->sig, u->ridx, 1, u->nbasis, u->rphase, u->nres, B,
+                                             u->res);
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
 // mode 0: energy (stages 0-2); 1: energy and gradient (0-3); 2: the gradient
 // sweep alone (stage 3) on psi and sigma as a mode-0 run left them; 3: energy
-// and the pool's gradients (stages 0-2, then the pool stage).
+// and the pool's gradients (stages 0-2, then the pool stage); 4: energy and
+// the PQE residuals (stages 0-2, then the residual stage).
 static int ucc_enqueue(qfb_ucc u, int mode) {
-    const int last = (mode == 3) ? 2 : 3;
+    const int last = (mode == 3 || mode == 4) ? 2 : 3;
     for (int st = (mode == 2 ? 3 : 0); st <= last; ++st) {
         int rc = ucc_stage(u, st, mode == 1 || mode == 2);
         if (rc) return rc;
     }
-    return mode == 3 ? ucc_pool_stage(u) : QFB_OK;
+    if (mode == 3) return ucc_pool_stage(u);
+    if (mode == 4) return ucc_resid_stage(u);
+    return QFB_OK;
 }
 
 extern "C" {
@@ -3237,6 +3305,7 @@ int qfb_ucc_sector(qfb_ucc u, int64_t *nsec) {
 int qfb_ucc_destroy(qfb_ucc u) {
     if (!u) return QFB_OK;
     dev_free(u->pblob);
+    dev_free(u->rblob);
     for (auto &x : u->exec)
         if (x) cudaGraphExecDestroy(x);
     if (u->cap_stream) cudaStreamDestroy(u->cap_stream);
@@ -3334,6 +3403,104 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
     return QFB_OK;
 }
 
+int qfb_ucc_set_residuals(qfb_ucc u, const uint64_t *dets, const qfb_complex *phases, int32_t n) {
+    if (!u || n < 1 || !dets || !phases)
+        return fail(QFB_EINVAL, "qfb_ucc_set_residuals: bad arguments");
+    for (int32_t k = 0; k < n; ++k)
+        if (dets[k] >> u->nqubit)
+            return fail(QFB_EINVAL, "qfb_ucc_set_residuals: determinant %d beyond qubit %d", k,
+                        u->nqubit);
+    std::vector<int64_t> idx((size_t)n);
+    for (int32_t k = 0; k < n; ++k) {
+        if (u->compact || u->gsec) {
+            const SectorPlan &sp = *u->splan;
+            const int32_t ra = sp.arank[pext_parity_bits(dets[k], 0, u->nqubit)];
+            const int32_t rb = sp.brank[pext_parity_bits(dets[k], 1, u->nqubit)];
+            idx[k] = (ra < 0 || rb < 0) ? -1 : (int64_t)ra * sp.nbeta + rb;
+        } else {
+            idx[k] = (int64_t)dets[k];
+        }
+    }
+    // compact, shared memory: the forward records in reverse order
+    std::vector<int2> rspan;
+    std::vector<int32_t> rparam;
+    if (u->compact) {
+        const SectorPlan &sp = *u->splan;
+        for (size_t r = sp.fwd.span.size(); r-- > 0;) {
+            rspan.push_back(sp.fwd.span[r]);
+            rparam.push_back(sp.fwd.param[r]);
+        }
+    }
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const int B = u->nbatch;
+    const size_t o_res = 0, o_idx = al(sizeof(double) * (size_t)B * n),
+                 o_ph = o_idx + al(sizeof(int64_t) * n), o_sp = o_ph + al(sizeof(double2) * n),
+                 o_pa = o_sp + al(sizeof(int2) * std::max<size_t>(1, rspan.size())),
+                 total = o_pa + sizeof(int32_t) * std::max<size_t>(1, rparam.size());
+    void *blob = nullptr;
+    int rc = dev_alloc(&blob, total);
+    if (rc) return rc;
+    char *bp = (char *)blob;
+    std::vector<double2> ph((size_t)n);
+    for (int32_t k = 0; k < n; ++k) ph[k] = make_double2(phases[k].re, phases[k].im);
+    QFB_CUDA(cudaMemcpyAsync(bp + o_idx, idx.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice,
+                             t_stream));
+    QFB_CUDA(cudaMemcpyAsync(bp + o_ph, ph.data(), sizeof(double2) * n, cudaMemcpyHostToDevice,
+                             t_stream));
+    if (!rspan.empty()) {
+        QFB_CUDA(cudaMemcpyAsync(bp + o_sp, rspan.data(), sizeof(int2) * rspan.size(),
+                                 cudaMemcpyHostToDevice, t_stream));
+        QFB_CUDA(cudaMemcpyAsync(bp + o_pa, rparam.data(), sizeof(int32_t) * rparam.size(),
+                                 cudaMemcpyHostToDevice, t_stream));
+    }
+    QFB_CUDA(cudaMemsetAsync(bp + o_res, 0, sizeof(double) * (size_t)B * n, t_stream));
+    if (u->exec[4]) {  // a captured residual run refers to the old buffers
+        cudaGraphExecDestroy(u->exec[4]);
+        u->exec[4] = nullptr;
+    }
+    if (u->rblob) {
+        u->bytes -= u->rbytes;
+        dev_free(u->rblob);
+    }
+    u->rblob = blob;
+    u->rbytes = total;
+    u->bytes += total;
+    u->nres = n;
+    u->res = (double *)(bp + o_res);
+    u->ridx = (const int64_t *)(bp + o_idx);
+    u->rphase = (const double2 *)(bp + o_ph);
+    if (u->compact) {
+        u->rstream = u->SL.fwd;
+        u->rstream.span = (const int2 *)(bp + o_sp);
+        u->rstream.param = (const int32_t *)(bp + o_pa);
+    }
+    return QFB_OK;
+}
+
+int qfb_ucc_residual_buffer(qfb_ucc u, double **d_res) {
+    if (!u || !d_res) return fail(QFB_EINVAL, "qfb_ucc_residual_buffer: null argument");
+    if (!u->rblob) return fail(QFB_EINVAL, "qfb_ucc_residual_buffer: no residuals set");
+    *d_res = u->res;
+    return QFB_OK;
+}
+
+int qfb_ucc_eval_residuals(qfb_ucc u, const double *params, double *energy, double *res) {
+    if (!u || !energy || !res) return fail(QFB_EINVAL, "qfb_ucc_eval_residuals: null argument");
+    if (!u->rblob) return fail(QFB_EINVAL, "qfb_ucc_eval_residuals: no residuals set");
+    if (u->nparam > 0 && !params) return fail(QFB_EINVAL, "qfb_ucc_eval_residuals: null parameters");
+    const size_t np = (size_t)u->nbatch * u->nparam;
+    if (np) QFB_CUDA(cudaMemcpyAsync(u->params, params, sizeof(double) * np,
+                                     cudaMemcpyHostToDevice, t_stream));
+    int rc = qfb_ucc_run(u, 4);
+    if (rc) return rc;
+    QFB_CUDA(cudaMemcpyAsync(energy, u->energy, sizeof(double) * u->nbatch,
+                             cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaMemcpyAsync(res, u->res, sizeof(double) * u->nbatch * u->nres,
+                             cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
 int qfb_ucc_eval_pool(qfb_ucc u, const double *params, double *energy, double *pool_grad) {
     if (!u || !energy || !pool_grad) return fail(QFB_EINVAL, "qfb_ucc_eval_pool: null argument");
     if (!u->pool) return fail(QFB_EINVAL, "qfb_ucc_eval_pool: no pool set");
@@ -3374,7 +3541,7 @@ int qfb_ucc_buffers(qfb_ucc u, double **d_params, double **d_energy, double **d_
 
 int qfb_ucc_run(qfb_ucc u, int with_grad) {
     if (!u) return fail(QFB_EINVAL, "qfb_ucc_run: null evaluator");
-    if (with_grad < 0 || with_grad > 3) return fail(QFB_EINVAL, "qfb_ucc_run: mode %d", with_grad);
+    if (with_grad < 0 || with_grad > 4) return fail(QFB_EINVAL, "qfb_ucc_run: mode %d", with_grad);
     const int k = with_grad;
     if (u->exec[k]) {
         QFB_CUDA(cudaGraphLaunch(u->exec[k], t_stream));
@@ -3386,7 +3553,7 @@ int qfb_ucc_run(qfb_ucc u, int with_grad) {
 
 int qfb_ucc_capture(qfb_ucc u, int with_grad) {
     if (!u) return fail(QFB_EINVAL, "qfb_ucc_capture: null evaluator");
-    if (with_grad < 0 || with_grad > 3)
+    if (with_grad < 0 || with_grad > 4)
         return fail(QFB_EINVAL, "qfb_ucc_capture: mode %d", with_grad);
     const int k = with_grad;
     if (u->exec[k]) return QFB_OK;

@@ -285,6 +285,35 @@ __global__ void __launch_bounds__(512) k_sector_sweep(SLaunch L) {
     s_run<true>(L, L.sweep, s_cs, s_rec, psi, sig);
 }
 
+// PQE residuals on the compact states: sigma of slot blockIdx.x from the save
+// buffer, U^dagger applied to it in shared memory (stream R: the forward
+// records in reverse order, angles negated), then
+// res[b][k] = Re(sigma[idx[k]] * phase[k]) (0 where idx[k] < 0).
+__global__ void __launch_bounds__(512, 2) k_sector_resid(SLaunch L, SStream R,
+                                                         const int64_t *__restrict__ idx,
+                                                         const double2 *__restrict__ phase,
+                                                         int nres, double *__restrict__ res) {
+    extern __shared__ double2 s_mem[];
+    double2 *sig = s_mem, *s_cs = s_mem + L.nsec;
+    uint4 *s_rec = reinterpret_cast<uint4 *>(s_cs + R.n);
+    const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    const double *par = L.params + (size_t)b * L.nparam;
+    const double2 *sv = L.save + (size_t)b * 2 * L.nsec + L.nsec;
+    for (int i = tid; i < L.nsec; i += nth) sig[i] = sv[i];
+    s_angles(R, par, -1, s_cs);
+    __syncthreads();
+    s_run<false>(L, R, s_cs, s_rec, sig, nullptr);
+    for (int k = tid; k < nres; k += nth) {
+        const int64_t i = idx[k];
+        double r = 0.0;
+        if (i >= 0) {
+            const double2 v = sig[i], ph = phase[k];
+            r = v.x * ph.x - v.y * ph.y;
+        }
+        res[(size_t)b * nres + k] = r;
+    }
+}
+
 // Pool inner products on the compact states: each CTA loads psi and sigma of
 // slot blockIdx.y and runs the inner-product records r = blockIdx.x,
 // blockIdx.x + gridDim.x, ... of the pool stream (records leave the states

@@ -10,6 +10,8 @@ Hamiltonian, then evaluates, for one parameter vector or a batch of them:
                    (UCCVQE.measure_gradient, abc/uccvqeabc.py:122-251)
 * ``pool_gradients``  2 Re <H psi|K_k psi> for every pool operator
                    (UCCVQE.measure_gradient3, abc/uccvqeabc.py:253-283)
+* ``residuals``    the energy and the PQE residuals <I_mu|U^dagger H U|ref>
+                   (UCCNPQE.get_residual_vector, ucc/uccnpqe.py:249-292)
 
 The forward program holds, per selected operator mu, the JW strings of
 t_mu * tau_mu in the order ``get_qubit_operator('commuting_grp_lex')``
@@ -17,8 +19,8 @@ gives them (abc/ansatz.py:25-82, sq_op_pool.cc:97-104); the gradient program
 holds K_mu = c_mu * JW(tau_mu) in ``jw_transform`` order.  The strings of one
 excitation share their x-mask, so each excitation is one fused pass.
 
-``UCCNVQE`` and ``ADAPTVQE`` are thin drivers with the reference's
-energy/gradient entry points.  ``engine='percall'`` runs the same numbers
+``UCCNVQE``, ``ADAPTVQE`` and ``UCCNPQE`` are thin drivers with the
+reference's energy/gradient/residual entry points.  ``engine='percall'`` runs the same numbers
 through the public ``Computer`` API call for call as the reference's
 drivers do (state copies, apply_operator, vdot per parameter) -- the plain
 per-call path the fused engine is compared against.
@@ -34,6 +36,7 @@ from ._lib import check, lib, ptr
 from .circuit import Circuit
 from .computer import Computer, _new_state, inner_product
 from .device import prog_from_strings, sum_from_terms
+from .gate import gate
 from .sq_op_pool import SQOpPool
 from .sq_operator import SQOperator
 from .utils import build_refprep, ref_to_basis_idx, trotterize
@@ -139,11 +142,41 @@ class Evaluator:
         self.generation += 1
         return e, g
 
+    def set_residuals(self, dets, phases):
+        """Give the evaluator the PQE excited determinants (basis indices) and
+        their phase factors; eval_residuals / run(4) then return the residuals."""
+        d = np.ascontiguousarray(dets, dtype=np.uint64)
+        ph = np.ascontiguousarray(phases, dtype=np.complex128)
+        if d.shape != ph.shape or d.ndim != 1 or len(d) == 0:
+            raise ValueError("set_residuals: one phase per determinant, at least one")
+        check(lib().qfb_ucc_set_residuals(self.h, ptr(d), ptr(ph), len(d)),
+              "qfb_ucc_set_residuals")
+        self.nres = len(d)
+        r = ctypes.c_void_p()
+        check(lib().qfb_ucc_residual_buffer(self.h, ctypes.byref(r)), "qfb_ucc_residual_buffer")
+        self.d_res = r.value
+        self._captured.discard(4)
+
+    def eval_residuals(self, P):
+        """Energies and the PQE residuals Re(<I_k|U^dagger H U|ref> phase_k) per row."""
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        if P.shape != (self.nbatch, self.nparam):
+            raise ValueError(f"parameters of shape {P.shape}, expected "
+                             f"{(self.nbatch, self.nparam)}")
+        self._ensure_graph(4)
+        e = np.empty(self.nbatch)
+        r = np.empty((self.nbatch, self.nres))
+        check(lib().qfb_ucc_eval_residuals(self.h, ptr(P), ptr(e), ptr(r)),
+              "qfb_ucc_eval_residuals")
+        self.generation += 1
+        return e, r
+
     def run(self, with_grad=True):
         """Enqueue one evaluation on the library's stream (device buffers in and
         out, no host synchronisation).  ``with_grad`` 0/False: energies; 1/True:
         energies and gradients; 2: the gradient sweep alone on the states the
-        last energy-only run left."""
+        last energy-only run left; 3: energies and pool gradients (set_pool);
+        4: energies and PQE residuals (set_residuals)."""
         mode = int(with_grad)
         self._ensure_graph(mode)
         check(lib().qfb_ucc_run(self.h, mode), "qfb_ucc_run")
@@ -239,6 +272,46 @@ def gradient_strings(pool, tops, qubit_excitations=False):
         S += sc
         P += [mu] * len(sc)
     return X, Z, S, P
+
+
+def _creators_annihilators(sq_op, ref):
+    """Creation and annihilation indices of a particle-hole excitation read
+    as acting on the reference (uccnpqe.py:197-207, ansatz.py:136-144)."""
+    t = sq_op.terms()[0]
+    if ref[t[2][-1]]:
+        return t[1], t[2]
+    return t[2], t[1]
+
+
+def excited_determinants(pool, tops, ref, qubit_excitations=False):
+    """(basis index, phase factor) of each operator's excited determinant
+    (UCCNPQE.fill_excited_dets, uccnpqe.py:193-247): the reference with the
+    operator's annihilators emptied and creators filled, and the coefficient
+    of that determinant in JW(operator)|ref>."""
+    ref_idx = ref_to_basis_idx(ref)
+    out = []
+    for top in tops:
+        sq_op = pool[top][1]
+        creators, annihilators = _creators_annihilators(sq_op, ref)
+        det = list(ref)
+        for p in reversed(annihilators):
+            if det[p] == 0:
+                raise ValueError("no ops should destroy reference, something went wrong!!")
+            det[p] = 0
+        for p in reversed(creators):
+            if det[p] == 1:
+                raise ValueError("no ops should destroy reference, something went wrong!!")
+            det[p] = 1
+        I = ref_to_basis_idx(det)
+        q = sq_op.jw_transform(qubit_excitations)
+        phase = 0.0 + 0.0j
+        for c, x, z in q._pauli_terms(applied=True):
+            if ref_idx ^ x == I:
+                ny = bin(x & z).count("1")
+                sgn = -1.0 if bin(ref_idx & z).count("1") & 1 else 1.0
+                phase += complex(c) * (1j ** ny) * sgn
+        out.append((I, phase))
+    return out
 
 
 class DUCC:
@@ -343,6 +416,29 @@ class DUCC:
         if np.ndim(params) == 1:
             return float(ev.real[0]), g[0]
         return ev.real, g
+
+    def residuals(self, params, dets=None):
+        """(energies, PQE residuals) for [nparam] or [batch, nparam] parameters:
+        Re(<I_k|U^dagger H U|ref> phase_k) for each excited determinant
+        (UCCNPQE.get_residual_vector, uccnpqe.py:249-292), all rows in one
+        graph-captured evaluator run (mode 4).  ``dets`` defaults to the
+        excited determinants of the ansatz operators."""
+        P = np.ascontiguousarray(np.atleast_2d(np.asarray(params, dtype=np.float64)))
+        if P.shape[1] != self.nparam:
+            raise ValueError(f"expected {self.nparam} parameters, got {P.shape[1]}")
+        if dets is None:
+            if getattr(self, "_exdets", None) is None:
+                self._exdets = excited_determinants(self._pool, self.tops, self.ref, self._qe)
+            dets = self._exdets
+        ev = self.evaluator(P.shape[0])
+        key = tuple(d for d, _ in dets)
+        if getattr(ev, "_res_key", None) != key:
+            ev.set_residuals([d for d, _ in dets], [ph for _, ph in dets])
+            ev._res_key = key
+        e, r = ev.eval_residuals(P)
+        if np.ndim(params) == 1:
+            return float(e[0]), r[0]
+        return e, r
 
     def _pool_sum_handle(self):
         if self._pool_sum is None:
@@ -576,6 +672,146 @@ class UCCNVQE(_UCCBase):
         self._tamps = list(res.x)
         self._final_result = res
         return self._Egs
+
+
+class UCCNPQE(_UCCBase):
+    """dUCC-PQE with all pool operators (ucc/uccnpqe.py:24-300): solve the
+    projective equations r_mu(t) = <I_mu|U^dagger H U|ref> = 0 by Jacobi
+    iterations with Moller-Plesset denominators and DIIS (maths/optimizer.py:
+    6-116).  Residuals come from the evaluator's residual run (psi, H psi,
+    U^dagger on sigma and the projections in one launch)."""
+
+    def run(self, pool_type="SD", opt_thresh=1.0e-5, opt_maxiter=40, noise_factor=0.0,
+            optimizer="jacobi", diis_max_dim=8):
+        if pool_type == "sa_SD":
+            raise ValueError("Must use single term particle-hole nbody operators for residual "
+                             "calculation")
+        if optimizer.lower() != "jacobi":
+            raise NotImplementedError("only the Jacobi solver is implemented")
+        self._pool_type = pool_type
+        self._opt_thresh = opt_thresh
+        self._opt_maxiter = opt_maxiter
+        self._noise_factor = noise_factor
+        self._diis_max_dim = diis_max_dim
+        self._res_vec_evals = 0
+        self._res_m_evals = 0
+        self.fill_pool()
+        self.initialize_ansatz()
+        self.fill_excited_dets()
+        self.build_orb_energies()
+        self.jacobi_solver()
+        return self._Egs
+
+    def initialize_ansatz(self):
+        self._tops = list(range(len(self._pool_obj)))
+        self._tamps = [0.0] * len(self._pool_obj)
+
+    def fill_excited_dets(self):
+        self._excited_dets = excited_determinants(self._pool_obj, self._tops, self._ref,
+                                                  self._qubit_excitations)
+
+    def build_orb_energies(self):
+        """Spin-orbital energies (abc/ansatz.py:84-119): the system's RHF
+        orbital energies when it has them, else from the reference energy
+        and its single flips."""
+        self._orb_e = []
+        if hasattr(self._sys, "hf_orbital_energies"):
+            for e in self._sys.hf_orbital_energies:
+                self._orb_e += [e] * 2
+            return
+        qc = Computer(self._nqb)
+        qc.apply_circuit(self._refprep)
+        E0 = float(np.real(qc.direct_op_exp_val(self._qb_ham)))
+        nocc = sum(self._ref)
+        for i in range(self._nqb):
+            qc = Computer(self._nqb)
+            qc.apply_circuit(self._refprep)
+            qc.apply_gate(gate("X", i, i))
+            Ei = float(np.real(qc.direct_op_exp_val(self._qb_ham)))
+            self._orb_e.append(E0 - Ei if i < nocc else Ei - E0)
+
+    def get_res_over_mpdenom(self, residuals):
+        out = []
+        for mu, m in enumerate(self._tops):
+            creators, annihilators = _creators_annihilators(self._pool_obj[m][1], self._ref)
+            denom = sum(self._orb_e[x] for x in annihilators) - sum(self._orb_e[x] for x in creators)
+            out.append(residuals[mu] / denom)
+        return out
+
+    def get_residual_vector(self, trial_amps):
+        p = np.asarray(trial_amps, dtype=np.float64)
+        if self._engine == "fused":
+            eng = self._engine_for_tops()
+            E, r = eng.residuals(p, self._excited_dets)
+            self._curr_energy = E
+        else:
+            r = self._residuals_percall(p)
+        r = np.asarray(r, dtype=np.float64)
+        if self._noise_factor > 1e-12:
+            r = np.random.normal(r, self._noise_factor)
+        self._res_vec_norm = float(np.linalg.norm(r))
+        self._res_vec_evals += 1
+        self._res_m_evals += len(self._tamps)
+        return list(r)
+
+    def _residuals_percall(self, params):
+        """uccnpqe.py:249-292 through the Computer API, call for call."""
+        U = self.ansatz_circuit(list(params))
+        qc = Computer(self._nqb)
+        qc.apply_circuit(self._Uprep)
+        qc.apply_circuit(U)
+        qc.apply_operator(self._qb_ham)
+        qc.apply_circuit(U.adjoint())
+        coeffs = qc.get_coeff_vec()
+        out = []
+        for I, ph in self._excited_dets:
+            r = coeffs[I] * ph
+            if abs(np.imag(r)) > 1.0e-12:
+                raise ValueError("residual has imaginary component, something went wrong!!")
+            out.append(float(np.real(r)))
+        return out
+
+    def jacobi_solver(self):
+        import copy
+        t_diis = [copy.deepcopy(self._tamps)]
+        e_diis = []
+        Ek = self.energy_feval(self._tamps)
+        self._energies = []
+        for _ in range(1, self._opt_maxiter + 1):
+            t_old = copy.deepcopy(self._tamps)
+            r_k = self.get_res_over_mpdenom(self.get_residual_vector(self._tamps))
+            self._tamps = list(np.add(self._tamps, r_k))
+            t_diis.append(copy.deepcopy(self._tamps))
+            e_diis.append(np.subtract(copy.deepcopy(self._tamps), t_old))
+            if self._diis_max_dim >= 2:
+                self._tamps = _diis(self._diis_max_dim, t_diis, e_diis)
+            Ek = self.energy_feval(self._tamps)
+            self._energies.append(Ek)
+            if self._res_vec_norm < self._opt_thresh:
+                break
+        self._Egs = Ek
+
+
+def _diis(diis_max_dim, t_diis, e_diis):
+    """DIIS extrapolation of the amplitudes (maths/optimizer.py:6-37)."""
+    import copy
+    if len(t_diis) > diis_max_dim:
+        del t_diis[0]
+        del e_diis[0]
+    dim = len(t_diis) - 1
+    B = np.ones((dim + 1, dim + 1)) * -1
+    bsol = np.zeros(dim + 1)
+    B[-1, -1] = 0.0
+    bsol[-1] = -1.0
+    for i, ei in enumerate(e_diis):
+        for j, ej in enumerate(e_diis):
+            B[i, j] = np.dot(np.real(ei), np.real(ej))
+    B[:-1, :-1] /= np.abs(B[:-1, :-1]).max()
+    x = np.linalg.lstsq(B, bsol, rcond=None)[0][:-1]
+    t_new = np.zeros(len(t_diis[0]))
+    for l in range(dim):
+        t_new = np.add(t_new, x[l] * np.asarray(t_diis[l + 1]))
+    return copy.deepcopy(list(np.real(t_new)))
 
 
 class ADAPTVQE(_UCCBase):

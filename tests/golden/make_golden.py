@@ -147,6 +147,37 @@ def ucc_fixture(qf, norb, seed, out):
     print(f"{out}: {nq} q, {len(hc)} H terms, {M} SD params, {P} GSD ops, E = {E:.12f}")
 
 
+def pqe_fixture(qf, norb, seed, out):
+    """UCCNPQE (ucc/uccnpqe.py): excited determinants and phase factors, and
+    the residual vector at seeded dUCCSD amplitudes."""
+    h, g = random_integrals(norb, seed)
+    H = ref_sq_ham(qf, h, g).jw_transform()
+    ref = hf_reference(norb, norb)
+    rng = np.random.default_rng(1000 + seed)
+    s = _Sys()
+    s.hamiltonian = H
+    s.hf_reference = ref
+    s.hf_energy = 0.0
+    alg = qf.UCCNPQE(s)
+    alg._pool_type = "SD"
+    alg._noise_factor = 0.0
+    alg._res_vec_evals = 0
+    alg._res_m_evals = 0
+    alg._excited_dets = []
+    alg._tops, alg._tamps = [], []
+    alg.fill_pool()
+    alg.initialize_ansatz()
+    alg.fill_excited_dets()
+    M = len(alg._tops)
+    amps = rng.uniform(-0.1, 0.1, M)
+    res = np.array(alg.get_residual_vector(list(amps)))
+    dets = np.array([d for d, _ in alg._excited_dets], dtype=np.uint64)
+    phases = np.array([complex(p) for _, p in alg._excited_dets], dtype=np.complex128)
+    np.savez_compressed(out, norb=norb, seed=seed, amps=amps, residuals=res, dets=dets,
+                        phases=phases)
+    print(f"{out}: {M} residuals")
+
+
 def pools_fixture(qf, norb, out):
     ref = hf_reference(norb, norb)
     arrs = {}
@@ -234,9 +265,15 @@ def integrals_fixture(path, out):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-src", default="/root/reference/src/qforte")
+    ap.add_argument("--only", default=None, help="one fixture family (pqe)")
     a = ap.parse_args()
     qf = O.load_reference(a.ref_src)
     tests_dir = os.path.join(os.path.dirname(a.ref_src.rstrip("/")), "..", "tests")
+    if a.only in ("pqe", None):
+        pqe_fixture(qf, 4, 11, os.path.join(HERE, "pqe_norb4_seed11.npz"))
+        pqe_fixture(qf, 6, 11, os.path.join(HERE, "pqe_norb6_seed11.npz"))
+    if a.only is not None:
+        return
     ucc_fixture(qf, 4, 11, os.path.join(HERE, "ucc_norb4_seed11.npz"))
     ucc_fixture(qf, 6, 11, os.path.join(HERE, "ucc_norb6_seed11.npz"))
     pools_fixture(qf, 4, os.path.join(HERE, "pools_norb4.npz"))

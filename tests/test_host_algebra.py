@@ -119,3 +119,15 @@ def test_jw_small_known_answer(ref_qforte):
         ta = [(complex(c), circ.str()) for c, circ in qa.terms()]
         tb = [(complex(c), circ.str()) for c, circ in qb_.terms()]
         assert ta == tb
+
+
+@pytest.mark.parametrize("name", ["pqe_norb4_seed11.npz", "pqe_norb6_seed11.npz"])
+def test_excited_determinants_match_reference(name):
+    """UCCNPQE.fill_excited_dets (uccnpqe.py:193-247): the same determinants
+    and phase factors as the reference, computed on the host."""
+    from qforte_b200.ucc import excited_determinants
+    z = golden(name)
+    mol, pool = random_problem(int(z["norb"]), int(z["seed"]))
+    ex = excited_determinants(pool, range(len(pool)), mol.hf_reference)
+    assert [d for d, _ in ex] == z["dets"].tolist()
+    assert np.max(np.abs(np.array([p for _, p in ex]) - z["phases"])) == 0.0

@@ -94,3 +94,17 @@ def test_oracle_operator_expval():
     s2.apply_pauli_operator(op)
     assert np.array_equal(s2.psi, z["op_psi"])
     assert st.direct_op_exp_val(op) == complex(z["op_expval"])
+
+
+@pytest.mark.parametrize("name", ["pqe_norb4_seed11.npz", "pqe_norb6_seed11.npz"])
+def test_oracle_pqe_residuals(name):
+    """The oracle's restatement of UCCNPQE.get_residual_vector reproduces the
+    reference's residuals at the same amplitudes (uccnpqe.py:249-292)."""
+    z = golden(name)
+    u = golden(name.replace("pqe_", "ucc_"))
+    mol, pool, hterms = _ucc_inputs(u)
+    nq = int(u["nqubit"])
+    tops = list(range(len(pool)))
+    dets = list(zip(z["dets"].tolist(), z["phases"].tolist()))
+    r = O.pqe_residuals(nq, list(u["ref"]), kops_forward(pool, tops), z["amps"], hterms, dets)
+    assert np.max(np.abs(r - z["residuals"])) < 1e-12
