@@ -39,7 +39,7 @@ from .device import prog_from_strings, sum_from_terms
 from .gate import gate
 from .sq_op_pool import SQOpPool
 from .sq_operator import SQOperator
-from .utils import build_refprep, ref_to_basis_idx, trotterize
+from .utils import build_refprep, compact_excitation_circuit, ref_to_basis_idx, trotterize
 
 __all__ = ["DUCC", "Evaluator", "evaluator_config", "UCCNVQE", "ADAPTVQE", "ansatz_strings", "gradient_strings"]
 
@@ -500,13 +500,16 @@ class DUCC:
 
 class _UCCBase:
     def __init__(self, system, reference=None, pool_type="SD", qubit_excitations=False,
-                 engine="fused", trotter_number=1):
+                 engine="fused", trotter_number=1, compact_excitations=False):
         self._sys = system
         self._ref = list(system.hf_reference if reference is None else reference)
         self._nqb = len(self._ref)
         self._qb_ham = system.hamiltonian
         self._pool_type = pool_type
         self._qubit_excitations = qubit_excitations
+        # compact (FEB / QEB) excitation circuits apply exp(t kappa) exactly, the
+        # unitary the fused program applies: only the per-call gate path differs
+        self._compact_excitations = compact_excitations
         self._engine = engine
         self._trotter_number = trotter_number
         self._refprep = build_refprep(self._ref)
@@ -547,6 +550,13 @@ class _UCCBase:
         else:
             for t, top in zip(tamps, self._tops):
                 temp.add(t, self._pool_obj[top][1])
+        if self._compact_excitations:
+            U = Circuit()
+            for t, sq_op in temp:
+                exc = sq_op.terms()[1]
+                U.add(compact_excitation_circuit(t * exc[0], exc[1], exc[2],
+                                                 self._qubit_excitations))
+            return U
         A = temp.get_qubit_operator("commuting_grp_lex", qubit_excitations=self._qubit_excitations)
         U, phase = trotterize(A, trotter_number=self._trotter_number)
         if phase != 1.0 + 0.0j:

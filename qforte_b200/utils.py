@@ -196,3 +196,106 @@ def smart_print(obj):
     if isinstance(obj, Computer):
         print("\n Quantum Computer:")
         print(obj.str())
+
+
+# ---------------------------------------------------------------------------
+# compact excitation circuits (utils/compact_excitation_circuits.py:9-291)
+# ---------------------------------------------------------------------------
+
+def compact_excitation_circuit(theta, creation, annihilation, qubit_excitations):
+    """Circuit of exp(theta * kappa) for a particle-number-conserving
+    fermionic (kappa = t - t^dagger) or qubit (Q - Q^dagger) excitation with
+    few CNOTs (utils/compact_excitation_circuits.py:9-91): a CNOT staircase
+    carrying the fermionic sign, a multi-qubit-controlled Ry between CNOT
+    ladders, the staircase undone.  The gate list equals the reference's gate
+    for gate, so results and CNOT counts match."""
+    creation, annihilation = list(creation), list(annihilation)
+    if len(creation) != len(annihilation):
+        raise ValueError("Compact fermionic/qubit excitations are implemented for "
+                         "particle-number-conserving operators only.")
+    shared = sorted(set(creation) & set(annihilation))
+    if len(shared) > 1:
+        raise ValueError("A GSD excitation of the form p^ q^ p q was encountered!")
+    cre_u = [p for p in creation if p not in annihilation]
+    ann_u = [p for p in annihilation if p not in creation]
+    gsd_sign, unique_stair = 1, False
+    if shared:
+        gsd_sign = -1
+        # the repeated index sits at the same position in both lists
+        pos = [i for i in range(2) for lst in (creation, annihilation) if lst[i] == shared[0]]
+        unique_stair = pos in ([0, 0], [1, 1])
+    circ = Circuit()
+    stair = None
+    if not qubit_excitations:
+        stair = (_fermion_sign_circuit(cre_u, ann_u) if unique_stair
+                 else _fermion_sign_circuit(creation, annihilation))
+        circ.add(stair)
+    circ.add(_qubit_excitation(theta, cre_u, ann_u, shared, gsd_sign, qubit_excitations))
+    if stair is not None:
+        circ.add(stair.adjoint())
+    return circ
+
+
+def _fermion_sign_circuit(creation, annihilation):
+    """CNOT staircase and one CZ that give the excitation's fermionic sign
+    (compact_excitation_circuits.py:94-149): the qubits below the operator
+    indices whose Jordan-Wigner Z strings survive the product, less the
+    operator indices themselves."""
+    ops = list(creation) + list(annihilation)
+    parity = {}
+    for p in ops:
+        for q in range(p):
+            parity[q] = parity.get(q, 0) ^ 1
+    keep = [q for q in range(max(ops) + 1) if parity.get(q, 0) and q not in ops]
+    keep.reverse()
+    circ = Circuit()
+    if not keep:
+        return circ
+    for a, b in zip(keep[1:], keep[:-1]):
+        circ.add(_gate("CNOT", a, b))
+    circ.add(_gate("cZ", creation[0], keep[-1]))
+    return circ
+
+
+def _qubit_excitation(theta, creation, annihilation, shared, gsd_sign, qubit_excitations):
+    """CNOT ladders around the multi-qubit-controlled Ry
+    (compact_excitation_circuits.py:152-207)."""
+    ladder = Circuit()
+    for t in creation[1:]:
+        ladder.add(_gate("CNOT", t, creation[0]))
+    for t in annihilation[1:]:
+        ladder.add(_gate("CNOT", t, annihilation[0]))
+    ladder.add(_gate("CNOT", annihilation[0], creation[0]))
+    circ = Circuit()
+    circ.add(ladder)
+    circ.add(_controlled_ry(theta, creation[0], creation[1:], annihilation, shared, gsd_sign,
+                            qubit_excitations))
+    circ.add(ladder.adjoint())
+    return circ
+
+
+def _controlled_ry(theta, target, ctrl_cre, ctrl_ann, shared, gsd_sign, qubit_excitations):
+    """Multi-qubit-controlled Ry(2 theta) as 2^c single-qubit Ry rotations of
+    +-theta / 2^(c-1) interleaved with CNOT / anti-controlled CNOT gates in
+    Gray-code order (compact_excitation_circuits.py:210-291)."""
+    controls = list(ctrl_ann) + list(reversed(ctrl_cre)) + list(shared)
+    c = len(controls)
+    n_ry = 1 << c
+    step = theta / (1 << (c - 1))
+    sign_f = 1
+    if not qubit_excitations:
+        # fermionic sign of the rotation angle by many-body rank
+        rank = len(ctrl_ann)
+        sign_f = -1
+        if rank == 1 or rank % 4 == 0 or (rank - 1) % 4 == 0:
+            sign_f = 1
+        sign_f *= gsd_sign
+    circ = Circuit()
+    for i in range(n_ry):
+        circ.add(_gate("Ry", target, target, (1 - 2 * (i % 2)) * sign_f * step))
+        for j, ctl in enumerate(controls):
+            if (i + 1) % (n_ry // (1 << (j + 1))) == 0:
+                last = (i + 1) % (n_ry // 2) == 0 or i == n_ry - 1
+                circ.add(_gate("CNOT" if (last or shared) else "aCNOT", target, ctl))
+                break
+    return circ

@@ -178,6 +178,64 @@ def pqe_fixture(qf, norb, seed, out):
     print(f"{out}: {M} residuals")
 
 
+def compact_fixture(qf, norb, seed, out):
+    """Compact (FEB / QEB) excitation circuits (utils/compact_excitation_circuits.py):
+    each pool operator's gate list at a seeded amplitude, and the state of the
+    whole compact ansatz on the reference, for SD, GSD and sa_SD pools with
+    fermionic and qubit excitations."""
+    from qforte.utils.compact_excitation_circuits import compact_excitation_circuit
+    ref = hf_reference(norb, norb)
+    rng = np.random.default_rng(2000 + seed)
+    arrs = {}
+    for pt in ("SD", "GSD", "sa_SD"):
+        pool = qf.SQOpPool()
+        pool.set_orb_spaces(ref)
+        pool.fill_pool(pt)
+        temp = []
+        for c, op in pool:
+            if pt == "sa_SD":
+                terms = op.terms()
+                for coeff, cr, an in terms[:len(terms) // 2]:
+                    s = qf.SQOperator()
+                    s.add_term(coeff, cr, an)
+                    s.add_term(-coeff, an, cr)
+                    temp.append(s)
+            else:
+                temp.append(op)
+        amps = rng.uniform(-0.5, 0.5, len(temp))
+        for qe in (False, True):
+            key = f"{pt}_{'qe' if qe else 'fe'}"
+            ids, tg, ct, pr, owner = [], [], [], [], []
+            U = qf.Circuit()
+            for k, (t, op) in enumerate(zip(amps, temp)):
+                e = op.terms()[1]
+                circ = compact_excitation_circuit(t * e[0], e[1], e[2], qe)
+                U.add(circ)
+                for g in circ.gates():
+                    ids.append(g.gate_id())
+                    tg.append(g.target())
+                    ct.append(g.control())
+                    pr.append(float(g.parameter()) if g.has_parameter() else 0.0)
+                    owner.append(k)
+            qc = qf.Computer(2 * norb)
+            prep = qf.Circuit()
+            for j, occ in enumerate(ref):
+                if occ:
+                    prep.add(qf.gate("X", j, j))
+            qc.apply_circuit(prep)
+            qc.apply_circuit(U)
+            arrs[f"{key}_ids"] = np.array(ids)
+            arrs[f"{key}_target"] = np.array(tg, dtype=np.int32)
+            arrs[f"{key}_control"] = np.array(ct, dtype=np.int32)
+            arrs[f"{key}_owner"] = np.array(owner, dtype=np.int32)
+            arrs[f"{key}_param"] = np.array(pr)
+            arrs[f"{key}_psi"] = np.array(qc.get_coeff_vec())
+            arrs[f"{key}_cnots"] = U.get_num_cnots()
+        arrs[f"{pt}_amps"] = amps
+    np.savez_compressed(out, norb=norb, **arrs)
+    print(f"{out}: compact circuits of {[k for k in arrs if k.endswith('_cnots')]}")
+
+
 def pools_fixture(qf, norb, out):
     ref = hf_reference(norb, norb)
     arrs = {}
@@ -265,10 +323,12 @@ def integrals_fixture(path, out):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-src", default="/root/reference/src/qforte")
-    ap.add_argument("--only", default=None, help="one fixture family (pqe)")
+    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact)")
     a = ap.parse_args()
     qf = O.load_reference(a.ref_src)
     tests_dir = os.path.join(os.path.dirname(a.ref_src.rstrip("/")), "..", "tests")
+    if a.only in ("compact", None):
+        compact_fixture(qf, 4, 11, os.path.join(HERE, "compact_norb4.npz"))
     if a.only in ("pqe", None):
         pqe_fixture(qf, 4, 11, os.path.join(HERE, "pqe_norb4_seed11.npz"))
         pqe_fixture(qf, 6, 11, os.path.join(HERE, "pqe_norb6_seed11.npz"))

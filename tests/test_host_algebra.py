@@ -131,3 +131,40 @@ def test_excited_determinants_match_reference(name):
     ex = excited_determinants(pool, range(len(pool)), mol.hf_reference)
     assert [d for d, _ in ex] == z["dets"].tolist()
     assert np.max(np.abs(np.array([p for _, p in ex]) - z["phases"])) == 0.0
+
+
+def _compact_ops(pool_type, norb=4):
+    from qforte_b200.ucc import _sa_components
+    ref = [1] * norb + [0] * norb
+    pool = qb.SQOpPool()
+    pool.set_orb_spaces(ref)
+    pool.fill_pool(pool_type)
+    if pool_type == "sa_SD":
+        return [c for _, op in pool for c in _sa_components(op)]
+    return [op for _, op in pool]
+
+
+@pytest.mark.parametrize("pool_type", ["SD", "GSD", "sa_SD"])
+@pytest.mark.parametrize("qe", [False, True])
+def test_compact_excitation_circuits_match_reference(pool_type, qe):
+    """utils/compact_excitation_circuits.py:9-291: every pool operator's FEB /
+    QEB circuit has the reference's gates, targets, controls and angles."""
+    z = golden("compact_norb4.npz")
+    key = f"{pool_type}_{'qe' if qe else 'fe'}"
+    ops = _compact_ops(pool_type)
+    amps = z[f"{pool_type}_amps"]
+    ids, tg, ct, pr = [], [], [], []
+    U = qb.Circuit()
+    for t, op in zip(amps, ops):
+        e = op.terms()[1]
+        circ = qb.compact_excitation_circuit(t * e[0], e[1], e[2], qe)
+        U.add(circ)
+        for g in circ.gates():
+            ids.append(g.gate_id())
+            tg.append(g.target())
+            ct.append(g.control())
+            pr.append(float(g.parameter()) if g.has_parameter() else 0.0)
+    assert ids == z[f"{key}_ids"].tolist()
+    assert tg == z[f"{key}_target"].tolist() and ct == z[f"{key}_control"].tolist()
+    assert pr == z[f"{key}_param"].tolist()
+    assert U.get_num_cnots() == int(z[f"{key}_cnots"])

@@ -108,3 +108,16 @@ def test_oracle_pqe_residuals(name):
     dets = list(zip(z["dets"].tolist(), z["phases"].tolist()))
     r = O.pqe_residuals(nq, list(u["ref"]), kops_forward(pool, tops), z["amps"], hterms, dets)
     assert np.max(np.abs(r - z["residuals"])) < 1e-12
+
+
+@pytest.mark.parametrize("key", ["SD_fe", "SD_qe", "GSD_fe", "sa_SD_qe"])
+def test_oracle_applies_compact_circuits_as_the_reference(key):
+    """The oracle's gate kernels give the reference's state for the compact
+    ansatz circuits (fixtures from the reference's builder)."""
+    z = golden("compact_norb4.npz")
+    gates = [O.make_gate("X", j, j) for j in range(4)]
+    ids, tg, ct, pr = (z[f"{key}_{f}"] for f in ("ids", "target", "control", "param"))
+    gates += [O.make_gate(str(k), int(t), int(c), float(p)) for k, t, c, p in zip(ids, tg, ct, pr)]
+    st = O.State(8)
+    st.apply_gates(gates)
+    assert np.max(np.abs(st.psi - z[f"{key}_psi"])) < 1e-13
