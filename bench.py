@@ -51,12 +51,12 @@ def parse():
     ap.add_argument("--full-space", action="store_true",
                     help="keep full-space states (no compact sector evaluator)")
     ap.add_argument("--workload", default="ucc",
-                    choices=["ucc", "gates", "grad", "adapt", "serve", "pexp", "pqe"],
+                    choices=["ucc", "gates", "grad", "adapt", "serve", "pexp", "pqe", "sample"],
                     help="ucc: batched dUCCSD energy+gradient (default); gates: the gate sweep; "
                          "grad: differentiable energy, forward+backward against forward alone; "
                          "adapt: every ADAPT pool gradient of a 12-operator state in one launch; "
                          "pexp: Pauli-exponential passes on one large state; "
-                         "pqe: batched PQE residual vectors")
+                         "pqe: batched PQE residual vectors; sample: measurement draws")
     ap.add_argument("--pexp-n", type=int, default=28, help="pexp: qubits")
     ap.add_argument("--pexp-strings", type=int, default=64,
                     help="pexp: random Pauli strings, and dUCC operators, per program")
@@ -543,6 +543,78 @@ def run_pqe(a, local):
     return line
 
 
+def run_sample(a, local):
+    """Measurement draws (Computer::measure_z_readouts_fast's sampling,
+    computer.cc:185-211): 10^6 seeded basis-state draws from one n-qubit
+    state (default 28 qubits) per step, host indices out."""
+    import time
+    import torch
+    import qforte_b200 as qb
+    from qforte_b200._lib import check, launch_count, lib, ptr
+    torch.cuda.set_device(local)
+    n, shots = a.pexp_n, 1_000_000
+    qc = qb.Computer(n)
+    t = qc.tensor()
+    g = torch.Generator(device="cuda").manual_seed(a.seed)
+    t.copy_(torch.complex(torch.randn(t.shape, dtype=torch.float64, device="cuda", generator=g),
+                          torch.randn(t.shape, dtype=torch.float64, device="cuda", generator=g)))
+    t.div_(torch.linalg.vector_norm(t))
+    out = np.empty(shots, dtype=np.uint64)
+    for k in range(max(a.warmup, 3)):
+        check(lib().qfb_state_sample(qc._h, 0, k, shots, ptr(out)))
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(a.steps):
+        check(lib().qfb_state_sample(qc._h, 0, 100 + k, shots, ptr(out)))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    launches = (launch_count() - l0) // a.steps
+    ck = clocks.stop()
+    peak, src = peaks()
+    state_gbs = 16.0 * 2 ** n / (ms * 1e-3) / 1e9
+    line = {"metric": "measurement draws/s", "value": shots / (ms * 1e-3), "unit": "draws/s",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic",
+            "config": {"workload": f"{shots} seeded draws from one random {n}-qubit state per "
+                                   "step, indices copied to the host",
+                       "nqubit": n},
+            "roofline": {"bound": "hbm", "kernel": "k_samp_weights + k_samp_draw",
+                         "achieved": state_gbs, "peak": peak, "peak_source": src, "unit": "GB/s",
+                         "frac": state_gbs / peak, "algorithmic_bytes_per_launch": 16.0 * 2 ** n,
+                         "note": "one read of the state per step; the whole call is timed",
+                         "traffic": None},
+            "gpu_launches": int(launches), "clocks": ck}
+    if not a.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            qf = O.load_reference_engine()
+            nr = 20
+            rc = qf.Computer(nr)
+            rng = np.random.default_rng(1)
+            v = rng.normal(size=2 ** nr) + 1j * rng.normal(size=2 ** nr)
+            v /= np.linalg.norm(v)
+            rc.set_coeff_vec(list(v))
+            rs = 100_000
+            t0 = time.perf_counter()
+            rc.measure_z_readouts_fast(0, 0, rs)
+            tc = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": rs / tc, "unit": "draws/s", "cores": 1,
+                                    "kind": "reference",
+                                    "sample": f"measure_z_readouts_fast(0, 0, {rs}) on a random "
+                                              f"{nr}-qubit state (the 28-qubit state does not fit "
+                                              "the bounded sample), serial shipped build"}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    print(json.dumps(line))
+    return line
+
+
 def run_grad(a, local):
     """Differentiable dUCCSD energy: forward (energy) and forward+backward
     (energy and the adjoint gradient through torch.autograd) per parameter
@@ -803,6 +875,10 @@ def main():
     if a.workload == "pqe":
         if rank == 0:
             run_pqe(a, local)
+        return
+    if a.workload == "sample":
+        if rank == 0:
+            run_sample(a, local)
         return
 
     import torch

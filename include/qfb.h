@@ -99,6 +99,17 @@ QFB_API int qfb_state_upload(qfb_state s, int b, const qfb_complex *host, uint64
 QFB_API int qfb_state_download(qfb_state s, int b, qfb_complex *host, uint64_t n);
 QFB_API int qfb_state_get_amp(qfb_state s, int b, uint64_t index, qfb_complex *out);
 
+/* nshots basis indices sampled from |c_i|^2 of slot b (the draws of
+ * Computer::measure_circuit / measure_readouts / measure_z_readouts_fast,
+ * computer.cc:135-315, which use an unseeded std::discrete_distribution).
+ * Seeded and reproducible: weights trunc(|c_i|^2 2^56) with |c_i|^2 = re*re +
+ * im*im rounded as written, draw k = the smallest i whose inclusive weight
+ * prefix exceeds floor(u_k T / 2^64), T the weight total and u_k the k-th
+ * output of SplitMix64 seeded with `seed`; equal seeds give equal indices on
+ * any device and in a CPU restatement.  The squared norm must be below 1.5
+ * (QFB_EINVAL otherwise); amplitudes with |c|^2 < 2^-56 are never drawn. */
+QFB_API int qfb_state_sample(qfb_state s, int b, uint64_t seed, int64_t nshots, uint64_t *out);
+
 /* ---- gates: Computer::apply_circuit / apply_gate ---------------------------
  * computer.cc:93-114, :340-751.  The result is that of applying the gates one
  * by one in list order.  Runs of gates whose qubits fit in one set of

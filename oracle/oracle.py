@@ -290,6 +290,29 @@ class State:
 # --------------------------------------------------------------------------
 
 
+def sample_indices(psi, seed, nshots):
+    """Seeded sampling of basis indices from |c_i|^2, the CPU restatement of
+    the device sampler (the draws of Computer::measure_circuit,
+    computer.cc:135-315, whose own generator is unseeded): weights
+    trunc(|c|^2 2^56), exact integer prefix sums, SplitMix64 draw u_k of the
+    seed, r_k = floor(u_k T / 2^64), sample = first index whose inclusive
+    prefix exceeds r_k."""
+    psi = np.asarray(psi, dtype=np.complex128)
+    p = psi.real * psi.real + psi.imag * psi.imag
+    w = (p * 2.0 ** 56).astype(np.uint64)
+    cum = np.cumsum(w, dtype=np.uint64)
+    T = int(cum[-1])
+    M = (1 << 64) - 1
+    r = np.empty(nshots, dtype=np.uint64)
+    for k in range(nshots):
+        z = (int(seed) + (k + 1) * 0x9E3779B97F4A7C15) & M
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        z ^= z >> 31
+        r[k] = (z * T) >> 64
+    return np.searchsorted(cum, r, side="right").astype(np.uint64)
+
+
 def refprep(ref):
     """utils/state_prep.py:5-11: X on every occupied spin-orbital."""
     return [make_gate("X", j, j) for j, occ in enumerate(ref) if occ]

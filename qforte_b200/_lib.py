@@ -55,6 +55,7 @@ SIGNATURES = {
     "qfb_state_set_basis": (ctypes.c_int, [c_state, ctypes.c_int, _vp, _vp, _i64]),
     "qfb_state_upload": (ctypes.c_int, [c_state, ctypes.c_int, _vp, _u64]),
     "qfb_state_download": (ctypes.c_int, [c_state, ctypes.c_int, _vp, _u64]),
+    "qfb_state_sample": (ctypes.c_int, [c_state, ctypes.c_int, _u64, _i64, _vp]),
     "qfb_state_get_amp": (ctypes.c_int, [c_state, ctypes.c_int, _u64, _vp]),
     "qfb_apply_gates": (ctypes.c_int, [c_state, _vp, _i64]),
     "qfb_gates_config": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),

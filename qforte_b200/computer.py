@@ -31,7 +31,22 @@ from .qubit_basis import QubitBasis
 from .qubit_operator import QubitOperator, to_string
 
 __all__ = ["Computer", "inner_product", "prepare_computer_from_circuit",
-           "prepare_computer_from_gates", "add_gate_to_computer"]
+           "prepare_computer_from_gates", "add_gate_to_computer", "set_sampling_seed"]
+
+
+_SEED = [int.from_bytes(__import__("os").urandom(8), "little")]
+
+
+def set_sampling_seed(seed):
+    """Start the process-wide seed sequence of Computer's measurement draws
+    (the reference's draws are unseeded; equal seeds here give equal draws)."""
+    _SEED[0] = int(seed) & ((1 << 64) - 1)
+
+
+def _next_seed():
+    s = _SEED[0]
+    _SEED[0] = (s + 0xD1B54A32D192ED03) & ((1 << 64) - 1)
+    return s
 
 
 def _new_state(nqubit, nbatch=1):
@@ -375,40 +390,43 @@ class Computer:
         tmp = self._rotated_copy(qc)
         return float(tmp._expval_terms([(1.0 + 0j, 0, zm)])[0].real)
 
-    def _probabilities(self, qc):
-        import torch
-        tmp = self._rotated_copy(qc)
-        p = tmp.tensor().abs().pow(2)
-        return tmp, p
+    def sample(self, n_measurements, seed=None):
+        """Basis indices of ``n_measurements`` draws from |c_i|^2 (libqfb's
+        seeded sampler, qfb_state_sample; ``seed`` None takes the next seed of
+        the process-wide sequence, see ``set_sampling_seed``)."""
+        n = int(n_measurements)
+        out = np.empty(n, dtype=np.uint64)
+        if n:
+            check(lib().qfb_state_sample(self._h, 0, _next_seed() if seed is None else int(seed),
+                                         n, ptr(out)), "sample")
+        return out
 
     def measure_circuit(self, qc, n_measurements):
-        import torch
-        tmp, p = self._probabilities(qc)
-        idx = torch.multinomial(p, int(n_measurements), replacement=True)
+        """computer.cc:135-183: rotate X / Y measured qubits to Z on a copy,
+        draw basis states, return the product of the measured qubits' +-1."""
+        tmp = self._rotated_copy(qc)
+        idx = tmp.sample(n_measurements)
+        del tmp
         zm = 0
         for g in qc.gates():
             zm ^= 1 << g.target()
-        bits = torch.zeros_like(idx)
+        bits = np.zeros(len(idx), dtype=np.uint64)
         for q in range(self._n):
             if (zm >> q) & 1:
-                bits ^= (idx >> q) & 1
-        vals = (1 - 2 * bits).to(torch.float64)
-        out = vals.cpu().tolist()
-        del tmp
-        return out
+                bits ^= (idx >> np.uint64(q)) & np.uint64(1)
+        return (1.0 - 2.0 * bits.astype(np.float64)).tolist()
 
     def measure_readouts(self, qc, n_measurements):
-        import torch
-        tmp, p = self._probabilities(qc)
-        idx = torch.multinomial(p, int(n_measurements), replacement=True).cpu().numpy()
-        tg = [g.target() for g in qc.gates()]
+        """computer.cc:213-259: the measured qubits' bits of each draw."""
+        tmp = self._rotated_copy(qc)
+        idx = tmp.sample(n_measurements)
         del tmp
+        tg = [g.target() for g in qc.gates()]
         return [[int((int(i) >> t) & 1) for t in tg] for i in idx]
 
     def measure_z_readouts_fast(self, na, nb, n_measurements):
-        import torch
-        p = self.tensor().abs().pow(2)
-        idx = torch.multinomial(p, int(n_measurements), replacement=True).cpu().numpy()
+        """computer.cc:185-211: bits na..nb of each draw, no rotation."""
+        idx = self.sample(n_measurements)
         return [[int((int(i) >> l) & 1) for l in range(na, nb + 1)] for i in idx]
 
     # ---- printing / comparison ----------------------------------------------

@@ -245,6 +245,168 @@ __global__ void k_rows_sum(const double2 *__restrict__ partial, int64_t n,
     if (threadIdx.x == 0) out[blockIdx.x] = acc;
 }
 
+// ---------------------------------------------------------------------------
+// Sampling of basis states (Computer::measure_circuit / measure_readouts /
+// measure_z_readouts_fast, computer.cc:135-315), seeded and reproducible:
+//   weight w_i = trunc(|c_i|^2 * 2^56), |c_i|^2 = re*re + im*im rounded as
+//     written (no fused multiply-add), so any implementation gets the same w;
+//   T = sum of the weights (exact integer sums, any order);
+//   draw k: u = mix64(seed + (k + 1) * 0x9E3779B97F4A7C15) (the SplitMix64
+//     generator of Steele, Lea and Flood, finaliser constants of Vigna),
+//     r = floor(u * T / 2^64);
+//   sample = the smallest i whose inclusive prefix sum of weights exceeds r.
+// Blocks of 4096 amplitudes, sub-blocks of 64: k_samp_weights forms each
+// block's inclusive sub-block prefixes and total, k_samp_scan the inclusive
+// prefixes of the block totals, k_samp_draw searches block, sub-block, then
+// at most 64 amplitudes.
+// ---------------------------------------------------------------------------
+constexpr int kSampBlock = 4096, kSampSub = 64;
+
+__device__ __forceinline__ uint64_t samp_weight(double2 c) {
+    const double p = __dadd_rn(__dmul_rn(c.x, c.x), __dmul_rn(c.y, c.y));
+    return (uint64_t)__double2ull_rz(__dmul_rn(p, 72057594037927936.0));  // 2^56
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// grid: blocks of 4096 amplitudes; 256 threads (8 warps), each warp sums 8 of
+// the block's 64-amplitude sub-blocks with coalesced reads (two amplitudes a
+// lane).  sub_incl[blk * 64 + j]: inclusive prefix of the block's sub-block
+// sums; blk_tot[blk]: its total; blk_p[blk]: its sum of |c|^2 in double (the
+// norm check).
+__global__ void __launch_bounds__(256) k_samp_weights(const double2 *__restrict__ s, uint64_t n,
+                                                      uint64_t *__restrict__ sub_incl,
+                                                      uint64_t *__restrict__ blk_tot,
+                                                      double *__restrict__ blk_p) {
+    __shared__ uint64_t s_sub[kSampSub];
+    __shared__ double s_p[kSampSub];
+    const uint64_t base = (uint64_t)blockIdx.x * kSampBlock;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    double2 c[2 * (kSampSub / 8)];
+#pragma unroll
+    for (int k = 0; k < kSampSub / 8; ++k) {  // all loads in flight first
+        const uint64_t i0 = base + (uint64_t)(wid * (kSampSub / 8) + k) * kSampSub + lane;
+        c[2 * k] = i0 < n ? s[i0] : make_double2(0.0, 0.0);
+        c[2 * k + 1] = i0 + 32 < n ? s[i0 + 32] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int k = 0; k < kSampSub / 8; ++k) {
+        uint64_t w = samp_weight(c[2 * k]) + samp_weight(c[2 * k + 1]);
+        double pd = c[2 * k].x * c[2 * k].x + c[2 * k].y * c[2 * k].y + c[2 * k + 1].x * c[2 * k + 1].x +
+                    c[2 * k + 1].y * c[2 * k + 1].y;
+        for (int o = 16; o > 0; o >>= 1) {
+            w += __shfl_down_sync(0xffffffffu, w, o);
+            pd += __shfl_down_sync(0xffffffffu, pd, o);
+        }
+        if (lane == 0) {
+            s_sub[wid * (kSampSub / 8) + k] = w;
+            s_p[wid * (kSampSub / 8) + k] = pd;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        uint64_t acc = 0;
+        double pa = 0.0;
+        for (int j = 0; j < kSampSub; ++j) {
+            acc += s_sub[j];
+            pa += s_p[j];
+            sub_incl[(uint64_t)blockIdx.x * kSampSub + j] = acc;
+        }
+        blk_tot[blockIdx.x] = acc;
+        blk_p[blockIdx.x] = pa;
+    }
+}
+
+// One CTA of 1024 threads: blk_incl = inclusive prefix of the block totals,
+// *total = T, *bad = 1 when the sum of |c|^2 is 1.5 or more (weights could
+// overflow 64 bits) or T is 0.
+__global__ void __launch_bounds__(1024) k_samp_scan(const uint64_t *__restrict__ blk_tot,
+                                                    const double *__restrict__ blk_p, int64_t nblk,
+                                                    uint64_t *__restrict__ blk_incl,
+                                                    uint64_t *__restrict__ total, int *__restrict__ bad) {
+    __shared__ uint64_t s_w[32];
+    __shared__ double s_d[32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int64_t per = (nblk + 1023) / 1024, b0 = (int64_t)tid * per,
+                  b1 = b0 + per < nblk ? b0 + per : nblk;
+    uint64_t mine = 0;
+    double pd = 0.0;
+    for (int64_t k = b0; k < b1; ++k) {
+        mine += blk_tot[k];
+        pd += blk_p[k];
+    }
+    // exclusive scan of the 1024 thread sums
+    uint64_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    for (int o = 16; o > 0; o >>= 1) pd += __shfl_down_sync(0xffffffffu, pd, o);
+    if (lane == 31) s_w[wid] = incl;
+    if (lane == 0) s_d[wid] = pd;
+    __syncthreads();
+    if (wid == 0) {
+        uint64_t x = s_w[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t t = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += t;
+        }
+        s_w[lane] = x;  // inclusive over warps
+    }
+    __syncthreads();
+    uint64_t acc = incl - mine + (wid > 0 ? s_w[wid - 1] : 0ull);
+    for (int64_t k = b0; k < b1; ++k) {
+        acc += blk_tot[k];
+        blk_incl[k] = acc;
+    }
+    if (tid == 0) {
+        double ps = 0.0;
+        for (int k = 0; k < 32; ++k) ps += s_d[k];
+        const uint64_t T = s_w[31];
+        *total = T;
+        *bad = (!(ps < 1.5) || T == 0) ? 1 : 0;
+    }
+}
+
+// One thread per draw.
+__global__ void k_samp_draw(const double2 *__restrict__ s, uint64_t n,
+                            const uint64_t *__restrict__ sub_incl,
+                            const uint64_t *__restrict__ blk_incl, int64_t nblk,
+                            const uint64_t *__restrict__ total, const int *__restrict__ bad,
+                            uint64_t seed, int64_t nshots, uint64_t *__restrict__ out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nshots || *bad) return;
+    const uint64_t T = *total;
+    const uint64_t u = mix64(seed + (uint64_t)(k + 1) * 0x9E3779B97F4A7C15ull);
+    uint64_t r = __umul64hi(u, T);
+    // smallest block whose inclusive prefix exceeds r
+    int64_t lo = 0, hi = nblk - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (blk_incl[mid] > r) hi = mid; else lo = mid + 1;
+    }
+    if (lo > 0) r -= blk_incl[lo - 1];
+    const uint64_t *sub = sub_incl + (uint64_t)lo * kSampSub;
+    int a = 0, c = kSampSub - 1;
+    while (a < c) {
+        const int mid = (a + c) >> 1;
+        if (sub[mid] > r) c = mid; else a = mid + 1;
+    }
+    if (a > 0) r -= sub[a - 1];
+    uint64_t i = (uint64_t)lo * kSampBlock + (uint64_t)a * kSampSub;
+    const uint64_t iend = i + kSampSub < n ? i + kSampSub : n;
+    uint64_t acc = 0;
+    for (; i + 1 < iend; ++i) {
+        acc += samp_weight(s[i]);
+        if (acc > r) break;
+    }
+    out[k] = i;
+}
+
 inline double2 d2(const qfb_complex &c) { return make_double2(c.re, c.im); }
 inline bool is_one(const qfb_complex &c) { return c.re == 1.0 && c.im == 0.0; }
 inline bool ceq(const qfb_complex &a, const qfb_complex &b) {
@@ -1081,6 +1243,56 @@ int qfb_axpy(qfb_state y, qfb_complex alpha, qfb_state x) {
     const uint64_t n = y->nbasis * y->nbatch;
     k_axpy<<<grid_for(n, 256), 256, 0, t_stream>>>(y->d, x->d, n, d2(alpha));
     QFB_LAUNCHED();
+    return QFB_OK;
+}
+
+int qfb_state_sample(qfb_state s, int b, uint64_t seed, int64_t nshots, uint64_t *out) {
+    if (!s || (nshots > 0 && !out)) return fail(QFB_EINVAL, "qfb_state_sample: null argument");
+    if (b < 0 || b >= s->nbatch) return fail(QFB_EINVAL, "qfb_state_sample: bad slot %d", b);
+    if (nshots < 0) return fail(QFB_EINVAL, "qfb_state_sample: nshots = %lld", (long long)nshots);
+    if (nshots == 0) return QFB_OK;
+    const uint64_t n = s->nbasis;
+    const int64_t nblk = (int64_t)((n + kSampBlock - 1) / kSampBlock);
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_sub = 0, o_tot = al(sizeof(uint64_t) * nblk * kSampSub),
+                 o_p = o_tot + al(sizeof(uint64_t) * nblk), o_inc = o_p + al(sizeof(double) * nblk),
+                 o_T = o_inc + al(sizeof(uint64_t) * nblk), o_bad = o_T + 256,
+                 o_out = o_bad + 256, bytes = o_out + sizeof(uint64_t) * (size_t)nshots;
+    void *buf = nullptr;
+    int rc = dev_alloc(&buf, bytes);
+    if (rc) return rc;
+    char *p = (char *)buf;
+    const double2 *st = s->d + (uint64_t)b * n;
+    k_samp_weights<<<(unsigned)nblk, 256, 0, t_stream>>>(st, n, (uint64_t *)(p + o_sub),
+                                                        (uint64_t *)(p + o_tot), (double *)(p + o_p));
+    rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
+    if (rc == QFB_OK) {
+        k_samp_scan<<<1, 1024, 0, t_stream>>>((const uint64_t *)(p + o_tot), (const double *)(p + o_p),
+                                              nblk, (uint64_t *)(p + o_inc), (uint64_t *)(p + o_T),
+                                              (int *)(p + o_bad));
+        rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
+    }
+    if (rc == QFB_OK) {
+        k_samp_draw<<<(unsigned)((nshots + 255) / 256), 256, 0, t_stream>>>(
+            st, n, (const uint64_t *)(p + o_sub), (const uint64_t *)(p + o_inc), nblk,
+            (const uint64_t *)(p + o_T), (const int *)(p + o_bad), seed, nshots,
+            (uint64_t *)(p + o_out));
+        rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
+    }
+    int bad = 0;
+    if (rc == QFB_OK) {
+        cudaError_t e = cudaMemcpyAsync(&bad, p + o_bad, sizeof(int), cudaMemcpyDeviceToHost, t_stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out, p + o_out, sizeof(uint64_t) * (size_t)nshots,
+                                cudaMemcpyDeviceToHost, t_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "qfb_state_sample");
+    }
+    dev_free(buf);
+    if (rc) return rc;
+    if (bad)
+        return fail(QFB_EINVAL, "qfb_state_sample: the state's squared norm is 0 or 1.5 or more; "
+                                "normalise it before sampling");
     return QFB_OK;
 }
 

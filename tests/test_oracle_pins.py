@@ -121,3 +121,19 @@ def test_oracle_applies_compact_circuits_as_the_reference(key):
     st = O.State(8)
     st.apply_gates(gates)
     assert np.max(np.abs(st.psi - z[f"{key}_psi"])) < 1e-13
+
+
+def test_oracle_sampler_frequencies():
+    """The oracle's seeded sampler draws with the state's probabilities
+    (chi-square on a 5-qubit state) and is a function of the seed."""
+    rng = np.random.default_rng(3)
+    psi = rng.normal(size=32) + 1j * rng.normal(size=32)
+    psi /= np.linalg.norm(psi)
+    shots = 40000
+    idx = O.sample_indices(psi, 11, shots)
+    counts = np.bincount(idx.astype(np.int64), minlength=32)
+    expect = shots * np.abs(psi) ** 2
+    chi2 = float(np.sum((counts - expect) ** 2 / expect))
+    assert chi2 < 80.0  # 31 degrees of freedom: p < 1e-5 above 70
+    assert np.array_equal(idx, O.sample_indices(psi, 11, shots))
+    assert not np.array_equal(idx[:100], O.sample_indices(psi, 12, 100))
