@@ -1016,13 +1016,17 @@ def main():
         per_launch_bytes = {1: 32 * nsec * a.batch, 2: (12 * nnz / max(1, a.batch) + 32 * nsec) * a.batch,
                             3: 64 * nsec * a.batch}
     elif compact:
-        # one CTA per parameter set, states in shared memory: the bytes each
-        # kernel must move per launch are the save buffer it writes / reads
-        # and (H) the H rows, streamed once per parameter set
+        # one CTA per parameter set, states in shared memory: the HBM bytes
+        # each kernel must move per launch are the save buffer it writes /
+        # reads (8 bytes an amplitude with real states, else 16) and, for H,
+        # the H rows once (12 bytes an entry); every parameter set then
+        # streams the rows again from L2, reported beside it
         nsec, nnz = ev.sector_size, ev.h_rows
-        per_launch_bytes = {1: 16 * nsec * a.batch,
-                            2: (12 * nnz + 32 * nsec) * a.batch,
-                            3: 32 * nsec * a.batch}
+        elem = 8 if ev.real_states else 16
+        per_launch_bytes = {1: elem * nsec * a.batch,
+                            2: 12 * nnz + 2 * elem * nsec * a.batch,
+                            3: 2 * elem * nsec * a.batch}
+        l2_stream = {2: 12 * nnz * a.batch}
     else:
         state_bytes = 16 * N * a.batch
         # algorithmic bytes per launch of each stage's main kernel
@@ -1056,6 +1060,14 @@ def main():
     if ev.path in (2, 3):
         roof["sector_amplitudes"] = ev.sector_size
         roof["h_row_entries"] = ev.h_rows
+    if compact:
+        roof["real_states"] = ev.real_states
+        roof["bound_note"] = ("states live in shared memory: the binding resource is the "
+                              "L1 / shared-memory pipe (profiles/k_sector_kernels_ucc16_b256.md), "
+                              "not HBM")
+        if dom in l2_stream:
+            roof["l2_stream_bytes_per_launch"] = l2_stream[dom]
+            roof["l2_stream_gbs"] = l2_stream[dom] / (avg_ms / 1000.0) / 1e9
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": max(a.warmup, 3), "ms_per_step": ms_all, "higher_is_better": True,

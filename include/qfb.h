@@ -236,6 +236,9 @@ QFB_API int qfb_ucc_sector(qfb_ucc u, int64_t *nsec);
  * and 3 need every program step in Givens form.  No counterpart in the
  * reference. */
 QFB_API int qfb_ucc_path(qfb_ucc u, int32_t *path);
+/* 1 when the evaluator's compact states are stored as real doubles (see
+ * qfb_ucc_config), else 0.  No counterpart in the reference. */
+QFB_API int qfb_ucc_real_states(qfb_ucc u, int32_t *real);
 /* Entries of the H rows the compact path streams for each parameter set (0
  * on the other paths).  No counterpart in the reference. */
 QFB_API int qfb_ucc_rows(qfb_ucc u, int64_t *nnz);
@@ -243,8 +246,11 @@ QFB_API int qfb_ucc_rows(qfb_ucc u, int64_t *nnz);
  * sector paths (1, the default: shared memory when the sector fits, else
  * global memory), only the global-memory one (2), only the global-memory one
  * with sigma formed from the grouped terms instead of stored H rows (3; the
- * rows are over 24 GB beyond ~24 qubits, where this happens by itself), or
- * neither (0).  No counterpart in the reference. */
+ * rows are over 24 GB beyond ~24 qubits, where this happens by itself), the
+ * default with complex state storage on the shared-memory path (4), or
+ * neither (0).  Under 1, a shared-memory evaluator whose H and step
+ * coefficients are all real keeps psi and sigma as real doubles (half the
+ * shared memory and traffic).  No counterpart in the reference. */
 QFB_API int qfb_ucc_config(int compact);
 /* Process-wide tile shape of the full-space windows of evaluators created
  * from now on: fwd_bits qubits per forward tile (default 12, at most 13),

@@ -88,6 +88,7 @@ SIGNATURES = {
     "qfb_ucc_pool_buffer": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_eval_pool": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "qfb_ucc_path": (ctypes.c_int, [_vp, _vp]),
+    "qfb_ucc_real_states": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_rows": (ctypes.c_int, [_vp, _vp]),
     "qfb_ucc_config": (ctypes.c_int, [ctypes.c_int]),
     "qfb_ucc_tiles": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),

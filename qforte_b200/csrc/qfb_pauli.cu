@@ -2446,6 +2446,7 @@ struct qfb_ucc_s {
     int64_t nsec = 0;
     size_t bytes = 0;     // device bytes held (blobs)
     int compact = 0;      // compact sector evaluator (qfb_sector.cuh)
+    int sreal = 0;        // compact: real states (every coefficient and H real)
     int64_t nnz = 0;      // entries of the H rows on the compact sector
     std::shared_ptr<SectorRows> rows;  // compact paths: H rows on the sector
     qfbs::SLaunch SL{};
@@ -2483,13 +2484,30 @@ struct qfb_ucc_s {
     qfbs::SStream rstream{};          // compact: forward records in reverse order
 };
 
-// Reorder the entries of every H row so that each run of 8 consecutive
-// entries (the 8 lanes of a quarter warp in k_sector_h) gathers psi from 8
-// different 16-byte bank slots (column mod 8) as far as the row allows:
-// entries are bucketed by column mod 8 and dealt out one bucket after the
-// other, fullest bucket first.  Only the order of the row's sum changes.
+// Whether every pattern of every record of a stream has real coefficients.
+static bool stream_is_real(const StreamHost &S) {
+    for (const int2 &sp : S.span) {
+        const char *rec = (const char *)&S.rec[sp.x];
+        qfbs::RHead hd;
+        std::memcpy(&hd, rec, sizeof(hd));
+        for (int p = 0; p < (hd.npf & 255); ++p) {
+            qfbs::RPat pt;
+            std::memcpy(&pt, rec + sizeof(qfbs::RHead) + p * sizeof(qfbs::RPat), sizeof(pt));
+            if (pt.gn.y != 0.0 || pt.hn.y != 0.0) return false;
+        }
+    }
+    return true;
+}
+
+// Reorder the entries of every H row so that each run of S consecutive
+// entries gathers psi from S different bank slots as far as the row allows:
+// S = 8 for complex states (the 8 lanes of a quarter warp in k_sector_h read
+// 16-byte amplitudes, slot = column mod 8), S = 16 for real states (a half
+// warp reads 8-byte amplitudes, slot = column mod 16).  Entries are bucketed
+// by slot and dealt out one bucket after the other, fullest bucket first.
+// Only the order of the row's sum changes.
 static int sector_rows_interleave(const std::vector<int32_t> &rowptr, int64_t nnz, uint32_t *d_col,
-                                  void *d_val, size_t vbytes) {
+                                  void *d_val, size_t vbytes, int S) {
     if (nnz == 0) return QFB_OK;
     std::vector<uint32_t> col((size_t)nnz), col2((size_t)nnz);
     std::vector<char> val((size_t)nnz * vbytes), val2((size_t)nnz * vbytes);
@@ -2497,12 +2515,14 @@ static int sector_rows_interleave(const std::vector<int32_t> &rowptr, int64_t nn
                              t_stream));
     QFB_CUDA(cudaMemcpyAsync(val.data(), d_val, vbytes * nnz, cudaMemcpyDeviceToHost, t_stream));
     QFB_CUDA(cudaStreamSynchronize(t_stream));
-    std::vector<int64_t> bucket[8];
+    std::vector<std::vector<int64_t>> bucket((size_t)S);
+    std::vector<size_t> next((size_t)S);
+    std::vector<int> order((size_t)S);
     const size_t nrow = rowptr.size() - 1;
     for (size_t i = 0; i < nrow; ++i) {
         for (auto &b : bucket) b.clear();
-        for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) bucket[col[e] & 7u].push_back(e);
-        size_t next[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) bucket[col[e] % (uint32_t)S].push_back(e);
+        std::fill(next.begin(), next.end(), 0);
         int64_t out = rowptr[i];
         auto left = [&](int r) { return bucket[r].size() - next[r]; };
         auto emit = [&](int r) {
@@ -2511,19 +2531,19 @@ static int sector_rows_interleave(const std::vector<int32_t> &rowptr, int64_t nn
             std::memcpy(&val2[(size_t)out * vbytes], &val[(size_t)e * vbytes], vbytes);
             ++out;
         };
-        while (out < rowptr[i + 1]) {  // one group of (up to) 8 positions
-            const int64_t n = std::min<int64_t>(8, rowptr[i + 1] - out);
-            int order[8] = {0, 1, 2, 3, 4, 5, 6, 7};
-            std::sort(order, order + 8, [&](int a, int b) { return left(a) > left(b); });
+        while (out < rowptr[i + 1]) {  // one group of (up to) S positions
+            const int64_t n = std::min<int64_t>(S, rowptr[i + 1] - out);
+            for (int r = 0; r < S; ++r) order[r] = r;
+            std::sort(order.begin(), order.end(), [&](int a, int b) { return left(a) > left(b); });
             int64_t taken = 0;
-            for (int k = 0; k < 8 && taken < n; ++k)
+            for (int k = 0; k < S && taken < n; ++k)
                 if (left(order[k]) > 0) {
                     emit(order[k]);
                     ++taken;
                 }
-            while (taken < n) {  // fewer distinct residues than positions left
+            while (taken < n) {  // fewer distinct slots than positions left
                 int best = 0;
-                for (int r = 1; r < 8; ++r)
+                for (int r = 1; r < S; ++r)
                     if (left(r) > left(best)) best = r;
                 emit(best);
                 ++taken;
@@ -2610,8 +2630,9 @@ static int plan_upload(SectorPlan &sp) {
 // `global`, rows over kRowsBudget are refused (QFB_ENOMEM) and the refusal
 // is cached too; `interleave` orders each row's entries for k_sector_h.
 static int get_sector_rows(qfb_sum_s *ham, const SectorPlan &sp, const std::vector<SecGroup> &sg,
-                           int n, bool interleave, bool global, std::shared_ptr<SectorRows> *out) {
-    const int layout = interleave ? 1 : (global && g_ucc_compact == 3) ? 2 : 0;
+                           int n, int interleave, bool global, std::shared_ptr<SectorRows> *out) {
+    // interleave: 0 none, else the bank slots of one gather group (8 or 16)
+    const int layout = interleave == 8 ? 1 : interleave == 16 ? 3 : (global && g_ucc_compact == 3) ? 2 : 0;
     const auto key = std::make_tuple(n, sp.ka, sp.kb, layout);
     auto it = ham->rows_cache.find(key);
     if (it != ham->rows_cache.end()) {
@@ -2719,7 +2740,7 @@ static int get_sector_rows(qfb_sum_s *ham, const SectorPlan &sp, const std::vect
     QFB_CUDA(cudaStreamSynchronize(t_stream));
     if (interleave) {
         rc = sector_rows_interleave(rowptr, nnz, d_col, real ? (void *)d_vr : (void *)d_vc,
-                                    real ? sizeof(double) : sizeof(double2));
+                                    real ? sizeof(double) : sizeof(double2), interleave);
         if (rc) return rc;
     }
     rows->rowptr = d_rp;
@@ -2739,7 +2760,9 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
     int rc = plan_upload(sp);
     if (rc) return rc;
     std::shared_ptr<SectorRows> rows;
-    rc = get_sector_rows(ham, sp, sg, u->nqubit, !global, global, &rows);
+    // real states gather 8-byte amplitudes: interleave rows for 16 bank slots
+    const bool real_steps = g_ucc_compact != 4 && stream_is_real(sp.fwd) && stream_is_real(sp.sweep);
+    rc = get_sector_rows(ham, sp, sg, u->nqubit, global ? 0 : (real_steps ? 16 : 8), global, &rows);
     if (rc) return rc;
     u->splan = plan;
     u->rows = rows;
@@ -2780,55 +2803,73 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
     return QFB_OK;
 }
 
+template <class V>
+static cudaError_t sector_smem_attr_v() {
+    const int m = (int)kSectorSmemMax;
+    cudaError_t err = cudaFuncSetAttribute(qfbs::k_sector_forward<V>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(qfbs::k_sector_h<true, V>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(qfbs::k_sector_h<false, V>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(qfbs::k_sector_sweep<V>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(qfbs::k_sector_resid<V>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(qfbs::k_sector_pool<V>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    return err;
+}
+
 static int sector_smem_attr() {
     static std::once_flag once;
     static cudaError_t err = cudaSuccess;
     std::call_once(once, [] {
-        err = cudaFuncSetAttribute(qfbs::k_sector_forward,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(qfbs::k_sector_h<true>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(qfbs::k_sector_h<false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(qfbs::k_sector_sweep,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(qfbs::k_sector_resid,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSectorSmemMax);
+        err = sector_smem_attr_v<double2>();
+        if (err == cudaSuccess) err = sector_smem_attr_v<double>();
     });
     return err == cudaSuccess ? QFB_OK : cuda_fail(err, "sector evaluator shared memory");
 }
 
-// Compact evaluator: stage 1 the forward program, stage 2 sigma = H psi and
-// the energy, stage 3 the reverse sweep (psi and sigma pass through the save
-// buffer between them).
-static int ucc_stage_compact(qfb_ucc u, int stage, int with_grad) {
+template <class V>
+static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
     const qfbs::SLaunch &L = u->SL;
     const size_t n = (size_t)L.nsec;
+    const bool real = sizeof(V) == sizeof(double);
     switch (stage) {
         case 1:
-            qfbs::k_sector_forward<<<u->nbatch, kSectorThreads,
-                                     sizeof(double2) * (n + (size_t)L.fwd.n) +
-                                         sizeof(uint4) * 3 * (size_t)L.fwd.maxw,
-                                     t_stream>>>(L);
+            qfbs::k_sector_forward<V><<<u->nbatch, kSectorThreads,
+                                        qfbs::sector_smem_states(1, n, real) +
+                                            sizeof(double2) * (size_t)L.fwd.n +
+                                            sizeof(uint4) * 3 * (size_t)L.fwd.maxw,
+                                        t_stream>>>(L);
             QFB_LAUNCHED();
             break;
         case 2:
-            if (L.val_c)
-                qfbs::k_sector_h<false><<<u->nbatch, kSectorThreads, sizeof(double2) * n, t_stream>>>(L);
-            else
-                qfbs::k_sector_h<true><<<u->nbatch, kSectorThreads, sizeof(double2) * n, t_stream>>>(L);
+            if constexpr (sizeof(V) == sizeof(double2)) {
+                if (L.val_c) {
+                    qfbs::k_sector_h<false, V><<<u->nbatch, kSectorThreads,
+                                                 qfbs::sector_smem_states(1, n, real), t_stream>>>(L);
+                    QFB_LAUNCHED();
+                    break;
+                }
+            }
+            qfbs::k_sector_h<true, V><<<u->nbatch, kSectorThreads, qfbs::sector_smem_states(1, n, real),
+                                        t_stream>>>(L);
             QFB_LAUNCHED();
             break;
         case 3:
             if (!(with_grad && u->grad && u->nparam > 0)) break;
-            qfbs::k_sector_sweep<<<u->nbatch, kSectorThreads,
-                                   sizeof(double2) * (2 * n + (size_t)L.sweep.n) +
-                                       sizeof(uint4) * 3 * (size_t)L.sweep.maxw,
-                                   t_stream>>>(L);
+            qfbs::k_sector_sweep<V><<<u->nbatch, kSectorThreads,
+                                      qfbs::sector_smem_states(2, n, real) +
+                                          sizeof(double2) * (size_t)L.sweep.n +
+                                          sizeof(uint4) * 3 * (size_t)L.sweep.maxw,
+                                      t_stream>>>(L);
             QFB_LAUNCHED();
             k_grad_final<<<dim3(u->nparam, u->nbatch), 128, 0, t_stream>>>(u->gpart, u->psteps,
                                                                          u->gchunks, u->gradv);
@@ -2838,6 +2879,14 @@ static int ucc_stage_compact(qfb_ucc u, int stage, int with_grad) {
             break;
     }
     return QFB_OK;
+}
+
+// Compact evaluator: stage 1 the forward program, stage 2 sigma = H psi and
+// the energy, stage 3 the reverse sweep (psi and sigma pass through the save
+// buffer between them); real states when every coefficient is real.
+static int ucc_stage_compact(qfb_ucc u, int stage, int with_grad) {
+    return u->sreal ? ucc_stage_compact_v<double>(u, stage, with_grad)
+                    : ucc_stage_compact_v<double2>(u, stage, with_grad);
 }
 
 // Pairs of the largest record of a stream (grid sizing of the global path).
@@ -2995,8 +3044,12 @@ static int ucc_pool_stage(qfb_ucc u) {
         L.partial = u->ppart;
         const int sm = sm_count();
         const int G = std::max(1, std::min(u->pstream.n, (2 * sm + B - 1) / B));
-        const size_t smem = sizeof(double2) * 2 * (size_t)L.nsec + sizeof(uint4) * u->pstream.maxw;
-        qfbs::k_sector_pool<<<dim3(G, B), kSectorThreads, smem, t_stream>>>(L, u->pstream);
+        const size_t smem = qfbs::sector_smem_states(2, (size_t)L.nsec, u->sreal) +
+                            sizeof(uint4) * u->pstream.maxw;
+        if (u->sreal)
+            qfbs::k_sector_pool<double><<<dim3(G, B), kSectorThreads, smem, t_stream>>>(L, u->pstream);
+        else
+            qfbs::k_sector_pool<double2><<<dim3(G, B), kSectorThreads, smem, t_stream>>>(L, u->pstream);
         QFB_LAUNCHED();
         chunks = kSectorThreads / 32;
     } else {
@@ -3018,10 +3071,15 @@ static int ucc_resid_stage(qfb_ucc u) {
     const unsigned gg = (unsigned)(((int64_t)u->nres * B + 255) / 256);
     if (u->compact) {
         const qfbs::SLaunch &L = u->SL;
-        const size_t smem = sizeof(double2) * ((size_t)L.nsec + (size_t)u->rstream.n) +
+        const size_t smem = qfbs::sector_smem_states(1, (size_t)L.nsec, u->sreal) +
+                            sizeof(double2) * (size_t)u->rstream.n +
                             sizeof(uint4) * 3 * (size_t)u->rstream.maxw;
-        qfbs::k_sector_resid<<<B, kSectorThreads, smem, t_stream>>>(L, u->rstream, u->ridx,
-                                                                   u->rphase, u->nres, u->res);
+        if (u->sreal)
+            qfbs::k_sector_resid<double><<<B, kSectorThreads, smem, t_stream>>>(
+                L, u->rstream, u->ridx, u->rphase, u->nres, u->res);
+        else
+            qfbs::k_sector_resid<double2><<<B, kSectorThreads, smem, t_stream>>>(
+                L, u->rstream, u->ridx, u->rphase, u->nres, u->res);
         QFB_LAUNCHED();
         return QFB_OK;
     }
@@ -3139,7 +3197,7 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
             fprog->sector_plans[key] = r;
             return r;
         };
-        if (g_ucc_compact == 1) {  // 2, 3: global memory only (3: sigma without stored rows)
+        if (g_ucc_compact == 1 || g_ucc_compact == 4) {  // 2, 3: global memory only (3: sigma without stored rows)
             plan = get_plan(true);
             compact = plan != nullptr;
         }
@@ -3262,6 +3320,11 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
             qfb_ucc_destroy(u);
             return rc;
         }
+        // real states: real H rows, real pair coefficients in both streams
+        u->sreal = (compact && g_ucc_compact != 4 && u->SL.val_c == nullptr &&
+                    stream_is_real(plan->fwd) && stream_is_real(plan->sweep))
+                       ? 1
+                       : 0;
     }
     *out = u;
     return QFB_OK;
@@ -3279,8 +3342,14 @@ int qfb_ucc_tiles(int fwd_bits, int grad_bits, int low_bits) {
 }
 
 int qfb_ucc_config(int compact) {
-    if (compact < 0 || compact > 3) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
+    if (compact < 0 || compact > 4) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
     g_ucc_compact = compact;
+    return QFB_OK;
+}
+
+int qfb_ucc_real_states(qfb_ucc u, int32_t *real) {
+    if (!u || !real) return fail(QFB_EINVAL, "qfb_ucc_real_states: null argument");
+    *real = u->sreal;
     return QFB_OK;
 }
 
@@ -3333,6 +3402,9 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
         for (size_t k = 0; k < cs.size(); ++k)
             if (!push_record(sh, cs[k], qfbs::R_IP, (int)k, u->gsec ? (1 << 30) : kSectorThreads))
                 return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool step too large");
+        if (u->sreal && !stream_is_real(sh))
+            return fail(QFB_ENOSYS, "qfb_ucc_set_pool: complex pool coefficients on an evaluator "
+                                    "with real states (create it with qfb_ucc_config(4))");
         chunks = u->compact ? kSectorThreads / 32 : global_grid(stream_max_pairs(sh), u->GL.spw);
     } else {
         uint64_t most = 1;

@@ -46,9 +46,10 @@ __all__ = ["DUCC", "Evaluator", "evaluator_config", "UCCNVQE", "ADAPTVQE", "ansa
 
 def evaluator_config(compact=True):
     """Process-wide: let evaluators created from now on use the compact
-    sector paths (True, the default), only the global-memory one ("global"),
-    or keep full-space states (False)."""
-    mode = {"global": 2, "global-no-rows": 3}.get(compact, 1 if compact else 0)
+    sector paths (True, the default; real states where every coefficient is
+    real), the same with complex state storage ("complex"), only the
+    global-memory one ("global"), or keep full-space states (False)."""
+    mode = {"global": 2, "global-no-rows": 3, "complex": 4}.get(compact, 1 if compact else 0)
     check(lib().qfb_ucc_config(mode), "qfb_ucc_config")
 
 
@@ -87,6 +88,13 @@ class Evaluator:
         n = ctypes.c_int32()
         check(lib().qfb_ucc_path(self.h, ctypes.byref(n)), "qfb_ucc_path")
         return n.value
+
+    @property
+    def real_states(self):
+        """True when the compact states are kept as real doubles."""
+        n = ctypes.c_int32()
+        check(lib().qfb_ucc_real_states(self.h, ctypes.byref(n)), "qfb_ucc_real_states")
+        return bool(n.value)
 
     @property
     def h_rows(self):

@@ -521,3 +521,38 @@ def test_global_sector_pool_gradients(cuda):
         evaluator_config(True)
     g2 = np.vstack([eng.pool_gradients_grouped(P[b]) for b in range(2)])
     assert np.max(np.abs(g - g2)) < 1e-12
+
+
+@pytest.mark.parametrize("norb,seed,pool_type", [(4, 11, "SD"), (6, 3, "SD"), (5, 9, "GSD")])
+def test_real_state_storage_matches_complex(cuda, norb, seed, pool_type):
+    """The shared-memory compact path keeps psi and sigma as real doubles when
+    H and every step coefficient are real: energies, gradients, pool
+    gradients and PQE residuals equal those of complex storage and of the
+    full-space path."""
+    from qforte_b200.ucc import evaluator_config
+    mol, pool = random_problem(norb, seed, pool_type)
+    tops = list(range(0, len(pool), 1 if len(pool) < 400 else 3))
+    P = np.random.default_rng(seed).uniform(-0.1, 0.1, (5, len(tops)))
+    res = {}
+    for mode in (True, "complex", False):
+        evaluator_config(mode)
+        try:
+            eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
+            E, G = eng.energy_grad(P)
+            ev = eng.evaluator(5)
+            pg = eng.pool_gradients(P)
+            out = (E, G, pg, ev.path, ev.real_states)
+            if pool_type == "SD":
+                out += (eng.residuals(P)[1],)
+            res[mode] = out
+        finally:
+            evaluator_config(True)
+    assert res[True][3] == 2 and res[True][4] is True
+    assert res["complex"][3] == 2 and res["complex"][4] is False
+    assert res[False][3] in (0, 1)
+    for other in ("complex", False):
+        assert np.max(np.abs(res[True][0] - res[other][0])) < 1e-12
+        assert np.max(np.abs(res[True][1] - res[other][1])) < 1e-11
+        assert np.max(np.abs(res[True][2] - res[other][2])) < 1e-11
+        if pool_type == "SD":
+            assert np.max(np.abs(res[True][5] - res[other][5])) < 1e-11
