@@ -299,99 +299,129 @@ __global__ void __launch_bounds__(256) k_cg_h_groups(GLaunch L, const uint64_t *
     }
 }
 
-constexpr int kRowCap = 224;  // entries of one row staged per warp before they are consumed
+// ---- H psi without stored rows: H as one pair record per x-group ----------
+//
+// Within one x-group of H (terms c_t P_t sharing x), the sector indices the
+// group connects come in pairs (i0, i1 = i0 ^ x on the determinants), i0 the
+// one with x's highest bit clear, and each sector index is in at most one
+// pair.  The group's record lists them as alpha list x beta list per
+// pattern of the determinant's bits at the group's pattern positions; the
+// kernels below add H_g psi into sigma one group per launch, so no two
+// threads of a launch touch one sigma entry.
 
-// The same without scanning the groups slot by slot: each warp takes one
-// output row, its 32 lanes test 32 groups at a time, and the groups that
-// connect the row inside the sector are compacted (column, f) into a
-// shared-memory list with a ballot; the list is then consumed with the lanes
-// over (slot, entry), kRowUnrollG entries in flight per lane.
-constexpr int kRowUnrollG = 4;
-
-__global__ void __launch_bounds__(256) k_cg_h_list(GLaunch L, const uint64_t *__restrict__ det,
-                                                   const GGroup *__restrict__ groups, int ngroups,
+// sigma = f psi per row, f = sum_t c_t (-1)^popcount(det & z_t) over the
+// diagonal group's terms [t0, t1) (one warp per row, terms over the lanes);
+// every slot of the row.  This is the first H kernel: it writes sigma.
+__global__ void __launch_bounds__(256) k_cg_h_diag(GLaunch L, const uint64_t *__restrict__ det,
                                                    const GTerm *__restrict__ terms,
-                                                   const double2 *__restrict__ rterms,
-                                                   const int32_t *__restrict__ arank,
-                                                   const int32_t *__restrict__ brank,
-                                                   double2 *__restrict__ epart) {
-    __shared__ double2 s_f[8][kRowCap];
-    __shared__ uint32_t s_c[8][kRowCap];
+                                                   const double2 *__restrict__ rterms, int t0,
+                                                   int t1, int real) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int i = blockIdx.x * nwarp + warp; i < L.nsec; i += gridDim.x * nwarp) {
+        const uint64_t k = det[i];
+        double2 f = make_double2(0.0, 0.0);
+        if (real) {
+            for (int t = t0 + lane; t < t1; t += 32) {
+                const double2 zc = __ldg(&rterms[t]);
+                f.x += (__popcll(k & (uint64_t)__double_as_longlong(zc.x)) & 1) ? -zc.y : zc.y;
+            }
+        } else {
+            for (int t = t0 + lane; t < t1; t += 32) {
+                const double2 c = __ldg(&terms[t].c);
+                if (__popcll(k & __ldg(&terms[t].z)) & 1) { f.x -= c.x; f.y -= c.y; }
+                else { f.x += c.x; f.y += c.y; }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            f.x += __shfl_xor_sync(0xffffffffu, f.x, o);
+            f.y += __shfl_xor_sync(0xffffffffu, f.y, o);
+        }
+        for (int s = lane; s < L.B; s += 32)
+            L.sig[(size_t)i * L.B + s] = g_cmul(f, L.psi[(size_t)i * L.B + s]);
+    }
+}
+
+// sigma += H_g psi for one x-group.  TABLE: per pattern, sigma[i1] +=
+// sgn gn psi[i0] and sigma[i0] += sgn hn psi[i1] with sgn = (-1)^(ea.s ^ eb.s)
+// (the sign of the group's first z-mask on i0's determinant).  Otherwise the
+// two matrix elements are summed per pair from the group's terms [t0, t1):
+// H[i1][i0] = sum_t c_t (-1)^popcount(j0 & z_t), H[i0][i1] the same at
+// j1 = j0 ^ x.  Lanes over (pair, slot) as in k_cg_step.
+template <bool TABLE>
+__global__ void __launch_bounds__(256) k_cg_h_group(GLaunch L, const uint4 *__restrict__ rec,
+                                                    const uint64_t *__restrict__ det,
+                                                    const GTerm *__restrict__ terms,
+                                                    const double2 *__restrict__ rterms, int t0,
+                                                    int t1, int real, uint64_t x) {
+    const RHead hd = *reinterpret_cast<const RHead *>(rec);
+    const RPat *pats = reinterpret_cast<const RPat *>(rec + 1);
+    const SEntry *ents = reinterpret_cast<const SEntry *>(rec);
+    const int np = hd.npf & 255;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int per = 32 / L.spw;
+    const int s = blockIdx.y * L.spw + (lane % L.spw);
+    const bool live = s < L.B;
+    const int sub = lane / L.spw;
+    const int stride = gridDim.x * nwarp * per;
+    for (int p = 0; p < np; ++p) {
+        const RPat pt = pats[p];
+        const int total = (int)pt.na * (int)pt.nb;
+        for (int q = (blockIdx.x * nwarp + warp) * per + sub; q < total; q += stride) {
+            const int ai = pt.inv ? (int)__umulhi((uint32_t)q, pt.inv) : q;
+            const int bi = q - ai * (int)pt.nb;
+            const SEntry ea = ents[pt.a0 + ai], eb = ents[pt.b0 + bi];
+            if (!live) continue;
+            const size_t c0 = (size_t)ea.r0 * L.nbeta + eb.r0, c1 = (size_t)ea.r1 * L.nbeta + eb.r1;
+            double2 k10, k01;
+            if (TABLE) {
+                const bool neg = (ea.s ^ eb.s) & 1u;
+                k10 = neg ? make_double2(-pt.gn.x, -pt.gn.y) : pt.gn;
+                k01 = neg ? make_double2(-pt.hn.x, -pt.hn.y) : pt.hn;
+            } else {
+                const uint64_t j0 = det[c0], j1 = j0 ^ x;
+                k10 = make_double2(0.0, 0.0);
+                k01 = make_double2(0.0, 0.0);
+                if (real) {
+                    for (int t = t0; t < t1; ++t) {
+                        const double2 zc = __ldg(&rterms[t]);
+                        const uint64_t z = (uint64_t)__double_as_longlong(zc.x);
+                        k10.x += (__popcll(j0 & z) & 1) ? -zc.y : zc.y;
+                        k01.x += (__popcll(j1 & z) & 1) ? -zc.y : zc.y;
+                    }
+                } else {
+                    for (int t = t0; t < t1; ++t) {
+                        const double2 c = __ldg(&terms[t].c);
+                        const uint64_t z = __ldg(&terms[t].z);
+                        if (__popcll(j0 & z) & 1) { k10.x -= c.x; k10.y -= c.y; }
+                        else { k10.x += c.x; k10.y += c.y; }
+                        if (__popcll(j1 & z) & 1) { k01.x -= c.x; k01.y -= c.y; }
+                        else { k01.x += c.x; k01.y += c.y; }
+                    }
+                }
+            }
+            const size_t i0 = c0 * L.B + s, i1 = c1 * L.B + s;
+            const double2 v0 = L.psi[i0], v1 = L.psi[i1];
+            L.sig[i1] = g_cadd(L.sig[i1], g_cmul(k10, v0));
+            L.sig[i0] = g_cadd(L.sig[i0], g_cmul(k01, v1));
+        }
+    }
+}
+
+// epart[s * gridDim.x + blockIdx.x] = this block's share of <psi_s|sigma_s>.
+__global__ void __launch_bounds__(256) k_cg_dot(GLaunch L, double2 *__restrict__ epart) {
     __shared__ double2 s_e[8][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int per = 32 / L.spw, sub = lane / L.spw;
     const int s = blockIdx.y * L.spw + (lane % L.spw);
-    const bool live = s < L.B;
-    const uint64_t A = 0x5555555555555555ull;
-    double2 *lf = s_f[warp];
-    uint32_t *lc = s_c[warp];
-    double2 en = make_double2(0.0, 0.0);
-    for (int i = blockIdx.x * nwarp + warp; i < L.nsec; i += gridDim.x * nwarp) {
-        const uint64_t k = det[i];
-        double2 acc = make_double2(0.0, 0.0);
-        int cnt = 0;
-        for (int g0 = 0; g0 < ngroups; g0 += 32) {
-            const int g = g0 + lane;
-            bool valid = false;
-            double2 f = make_double2(0.0, 0.0);
-            uint32_t col = 0;
-            if (g < ngroups) {
-                const GGroup gr = groups[g];
-                const uint64_t kx = k & gr.x;
-                valid = (__popcll(kx & A) | __popcll(kx & ~A) << 8) == gr.halves;
-                if (valid) {
-                    const uint64_t j = k ^ gr.x;
-                    if (gr.real) {
-                        for (int t = gr.begin; t < gr.end; ++t) {
-                            const double2 zc = __ldg(&rterms[t]);
-                            f.x += (__popcll(j & (uint64_t)__double_as_longlong(zc.x)) & 1) ? -zc.y : zc.y;
-                        }
-                    } else {
-                        for (int t = gr.begin; t < gr.end; ++t) {
-                            const double2 c = __ldg(&terms[t].c);
-                            if (__popcll(j & __ldg(&terms[t].z)) & 1) { f.x -= c.x; f.y -= c.y; }
-                            else { f.x += c.x; f.y += c.y; }
-                        }
-                    }
-                    col = (uint32_t)(arank[g_pext_parity(j, 0)] * L.nbeta + brank[g_pext_parity(j, 1)]);
-                }
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, valid);
-            if (valid) {
-                const int pos = cnt + __popc(m & ((1u << lane) - 1u));
-                lf[pos] = f;
-                lc[pos] = col;
-            }
-            cnt += __popc(m);
-            if (cnt > kRowCap - 32 || g0 + 32 >= ngroups) {  // consume the list
-                __syncwarp();
-                for (int e0 = sub; e0 < cnt; e0 += per * kRowUnrollG) {
-                    double2 x[kRowUnrollG];
-#pragma unroll
-                    for (int u = 0; u < kRowUnrollG; ++u) {
-                        const int e = e0 + per * u;
-                        x[u] = (live && e < cnt) ? L.psi[(size_t)lc[e] * L.B + s] : make_double2(0.0, 0.0);
-                    }
-#pragma unroll
-                    for (int u = 0; u < kRowUnrollG; ++u) {
-                        const int e = e0 + per * u;
-                        if (e < cnt) acc = g_cadd(acc, g_cmul(lf[e], x[u]));
-                    }
-                }
-                __syncwarp();
-                cnt = 0;
-            }
-        }
-        for (int o = L.spw; o < 32; o <<= 1) {
-            acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-            acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-        }
-        if (sub == 0 && live) {
-            L.sig[(size_t)i * L.B + s] = acc;
-            en = g_cadd(en, g_cjmul(L.psi[(size_t)i * L.B + s], acc));
-        }
+    double2 acc = make_double2(0.0, 0.0);
+    if (s < L.B)
+        for (int i = (blockIdx.x * nwarp + warp) * per + sub; i < L.nsec; i += gridDim.x * nwarp * per)
+            acc = g_cadd(acc, g_cjmul(L.psi[(size_t)i * L.B + s], L.sig[(size_t)i * L.B + s]));
+    for (int o = L.spw; o < 32; o <<= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
     }
-    if (lane < L.spw) s_e[warp][lane] = en;
+    if (lane < L.spw) s_e[warp][lane] = acc;
     __syncthreads();
     if (threadIdx.x < L.spw) {
         double2 t = make_double2(0.0, 0.0);

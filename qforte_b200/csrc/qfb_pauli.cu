@@ -881,6 +881,7 @@ struct qfb_sum_s {
     double2 *d_rterms = nullptr;  // (z bits, Re c) per term, for real groups
     int32_t *d_seg_g0 = nullptr;
     std::vector<GroupDev> h_groups;
+    std::vector<TermDev> h_terms;  // host copy of the terms (H records of the sector)
     std::vector<int32_t> h_seg_g0;
     // (nqubit, alpha count, beta count, bank-interleaved) -> rows
     std::map<std::tuple<int, int, int, int>, std::shared_ptr<SectorRows>> rows_cache;
@@ -1512,6 +1513,7 @@ int qfb_sum_create(const qfb_pauli *paulis, const qfb_complex *coeffs, const int
         h->h_seg_g0.push_back((int32_t)h->h_groups.size());
     }
     h->ngroups = (int32_t)h->h_groups.size();
+    h->h_terms = terms;
     // each sub-array starts on a 256-byte boundary (TermDev holds a double2)
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t gbytes = al(sizeof(GroupDev) * std::max<size_t>(1, h->h_groups.size()));
@@ -2579,9 +2581,22 @@ struct SectorRows {
     const double2 *vc = nullptr;   // ... or complex
     int64_t nnz = 0;
     bool too_big = false;          // over kRowsBudget: no rows held
+    // too_big: H as pair records, one or more per x-group (build_h_records)
+    struct HRec {
+        int2 span;       // words of the record in hrec
+        int table;       // 1: (gn, hn) per pattern; 0: matrix elements from the terms
+        int t0, t1, real;
+        uint64_t x;
+        int64_t pairs;
+    };
+    std::vector<HRec> hrecs;
+    void *hblob = nullptr;
+    const uint4 *d_hrec = nullptr;
+    int diag_t0 = 0, diag_t1 = 0, diag_real = 1;  // the x = 0 group (t0 == t1: none)
     ~SectorRows() {
         dev_free(blob);
         dev_free(tblob);
+        dev_free(hblob);
     }
 };
 
@@ -2622,6 +2637,111 @@ static int plan_upload(SectorPlan &sp) {
     d->sspan = (const int2 *)(base + o_ss);
     d->sparam = (const int32_t *)(base + o_sp);
     sp.dev = d;
+    return QFB_OK;
+}
+
+// H of `ham` on the plan's sector as pair records (sigma without stored
+// rows): per x-group, the patterns of j0's bits (x's highest bit clear) at
+// the group's pattern positions -- the bits where its z-masks differ and x's
+// other bits -- that keep the alpha and beta counts, each with its alpha and
+// beta lists.  Up to kHTableBits pattern bits the record holds each
+// pattern's two matrix elements (gn = H[i1][i0], hn = H[i0][i1], divided by
+// the sign of the first z-mask on j0); beyond that its patterns cover x's
+// bits only and the kernel sums the terms per pair.  The x = 0 group is kept
+// as a term range.
+constexpr int kHTableBits = 7;
+constexpr size_t kHRecEntries = 60000;  // SEntry offsets of a record are 16-bit
+
+static int build_h_records(const qfb_sum_s *ham, const SectorPlan &sp,
+                           const std::vector<SecGroup> &sg, int n, SectorRows &rows) {
+    const uint64_t A = 0x5555555555555555ull;
+    StreamHost S;
+    for (const SecGroup &g : sg) {
+        const TermDev *T = ham->h_terms.data() + g.begin;
+        const int nt = g.end - g.begin;
+        if (g.x == 0) {
+            rows.diag_t0 = g.begin;
+            rows.diag_t1 = g.end;
+            rows.diag_real = g.real;
+            continue;
+        }
+        const int h = highest_bit(g.x);
+        const uint64_t hb = 1ull << h, zb = T[0].z;
+        uint64_t D = 0;
+        for (int t = 0; t < nt; ++t) D |= T[t].z ^ zb;
+        const uint64_t PBt = (D | g.x) & ~hb;
+        const bool table = __builtin_popcountll(PBt) <= kHTableBits;
+        const uint64_t PB = table ? PBt : (g.x & ~hb);
+        int pos[64], npb = 0;
+        for (uint64_t m = PB; m; m &= m - 1) pos[npb++] = __builtin_ctzll(m);
+        const int ka = __builtin_popcountll(g.x & A) / 2, kb = __builtin_popcountll(g.x & ~A) / 2;
+        CStep cs;
+        size_t nent = 0;
+        int64_t pairs = 0;
+        auto flush = [&]() -> int {
+            if (cs.pats.empty()) return QFB_OK;
+            if (!push_record(S, cs, 0, 0, 1 << 30))
+                return fail(QFB_ENOSYS, "H record of an x-group too large");
+            SectorRows::HRec r{};
+            r.span = S.span.back();
+            r.table = table ? 1 : 0;
+            r.t0 = g.begin;
+            r.t1 = g.end;
+            r.real = g.real;
+            r.x = g.x;
+            r.pairs = pairs;
+            rows.hrecs.push_back(r);
+            cs.pats.clear();
+            nent = 0;
+            pairs = 0;
+            return QFB_OK;
+        };
+        for (uint64_t pat = 0; pat < (1ull << npb); ++pat) {
+            uint64_t jd = 0;
+            for (int i = 0; i < npb; ++i)
+                if (pat >> i & 1) jd |= 1ull << pos[i];
+            if (__builtin_popcountll(jd & g.x & A) != ka || __builtin_popcountll(jd & g.x & ~A) != kb)
+                continue;  // the pair would leave the sector
+            CStep::Pat pt;
+            if (table) {
+                std::complex<double> gn = 0.0, hn = 0.0;
+                for (int t = 0; t < nt; ++t) {
+                    const std::complex<double> c(T[t].c.x, T[t].c.y);
+                    const double sg0 = (__builtin_popcountll(jd & (T[t].z ^ zb)) & 1) ? -1.0 : 1.0;
+                    const double sx = (__builtin_popcountll(g.x & T[t].z) & 1) ? -1.0 : 1.0;
+                    gn += c * sg0;
+                    hn += c * (sg0 * sx);
+                }
+                if (gn == 0.0 && hn == 0.0) continue;
+                pt.gn = make_double2(gn.real(), gn.imag());
+                pt.hn = make_double2(hn.real(), hn.imag());
+            } else {
+                pt.gn = pt.hn = make_double2(0.0, 0.0);
+            }
+            const uint64_t zl = table ? zb : 0;
+            if (!sector_list(sp, 0, n, PB | hb, jd, g.x, zl, pt.a) ||
+                !sector_list(sp, 1, n, PB | hb, jd, g.x, zl, pt.b))
+                return fail(QFB_EDEVICE, "H record: a pair leaves the sector");
+            if (pt.a.empty() || pt.b.empty()) continue;
+            if (nent + pt.a.size() + pt.b.size() > kHRecEntries || cs.pats.size() >= 255) {
+                const int rc = flush();
+                if (rc) return rc;
+            }
+            nent += pt.a.size() + pt.b.size();
+            pairs += (int64_t)pt.a.size() * (int64_t)pt.b.size();
+            cs.pats.push_back(std::move(pt));
+        }
+        const int rc = flush();
+        if (rc) return rc;
+    }
+    if (!S.rec.empty()) {
+        const int rc = dev_alloc(&rows.hblob, sizeof(uint4) * S.rec.size());
+        if (rc) return rc;
+        QFB_CUDA(cudaMemcpyAsync(rows.hblob, S.rec.data(), sizeof(uint4) * S.rec.size(),
+                                 cudaMemcpyHostToDevice, t_stream));
+        rows.d_hrec = (const uint4 *)rows.hblob;
+        rows.tbytes += sizeof(uint4) * S.rec.size();
+    }
     return QFB_OK;
 }
 
@@ -2682,6 +2802,10 @@ static int get_sector_rows(qfb_sum_s *ham, const SectorPlan &sp, const std::vect
     rows->ngroups = (int)sg.size();
     auto over_budget = [&]() -> int {  // rows kept without entries: sigma from the groups
         rows->too_big = true;
+        if (global) {
+            const int hrc = build_h_records(ham, sp, sg, n, *rows);
+            if (hrc) return hrc;
+        }
         QFB_CUDA(cudaStreamSynchronize(t_stream));
         ham->rows_cache[key] = rows;
         if (!global) return fail(QFB_ENOMEM, "sector H rows exceed their budget");
@@ -2934,11 +3058,28 @@ static int ucc_stage_global(qfb_ucc u, int stage, int with_grad) {
             break;
         case 2: {
             const dim3 hg(u->g_hgrid, u->g_ygrid);
-            if (u->rows->too_big)
-                qfbg::k_cg_h_list<<<hg, 256, 0, t_stream>>>(
-                    L, u->rows->det, (const qfbg::GGroup *)u->rows->groups, u->rows->ngroups,
-                    (const qfbg::GTerm *)u->ham->d_terms, u->ham->d_rterms, u->rows->arank,
-                    u->rows->brank, u->g_epart);
+            if (u->rows->too_big) {
+                const SectorRows &R = *u->rows;
+                const qfbg::GTerm *gt = (const qfbg::GTerm *)u->ham->d_terms;
+                if (R.diag_t1 > R.diag_t0) {
+                    qfbg::k_cg_h_diag<<<u->g_hgrid, 256, 0, t_stream>>>(
+                        L, R.det, gt, u->ham->d_rterms, R.diag_t0, R.diag_t1, R.diag_real);
+                    QFB_LAUNCHED();
+                } else {
+                    QFB_CUDA(cudaMemsetAsync(L.sig, 0, sizeof(double2) * (size_t)L.nsec * L.B, t_stream));
+                }
+                for (const auto &r : R.hrecs) {
+                    const dim3 rg(global_grid(r.pairs, L.spw), u->g_ygrid);
+                    if (r.table)
+                        qfbg::k_cg_h_group<true><<<rg, 256, 0, t_stream>>>(
+                            L, R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
+                    else
+                        qfbg::k_cg_h_group<false><<<rg, 256, 0, t_stream>>>(
+                            L, R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
+                    QFB_LAUNCHED();
+                }
+                qfbg::k_cg_dot<<<hg, 256, 0, t_stream>>>(L, u->g_epart);
+            }
             else if (u->g_vc)
                 qfbg::k_cg_h_rows<false><<<hg, 256, 0, t_stream>>>(L, u->g_rowptr, u->g_col, nullptr,
                                                                   u->g_vc, u->g_epart);
