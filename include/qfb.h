@@ -246,11 +246,11 @@ QFB_API int qfb_ucc_rows(qfb_ucc u, int64_t *nnz);
  * sector paths (1, the default: shared memory when the sector fits, else
  * global memory), only the global-memory one (2), only the global-memory one
  * with sigma formed from the grouped terms instead of stored H rows (3; the
- * rows are over 24 GB beyond ~24 qubits, where this happens by itself), the
- * default with complex state storage on the shared-memory path (4), or
- * neither (0).  Under 1, a shared-memory evaluator whose H and step
- * coefficients are all real keeps psi and sigma as real doubles (half the
- * shared memory and traffic).  No counterpart in the reference. */
+ * rows are over 24 GB beyond ~24 qubits, where this happens by itself), 1
+ * or 2 with complex state storage (4, 5), or neither (0).  Otherwise a
+ * compact evaluator whose H and step coefficients are all real keeps psi and
+ * sigma as real doubles (half the memory and traffic).  No counterpart in the
+ * reference. */
 QFB_API int qfb_ucc_config(int compact);
 /* Process-wide tile shape of the full-space windows of evaluators created
  * from now on: fwd_bits qubits per forward tile (default 12, at most 13),

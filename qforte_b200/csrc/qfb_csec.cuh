@@ -8,8 +8,9 @@
 // are the alpha-list x beta-list products of the step's record (the same
 // records as the shared-memory path, qfb_sector.cuh), read from global
 // memory.  sigma = H psi runs one warp per output amplitude with the lanes
-// over slots, from the sector's H rows (an evaluator whose rows would exceed
-// their memory budget keeps full-space states instead).
+// over slots, from the sector's H rows, or (rows over their budget) one
+// x-group of H per launch from pair records.  When H and every step are real
+// the states are stored as doubles (V = double), else as complex (double2).
 #pragma once
 
 #include <cstdint>
@@ -25,7 +26,7 @@ using qfbs::SEntry;
 struct GLaunch {
     int nsec, nbeta, B;
     int spw;                   // slots per warp: min(32, B rounded up to a power of two)
-    double2 *psi, *sig;        // [nsec][B]
+    void *psi, *sig;           // V [nsec][B]
     const double *params;      // [B][nparam]
     int nparam;
 };
@@ -40,14 +41,21 @@ __device__ __forceinline__ double2 g_cjmul(double2 a, double2 b) {
     return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
 }
 
+using qfbs::v_add;
+using qfbs::v_cj;
+using qfbs::v_lin;
+using qfbs::v_mul;
+using qfbs::v_zero;
+
 // One step record over (pair, slot): lane l of a warp takes slot
 // group * spw + l % spw and pair sub-index l / spw.  ROT rotates psi (and
 // sigma when TWO) by sign * gamma * theta_slot; IP accumulates <sigma|K|psi>
 // per slot into partial[(row * B + s) * gridDim.x + blockIdx.x].
-template <bool ROT, bool IP, bool TWO>
+template <bool ROT, bool IP, bool TWO, class V>
 __global__ void __launch_bounds__(256) k_cg_step(GLaunch L, const uint4 *__restrict__ rec,
                                                  int param, int sign, int row,
                                                  double2 *__restrict__ partial) {
+    V *psi = reinterpret_cast<V *>(L.psi), *sig = reinterpret_cast<V *>(L.sig);
     __shared__ double2 s_acc[8][32];
     const RHead hd = *reinterpret_cast<const RHead *>(rec);
     const RPat *pats = reinterpret_cast<const RPat *>(rec + 1);
@@ -73,24 +81,22 @@ __global__ void __launch_bounds__(256) k_cg_step(GLaunch L, const uint4 *__restr
             const size_t i0 = ((size_t)ea.r0 * L.nbeta + eb.r0) * L.B + s;
             const size_t i1 = ((size_t)ea.r1 * L.nbeta + eb.r1) * L.B + s;
             const bool neg = (ea.s ^ eb.s) & 1u;
-            double2 v0 = L.psi[i0], v1 = L.psi[i1];
+            const V v0 = psi[i0], v1 = psi[i1];
             if (IP) {
-                const double2 w0 = L.sig[i0], w1 = L.sig[i1];
-                const double2 t = g_cadd(g_cjmul(w0, g_cmul(pt.hn, v1)), g_cjmul(w1, g_cmul(pt.gn, v0)));
+                const V w0 = sig[i0], w1 = sig[i1];
+                const double2 t = g_cadd(v_cj(w0, v_mul(pt.hn, v1)), v_cj(w1, v_mul(pt.gn, v0)));
                 const double gs = neg ? -hd.gamma : hd.gamma;
                 acc.x += gs * t.x;
                 acc.y += gs * t.y;
             }
             if (ROT) {
                 const double ss = neg ? -sn : sn;
-                const double2 a = g_cmul(pt.hn, v1), b = g_cmul(pt.gn, v0);
-                L.psi[i0] = make_double2(cs * v0.x + ss * a.x, cs * v0.y + ss * a.y);
-                L.psi[i1] = make_double2(cs * v1.x + ss * b.x, cs * v1.y + ss * b.y);
+                psi[i0] = v_lin(cs, v0, ss, v_mul(pt.hn, v1));
+                psi[i1] = v_lin(cs, v1, ss, v_mul(pt.gn, v0));
                 if (TWO) {
-                    const double2 w0 = L.sig[i0], w1 = L.sig[i1];
-                    const double2 c = g_cmul(pt.hn, w1), d = g_cmul(pt.gn, w0);
-                    L.sig[i0] = make_double2(cs * w0.x + ss * c.x, cs * w0.y + ss * c.y);
-                    L.sig[i1] = make_double2(cs * w1.x + ss * d.x, cs * w1.y + ss * d.y);
+                    const V w0 = sig[i0], w1 = sig[i1];
+                    sig[i0] = v_lin(cs, w0, ss, v_mul(pt.hn, w1));
+                    sig[i1] = v_lin(cs, w1, ss, v_mul(pt.gn, w0));
                 }
             }
         }
@@ -113,9 +119,11 @@ __global__ void __launch_bounds__(256) k_cg_step(GLaunch L, const uint4 *__restr
 
 // Inner products of many independent records in one launch (blockIdx.z =
 // record; ADAPT pool operators): partial[(row * B + s) * gridDim.x + blockIdx.x].
+template <class V>
 __global__ void __launch_bounds__(256) k_cg_ip_many(GLaunch L, const uint4 *__restrict__ recs,
                                                     const int2 *__restrict__ span,
                                                     double2 *__restrict__ partial) {
+    const V *psi = reinterpret_cast<const V *>(L.psi), *sig = reinterpret_cast<const V *>(L.sig);
     __shared__ double2 s_acc[8][32];
     const uint4 *rec = recs + span[blockIdx.z].x;
     const RHead hd = *reinterpret_cast<const RHead *>(rec);
@@ -138,8 +146,8 @@ __global__ void __launch_bounds__(256) k_cg_ip_many(GLaunch L, const uint4 *__re
             if (!live) continue;
             const size_t i0 = ((size_t)ea.r0 * L.nbeta + eb.r0) * L.B + s;
             const size_t i1 = ((size_t)ea.r1 * L.nbeta + eb.r1) * L.B + s;
-            const double2 v0 = L.psi[i0], v1 = L.psi[i1], w0 = L.sig[i0], w1 = L.sig[i1];
-            const double2 t = g_cadd(g_cjmul(w0, g_cmul(pt.hn, v1)), g_cjmul(w1, g_cmul(pt.gn, v0)));
+            const V v0 = psi[i0], v1 = psi[i1], w0 = sig[i0], w1 = sig[i1];
+            const double2 t = g_cadd(v_cj(w0, v_mul(pt.hn, v1)), v_cj(w1, v_mul(pt.gn, v0)));
             const double gs = ((ea.s ^ eb.s) & 1u) ? -hd.gamma : hd.gamma;
             acc.x += gs * t.x;
             acc.y += gs * t.y;
@@ -160,20 +168,23 @@ __global__ void __launch_bounds__(256) k_cg_ip_many(GLaunch L, const uint4 *__re
 }
 
 // psi = |ref> in every slot (psi zeroed beforehand).
+template <class V>
 __global__ void k_cg_ref(GLaunch L, int ref_i) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < L.B) L.psi[(size_t)ref_i * L.B + s] = make_double2(1.0, 0.0);
+    if (s < L.B) qfbs::v_one(reinterpret_cast<V *>(L.psi)[(size_t)ref_i * L.B + s]);
 }
 
 // sigma = H psi from the sector's H rows: one warp per output row i, lanes
 // over (slot, entry sub-index) as in k_cg_step; energy partials per slot.
 // epart[s * gridDim.x + blockIdx.x] = sum over this block's rows of conj(psi) sigma.
-template <bool REAL>
+template <bool REAL, class V>
 __global__ void __launch_bounds__(256) k_cg_h_rows(GLaunch L, const int32_t *__restrict__ rowptr,
                                                    const uint32_t *__restrict__ col,
                                                    const double *__restrict__ val_r,
                                                    const double2 *__restrict__ val_c,
                                                    double2 *__restrict__ epart) {
+    const V *psi = reinterpret_cast<const V *>(L.psi);
+    V *sig = reinterpret_cast<V *>(L.sig);
     __shared__ double2 s_e[8][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int per = 32 / L.spw, sub = lane / L.spw;
@@ -181,26 +192,21 @@ __global__ void __launch_bounds__(256) k_cg_h_rows(GLaunch L, const int32_t *__r
     const bool live = s < L.B;
     double2 en = make_double2(0.0, 0.0);
     for (int i = blockIdx.x * nwarp + warp; i < L.nsec; i += gridDim.x * nwarp) {
-        double2 acc = make_double2(0.0, 0.0);
+        V acc = v_zero(V());
         const int e1 = rowptr[i + 1];
         for (int e = rowptr[i] + sub; e < e1; e += per) {
             const uint32_t c = __ldg(&col[e]);
-            const double2 x = live ? L.psi[(size_t)c * L.B + s] : make_double2(0.0, 0.0);
-            if (REAL) {
-                const double f = __ldg(&val_r[e]);
-                acc.x += f * x.x;
-                acc.y += f * x.y;
+            const V x = live ? psi[(size_t)c * L.B + s] : v_zero(V());
+            if constexpr (REAL) {
+                qfbs::v_acc(acc, __ldg(&val_r[e]), x);
             } else {
-                acc = g_cadd(acc, g_cmul(__ldg(&val_c[e]), x));
+                acc = v_add(acc, v_mul(__ldg(&val_c[e]), x));
             }
         }
-        for (int o = L.spw; o < 32; o <<= 1) {
-            acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-            acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-        }
+        for (int o = L.spw; o < 32; o <<= 1) acc = v_add(acc, qfbs::v_shfl_down(acc, o));
         if (sub == 0 && live) {
-            L.sig[(size_t)i * L.B + s] = acc;
-            en = g_cadd(en, g_cjmul(L.psi[(size_t)i * L.B + s], acc));
+            sig[(size_t)i * L.B + s] = acc;
+            en = g_cadd(en, v_cj(psi[(size_t)i * L.B + s], acc));
         }
     }
     if (lane < L.spw) s_e[warp][lane] = en;
@@ -235,70 +241,6 @@ struct GTerm {  // one term of a grouped sum (layout of TermDev)
     double2 c;
 };
 
-// sigma = H psi without stored rows (sectors whose rows would exceed their
-// budget): one warp per output row i, lanes over (slot, group sub-index);
-// each lane scans its share of the groups, forms f_x(j) for the groups that
-// connect det[i] to j = det[i] ^ x inside the sector and gathers psi at j's
-// sector index (alpha rank * nbeta + beta rank).
-__global__ void __launch_bounds__(256) k_cg_h_groups(GLaunch L, const uint64_t *__restrict__ det,
-                                                     const GGroup *__restrict__ groups, int ngroups,
-                                                     const GTerm *__restrict__ terms,
-                                                     const double2 *__restrict__ rterms,
-                                                     const int32_t *__restrict__ arank,
-                                                     const int32_t *__restrict__ brank,
-                                                     double2 *__restrict__ epart) {
-    __shared__ double2 s_e[8][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int per = 32 / L.spw, sub = lane / L.spw;
-    const int s = blockIdx.y * L.spw + (lane % L.spw);
-    const bool live = s < L.B;
-    const uint64_t A = 0x5555555555555555ull;
-    double2 en = make_double2(0.0, 0.0);
-    for (int i = blockIdx.x * nwarp + warp; i < L.nsec; i += gridDim.x * nwarp) {
-        const uint64_t k = det[i];
-        double2 acc = make_double2(0.0, 0.0);
-        for (int g = sub; g < ngroups; g += per) {
-            const uint64_t x = __ldg(&groups[g].x);
-            const uint64_t kx = k & x;
-            if ((__popcll(kx & A) | __popcll(kx & ~A) << 8) != __ldg(&groups[g].halves)) continue;
-            const uint64_t j = k ^ x;
-            const int t0 = __ldg(&groups[g].begin), t1 = __ldg(&groups[g].end);
-            double2 f = make_double2(0.0, 0.0);
-            if (__ldg(&groups[g].real)) {
-                for (int t = t0; t < t1; ++t) {
-                    const double2 zc = __ldg(&rterms[t]);
-                    f.x += (__popcll(j & (uint64_t)__double_as_longlong(zc.x)) & 1) ? -zc.y : zc.y;
-                }
-            } else {
-                for (int t = t0; t < t1; ++t) {
-                    const double2 c = __ldg(&terms[t].c);
-                    if (__popcll(j & __ldg(&terms[t].z)) & 1) { f.x -= c.x; f.y -= c.y; }
-                    else { f.x += c.x; f.y += c.y; }
-                }
-            }
-            if (!live) continue;
-            const size_t col = (size_t)arank[g_pext_parity(j, 0)] * L.nbeta + brank[g_pext_parity(j, 1)];
-            acc = g_cadd(acc, g_cmul(f, L.psi[col * L.B + s]));
-        }
-        for (int o = L.spw; o < 32; o <<= 1) {
-            acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-            acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-        }
-        if (sub == 0 && live) {
-            L.sig[(size_t)i * L.B + s] = acc;
-            en = g_cadd(en, g_cjmul(L.psi[(size_t)i * L.B + s], acc));
-        }
-    }
-    if (lane < L.spw) s_e[warp][lane] = en;
-    __syncthreads();
-    if (threadIdx.x < L.spw) {
-        double2 t = make_double2(0.0, 0.0);
-        for (int w = 0; w < nwarp; ++w) t = g_cadd(t, s_e[w][threadIdx.x]);
-        const int ss = blockIdx.y * L.spw + threadIdx.x;
-        if (ss < L.B) epart[(size_t)ss * gridDim.x + blockIdx.x] = t;
-    }
-}
-
 // ---- H psi without stored rows: H as one pair record per x-group ----------
 //
 // Within one x-group of H (terms c_t P_t sharing x), the sector indices the
@@ -312,10 +254,13 @@ __global__ void __launch_bounds__(256) k_cg_h_groups(GLaunch L, const uint64_t *
 // sigma = f psi per row, f = sum_t c_t (-1)^popcount(det & z_t) over the
 // diagonal group's terms [t0, t1) (one warp per row, terms over the lanes);
 // every slot of the row.  This is the first H kernel: it writes sigma.
+template <class V>
 __global__ void __launch_bounds__(256) k_cg_h_diag(GLaunch L, const uint64_t *__restrict__ det,
                                                    const GTerm *__restrict__ terms,
                                                    const double2 *__restrict__ rterms, int t0,
                                                    int t1, int real) {
+    const V *psi = reinterpret_cast<const V *>(L.psi);
+    V *sig = reinterpret_cast<V *>(L.sig);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int i = blockIdx.x * nwarp + warp; i < L.nsec; i += gridDim.x * nwarp) {
         const uint64_t k = det[i];
@@ -337,7 +282,7 @@ __global__ void __launch_bounds__(256) k_cg_h_diag(GLaunch L, const uint64_t *__
             f.y += __shfl_xor_sync(0xffffffffu, f.y, o);
         }
         for (int s = lane; s < L.B; s += 32)
-            L.sig[(size_t)i * L.B + s] = g_cmul(f, L.psi[(size_t)i * L.B + s]);
+            sig[(size_t)i * L.B + s] = v_mul(f, psi[(size_t)i * L.B + s]);
     }
 }
 
@@ -347,12 +292,14 @@ __global__ void __launch_bounds__(256) k_cg_h_diag(GLaunch L, const uint64_t *__
 // two matrix elements are summed per pair from the group's terms [t0, t1):
 // H[i1][i0] = sum_t c_t (-1)^popcount(j0 & z_t), H[i0][i1] the same at
 // j1 = j0 ^ x.  Lanes over (pair, slot) as in k_cg_step.
-template <bool TABLE>
+template <bool TABLE, class V>
 __global__ void __launch_bounds__(256) k_cg_h_group(GLaunch L, const uint4 *__restrict__ rec,
                                                     const uint64_t *__restrict__ det,
                                                     const GTerm *__restrict__ terms,
                                                     const double2 *__restrict__ rterms, int t0,
                                                     int t1, int real, uint64_t x) {
+    const V *psi = reinterpret_cast<const V *>(L.psi);
+    V *sig = reinterpret_cast<V *>(L.sig);
     const RHead hd = *reinterpret_cast<const RHead *>(rec);
     const RPat *pats = reinterpret_cast<const RPat *>(rec + 1);
     const SEntry *ents = reinterpret_cast<const SEntry *>(rec);
@@ -400,15 +347,17 @@ __global__ void __launch_bounds__(256) k_cg_h_group(GLaunch L, const uint4 *__re
                 }
             }
             const size_t i0 = c0 * L.B + s, i1 = c1 * L.B + s;
-            const double2 v0 = L.psi[i0], v1 = L.psi[i1];
-            L.sig[i1] = g_cadd(L.sig[i1], g_cmul(k10, v0));
-            L.sig[i0] = g_cadd(L.sig[i0], g_cmul(k01, v1));
+            const V v0 = psi[i0], v1 = psi[i1];
+            sig[i1] = v_add(sig[i1], v_mul(k10, v0));
+            sig[i0] = v_add(sig[i0], v_mul(k01, v1));
         }
     }
 }
 
 // epart[s * gridDim.x + blockIdx.x] = this block's share of <psi_s|sigma_s>.
+template <class V>
 __global__ void __launch_bounds__(256) k_cg_dot(GLaunch L, double2 *__restrict__ epart) {
+    const V *psi = reinterpret_cast<const V *>(L.psi), *sig = reinterpret_cast<const V *>(L.sig);
     __shared__ double2 s_e[8][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int per = 32 / L.spw, sub = lane / L.spw;
@@ -416,7 +365,7 @@ __global__ void __launch_bounds__(256) k_cg_dot(GLaunch L, double2 *__restrict__
     double2 acc = make_double2(0.0, 0.0);
     if (s < L.B)
         for (int i = (blockIdx.x * nwarp + warp) * per + sub; i < L.nsec; i += gridDim.x * nwarp * per)
-            acc = g_cadd(acc, g_cjmul(L.psi[(size_t)i * L.B + s], L.sig[(size_t)i * L.B + s]));
+            acc = g_cadd(acc, v_cj(psi[(size_t)i * L.B + s], sig[(size_t)i * L.B + s]));
     for (int o = L.spw; o < 32; o <<= 1) {
         acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
         acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);

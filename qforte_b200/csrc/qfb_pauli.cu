@@ -809,7 +809,8 @@ __global__ void __launch_bounds__(256) k_pool_ip(const double2 *__restrict__ psi
 // grad[b * M + mu] = 2 Re sum over mu's steps s and chunks c of
 // partial[((s * B) + b) * chunks + c].  grid = (M, B).
 // res[b][k] = Re(st[idx[k] * s_i + b * s_b] * phase[k]) (0 where idx[k] < 0)
-__global__ void k_resid_gather(const double2 *__restrict__ st, const int64_t *__restrict__ idx,
+template <class V>
+__global__ void k_resid_gather(const V *__restrict__ st, const int64_t *__restrict__ idx,
                                uint64_t s_i, uint64_t s_b, const double2 *__restrict__ phase,
                                int nres, int B, double *__restrict__ res) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -818,7 +819,8 @@ __global__ void k_resid_gather(const double2 *__restrict__ st, const int64_t *__
     const int64_t i = idx[k];
     double r = 0.0;
     if (i >= 0) {
-        const double2 v = st[(uint64_t)i * s_i + (uint64_t)b * s_b], ph = phase[k];
+        const double2 v = qfbs::v_cj(qfbs::v_one_of<V>(), st[(uint64_t)i * s_i + (uint64_t)b * s_b]);
+        const double2 ph = phase[k];
         r = v.x * ph.x - v.y * ph.y;
     }
     res[(size_t)b * nres + k] = r;
@@ -2161,6 +2163,8 @@ static std::vector<uint64_t> sector_indices(int n, uint64_t ref) {
 constexpr size_t kSectorSmemMax = 200 * 1024;  // psi + sigma of one parameter set
 constexpr int kSectorThreads = 512;
 static int g_ucc_compact = 1;  // process-wide: use the compact evaluator when it applies
+// qfb_ucc_config 4 and 5: complex state storage even where every coefficient is real
+static bool ucc_complex_states() { return g_ucc_compact == 4 || g_ucc_compact == 5; }
 
 // Rows of H on the compact sector: row i (the sector index of det[i]) holds,
 // for every group x connecting det[i] to j = det[i] ^ x inside the sector,
@@ -2449,6 +2453,7 @@ struct qfb_ucc_s {
     size_t bytes = 0;     // device bytes held (blobs)
     int compact = 0;      // compact sector evaluator (qfb_sector.cuh)
     int sreal = 0;        // compact: real states (every coefficient and H real)
+    int greal = 0;        // compact in global memory: real states
     int64_t nnz = 0;      // entries of the H rows on the compact sector
     std::shared_ptr<SectorRows> rows;  // compact paths: H rows on the sector
     qfbs::SLaunch SL{};
@@ -2885,7 +2890,7 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
     if (rc) return rc;
     std::shared_ptr<SectorRows> rows;
     // real states gather 8-byte amplitudes: interleave rows for 16 bank slots
-    const bool real_steps = g_ucc_compact != 4 && stream_is_real(sp.fwd) && stream_is_real(sp.sweep);
+    const bool real_steps = !ucc_complex_states() && stream_is_real(sp.fwd) && stream_is_real(sp.sweep);
     rc = get_sector_rows(ham, sp, sg, u->nqubit, global ? 0 : (real_steps ? 16 : 8), global, &rows);
     if (rc) return rc;
     u->splan = plan;
@@ -3039,19 +3044,20 @@ static unsigned global_grid(int64_t pairs, int spw) {
 
 // Compact sector in global memory: stage 0 the reference, 1 the forward
 // records, 2 sigma = H psi and the energy, 3 the sweep records.
-static int ucc_stage_global(qfb_ucc u, int stage, int with_grad) {
+template <class V>
+static int ucc_stage_global_v(qfb_ucc u, int stage, int with_grad) {
     const qfbg::GLaunch &L = u->GL;
     const SectorPlan &sp = *u->splan;
     const dim3 grid(u->g_sgrid, u->g_ygrid);
     switch (stage) {
         case 0:
-            QFB_CUDA(cudaMemsetAsync(L.psi, 0, sizeof(double2) * (size_t)L.nsec * L.B, t_stream));
-            qfbg::k_cg_ref<<<(L.B + 127) / 128, 128, 0, t_stream>>>(L, sp.ref_i);
+            QFB_CUDA(cudaMemsetAsync(L.psi, 0, sizeof(V) * (size_t)L.nsec * L.B, t_stream));
+            qfbg::k_cg_ref<V><<<(L.B + 127) / 128, 128, 0, t_stream>>>(L, sp.ref_i);
             QFB_LAUNCHED();
             break;
         case 1:
             for (size_t r = 0; r < sp.fwd.span.size(); ++r) {
-                qfbg::k_cg_step<true, false, false><<<grid, 256, 0, t_stream>>>(
+                qfbg::k_cg_step<true, false, false, V><<<grid, 256, 0, t_stream>>>(
                     L, u->g_frec + sp.fwd.span[r].x, sp.fwd.param[r], 1, -1, nullptr);
                 QFB_LAUNCHED();
             }
@@ -3062,30 +3068,32 @@ static int ucc_stage_global(qfb_ucc u, int stage, int with_grad) {
                 const SectorRows &R = *u->rows;
                 const qfbg::GTerm *gt = (const qfbg::GTerm *)u->ham->d_terms;
                 if (R.diag_t1 > R.diag_t0) {
-                    qfbg::k_cg_h_diag<<<u->g_hgrid, 256, 0, t_stream>>>(
+                    qfbg::k_cg_h_diag<V><<<u->g_hgrid, 256, 0, t_stream>>>(
                         L, R.det, gt, u->ham->d_rterms, R.diag_t0, R.diag_t1, R.diag_real);
                     QFB_LAUNCHED();
                 } else {
-                    QFB_CUDA(cudaMemsetAsync(L.sig, 0, sizeof(double2) * (size_t)L.nsec * L.B, t_stream));
+                    QFB_CUDA(cudaMemsetAsync(L.sig, 0, sizeof(V) * (size_t)L.nsec * L.B, t_stream));
                 }
                 for (const auto &r : R.hrecs) {
                     const dim3 rg(global_grid(r.pairs, L.spw), u->g_ygrid);
                     if (r.table)
-                        qfbg::k_cg_h_group<true><<<rg, 256, 0, t_stream>>>(
+                        qfbg::k_cg_h_group<true, V><<<rg, 256, 0, t_stream>>>(
                             L, R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
                     else
-                        qfbg::k_cg_h_group<false><<<rg, 256, 0, t_stream>>>(
+                        qfbg::k_cg_h_group<false, V><<<rg, 256, 0, t_stream>>>(
                             L, R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
                     QFB_LAUNCHED();
                 }
-                qfbg::k_cg_dot<<<hg, 256, 0, t_stream>>>(L, u->g_epart);
+                qfbg::k_cg_dot<V><<<hg, 256, 0, t_stream>>>(L, u->g_epart);
             }
-            else if (u->g_vc)
-                qfbg::k_cg_h_rows<false><<<hg, 256, 0, t_stream>>>(L, u->g_rowptr, u->g_col, nullptr,
-                                                                  u->g_vc, u->g_epart);
-            else
-                qfbg::k_cg_h_rows<true><<<hg, 256, 0, t_stream>>>(L, u->g_rowptr, u->g_col, u->g_vr,
-                                                                 nullptr, u->g_epart);
+            else if (u->g_vc) {
+                if constexpr (sizeof(V) == sizeof(double2))
+                    qfbg::k_cg_h_rows<false, V><<<hg, 256, 0, t_stream>>>(L, u->g_rowptr, u->g_col,
+                                                                         nullptr, u->g_vc, u->g_epart);
+            } else {
+                qfbg::k_cg_h_rows<true, V><<<hg, 256, 0, t_stream>>>(L, u->g_rowptr, u->g_col, u->g_vr,
+                                                                    nullptr, u->g_epart);
+            }
             QFB_LAUNCHED();
             qfbg::k_cg_energy<<<(L.B + 7) / 8, 256, 0, t_stream>>>(u->g_epart, (int)u->g_hgrid, L.B,
                                                                   u->energy);
@@ -3101,13 +3109,13 @@ static int ucc_stage_global(qfb_ucc u, int stage, int with_grad) {
                 const uint4 *rec = u->g_srec + sp.sweep.span[r].x;
                 const int par = sp.sweep.param[r];
                 if (fl == (qfbs::R_ROT | qfbs::R_IP | qfbs::R_TWO))
-                    qfbg::k_cg_step<true, true, true><<<grid, 256, 0, t_stream>>>(L, rec, par, -1, hd.row,
+                    qfbg::k_cg_step<true, true, true, V><<<grid, 256, 0, t_stream>>>(L, rec, par, -1, hd.row,
                                                                                  u->gpart);
                 else if (fl == qfbs::R_IP)
-                    qfbg::k_cg_step<false, true, false><<<grid, 256, 0, t_stream>>>(L, rec, par, -1,
+                    qfbg::k_cg_step<false, true, false, V><<<grid, 256, 0, t_stream>>>(L, rec, par, -1,
                                                                                    hd.row, u->gpart);
                 else
-                    qfbg::k_cg_step<true, false, true><<<grid, 256, 0, t_stream>>>(L, rec, par, -1, -1,
+                    qfbg::k_cg_step<true, false, true, V><<<grid, 256, 0, t_stream>>>(L, rec, par, -1, -1,
                                                                                   nullptr);
                 QFB_LAUNCHED();
             }
@@ -3118,6 +3126,12 @@ static int ucc_stage_global(qfb_ucc u, int stage, int with_grad) {
         }
     }
     return QFB_OK;
+}
+
+// Compact sector in global memory, real or complex state storage.
+static int ucc_stage_global(qfb_ucc u, int stage, int with_grad) {
+    return u->greal ? ucc_stage_global_v<double>(u, stage, with_grad)
+                    : ucc_stage_global_v<double2>(u, stage, with_grad);
 }
 
 static int ucc_stage(qfb_ucc u, int stage, int with_grad) {
@@ -3177,8 +3191,12 @@ static int ucc_pool_stage(qfb_ucc u) {
     unsigned chunks = u->pchunks;
     if (u->gsec) {
         const dim3 grid(u->pchunks, u->g_ygrid, (unsigned)u->pstream.n);
-        qfbg::k_cg_ip_many<<<grid, 256, 0, t_stream>>>(u->GL, u->pstream.rec, u->pstream.span,
-                                                       u->ppart);
+        if (u->greal)
+            qfbg::k_cg_ip_many<double><<<grid, 256, 0, t_stream>>>(u->GL, u->pstream.rec,
+                                                                   u->pstream.span, u->ppart);
+        else
+            qfbg::k_cg_ip_many<double2><<<grid, 256, 0, t_stream>>>(u->GL, u->pstream.rec,
+                                                                    u->pstream.span, u->ppart);
         QFB_LAUNCHED();
     } else if (u->compact) {
         qfbs::SLaunch L = u->SL;
@@ -3230,19 +3248,29 @@ static int ucc_resid_stage(qfb_ucc u) {
         const SectorPlan &sp = *u->splan;
         const dim3 grid(u->g_sgrid, u->g_ygrid);
         for (size_t r = sp.fwd.span.size(); r-- > 0;) {
-            qfbg::k_cg_step<true, false, false><<<grid, 256, 0, t_stream>>>(
-                Ls, u->g_frec + sp.fwd.span[r].x, sp.fwd.param[r], -1, -1, nullptr);
+            if (u->greal)
+                qfbg::k_cg_step<true, false, false, double><<<grid, 256, 0, t_stream>>>(
+                    Ls, u->g_frec + sp.fwd.span[r].x, sp.fwd.param[r], -1, -1, nullptr);
+            else
+                qfbg::k_cg_step<true, false, false, double2><<<grid, 256, 0, t_stream>>>(
+                    Ls, u->g_frec + sp.fwd.span[r].x, sp.fwd.param[r], -1, -1, nullptr);
             QFB_LAUNCHED();
         }
-        k_resid_gather<<<gg, 256, 0, t_stream>>>(u->GL.sig, u->ridx, (uint64_t)B, 1, u->rphase,
-                                                 u->nres, B, u->res);
+        if (u->greal)
+            k_resid_gather<double><<<gg, 256, 0, t_stream>>>((const double *)u->GL.sig, u->ridx,
+                                                             (uint64_t)B, 1, u->rphase, u->nres, B,
+                                                             u->res);
+        else
+            k_resid_gather<double2><<<gg, 256, 0, t_stream>>>((const double2 *)u->GL.sig, u->ridx,
+                                                              (uint64_t)B, 1, u->rphase, u->nres, B,
+                                                              u->res);
         QFB_LAUNCHED();
         return QFB_OK;
     }
     int rc = enqueue_prog(u->fwd, u->sig, u->nqubit, B, u->params, 0, -1);
     if (rc) return rc;
-    k_resid_gather<<<gg, 256, 0, t_stream>>>(u->sig, u->ridx, 1, u->nbasis, u->rphase, u->nres, B,
-                                             u->res);
+    k_resid_gather<double2><<<gg, 256, 0, t_stream>>>(u->sig, u->ridx, 1, u->nbasis, u->rphase,
+                                                      u->nres, B, u->res);
     QFB_LAUNCHED();
     return QFB_OK;
 }
@@ -3394,7 +3422,10 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
     const size_t o_sec = take(idx_bytes * std::max<size_t>(sector.size(), 1));
     const size_t o_sg = take(sizeof(SecGroup) * std::max<size_t>(sgroups.size(), 1));
     const size_t o_save = take(compact ? sizeof(double2) * 2 * (size_t)splan.nsec * B : 16);
-    const size_t b_cstate = gsec ? sizeof(double2) * (size_t)splan.nsec * B : 16;
+    // global-memory compact states are real doubles when H and every step are real
+    bool greal = gsec && !ucc_complex_states() && stream_is_real(splan.fwd) && stream_is_real(splan.sweep);
+    for (const SecGroup &g : sgroups) greal = greal && g.real;
+    const size_t b_cstate = gsec ? (greal ? sizeof(double) : sizeof(double2)) * (size_t)splan.nsec * B : 16;
     const size_t o_cpsi = take(b_cstate), o_csig = take(b_cstate);
     const size_t o_epart = take(gsec ? sizeof(double2) * B * hgrid : 16);
     int rc = dev_alloc(&u->blob, off);
@@ -3420,8 +3451,9 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
         u->GL.nbeta = splan.nbeta;
         u->GL.B = nbatch;
         u->GL.spw = spw;
-        u->GL.psi = (double2 *)(base + o_cpsi);
-        u->GL.sig = (double2 *)(base + o_csig);
+        u->GL.psi = base + o_cpsi;
+        u->GL.sig = base + o_csig;
+        u->greal = greal ? 1 : 0;
         u->GL.params = u->params;
         u->GL.nparam = u->nparam;
         u->g_sgrid = sgrid;
@@ -3462,7 +3494,7 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
             return rc;
         }
         // real states: real H rows, real pair coefficients in both streams
-        u->sreal = (compact && g_ucc_compact != 4 && u->SL.val_c == nullptr &&
+        u->sreal = (compact && !ucc_complex_states() && u->SL.val_c == nullptr &&
                     stream_is_real(plan->fwd) && stream_is_real(plan->sweep))
                        ? 1
                        : 0;
@@ -3483,14 +3515,14 @@ int qfb_ucc_tiles(int fwd_bits, int grad_bits, int low_bits) {
 }
 
 int qfb_ucc_config(int compact) {
-    if (compact < 0 || compact > 4) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
+    if (compact < 0 || compact > 5) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
     g_ucc_compact = compact;
     return QFB_OK;
 }
 
 int qfb_ucc_real_states(qfb_ucc u, int32_t *real) {
     if (!u || !real) return fail(QFB_EINVAL, "qfb_ucc_real_states: null argument");
-    *real = u->sreal;
+    *real = u->sreal | u->greal;
     return QFB_OK;
 }
 
@@ -3543,7 +3575,7 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
         for (size_t k = 0; k < cs.size(); ++k)
             if (!push_record(sh, cs[k], qfbs::R_IP, (int)k, u->gsec ? (1 << 30) : kSectorThreads))
                 return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool step too large");
-        if (u->sreal && !stream_is_real(sh))
+        if ((u->sreal || u->greal) && !stream_is_real(sh))
             return fail(QFB_ENOSYS, "qfb_ucc_set_pool: complex pool coefficients on an evaluator "
                                     "with real states (create it with qfb_ucc_config(4))");
         chunks = u->compact ? kSectorThreads / 32 : global_grid(stream_max_pairs(sh), u->GL.spw);

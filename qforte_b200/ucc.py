@@ -48,8 +48,10 @@ def evaluator_config(compact=True):
     """Process-wide: let evaluators created from now on use the compact
     sector paths (True, the default; real states where every coefficient is
     real), the same with complex state storage ("complex"), only the
-    global-memory one ("global"), or keep full-space states (False)."""
-    mode = {"global": 2, "global-no-rows": 3, "complex": 4}.get(compact, 1 if compact else 0)
+    global-memory one ("global"; "global-complex" with complex storage), or
+    keep full-space states (False)."""
+    mode = {"global": 2, "global-no-rows": 3, "complex": 4, "global-complex": 5}.get(
+        compact, 1 if compact else 0)
     check(lib().qfb_ucc_config(mode), "qfb_ucc_config")
 
 

@@ -525,16 +525,17 @@ def test_global_sector_pool_gradients(cuda):
 
 @pytest.mark.parametrize("norb,seed,pool_type", [(4, 11, "SD"), (6, 3, "SD"), (5, 9, "GSD")])
 def test_real_state_storage_matches_complex(cuda, norb, seed, pool_type):
-    """The shared-memory compact path keeps psi and sigma as real doubles when
-    H and every step coefficient are real: energies, gradients, pool
-    gradients and PQE residuals equal those of complex storage and of the
-    full-space path."""
+    """The compact paths keep psi and sigma as real doubles when H and every
+    step coefficient are real: energies, gradients, pool gradients and PQE
+    residuals equal those of complex storage and of the full-space path, in
+    shared memory and in global memory (with H rows and without)."""
     from qforte_b200.ucc import evaluator_config
     mol, pool = random_problem(norb, seed, pool_type)
     tops = list(range(0, len(pool), 1 if len(pool) < 400 else 3))
     P = np.random.default_rng(seed).uniform(-0.1, 0.1, (5, len(tops)))
     res = {}
-    for mode in (True, "complex", False):
+    modes = (True, "complex", "global", "global-complex", "global-no-rows", False)
+    for mode in modes:
         evaluator_config(mode)
         try:
             eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
@@ -547,12 +548,14 @@ def test_real_state_storage_matches_complex(cuda, norb, seed, pool_type):
             res[mode] = out
         finally:
             evaluator_config(True)
-    assert res[True][3] == 2 and res[True][4] is True
-    assert res["complex"][3] == 2 and res["complex"][4] is False
+    expect = {True: (2, True), "complex": (2, False), "global": (3, True),
+              "global-complex": (3, False), "global-no-rows": (3, True)}
+    for mode, (path, real) in expect.items():
+        assert res[mode][3] == path and res[mode][4] is real, mode
     assert res[False][3] in (0, 1)
-    for other in ("complex", False):
-        assert np.max(np.abs(res[True][0] - res[other][0])) < 1e-12
-        assert np.max(np.abs(res[True][1] - res[other][1])) < 1e-11
-        assert np.max(np.abs(res[True][2] - res[other][2])) < 1e-11
+    for mode in modes[1:]:
+        assert np.max(np.abs(res[True][0] - res[mode][0])) < 1e-12
+        assert np.max(np.abs(res[True][1] - res[mode][1])) < 1e-11
+        assert np.max(np.abs(res[True][2] - res[mode][2])) < 1e-11
         if pool_type == "SD":
-            assert np.max(np.abs(res[True][5] - res[other][5])) < 1e-11
+            assert np.max(np.abs(res[True][5] - res[mode][5])) < 1e-11
