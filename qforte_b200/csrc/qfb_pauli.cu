@@ -36,6 +36,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -2247,16 +2248,32 @@ struct SectorPlanDev {
     ~SectorPlanDev() { dev_free(blob); }
 };
 
+// Device copies of a plan's pair-list streams (qfbs::PStream) for one bank
+// slot width, uploaded once and shared by the plan's evaluators.
+struct PairPlanDev {
+    void *blob = nullptr;
+    size_t bytes = 0;
+    qfbs::PStream fwd{}, sweep{};
+    std::vector<qfbs::PHead> fwd_hd;  // host copy (residual streams run it in reverse)
+    ~PairPlanDev() { dev_free(blob); }
+};
+
 struct SectorPlan {
     int na_orb = 0, nb_orb = 0, nalpha = 0, nbeta = 0, nsec = 0, ref_i = 0;
     int ka = 0, kb = 0;  // alpha and beta electrons of the sector
     std::shared_ptr<SectorPlanDev> dev;
+    std::shared_ptr<PairPlanDev> pdev[2];  // pair lists ordered for 8 / 16 bank slots
     std::vector<uint64_t> adet, bdet;
     std::vector<int32_t> arank, brank;
     std::vector<CStep> fsteps, ksteps, usteps;
     std::vector<int2> kmu, umu;
     int fused = 0;
     StreamHost fwd, sweep;
+    struct SweepItem {
+        int unrot;  // step of usteps (1) or ksteps (0)
+        int step, flags, row;
+    };
+    std::vector<SweepItem> sweep_items;  // the sweep stream's records, in order
 };
 
 static uint32_t pext_parity_bits(uint64_t v, int odd, int n) {
@@ -2359,7 +2376,7 @@ static bool push_record(StreamHost &S, const CStep &cs, int flags, int row,
 // do not fit 16 bits, a step record larger than the block).
 static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_prog_s *kp,
                               const qfb_prog_s *up, int n, uint64_t ref, bool shared = true) {
-    const int mw = shared ? kSectorThreads : (1 << 30);
+    const int mw = 1 << 30;  // records of any size (the shared path reads pair lists)
     const uint64_t A = 0x5555555555555555ull;
     const uint64_t all = (1ull << n) - 1ull;
     sp.na_orb = (n + 1) / 2;
@@ -2408,27 +2425,185 @@ static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_pr
         // from last to first, <sigma|K_mu|psi> on each K step, then (mu > 0)
         // U_mu^dagger on both states; a single step that is both K and U does
         // the two at once
+        auto sweep_rec = [&](int unrot, int s, int fl, int row) {
+            sp.sweep_items.push_back(SectorPlan::SweepItem{unrot, s, fl, row});
+            return push_record(sp.sweep, unrot ? sp.usteps[s] : sp.ksteps[s], fl, row, mw);
+        };
         for (int mu = M - 1; mu >= 0; --mu) {
             const int s0 = kp->p_step0[mu], s1 = kp->p_step1[mu];
             if (sp.fused) {
                 const int fl = mu > 0 ? (qfbs::R_ROT | qfbs::R_IP | qfbs::R_TWO) : qfbs::R_IP;
-                if (!push_record(sp.sweep, sp.ksteps[s0], fl, s0, mw)) return false;
+                if (!sweep_rec(0, s0, fl, s0)) return false;
                 continue;
             }
             for (int s = s0; s >= 0 && s < s1; ++s)
-                if (!push_record(sp.sweep, sp.ksteps[s], qfbs::R_IP, s, mw)) return false;
+                if (!sweep_rec(0, s, qfbs::R_IP, s)) return false;
             if (mu == 0) break;
             const int u0 = up->p_step0[mu], u1 = up->p_step1[mu];
             for (int s = u0; u0 >= 0 && s < u1; ++s)
-                if (!push_record(sp.sweep, sp.usteps[s], qfbs::R_ROT | qfbs::R_TWO, -1, mw))
-                    return false;
+                if (!sweep_rec(1, s, qfbs::R_ROT | qfbs::R_TWO, -1)) return false;
         }
     }
     if (!shared) return true;
-    const size_t ring = 3 * (size_t)std::max(sp.fwd.maxw, sp.sweep.maxw) * 16;
-    const size_t ang = sizeof(double2) * std::max(sp.fwd.span.size(), sp.sweep.span.size());
-    if (nsec * 2 * sizeof(double2) + ang + ring > kSectorSmemMax) return false;
+    const size_t ang = sizeof(qfbs::PSmem) * std::max(sp.fwd.span.size(), sp.sweep.span.size());
+    if (nsec * 2 * sizeof(double2) + ang > kSectorSmemMax) return false;
     return true;
+}
+
+// One kernel's pair-list records (qfbs::PStream) on the host.
+struct PairHost {
+    std::vector<qfbs::PHead> hd;
+    std::vector<uint2> pair;
+    std::vector<double2> coef;  // per pattern: gn, hn
+};
+
+// Order the pairs of one record so that each run of S consecutive pairs (the
+// lanes of a half warp reading 8-byte amplitudes, S = 16, or of a quarter warp
+// reading 16-byte amplitudes, S = 8) reads S distinct bank slots (index mod S)
+// at i0 and S distinct slots at i1 as far as the record allows.  Each run is a
+// maximum matching between i0 slots and i1 slots over the pairs left (Kuhn's
+// augmenting paths, fullest slots tried first), topped up from the fullest
+// (i0 slot, i1 slot) buckets.  Only the order in which threads take the
+// record's pairs changes; the pairs of a record touch distinct amplitudes.
+static void order_pairs(uint2 *p, size_t n, int S) {
+    if (n <= 1) return;
+    std::vector<std::vector<uint2>> bk((size_t)S * S);
+    for (size_t k = 0; k < n; ++k) {
+        const uint32_t a = (p[k].x & 0x7fffffffu) % (uint32_t)S, b = (p[k].y & 0xffffffu) % (uint32_t)S;
+        bk[(size_t)a * S + b].push_back(p[k]);
+    }
+    std::vector<int> d0(S), d1(S), m1(S), ord0(S), ord1(S);
+    size_t out = 0;
+    std::function<bool(int, uint32_t &)> augment = [&](int a, uint32_t &seen) -> bool {
+        for (int b : ord1) {
+            if (bk[(size_t)a * S + b].empty() || (seen >> b & 1u)) continue;
+            seen |= 1u << b;
+            if (m1[b] < 0 || augment(m1[b], seen)) {
+                m1[b] = a;
+                return true;
+            }
+        }
+        return false;
+    };
+    while (out < n) {
+        std::fill(d0.begin(), d0.end(), 0);
+        std::fill(d1.begin(), d1.end(), 0);
+        for (int a = 0; a < S; ++a)
+            for (int b = 0; b < S; ++b) {
+                const int c = (int)bk[(size_t)a * S + b].size();
+                d0[a] += c;
+                d1[b] += c;
+            }
+        for (int k = 0; k < S; ++k) ord0[k] = ord1[k] = k;
+        std::stable_sort(ord0.begin(), ord0.end(), [&](int x, int y) { return d0[x] > d0[y]; });
+        std::stable_sort(ord1.begin(), ord1.end(), [&](int x, int y) { return d1[x] > d1[y]; });
+        std::fill(m1.begin(), m1.end(), -1);
+        for (int a : ord0) {
+            if (!d0[a]) continue;
+            uint32_t seen = 0;
+            augment(a, seen);
+        }
+        const size_t want = std::min<size_t>((size_t)S, n - out), first = out;
+        for (int b = 0; b < S; ++b)
+            if (m1[b] >= 0) {
+                auto &v = bk[(size_t)m1[b] * S + b];
+                p[out++] = v.back();
+                v.pop_back();
+            }
+        while (out - first < want) {  // fewer distinct slots than lanes left
+            size_t best = 0;
+            for (size_t k = 1; k < bk.size(); ++k)
+                if (bk[k].size() > bk[best].size()) best = k;
+            p[out++] = bk[best].back();
+            bk[best].pop_back();
+        }
+    }
+}
+
+// Append one step as a pair-list record: every pair (i0, i1) of its patterns
+// with the sign bit of (-1)^popcount(j0 & zbase) and the pattern's number.
+static bool push_pairs(PairHost &P, const SectorPlan &sp, const CStep &cs, int flags, int row, int S) {
+    const int npat = (int)cs.pats.size();
+    if (npat > 255 || sp.nsec >= (1 << 24)) return false;
+    qfbs::PHead h{};
+    h.p0 = (int32_t)P.pair.size();
+    h.c0 = (int32_t)(P.coef.size() / 2);
+    h.fl = flags | npat << 8;
+    h.row = row;
+    h.gamma = cs.gamma;
+    h.param = cs.param;
+    for (int k = 0; k < npat; ++k) {
+        const auto &pt = cs.pats[k];
+        P.coef.push_back(pt.gn);
+        P.coef.push_back(pt.hn);
+        for (const qfbs::SEntry &ea : pt.a)
+            for (const qfbs::SEntry &eb : pt.b) {
+                const uint32_t i0 = (uint32_t)ea.r0 * (uint32_t)sp.nbeta + eb.r0;
+                const uint32_t i1 = (uint32_t)ea.r1 * (uint32_t)sp.nbeta + eb.r1;
+                P.pair.push_back(make_uint2(i0 | ((ea.s ^ eb.s) & 1u) << 31, i1 | (uint32_t)k << 24));
+            }
+    }
+    if (P.pair.size() >= (1ull << 31)) return false;
+    h.np = (int32_t)(P.pair.size() - (size_t)h.p0);
+    order_pairs(P.pair.data() + h.p0, (size_t)h.np, S);
+    P.hd.push_back(h);
+    return true;
+}
+
+// Upload one stream's headers, pairs and coefficients at base + off (256-byte
+// aligned pieces); returns the device stream.
+static size_t pair_bytes(const PairHost &P) {
+    auto al = [](size_t x) { return (std::max<size_t>(x, 16) + 255) & ~(size_t)255; };
+    return al(sizeof(qfbs::PHead) * P.hd.size()) + al(sizeof(uint2) * P.pair.size()) +
+           al(sizeof(double2) * P.coef.size());
+}
+static int pair_upload(const PairHost &P, char *base, qfbs::PStream &out) {
+    auto al = [](size_t x) { return (std::max<size_t>(x, 16) + 255) & ~(size_t)255; };
+    char *hd = base, *pr = hd + al(sizeof(qfbs::PHead) * P.hd.size());
+    char *cf = pr + al(sizeof(uint2) * P.pair.size());
+    if (!P.hd.empty())
+        QFB_CUDA(cudaMemcpyAsync(hd, P.hd.data(), sizeof(qfbs::PHead) * P.hd.size(),
+                                 cudaMemcpyHostToDevice, t_stream));
+    if (!P.pair.empty())
+        QFB_CUDA(cudaMemcpyAsync(pr, P.pair.data(), sizeof(uint2) * P.pair.size(),
+                                 cudaMemcpyHostToDevice, t_stream));
+    if (!P.coef.empty())
+        QFB_CUDA(cudaMemcpyAsync(cf, P.coef.data(), sizeof(double2) * P.coef.size(),
+                                 cudaMemcpyHostToDevice, t_stream));
+    out.hd = (const qfbs::PHead *)hd;
+    out.pair = (const uint2 *)pr;
+    out.coef = (const double2 *)cf;
+    out.n = (int)P.hd.size();
+    return QFB_OK;
+}
+
+// The plan's forward and sweep streams as pair lists ordered for S bank slots.
+static int pair_plan(SectorPlan &sp, int S, std::shared_ptr<PairPlanDev> *out) {
+    std::shared_ptr<PairPlanDev> &slot = sp.pdev[S == 16 ? 1 : 0];
+    if (slot) {
+        *out = slot;
+        return QFB_OK;
+    }
+    PairHost F, W;
+    for (const CStep &cs : sp.fsteps)
+        if (!push_pairs(F, sp, cs, qfbs::R_ROT, -1, S))
+            return fail(QFB_ENOSYS, "compact sector: forward step outside the pair-list limits");
+    for (const auto &it : sp.sweep_items)
+        if (!push_pairs(W, sp, it.unrot ? sp.usteps[it.step] : sp.ksteps[it.step], it.flags, it.row, S))
+            return fail(QFB_ENOSYS, "compact sector: sweep step outside the pair-list limits");
+    auto d = std::make_shared<PairPlanDev>();
+    const size_t bf = pair_bytes(F), bw = pair_bytes(W);
+    int rc = dev_alloc(&d->blob, bf + bw);
+    if (rc) return rc;
+    d->bytes = bf + bw;
+    rc = pair_upload(F, (char *)d->blob, d->fwd);
+    if (!rc) rc = pair_upload(W, (char *)d->blob + bf, d->sweep);
+    if (!rc) QFB_CUDA(cudaStreamSynchronize(t_stream));
+    if (rc) return rc;
+    d->fwd_hd = F.hd;
+    slot = d;
+    *out = d;
+    return QFB_OK;
 }
 
 struct qfb_ucc_s {
@@ -2480,7 +2655,8 @@ struct qfb_ucc_s {
     int2 *pranges = nullptr;   // pool steps of each operator
     StepDev *pool_steps = nullptr;  // full space: the pool's steps on the device
     unsigned pchunks = 1;
-    qfbs::SStream pstream{};   // compact: the pool's inner-product records
+    qfbs::SStream pstream{};   // global-memory sector: the pool's inner-product records
+    qfbs::PStream ppairs{};    // shared-memory sector: the pool's pair lists
     // PQE residuals (qfb_ucc_set_residuals): Re(<I_k|U^dagger H U|ref> phase_k)
     int nres = 0;
     void *rblob = nullptr;
@@ -2488,7 +2664,8 @@ struct qfb_ucc_s {
     double *res = nullptr;            // [B][nres]
     const int64_t *ridx = nullptr;    // full-space index, or compact index (-1: outside)
     const double2 *rphase = nullptr;  // [nres]
-    qfbs::SStream rstream{};          // compact: forward records in reverse order
+    qfbs::PStream rstream{};          // compact: forward pair lists in reverse order
+    std::shared_ptr<PairPlanDev> pairs;  // compact: the plan's pair lists in use
 };
 
 // Whether every pattern of every record of a stream has real coefficients.
@@ -2893,6 +3070,15 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
     const bool real_steps = !ucc_complex_states() && stream_is_real(sp.fwd) && stream_is_real(sp.sweep);
     rc = get_sector_rows(ham, sp, sg, u->nqubit, global ? 0 : (real_steps ? 16 : 8), global, &rows);
     if (rc) return rc;
+    std::shared_ptr<PairPlanDev> pairs;
+    if (!global) {
+        // real states: real H rows and real pair coefficients in both streams
+        u->sreal = (real_steps && rows->vc == nullptr) ? 1 : 0;
+        rc = pair_plan(sp, u->sreal ? 16 : 8, &pairs);
+        if (rc) return rc;
+        u->pairs = pairs;
+        u->bytes += pairs->bytes;
+    }
     u->splan = plan;
     u->rows = rows;
     u->nnz = rows->nnz;
@@ -2912,16 +3098,8 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
     L.nbeta = sp.nbeta;
     L.ref_i = sp.ref_i;
     L.nparam = u->nparam;
-    L.fwd.rec = d.frec;
-    L.fwd.span = d.fspan;
-    L.fwd.param = d.fparam;
-    L.fwd.n = (int)sp.fwd.span.size();
-    L.fwd.maxw = std::max(sp.fwd.maxw, 1);
-    L.sweep.rec = d.srec;
-    L.sweep.span = d.sspan;
-    L.sweep.param = d.sparam;
-    L.sweep.n = (int)sp.sweep.span.size();
-    L.sweep.maxw = std::max(sp.sweep.maxw, 1);
+    L.fwd = pairs->fwd;
+    L.sweep = pairs->sweep;
     L.rowptr = rows->rowptr;
     L.col = rows->col;
     L.val_r = rows->vr;
@@ -2974,8 +3152,7 @@ static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
         case 1:
             qfbs::k_sector_forward<V><<<u->nbatch, kSectorThreads,
                                         qfbs::sector_smem_states(1, n, real) +
-                                            sizeof(double2) * (size_t)L.fwd.n +
-                                            sizeof(uint4) * 3 * (size_t)L.fwd.maxw,
+                                            sizeof(qfbs::PSmem) * (size_t)L.fwd.n,
                                         t_stream>>>(L);
             QFB_LAUNCHED();
             break;
@@ -2996,8 +3173,7 @@ static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
             if (!(with_grad && u->grad && u->nparam > 0)) break;
             qfbs::k_sector_sweep<V><<<u->nbatch, kSectorThreads,
                                       qfbs::sector_smem_states(2, n, real) +
-                                          sizeof(double2) * (size_t)L.sweep.n +
-                                          sizeof(uint4) * 3 * (size_t)L.sweep.maxw,
+                                          sizeof(qfbs::PSmem) * (size_t)L.sweep.n,
                                       t_stream>>>(L);
             QFB_LAUNCHED();
             k_grad_final<<<dim3(u->nparam, u->nbatch), 128, 0, t_stream>>>(u->gpart, u->psteps,
@@ -3202,13 +3378,12 @@ static int ucc_pool_stage(qfb_ucc u) {
         qfbs::SLaunch L = u->SL;
         L.partial = u->ppart;
         const int sm = sm_count();
-        const int G = std::max(1, std::min(u->pstream.n, (2 * sm + B - 1) / B));
-        const size_t smem = qfbs::sector_smem_states(2, (size_t)L.nsec, u->sreal) +
-                            sizeof(uint4) * u->pstream.maxw;
+        const int G = std::max(1, std::min(u->ppairs.n, (2 * sm + B - 1) / B));
+        const size_t smem = qfbs::sector_smem_states(2, (size_t)L.nsec, u->sreal);
         if (u->sreal)
-            qfbs::k_sector_pool<double><<<dim3(G, B), kSectorThreads, smem, t_stream>>>(L, u->pstream);
+            qfbs::k_sector_pool<double><<<dim3(G, B), kSectorThreads, smem, t_stream>>>(L, u->ppairs);
         else
-            qfbs::k_sector_pool<double2><<<dim3(G, B), kSectorThreads, smem, t_stream>>>(L, u->pstream);
+            qfbs::k_sector_pool<double2><<<dim3(G, B), kSectorThreads, smem, t_stream>>>(L, u->ppairs);
         QFB_LAUNCHED();
         chunks = kSectorThreads / 32;
     } else {
@@ -3231,8 +3406,7 @@ static int ucc_resid_stage(qfb_ucc u) {
     if (u->compact) {
         const qfbs::SLaunch &L = u->SL;
         const size_t smem = qfbs::sector_smem_states(1, (size_t)L.nsec, u->sreal) +
-                            sizeof(double2) * (size_t)u->rstream.n +
-                            sizeof(uint4) * 3 * (size_t)u->rstream.maxw;
+                            sizeof(qfbs::PSmem) * (size_t)u->rstream.n;
         if (u->sreal)
             qfbs::k_sector_resid<double><<<B, kSectorThreads, smem, t_stream>>>(
                 L, u->rstream, u->ridx, u->rphase, u->nres, u->res);
@@ -3493,11 +3667,6 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
             qfb_ucc_destroy(u);
             return rc;
         }
-        // real states: real H rows, real pair coefficients in both streams
-        u->sreal = (compact && !ucc_complex_states() && u->SL.val_c == nullptr &&
-                    stream_is_real(plan->fwd) && stream_is_real(plan->sweep))
-                       ? 1
-                       : 0;
     }
     *out = u;
     return QFB_OK;
@@ -3567,15 +3736,21 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
     if (nst == 0 || nst > 65535) return fail(QFB_ENOSYS, "qfb_ucc_set_pool: %zu pool steps", nst);
     qfbs::SStream ps{};
     StreamHost sh;
+    PairHost ph;  // shared-memory sector: the pool as pair lists
     unsigned chunks = 1;
     if (u->compact || u->gsec) {
         std::vector<CStep> cs;
         if (!sector_steps(*u->splan, pool, u->nqubit, cs))
             return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool outside the Givens form on the sector");
-        for (size_t k = 0; k < cs.size(); ++k)
-            if (!push_record(sh, cs[k], qfbs::R_IP, (int)k, u->gsec ? (1 << 30) : kSectorThreads))
+        for (size_t k = 0; k < cs.size(); ++k) {
+            if (u->gsec && !push_record(sh, cs[k], qfbs::R_IP, (int)k, 1 << 30))
                 return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool step too large");
-        if ((u->sreal || u->greal) && !stream_is_real(sh))
+            if (u->compact && !push_pairs(ph, *u->splan, cs[k], qfbs::R_IP, (int)k, u->sreal ? 16 : 8))
+                return fail(QFB_ENOSYS, "qfb_ucc_set_pool: pool step too large");
+        }
+        bool real = true;
+        for (const double2 &c : ph.coef) real = real && c.y == 0.0;
+        if ((u->sreal && !real) || (u->greal && !stream_is_real(sh)))
             return fail(QFB_ENOSYS, "qfb_ucc_set_pool: complex pool coefficients on an evaluator "
                                     "with real states (create it with qfb_ucc_config(4))");
         chunks = u->compact ? kSectorThreads / 32 : global_grid(stream_max_pairs(sh), u->GL.spw);
@@ -3602,6 +3777,7 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
     const size_t o_ps = take((u->compact || u->gsec) ? 16 : sizeof(StepDev) * nst);
     const size_t o_rec = take(sizeof(uint4) * sh.rec.size());
     const size_t o_sp = take(sizeof(int2) * sh.span.size());
+    const size_t o_pl = take(u->compact ? pair_bytes(ph) : 16);
     void *blob = nullptr;
     int rc = dev_alloc(&blob, off);
     if (rc) return rc;
@@ -3621,6 +3797,8 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
     if (e == cudaSuccess && !sh.span.empty())
         e = cudaMemcpyAsync(base + o_sp, sh.span.data(), sizeof(int2) * sh.span.size(),
                             cudaMemcpyHostToDevice, t_stream);
+    qfbs::PStream pp{};
+    if (e == cudaSuccess && u->compact && pair_upload(ph, base + o_pl, pp)) e = cudaErrorUnknown;
     if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);
     if (e != cudaSuccess) {
         dev_free(blob);
@@ -3645,6 +3823,7 @@ int qfb_ucc_set_pool(qfb_ucc u, qfb_prog pool) {
     ps.n = (int)sh.span.size();
     ps.maxw = std::max(sh.maxw, 1);
     u->pstream = ps;
+    u->ppairs = pp;
     return QFB_OK;
 }
 
@@ -3666,22 +3845,14 @@ int qfb_ucc_set_residuals(qfb_ucc u, const uint64_t *dets, const qfb_complex *ph
             idx[k] = (int64_t)dets[k];
         }
     }
-    // compact, shared memory: the forward records in reverse order
-    std::vector<int2> rspan;
-    std::vector<int32_t> rparam;
-    if (u->compact) {
-        const SectorPlan &sp = *u->splan;
-        for (size_t r = sp.fwd.span.size(); r-- > 0;) {
-            rspan.push_back(sp.fwd.span[r]);
-            rparam.push_back(sp.fwd.param[r]);
-        }
-    }
+    // compact, shared memory: the forward pair-list headers in reverse order
+    std::vector<qfbs::PHead> rhd;
+    if (u->compact) rhd.assign(u->pairs->fwd_hd.rbegin(), u->pairs->fwd_hd.rend());
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const int B = u->nbatch;
     const size_t o_res = 0, o_idx = al(sizeof(double) * (size_t)B * n),
                  o_ph = o_idx + al(sizeof(int64_t) * n), o_sp = o_ph + al(sizeof(double2) * n),
-                 o_pa = o_sp + al(sizeof(int2) * std::max<size_t>(1, rspan.size())),
-                 total = o_pa + sizeof(int32_t) * std::max<size_t>(1, rparam.size());
+                 total = o_sp + sizeof(qfbs::PHead) * std::max<size_t>(1, rhd.size());
     void *blob = nullptr;
     int rc = dev_alloc(&blob, total);
     if (rc) return rc;
@@ -3692,12 +3863,9 @@ int qfb_ucc_set_residuals(qfb_ucc u, const uint64_t *dets, const qfb_complex *ph
                              t_stream));
     QFB_CUDA(cudaMemcpyAsync(bp + o_ph, ph.data(), sizeof(double2) * n, cudaMemcpyHostToDevice,
                              t_stream));
-    if (!rspan.empty()) {
-        QFB_CUDA(cudaMemcpyAsync(bp + o_sp, rspan.data(), sizeof(int2) * rspan.size(),
+    if (!rhd.empty())
+        QFB_CUDA(cudaMemcpyAsync(bp + o_sp, rhd.data(), sizeof(qfbs::PHead) * rhd.size(),
                                  cudaMemcpyHostToDevice, t_stream));
-        QFB_CUDA(cudaMemcpyAsync(bp + o_pa, rparam.data(), sizeof(int32_t) * rparam.size(),
-                                 cudaMemcpyHostToDevice, t_stream));
-    }
     QFB_CUDA(cudaMemsetAsync(bp + o_res, 0, sizeof(double) * (size_t)B * n, t_stream));
     if (u->exec[4]) {  // a captured residual run refers to the old buffers
         cudaGraphExecDestroy(u->exec[4]);
@@ -3716,8 +3884,7 @@ int qfb_ucc_set_residuals(qfb_ucc u, const uint64_t *dets, const qfb_complex *ph
     u->rphase = (const double2 *)(bp + o_ph);
     if (u->compact) {
         u->rstream = u->SL.fwd;
-        u->rstream.span = (const int2 *)(bp + o_sp);
-        u->rstream.param = (const int32_t *)(bp + o_pa);
+        u->rstream.hd = (const qfbs::PHead *)(bp + o_sp);
     }
     return QFB_OK;
 }

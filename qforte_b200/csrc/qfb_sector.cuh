@@ -9,8 +9,9 @@
 // sigma of one parameter set in shared memory and runs the whole evaluation
 // there: the forward program, sigma = H psi from a sparse row list of H built
 // once per evaluator, the energy, and the adjoint reverse sweep, with one
-// barrier per program step and no global traffic besides the H rows and one
-// save of psi and sigma between the kernels.
+// barrier per program step and no global traffic besides the H rows, the
+// steps' pair lists (read-only, L2-resident, shared by every CTA) and one save
+// of psi and sigma between the kernels.
 //
 // When every step's pair coefficients and H are real (particle-hole and
 // generalised pools of real excitations, real integrals), psi and sigma stay
@@ -24,8 +25,13 @@
 // pattern's alpha and beta bits, so the pairs of one pattern are the product
 // of an alpha list and a beta list, each entry holding a string's rank, its
 // partner's rank (string ^ x) and its share of the sign
-// sigma(j0) = (-1)^popcount(j0 & zbase).  The arithmetic on each pair is that
-// of the full-space kernels (givens_pair and the gradient inner product).
+// sigma(j0) = (-1)^popcount(j0 & zbase).  The global-memory path
+// (qfb_csec.cuh) reads those lists (records of RHead / RPat / SEntry); the
+// shared-memory kernels here read the product expanded on the host into one
+// word pair per amplitude pair (PHead / PStream), ordered so that each half
+// warp (quarter warp for complex amplitudes) touches distinct banks.  The
+// arithmetic on each pair is that of the full-space kernels (givens_pair and
+// the gradient inner product).
 #pragma once
 
 #include <cstdint>
@@ -38,8 +44,8 @@ struct SEntry {  // one string of an alpha or beta list
 };
 
 // A step record: the 16-byte header, the patterns, then the entries of their
-// lists, contiguous so that one cooperative copy brings a whole step into
-// shared memory.  Records run in the order a kernel executes them.
+// lists, contiguous in one stream of 16-byte words.  Records run in the order
+// a kernel executes them.
 struct RHead {
     int32_t npf;   // patterns | flags << 8
     int32_t row;   // partial row of an inner product
@@ -58,12 +64,35 @@ struct SStream {          // one kernel's records
     const int2 *span;     // per record: first word, words
     const int32_t *param; // per record: parameter of its angle
     int n;
-    int maxw;             // longest record (words), <= block size
+    int maxw;             // longest record (words)
+};
+
+// A step record on the pair list, used by the shared-memory kernels: the
+// pairs of the step's patterns as explicit sector index pairs, ordered on the
+// host so that the lanes of a warp reach distinct shared-memory banks, and the
+// step's constants.  A stream's headers, pairs and pattern coefficients are
+// three arrays.
+struct PHead {
+    int32_t p0;     // first pair
+    int32_t np;     // pairs
+    int32_t fl;     // flags (R_ROT | R_IP | R_TWO) | patterns << 8
+    int32_t row;    // partial row of an inner product
+    double gamma;
+    int32_t c0;     // first pattern's (gn, hn) in coef
+    int32_t param;  // parameter of the record's angle
+};
+static_assert(sizeof(PHead) == 32, "PHead is two 16-byte words");
+
+struct PStream {
+    const PHead *hd;
+    const uint2 *pair;     // x = i0 | neg << 31, y = i1 | pattern << 24
+    const double2 *coef;   // per pattern: gn, hn
+    int n;
 };
 
 struct SLaunch {
     int nsec, nbeta, ref_i, nparam;
-    SStream fwd, sweep;
+    PStream fwd, sweep;
     const int32_t *rowptr;     // H rows
     const uint32_t *col;
     const double *val_r;       // real H (val_c == nullptr) ...
@@ -98,6 +127,7 @@ __device__ __forceinline__ V v_one_of() {
 // coefficient g times amplitude x (real storage: g is real)
 __device__ __forceinline__ double2 v_mul(double2 g, double2 x) { return s_cmul(g, x); }
 __device__ __forceinline__ double v_mul(double2 g, double x) { return g.x * x; }
+__device__ __forceinline__ double v_mul(double g, double x) { return g * x; }
 // c x + s y
 __device__ __forceinline__ double2 v_lin(double c, double2 x, double s, double2 y) {
     return make_double2(c * x.x + s * y.x, c * x.y + s * y.y);
@@ -122,118 +152,197 @@ __device__ __forceinline__ double2 v_shfl_down(double2 v, int o) {
 }
 
 // new0 = c v0 + s hn v1, new1 = c v1 + s gn v0 (as givens_pair)
-template <class V>
-__device__ __forceinline__ void s_givens(V &v0, V &v1, double c, double s, double2 gn, double2 hn) {
+template <class V, class K>
+__device__ __forceinline__ void s_givens(V &v0, V &v1, double c, double s, K gn, K hn) {
     const V a = v_mul(hn, v1), b = v_mul(gn, v0);
     const V n0 = v_lin(c, v0, s, a);
     v1 = v_lin(c, v1, s, b);
     v0 = n0;
 }
 
-// One record on the compact states: rotation of v (and w when TWO) by the
-// angle whose cos / sin is csn, and / or the inner product <w|K|v> of the
-// step's generator into acc.  rec is the record in shared memory.
-template <bool ROT, bool IP, bool TWO, class V>
-__device__ __forceinline__ void s_record(const uint4 *rec, int nbeta, double2 csn, V *v, V *w,
-                                         double2 &acc) {
-    const RHead hd = *reinterpret_cast<const RHead *>(rec);
-    const RPat *pats = reinterpret_cast<const RPat *>(rec + 1);
-    const SEntry *ents = reinterpret_cast<const SEntry *>(rec);
-    const int np = hd.npf & 255;
-    const double cs = csn.x, sn = csn.y;
-    for (int p = 0; p < np; ++p) {
-        const RPat pt = pats[p];
-        const int total = (int)pt.na * (int)pt.nb;
-        for (int q = threadIdx.x; q < total; q += blockDim.x) {
-            const int ai = pt.inv ? (int)__umulhi((uint32_t)q, pt.inv) : q;
-            const int bi = q - ai * (int)pt.nb;
-            const SEntry ea = ents[pt.a0 + ai], eb = ents[pt.b0 + bi];
-            const int i0 = (int)ea.r0 * nbeta + (int)eb.r0, i1 = (int)ea.r1 * nbeta + (int)eb.r1;
-            const bool neg = (ea.s ^ eb.s) & 1u;
-            V v0 = v[i0], v1 = v[i1];
-            if (IP) {
-                const V w0 = w[i0], w1 = w[i1];
-                const double2 t = s_cadd(v_cj(w0, v_mul(pt.hn, v1)), v_cj(w1, v_mul(pt.gn, v0)));
-                const double gs = neg ? -hd.gamma : hd.gamma;
-                acc.x += gs * t.x;
-                acc.y += gs * t.y;
-            }
-            if (ROT) {
-                const double ss = neg ? -sn : sn;
-                s_givens(v0, v1, cs, ss, pt.gn, pt.hn);
-                v[i0] = v0;
-                v[i1] = v1;
-                if (TWO) {
-                    V w0 = w[i0], w1 = w[i1];
-                    s_givens(w0, w1, cs, ss, pt.gn, pt.hn);
-                    w[i0] = w0;
-                    w[i1] = w1;
-                }
-            }
-        }
-    }
+// A pair's share of <w|K|v>: conj(w0) hn v1 + conj(w1) gn v0
+__device__ __forceinline__ double v_ip(double w0, double w1, double v0, double v1, double gn,
+                                       double hn) {
+    return w0 * (hn * v1) + w1 * (gn * v0);
+}
+__device__ __forceinline__ double2 v_ip(double2 w0, double2 w1, double2 v0, double2 v1, double2 gn,
+                                        double2 hn) {
+    return s_cadd(s_cjmul(w0, s_cmul(hn, v1)), s_cjmul(w1, s_cmul(gn, v0)));
+}
+__device__ __forceinline__ double2 v_as2(double x) { return make_double2(x, 0.0); }
+__device__ __forceinline__ double2 v_as2(double2 x) { return x; }
+
+__device__ __forceinline__ PHead p_head(const PHead *p) {
+    const int4 a = __ldg(reinterpret_cast<const int4 *>(p));
+    const int4 b = __ldg(reinterpret_cast<const int4 *>(p) + 1);
+    PHead h;
+    h.p0 = a.x;
+    h.np = a.y;
+    h.fl = a.z;
+    h.row = a.w;
+    h.gamma = __hiloint2double(b.y, b.x);
+    h.c0 = b.z;
+    h.param = b.w;
+    return h;
 }
 
-__device__ __forceinline__ double2 s_warp_sum(double2 v) {
+// Pair words of the next record held per thread: two for real amplitudes,
+// one for complex ones (whose pairs need twice the registers).
+template <class V>
+__host__ __device__ constexpr int pair_slots() {
+    return sizeof(V) == sizeof(double) ? 2 : 1;
+}
+
+// This thread's first KP pair words of record h (pairs tid, tid + nth, ...)
+template <int KP>
+__device__ __forceinline__ void p_words(const PStream &S, const PHead &h, uint2 (&pw)[KP]) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        v.x += __shfl_down_sync(0xffffffffu, v.x, o);
-        v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+    for (int j = 0; j < KP; ++j) {
+        const int k = threadIdx.x + j * blockDim.x;
+        pw[j] = k < h.np ? __ldg(S.pair + h.p0 + k) : make_uint2(0u, 0u);
     }
-    return v;
 }
 
-// cos and sin of sign * gamma * theta of every record of a stream, into s_cs
-__device__ __forceinline__ void s_angles(const SStream &S, const double *par, int sign,
-                                         double2 *s_cs) {
+// One pair: the share of <w|K|v> into acc and / or the rotation of v (and w
+// when TWO) by the angle whose cos / sin is (c, s).
+template <bool ROT, bool IP, bool TWO, class V>
+__device__ __forceinline__ void p_pair(uint2 pw, double c, double s, double gamma, V gn, V hn, V *v,
+                                       V *w, V &acc) {
+    const int i0 = (int)(pw.x & 0x7fffffffu), i1 = (int)(pw.y & 0xffffffu);
+    const bool neg = pw.x >> 31;
+    V v0 = v[i0], v1 = v[i1];
+    V w0 = v_zero(V()), w1 = w0;
+    if (IP || TWO) {
+        w0 = w[i0];
+        w1 = w[i1];
+    }
+    if (IP) v_acc(acc, neg ? -gamma : gamma, v_ip(w0, w1, v0, v1, gn, hn));
+    if (ROT) {
+        const double ss = neg ? -s : s;
+        s_givens(v0, v1, c, ss, gn, hn);
+        v[i0] = v0;
+        v[i1] = v1;
+        if (TWO) {
+            s_givens(w0, w1, c, ss, gn, hn);
+            w[i0] = w0;
+            w[i1] = w1;
+        }
+    }
+}
+
+// One record on the compact states: this thread's pairs (the prefetched
+// words first, then any beyond KP per thread).  The pairs of one record touch
+// distinct amplitudes, so threads need no ordering within it.
+// The coefficients (gn, hn) of pattern k of a stream: real parts only for
+// real amplitudes.
+__device__ __forceinline__ void p_ldcoef(const PStream &S, int k, double &gn, double &hn) {
+    gn = __ldg(reinterpret_cast<const double *>(S.coef + 2 * k));
+    hn = __ldg(reinterpret_cast<const double *>(S.coef + 2 * k + 1));
+}
+__device__ __forceinline__ void p_ldcoef(const PStream &S, int k, double2 &gn, double2 &hn) {
+    gn = __ldg(S.coef + 2 * k);
+    hn = __ldg(S.coef + 2 * k + 1);
+}
+
+// gn, hn: the coefficients of a single-pattern record (p_coef); records of
+// several patterns load each pair's from its pattern number.
+template <bool ROT, bool IP, bool TWO, class V, int KP>
+__device__ __forceinline__ void p_record(const PStream &S, const PHead &h, const uint2 (&pw)[KP],
+                                         double2 csn, V gn, V hn, V *v, V *w, V &acc) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const bool one = (h.fl >> 8) == 1;
+    auto run = [&](uint2 p) {
+        if (!one) p_ldcoef(S, h.c0 + (int)(p.y >> 24), gn, hn);
+        p_pair<ROT, IP, TWO, V>(p, csn.x, csn.y, h.gamma, gn, hn, v, w, acc);
+    };
+#pragma unroll
+    for (int j = 0; j < KP; ++j)
+        if (tid + j * nth < h.np) run(pw[j]);
+    for (int k = tid + KP * nth; k < h.np; k += nth) run(__ldg(S.pair + h.p0 + k));
+}
+
+// The coefficients of record h when it has a single pattern (else zeros)
+template <class V>
+__device__ __forceinline__ void p_coef(const PStream &S, const PHead &h, V &gn, V &hn) {
+    gn = hn = v_zero(V());
+    if ((h.fl >> 8) == 1) p_ldcoef(S, h.c0, gn, hn);
+}
+
+// A record as the kernels keep it in shared memory: its header and the cos /
+// sin of its angle for this CTA's parameter set.
+struct PSmem {
+    PHead h;
+    double2 cs;
+};
+static_assert(sizeof(PSmem) == 48, "PSmem is three 16-byte words");
+
+// Every record's header and cos / sin of sign * gamma * theta into s_pr
+__device__ __forceinline__ void p_angles(const PStream &S, const double *par, int sign,
+                                         PSmem *s_pr) {
     for (int r = threadIdx.x; r < S.n; r += blockDim.x) {
-        const RHead hd = *reinterpret_cast<const RHead *>(S.rec + S.span[r].x);
+        const PHead h = p_head(S.hd + r);
         double sn, cs;
-        sincos((double)sign * hd.gamma * par[S.param[r]], &sn, &cs);
-        s_cs[r] = make_double2(cs, sn);
+        sincos((double)sign * h.gamma * par[h.param], &sn, &cs);
+        s_pr[r].h = h;
+        s_pr[r].cs = make_double2(cs, sn);
     }
 }
 
-// Run a stream: record r + 2 is copied from global memory into registers
-// while record r is applied from shared memory (three buffers of maxw words
-// at s_rec), and stored after it; one barrier per record.
-template <bool SWEEP, class V>
-__device__ __forceinline__ void s_run(const SLaunch &L, const SStream &S, const double2 *s_cs,
-                                      uint4 *s_rec, V *v, V *w) {
-    const int tid = threadIdx.x, nw = blockDim.x >> 5;
-    for (int r = 0; r < 2 && r < S.n; ++r) {
-        const int2 sp = S.span[r];
-        if (tid < sp.y) s_rec[r * S.maxw + tid] = S.rec[sp.x + tid];
+// This thread's pair words and the coefficients of record h
+template <class V, int KP>
+__device__ __forceinline__ void p_fetch(const PStream &S, const PHead &h, uint2 (&pw)[KP], V &gn,
+                                        V &hn) {
+    p_words(S, h, pw);
+    p_coef(S, h, gn, hn);
+}
+
+// Apply record r (header and angle from shared memory) with this thread's
+// prefetched words; SWEEP records carry flags (rotation of both states, inner
+// product or both) and write one partial per warp of each inner product.
+template <bool SWEEP, class V, int KP>
+__device__ __forceinline__ void p_step(const PStream &S, const PSmem *s_pr, int r,
+                                       const uint2 (&pw)[KP], V gn, V hn, V *v, V *w,
+                                       double2 *partial) {
+    const PHead h = s_pr[r].h;
+    const double2 csn = s_pr[r].cs;
+    const int fl = h.fl & 255;
+    V acc = v_zero(V());
+    if (!SWEEP) {
+        p_record<true, false, false, V, KP>(S, h, pw, csn, gn, hn, v, w, acc);
+    } else if (fl == (R_ROT | R_IP | R_TWO)) {
+        p_record<true, true, true, V, KP>(S, h, pw, csn, gn, hn, v, w, acc);
+    } else if (fl == R_IP) {
+        p_record<false, true, false, V, KP>(S, h, pw, csn, gn, hn, v, w, acc);
+    } else {
+        p_record<true, false, true, V, KP>(S, h, pw, csn, gn, hn, v, w, acc);
     }
-    __syncthreads();
-    for (int r = 0; r < S.n; ++r) {
-        uint4 nxt = make_uint4(0, 0, 0, 0);
-        bool have = false;
-        if (r + 2 < S.n) {
-            const int2 sp = S.span[r + 2];
-            have = tid < sp.y;
-            if (have) nxt = S.rec[sp.x + tid];
-        }
-        const uint4 *rec = s_rec + (r % 3) * S.maxw;
-        const int npf = reinterpret_cast<const RHead *>(rec)->npf;
-        const int fl = npf >> 8;
-        double2 acc = make_double2(0.0, 0.0);
-        if (!SWEEP) {
-            s_record<true, false, false, V>(rec, L.nbeta, s_cs[r], v, nullptr, acc);
-        } else if (fl == (R_ROT | R_IP | R_TWO)) {
-            s_record<true, true, true, V>(rec, L.nbeta, s_cs[r], v, w, acc);
-        } else if (fl == R_IP) {
-            s_record<false, true, false, V>(rec, L.nbeta, s_cs[r], v, w, acc);
-        } else {
-            s_record<true, false, true, V>(rec, L.nbeta, s_cs[r], v, w, acc);
-        }
-        if (SWEEP && (fl & R_IP)) {
-            acc = s_warp_sum(acc);
-            const int row = reinterpret_cast<const RHead *>(rec)->row;
-            if ((tid & 31) == 0)
-                L.partial[((size_t)row * gridDim.x + blockIdx.x) * nw + (tid >> 5)] = acc;
-        }
-        if (have) s_rec[((r + 2) % 3) * S.maxw + tid] = nxt;
+    if (SWEEP && (fl & R_IP)) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc = v_add(acc, v_shfl_down(acc, o));
+        if ((threadIdx.x & 31) == 0)
+            partial[((size_t)h.row * gridDim.x + blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)] =
+                v_as2(acc);
+    }
+}
+
+// Run a stream, one barrier per record.  Two register sets alternate: while
+// record r is applied from one, the pair words and coefficients of record
+// r + 1 load into the other, so no load is waited on before its record runs.
+template <bool SWEEP, class V>
+__device__ __forceinline__ void p_run(const PStream &S, const PSmem *s_pr, V *v, V *w,
+                                      double2 *partial) {
+    constexpr int KP = pair_slots<V>();
+    const int n = S.n;
+    uint2 wa[KP], wb[KP];
+    V ga, ha, gb, hb;
+    if (n > 0) p_fetch(S, s_pr[0].h, wa, ga, ha);
+    for (int r = 0; r < n; r += 2) {
+        if (r + 1 < n) p_fetch(S, s_pr[r + 1].h, wb, gb, hb);
+        p_step<SWEEP, V, KP>(S, s_pr, r, wa, ga, ha, v, w, partial);
+        __syncthreads();
+        if (r + 1 >= n) break;
+        if (r + 2 < n) p_fetch(S, s_pr[r + 2].h, wa, ga, ha);
+        p_step<SWEEP, V, KP>(S, s_pr, r + 1, wb, gb, hb, v, w, partial);
         __syncthreads();
     }
 }
@@ -245,21 +354,19 @@ constexpr int kRowUnroll = 8;  // H row entries in flight per lane
 // with the energy (psi in shared memory, sigma rows straight to the save
 // buffer), and the reverse sweep (psi and sigma in shared memory).  The
 // first two hold one state and fit two CTAs per SM.  Shared memory: the
-// states, then the cos / sin of every record's angle, then the record ring.
+// states, then every record's header with the cos / sin of its angle (PSmem).
 
 template <class V>
 __global__ void __launch_bounds__(512, 2) k_sector_forward(SLaunch L) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *psi = reinterpret_cast<V *>(s_raw);
-    double2 *s_cs = reinterpret_cast<double2 *>(s_raw + ((sizeof(V) * L.nsec + 15) & ~(size_t)15));
-    uint4 *s_rec = reinterpret_cast<uint4 *>(s_cs + L.fwd.n);
+    PSmem *s_pr = reinterpret_cast<PSmem *>(s_raw + ((sizeof(V) * L.nsec + 15) & ~(size_t)15));
     const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
     const double *par = L.params + (size_t)b * L.nparam;
-    for (int i = tid; i < L.nsec; i += nth) psi[i] = v_zero(V());
-    s_angles(L.fwd, par, 1, s_cs);
+    for (int i = tid; i < L.nsec; i += nth) psi[i] = i == L.ref_i ? v_one_of<V>() : v_zero(V());
+    p_angles(L.fwd, par, 1, s_pr);
     __syncthreads();
-    if (tid == 0) v_one(psi[L.ref_i]);
-    s_run<false, V>(L, L.fwd, s_cs, s_rec, psi, (V *)nullptr);
+    p_run<false, V>(L.fwd, s_pr, psi, (V *)nullptr, nullptr);
     V *sv = reinterpret_cast<V *>(L.save) + (size_t)b * 2 * L.nsec;
     for (int i = tid; i < L.nsec; i += nth) sv[i] = psi[i];
 }
@@ -320,15 +427,14 @@ template <class V>
 __global__ void __launch_bounds__(512, 2) k_sector_sweep(SLaunch L) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *psi = reinterpret_cast<V *>(s_raw), *sig = psi + L.nsec;
-    double2 *s_cs = reinterpret_cast<double2 *>(s_raw + ((sizeof(V) * 2 * L.nsec + 15) & ~(size_t)15));
-    uint4 *s_rec = reinterpret_cast<uint4 *>(s_cs + L.sweep.n);
+    PSmem *s_pr = reinterpret_cast<PSmem *>(s_raw + ((sizeof(V) * 2 * L.nsec + 15) & ~(size_t)15));
     const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
     const double *par = L.params + (size_t)b * L.nparam;
     const V *sv = reinterpret_cast<const V *>(L.save) + (size_t)b * 2 * L.nsec;
     for (int i = tid; i < 2 * L.nsec; i += nth) psi[i] = sv[i];
-    s_angles(L.sweep, par, -1, s_cs);
+    p_angles(L.sweep, par, -1, s_pr);
     __syncthreads();
-    s_run<true, V>(L, L.sweep, s_cs, s_rec, psi, sig);
+    p_run<true, V>(L.sweep, s_pr, psi, sig, L.partial);
 }
 
 // PQE residuals on the compact states: sigma of slot blockIdx.x from the save
@@ -336,21 +442,20 @@ __global__ void __launch_bounds__(512, 2) k_sector_sweep(SLaunch L) {
 // records in reverse order, angles negated), then
 // res[b][k] = Re(sigma[idx[k]] * phase[k]) (0 where idx[k] < 0).
 template <class V>
-__global__ void __launch_bounds__(512, 2) k_sector_resid(SLaunch L, SStream R,
+__global__ void __launch_bounds__(512, 2) k_sector_resid(SLaunch L, PStream R,
                                                          const int64_t *__restrict__ idx,
                                                          const double2 *__restrict__ phase,
                                                          int nres, double *__restrict__ res) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *sig = reinterpret_cast<V *>(s_raw);
-    double2 *s_cs = reinterpret_cast<double2 *>(s_raw + ((sizeof(V) * L.nsec + 15) & ~(size_t)15));
-    uint4 *s_rec = reinterpret_cast<uint4 *>(s_cs + R.n);
+    PSmem *s_pr = reinterpret_cast<PSmem *>(s_raw + ((sizeof(V) * L.nsec + 15) & ~(size_t)15));
     const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
     const double *par = L.params + (size_t)b * L.nparam;
     const V *sv = reinterpret_cast<const V *>(L.save) + (size_t)b * 2 * L.nsec + L.nsec;
     for (int i = tid; i < L.nsec; i += nth) sig[i] = sv[i];
-    s_angles(R, par, -1, s_cs);
+    p_angles(R, par, -1, s_pr);
     __syncthreads();
-    s_run<false, V>(L, R, s_cs, s_rec, sig, (V *)nullptr);
+    p_run<false, V>(R, s_pr, sig, (V *)nullptr, nullptr);
     for (int k = tid; k < nres; k += nth) {
         const int64_t i = idx[k];
         double r = 0.0;
@@ -364,27 +469,28 @@ __global__ void __launch_bounds__(512, 2) k_sector_resid(SLaunch L, SStream R,
 
 // Pool inner products on the compact states: each CTA loads psi and sigma of
 // slot blockIdx.y and runs the inner-product records r = blockIdx.x,
-// blockIdx.x + gridDim.x, ... of the pool stream (records leave the states
-// unchanged, so CTAs share none).
+// blockIdx.x + gridDim.x, ... of the pool stream.  The records leave the
+// states unchanged, so they need no barrier between them.
 template <class V>
-__global__ void __launch_bounds__(512, 2) k_sector_pool(SLaunch L, SStream P) {
+__global__ void __launch_bounds__(512, 2) k_sector_pool(SLaunch L, PStream P) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *psi = reinterpret_cast<V *>(s_raw), *sig = psi + L.nsec;
-    uint4 *s_rec = reinterpret_cast<uint4 *>(s_raw + ((sizeof(V) * 2 * L.nsec + 15) & ~(size_t)15));
     const int b = blockIdx.y, tid = threadIdx.x, nth = blockDim.x, nw = nth >> 5;
     const V *sv = reinterpret_cast<const V *>(L.save) + (size_t)b * 2 * L.nsec;
     for (int i = tid; i < 2 * L.nsec; i += nth) psi[i] = sv[i];
+    __syncthreads();
     for (int r = blockIdx.x; r < P.n; r += gridDim.x) {
-        const int2 sp = P.span[r];
-        if (tid < sp.y) s_rec[tid] = P.rec[sp.x + tid];
-        __syncthreads();
-        double2 acc = make_double2(0.0, 0.0);
-        s_record<false, true, false, V>(s_rec, L.nbeta, make_double2(1.0, 0.0), psi, sig, acc);
-        acc = s_warp_sum(acc);
-        const int row = reinterpret_cast<const RHead *>(s_rec)->row;
-        if ((tid & 31) == 0)
-            L.partial[((size_t)row * gridDim.y + b) * nw + (tid >> 5)] = acc;
-        __syncthreads();
+        constexpr int KP = pair_slots<V>();
+        const PHead h = p_head(P.hd + r);
+        uint2 pw[KP];
+        p_words(P, h, pw);
+        V gn, hn;
+        p_coef(P, h, gn, hn);
+        V acc = v_zero(V());
+        p_record<false, true, false, V, KP>(P, h, pw, make_double2(1.0, 0.0), gn, hn, psi, sig, acc);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc = v_add(acc, v_shfl_down(acc, o));
+        if ((tid & 31) == 0) L.partial[((size_t)h.row * gridDim.y + b) * nw + (tid >> 5)] = v_as2(acc);
     }
 }
 
