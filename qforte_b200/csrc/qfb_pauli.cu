@@ -2163,6 +2163,7 @@ static std::vector<uint64_t> sector_indices(int n, uint64_t ref) {
 
 constexpr size_t kSectorSmemMax = 200 * 1024;  // psi + sigma of one parameter set
 constexpr int kSectorThreads = 512;
+constexpr int kSectorHSlicesMax = 64;  // row slices of k_sector_h
 static int g_ucc_compact = 1;  // process-wide: use the compact evaluator when it applies
 // qfb_ucc_config 4 and 5: complex state storage even where every coefficient is real
 static bool ucc_complex_states() { return g_ucc_compact == 4 || g_ucc_compact == 5; }
@@ -2631,6 +2632,11 @@ struct qfb_ucc_s {
     int greal = 0;        // compact in global memory: real states
     int64_t nnz = 0;      // entries of the H rows on the compact sector
     std::shared_ptr<SectorRows> rows;  // compact paths: H rows on the sector
+    // compact, shared memory: k_sector_h shape (parameter sets per CTA, block
+    // size, row slices), partial energies [B][slices] and group tickets
+    int h_sets = 1, h_threads = kSectorThreads, h_slices = 1;
+    double *h_epart = nullptr;
+    unsigned *h_count = nullptr;
     qfbs::SLaunch SL{};
     void *sec = nullptr;  // uint32_t (nqubit <= 32) or uint64_t indices
     SecGroup *sgroups = nullptr;
@@ -3058,6 +3064,38 @@ static int get_sector_rows(qfb_sum_s *ham, const SectorPlan &sp, const std::vect
     return QFB_OK;
 }
 
+// The shape of k_sector_h for an evaluator: P parameter sets per CTA (as
+// many as shared memory holds, up to 4 real or 2 complex: each H row entry
+// loaded serves P gathers), the block size (1024 threads for the shapes whose
+// shared memory leaves one CTA per SM) and the row slices Q per group that minimise the estimated makespan
+// ceil(G Q / slots) (1 / Q + c) over G = ceil(B / P) groups, c being a CTA's
+// fixed cost (loading the group's psi) relative to a whole group's rows.
+static void sector_h_shape(qfb_ucc u, int nsec) {
+    const size_t elem = u->sreal ? sizeof(double) : sizeof(double2);
+    const int B = u->nbatch;
+    int P = u->sreal ? 4 : 2;
+    while (P > 1 && ((size_t)P * nsec * elem > kSectorSmemMax || P > B)) P >>= 1;
+    const size_t smem = qfbs::sector_smem_states((size_t)P, (size_t)nsec, u->sreal);
+    // 1024 threads for the shapes that hold one CTA per SM (launched so)
+    const int NT = (P == 4 || (P == 2 && !u->sreal)) ? 1024 : kSectorThreads;
+    const int cps = std::max(1, std::min(2048 / NT, (int)((227 * 1024) / (smem + 1024))));
+    const int slots = sm_count() * cps, G = (B + P - 1) / P;
+    const int qmax = std::max(1, std::min(kSectorHSlicesMax, nsec / 64));
+    int best = 1;
+    double bcost = 1e300;
+    for (int Q = 1; Q <= qmax; ++Q) {
+        const double waves = std::ceil((double)G * Q / slots);
+        const double cost = waves * (1.0 / Q + 0.01);
+        if (cost < bcost - 1e-12) {
+            bcost = cost;
+            best = Q;
+        }
+    }
+    u->h_sets = P;
+    u->h_threads = NT;
+    u->h_slices = best;
+}
+
 // Attach a compact plan and its H rows to an evaluator (shared memory or,
 // with `global`, global memory states).
 static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<SectorPlan> &plan,
@@ -3076,6 +3114,7 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
         u->sreal = (real_steps && rows->vc == nullptr) ? 1 : 0;
         rc = pair_plan(sp, u->sreal ? 16 : 8, &pairs);
         if (rc) return rc;
+        sector_h_shape(u, sp.nsec);
         u->pairs = pairs;
         u->bytes += pairs->bytes;
     }
@@ -3115,12 +3154,19 @@ static cudaError_t sector_smem_attr_v() {
     const int m = (int)kSectorSmemMax;
     cudaError_t err = cudaFuncSetAttribute(qfbs::k_sector_forward<V>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, m);
-    if (err == cudaSuccess)
-        err = cudaFuncSetAttribute(qfbs::k_sector_h<true, V>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, m);
-    if (err == cudaSuccess)
-        err = cudaFuncSetAttribute(qfbs::k_sector_h<false, V>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    auto attr = [&](const void *f) {
+        if (err == cudaSuccess) err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    };
+    if constexpr (sizeof(V) == sizeof(double)) {
+        attr((const void *)qfbs::k_sector_h<true, V, 4, 1024>);
+        attr((const void *)qfbs::k_sector_h<true, V, 2, 512>);
+        attr((const void *)qfbs::k_sector_h<true, V, 1, 512>);
+    } else {
+        attr((const void *)qfbs::k_sector_h<true, V, 2, 1024>);
+        attr((const void *)qfbs::k_sector_h<true, V, 1, 512>);
+        attr((const void *)qfbs::k_sector_h<false, V, 2, 1024>);
+        attr((const void *)qfbs::k_sector_h<false, V, 1, 512>);
+    }
     if (err == cudaSuccess)
         err = cudaFuncSetAttribute(qfbs::k_sector_sweep<V>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, m);
@@ -3156,19 +3202,27 @@ static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
                                         t_stream>>>(L);
             QFB_LAUNCHED();
             break;
-        case 2:
-            if constexpr (sizeof(V) == sizeof(double2)) {
-                if (L.val_c) {
-                    qfbs::k_sector_h<false, V><<<u->nbatch, kSectorThreads,
-                                                 qfbs::sector_smem_states(1, n, real), t_stream>>>(L);
-                    QFB_LAUNCHED();
-                    break;
-                }
+        case 2: {
+            const int P = u->h_sets, Q = u->h_slices, B = u->nbatch;
+            const unsigned grid = (unsigned)(((B + P - 1) / P) * Q);
+            const size_t smem = qfbs::sector_smem_states((size_t)P, n, real);
+#define QFB_SECTOR_H(RE, PP, NT)                                                              \
+    qfbs::k_sector_h<RE, V, PP, NT><<<grid, NT, smem, t_stream>>>(L, B, Q, u->h_epart, u->h_count)
+            if constexpr (sizeof(V) == sizeof(double)) {
+                if (P == 4) QFB_SECTOR_H(true, 4, 1024);
+                else if (P == 2) QFB_SECTOR_H(true, 2, 512);
+                else QFB_SECTOR_H(true, 1, 512);
+            } else if (L.val_c) {
+                if (P == 2) QFB_SECTOR_H(false, 2, 1024);
+                else QFB_SECTOR_H(false, 1, 512);
+            } else {
+                if (P == 2) QFB_SECTOR_H(true, 2, 1024);
+                else QFB_SECTOR_H(true, 1, 512);
             }
-            qfbs::k_sector_h<true, V><<<u->nbatch, kSectorThreads, qfbs::sector_smem_states(1, n, real),
-                                        t_stream>>>(L);
+#undef QFB_SECTOR_H
             QFB_LAUNCHED();
             break;
+        }
         case 3:
             if (!(with_grad && u->grad && u->nparam > 0)) break;
             qfbs::k_sector_sweep<V><<<u->nbatch, kSectorThreads,
@@ -3596,6 +3650,8 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
     const size_t o_sec = take(idx_bytes * std::max<size_t>(sector.size(), 1));
     const size_t o_sg = take(sizeof(SecGroup) * std::max<size_t>(sgroups.size(), 1));
     const size_t o_save = take(compact ? sizeof(double2) * 2 * (size_t)splan.nsec * B : 16);
+    const size_t o_hep = take(compact ? sizeof(double) * B * kSectorHSlicesMax : 16);
+    const size_t o_hcnt = take(compact ? sizeof(unsigned) * B : 16);
     // global-memory compact states are real doubles when H and every step are real
     bool greal = gsec && !ucc_complex_states() && stream_is_real(splan.fwd) && stream_is_real(splan.sweep);
     for (const SecGroup &g : sgroups) greal = greal && g.real;
@@ -3619,6 +3675,8 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
     u->psteps = (int2 *)(base + o_ps);
     u->nsec = compact ? (int64_t)splan.nsec : (int64_t)sector.size();
     u->SL.save = (double2 *)(base + o_save);
+    u->h_epart = (double *)(base + o_hep);
+    u->h_count = (unsigned *)(base + o_hcnt);
     if (gsec) {
         u->nsec = splan.nsec;
         u->GL.nsec = splan.nsec;

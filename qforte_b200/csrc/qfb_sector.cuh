@@ -347,14 +347,13 @@ __device__ __forceinline__ void p_run(const PStream &S, const PSmem *s_pr, V *v,
     }
 }
 
-constexpr int kRowUnroll = 8;  // H row entries in flight per lane
-
-// The evaluation runs as three kernels, one CTA per parameter set
-// (blockIdx.x) each: the forward program (psi in shared memory), sigma = H psi
-// with the energy (psi in shared memory, sigma rows straight to the save
-// buffer), and the reverse sweep (psi and sigma in shared memory).  The
-// first two hold one state and fit two CTAs per SM.  Shared memory: the
-// states, then every record's header with the cos / sin of its angle (PSmem).
+// The evaluation runs as three kernels: the forward program (one CTA per
+// parameter set, psi in shared memory), sigma = H psi with the energy (a few
+// parameter sets and a slice of the rows per CTA, sigma rows straight to the
+// save buffer), and the reverse sweep (one CTA per parameter set, psi and
+// sigma in shared memory).  Shared memory of the forward and sweep kernels:
+// the states, then every record's header with the cos / sin of its angle
+// (PSmem).
 
 template <class V>
 __global__ void __launch_bounds__(512, 2) k_sector_forward(SLaunch L) {
@@ -371,55 +370,101 @@ __global__ void __launch_bounds__(512, 2) k_sector_forward(SLaunch L) {
     for (int i = tid; i < L.nsec; i += nth) sv[i] = psi[i];
 }
 
-template <bool REAL, class V>
-__global__ void __launch_bounds__(512, 2) k_sector_h(SLaunch L) {
+// sigma = H psi and the energy, P parameter sets per CTA.  CTA x works on
+// group g = x / Q (sets g P .. g P + P - 1) and row slice q = x % Q: it loads
+// the group's psi into shared memory, streams the slice's H rows once for all
+// P sets (one warp per row, U entries in flight per lane, each entry's column
+// gathered from every set), writes the sigma rows to the save
+// buffer and one partial energy per set to epart[set][q].  The CTA that
+// completes a group last (a ticket on count[g], which it resets) sums the
+// group's partials in q order into energy, so the sum's order is fixed.
+template <bool REAL, class V, int P, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_sector_h(
+    SLaunch L, int nbatch, int Q, double *__restrict__ epart, unsigned *__restrict__ count) {
     extern __shared__ __align__(16) unsigned char s_raw[];
-    __shared__ double2 s_red[32];
-    V *psi = reinterpret_cast<V *>(s_raw);
-    const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
-    V *sv = reinterpret_cast<V *>(L.save) + (size_t)b * 2 * L.nsec;
-    for (int i = tid; i < L.nsec; i += nth) psi[i] = sv[i];
-    __syncthreads();
-    // one warp per row, kRowUnroll entries in flight per lane
-    const int lane = tid & 31, nw = nth >> 5;
-    double2 en = make_double2(0.0, 0.0);
-    for (int i = tid >> 5; i < L.nsec; i += nw) {
-        V acc = v_zero(V());
-        const int e1 = L.rowptr[i + 1];
-        for (int e0 = L.rowptr[i] + lane; e0 < e1; e0 += 32 * kRowUnroll) {
-            uint32_t c[kRowUnroll];
-            double fr[REAL ? kRowUnroll : 1];
-            double2 fc[REAL ? 1 : kRowUnroll];
+    __shared__ double s_red[NT / 32][P];
+    __shared__ unsigned s_ticket;
+    V *psi = reinterpret_cast<V *>(s_raw);  // [P][nsec]
+    const int g = blockIdx.x / Q, q = blockIdx.x - g * Q, tid = threadIdx.x;
+    const int b0 = g * P, nb = min(P, nbatch - b0), n = L.nsec;
+    V *save = reinterpret_cast<V *>(L.save);
 #pragma unroll
-            for (int u = 0; u < kRowUnroll; ++u) {
+    for (int p = 0; p < P; ++p) {
+        const V *sv = save + (size_t)(b0 + (p < nb ? p : 0)) * 2 * n;
+        for (int i = tid; i < n; i += NT) psi[p * n + i] = sv[i];
+    }
+    __syncthreads();
+    const int r0 = (int)((int64_t)q * n / Q), r1 = (int)((int64_t)(q + 1) * n / Q);
+    const int lane = tid & 31, warp = tid >> 5;
+    constexpr int U = P >= 2 ? 4 : 8;  // H row entries in flight per lane
+    double en[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) en[p] = 0.0;
+    for (int i = r0 + warp; i < r1; i += NT / 32) {
+        V acc[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[p] = v_zero(V());
+        const int e1 = L.rowptr[i + 1];
+        for (int e0 = L.rowptr[i] + lane; e0 < e1; e0 += 32 * U) {
+            uint32_t c[U];
+            double fr[REAL ? U : 1];
+            double2 fc[REAL ? 1 : U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
                 const int e = e0 + 32 * u;
                 c[u] = (e < e1) ? __ldg(&L.col[e]) : 0u;
                 if (REAL) fr[u] = (e < e1) ? __ldg(&L.val_r[e]) : 0.0;
                 else fc[REAL ? 0 : u] = (e < e1) ? __ldg(&L.val_c[e]) : make_double2(0.0, 0.0);
             }
 #pragma unroll
-            for (int u = 0; u < kRowUnroll; ++u) {
-                const V x = psi[c[u]];
-                if constexpr (REAL) {
-                    v_acc(acc, fr[u], x);
-                } else {
-                    acc = v_add(acc, v_mul(fc[REAL ? 0 : u], x));
+            for (int u = 0; u < U; ++u) {
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const V x = psi[p * n + (int)c[u]];
+                    if constexpr (REAL) {
+                        v_acc(acc[p], fr[u], x);
+                    } else {
+                        acc[p] = v_add(acc[p], v_mul(fc[REAL ? 0 : u], x));
+                    }
                 }
             }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc = v_add(acc, v_shfl_down(acc, o));
+        for (int p = 0; p < P; ++p) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[p] = v_add(acc[p], v_shfl_down(acc[p], o));
+        }
         if (lane == 0) {
-            sv[L.nsec + i] = acc;
-            en = s_cadd(en, v_cj(psi[i], acc));
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                if (p < nb) save[(size_t)(b0 + p) * 2 * n + n + i] = acc[p];
+                en[p] += v_cj(psi[p * n + i], acc[p]).x;
+            }
         }
     }
-    if (lane == 0) s_red[tid >> 5] = en;
+    if (lane == 0) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) s_red[warp][p] = en[p];
+    }
     __syncthreads();
     if (tid == 0) {
-        double2 t = make_double2(0.0, 0.0);
-        for (int k = 0; k < nw; ++k) t = s_cadd(t, s_red[k]);
-        L.energy[b] = t.x;
+        for (int p = 0; p < nb; ++p) {
+            double t = 0.0;
+            for (int k = 0; k < NT / 32; ++k) t += s_red[k][p];
+            epart[(size_t)(b0 + p) * Q + q] = t;
+        }
+        __threadfence();
+        s_ticket = atomicAdd(&count[g], 1u);
+    }
+    __syncthreads();
+    if (s_ticket == (unsigned)Q - 1u) {  // every slice of the group is in
+        __threadfence();
+        if (tid < nb) {
+            double t = 0.0;
+            for (int k = 0; k < Q; ++k) t += __ldcg(&epart[(size_t)(b0 + tid) * Q + k]);
+            L.energy[b0 + tid] = t;
+        }
+        if (tid == 0) count[g] = 0u;
     }
 }
 
