@@ -2446,7 +2446,7 @@ static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_pr
         }
     }
     if (!shared) return true;
-    const size_t ang = sizeof(qfbs::PSmem) * std::max(sp.fwd.span.size(), sp.sweep.span.size());
+    const size_t ang = sizeof(qfbs::PSmem<double2>) * std::max(sp.fwd.span.size(), sp.sweep.span.size());
     if (nsec * 2 * sizeof(double2) + ang > kSectorSmemMax) return false;
     return true;
 }
@@ -3198,7 +3198,7 @@ static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
         case 1:
             qfbs::k_sector_forward<V><<<u->nbatch, kSectorThreads,
                                         qfbs::sector_smem_states(1, n, real) +
-                                            sizeof(qfbs::PSmem) * (size_t)L.fwd.n,
+                                            sizeof(qfbs::PSmem<V>) * (size_t)L.fwd.n,
                                         t_stream>>>(L);
             QFB_LAUNCHED();
             break;
@@ -3227,7 +3227,7 @@ static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
             if (!(with_grad && u->grad && u->nparam > 0)) break;
             qfbs::k_sector_sweep<V><<<u->nbatch, kSectorThreads,
                                       qfbs::sector_smem_states(2, n, real) +
-                                          sizeof(qfbs::PSmem) * (size_t)L.sweep.n,
+                                          sizeof(qfbs::PSmem<V>) * (size_t)L.sweep.n,
                                       t_stream>>>(L);
             QFB_LAUNCHED();
             k_grad_final<<<dim3(u->nparam, u->nbatch), 128, 0, t_stream>>>(u->gpart, u->psteps,
@@ -3460,7 +3460,8 @@ static int ucc_resid_stage(qfb_ucc u) {
     if (u->compact) {
         const qfbs::SLaunch &L = u->SL;
         const size_t smem = qfbs::sector_smem_states(1, (size_t)L.nsec, u->sreal) +
-                            sizeof(qfbs::PSmem) * (size_t)u->rstream.n;
+                            (u->sreal ? sizeof(qfbs::PSmem<double>) : sizeof(qfbs::PSmem<double2>)) *
+                                (size_t)u->rstream.n;
         if (u->sreal)
             qfbs::k_sector_resid<double><<<B, kSectorThreads, smem, t_stream>>>(
                 L, u->rstream, u->ridx, u->rphase, u->nres, u->res);

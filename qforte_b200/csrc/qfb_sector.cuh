@@ -268,43 +268,66 @@ __device__ __forceinline__ void p_coef(const PStream &S, const PHead &h, V &gn, 
     if ((h.fl >> 8) == 1) p_ldcoef(S, h.c0, gn, hn);
 }
 
-// A record as the kernels keep it in shared memory: its header and the cos /
-// sin of its angle for this CTA's parameter set.
+// A record as the kernels keep it in shared memory: its header, the cos / sin
+// of its angle for this CTA's parameter set and, for a single-pattern record,
+// its coefficients.
+template <class V>
 struct PSmem {
     PHead h;
     double2 cs;
+    V gn, hn;
 };
-static_assert(sizeof(PSmem) == 48, "PSmem is three 16-byte words");
+static_assert(sizeof(PSmem<double>) == 64 && sizeof(PSmem<double2>) == 80, "PSmem layout");
 
-// Every record's header and cos / sin of sign * gamma * theta into s_pr
+// Every record's header, coefficients and cos / sin of sign * gamma * theta
+// into s_pr
+template <class V>
 __device__ __forceinline__ void p_angles(const PStream &S, const double *par, int sign,
-                                         PSmem *s_pr) {
+                                         PSmem<V> *s_pr) {
     for (int r = threadIdx.x; r < S.n; r += blockDim.x) {
         const PHead h = p_head(S.hd + r);
         double sn, cs;
         sincos((double)sign * h.gamma * par[h.param], &sn, &cs);
+        V gn, hn;
+        p_coef(S, h, gn, hn);
         s_pr[r].h = h;
         s_pr[r].cs = make_double2(cs, sn);
+        s_pr[r].gn = gn;
+        s_pr[r].hn = hn;
     }
 }
 
-// This thread's pair words and the coefficients of record h
-template <class V, int KP>
-__device__ __forceinline__ void p_fetch(const PStream &S, const PHead &h, uint2 (&pw)[KP], V &gn,
-                                        V &hn) {
-    p_words(S, h, pw);
-    p_coef(S, h, gn, hn);
+__device__ __forceinline__ double v_shfl_xor(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+__device__ __forceinline__ double2 v_shfl_xor(double2 v, int o) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
 }
 
-// Apply record r (header and angle from shared memory) with this thread's
-// prefetched words; SWEEP records carry flags (rotation of both states, inner
-// product or both) and write one partial per warp of each inner product.
+// Warp sums of two values at once: a's into lane 0, b's into lane 16 (the
+// first exchange halves the work of two separate reductions).
+template <class V>
+__device__ __forceinline__ V p_sum2(V a, V b) {
+    const bool hi = threadIdx.x & 16;
+    V k = v_add(hi ? b : a, v_shfl_xor(hi ? a : b, 16));
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) k = v_add(k, v_shfl_down(k, o));
+    return k;
+}
+template <class V>
+__device__ __forceinline__ V p_sum1(V a) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a = v_add(a, v_shfl_down(a, o));
+    return a;
+}
+
+// Apply record rec with this thread's prefetched words; returns this
+// thread's share of the record's inner product (SWEEP records carry flags:
+// rotation of both states, inner product or both).
 template <bool SWEEP, class V, int KP>
-__device__ __forceinline__ void p_step(const PStream &S, const PSmem *s_pr, int r,
-                                       const uint2 (&pw)[KP], V gn, V hn, V *v, V *w,
-                                       double2 *partial) {
-    const PHead h = s_pr[r].h;
-    const double2 csn = s_pr[r].cs;
+__device__ __forceinline__ V p_step(const PStream &S, const PSmem<V> &rec, const uint2 (&pw)[KP],
+                                    V *v, V *w) {
+    const PHead h = rec.h;
+    const double2 csn = rec.cs;
+    const V gn = rec.gn, hn = rec.hn;
     const int fl = h.fl & 255;
     V acc = v_zero(V());
     if (!SWEEP) {
@@ -316,33 +339,68 @@ __device__ __forceinline__ void p_step(const PStream &S, const PSmem *s_pr, int 
     } else {
         p_record<true, false, true, V, KP>(S, h, pw, csn, gn, hn, v, w, acc);
     }
-    if (SWEEP && (fl & R_IP)) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc = v_add(acc, v_shfl_down(acc, o));
-        if ((threadIdx.x & 31) == 0)
-            partial[((size_t)h.row * gridDim.x + blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)] =
-                v_as2(acc);
+    return acc;
+}
+
+// The warp partials of the inner products of records a and b (b < 0: none):
+// one per warp and record at partial[row][CTA][warp], zero from warps that
+// hold no pair of the record, two records reduced together where both have
+// one.
+template <class V>
+__device__ __forceinline__ void p_partials(const PSmem<V> *s_pr, int a, V acca, int b, V accb,
+                                           double2 *partial) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const PHead ha = s_pr[a].h;
+    const bool ipa = ha.fl & R_IP;
+    bool ipb = false;
+    PHead hb = ha;
+    if (b >= 0) {
+        hb = s_pr[b].h;
+        ipb = hb.fl & R_IP;
+    }
+    if (!ipa && !ipb) return;
+    const bool ida = 32 * warp >= ha.np, idb = 32 * warp >= hb.np;  // warp holds no pair
+    auto put = [&](const PHead &h, V x) {
+        partial[((size_t)h.row * gridDim.x + blockIdx.x) * nw + warp] = v_as2(x);
+    };
+    if (ipa && ipb && !ida && !idb) {
+        const V k = p_sum2(acca, accb);
+        if (lane == 0) put(ha, k);
+        if (lane == 16) put(hb, k);
+        return;
+    }
+    if (ipa) {
+        const V k = ida ? v_zero(V()) : p_sum1(acca);
+        if (lane == 0) put(ha, k);
+    }
+    if (ipb) {
+        const V k = idb ? v_zero(V()) : p_sum1(accb);
+        if (lane == 0) put(hb, k);
     }
 }
 
 // Run a stream, one barrier per record.  Two register sets alternate: while
-// record r is applied from one, the pair words and coefficients of record
-// r + 1 load into the other, so no load is waited on before its record runs.
+// record r is applied from one, the pair words of record r + 1 load into the
+// other, so no load is waited on before its record runs.  SWEEP: the inner
+// products of each two records are reduced together after the second.
 template <bool SWEEP, class V>
-__device__ __forceinline__ void p_run(const PStream &S, const PSmem *s_pr, V *v, V *w,
+__device__ __forceinline__ void p_run(const PStream &S, const PSmem<V> *s_pr, V *v, V *w,
                                       double2 *partial) {
     constexpr int KP = pair_slots<V>();
     const int n = S.n;
     uint2 wa[KP], wb[KP];
-    V ga, ha, gb, hb;
-    if (n > 0) p_fetch(S, s_pr[0].h, wa, ga, ha);
+    if (n > 0) p_words(S, s_pr[0].h, wa);
     for (int r = 0; r < n; r += 2) {
-        if (r + 1 < n) p_fetch(S, s_pr[r + 1].h, wb, gb, hb);
-        p_step<SWEEP, V, KP>(S, s_pr, r, wa, ga, ha, v, w, partial);
+        if (r + 1 < n) p_words(S, s_pr[r + 1].h, wb);
+        const V acca = p_step<SWEEP, V, KP>(S, s_pr[r], wa, v, w);
         __syncthreads();
-        if (r + 1 >= n) break;
-        if (r + 2 < n) p_fetch(S, s_pr[r + 2].h, wa, ga, ha);
-        p_step<SWEEP, V, KP>(S, s_pr, r + 1, wb, gb, hb, v, w, partial);
+        if (r + 1 >= n) {
+            if (SWEEP) p_partials(s_pr, r, acca, -1, acca, partial);
+            break;
+        }
+        if (r + 2 < n) p_words(S, s_pr[r + 2].h, wa);
+        const V accb = p_step<SWEEP, V, KP>(S, s_pr[r + 1], wb, v, w);
+        if (SWEEP) p_partials(s_pr, r, acca, r + 1, accb, partial);
         __syncthreads();
     }
 }
@@ -359,7 +417,7 @@ template <class V>
 __global__ void __launch_bounds__(512, 2) k_sector_forward(SLaunch L) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *psi = reinterpret_cast<V *>(s_raw);
-    PSmem *s_pr = reinterpret_cast<PSmem *>(s_raw + ((sizeof(V) * L.nsec + 15) & ~(size_t)15));
+    PSmem<V> *s_pr = reinterpret_cast<PSmem<V> *>(s_raw + ((sizeof(V) * L.nsec + 15) & ~(size_t)15));
     const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
     const double *par = L.params + (size_t)b * L.nparam;
     for (int i = tid; i < L.nsec; i += nth) psi[i] = i == L.ref_i ? v_one_of<V>() : v_zero(V());
@@ -397,9 +455,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_sector_h(
     const int r0 = (int)((int64_t)q * n / Q), r1 = (int)((int64_t)(q + 1) * n / Q);
     const int lane = tid & 31, warp = tid >> 5;
     constexpr int U = P >= 2 ? 4 : 8;  // H row entries in flight per lane
-    double en[P];
-#pragma unroll
-    for (int p = 0; p < P; ++p) en[p] = 0.0;
+    // after a row's reduction, lane GL p holds set p's sum (GL lanes per set)
+    constexpr int GL = 32 / P;
+    const int lp = lane / GL;
+    double en = 0.0;  // energy share of set lp (lanes lane % GL == 0)
     for (int i = r0 + warp; i < r1; i += NT / 32) {
         V acc[P];
 #pragma unroll
@@ -429,23 +488,31 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_sector_h(
                 }
             }
         }
+        // reduce-scatter: each exchange halves the values a lane carries
+        V m;
+        if constexpr (P == 4) {
+            const bool b4 = lane & 16, b3 = lane & 8;
+            const V k0 = v_add(b4 ? acc[2] : acc[0], v_shfl_xor(b4 ? acc[0] : acc[2], 16));
+            const V k1 = v_add(b4 ? acc[3] : acc[1], v_shfl_xor(b4 ? acc[1] : acc[3], 16));
+            m = v_add(b3 ? k1 : k0, v_shfl_xor(b3 ? k0 : k1, 8));
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
+            for (int o = 4; o > 0; o >>= 1) m = v_add(m, v_shfl_down(m, o));
+        } else if constexpr (P == 2) {
+            const bool b4 = lane & 16;
+            m = v_add(b4 ? acc[1] : acc[0], v_shfl_xor(b4 ? acc[0] : acc[1], 16));
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[p] = v_add(acc[p], v_shfl_down(acc[p], o));
+            for (int o = 8; o > 0; o >>= 1) m = v_add(m, v_shfl_down(m, o));
+        } else {
+            m = acc[0];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = v_add(m, v_shfl_down(m, o));
         }
-        if (lane == 0) {
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-                if (p < nb) save[(size_t)(b0 + p) * 2 * n + n + i] = acc[p];
-                en[p] += v_cj(psi[p * n + i], acc[p]).x;
-            }
+        if ((lane & (GL - 1)) == 0) {
+            if (lp < nb) save[(size_t)(b0 + lp) * 2 * n + n + i] = m;
+            en += v_cj(psi[lp * n + i], m).x;
         }
     }
-    if (lane == 0) {
-#pragma unroll
-        for (int p = 0; p < P; ++p) s_red[warp][p] = en[p];
-    }
+    if ((lane & (GL - 1)) == 0) s_red[warp][lp] = en;
     __syncthreads();
     if (tid == 0) {
         for (int p = 0; p < nb; ++p) {
@@ -472,7 +539,7 @@ template <class V>
 __global__ void __launch_bounds__(512, 2) k_sector_sweep(SLaunch L) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *psi = reinterpret_cast<V *>(s_raw), *sig = psi + L.nsec;
-    PSmem *s_pr = reinterpret_cast<PSmem *>(s_raw + ((sizeof(V) * 2 * L.nsec + 15) & ~(size_t)15));
+    PSmem<V> *s_pr = reinterpret_cast<PSmem<V> *>(s_raw + ((sizeof(V) * 2 * L.nsec + 15) & ~(size_t)15));
     const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
     const double *par = L.params + (size_t)b * L.nparam;
     const V *sv = reinterpret_cast<const V *>(L.save) + (size_t)b * 2 * L.nsec;
@@ -493,7 +560,7 @@ __global__ void __launch_bounds__(512, 2) k_sector_resid(SLaunch L, PStream R,
                                                          int nres, double *__restrict__ res) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *sig = reinterpret_cast<V *>(s_raw);
-    PSmem *s_pr = reinterpret_cast<PSmem *>(s_raw + ((sizeof(V) * L.nsec + 15) & ~(size_t)15));
+    PSmem<V> *s_pr = reinterpret_cast<PSmem<V> *>(s_raw + ((sizeof(V) * L.nsec + 15) & ~(size_t)15));
     const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
     const double *par = L.params + (size_t)b * L.nparam;
     const V *sv = reinterpret_cast<const V *>(L.save) + (size_t)b * 2 * L.nsec + L.nsec;
