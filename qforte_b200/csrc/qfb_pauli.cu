@@ -2409,6 +2409,7 @@ static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_pr
     if (sp.nalpha == 0 || sp.nbeta == 0 || sp.nalpha > 65535 || sp.nbeta > 65535) return false;
     const size_t nsec = (size_t)sp.nalpha * sp.nbeta;
     if (shared && nsec * 2 * sizeof(double2) > kSectorSmemMax) return false;
+    if (shared && nsec > (1u << qfbs::kPairIdxBits)) return false;  // pair words hold 14-bit indices
     if (nsec >= (1ull << 31)) return false;
     sp.nsec = (int)nsec;
     sp.ref_i = sp.arank[pext_parity_bits(ref, 0, n)] * sp.nbeta + sp.brank[pext_parity_bits(ref, 1, n)];
@@ -2454,9 +2455,13 @@ static bool build_sector_plan(SectorPlan &sp, const qfb_prog_s *fp, const qfb_pr
 // One kernel's pair-list records (qfbs::PStream) on the host.
 struct PairHost {
     std::vector<qfbs::PHead> hd;
-    std::vector<uint2> pair;
+    std::vector<uint32_t> pair;
     std::vector<double2> coef;  // per pattern: gn, hn
 };
+
+constexpr uint32_t kPairIdxMask = (1u << qfbs::kPairIdxBits) - 1u;
+static inline uint32_t pair_i0(uint32_t w) { return w & kPairIdxMask; }
+static inline uint32_t pair_i1(uint32_t w) { return (w >> qfbs::kPairIdxBits) & kPairIdxMask; }
 
 // Order the pairs of one record so that each run of S consecutive pairs (the
 // lanes of a half warp reading 8-byte amplitudes, S = 16, or of a quarter warp
@@ -2466,11 +2471,11 @@ struct PairHost {
 // augmenting paths, fullest slots tried first), topped up from the fullest
 // (i0 slot, i1 slot) buckets.  Only the order in which threads take the
 // record's pairs changes; the pairs of a record touch distinct amplitudes.
-static void order_pairs(uint2 *p, size_t n, int S) {
+static void order_pairs(uint32_t *p, size_t n, int S) {
     if (n <= 1) return;
-    std::vector<std::vector<uint2>> bk((size_t)S * S);
+    std::vector<std::vector<uint32_t>> bk((size_t)S * S);
     for (size_t k = 0; k < n; ++k) {
-        const uint32_t a = (p[k].x & 0x7fffffffu) % (uint32_t)S, b = (p[k].y & 0xffffffu) % (uint32_t)S;
+        const uint32_t a = pair_i0(p[k]) % (uint32_t)S, b = pair_i1(p[k]) % (uint32_t)S;
         bk[(size_t)a * S + b].push_back(p[k]);
     }
     std::vector<int> d0(S), d1(S), m1(S), ord0(S), ord1(S);
@@ -2522,10 +2527,11 @@ static void order_pairs(uint2 *p, size_t n, int S) {
 }
 
 // Append one step as a pair-list record: every pair (i0, i1) of its patterns
-// with the sign bit of (-1)^popcount(j0 & zbase) and the pattern's number.
+// with the sign bit of (-1)^popcount(j0 & zbase) and the pattern's number,
+// ordered for the banks.
 static bool push_pairs(PairHost &P, const SectorPlan &sp, const CStep &cs, int flags, int row, int S) {
     const int npat = (int)cs.pats.size();
-    if (npat > 255 || sp.nsec >= (1 << 24)) return false;
+    if (npat > qfbs::kPairPatterns || sp.nsec > (1 << qfbs::kPairIdxBits)) return false;
     qfbs::PHead h{};
     h.p0 = (int32_t)P.pair.size();
     h.c0 = (int32_t)(P.coef.size() / 2);
@@ -2537,11 +2543,13 @@ static bool push_pairs(PairHost &P, const SectorPlan &sp, const CStep &cs, int f
         const auto &pt = cs.pats[k];
         P.coef.push_back(pt.gn);
         P.coef.push_back(pt.hn);
+        const uint32_t pat = (uint32_t)k << (2 * qfbs::kPairIdxBits + 1);
         for (const qfbs::SEntry &ea : pt.a)
             for (const qfbs::SEntry &eb : pt.b) {
                 const uint32_t i0 = (uint32_t)ea.r0 * (uint32_t)sp.nbeta + eb.r0;
                 const uint32_t i1 = (uint32_t)ea.r1 * (uint32_t)sp.nbeta + eb.r1;
-                P.pair.push_back(make_uint2(i0 | ((ea.s ^ eb.s) & 1u) << 31, i1 | (uint32_t)k << 24));
+                const uint32_t neg = ((ea.s ^ eb.s) & 1u) << (2 * qfbs::kPairIdxBits);
+                P.pair.push_back(i0 | i1 << qfbs::kPairIdxBits | neg | pat);
             }
     }
     if (P.pair.size() >= (1ull << 31)) return false;
@@ -2551,28 +2559,29 @@ static bool push_pairs(PairHost &P, const SectorPlan &sp, const CStep &cs, int f
     return true;
 }
 
-// Upload one stream's headers, pairs and coefficients at base + off (256-byte
-// aligned pieces); returns the device stream.
+// Device bytes of one stream (headers, pair words, coefficients, each piece
+// 256-byte aligned), and its upload to base.
 static size_t pair_bytes(const PairHost &P) {
     auto al = [](size_t x) { return (std::max<size_t>(x, 16) + 255) & ~(size_t)255; };
-    return al(sizeof(qfbs::PHead) * P.hd.size()) + al(sizeof(uint2) * P.pair.size()) +
+    return al(sizeof(qfbs::PHead) * P.hd.size()) + al(sizeof(uint32_t) * P.pair.size()) +
            al(sizeof(double2) * P.coef.size());
 }
 static int pair_upload(const PairHost &P, char *base, qfbs::PStream &out) {
     auto al = [](size_t x) { return (std::max<size_t>(x, 16) + 255) & ~(size_t)255; };
     char *hd = base, *pr = hd + al(sizeof(qfbs::PHead) * P.hd.size());
-    char *cf = pr + al(sizeof(uint2) * P.pair.size());
+    char *cf = pr + al(sizeof(uint32_t) * P.pair.size());
     if (!P.hd.empty())
         QFB_CUDA(cudaMemcpyAsync(hd, P.hd.data(), sizeof(qfbs::PHead) * P.hd.size(),
                                  cudaMemcpyHostToDevice, t_stream));
     if (!P.pair.empty())
-        QFB_CUDA(cudaMemcpyAsync(pr, P.pair.data(), sizeof(uint2) * P.pair.size(),
+        QFB_CUDA(cudaMemcpyAsync(pr, P.pair.data(), sizeof(uint32_t) * P.pair.size(),
                                  cudaMemcpyHostToDevice, t_stream));
+
     if (!P.coef.empty())
         QFB_CUDA(cudaMemcpyAsync(cf, P.coef.data(), sizeof(double2) * P.coef.size(),
                                  cudaMemcpyHostToDevice, t_stream));
     out.hd = (const qfbs::PHead *)hd;
-    out.pair = (const uint2 *)pr;
+    out.pair = (const uint32_t *)pr;
     out.coef = (const double2 *)cf;
     out.n = (int)P.hd.size();
     return QFB_OK;

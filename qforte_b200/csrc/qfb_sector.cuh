@@ -83,10 +83,15 @@ struct PHead {
 };
 static_assert(sizeof(PHead) == 32, "PHead is two 16-byte words");
 
+// A pair word: i0 (bits 0-13) | i1 << 14 | neg << 28 | pattern << 29 (a
+// Givens-form step has at most 8 active patterns).
+constexpr int kPairIdxBits = 14;  // sector indices below 16384
+constexpr int kSweepRing = 2;     // register sets of pair words in the sweep (2 or 4)
+constexpr int kPairPatterns = 8;
 struct PStream {
     const PHead *hd;
-    const uint2 *pair;     // x = i0 | neg << 31, y = i1 | pattern << 24
-    const double2 *coef;   // per pattern: gn, hn
+    const uint32_t *pair;
+    const double2 *coef;  // per pattern: gn, hn
     int n;
 };
 
@@ -186,30 +191,32 @@ __device__ __forceinline__ PHead p_head(const PHead *p) {
     return h;
 }
 
-// Pair words of the next record held per thread: two for real amplitudes,
-// one for complex ones (whose pairs need twice the registers).
+// Pair words of a record held per thread: three for real amplitudes, two
+// for complex ones (whose pairs need twice the registers).
 template <class V>
 __host__ __device__ constexpr int pair_slots() {
-    return sizeof(V) == sizeof(double) ? 2 : 1;
+    return sizeof(V) == sizeof(double) ? 3 : 2;
 }
 
 // This thread's first KP pair words of record h (pairs tid, tid + nth, ...)
 template <int KP>
-__device__ __forceinline__ void p_words(const PStream &S, const PHead &h, uint2 (&pw)[KP]) {
+__device__ __forceinline__ void p_words(const PStream &S, const PHead &h, uint32_t (&pw)[KP]) {
 #pragma unroll
     for (int j = 0; j < KP; ++j) {
         const int k = threadIdx.x + j * blockDim.x;
-        pw[j] = k < h.np ? __ldg(S.pair + h.p0 + k) : make_uint2(0u, 0u);
+        pw[j] = k < h.np ? __ldg(S.pair + h.p0 + k) : 0u;
     }
 }
+
 
 // One pair: the share of <w|K|v> into acc and / or the rotation of v (and w
 // when TWO) by the angle whose cos / sin is (c, s).
 template <bool ROT, bool IP, bool TWO, class V>
-__device__ __forceinline__ void p_pair(uint2 pw, double c, double s, double gamma, V gn, V hn, V *v,
+__device__ __forceinline__ void p_pair(uint32_t pw, double c, double s, double gamma, V gn, V hn, V *v,
                                        V *w, V &acc) {
-    const int i0 = (int)(pw.x & 0x7fffffffu), i1 = (int)(pw.y & 0xffffffu);
-    const bool neg = pw.x >> 31;
+    constexpr uint32_t M = (1u << kPairIdxBits) - 1u;
+    const int i0 = (int)(pw & M), i1 = (int)((pw >> kPairIdxBits) & M);
+    const bool neg = (pw >> (2 * kPairIdxBits)) & 1u;
     V v0 = v[i0], v1 = v[i1];
     V w0 = v_zero(V()), w1 = w0;
     if (IP || TWO) {
@@ -247,12 +254,12 @@ __device__ __forceinline__ void p_ldcoef(const PStream &S, int k, double2 &gn, d
 // gn, hn: the coefficients of a single-pattern record (p_coef); records of
 // several patterns load each pair's from its pattern number.
 template <bool ROT, bool IP, bool TWO, class V, int KP>
-__device__ __forceinline__ void p_record(const PStream &S, const PHead &h, const uint2 (&pw)[KP],
+__device__ __forceinline__ void p_record(const PStream &S, const PHead &h, const uint32_t (&pw)[KP],
                                          double2 csn, V gn, V hn, V *v, V *w, V &acc) {
     const int tid = threadIdx.x, nth = blockDim.x;
     const bool one = (h.fl >> 8) == 1;
-    auto run = [&](uint2 p) {
-        if (!one) p_ldcoef(S, h.c0 + (int)(p.y >> 24), gn, hn);
+    auto run = [&](uint32_t p) {
+        if (!one) p_ldcoef(S, h.c0 + (int)(p >> (2 * kPairIdxBits + 1)), gn, hn);
         p_pair<ROT, IP, TWO, V>(p, csn.x, csn.y, h.gamma, gn, hn, v, w, acc);
     };
 #pragma unroll
@@ -323,7 +330,7 @@ __device__ __forceinline__ V p_sum1(V a) {
 // thread's share of the record's inner product (SWEEP records carry flags:
 // rotation of both states, inner product or both).
 template <bool SWEEP, class V, int KP>
-__device__ __forceinline__ V p_step(const PStream &S, const PSmem<V> &rec, const uint2 (&pw)[KP],
+__device__ __forceinline__ V p_step(const PStream &S, const PSmem<V> &rec, const uint32_t (&pw)[KP],
                                     V *v, V *w) {
     const PHead h = rec.h;
     const double2 csn = rec.cs;
@@ -379,28 +386,48 @@ __device__ __forceinline__ void p_partials(const PSmem<V> *s_pr, int a, V acca, 
     }
 }
 
-// Run a stream, one barrier per record.  Two register sets alternate: while
-// record r is applied from one, the pair words of record r + 1 load into the
-// other, so no load is waited on before its record runs.  SWEEP: the inner
-// products of each two records are reduced together after the second.
+// Run a stream, one barrier per record.  RING register sets rotate: while
+// record r is applied from one, the pair words of the next RING - 1 records
+// are in flight in the others (each set is refilled right after its record
+// ran), so a record's words have had RING - 1 records' time to arrive from
+// L2.  SWEEP: the inner products of records (r, r + 1) are reduced together.
 template <bool SWEEP, class V>
 __device__ __forceinline__ void p_run(const PStream &S, const PSmem<V> *s_pr, V *v, V *w,
                                       double2 *partial) {
     constexpr int KP = pair_slots<V>();
+    constexpr int RING = SWEEP ? kSweepRing : 4;
     const int n = S.n;
-    uint2 wa[KP], wb[KP];
-    if (n > 0) p_words(S, s_pr[0].h, wa);
-    for (int r = 0; r < n; r += 2) {
-        if (r + 1 < n) p_words(S, s_pr[r + 1].h, wb);
-        const V acca = p_step<SWEEP, V, KP>(S, s_pr[r], wa, v, w);
+    uint32_t w0[KP], w1[KP], w2[KP], w3[KP];
+    if (n > 0) p_words(S, s_pr[0].h, w0);
+    if (n > 1) p_words(S, s_pr[1].h, w1);
+    if (RING == 4 && n > 2) p_words(S, s_pr[2].h, w2);
+    for (int r = 0; r < n; r += RING) {
+        if (RING == 4 && r + 3 < n) p_words(S, s_pr[r + 3].h, w3);
+        const V a0 = p_step<SWEEP, V, KP>(S, s_pr[r], w0, v, w);
         __syncthreads();
         if (r + 1 >= n) {
-            if (SWEEP) p_partials(s_pr, r, acca, -1, acca, partial);
+            if (SWEEP) p_partials(s_pr, r, a0, -1, a0, partial);
             break;
         }
-        if (r + 2 < n) p_words(S, s_pr[r + 2].h, wa);
-        const V accb = p_step<SWEEP, V, KP>(S, s_pr[r + 1], wb, v, w);
-        if (SWEEP) p_partials(s_pr, r, acca, r + 1, accb, partial);
+        if (r + RING < n) p_words(S, s_pr[r + RING].h, w0);
+        const V a1 = p_step<SWEEP, V, KP>(S, s_pr[r + 1], w1, v, w);
+        if (SWEEP) p_partials(s_pr, r, a0, r + 1, a1, partial);
+        __syncthreads();
+        if (RING == 2) {
+            if (r + 3 < n) p_words(S, s_pr[r + 3].h, w1);
+            continue;
+        }
+        if (r + 2 >= n) break;
+        if (r + 5 < n) p_words(S, s_pr[r + 5].h, w1);
+        const V a2 = p_step<SWEEP, V, KP>(S, s_pr[r + 2], w2, v, w);
+        __syncthreads();
+        if (r + 3 >= n) {
+            if (SWEEP) p_partials(s_pr, r + 2, a2, -1, a2, partial);
+            break;
+        }
+        if (r + 6 < n) p_words(S, s_pr[r + 6].h, w2);
+        const V a3 = p_step<SWEEP, V, KP>(S, s_pr[r + 3], w3, v, w);
+        if (SWEEP) p_partials(s_pr, r + 2, a2, r + 3, a3, partial);
         __syncthreads();
     }
 }
@@ -594,7 +621,7 @@ __global__ void __launch_bounds__(512, 2) k_sector_pool(SLaunch L, PStream P) {
     for (int r = blockIdx.x; r < P.n; r += gridDim.x) {
         constexpr int KP = pair_slots<V>();
         const PHead h = p_head(P.hd + r);
-        uint2 pw[KP];
+        uint32_t pw[KP];
         p_words(P, h, pw);
         V gn, hn;
         p_coef(P, h, gn, hn);

@@ -559,3 +559,68 @@ def test_real_state_storage_matches_complex(cuda, norb, seed, pool_type):
         assert np.max(np.abs(res[True][2] - res[mode][2])) < 1e-11
         if pool_type == "SD":
             assert np.max(np.abs(res[True][5] - res[mode][5])) < 1e-11
+
+
+def _gated_hop(i, a, ks, w, c=1.0):
+    """T - T^dagger for T = c a^_a a_i (1 + w prod_k n_k): the strings' z-masks
+    differ on the orbitals ks off the hop, so the step has one pattern per
+    occupation of ks; with 1 + w = -1 every pattern rotates by the same angle
+    (the Givens form).  c = 1j gives commuting XX / YY strings with imaginary
+    pattern coefficients."""
+    t = qb.SQOperator()
+    K = list(ks)
+    cw = complex(c) * w
+    t.add_term(c, [a], [i])
+    t.add_term(-complex(c).conjugate(), [i], [a])
+    t.add_term(cw, [a] + K, K[::-1] + [i])
+    t.add_term(-cw.conjugate(), [i] + K, K[::-1] + [a])
+    return t
+
+
+def _pattern_problem(custom, seed):
+    mol, pool = random_problem(5, seed, "SD")
+    pool2 = qb.SQOpPool()
+    for c, op in pool.terms():
+        pool2.add_term(c, op)
+    base = len(pool2.terms())
+    for op in custom:
+        pool2.add_term(1.0, op)
+    tops = [0]
+    for k in range(len(custom)):
+        tops += [base + k, 3 + 2 * k]
+    return mol, pool2, tops
+
+
+@pytest.mark.parametrize("case", ["real", "complex"])
+def test_multi_pattern_steps_on_the_compact_path(cuda, case):
+    """Steps whose Givens form has several active patterns (hops gated by
+    number operators on other orbitals: 4 and 8 real patterns, or 4 with
+    imaginary coefficients, which the compact path keeps as complex states)
+    run on the shared-memory compact path with the pattern number in each
+    pair word: energies and gradients equal the oracle's and the full-space
+    path's."""
+    from qforte_b200.ucc import evaluator_config
+    if case == "real":
+        custom = [_gated_hop(4, 6, [0, 3], -2.0), _gated_hop(2, 8, [0, 4, 3], -2.0)]
+    else:
+        custom = [_gated_hop(5, 7, [1, 3], -2.0, 1j), _gated_hop(4, 6, [0, 3], -2.0)]
+    mol, pool2, tops = _pattern_problem(custom, 7)
+    P = np.random.default_rng(12).uniform(-0.3, 0.3, (3, len(tops)))
+    eng = DUCC(mol.hamiltonian, pool2, tops, mol.hf_reference)
+    ev = eng.evaluator(3)
+    assert ev.path == 2 and ev.real_states is (case == "real")
+    E, G = eng.energy_grad(P)
+    evaluator_config(False)
+    try:
+        eng2 = DUCC(mol.hamiltonian, pool2, tops, mol.hf_reference)
+        assert eng2.evaluator(3).path != 2
+        E2, G2 = eng2.energy_grad(P)
+    finally:
+        evaluator_config(True)
+    assert np.max(np.abs(E - E2)) < 1e-12 and np.max(np.abs(G - G2)) < 1e-11
+    hterms = oracle_terms(mol.hamiltonian)
+    kf = kops_forward(pool2, tops)
+    E_o, _ = O.energy(10, mol.hf_reference, kf, P[1], hterms)
+    g_o = O.measure_gradient(10, mol.hf_reference, kf, P[1], hterms,
+                             kops_grad=kops_gradient(pool2, tops))
+    assert abs(E[1] - E_o) < E_TOL and np.max(np.abs(G[1] - g_o)) < G_TOL
