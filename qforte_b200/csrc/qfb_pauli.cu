@@ -3205,7 +3205,7 @@ static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
     const bool real = sizeof(V) == sizeof(double);
     switch (stage) {
         case 1:
-            qfbs::k_sector_forward<V><<<u->nbatch, kSectorThreads,
+            qfbs::k_sector_forward<V><<<u->nbatch, qfbs::kStepThreads,
                                         qfbs::sector_smem_states(1, n, real) +
                                             sizeof(qfbs::PSmem<V>) * (size_t)L.fwd.n,
                                         t_stream>>>(L);
@@ -3234,7 +3234,7 @@ static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
         }
         case 3:
             if (!(with_grad && u->grad && u->nparam > 0)) break;
-            qfbs::k_sector_sweep<V><<<u->nbatch, kSectorThreads,
+            qfbs::k_sector_sweep<V><<<u->nbatch, qfbs::kSweepThreads,
                                       qfbs::sector_smem_states(2, n, real) +
                                           sizeof(qfbs::PSmem<V>) * (size_t)L.sweep.n,
                                       t_stream>>>(L);
@@ -3472,10 +3472,10 @@ static int ucc_resid_stage(qfb_ucc u) {
                             (u->sreal ? sizeof(qfbs::PSmem<double>) : sizeof(qfbs::PSmem<double2>)) *
                                 (size_t)u->rstream.n;
         if (u->sreal)
-            qfbs::k_sector_resid<double><<<B, kSectorThreads, smem, t_stream>>>(
+            qfbs::k_sector_resid<double><<<B, qfbs::kStepThreads, smem, t_stream>>>(
                 L, u->rstream, u->ridx, u->rphase, u->nres, u->res);
         else
-            qfbs::k_sector_resid<double2><<<B, kSectorThreads, smem, t_stream>>>(
+            qfbs::k_sector_resid<double2><<<B, qfbs::kStepThreads, smem, t_stream>>>(
                 L, u->rstream, u->ridx, u->rphase, u->nres, u->res);
         QFB_LAUNCHED();
         return QFB_OK;
@@ -3639,7 +3639,7 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
     u->ref = ref_index;
     u->vchunks = grid_for(u->nbasis, 256, 2);
     if (u->vchunks * (unsigned)nbatch > 65535u) u->vchunks = std::max(1u, 65535u / nbatch);
-    u->gchunks = compact ? kSectorThreads / 32
+    u->gchunks = compact ? qfbs::kSweepThreads / 32
                          : gsec ? sgrid : (gprog ? grad_chunks(gprog, nqubit, nbatch) : 1);
     const size_t B = nbatch, M = std::max(u->nparam, 1);
     const size_t nsteps = gprog ? std::max<size_t>(gprog->h_steps.size(), 1) : 1;

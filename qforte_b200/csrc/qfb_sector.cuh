@@ -87,6 +87,8 @@ static_assert(sizeof(PHead) == 32, "PHead is two 16-byte words");
 // Givens-form step has at most 8 active patterns).
 constexpr int kPairIdxBits = 14;  // sector indices below 16384
 constexpr int kSweepRing = 2;     // register sets of pair words in the sweep (2 or 4)
+constexpr int kStepThreads = 512;   // block of the forward and residual kernels
+constexpr int kSweepThreads = 256;  // block of the sweep (more pairs per thread per record)
 constexpr int kPairPatterns = 8;
 struct PStream {
     const PHead *hd;
@@ -441,7 +443,7 @@ __device__ __forceinline__ void p_run(const PStream &S, const PSmem<V> *s_pr, V 
 // (PSmem).
 
 template <class V>
-__global__ void __launch_bounds__(512, 2) k_sector_forward(SLaunch L) {
+__global__ void __launch_bounds__(kStepThreads, 1024 / kStepThreads) k_sector_forward(SLaunch L) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *psi = reinterpret_cast<V *>(s_raw);
     PSmem<V> *s_pr = reinterpret_cast<PSmem<V> *>(s_raw + ((sizeof(V) * L.nsec + 15) & ~(size_t)15));
@@ -563,7 +565,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_sector_h(
 }
 
 template <class V>
-__global__ void __launch_bounds__(512, 2) k_sector_sweep(SLaunch L) {
+__global__ void __launch_bounds__(kSweepThreads, 1024 / kSweepThreads) k_sector_sweep(SLaunch L) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     V *psi = reinterpret_cast<V *>(s_raw), *sig = psi + L.nsec;
     PSmem<V> *s_pr = reinterpret_cast<PSmem<V> *>(s_raw + ((sizeof(V) * 2 * L.nsec + 15) & ~(size_t)15));
@@ -581,7 +583,7 @@ __global__ void __launch_bounds__(512, 2) k_sector_sweep(SLaunch L) {
 // records in reverse order, angles negated), then
 // res[b][k] = Re(sigma[idx[k]] * phase[k]) (0 where idx[k] < 0).
 template <class V>
-__global__ void __launch_bounds__(512, 2) k_sector_resid(SLaunch L, PStream R,
+__global__ void __launch_bounds__(kStepThreads, 1024 / kStepThreads) k_sector_resid(SLaunch L, PStream R,
                                                          const int64_t *__restrict__ idx,
                                                          const double2 *__restrict__ phase,
                                                          int nres, double *__restrict__ res) {
