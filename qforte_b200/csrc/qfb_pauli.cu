@@ -2563,19 +2563,21 @@ static bool push_pairs(PairHost &P, const SectorPlan &sp, const CStep &cs, int f
 // 256-byte aligned), and its upload to base.
 static size_t pair_bytes(const PairHost &P) {
     auto al = [](size_t x) { return (std::max<size_t>(x, 16) + 255) & ~(size_t)255; };
-    return al(sizeof(qfbs::PHead) * P.hd.size()) + al(sizeof(uint32_t) * P.pair.size()) +
-           al(sizeof(double2) * P.coef.size());
+    return al(sizeof(qfbs::PHead) * P.hd.size()) +
+           al(sizeof(uint32_t) * (P.pair.size() + qfbs::kPairPad)) + al(sizeof(double2) * P.coef.size());
 }
 static int pair_upload(const PairHost &P, char *base, qfbs::PStream &out) {
     auto al = [](size_t x) { return (std::max<size_t>(x, 16) + 255) & ~(size_t)255; };
     char *hd = base, *pr = hd + al(sizeof(qfbs::PHead) * P.hd.size());
-    char *cf = pr + al(sizeof(uint32_t) * P.pair.size());
+    char *cf = pr + al(sizeof(uint32_t) * (P.pair.size() + qfbs::kPairPad));
     if (!P.hd.empty())
         QFB_CUDA(cudaMemcpyAsync(hd, P.hd.data(), sizeof(qfbs::PHead) * P.hd.size(),
                                  cudaMemcpyHostToDevice, t_stream));
     if (!P.pair.empty())
         QFB_CUDA(cudaMemcpyAsync(pr, P.pair.data(), sizeof(uint32_t) * P.pair.size(),
                                  cudaMemcpyHostToDevice, t_stream));
+    QFB_CUDA(cudaMemsetAsync(pr + sizeof(uint32_t) * P.pair.size(), 0,
+                             sizeof(uint32_t) * qfbs::kPairPad, t_stream));
 
     if (!P.coef.empty())
         QFB_CUDA(cudaMemcpyAsync(cf, P.coef.data(), sizeof(double2) * P.coef.size(),

@@ -200,14 +200,16 @@ __host__ __device__ constexpr int pair_slots() {
     return sizeof(V) == sizeof(double) ? 3 : 2;
 }
 
-// This thread's first KP pair words of record h (pairs tid, tid + nth, ...)
+// Words past a stream's last pair (zeros), so that the prefetch below loads
+// without a bound check (a selected value would wait for its load at once).
+constexpr int kPairPad = 4 * 1024;
+
+// This thread's first KP pair words of record h (pairs tid, tid + nth, ...);
+// words past the record are loaded but never used (p_record checks np).
 template <int KP>
 __device__ __forceinline__ void p_words(const PStream &S, const PHead &h, uint32_t (&pw)[KP]) {
 #pragma unroll
-    for (int j = 0; j < KP; ++j) {
-        const int k = threadIdx.x + j * blockDim.x;
-        pw[j] = k < h.np ? __ldg(S.pair + h.p0 + k) : 0u;
-    }
+    for (int j = 0; j < KP; ++j) pw[j] = __ldg(S.pair + h.p0 + threadIdx.x + j * blockDim.x);
 }
 
 
