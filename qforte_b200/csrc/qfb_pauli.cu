@@ -3115,17 +3115,26 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
     int rc = plan_upload(sp);
     if (rc) return rc;
     std::shared_ptr<SectorRows> rows;
-    // real states gather 8-byte amplitudes: interleave rows for 16 bank slots
     const bool real_steps = !ucc_complex_states() && stream_is_real(sp.fwd) && stream_is_real(sp.sweep);
-    rc = get_sector_rows(ham, sp, sg, u->nqubit, global ? 0 : (real_steps ? 16 : 8), global, &rows);
+    bool h_real = true;
+    for (const SecGroup &g : sg) h_real = h_real && g.real;
+    int interleave = 0;
+    if (!global) {
+        // real states: real H rows and real pair coefficients in both streams
+        u->sreal = (real_steps && h_real) ? 1 : 0;
+        sector_h_shape(u, sp.nsec);
+        // the H kernel gathers 16-byte words (complex amplitudes, or two real
+        // sets at once) by quarter warps: 8 bank slots; single real sets 16
+        interleave = (u->sreal && u->h_sets == 1) ? 16 : 8;
+    }
+    rc = get_sector_rows(ham, sp, sg, u->nqubit, interleave, global, &rows);
     if (rc) return rc;
     std::shared_ptr<PairPlanDev> pairs;
     if (!global) {
-        // real states: real H rows and real pair coefficients in both streams
-        u->sreal = (real_steps && rows->vc == nullptr) ? 1 : 0;
+        if (u->sreal != ((real_steps && rows->vc == nullptr) ? 1 : 0))
+            return fail(QFB_EINVAL, "compact sector: H rows' type differs from their groups'");
         rc = pair_plan(sp, u->sreal ? 16 : 8, &pairs);
         if (rc) return rc;
-        sector_h_shape(u, sp.nsec);
         u->pairs = pairs;
         u->bytes += pairs->bytes;
     }

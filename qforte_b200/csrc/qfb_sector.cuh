@@ -473,14 +473,28 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_sector_h(
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ double s_red[NT / 32][P];
     __shared__ unsigned s_ticket;
-    V *psi = reinterpret_cast<V *>(s_raw);  // [P][nsec]
+    // real states of an even number of sets sit in pairs, [P / 2][nsec] of
+    // double2 (sets 2h, 2h + 1): one 16-byte gather reads two sets
+    constexpr bool PAIR = REAL && sizeof(V) == sizeof(double) && P % 2 == 0;
+    V *psi = reinterpret_cast<V *>(s_raw);  // [P][nsec] unless PAIR
+    double2 *ps2 = reinterpret_cast<double2 *>(s_raw);
     const int g = blockIdx.x / Q, q = blockIdx.x - g * Q, tid = threadIdx.x;
     const int b0 = g * P, nb = min(P, nbatch - b0), n = L.nsec;
     V *save = reinterpret_cast<V *>(L.save);
+    if constexpr (PAIR) {
+        const double *sd = reinterpret_cast<const double *>(L.save);
 #pragma unroll
-    for (int p = 0; p < P; ++p) {
-        const V *sv = save + (size_t)(b0 + (p < nb ? p : 0)) * 2 * n;
-        for (int i = tid; i < n; i += NT) psi[p * n + i] = sv[i];
+        for (int h = 0; h < P / 2; ++h) {
+            const double *s0 = sd + (size_t)(b0 + (2 * h < nb ? 2 * h : 0)) * 2 * n;
+            const double *s1 = sd + (size_t)(b0 + (2 * h + 1 < nb ? 2 * h + 1 : 0)) * 2 * n;
+            for (int i = tid; i < n; i += NT) ps2[h * n + i] = make_double2(s0[i], s1[i]);
+        }
+    } else {
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const V *sv = save + (size_t)(b0 + (p < nb ? p : 0)) * 2 * n;
+            for (int i = tid; i < n; i += NT) psi[p * n + i] = sv[i];
+        }
     }
     __syncthreads();
     const int r0 = (int)((int64_t)q * n / Q), r1 = (int)((int64_t)(q + 1) * n / Q);
@@ -508,13 +522,22 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_sector_h(
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
+                if constexpr (PAIR) {
 #pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    const V x = psi[p * n + (int)c[u]];
-                    if constexpr (REAL) {
-                        v_acc(acc[p], fr[u], x);
-                    } else {
-                        acc[p] = v_add(acc[p], v_mul(fc[REAL ? 0 : u], x));
+                    for (int h = 0; h < P / 2; ++h) {
+                        const double2 x = ps2[h * n + (int)c[u]];
+                        v_acc(acc[2 * h], fr[u], x.x);
+                        v_acc(acc[2 * h + 1], fr[u], x.y);
+                    }
+                } else {
+#pragma unroll
+                    for (int p = 0; p < P; ++p) {
+                        const V x = psi[p * n + (int)c[u]];
+                        if constexpr (REAL) {
+                            v_acc(acc[p], fr[u], x);
+                        } else {
+                            acc[p] = v_add(acc[p], v_mul(fc[REAL ? 0 : u], x));
+                        }
                     }
                 }
             }
@@ -540,7 +563,14 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_sector_h(
         }
         if ((lane & (GL - 1)) == 0) {
             if (lp < nb) save[(size_t)(b0 + lp) * 2 * n + n + i] = m;
-            en += v_cj(psi[lp * n + i], m).x;
+            V pv;
+            if constexpr (PAIR) {
+                const double2 x = ps2[(lp >> 1) * n + i];
+                pv = (lp & 1) ? x.y : x.x;
+            } else {
+                pv = psi[lp * n + i];
+            }
+            en += v_cj(pv, m).x;
         }
     }
     if ((lane & (GL - 1)) == 0) s_red[warp][lp] = en;
