@@ -1062,9 +1062,11 @@ def main():
         roof["h_row_entries"] = ev.h_rows
     if compact:
         roof["real_states"] = ev.real_states
-        roof["bound_note"] = ("states live in shared memory: the binding resource is the "
-                              "L1 / shared-memory pipe (profiles/k_sector_kernels_ucc16_b256.md), "
-                              "not HBM")
+        roof["bound_note"] = ("states live in shared memory, so HBM carries only the save "
+                              "buffer and the step lists: the forward and sweep kernels are "
+                              "latency bound (one barrier per step record; L1 / shared pipe "
+                              "47-50% of peak), the H kernel L1 / shared-pipe bound (88%), per "
+                              "profiles/k_sector_kernels_ucc16_b256.md")
         if dom in l2_stream:
             roof["l2_stream_bytes_per_launch"] = l2_stream[dom]
             roof["l2_stream_gbs"] = l2_stream[dom] / (avg_ms / 1000.0) / 1e9
