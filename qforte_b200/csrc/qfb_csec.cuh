@@ -249,7 +249,8 @@ struct GTerm {  // one term of a grouped sum (layout of TermDev)
 // pair.  The group's record lists them as alpha list x beta list per
 // pattern of the determinant's bits at the group's pattern positions; the
 // kernels below add H_g psi into sigma one group per launch, so no two
-// threads of a launch touch one sigma entry.
+// threads of a launch touch one sigma entry (groups launched concurrently add
+// into separate sigma copies, summed afterwards).
 
 // sigma = f psi per row, f = sum_t c_t (-1)^popcount(det & z_t) over the
 // diagonal group's terms [t0, t1) (one warp per row, terms over the lanes);
@@ -283,6 +284,17 @@ __global__ void __launch_bounds__(256) k_cg_h_diag(GLaunch L, const uint64_t *__
         }
         for (int s = lane; s < L.B; s += 32)
             sig[(size_t)i * L.B + s] = v_mul(f, psi[(size_t)i * L.B + s]);
+    }
+}
+
+// sig[i] += sum over c < ncopies of copies[c * n + i] (in copy order)
+template <class V>
+__global__ void __launch_bounds__(256) k_cg_add_copies(V *__restrict__ sig, const V *__restrict__ copies,
+                                                       size_t n, int ncopies) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        V t = sig[i];
+        for (int c = 0; c < ncopies; ++c) t = v_add(t, copies[(size_t)c * n + i]);
+        sig[i] = t;
     }
 }
 

@@ -2164,6 +2164,7 @@ static std::vector<uint64_t> sector_indices(int n, uint64_t ref) {
 constexpr size_t kSectorSmemMax = 200 * 1024;  // psi + sigma of one parameter set
 constexpr int kSectorThreads = 512;
 constexpr int kSectorHSlicesMax = 64;  // row slices of k_sector_h
+constexpr int kHChains = 4;            // concurrent x-group chains of H without rows
 static int g_ucc_compact = 1;  // process-wide: use the compact evaluator when it applies
 // qfb_ucc_config 4 and 5: complex state storage even where every coefficient is real
 static bool ucc_complex_states() { return g_ucc_compact == 4 || g_ucc_compact == 5; }
@@ -2659,6 +2660,11 @@ struct qfb_ucc_s {
     const uint4 *g_frec = nullptr, *g_srec = nullptr;  // device copies of the record streams
     unsigned g_sgrid = 1, g_hgrid = 1, g_ygrid = 1;
     double2 *g_epart = nullptr;
+    // H without rows: the x-groups' launches run on kHChains concurrent
+    // chains, chain k adding into its own sigma copy (k = 0: GL.sig)
+    void *hblob = nullptr;  // sigma copies of chains 1..
+    cudaStream_t hside[kHChains - 1] = {};
+    cudaEvent_t hfork = nullptr, hjoin[kHChains - 1] = {};
     const int32_t *g_rowptr = nullptr;
     const uint32_t *g_col = nullptr;
     const double *g_vr = nullptr;
@@ -3143,6 +3149,19 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
     u->nnz = rows->nnz;
     u->bytes += sp.dev->bytes + rows->bytes + rows->tbytes;
     const SectorPlanDev &d = *sp.dev;
+    if (global && rows->too_big) {
+        // sigma copies and streams of the concurrent x-group chains
+        const size_t sb = (u->greal ? sizeof(double) : sizeof(double2)) * (size_t)sp.nsec * u->nbatch;
+        rc = dev_alloc(&u->hblob, sb * (kHChains - 1));
+        if (rc) return rc;
+        u->bytes += sb * (kHChains - 1);
+        cudaError_t e = cudaEventCreateWithFlags(&u->hfork, cudaEventDisableTiming);
+        for (int k = 0; k < kHChains - 1 && e == cudaSuccess; ++k) {
+            e = cudaStreamCreateWithFlags(&u->hside[k], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&u->hjoin[k], cudaEventDisableTiming);
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "sector H chains");
+    }
     if (global) {
         u->g_frec = d.frec;
         u->g_srec = d.srec;
@@ -3317,23 +3336,50 @@ static int ucc_stage_global_v(qfb_ucc u, int stage, int with_grad) {
             if (u->rows->too_big) {
                 const SectorRows &R = *u->rows;
                 const qfbg::GTerm *gt = (const qfbg::GTerm *)u->ham->d_terms;
+                const size_t ns = (size_t)L.nsec * L.B;
                 if (R.diag_t1 > R.diag_t0) {
                     qfbg::k_cg_h_diag<V><<<u->g_hgrid, 256, 0, t_stream>>>(
                         L, R.det, gt, u->ham->d_rterms, R.diag_t0, R.diag_t1, R.diag_real);
                     QFB_LAUNCHED();
                 } else {
-                    QFB_CUDA(cudaMemsetAsync(L.sig, 0, sizeof(V) * (size_t)L.nsec * L.B, t_stream));
+                    QFB_CUDA(cudaMemsetAsync(L.sig, 0, sizeof(V) * ns, t_stream));
                 }
-                for (const auto &r : R.hrecs) {
+                // chain k takes groups k, k + kHChains, ... into its own sigma
+                // copy (no two launches in flight touch one copy); the copies
+                // are added into sigma in chain order afterwards
+                V *extra = reinterpret_cast<V *>(u->hblob);
+                QFB_CUDA(cudaMemsetAsync(extra, 0, sizeof(V) * ns * (kHChains - 1), t_stream));
+                QFB_CUDA(cudaEventRecord(u->hfork, t_stream));
+                qfbg::GLaunch Lk[kHChains];
+                cudaStream_t sk[kHChains];
+                for (int k = 0; k < kHChains; ++k) {
+                    Lk[k] = L;
+                    if (k > 0) {
+                        Lk[k].sig = extra + ns * (k - 1);
+                        QFB_CUDA(cudaStreamWaitEvent(u->hside[k - 1], u->hfork, 0));
+                    }
+                    sk[k] = k ? u->hside[k - 1] : t_stream;
+                }
+                for (size_t i = 0; i < R.hrecs.size(); ++i) {
+                    const auto &r = R.hrecs[i];
+                    const int k = (int)(i % kHChains);
                     const dim3 rg(global_grid(r.pairs, L.spw), u->g_ygrid);
                     if (r.table)
-                        qfbg::k_cg_h_group<true, V><<<rg, 256, 0, t_stream>>>(
-                            L, R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
+                        qfbg::k_cg_h_group<true, V><<<rg, 256, 0, sk[k]>>>(
+                            Lk[k], R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
                     else
-                        qfbg::k_cg_h_group<false, V><<<rg, 256, 0, t_stream>>>(
-                            L, R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
+                        qfbg::k_cg_h_group<false, V><<<rg, 256, 0, sk[k]>>>(
+                            Lk[k], R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
                     QFB_LAUNCHED();
                 }
+                for (int k = 1; k < kHChains; ++k) {
+                    QFB_CUDA(cudaEventRecord(u->hjoin[k - 1], u->hside[k - 1]));
+                    QFB_CUDA(cudaStreamWaitEvent(t_stream, u->hjoin[k - 1], 0));
+                }
+                qfbg::k_cg_add_copies<V><<<(unsigned)std::min<size_t>((ns + 255) / 256, 8192), 256, 0,
+                                           t_stream>>>(reinterpret_cast<V *>(L.sig), extra, ns,
+                                                       kHChains - 1);
+                QFB_LAUNCHED();
                 qfbg::k_cg_dot<V><<<hg, 256, 0, t_stream>>>(L, u->g_epart);
             }
             else if (u->g_vc) {
@@ -3799,6 +3845,12 @@ int qfb_ucc_destroy(qfb_ucc u) {
     for (auto &x : u->exec)
         if (x) cudaGraphExecDestroy(x);
     if (u->cap_stream) cudaStreamDestroy(u->cap_stream);
+    for (auto &x : u->hside)
+        if (x) cudaStreamDestroy(x);
+    for (auto &x : u->hjoin)
+        if (x) cudaEventDestroy(x);
+    if (u->hfork) cudaEventDestroy(u->hfork);
+    dev_free(u->hblob);
     dev_free(u->blob);
     delete u;
     return QFB_OK;
