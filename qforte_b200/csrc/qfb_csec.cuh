@@ -51,10 +51,21 @@ using qfbs::v_zero;
 // group * spw + l % spw and pair sub-index l / spw.  ROT rotates psi (and
 // sigma when TWO) by sign * gamma * theta_slot; IP accumulates <sigma|K|psi>
 // per slot into partial[(row * B + s) * gridDim.x + blockIdx.x].
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization waits here for the grid before it in the stream (and its
+// memory), then lets the grid after it begin launching, so at most two grids
+// of a chain of launches are resident and the next launch's latency hides
+// behind this grid's run.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void g_pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 template <bool ROT, bool IP, bool TWO, class V>
 __global__ void __launch_bounds__(256) k_cg_step(GLaunch L, const uint4 *__restrict__ rec,
                                                  int param, int sign, int row,
                                                  double2 *__restrict__ partial) {
+    g_pdl_enter();
     V *psi = reinterpret_cast<V *>(L.psi), *sig = reinterpret_cast<V *>(L.sig);
     __shared__ double2 s_acc[8][32];
     const RHead hd = *reinterpret_cast<const RHead *>(rec);
@@ -310,6 +321,7 @@ __global__ void __launch_bounds__(256) k_cg_h_group(GLaunch L, const uint4 *__re
                                                     const GTerm *__restrict__ terms,
                                                     const double2 *__restrict__ rterms, int t0,
                                                     int t1, int real, uint64_t x) {
+    g_pdl_enter();
     const V *psi = reinterpret_cast<const V *>(L.psi);
     V *sig = reinterpret_cast<V *>(L.sig);
     const RHead hd = *reinterpret_cast<const RHead *>(rec);

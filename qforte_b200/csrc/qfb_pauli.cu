@@ -3311,6 +3311,24 @@ static unsigned global_grid(int64_t pairs, int spw) {
                                                                      (2 * per_block)));
 }
 
+// Launch with programmatic stream serialization (the kernel opens with
+// g_pdl_enter): chains of short dependent launches overlap each launch's
+// latency with the previous grid's run.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // Compact sector in global memory: stage 0 the reference, 1 the forward
 // records, 2 sigma = H psi and the energy, 3 the sweep records.
 template <class V>
@@ -3326,8 +3344,9 @@ static int ucc_stage_global_v(qfb_ucc u, int stage, int with_grad) {
             break;
         case 1:
             for (size_t r = 0; r < sp.fwd.span.size(); ++r) {
-                qfbg::k_cg_step<true, false, false, V><<<grid, 256, 0, t_stream>>>(
-                    L, u->g_frec + sp.fwd.span[r].x, sp.fwd.param[r], 1, -1, nullptr);
+                QFB_CUDA(launch_pdl(qfbg::k_cg_step<true, false, false, V>, grid, dim3(256), t_stream, L,
+                                    u->g_frec + sp.fwd.span[r].x, sp.fwd.param[r], 1, -1,
+                                    (double2 *)nullptr));
                 QFB_LAUNCHED();
             }
             break;
@@ -3364,12 +3383,13 @@ static int ucc_stage_global_v(qfb_ucc u, int stage, int with_grad) {
                     const auto &r = R.hrecs[i];
                     const int k = (int)(i % kHChains);
                     const dim3 rg(global_grid(r.pairs, L.spw), u->g_ygrid);
+                    const uint4 *rec = R.d_hrec + r.span.x;
                     if (r.table)
-                        qfbg::k_cg_h_group<true, V><<<rg, 256, 0, sk[k]>>>(
-                            Lk[k], R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
+                        QFB_CUDA(launch_pdl(qfbg::k_cg_h_group<true, V>, rg, dim3(256), sk[k], Lk[k], rec,
+                                            R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x));
                     else
-                        qfbg::k_cg_h_group<false, V><<<rg, 256, 0, sk[k]>>>(
-                            Lk[k], R.d_hrec + r.span.x, R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x);
+                        QFB_CUDA(launch_pdl(qfbg::k_cg_h_group<false, V>, rg, dim3(256), sk[k], Lk[k], rec,
+                                            R.det, gt, u->ham->d_rterms, r.t0, r.t1, r.real, r.x));
                     QFB_LAUNCHED();
                 }
                 for (int k = 1; k < kHChains; ++k) {
@@ -3405,14 +3425,14 @@ static int ucc_stage_global_v(qfb_ucc u, int stage, int with_grad) {
                 const uint4 *rec = u->g_srec + sp.sweep.span[r].x;
                 const int par = sp.sweep.param[r];
                 if (fl == (qfbs::R_ROT | qfbs::R_IP | qfbs::R_TWO))
-                    qfbg::k_cg_step<true, true, true, V><<<grid, 256, 0, t_stream>>>(L, rec, par, -1, hd.row,
-                                                                                 u->gpart);
+                    QFB_CUDA(launch_pdl(qfbg::k_cg_step<true, true, true, V>, grid, dim3(256), t_stream, L,
+                                        rec, par, -1, (int)hd.row, u->gpart));
                 else if (fl == qfbs::R_IP)
-                    qfbg::k_cg_step<false, true, false, V><<<grid, 256, 0, t_stream>>>(L, rec, par, -1,
-                                                                                   hd.row, u->gpart);
+                    QFB_CUDA(launch_pdl(qfbg::k_cg_step<false, true, false, V>, grid, dim3(256), t_stream,
+                                        L, rec, par, -1, (int)hd.row, u->gpart));
                 else
-                    qfbg::k_cg_step<true, false, true, V><<<grid, 256, 0, t_stream>>>(L, rec, par, -1, -1,
-                                                                                  nullptr);
+                    QFB_CUDA(launch_pdl(qfbg::k_cg_step<true, false, true, V>, grid, dim3(256), t_stream, L,
+                                        rec, par, -1, -1, (double2 *)nullptr));
                 QFB_LAUNCHED();
             }
             k_grad_final<<<dim3(u->nparam, L.B), 128, 0, t_stream>>>(u->gpart, u->psteps, u->gchunks,
