@@ -1,5 +1,5 @@
 """GPU parity: the libqfb.so kernels against the oracle and the reference's
-golden vectors.  Tolerances (from the north-star contract): amplitudes 1e-12
+golden vectors.  Tolerances: amplitudes 1e-12
 max-abs, energies 1e-10, gradients 1e-8; basis-index work bit-exact."""
 
 import math
