@@ -839,6 +839,23 @@ __global__ void k_grad_final(const double2 *__restrict__ partial, const int2 *__
     if (threadIdx.x == 0) grad[(uint64_t)b * M + mu] = 2.0 * acc.x;
 }
 
+// The same for few partials per step row (chunks <= 32): one thread per
+// gradient entry, parameters fastest (coalesced writes), the partials summed
+// in row and chunk order.
+__global__ void k_grad_final_few(const double2 *__restrict__ partial, const int2 *__restrict__ psteps,
+                                 int chunks, int M, int B, double *__restrict__ grad) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)M * B) return;
+    const int mu = (int)(t % M), b = (int)(t / M);
+    const int2 r = psteps[mu];
+    double acc = 0.0;
+    for (int s = r.x; s < r.y; ++s) {
+        const double2 *p = partial + ((uint64_t)s * B + b) * chunks;
+        for (int c = 0; c < chunks; ++c) acc += p[c].x;
+    }
+    grad[(uint64_t)b * M + mu] = 2.0 * acc;
+}
+
 __global__ void k_set_ref(double2 *__restrict__ psi, uint64_t nbasis, uint64_t ref, int nbatch) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b < nbatch) psi[(uint64_t)b * nbasis + ref] = make_double2(1.0, 0.0);
@@ -3269,8 +3286,11 @@ static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
                                           sizeof(qfbs::PSmem<V>) * (size_t)L.sweep.n,
                                       t_stream>>>(L);
             QFB_LAUNCHED();
-            k_grad_final<<<dim3(u->nparam, u->nbatch), 128, 0, t_stream>>>(u->gpart, u->psteps,
-                                                                         u->gchunks, u->gradv);
+            {
+                const int64_t n = (int64_t)u->nparam * u->nbatch;
+                k_grad_final_few<<<(unsigned)((n + 255) / 256), 256, 0, t_stream>>>(
+                    u->gpart, u->psteps, (int)u->gchunks, u->nparam, u->nbatch, u->gradv);
+            }
             QFB_LAUNCHED();
             break;
         default:
@@ -3532,7 +3552,11 @@ static int ucc_pool_stage(qfb_ucc u) {
                                               u->pool->d_tab, u->ppart);
         QFB_LAUNCHED();
     }
-    k_grad_final<<<dim3(u->npool, B), 128, 0, t_stream>>>(u->ppart, u->pranges, chunks, u->pgrad);
+    if (chunks <= 32)
+        k_grad_final_few<<<(unsigned)(((int64_t)u->npool * B + 255) / 256), 256, 0, t_stream>>>(
+            u->ppart, u->pranges, (int)chunks, u->npool, B, u->pgrad);
+    else
+        k_grad_final<<<dim3(u->npool, B), 128, 0, t_stream>>>(u->ppart, u->pranges, chunks, u->pgrad);
     QFB_LAUNCHED();
     return QFB_OK;
 }
