@@ -89,6 +89,30 @@ def problem(norb, seed):
     return mol, pool
 
 
+def replica_parameters(seed, rank, batch, nparam):
+    """One replica's parameter rows: amplitudes U(-0.1, 0.1), seeded per rank so
+    every replica evaluates its own batch."""
+    return np.random.default_rng(seed + 1 + rank).uniform(-0.1, 0.1, (batch, nparam))
+
+
+def max_over_ranks(x, world, device):
+    """The largest of every rank's x (a device-timed duration): the job ends
+    when its slowest replica does.  One all-reduce, taken by every rank."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, batch, ms_max):
+    """Evaluations per second over all replicas: each rank evaluates `batch`
+    sets per step and the step lasts as long as the slowest rank's."""
+    return world * batch / (ms_max / 1000.0)
+
+
 def workload_config(a, nterms, nparam):
     return {"workload": f"batched dUCCSD energy + adjoint gradient, {2 * a.norb} qubits "
                         f"({a.norb} orbitals, {a.norb} electrons), {nparam} SD parameters, "
@@ -904,8 +928,7 @@ def main():
         evaluator_config(False)
     eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
     ev = eng.evaluator(a.batch)
-    rng = np.random.default_rng(a.seed + 1 + rank)
-    P = rng.uniform(-0.1, 0.1, (a.batch, M))
+    P = replica_parameters(a.seed, rank, a.batch, M)
     d_params, d_energy, d_grad = ev.tensors()
     d_params.copy_(torch.from_numpy(P))
     stream = torch.cuda.current_stream()
@@ -942,12 +965,8 @@ def main():
     ck = clocks.stop()
     if ck is not None:
         ck["window"] = "timed region plus untimed steps of the same workload to 0.8 s"
-    ms_all = ms
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_all = float(t.item())
-    value = world * a.batch / (ms_all / 1000.0)
+    ms_all = max_over_ranks(ms, world, "cuda")
+    value = whole_job_rate(world, a.batch, ms_all)
 
     # ---- end to end through the public API with host buffers ---------------
     hP = torch.from_numpy(P).pin_memory()
@@ -966,12 +985,8 @@ def main():
         stream.synchronize()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1) / a.steps
-    if world > 1:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e = world * a.batch / (ms_e2e / 1000.0)
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / a.steps, world, "cuda")
+    e2e = whole_job_rate(world, a.batch, ms_e2e)
     # the numbers coming back are the evaluator's
     assert np.all(np.isfinite(hE.numpy())) and np.all(np.isfinite(hG.numpy()))
 
