@@ -320,10 +320,59 @@ def integrals_fixture(path, out):
     print(f"{out}: {len(oei)} one-body, {len(tei)} two-body integrals")
 
 
+def _h2_qite_system(test_file):
+    """The H2/STO-3G qubit Hamiltonian, reference determinant and FCI energy of
+    the reference's QITE test (tests/test_qite.py:6-59), read from its source."""
+    import ast
+    tree = ast.parse(open(test_file).read())
+    found = {}
+    for node in ast.walk(tree):
+        if isinstance(node, ast.Assign) and isinstance(node.targets[0], ast.Name):
+            name = node.targets[0].id
+            if name in ("E_fci", "coef_vec", "ref"):
+                found[name] = ast.literal_eval(node.value)
+            elif name == "circ_vec":
+                found[name] = [c.args[0].value if c.args else "" for c in node.value.elts]
+    return found
+
+
+def qite_fixture(qf, test_file, norb, seed, out):
+    """QITE (ite/qite.py) run by the reference: the H2 case of its own test
+    (beta = 18, Lanczos every 49 steps), the same H2 with the dense cqoy
+    expansion, and a seeded random-integral system with the sparse SD one."""
+    h2 = _h2_qite_system(test_file)
+    H = qf.QubitOperator()
+    for c, s in zip(h2["coef_vec"], h2["circ_vec"]):
+        H.add(c, qf.build_circuit(s) if s else qf.Circuit())
+    mol = qf.Molecule()
+    mol.hamiltonian = H
+    alg = qf.QITE(mol, reference=h2["ref"])
+    alg.run(beta=18.0, do_lanczos=True, lanczos_gap=49)
+    res = {"h2_coeffs": np.array(h2["coef_vec"]), "h2_circs": np.array(h2["circ_vec"]),
+           "h2_ref": np.array(h2["ref"]), "h2_efci": h2["E_fci"],
+           "h2_ekb": np.array(alg._Ekb), "h2_lanczos": complex(alg._Egs_lanczos)}
+    h, g = random_integrals(norb, seed)
+    Hq = ref_sq_ham(qf, h, g).jw_transform()
+    s = _Sys()
+    s.hamiltonian = Hq
+    s.hf_reference = hf_reference(norb, norb)
+    s.hf_energy = 0.0
+    alg = qf.QITE(s)
+    alg.run(beta=0.6, db=0.2, expansion_type="SD", sparseSb=True)
+    res["rand_sd_ekb"] = np.array(alg._Ekb)
+    res["rand_sd_nparams"] = alg._n_classical_params
+    alg = qf.QITE(mol, reference=h2["ref"])
+    alg.run(beta=0.6, db=0.2, expansion_type="cqoy", sparseSb=False)
+    res["h2_cqoy_ekb"] = np.array(alg._Ekb)
+    res["h2_cqoy_nparams"] = alg._n_classical_params
+    np.savez_compressed(out, norb=norb, seed=seed, **res)
+    print(f"{out}: H2 QITE E = {res['h2_ekb'][-1]}, random SD E = {res['rand_sd_ekb'][-1]}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-src", default="/root/reference/src/qforte")
-    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact)")
+    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact, qite)")
     a = ap.parse_args()
     qf = O.load_reference(a.ref_src)
     tests_dir = os.path.join(os.path.dirname(a.ref_src.rstrip("/")), "..", "tests")
@@ -332,6 +381,9 @@ def main():
     if a.only in ("pqe", None):
         pqe_fixture(qf, 4, 11, os.path.join(HERE, "pqe_norb4_seed11.npz"))
         pqe_fixture(qf, 6, 11, os.path.join(HERE, "pqe_norb6_seed11.npz"))
+    if a.only in ("qite", None):
+        qite_fixture(qf, os.path.join(tests_dir, "test_qite.py"), 3, 11,
+                     os.path.join(HERE, "qite_norb3_seed11.npz"))
     if a.only is not None:
         return
     ucc_fixture(qf, 4, 11, os.path.join(HERE, "ucc_norb4_seed11.npz"))

@@ -1,0 +1,202 @@
+"""QITE's host logic on CPU, against the reference's own QITE runs.
+
+qforte_b200.qite keeps psi in HBM and forms QITE's b vector and S matrix as
+grouped expectation values (Pauli products with power-of-i phases, one result
+segment per element).  Here the driver runs unchanged except that the state is
+a host vector driven by the oracle's C restatement of the reference Computer,
+and the grouped expectation values are summed term by term with numpy.  So these
+tests check the expansion pool, the product terms and their phases, the
+thresholds, the least-squares step, the Trotter circuit and the Lanczos
+step against tests/golden/qite_norb3_seed11.npz, which the reference's QITE wrote
+(ite/qite.py, tests/test_qite.py:6-81).  The GPU tests run the same cases on
+the device.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+E_TOL = 1e-10
+
+
+def _gates(circ):
+    return [(g.target(), g.control(), g.matrix()) for g in circ.gates()]
+
+
+class HostComputer:
+    """A host state with the Computer methods QITE calls (test stand-in)."""
+
+    def __init__(self, n):
+        from oracle import oracle as O
+        if isinstance(n, HostComputer):
+            self.n, self.s = n.n, n.s.copy()
+        else:
+            self.n, self.s = int(n), O.State(int(n))
+
+    def _check_qubits(self, m):
+        assert m <= self.n
+
+    def apply_circuit(self, circ):
+        self.s.apply_gates(_gates(circ))
+
+    def apply_operator(self, qo):
+        self.s.apply_operator([(c, _gates(circ)) for c, circ in qo.terms()])
+
+    def direct_op_exp_val(self, qo):
+        t = HostComputer(self)
+        t.apply_operator(qo)
+        return self.s.dot(t.s)
+
+
+def host_segment_expvals(bra, ket, terms, segments, nsegment):
+    """out[g] = sum of c <bra| P(x, z) |ket> over segment g's terms, with
+    P(x, z) |i> = i^{|x & z|} (-1)^{|i & z|} |i ^ x>."""
+    N = 1 << bra.n
+    idx = np.arange(N, dtype=np.uint64)
+    out = np.zeros(nsegment, dtype=np.complex128)
+    for (c, x, z), g in zip(terms, segments):
+        x, z = np.uint64(x), np.uint64(z)
+        sign = 1 - 2 * (np.bitwise_count(idx & z).astype(np.int64) & 1)
+        v = np.zeros(N, dtype=np.complex128)
+        v[idx ^ x] = (1j ** int(np.bitwise_count(x & z))) * sign * ket.s.psi
+        out[g] += c * np.vdot(bra.s.psi, v)
+    return out
+
+
+@pytest.fixture
+def host_qite(monkeypatch):
+    from qforte_b200 import qite
+    monkeypatch.setattr(qite, "Computer", HostComputer)
+    monkeypatch.setattr(qite, "inner_product", lambda a, b: a.s.dot(b.s))
+    monkeypatch.setattr(qite, "_segment_expvals", host_segment_expvals)
+    return qite
+
+
+class _System:
+    pass
+
+
+def h2_system(d):
+    import qforte_b200 as qb
+    H = qb.QubitOperator()
+    for c, s in zip(d["h2_coeffs"], d["h2_circs"]):
+        H.add(float(c), qb.build_circuit(str(s)))
+    s = _System()
+    s.hamiltonian = H
+    s.hf_reference = [int(v) for v in d["h2_ref"]]
+    return s
+
+
+def random_system(d):
+    import qforte_b200 as qb
+    mol = qb.random_molecule(int(d["norb"]), int(d["norb"]), int(d["seed"]))
+    s = _System()
+    s.hamiltonian = mol.hamiltonian
+    s.hf_reference = mol.hf_reference
+    return s
+
+
+# After its first step the random system's S has 25 of 40 singular values
+# below 1e-10 of the largest, at the least-squares rank cutoff (~7e-14): adding
+# symmetric noise of 1e-16 to S moves the reference's own next energy by up to
+# 5e-8.  Its first step is pinned at E_TOL, later steps at this bound.
+ILL_POSED_TOL = 1e-6
+
+
+def run_cases(qite, d):
+    """The fixture's reference runs; returns (name, ours, golden, tolerance)."""
+    out = []
+    alg = qite.QITE(h2_system(d))
+    alg.run(beta=18.0, do_lanczos=True, lanczos_gap=49)
+    out.append(("H2 sparse SD, beta 18", np.array(alg._Ekb), d["h2_ekb"], E_TOL))
+    out.append(("H2 Lanczos", np.array([np.real(alg._Egs_lanczos)]),
+                np.array([np.real(d["h2_lanczos"])]), E_TOL))
+    assert abs(alg.get_gs_energy() - float(d["h2_efci"])) < E_TOL
+    alg = qite.QITE(h2_system(d))
+    alg.run(beta=0.6, db=0.2, expansion_type="cqoy", sparseSb=False)
+    assert alg._n_classical_params == int(d["h2_cqoy_nparams"])
+    out.append(("H2 dense cqoy", np.array(alg._Ekb), d["h2_cqoy_ekb"], E_TOL))
+    alg = qite.QITE(random_system(d))
+    alg.run(beta=0.6, db=0.2, expansion_type="SD", sparseSb=True)
+    assert alg._n_classical_params == int(d["rand_sd_nparams"])
+    ekb = np.array(alg._Ekb)
+    out.append(("random 6 q sparse SD, first step", ekb[:2], d["rand_sd_ekb"][:2], E_TOL))
+    out.append(("random 6 q sparse SD, later steps", ekb, d["rand_sd_ekb"], ILL_POSED_TOL))
+    return out
+
+
+def test_qite_host_replay_matches_reference(host_qite):
+    d = golden("qite_norb3_seed11.npz")
+    for name, ours, ref, tol in run_cases(host_qite, d):
+        assert ours.shape == ref.shape, name
+        assert np.max(np.abs(ours - ref)) < tol, (name, np.max(np.abs(ours - ref)))
+
+
+def test_S_products_equal_dense_overlaps(host_qite):
+    """S_IJ from Pauli products == Re <sigma_I psi | sigma_J psi> formed by
+    applying each operator to a random state; b likewise."""
+    import qforte_b200 as qb
+    from oracle import oracle as O
+    rng = np.random.default_rng(3)
+    n = 4
+    qc = HostComputer(n)
+    psi = rng.normal(size=16) + 1j * rng.normal(size=16)
+    qc.s = O.State(n, psi / np.linalg.norm(psi))
+    ops = []
+    for s, c in (("Y_0 X_1", 1.0), ("X_0 Y_1 Z_3", 0.5j), ("Z_2 Y_3", -0.25), ("Y_1", 1.0)):
+        op = qb.QubitOperator()
+        op.add(c, qb.build_circuit(s))
+        ops.append(op)
+    S = host_qite.qite_S(qc, ops)
+    vecs = []
+    for op in ops:
+        t = HostComputer(qc)
+        t.apply_operator(op)
+        vecs.append(t.s.psi)
+    for i in range(len(ops)):
+        for j in range(len(ops)):
+            want = 1.0 if i == j else np.real(np.vdot(vecs[i], vecs[j]))
+            assert abs(S[i, j] - want) < 1e-14
+    H = qb.QubitOperator()
+    H.add(0.3, qb.build_circuit("Z_0 Z_1"))
+    H.add(-0.7, qb.build_circuit("X_2 X_3"))
+    b = host_qite.qite_b(qc, H, ops, [1.0, 2.0, 1.0, 1.0], 0.2, -0.5)
+    hp = HostComputer(qc)
+    hp.apply_operator(H)
+    for i, op in enumerate(ops):
+        t = HostComputer(hp)
+        t.apply_operator(op)
+        c = [1.0, 2.0, 1.0, 1.0][i]
+        want = np.real(-1j / np.sqrt(1 + 0.2) * c * np.vdot(qc.s.psi, t.s.psi))
+        assert abs(b[i] - want) < 1e-14
+
+
+def test_canonical_geig_solve_matches_reference(ref_qforte):
+    from qforte.maths.eigsolve import canonical_geig_solve as ref_solve
+
+    from qforte_b200.qite import canonical_geig_solve
+    rng = np.random.default_rng(5)
+    V = rng.normal(size=(5, 3)) + 1j * rng.normal(size=(5, 3))
+    S = V.conj().T @ V
+    A = rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3))
+    Hm = A + A.conj().T
+    e1, _ = canonical_geig_solve(S, Hm, sort_ret_vals=True)
+    e2, _ = ref_solve(S, Hm, sort_ret_vals=True)
+    assert np.max(np.abs(np.real(e1) - np.real(e2))) < 1e-12
+    assert np.all(np.diff(np.real(e1)) >= 0)
+
+
+def test_segment_runs_split_on_segment_boundaries():
+    from qforte_b200.qite import _segment_runs
+    seg = [0, 0, 1, 2, 2, 2, 3, 4, 4]
+    runs = _segment_runs(seg, limit=4)
+    assert runs == [(0, 3), (3, 7), (7, 9)]
+    # every term lands in exactly one run, no segment is cut
+    assert [i for lo, hi in runs for i in range(lo, hi)] == list(range(len(seg)))
+    for lo, hi in runs:
+        assert hi - lo <= 4 and (hi == len(seg) or seg[hi] != seg[hi - 1])
+    assert _segment_runs(seg, limit=100) == [(0, 9)]
+    assert _segment_runs([], limit=4) == []
+    with pytest.raises(ValueError):
+        _segment_runs([0, 0, 0, 0, 0], limit=4)
