@@ -320,9 +320,11 @@ def integrals_fixture(path, out):
     print(f"{out}: {len(oei)} one-body, {len(tei)} two-body integrals")
 
 
-def _h2_qite_system(test_file):
-    """The H2/STO-3G qubit Hamiltonian, reference determinant and FCI energy of
-    the reference's QITE test (tests/test_qite.py:6-59), read from its source."""
+def _test_qubit_system(test_file):
+    """The qubit Hamiltonian (coef_vec, circ_vec), reference determinant and FCI
+    energy that one of the reference's algorithm tests builds, read from its
+    source (tests/test_qite.py:6-59: H2/STO-3G; tests/test_fast_qk.py:9-392:
+    H4/STO-6G)."""
     import ast
     tree = ast.parse(open(test_file).read())
     found = {}
@@ -340,7 +342,7 @@ def qite_fixture(qf, test_file, norb, seed, out):
     """QITE (ite/qite.py) run by the reference: the H2 case of its own test
     (beta = 18, Lanczos every 49 steps), the same H2 with the dense cqoy
     expansion, and a seeded random-integral system with the sparse SD one."""
-    h2 = _h2_qite_system(test_file)
+    h2 = _test_qubit_system(test_file)
     H = qf.QubitOperator()
     for c, s in zip(h2["coef_vec"], h2["circ_vec"]):
         H.add(c, qf.build_circuit(s) if s else qf.Circuit())
@@ -369,10 +371,40 @@ def qite_fixture(qf, test_file, norb, seed, out):
     print(f"{out}: H2 QITE E = {res['h2_ekb'][-1]}, random SD E = {res['rand_sd_ekb'][-1]}")
 
 
+def srqk_fixture(qf, test_file, norb, seed, out):
+    """SRQK (qkd/srqk.py:103-204 with abc/qsdabc.py:87-115) run by the
+    reference: the H4 case of its own test (trotter_number = 100, s = 6) and a
+    seeded random-integral system (s = 3, dt = 0.5, one Trotter step)."""
+    h4 = _test_qubit_system(test_file)
+    H = qf.QubitOperator()
+    for c, s in zip(h4["coef_vec"], h4["circ_vec"]):
+        H.add(c, qf.build_circuit(s) if s else qf.Circuit())
+    mol = qf.Molecule()
+    mol.hamiltonian = H
+    alg = qf.SRQK(mol, reference=h4["ref"], trotter_number=100)
+    alg.run(s=6)
+    res = {"h4_coeffs": np.array(h4["coef_vec"]), "h4_circs": np.array(h4["circ_vec"]),
+           "h4_ref": np.array(h4["ref"]), "h4_efci": h4["E_fci"], "h4_S": alg._S,
+           "h4_H": alg._Hbar, "h4_evals": np.array(alg._eigenvalues), "h4_egs": alg._Egs}
+    h, g = random_integrals(norb, seed)
+    s = _Sys()
+    s.hamiltonian = ref_sq_ham(qf, h, g).jw_transform()
+    s.hf_reference = hf_reference(norb, norb)
+    s.hf_energy = 0.0
+    alg = qf.SRQK(s)
+    alg.run(s=3, dt=0.5)
+    res.update({"rand_S": alg._S, "rand_H": alg._Hbar,
+                "rand_evals": np.array(alg._eigenvalues), "rand_egs": alg._Egs})
+    np.savez_compressed(out, norb=norb, seed=seed, **res)
+    print(f"{out}: H4 SRQK E = {res['h4_egs']} (FCI {h4['E_fci']}), cond S = "
+          f"{np.linalg.cond(res['h4_S']):.2e}; random E = {res['rand_egs']}, cond S = "
+          f"{np.linalg.cond(res['rand_S']):.2e}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-src", default="/root/reference/src/qforte")
-    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact, qite)")
+    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact, qite, srqk)")
     a = ap.parse_args()
     qf = O.load_reference(a.ref_src)
     tests_dir = os.path.join(os.path.dirname(a.ref_src.rstrip("/")), "..", "tests")
@@ -384,6 +416,9 @@ def main():
     if a.only in ("qite", None):
         qite_fixture(qf, os.path.join(tests_dir, "test_qite.py"), 3, 11,
                      os.path.join(HERE, "qite_norb3_seed11.npz"))
+    if a.only in ("srqk", None):
+        srqk_fixture(qf, os.path.join(tests_dir, "test_fast_qk.py"), 3, 11,
+                     os.path.join(HERE, "srqk_norb3_seed11.npz"))
     if a.only is not None:
         return
     ucc_fixture(qf, 4, 11, os.path.join(HERE, "ucc_norb4_seed11.npz"))

@@ -25,7 +25,7 @@ def _gates(circ):
 
 
 class HostComputer:
-    """A host state with the Computer methods QITE calls (test stand-in)."""
+    """A host state with the Computer methods QITE and SRQK call (test stand-in)."""
 
     def __init__(self, n):
         from oracle import oracle as O
@@ -42,6 +42,9 @@ class HostComputer:
 
     def apply_operator(self, qo):
         self.s.apply_operator([(c, _gates(circ)) for c, circ in qo.terms()])
+
+    def apply_constant(self, a):
+        self.s.apply_constant(a)
 
     def direct_op_exp_val(self, qo):
         t = HostComputer(self)
