@@ -1,8 +1,9 @@
-"""Single-reference quantum Krylov diagonalisation (SRQK) on the device state.
+"""Single-reference quantum Krylov diagonalisation (SRQK, NTSRQK) on the device state.
 
 Follows ``qkd/srqk.py``: ``SRQK.run`` (:46-61) and ``build_qk_mats_fast``
-(:103-204), with the generalised eigenproblem of ``abc/qsdabc.py:common_run``
-(:87-115).
+(:103-204); ``qkd/nt_srqk.py`` (``NTSRQK``: the basis from exact time
+evolution, ``utils/exp_ops.py``); and the generalised eigenproblem of
+``abc/qsdabc.py:common_run`` (:87-115).
 
 The Krylov basis is omega_m = U_m |Phi>, U_m the reference's circuit for
 exp(-i m dt H) (``trotterize`` with the run's Trotter number, then the global
@@ -15,14 +16,57 @@ device inner products (``qfb_vdot``): only the (s+1)^2 matrix elements reach
 the host.
 """
 
+import math
+
 import numpy as np
 
+from ._lib import check, cplx, lib
 from .circuit import Circuit
 from .computer import Computer, inner_product
 from .qite import canonical_geig_solve
 from .utils import build_refprep, trotterize
 
-__all__ = ["SRQK", "fill_krylov_row"]
+__all__ = ["SRQK", "NTSRQK", "evolve_exact", "fill_krylov_row"]
+
+
+def _axpy(dst, a, src):
+    """dst += a * src on the device (qfb_axpy)."""
+    check(lib().qfb_axpy(dst._h, cplx(a), src._h), "axpy")
+
+
+def _norm1(hamiltonian):
+    """Sum of |c| over the terms: a bound on the spectral norm of H."""
+    return sum(abs(complex(c)) for c, _ in hamiltonian.terms())
+
+
+def evolve_exact(qc, hamiltonian, t, max_order=60):
+    """A new Computer holding exp(-i t H) psi (psi = qc's state, left as it
+    is), by a scaled Taylor series on the device: t is cut into substeps with
+    |t| sum|c| / nsub <= 1/2, and in each substep the terms (-i h H)^k / k! psi
+    (one qfb_sum_apply each) are added until two in a row fall below 2^-53 of
+    the sum's norm.  Stands in for scipy's expm_multiply on the sparse matrix
+    of H (utils/exp_ops.py:30-33)."""
+    out = Computer(qc)
+    if t == 0.0:
+        return out
+    nsub = max(1, math.ceil(abs(t) * _norm1(hamiltonian) / 0.5))
+    h = t / nsub
+    eps = 2.0 ** -53
+    for _ in range(nsub):
+        term = Computer(out)
+        small = 0
+        for k in range(1, max_order + 1):
+            term.apply_operator(hamiltonian)
+            term.apply_constant(-1.0j * h / k)
+            _axpy(out, 1.0, term)
+            tn = abs(inner_product(term, term)) ** 0.5
+            an = abs(inner_product(out, out)) ** 0.5
+            small = small + 1 if tn <= eps * an else 0
+            if small == 2:
+                break
+        else:
+            raise RuntimeError("evolve_exact: Taylor series did not converge")
+    return out
 
 
 def fill_krylov_row(S, H, states, hstates, m):
@@ -124,3 +168,40 @@ class SRQK:
             self._S, self._Hbar, sort_ret_vals=True)
         self._Egs = np.real(self._eigenvalues[0])
         self._Ets = np.real(self._eigenvalues[self._target_root])
+
+
+class NTSRQK(SRQK):
+    """Non-Trotterized SRQK (qkd/nt_srqk.py:22-209): the basis states are exact
+    time evolutions of the reference at the points the reference samples,
+    expm_multiply(-i H, phi, start=0, stop=dt, num=s+1), i.e. t_m = m dt / s
+    (nt_srqk.py:135-137, utils/exp_ops.py:30-33).  Each state is the previous
+    one evolved by dt / s on the device (``evolve_exact``); H on it and the
+    matrix elements are as in SRQK."""
+
+    def build_qk_mats(self):
+        self._omega_lst, homega = [], []
+        self._step_energies = []
+        n = self._nstates
+        S = np.zeros((n, n), dtype=complex)
+        H = np.zeros((n, n), dtype=complex)
+        ts = np.linspace(0.0, self._dt, n)
+        qc = Computer(self._nqb)
+        qc.apply_circuit(self._Uprep)
+        for m in range(n):
+            if m > 0:
+                qc = evolve_exact(qc, self._qb_ham, ts[m] - ts[m - 1])
+            self._omega_lst.append(qc)
+            hq = Computer(qc)
+            hq.apply_operator(self._qb_ham)
+            homega.append(hq)
+            fill_krylov_row(S, H, self._omega_lst, homega, m)
+            if self._diagonalize_each_step:
+                k = m + 1
+                evals, _ = canonical_geig_solve(S[:k, :k], H[:k, :k], sort_ret_vals=True)
+                self._step_energies.append(np.real(evals[min(self._target_root, k - 1)]))
+        self._n_classical_params = n
+        self._n_cnot = 0
+        self._n_pauli_trm_measures = n * self._Nl
+        self._n_pauli_trm_measures += n * (n - 1) * self._Nl
+        self._n_pauli_trm_measures += n * (n - 1)
+        return S, H

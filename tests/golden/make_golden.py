@@ -372,9 +372,10 @@ def qite_fixture(qf, test_file, norb, seed, out):
 
 
 def srqk_fixture(qf, test_file, norb, seed, out):
-    """SRQK (qkd/srqk.py:103-204 with abc/qsdabc.py:87-115) run by the
-    reference: the H4 case of its own test (trotter_number = 100, s = 6) and a
-    seeded random-integral system (s = 3, dt = 0.5, one Trotter step)."""
+    """SRQK (qkd/srqk.py:103-204 with abc/qsdabc.py:87-115) and NTSRQK
+    (qkd/nt_srqk.py) run by the reference: the H4 cases of its own test
+    (SRQK: trotter_number = 100, s = 6; NTSRQK: s = 4, dt = 0.8) and a seeded
+    random-integral system (s = 3, dt = 0.5, one Trotter step)."""
     h4 = _test_qubit_system(test_file)
     H = qf.QubitOperator()
     for c, s in zip(h4["coef_vec"], h4["circ_vec"]):
@@ -395,7 +396,18 @@ def srqk_fixture(qf, test_file, norb, seed, out):
     alg.run(s=3, dt=0.5)
     res.update({"rand_S": alg._S, "rand_H": alg._Hbar,
                 "rand_evals": np.array(alg._eigenvalues), "rand_egs": alg._Egs})
+    # non-Trotterized SRQK (qkd/nt_srqk.py): the H4 case of the same test
+    # (s = 4, dt = 0.8) and the random system
+    alg = qf.NTSRQK(mol, reference=h4["ref"])
+    alg.run(s=4, dt=0.8)
+    res.update({"h4_nt_S": alg._S, "h4_nt_H": alg._Hbar, "h4_nt_egs": alg._Egs})
+    alg = qf.NTSRQK(s)
+    alg.run(s=3, dt=0.5)
+    res.update({"rand_nt_S": alg._S, "rand_nt_H": alg._Hbar, "rand_nt_egs": alg._Egs})
     np.savez_compressed(out, norb=norb, seed=seed, **res)
+    print(f"{out}: H4 NTSRQK E = {res['h4_nt_egs']}, cond S = "
+          f"{np.linalg.cond(res['h4_nt_S']):.2e}; random NTSRQK cond S = "
+          f"{np.linalg.cond(res['rand_nt_S']):.2e}")
     print(f"{out}: H4 SRQK E = {res['h4_egs']} (FCI {h4['E_fci']}), cond S = "
           f"{np.linalg.cond(res['h4_S']):.2e}; random E = {res['rand_egs']}, cond S = "
           f"{np.linalg.cond(res['rand_S']):.2e}")

@@ -1,4 +1,4 @@
-"""SRQK on the device against the reference's own SRQK runs.
+"""SRQK and NTSRQK on the device against the reference's own runs.
 
 The cases of the host replay in test_krylov_host.py with the Krylov basis in
 HBM: every basis state's Trotter circuit through Computer.apply_circuit, H on
@@ -14,7 +14,7 @@ system) from the reference's.
 import pytest
 
 from conftest import golden
-from test_krylov_host import check_srqk
+from test_krylov_host import check_ntsrqk, check_srqk
 
 pytestmark = pytest.mark.gpu
 
@@ -22,3 +22,10 @@ pytestmark = pytest.mark.gpu
 def test_srqk_on_device_matches_reference(cuda):
     from qforte_b200 import krylov
     check_srqk(krylov, golden("srqk_norb3_seed11.npz"))
+
+
+def test_ntsrqk_on_device_matches_reference(cuda):
+    """Exact time evolution by the device Taylor series (qfb_sum_apply, qfb_axpy)
+    against the reference's expm_multiply basis: matrix elements 1e-10."""
+    from qforte_b200 import krylov
+    check_ntsrqk(krylov, golden("srqk_norb3_seed11.npz"))

@@ -6,8 +6,9 @@ unchanged except that each state is a host vector driven by the oracle's C
 restatement of the reference Computer (the stand-in of test_qite_host.py), so
 these tests check the Trotter circuits of every basis state, their global
 phases, the matrix assembly and the generalised eigenproblem against
-tests/golden/srqk_norb3_seed11.npz, which the reference's SRQK wrote
-(qkd/srqk.py:103-204, abc/qsdabc.py:87-115, tests/test_fast_qk.py:9-411).
+tests/golden/srqk_norb3_seed11.npz, which the reference's SRQK and NTSRQK
+wrote (qkd/srqk.py:103-204, qkd/nt_srqk.py, abc/qsdabc.py:87-115,
+tests/test_fast_qk.py:9-417).
 
 Tolerances: matrix elements 1e-10 (here they agree with the reference's to
 1.4e-15).  The lowest generalised eigenvalue moves with rounding of the
@@ -30,11 +31,16 @@ H4_EIG_TOL = 1e-5
 RAND_EIG_TOL = 1e-8
 
 
+def _host_axpy(dst, a, src):
+    dst.s.psi += a * src.s.psi
+
+
 @pytest.fixture
 def host_krylov(monkeypatch):
     from qforte_b200 import krylov
     monkeypatch.setattr(krylov, "Computer", HostComputer)
     monkeypatch.setattr(krylov, "inner_product", lambda a, b: a.s.dot(b.s))
+    monkeypatch.setattr(krylov, "_axpy", _host_axpy)
     return krylov
 
 
@@ -75,5 +81,71 @@ def check_srqk(krylov, d):
             assert abs(egs - float(d["rand_egs"])) < RAND_EIG_TOL, (name, egs)
 
 
+# Non-Trotterized SRQK: the basis comes from exact time evolution (a Taylor
+# series on the device; scipy's expm_multiply in the reference).  The host
+# replay's matrices agree with the reference's to 3.1e-15; the overlap
+# condition numbers are 4.6e11 (H4) and 9.7e9 (random system), where 1e-16
+# noise on S moves the reference's own lowest eigenvalue by 3.5e-8 and 5.4e-7.
+NT_H4_EIG_TOL = 1e-5
+NT_RAND_EIG_TOL = 1e-4
+
+
+def check_ntsrqk(krylov, d):
+    import qforte_b200 as qb
+    H = qb.QubitOperator()
+    for c, s in zip(d["h4_coeffs"], d["h4_circs"]):
+        H.add(float(c), qb.build_circuit(str(s)))
+    h4 = _System()
+    h4.hamiltonian = H
+    h4.hf_reference = [int(v) for v in d["h4_ref"]]
+    a4 = krylov.NTSRQK(h4)
+    a4.run(s=4, dt=0.8)
+    mol = qb.random_molecule(int(d["norb"]), int(d["norb"]), int(d["seed"]))
+    rs = _System()
+    rs.hamiltonian = mol.hamiltonian
+    rs.hf_reference = mol.hf_reference
+    ar = krylov.NTSRQK(rs)
+    ar.run(s=3, dt=0.5)
+    for name, alg, p, tol in (("H4 NTSRQK", a4, "h4_nt", NT_H4_EIG_TOL),
+                              ("random NTSRQK", ar, "rand_nt", NT_RAND_EIG_TOL)):
+        for ours, ref in ((alg._S, d[f"{p}_S"]), (alg._Hbar, d[f"{p}_H"])):
+            assert np.max(np.abs(ours - ref)) < M_TOL, (name, np.max(np.abs(ours - ref)))
+        assert abs(alg.get_gs_energy() - float(d[f"{p}_egs"])) < tol, name
+    # the reference test's bar (tests/test_fast_qk.py:413-417)
+    assert abs(a4.get_gs_energy() - float(d["h4_efci"])) < 1e-3
+
+
 def test_srqk_host_replay_matches_reference(host_krylov):
     check_srqk(host_krylov, golden("srqk_norb3_seed11.npz"))
+
+
+def test_ntsrqk_host_replay_matches_reference(host_krylov):
+    check_ntsrqk(host_krylov, golden("srqk_norb3_seed11.npz"))
+
+
+def test_exact_evolution_matches_dense_exponential(host_krylov):
+    """evolve_exact == expm(-i t H) psi from the dense matrix, and leaves its
+    input unchanged."""
+    from scipy.linalg import expm
+
+    import qforte_b200 as qb
+    from oracle import oracle as O
+    mol = qb.random_molecule(2, 2, 5)
+    n = 4
+    Hd = np.zeros((16, 16), dtype=complex)
+    for j in range(16):
+        e = np.zeros(16, dtype=complex)
+        e[j] = 1.0
+        st = O.State(n, e)
+        st.apply_operator([(c, [(g.target(), g.control(), g.matrix()) for g in circ.gates()])
+                           for c, circ in mol.hamiltonian.terms()])
+        Hd[:, j] = st.psi
+    rng = np.random.default_rng(2)
+    psi = rng.normal(size=16) + 1j * rng.normal(size=16)
+    psi /= np.linalg.norm(psi)
+    qc = HostComputer(n)
+    qc.s = O.State(n, psi)
+    for t in (0.0, 0.05, -0.3, 1.7):
+        out = host_krylov.evolve_exact(qc, mol.hamiltonian, t)
+        assert np.max(np.abs(out.s.psi - expm(-1j * t * Hd) @ psi)) < 1e-13
+        assert np.array_equal(qc.s.psi, psi)
