@@ -37,11 +37,12 @@ from .circuit import Circuit
 from .computer import Computer, _new_state, inner_product
 from .device import prog_from_strings, sum_from_terms
 from .gate import gate
-from .sq_op_pool import SQOpPool
+from .sq_op_pool import SQOpPool, find_irrep
 from .sq_operator import SQOperator
 from .utils import build_refprep, compact_excitation_circuit, ref_to_basis_idx, trotterize
 
-__all__ = ["DUCC", "Evaluator", "evaluator_config", "UCCNVQE", "ADAPTVQE", "ansatz_strings", "gradient_strings"]
+__all__ = ["DUCC", "Evaluator", "evaluator_config", "UCCNVQE", "ADAPTVQE", "UCCNPQE", "SPQE",
+           "ansatz_strings", "gradient_strings"]
 
 
 def evaluator_config(compact=True):
@@ -810,6 +811,187 @@ class UCCNPQE(_UCCBase):
             if self._res_vec_norm < self._opt_thresh:
                 break
         self._Egs = Ek
+
+
+class SPQE(UCCNPQE):
+    """Selected PQE (ucc/spqe.py:24-605): grow the ansatz from the residuals of
+    every determinant of the reference's particle-number sector, then solve the
+    projective equations of the chosen operators with UCCNPQE's Jacobi / DIIS
+    iterations.
+
+    The selection step applies U, exp(i dt H) (trotterized) and U^dagger to the
+    reference as the reference does (spqe.py:427-442); |r_I|^2 is read from the
+    resulting amplitudes of the pool's determinants.  The micro-iterations take
+    their residuals from the evaluator's residual run (engine "fused") or from
+    the reference's Computer calls (engine "percall").  Only the Jacobi solver
+    and M_omega = "inf" (exact residuals) are built.
+    """
+
+    def __init__(self, system, reference=None, diis_max_dim=8, irrep=0, **kwargs):
+        super().__init__(system, reference, **kwargs)
+        self._diis_max_dim = diis_max_dim
+        self._irrep = irrep
+
+    def run(self, spqe_thresh=1.0e-2, spqe_maxiter=20, dt=0.001, M_omega="inf",
+            opt_thresh=1.0e-5, opt_maxiter=30, use_cumulative_thresh=True,
+            max_excit_rank=None, optimizer="Jacobi"):
+        if optimizer.lower() != "jacobi":
+            raise NotImplementedError("only the Jacobi solver is implemented")
+        if M_omega != "inf":
+            raise NotImplementedError("only exact residuals (M_omega = 'inf') are implemented")
+        self._spqe_thresh = spqe_thresh
+        self._spqe_maxiter = spqe_maxiter
+        self._dt = dt
+        self._M_omega = M_omega
+        self._use_cumulative_thresh = use_cumulative_thresh
+        self._optimizer = optimizer
+        self._opt_thresh = opt_thresh
+        self._opt_maxiter = opt_maxiter
+        self._noise_factor = 0.0
+        self._nbody_counts = []
+        self._n_classical_params_lst = []
+        self._energies = []
+        self._tops = []
+        self._tamps = []
+        self._stop_macro = False
+        self._converged = False
+        self._res_vec_evals = 0
+        self._res_m_evals = 0
+        self._curr_energy = 0.0
+        self._eiH, _ = trotterize(self._qb_ham, factor=self._dt * (0.0 + 1.0j),
+                                  trotter_number=self._trotter_number)
+        for occupation in self._ref:
+            if occupation:
+                self._nbody_counts.append(0)
+        self._build_determinant_pool(max_excit_rank)
+        self.build_orb_energies()
+        self._spqe_iter = 1
+        while not self._stop_macro:
+            self.update_ansatz()
+            if self._converged:
+                break
+            self.fill_excited_dets()
+            self.jacobi_solver()
+            self._spqe_iter += 1
+        self._Egs = self._energies[-1]
+        return self._Egs
+
+    def _build_determinant_pool(self, max_excit_rank):
+        """One operator per determinant of the reference's (N_alpha, N_beta)
+        sector and irrep, up to max_excit_rank-fold excitations, in basis-index
+        order (spqe.py:159-240): tau - tau^dagger with the determinant's
+        creators and annihilators in ascending order."""
+        ref_idx = ref_to_basis_idx(self._ref)
+        nalpha = sum(self._ref[0::2])
+        nbeta = sum(self._ref[1::2])
+        if max_excit_rank is None:
+            max_excit_rank = nalpha + nbeta
+        elif not isinstance(max_excit_rank, int) or max_excit_rank <= 0:
+            raise TypeError("The maximum excitation rank max_excit_rank must be a positive integer!")
+        elif max_excit_rank > nalpha + nbeta:
+            max_excit_rank = nalpha + nbeta
+        self._pool_type = max_excit_rank
+        irreps = getattr(self._sys, "orb_irreps_to_int", None) or [0] * (self._nqb // 2 + 1)
+        self._pool_obj = SQOpPool()
+        self._coeff_idx_to_pool_idx = {}
+        self._indices_of_zeroable_residuals_for_pool = set()
+        for I in range(1 << self._nqb):
+            occ = [q for q in range(self._nqb) if I >> q & 1]
+            if sum(1 for q in occ if q % 2 == 0) != nalpha or sum(1 for q in occ if q % 2) != nbeta:
+                continue
+            if find_irrep(irreps, occ) != self._irrep:
+                continue
+            excit = ref_idx ^ I
+            if excit == 0 or bin(excit).count("1") // 2 > max_excit_rank:
+                continue
+            occ_idx = [q for q in range(self._nqb) if excit >> q & 1 and self._ref[q] == 1]
+            unocc_idx = [q for q in range(self._nqb) if excit >> q & 1 and self._ref[q] == 0]
+            sq_op = SQOperator()
+            sq_op.add(+1.0, unocc_idx, occ_idx)
+            sq_op.add(-1.0, occ_idx[::-1], unocc_idx[::-1])
+            sq_op.simplify()
+            self._coeff_idx_to_pool_idx[I] = len(self._pool_obj)
+            self._indices_of_zeroable_residuals_for_pool.add(I)
+            self._pool_obj.add_term(0.0, sq_op)
+        self._pool_idx_to_coeff_idx = {v: k for k, v in self._coeff_idx_to_pool_idx.items()}
+
+    def update_ansatz(self):
+        """spqe.py:427-590 (M_omega = 'inf'): residuals of every pool
+        determinant not yet in the ansatz from U^dagger exp(i dt H) U |ref>.
+        The reference's energy evaluation at the start of this step only
+        feeds a printout and is not repeated here."""
+        U = self.ansatz_circuit()
+        qc = Computer(self._nqb)
+        qc.apply_circuit(self._Uprep)
+        qc.apply_circuit(U)
+        qc.apply_circuit(self._eiH)
+        qc.apply_circuit(U.adjoint())
+        coeffs = qc.get_coeff_array()
+        in_ansatz = {self._pool_idx_to_coeff_idx[i] for i in self._tops}
+        res_sq = [(float(np.real(np.conj(coeffs[I]) * coeffs[I])), I)
+                  for I in self._indices_of_zeroable_residuals_for_pool - in_ansatz]
+        res_sq.sort()
+        self._curr_res_sq_norm = sum(r for r, _ in res_sq) / (self._dt * self._dt)
+        self.conv_status()
+        if self._converged:
+            return
+        if self._use_cumulative_thresh:
+            res_sq_sum = 0.0
+            temp_ops = []
+            for rmu_sq, I in res_sq:
+                res_sq_sum += rmu_sq / (self._dt * self._dt)
+                if res_sq_sum > self._spqe_thresh * self._spqe_thresh:
+                    pool_idx = self._coeff_idx_to_pool_idx[I]
+                    if pool_idx not in self._tops:
+                        temp_ops.append(pool_idx)
+                        rank = len(self._pool_obj[pool_idx][1].terms()[0][1])
+                        self._nbody_counts[rank - 1] += 1
+            for op in temp_ops[::-1]:
+                self._tops.insert(0, op)
+                self._tamps.insert(0, 0.0)
+        else:
+            for rmu_sq, I in reversed(res_sq):
+                pool_idx = self._coeff_idx_to_pool_idx[I]
+                if pool_idx not in self._tops:
+                    self._tops.insert(0, pool_idx)
+                    self._tamps.insert(0, 0.0)
+                    rank = len(self._pool_obj[pool_idx][1].terms()[0][1])
+                    self._nbody_counts[rank - 1] += 1
+                    break
+        self._n_classical_params_lst.append(len(self._tops))
+
+    def conv_status(self):
+        """spqe.py:593-603."""
+        if abs(self._curr_res_sq_norm) < abs(self._spqe_thresh * self._spqe_thresh):
+            self._converged = True
+            self._stop_macro = True
+        elif self._spqe_iter > self._spqe_maxiter:
+            self._converged = False
+            self._stop_macro = True
+        elif len(self._tops) == len(self._pool_obj):
+            self._converged = True
+            self._stop_macro = True
+
+    def jacobi_solver(self):
+        """maths/optimizer.py:40-116 as SPQE runs it: the energies list gets
+        one entry per macro-iteration, the final one."""
+        import copy
+        t_diis = [copy.deepcopy(self._tamps)]
+        e_diis = []
+        Ek = self.energy_feval(self._tamps)
+        for _ in range(1, self._opt_maxiter + 1):
+            t_old = copy.deepcopy(self._tamps)
+            r_k = self.get_res_over_mpdenom(self.get_residual_vector(self._tamps))
+            self._tamps = list(np.add(self._tamps, r_k))
+            t_diis.append(copy.deepcopy(self._tamps))
+            e_diis.append(np.subtract(copy.deepcopy(self._tamps), t_old))
+            if self._diis_max_dim >= 2:
+                self._tamps = _diis(self._diis_max_dim, t_diis, e_diis)
+            Ek = self.energy_feval(self._tamps)
+            if self._res_vec_norm < self._opt_thresh:
+                break
+        self._Egs = Ek
+        self._energies.append(Ek)
 
 
 def _diis(diis_max_dim, t_diis, e_diis):

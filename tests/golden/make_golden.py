@@ -413,10 +413,44 @@ def srqk_fixture(qf, test_file, norb, seed, out):
           f"{np.linalg.cond(res['rand_S']):.2e}")
 
 
+def spqe_fixture(qf, tests_dir, norb, seed, out):
+    """SPQE (ucc/spqe.py) run by the reference: the H4/STO-6G case of its own
+    test (tests/test_spqe.py:11-39: external integrals, zero terms dropped,
+    spqe_thresh 1e-4, dt 1e-4) and a seeded random-integral system."""
+    mol = qf.system_factory(stytem_type="molecule", build_type="external", basis="sto-6g",
+                            filename=os.path.join(tests_dir, "H4-sto6g-075a.json"))
+    Hnz = qf.QubitOperator()
+    for c, circ in mol._hamiltonian.terms():
+        if abs(c) > 1.0e-14:
+            Hnz.add(c, circ)
+    mol._hamiltonian = Hnz
+    alg = qf.SPQE(mol, print_summary_file=False)
+    alg.run(spqe_maxiter=20, spqe_thresh=1.0e-4, opt_thresh=1.0e-5, dt=0.0001)
+    res = {"h4_egs": alg.get_gs_energy(), "h4_energies": np.array(alg._energies),
+           "h4_nparams": np.array(alg._n_classical_params_lst), "h4_npool": len(alg._pool_obj),
+           "h4_tops": np.array(alg._tops),
+           "h4_orb_e": np.array(alg._orb_e)}
+    h, g = random_integrals(norb, seed)
+    s = _Sys()
+    s.hamiltonian = ref_sq_ham(qf, h, g).jw_transform()
+    s.hf_reference = hf_reference(norb, norb)
+    s.hf_energy = 0.0
+    s.orb_irreps_to_int = [0] * norb
+    s.point_group = ["c1", ["A"]]
+    alg = qf.SPQE(s)
+    alg.run(spqe_maxiter=10, spqe_thresh=1.0e-3, opt_thresh=1.0e-7, opt_maxiter=60, dt=0.001)
+    res.update({"rand_egs": alg.get_gs_energy(), "rand_energies": np.array(alg._energies),
+                "rand_nparams": np.array(alg._n_classical_params_lst),
+                "rand_tops": np.array(alg._tops), "rand_npool": len(alg._pool_obj)})
+    np.savez_compressed(out, norb=norb, seed=seed, **res)
+    print(f"{out}: H4 SPQE E = {res['h4_egs']} ({len(res['h4_energies'])} macro-iterations, "
+          f"params {res['h4_nparams']}); random E = {res['rand_egs']}, params {res['rand_nparams']}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-src", default="/root/reference/src/qforte")
-    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact, qite, srqk)")
+    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact, qite, srqk, spqe)")
     a = ap.parse_args()
     qf = O.load_reference(a.ref_src)
     tests_dir = os.path.join(os.path.dirname(a.ref_src.rstrip("/")), "..", "tests")
@@ -431,6 +465,8 @@ def main():
     if a.only in ("srqk", None):
         srqk_fixture(qf, os.path.join(tests_dir, "test_fast_qk.py"), 3, 11,
                      os.path.join(HERE, "srqk_norb3_seed11.npz"))
+    if a.only in ("spqe", None):
+        spqe_fixture(qf, tests_dir, 3, 11, os.path.join(HERE, "spqe_norb3_seed11.npz"))
     if a.only is not None:
         return
     ucc_fixture(qf, 4, 11, os.path.join(HERE, "ucc_norb4_seed11.npz"))

@@ -1,0 +1,23 @@
+"""SPQE on the device against the reference's own SPQE runs.
+
+The cases of the host replay in test_spqe_host.py on the fused engine: the
+selection step's U, exp(i dt H) and U^dagger as fused Pauli-exponential passes,
+the micro-iterations' residuals and energies from the evaluator's residual
+run.  Golden values: tests/golden/spqe_norb3_seed11.npz, written by the
+reference's SPQE (ucc/spqe.py).  Pins: the H4 run reaches FCI within 5e-11
+(tests/test_spqe.py:11-39); every selection picks the reference's operators
+with the same counts per macro-iteration; per-iteration energies 1e-10 where
+the selection order matches the reference's (mirror-image determinants tie in
+H4's first selection, so rounding may swap their order: test_spqe_host.py).
+"""
+
+import pytest
+
+from test_spqe_host import check_spqe
+
+pytestmark = pytest.mark.gpu
+
+
+def test_spqe_on_device_matches_reference(cuda):
+    from qforte_b200 import ucc
+    check_spqe(ucc, "fused", strict=False)

@@ -25,7 +25,8 @@ def _gates(circ):
 
 
 class HostComputer:
-    """A host state with the Computer methods QITE and SRQK call (test stand-in)."""
+    """A host state with the Computer methods the QITE, SRQK and SPQE drivers
+    call (test stand-in)."""
 
     def __init__(self, n):
         from oracle import oracle as O
@@ -45,6 +46,15 @@ class HostComputer:
 
     def apply_constant(self, a):
         self.s.apply_constant(a)
+
+    def apply_gate(self, g):
+        self.s.apply_gates([(g.target(), g.control(), g.matrix())])
+
+    def get_coeff_array(self):
+        return self.s.psi.copy()
+
+    def get_coeff_vec(self):
+        return list(self.s.psi)
 
     def direct_op_exp_val(self, qo):
         t = HostComputer(self)
