@@ -12,13 +12,14 @@ Here the state stays in HBM and both come from segmented expectation values
 of its terms, and the only data crossing to the host are the results.
 
 * b_I = Re(-i c_I / sqrt(1 - 2 db E) <psi| sigma_I H |psi>): H psi is formed
-  once (``qfb_sum_apply``), then <psi| sigma_I |H psi> for every I in one
-  ``qfb_sum_expval`` with bra psi, ket H psi and one result segment per I.
+  once (``qfb_sum_apply``), then <psi| P |H psi> for every distinct Pauli
+  string P of the operators, one result segment each, with bra psi and ket
+  H psi.
 * S_IJ = Re <sigma_I psi | sigma_J psi> = Re <psi| sigma_I^dag sigma_J |psi>:
   a product of two Pauli strings is one Pauli string times a power of i
-  (``pauli_mul``, exact), so every pair I < J is a segment of one
-  ``qfb_sum_expval`` over psi.  S_II = 1 as in the reference (a Pauli string
-  squares to one).
+  (``pauli_mul``, exact), so S needs <psi| P |psi> once per distinct product
+  string, and each pair I < J combines them with its coefficients on the
+  host.  S_II = 1 as in the reference (a Pauli string squares to one).
 
 The evolution step exp(A), A = -i db sum_I x_I sigma_I, is trotterized as in the
 reference and applied through ``Computer.apply_circuit``, which runs Pauli
@@ -90,46 +91,56 @@ def _op_terms(qo):
     return pt
 
 
+def _distinct_string_expvals(bra, ket, strings):
+    """<bra| P(x, z) |ket> for every distinct (x, z) of ``strings``, one
+    result segment each: returns ({(x, z): value})."""
+    keys = list(dict.fromkeys(strings))
+    vals = _segment_expvals(bra, ket, [(1.0, x, z) for x, z in keys], list(range(len(keys))),
+                            len(keys))
+    return dict(zip(keys, vals))
+
+
 def qite_b(qc, hamiltonian, sig_ops, sig_coeffs, db, energy):
     """build_b (ite/qite.py:305-326): b_I = Re(-i c_I <psi| sigma_I H |psi>) /
-    sqrt(1 - 2 db E), every I from one grouped expectation-value call."""
+    sqrt(1 - 2 db E).  H psi is formed once; <psi| P |H psi> is read once per
+    distinct Pauli string P among the operators' terms."""
     prefactor = -1.0j / np.sqrt(1 - 2 * db * energy)
     hpsi = Computer(qc)
     hpsi.apply_operator(hamiltonian)
-    terms, seg = [], []
-    for i, op in enumerate(sig_ops):
-        pt = _op_terms(op)
-        terms.extend(pt)
-        seg.extend([i] * len(pt))
-    vals = _segment_expvals(qc, hpsi, terms, seg, len(sig_ops))
+    ops = [_op_terms(op) for op in sig_ops]
+    ev = _distinct_string_expvals(qc, hpsi, [(x, z) for pt in ops for _, x, z in pt])
+    vals = np.array([sum(complex(c) * ev[(x, z)] for c, x, z in pt) for pt in ops],
+                    dtype=np.complex128)
     b = prefactor * np.asarray(sig_coeffs, dtype=np.complex128) * vals
     return np.real(b)
 
 
 def qite_S(qc, sig_ops):
     """build_S (ite/qite.py:256-276) over the given operators: S_II = 1 and
-    S_IJ = S_JI = Re <sigma_I psi | sigma_J psi> for I != J, each pair I < J a
-    segment of one grouped expectation-value call over psi."""
+    S_IJ = S_JI = Re <sigma_I psi | sigma_J psi> for I != J.  Each product of
+    two terms' Pauli strings is one string times a power of i, so
+    <sigma_I psi | sigma_J psi> = sum_ab conj(c_a) c_b i^e <psi| P_ab |psi>,
+    and <psi| P |psi> is read once per distinct product string P (for
+    single-string operators on n qubits: at most 4^n reads, not NI^2 / 2)."""
     n = len(sig_ops)
     S = np.eye(n)
     if n < 2:
         return S
     ops = [_op_terms(op) for op in sig_ops]
-    terms, seg, pairs = [], [], []
+    # (i, j) -> [(coefficient, (x, z))] of sigma_i^dag sigma_j
+    prods = {}
     for i in range(n):
         for j in range(i):
-            k = len(pairs)
-            pairs.append((i, j))
-            # <sigma_i psi | sigma_j psi> = sum_ab conj(c_a) c_b <psi| P_a P_b |psi>
+            lst = []
             for ca, xa, za in ops[i]:
                 ca = complex(ca).conjugate()
                 for cb, xb, zb in ops[j]:
                     x, z, e = pauli_mul(xa, za, xb, zb)
-                    terms.append((ipow_mul(ca * complex(cb), e), x, z))
-                    seg.append(k)
-    vals = _segment_expvals(qc, qc, terms, seg, len(pairs))
-    for k, (i, j) in enumerate(pairs):
-        S[i, j] = S[j, i] = np.real(vals[k])
+                    lst.append((ipow_mul(ca * complex(cb), e), (x, z)))
+            prods[(i, j)] = lst
+    ev = _distinct_string_expvals(qc, qc, [k for lst in prods.values() for _, k in lst])
+    for (i, j), lst in prods.items():
+        S[i, j] = S[j, i] = np.real(sum(c * ev[k] for c, k in lst))
     return S
 
 
