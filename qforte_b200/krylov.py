@@ -24,9 +24,10 @@ from ._lib import check, cplx, lib
 from .circuit import Circuit
 from .computer import Computer, inner_product
 from .qite import canonical_geig_solve
-from .utils import build_refprep, trotterize
+from .qubit_basis import QubitBasis
+from .utils import build_eq_dets, build_refprep, integer_to_ref, open_shell, ref_to_basis_idx, trotterize
 
-__all__ = ["SRQK", "NTSRQK", "evolve_exact", "fill_krylov_row"]
+__all__ = ["SRQK", "NTSRQK", "MRSQK", "evolve_exact", "fill_krylov_row"]
 
 
 def _axpy(dst, a, src):
@@ -204,4 +205,190 @@ class NTSRQK(SRQK):
         self._n_pauli_trm_measures = n * self._Nl
         self._n_pauli_trm_measures += n * (n - 1) * self._Nl
         self._n_pauli_trm_measures += n * (n - 1)
+        return S, H
+
+
+def _stable_order(values, rev):
+    """Indices by real part, ascending (rev=False) or descending (rev=True),
+    ties in input order (helper/idx_org.py:sorted_largest_idxs)."""
+    return sorted(range(len(values)), key=lambda i: np.real(values[i]), reverse=rev)
+
+
+class MRSQK(SRQK):
+    """Multireference SQK (qkd/mrsqk.py:30-721): an SRQK run picks the
+    determinants that dominate the target root, optionally combined into
+    spin-adapted references by a small CI, and each reference gets its own
+    trotterized time-evolution basis.  Every basis state, H on it and the
+    CI states stay on the device; the matrix elements are device inner
+    products.  The SRQK basis is read back once to weigh the determinants, as
+    the reference does (mrsqk.py:485-598)."""
+
+    def run(self, d=2, s=3, mr_dt=0.5, target_root=0, reference_generator="SRQK",
+            use_phase_based_selection=False, use_spin_adapted_refs=True, s_o=4, dt_o=0.25,
+            trotter_order_o=1, trotter_number_o=1, diagonalize_each_step=True):
+        if reference_generator != "SRQK":
+            raise ValueError("Incorrect value passed for reference_generator, can be 'SRQK'.")
+        if trotter_order_o != 1:
+            raise NotImplementedError("Higher order trotterization is not yet implemented.")
+        self._d = d
+        self._s = s
+        self._nstates_per_ref = s + 1
+        self._nstates = d * (s + 1)
+        self._mr_dt = mr_dt
+        self._target_root = target_root
+        self._reference_generator = reference_generator
+        self._use_phase_based_selection = use_phase_based_selection
+        self._use_spin_adapted_refs = use_spin_adapted_refs
+        self._s_o = s_o
+        self._ninitial_states = s_o + 1
+        self._dt_o = dt_o
+        self._trotter_number_o = trotter_number_o
+        self._diagonalize_each_step = diagonalize_each_step
+        self._srqk = SRQK(self._sys, self._ref, trotter_number=trotter_number_o)
+        self._srqk.run(s=s_o, dt=dt_o)
+        self._n_classical_params = self._srqk._n_classical_params
+        self._n_cnot = self._srqk._n_cnot
+        self.build_refs()
+        if use_spin_adapted_refs:
+            self.build_sa_refs()
+        self.common_run()
+        self._n_classical_params = self._nstates
+        self._n_pauli_trm_measures = self._nstates * self._Nl + self._srqk._n_pauli_trm_measures
+        self._n_pauli_trm_measures += self._nstates * (self._nstates - 1) * self._Nl
+        self._n_pauli_trm_measures += self._nstates * (self._nstates - 1)
+        return self._Egs
+
+    # ---- reference selection (mrsqk.py:485-598) -------------------------------
+    def build_refs(self):
+        srqk = self._srqk
+        n_untruncated = self._ninitial_states
+        if self._ninitial_states > len(srqk._eigenvalues):
+            self._ninitial_states = len(srqk._eigenvalues)
+        order = _stable_order(srqk._eigenvalues, rev=False)
+        sorted_evecs = np.zeros((n_untruncated, self._ninitial_states), dtype=complex)
+        for n in range(self._ninitial_states):
+            sorted_evecs[:, n] = srqk._eigenvectors[:, order[n]]
+        sorted_sq_mod_evecs = sorted_evecs * np.conjugate(sorted_evecs)
+        basis = np.array([qc.get_coeff_array() for qc in srqk._omega_lst])
+        Cprime = np.conj(sorted_evecs.transpose()).dot(basis)
+        Cprime = Cprime * np.conj(Cprime)
+        # only the first ninitial_states rows are squared, as mrsqk.py:531-533
+        for n in range(self._ninitial_states):
+            basis[n] = basis[n] * np.conj(basis[n])
+        Cprime_sq_mod = sorted_sq_mod_evecs.transpose().dot(basis)
+        nsel = 2 * self._d if self._use_spin_adapted_refs else self._d
+        if self._target_root is None:
+            raise NotImplementedError("psudo state-avaraged selection approach not yet functional")
+        true_idx = _stable_order(Cprime[self._target_root, :], rev=True)[:nsel]
+        idx = _stable_order(Cprime_sq_mod[self._target_root, :], rev=True)[:nsel]
+        # where the reference determinant is missing the reference code names
+        # an undefined variable; its evident intent, the reference determinant
+        # first, is what runs here
+        initial_ref = list(self._ref)
+        true_refs = [integer_to_ref(i, self._nqb) for i in true_idx]
+        if self._ref not in true_refs:
+            for i in range(len(true_refs) - 1):
+                true_refs[i + 1] = true_refs[i]
+            true_refs[0] = initial_ref
+        refs = [integer_to_ref(i, self._nqb) for i in idx]
+        if self._ref not in refs:
+            refs = [initial_ref] + [list(r) for r in refs[:-1]]
+        self._single_det_refs = true_refs if self._use_phase_based_selection else refs
+
+    def build_classical_CI_mats(self):
+        """H among the candidate determinants (mrsqk.py:357-385)."""
+        n = len(self._pre_sa_ref_lst)
+        h_CI = np.zeros((n, n), dtype=complex)
+        dets, hdets = [], []
+        for i, ref in enumerate(self._pre_sa_ref_lst):
+            qc = Computer(self._nqb)
+            qc.apply_circuit(build_refprep(ref))
+            dets.append(qc)
+            hq = Computer(qc)
+            hq.apply_operator(self._qb_ham)
+            hdets.append(hq)
+            for j in range(i + 1):
+                h_CI[i][j] = inner_product(dets[i], hdets[j])
+                h_CI[j][i] = np.conj(h_CI[i][j])
+        return h_CI
+
+    def build_sa_refs(self):
+        """Spin-adapted references from the CI of the selected determinants
+        and their spin-flip partners (mrsqk.py:600-721)."""
+        from scipy.linalg import eig
+        target_root = self._target_root
+        self._pre_sa_ref_lst = []
+        num_refs_per_config = []
+        for ref in self._single_det_refs:
+            if ref not in self._pre_sa_ref_lst:
+                if open_shell(ref):
+                    temp = build_eq_dets(ref)
+                    self._pre_sa_ref_lst = self._pre_sa_ref_lst + temp
+                    num_refs_per_config.append(len(temp))
+                else:
+                    self._pre_sa_ref_lst.append(ref)
+                    num_refs_per_config.append(1)
+        evals, evecs = eig(self.build_classical_CI_mats())
+        order = _stable_order(evals, rev=False)
+        sorted_evecs = np.real(evecs[:, order])
+        if np.abs(sorted_evecs[:, 0][0]) < 1.0e-6:
+            adjusted_root = 0
+            co_val = 0.0
+            while co_val < 1.0e-6:
+                adjusted_root += 1
+                co_val = np.abs(sorted_evecs[:, adjusted_root][0])
+            target_root = adjusted_root
+        target_state = sorted_evecs[:, target_root]
+        basis_coeff_lst, norm_basis_coeff_lst, det_lst = [], [], []
+        start = 0
+        for num_refs in num_refs_per_config:
+            part = target_state[start:start + num_refs]
+            summ = sum(v * v for v in part)
+            norm_basis_coeff_lst.append([x / np.sqrt(summ) for x in part])
+            basis_coeff_lst.append(part)
+            det_lst.append(self._pre_sa_ref_lst[start:start + num_refs])
+            start += num_refs
+        # a configuration's weight is its last coefficient squared, as the
+        # reference's loop computes it (mrsqk.py:689-694)
+        importance = [float(c[-1] * c[-1]) for c in basis_coeff_lst]
+        by_importance = _stable_order(importance, rev=True)
+        self._sa_ref_lst = []
+        for i in range(self._d):
+            k = by_importance[i]
+            self._sa_ref_lst.append([(norm_basis_coeff_lst[k][j], det_lst[k][j])
+                                     for j in range(len(basis_coeff_lst[k]))])
+
+    # ---- the multireference Krylov matrices (mrsqk.py:270-474) ----------------
+    def build_qk_mats(self):
+        refs = self._sa_ref_lst if self._use_spin_adapted_refs else \
+            [[(1.0, r)] for r in self._single_det_refs]
+        omega, homega = [], []
+        Um = None
+        for ref in refs:
+            for m in range(self._nstates_per_ref):
+                Um = Circuit()
+                phase1 = 1.0
+                if m > 0:
+                    fact = (0.0 - 1.0j) * m * self._mr_dt
+                    expn_op1, phase1 = trotterize(self._qb_ham, factor=fact,
+                                                  trotter_number=self._trotter_number)
+                    Um.add(expn_op1)
+                qc = Computer(self._nqb)
+                qc.set_state([(QubitBasis(ref_to_basis_idx(det)), coeff) for coeff, det in ref])
+                qc.apply_circuit(Um)
+                qc.apply_constant(phase1)
+                omega.append(qc)
+                hq = Computer(qc)
+                hq.apply_operator(self._qb_ham)
+                homega.append(hq)
+        n = len(omega)
+        S = np.zeros((n, n), dtype=complex)
+        H = np.zeros((n, n), dtype=complex)
+        for p in range(n):
+            for q in range(p, n):
+                H[p][q] = inner_product(omega[p], homega[q])
+                H[q][p] = np.conj(H[p][q])
+                S[p][q] = inner_product(omega[p], omega[q])
+                S[q][p] = np.conj(S[p][q])
+        self._n_cnot = 2 * Um.get_num_cnots() if n > 1 else self._srqk._n_cnot
         return S, H

@@ -23,7 +23,8 @@ from .qubit_basis import QubitBasis
 from .qubit_operator import QubitOperator
 
 __all__ = ["exponentiate_pauli_string", "trotterize", "trotterize_w_cRz", "build_refprep",
-           "ref_string", "integer_to_ref", "build_circuit", "build_operator", "smart_print"]
+           "ref_string", "integer_to_ref", "build_circuit", "build_operator", "smart_print",
+           "open_shell", "correct_spin", "flip_spin", "build_eq_dets"]
 
 
 def exponentiate_pauli_string(coefficient, term, Use_cRz=False, ancilla_idx=None,
@@ -299,3 +300,42 @@ def _controlled_ry(theta, target, ctrl_cre, ctrl_ann, shared, gsd_sign, qubit_ex
                 circ.add(_gate("CNOT" if (last or shared) else "aCNOT", target, ctl))
                 break
     return circ
+
+
+# ---- open-shell helpers (utils/state_prep.py:53-141) -----------------------
+def open_shell(ref):
+    """True when some spatial orbital of the determinant is singly occupied."""
+    return any(ref[2 * i] + ref[2 * i + 1] == 1 for i in range(len(ref) // 2))
+
+
+def _spin(ref):
+    return sum(0.5 * ref[2 * i] - 0.5 * ref[2 * i + 1] for i in range(len(ref) // 2))
+
+
+def correct_spin(ref, abs_spin):
+    """True when |S_z| of the determinant equals abs_spin."""
+    return abs(_spin(ref)) == abs_spin
+
+
+def flip_spin(ref, orb_idx):
+    """The determinant with the alpha and beta occupations of spatial orbital
+    orb_idx exchanged."""
+    temp = list(ref)
+    temp[2 * orb_idx], temp[2 * orb_idx + 1] = ref[2 * orb_idx + 1], ref[2 * orb_idx]
+    return temp
+
+
+def build_eq_dets(open_shell_ref):
+    """Every determinant reachable from open_shell_ref by spin flips of its
+    singly occupied orbitals with the same |S_z|, the input first, in the order
+    the flips discover them (utils/state_prep.py:143-187)."""
+    one_e_orbs = [i for i in range(len(open_shell_ref) // 2)
+                  if open_shell_ref[2 * i] + open_shell_ref[2 * i + 1] == 1]
+    abs_spin = abs(_spin(open_shell_ref))
+    found = [list(open_shell_ref)]
+    for ref in found:
+        for orb in one_e_orbs:
+            temp = flip_spin(ref, orb)
+            if temp not in found:
+                found.append(temp)
+    return [r for r in found if correct_spin(r, abs_spin)]

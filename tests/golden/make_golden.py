@@ -447,10 +447,51 @@ def spqe_fixture(qf, tests_dir, norb, seed, out):
           f"params {res['h4_nparams']}); random E = {res['rand_egs']}, params {res['rand_nparams']}")
 
 
+def mrsqk_fixture(qf, test_file, norb, seed, out):
+    """MRSQK (qkd/mrsqk.py) run by the reference: the H4 case of its own test
+    (tests/test_fast_qk.py:401-405: trotter_number = 100, s = 3, d = 3) and a
+    seeded random-integral system with and without spin-adapted references."""
+    h4 = _test_qubit_system(test_file)
+    H = qf.QubitOperator()
+    for c, s in zip(h4["coef_vec"], h4["circ_vec"]):
+        H.add(c, qf.build_circuit(s) if s else qf.Circuit())
+    mol = qf.Molecule()
+    mol.hamiltonian = H
+    res = {"h4_coeffs": np.array(h4["coef_vec"]), "h4_circs": np.array(h4["circ_vec"]),
+           "h4_ref": np.array(h4["ref"]), "h4_efci": h4["E_fci"]}
+
+    def record(tag, alg):
+        res[f"{tag}_egs"] = alg._Egs
+        res[f"{tag}_evals"] = np.array(alg._eigenvalues)
+        res[f"{tag}_single_refs"] = np.array(alg._single_det_refs)
+        if alg._use_spin_adapted_refs:
+            res[f"{tag}_sa_ndet"] = np.array([len(r) for r in alg._sa_ref_lst])
+            res[f"{tag}_sa_flat_dets"] = np.array([d for r in alg._sa_ref_lst for _, d in r])
+            res[f"{tag}_sa_flat_coeffs"] = np.array([c for r in alg._sa_ref_lst for c, _ in r])
+
+    alg = qf.MRSQK(mol, reference=h4["ref"], trotter_number=100)
+    alg.run(s=3, d=3)
+    record("h4", alg)
+    h, g = random_integrals(norb, seed)
+    sy = _Sys()
+    sy.hamiltonian = ref_sq_ham(qf, h, g).jw_transform()
+    sy.hf_reference = hf_reference(norb, norb)
+    sy.hf_energy = 0.0
+    alg = qf.MRSQK(sy)
+    alg.run(s=2, d=2, mr_dt=0.4)
+    record("rand_sa", alg)
+    alg = qf.MRSQK(sy)
+    alg.run(s=2, d=2, mr_dt=0.4, use_spin_adapted_refs=False)
+    record("rand", alg)
+    np.savez_compressed(out, norb=norb, seed=seed, **res)
+    print(f"{out}: H4 MRSQK E = {res['h4_egs']} (FCI {h4['E_fci']}); random SA E = "
+          f"{res['rand_sa_egs']}, single-reference E = {res['rand_egs']}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-src", default="/root/reference/src/qforte")
-    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact, qite, srqk, spqe)")
+    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact, qite, srqk, spqe, mrsqk)")
     a = ap.parse_args()
     qf = O.load_reference(a.ref_src)
     tests_dir = os.path.join(os.path.dirname(a.ref_src.rstrip("/")), "..", "tests")
@@ -467,6 +508,9 @@ def main():
                      os.path.join(HERE, "srqk_norb3_seed11.npz"))
     if a.only in ("spqe", None):
         spqe_fixture(qf, tests_dir, 3, 11, os.path.join(HERE, "spqe_norb3_seed11.npz"))
+    if a.only in ("mrsqk", None):
+        mrsqk_fixture(qf, os.path.join(tests_dir, "test_fast_qk.py"), 3, 11,
+                      os.path.join(HERE, "mrsqk_norb3_seed11.npz"))
     if a.only is not None:
         return
     ucc_fixture(qf, 4, 11, os.path.join(HERE, "ucc_norb4_seed11.npz"))

@@ -1,4 +1,4 @@
-"""SRQK and NTSRQK on the device against the reference's own runs.
+"""SRQK, NTSRQK and MRSQK on the device against the reference's own runs.
 
 The cases of the host replay in test_krylov_host.py with the Krylov basis in
 HBM: every basis state's Trotter circuit through Computer.apply_circuit, H on
@@ -14,7 +14,7 @@ system) from the reference's.
 import pytest
 
 from conftest import golden
-from test_krylov_host import check_ntsrqk, check_srqk
+from test_krylov_host import MRSQK_EIG_TOL, check_mrsqk, check_ntsrqk, check_srqk
 
 pytestmark = pytest.mark.gpu
 
@@ -29,3 +29,12 @@ def test_ntsrqk_on_device_matches_reference(cuda):
     against the reference's expm_multiply basis: matrix elements 1e-10."""
     from qforte_b200 import krylov
     check_ntsrqk(krylov, golden("srqk_norb3_seed11.npz"))
+
+
+def test_mrsqk_on_device_matches_reference(cuda):
+    """Reference selection from the device SRQK basis, the CI of the candidate
+    determinants and the multireference basis on the device: the reference's
+    selections and spin-adapted references, lowest eigenvalues within 1e-7 and
+    H4 within 1e-6 of FCI (tests/test_fast_qk.py:401-405)."""
+    from qforte_b200 import krylov
+    check_mrsqk(krylov, golden("mrsqk_norb3_seed11.npz"), MRSQK_EIG_TOL)

@@ -6,9 +6,9 @@ unchanged except that each state is a host vector driven by the oracle's C
 restatement of the reference Computer (the stand-in of test_qite_host.py), so
 these tests check the Trotter circuits of every basis state, their global
 phases, the matrix assembly and the generalised eigenproblem against
-tests/golden/srqk_norb3_seed11.npz, which the reference's SRQK and NTSRQK
-wrote (qkd/srqk.py:103-204, qkd/nt_srqk.py, abc/qsdabc.py:87-115,
-tests/test_fast_qk.py:9-417).
+tests/golden/srqk_norb3_seed11.npz and mrsqk_norb3_seed11.npz, which the
+reference's SRQK, NTSRQK and MRSQK wrote (qkd/srqk.py:103-204, qkd/nt_srqk.py,
+qkd/mrsqk.py, abc/qsdabc.py:87-115, tests/test_fast_qk.py:9-417).
 
 Tolerances: matrix elements 1e-10 (here they agree with the reference's to
 1.4e-15).  The lowest generalised eigenvalue moves with rounding of the
@@ -149,3 +149,53 @@ def test_exact_evolution_matches_dense_exponential(host_krylov):
         out = host_krylov.evolve_exact(qc, mol.hamiltonian, t)
         assert np.max(np.abs(out.s.psi - expm(-1j * t * Hd) @ psi)) < 1e-13
         assert np.array_equal(qc.s.psi, psi)
+
+
+def check_mrsqk(krylov, d, eig_tol):
+    """MRSQK: the reference's determinant selections, spin-adapted references
+    (coefficients up to the overall sign an eigensolver leaves free) and lowest
+    eigenvalues."""
+    import qforte_b200 as qb
+    H = qb.QubitOperator()
+    for c, s in zip(d["h4_coeffs"], d["h4_circs"]):
+        H.add(float(c), qb.build_circuit(str(s)))
+    h4 = _System()
+    h4.hamiltonian = H
+    h4.hf_reference = [int(v) for v in d["h4_ref"]]
+    a4 = krylov.MRSQK(h4, trotter_number=100)
+    a4.run(s=3, d=3)
+    mol = qb.random_molecule(int(d["norb"]), int(d["norb"]), int(d["seed"]))
+    rs = _System()
+    rs.hamiltonian = mol.hamiltonian
+    rs.hf_reference = mol.hf_reference
+    asa = krylov.MRSQK(rs)
+    asa.run(s=2, d=2, mr_dt=0.4)
+    a1 = krylov.MRSQK(rs)
+    a1.run(s=2, d=2, mr_dt=0.4, use_spin_adapted_refs=False)
+    for tag, alg in (("h4", a4), ("rand_sa", asa), ("rand", a1)):
+        assert np.array_equal(np.array(alg._single_det_refs), d[f"{tag}_single_refs"]), tag
+        if alg._use_spin_adapted_refs:
+            assert [len(r) for r in alg._sa_ref_lst] == list(d[f"{tag}_sa_ndet"]), tag
+            dets = np.array([det for r in alg._sa_ref_lst for _, det in r])
+            assert np.array_equal(dets, d[f"{tag}_sa_flat_dets"]), tag
+            k = 0
+            for r in alg._sa_ref_lst:
+                ours = np.array([c for c, _ in r])
+                ref = d[f"{tag}_sa_flat_coeffs"][k:k + len(r)]
+                k += len(r)
+                assert min(np.max(np.abs(ours - ref)), np.max(np.abs(ours + ref))) < 1e-10, tag
+        assert abs(alg.get_gs_energy() - float(d[f"{tag}_egs"])) < eig_tol[tag], \
+            (tag, alg.get_gs_energy() - float(d[f"{tag}_egs"]))
+    # the reference test's bar (tests/test_fast_qk.py:401-405)
+    assert abs(a4.get_gs_energy() - float(d["h4_efci"])) < 1e-6
+
+
+# MRSQK lowest eigenvalues: the host replay differs from the reference by
+# 2.2e-13 (H4), 5.1e-12 and 2.5e-11 (random system with and without
+# spin-adapted references) at overlap condition numbers 3.0e9, 9.3e5 and 6.6e5;
+# the bound leaves room for the device's rounding.
+MRSQK_EIG_TOL = {"h4": 1e-7, "rand_sa": 1e-7, "rand": 1e-7}
+
+
+def test_mrsqk_host_replay_matches_reference(host_krylov):
+    check_mrsqk(host_krylov, golden("mrsqk_norb3_seed11.npz"), MRSQK_EIG_TOL)

@@ -25,8 +25,8 @@ def _gates(circ):
 
 
 class HostComputer:
-    """A host state with the Computer methods the QITE, SRQK and SPQE drivers
-    call (test stand-in)."""
+    """A host state with the Computer methods the QITE, SRQK, NTSRQK, MRSQK and
+    SPQE drivers call (test stand-in)."""
 
     def __init__(self, n):
         from oracle import oracle as O
@@ -55,6 +55,11 @@ class HostComputer:
 
     def get_coeff_vec(self):
         return list(self.s.psi)
+
+    def set_state(self, state):
+        self.s.psi[:] = 0.0
+        for b, c in state:
+            self.s.psi[b.index()] = c
 
     def direct_op_exp_val(self, qo):
         t = HostComputer(self)
