@@ -272,7 +272,7 @@ class MRSQK(SRQK):
         basis = np.array([qc.get_coeff_array() for qc in srqk._omega_lst])
         Cprime = np.conj(sorted_evecs.transpose()).dot(basis)
         Cprime = Cprime * np.conj(Cprime)
-        # only the first ninitial_states rows are squared, as mrsqk.py:531-533
+        # only the first ninitial_states rows are squared, as mrsqk.py:526-528
         for n in range(self._ninitial_states):
             basis[n] = basis[n] * np.conj(basis[n])
         Cprime_sq_mod = sorted_sq_mod_evecs.transpose().dot(basis)
@@ -349,7 +349,7 @@ class MRSQK(SRQK):
             det_lst.append(self._pre_sa_ref_lst[start:start + num_refs])
             start += num_refs
         # a configuration's weight is its last coefficient squared, as the
-        # reference's loop computes it (mrsqk.py:689-694)
+        # reference's loop computes it (mrsqk.py:690-694)
         importance = [float(c[-1] * c[-1]) for c in basis_coeff_lst]
         by_importance = _stable_order(importance, rev=True)
         self._sa_ref_lst = []
