@@ -699,16 +699,20 @@ class UCCNPQE(_UCCBase):
     """dUCC-PQE with all pool operators (ucc/uccnpqe.py:24-300): solve the
     projective equations r_mu(t) = <I_mu|U^dagger H U|ref> = 0 by Jacobi
     iterations with Moller-Plesset denominators and DIIS (maths/optimizer.py:
-    6-116).  Residuals come from the evaluator's residual run (psi, H psi,
+    6-116), or by a scipy minimiser of the summed squared residuals
+    (:119-176).  Residuals come from the evaluator's residual run (psi, H psi,
     U^dagger on sigma and the projections in one launch)."""
+
+    _SCIPY_SOLVERS = ("nelder-mead", "powell", "bfgs", "l-bfgs-b", "cg", "slsqp")
 
     def run(self, pool_type="SD", opt_thresh=1.0e-5, opt_maxiter=40, noise_factor=0.0,
             optimizer="jacobi", diis_max_dim=8):
         if pool_type == "sa_SD":
             raise ValueError("Must use single term particle-hole nbody operators for residual "
                              "calculation")
-        if optimizer.lower() != "jacobi":
-            raise NotImplementedError("only the Jacobi solver is implemented")
+        self._check_optimizer(optimizer)
+        self._optimizer = optimizer
+        self._energies = []
         self._pool_type = pool_type
         self._opt_thresh = opt_thresh
         self._opt_maxiter = opt_maxiter
@@ -720,8 +724,44 @@ class UCCNPQE(_UCCBase):
         self.initialize_ansatz()
         self.fill_excited_dets()
         self.build_orb_energies()
-        self.jacobi_solver()
+        self.solve()
         return self._Egs
+
+    def _check_optimizer(self, optimizer):
+        if optimizer.lower() != "jacobi" and optimizer.lower() not in self._SCIPY_SOLVERS:
+            raise NotImplementedError("Currently only Jacobi, Nelder-Mead, Powell, BFGS, "
+                                      "L-BFGS-B, CG, and SLSQP solvers are implemented")
+
+    def solve(self):
+        """abc/uccpqeabc.py:108-123."""
+        if self._optimizer.lower() == "jacobi":
+            self.jacobi_solver()
+        else:
+            self.scipy_solver(self.get_sum_residual_square)
+
+    def get_sum_residual_square(self, tamps):
+        """abc/uccpqeabc.py:101-106: the function the scipy solvers minimise."""
+        r = self.get_residual_vector(tamps)
+        return float(np.sum(np.square(np.abs(r))))
+
+    def scipy_solver(self, function_to_minimize):
+        """maths/optimizer.py:119-176: scipy.optimize.minimize of the summed
+        squared residuals, with the reference's tolerance options."""
+        from scipy.optimize import minimize
+        opts = {"maxiter": self._opt_maxiter}
+        method = self._optimizer.lower()
+        if method in ("bfgs", "cg", "l-bfgs-b"):
+            opts["gtol"] = self._opt_thresh
+        if method == "nelder-mead":
+            opts["fatol"] = self._opt_thresh
+            opts["adaptive"] = True
+        if method in ("powell", "l-bfgs-b", "slsqp"):
+            opts["ftol"] = self._opt_thresh
+        res = minimize(function_to_minimize, list(self._tamps), method=self._optimizer,
+                       options=opts)
+        self._tamps = list(res.x)
+        self._Egs = self.energy_feval(self._tamps)
+        self._energies.append(self._Egs)
 
     def initialize_ansatz(self):
         self._tops = list(range(len(self._pool_obj)))
@@ -823,8 +863,9 @@ class SPQE(UCCNPQE):
     reference as the reference does (spqe.py:427-442); |r_I|^2 is read from the
     resulting amplitudes of the pool's determinants.  The micro-iterations take
     their residuals from the evaluator's residual run (engine "fused") or from
-    the reference's Computer calls (engine "percall").  Only the Jacobi solver
-    and M_omega = "inf" (exact residuals) are built.
+    the reference's Computer calls (engine "percall"), solved by Jacobi / DIIS
+    or a scipy minimiser of the summed squared residuals.  Only M_omega = "inf"
+    (exact residuals) is built.
     """
 
     def __init__(self, system, reference=None, diis_max_dim=8, irrep=0, **kwargs):
@@ -835,8 +876,7 @@ class SPQE(UCCNPQE):
     def run(self, spqe_thresh=1.0e-2, spqe_maxiter=20, dt=0.001, M_omega="inf",
             opt_thresh=1.0e-5, opt_maxiter=30, use_cumulative_thresh=True,
             max_excit_rank=None, optimizer="Jacobi"):
-        if optimizer.lower() != "jacobi":
-            raise NotImplementedError("only the Jacobi solver is implemented")
+        self._check_optimizer(optimizer)
         if M_omega != "inf":
             raise NotImplementedError("only exact residuals (M_omega = 'inf') are implemented")
         self._spqe_thresh = spqe_thresh
@@ -871,7 +911,7 @@ class SPQE(UCCNPQE):
             if self._converged:
                 break
             self.fill_excited_dets()
-            self.jacobi_solver()
+            self.solve()
             self._spqe_iter += 1
         self._Egs = self._energies[-1]
         return self._Egs

@@ -21,3 +21,9 @@ pytestmark = pytest.mark.gpu
 def test_spqe_on_device_matches_reference(cuda):
     from qforte_b200 import ucc
     check_spqe(ucc, "fused", strict=False)
+
+
+def test_scipy_solver_matches_jacobi_on_device(cuda):
+    from qforte_b200 import ucc
+    from test_spqe_host import check_scipy_matches_jacobi
+    check_scipy_matches_jacobi(ucc, "fused")

@@ -109,3 +109,29 @@ def test_spqe_pool_is_the_sector(host_ucc):
     alg._build_determinant_pool(1)
     # singles: alpha 2 occupied x 1 virtual, beta 1 occupied x 2 virtual
     assert len(alg._pool_obj) == 2 * 1 + 1 * 2
+
+
+def check_scipy_matches_jacobi(ucc, engine):
+    """The scipy path (BFGS on the summed squared residuals) reaches the
+    Jacobi / DIIS solution within 1e-8, the reference test's bar
+    (tests/test_spqe.py:80-119), for UCCNPQE and SPQE."""
+    mol, _ = random_problem(3, 11)
+    E = {}
+    for opt in ("jacobi", "BFGS"):
+        a = ucc.UCCNPQE(mol, engine=engine)
+        a.run(pool_type="SD", optimizer=opt, opt_maxiter=50)
+        b = ucc.SPQE(mol, engine=engine)
+        b.run(optimizer=opt, opt_maxiter=50)
+        E[opt] = (a.get_gs_energy(), b.get_gs_energy())
+    for k in range(2):
+        assert abs(E["jacobi"][k] - E["BFGS"][k]) < 1e-8, E
+
+
+def test_scipy_solver_matches_jacobi(host_ucc):
+    check_scipy_matches_jacobi(host_ucc, "percall")
+
+
+def test_unknown_solver_is_refused(host_ucc):
+    mol, _ = random_problem(2, 11)
+    with pytest.raises(NotImplementedError):
+        host_ucc.UCCNPQE(mol, engine="percall").run(optimizer="newton")
