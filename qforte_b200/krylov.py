@@ -363,19 +363,19 @@ class MRSQK(SRQK):
         refs = self._sa_ref_lst if self._use_spin_adapted_refs else \
             [[(1.0, r)] for r in self._single_det_refs]
         omega, homega = [], []
-        Um = None
+        # U_m is the same circuit for every reference: built (and compiled to
+        # a device program) once per m
+        evolutions = [(Circuit(), 1.0)]
+        for m in range(1, self._nstates_per_ref):
+            fact = (0.0 - 1.0j) * m * self._mr_dt
+            evolutions.append(trotterize(self._qb_ham, factor=fact,
+                                         trotter_number=self._trotter_number))
+        Um = evolutions[-1][0]
         for ref in refs:
-            for m in range(self._nstates_per_ref):
-                Um = Circuit()
-                phase1 = 1.0
-                if m > 0:
-                    fact = (0.0 - 1.0j) * m * self._mr_dt
-                    expn_op1, phase1 = trotterize(self._qb_ham, factor=fact,
-                                                  trotter_number=self._trotter_number)
-                    Um.add(expn_op1)
+            for Um_m, phase1 in evolutions:
                 qc = Computer(self._nqb)
                 qc.set_state([(QubitBasis(ref_to_basis_idx(det)), coeff) for coeff, det in ref])
-                qc.apply_circuit(Um)
+                qc.apply_circuit(Um_m)
                 qc.apply_constant(phase1)
                 omega.append(qc)
                 hq = Computer(qc)
