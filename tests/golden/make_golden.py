@@ -341,7 +341,8 @@ def _test_qubit_system(test_file):
 def qite_fixture(qf, test_file, norb, seed, out):
     """QITE (ite/qite.py) run by the reference: the H2 case of its own test
     (beta = 18, Lanczos every 49 steps), the same H2 with the dense cqoy
-    expansion, and a seeded random-integral system with the sparse SD one."""
+    expansion, and a seeded random-integral system with the sparse SD
+    expansion and with the GSD one at two Trotter steps."""
     h2 = _test_qubit_system(test_file)
     H = qf.QubitOperator()
     for c, s in zip(h2["coef_vec"], h2["circ_vec"]):
@@ -363,6 +364,10 @@ def qite_fixture(qf, test_file, norb, seed, out):
     alg.run(beta=0.6, db=0.2, expansion_type="SD", sparseSb=True)
     res["rand_sd_ekb"] = np.array(alg._Ekb)
     res["rand_sd_nparams"] = alg._n_classical_params
+    alg = qf.QITE(s, trotter_number=2)
+    alg.run(beta=0.4, db=0.2, expansion_type="GSD", sparseSb=True)
+    res["rand_gsd_ekb"] = np.array(alg._Ekb)
+    res["rand_gsd_nparams"] = alg._n_classical_params
     alg = qf.QITE(mol, reference=h2["ref"])
     alg.run(beta=0.6, db=0.2, expansion_type="cqoy", sparseSb=False)
     res["h2_cqoy_ekb"] = np.array(alg._Ekb)

@@ -118,7 +118,8 @@ def random_system(d):
 # After its first step the random system's S has 25 of 40 singular values
 # below 1e-10 of the largest, at the least-squares rank cutoff (~7e-14): adding
 # symmetric noise of 1e-16 to S moves the reference's own next energy by up to
-# 5e-8.  Its first step is pinned at E_TOL, later steps at this bound.
+# 5e-8 (the host replay differs by 5.3e-9 with the SD expansion and 2.6e-8 with
+# GSD).  First steps are pinned at E_TOL, later steps at this bound.
 ILL_POSED_TOL = 1e-6
 
 
@@ -141,6 +142,13 @@ def run_cases(qite, d):
     ekb = np.array(alg._Ekb)
     out.append(("random 6 q sparse SD, first step", ekb[:2], d["rand_sd_ekb"][:2], E_TOL))
     out.append(("random 6 q sparse SD, later steps", ekb, d["rand_sd_ekb"], ILL_POSED_TOL))
+    alg = qite.QITE(random_system(d), trotter_number=2)
+    alg.run(beta=0.4, db=0.2, expansion_type="GSD", sparseSb=True)
+    assert alg._n_classical_params == int(d["rand_gsd_nparams"])
+    ekb = np.array(alg._Ekb)
+    out.append(("random 6 q GSD, 2 Trotter steps, first step", ekb[:2], d["rand_gsd_ekb"][:2],
+                E_TOL))
+    out.append(("random 6 q GSD, 2 Trotter steps", ekb, d["rand_gsd_ekb"], ILL_POSED_TOL))
     return out
 
 
