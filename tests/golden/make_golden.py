@@ -401,6 +401,11 @@ def srqk_fixture(qf, test_file, norb, seed, out):
     alg.run(s=3, dt=0.5)
     res.update({"rand_S": alg._S, "rand_H": alg._Hbar,
                 "rand_evals": np.array(alg._eigenvalues), "rand_egs": alg._Egs})
+    alg = qf.SRQK(s, trotter_number=2)
+    # the per-step printout indexes root 1 of a 1x1 problem: run without it
+    alg.run(s=3, dt=0.5, target_root=1, diagonalize_each_step=False)
+    res.update({"rand_t2_S": alg._S, "rand_t2_H": alg._Hbar, "rand_t2_egs": alg._Egs,
+                "rand_t2_ets": alg._Ets})
     # non-Trotterized SRQK (qkd/nt_srqk.py): the H4 case of the same test
     # (s = 4, dt = 0.8) and the random system
     alg = qf.NTSRQK(mol, reference=h4["ref"])

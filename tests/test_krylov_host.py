@@ -65,7 +65,10 @@ def srqk_cases(krylov, d):
     rs.hf_reference = mol.hf_reference
     ar = krylov.SRQK(rs)
     ar.run(s=3, dt=0.5)
-    return [("H4, 100 Trotter steps, s = 6", a4, "h4"), ("random 6 q, s = 3", ar, "rand")]
+    a2 = krylov.SRQK(rs, trotter_number=2)
+    a2.run(s=3, dt=0.5, target_root=1, diagonalize_each_step=False)
+    return [("H4, 100 Trotter steps, s = 6", a4, "h4"), ("random 6 q, s = 3", ar, "rand"),
+            ("random 6 q, 2 Trotter steps, root 1", a2, "rand_t2")]
 
 
 def check_srqk(krylov, d):
@@ -78,7 +81,9 @@ def check_srqk(krylov, d):
             assert abs(egs - float(d["h4_efci"])) < 1e-4, (name, egs)
             assert abs(egs - float(d["h4_egs"])) < H4_EIG_TOL, (name, egs)
         else:
-            assert abs(egs - float(d["rand_egs"])) < RAND_EIG_TOL, (name, egs)
+            assert abs(egs - float(d[f"{p}_egs"])) < RAND_EIG_TOL, (name, egs)
+        if p == "rand_t2":
+            assert abs(alg.get_ts_energy() - float(d["rand_t2_ets"])) < RAND_EIG_TOL, name
 
 
 # Non-Trotterized SRQK: the basis comes from exact time evolution (a Taylor
