@@ -864,8 +864,8 @@ class SPQE(UCCNPQE):
     resulting amplitudes of the pool's determinants.  The micro-iterations take
     their residuals from the evaluator's residual run (engine "fused") or from
     the reference's Computer calls (engine "percall"), solved by Jacobi / DIIS
-    or a scipy minimiser of the summed squared residuals.  Only M_omega = "inf"
-    (exact residuals) is built.
+    or a scipy minimiser of the summed squared residuals.  A finite M_omega
+    estimates the selection residuals from seeded device draws.
     """
 
     def __init__(self, system, reference=None, diis_max_dim=8, irrep=0, **kwargs):
@@ -875,14 +875,16 @@ class SPQE(UCCNPQE):
 
     def run(self, spqe_thresh=1.0e-2, spqe_maxiter=20, dt=0.001, M_omega="inf",
             opt_thresh=1.0e-5, opt_maxiter=30, use_cumulative_thresh=True,
-            max_excit_rank=None, optimizer="Jacobi"):
+            max_excit_rank=None, optimizer="Jacobi", seed=None):
+        """``seed`` (not in the reference, whose draws are unseeded) fixes the
+        device sampler's draws of a finite ``M_omega``: macro-iteration k
+        draws with seed + k."""
         self._check_optimizer(optimizer)
-        if M_omega != "inf":
-            raise NotImplementedError("only exact residuals (M_omega = 'inf') are implemented")
         self._spqe_thresh = spqe_thresh
         self._spqe_maxiter = spqe_maxiter
         self._dt = dt
-        self._M_omega = M_omega
+        self._M_omega = M_omega if M_omega == "inf" else int(M_omega)
+        self._seed = seed
         self._use_cumulative_thresh = use_cumulative_thresh
         self._optimizer = optimizer
         self._opt_thresh = opt_thresh
@@ -966,6 +968,9 @@ class SPQE(UCCNPQE):
         qc.apply_circuit(U)
         qc.apply_circuit(self._eiH)
         qc.apply_circuit(U.adjoint())
+        if self._M_omega != "inf":
+            self._update_ansatz_sampled(qc)
+            return
         coeffs = qc.get_coeff_array()
         in_ansatz = {self._pool_idx_to_coeff_idx[i] for i in self._tops}
         res_sq = [(float(np.real(np.conj(coeffs[I]) * coeffs[I])), I)
@@ -998,6 +1003,42 @@ class SPQE(UCCNPQE):
                     rank = len(self._pool_obj[pool_idx][1].terms()[0][1])
                     self._nbody_counts[rank - 1] += 1
                     break
+        self._n_classical_params_lst.append(len(self._tops))
+
+    def _update_ansatz_sampled(self, qc):
+        """spqe.py:444-503: M_omega draws of basis states from |r_I|^2 estimate
+        the residuals.  The draws come from the device sampler (no read-back of
+        the state); the estimated norm sums every sampled fraction but the
+        largest, and the step converges when one determinant takes every
+        draw.  Otherwise every sampled determinant but the most frequent one
+        enters the ansatz front first, in increasing count order.  Two
+        departures from the reference: a determinant enters only if its
+        operator is not already in the ansatz (the reference compares the
+        determinant's index with the operator indices, so it can add an
+        operator twice), and spqe_maxiter bounds the macro-iterations here as
+        it does with exact residuals (the reference's sampled loop has no
+        bound).  Determinants outside the pool are skipped."""
+        seed = None if self._seed is None else int(self._seed) + self._spqe_iter
+        draws = np.asarray(qc.sample(self._M_omega, seed), dtype=np.int64)
+        mus, counts = np.unique(draws, return_counts=True)
+        nmu = sorted(zip(counts.tolist(), mus.tolist()))
+        frac = [(c / self._M_omega, mu) for c, mu in nmu]
+        self._curr_res_sq_norm = sum(f for f, _ in sorted(frac)[:-1]) / (self._dt * self._dt)
+        if len(nmu) == 1:
+            self._converged = True
+            self._stop_macro = True
+            return
+        if self._spqe_iter > self._spqe_maxiter:
+            self._stop_macro = True
+            return
+        for _, mu in nmu[:-1]:
+            pool_idx = self._coeff_idx_to_pool_idx.get(mu)
+            if pool_idx is None or pool_idx in self._tops:
+                continue
+            self._tops.insert(0, pool_idx)
+            self._tamps.insert(0, 0.0)
+            rank = len(self._pool_obj[pool_idx][1].terms()[0][1])
+            self._nbody_counts[rank - 1] += 1
         self._n_classical_params_lst.append(len(self._tops))
 
     def conv_status(self):

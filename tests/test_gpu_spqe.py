@@ -11,6 +11,7 @@ the selection order matches the reference's (mirror-image determinants tie in
 H4's first selection, so rounding may swap their order: test_spqe_host.py).
 """
 
+import numpy as np
 import pytest
 
 from test_spqe_host import check_spqe
@@ -27,3 +28,17 @@ def test_scipy_solver_matches_jacobi_on_device(cuda):
     from qforte_b200 import ucc
     from test_spqe_host import check_scipy_matches_jacobi
     check_scipy_matches_jacobi(ucc, "fused")
+
+
+def test_sampled_spqe_on_device_matches_oracle_sampler(cuda, monkeypatch):
+    """Sampled SPQE with seeded device draws (qfb_state_sample) selects what
+    the oracle's restatement of the sampler selects from the host replay's
+    state, and reaches the same energies (1e-10)."""
+    from qforte_b200 import ucc
+    from test_qite_host import HostComputer
+    from test_spqe_host import run_sampled
+    dev = run_sampled(ucc, "fused")
+    monkeypatch.setattr(ucc, "Computer", HostComputer)
+    host = run_sampled(ucc, "percall")
+    assert list(dev._tops) == list(host._tops)
+    assert np.max(np.abs(np.array(dev._energies) - np.array(host._energies))) < 1e-10

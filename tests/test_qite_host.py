@@ -56,6 +56,10 @@ class HostComputer:
     def get_coeff_vec(self):
         return list(self.s.psi)
 
+    def sample(self, n, seed=None):
+        from oracle import oracle as O
+        return O.sample_indices(self.s.psi, seed, n)
+
     def set_state(self, state):
         self.s.psi[:] = 0.0
         for b, c in state:

@@ -135,3 +135,38 @@ def test_unknown_solver_is_refused(host_ucc):
     mol, _ = random_problem(2, 11)
     with pytest.raises(NotImplementedError):
         host_ucc.UCCNPQE(mol, engine="percall").run(optimizer="newton")
+
+
+def run_sampled(ucc, engine, seed=5):
+    """Sampled SPQE (finite M_omega) on the random system with seeded draws."""
+    mol, _ = random_problem(3, 11)
+    alg = ucc.SPQE(mol, engine=engine)
+    alg.run(spqe_maxiter=4, spqe_thresh=1.0e-3, dt=0.1, M_omega=20000, opt_thresh=1.0e-7,
+            opt_maxiter=60, seed=seed)
+    return alg
+
+
+def test_sampled_residual_norm_estimates_the_exact_one(host_ucc):
+    """The first selection's sampled norm (every sampled fraction but the
+    largest, over dt^2) estimates the exact one (ucc/spqe.py:444-470) within
+    5 standard errors of its M_omega draws."""
+    mol, _ = random_problem(3, 11)
+
+    def first_selection(**kw):
+        alg = host_ucc.SPQE(mol, engine="percall")
+        # stop after the first selection: no solve, one placeholder energy
+        alg.solve = lambda: alg._energies.append(0.0)
+        alg.run(spqe_maxiter=0, spqe_thresh=1.0e-3, dt=0.1, **kw)
+        return alg
+
+    exact = first_selection()
+    samp = first_selection(M_omega=20000, seed=5)
+    p = exact._curr_res_sq_norm * 0.1 ** 2
+    se = np.sqrt(p * (1 - p) / 20000) / 0.1 ** 2
+    assert abs(samp._curr_res_sq_norm - exact._curr_res_sq_norm) < 5 * se
+
+
+def test_sampled_spqe_host_run(host_ucc):
+    alg = run_sampled(host_ucc, "percall")
+    assert len(alg._energies) >= 1 and len(set(alg._tops)) == len(alg._tops)
+    assert alg._n_classical_params_lst == sorted(alg._n_classical_params_lst)
