@@ -705,6 +705,11 @@ class UCCNPQE(_UCCBase):
 
     _SCIPY_SOLVERS = ("nelder-mead", "powell", "bfgs", "l-bfgs-b", "cg", "slsqp")
 
+    def __init__(self, system, reference=None, max_moment_rank=0, moment_dt=None, **kwargs):
+        super().__init__(system, reference, **kwargs)
+        self._max_moment_rank = max_moment_rank
+        self._moment_dt = moment_dt
+
     def run(self, pool_type="SD", opt_thresh=1.0e-5, opt_maxiter=40, noise_factor=0.0,
             optimizer="jacobi", diis_max_dim=8):
         if pool_type == "sa_SD":
@@ -725,7 +730,61 @@ class UCCNPQE(_UCCBase):
         self.fill_excited_dets()
         self.build_orb_energies()
         self.solve()
+        if self._max_moment_rank:
+            self.construct_moment_space()
+            self.compute_moment_energies()
         return self._Egs
+
+    # ---- moment energy corrections (utils/moment_energy_corrections.py) -------
+    def construct_moment_space(self):
+        """utils/moment_energy_corrections.py:19-98: the determinants of the
+        reference's sector (irrep 0) up to max_moment_rank-fold excitations,
+        with their Moller-Plesset denominators and Epstein-Nesbet diagonal
+        energies <det|H|det>.  The latter are the sums of H's diagonal terms
+        c (-1)^{|det & z|} (only x = 0 strings have diagonal elements), formed
+        from the term table rather than by a state-vector pass per
+        determinant as in the reference."""
+        self._E_mmcc_mp, self._E_mmcc_en = [], []
+        if not hasattr(self, "_orb_e"):
+            self.build_orb_energies()
+        nel = sum(self._ref)
+        if not isinstance(self._max_moment_rank, int) or self._max_moment_rank < 0:
+            raise TypeError("The maximum moment rank must be a non-negative integer!")
+        if self._max_moment_rank > nel:
+            self._max_moment_rank = nel
+        ex = _sector_excitations(self, self._max_moment_rank, 0)
+        self._mmcc_pool = SQOpPool()
+        for _, _, _, sq_op in ex:
+            self._mmcc_pool.add_term(0.0, sq_op)
+        self._mmcc_excitation_indices = [I for I, _, _, _ in ex]
+        self._mpdenom = [sum(self._orb_e[x] for x in occ) - sum(self._orb_e[x] for x in unocc)
+                         for _, occ, unocc, _ in ex]
+        diag = [(complex(c), z) for c, x, z in self._qb_ham._pauli_terms(applied=True) if x == 0]
+        self._epstein_nesbet = [
+            sum(c * (-1.0 if bin(I & z).count("1") & 1 else 1.0) for c, z in diag)
+            for I in self._mmcc_excitation_indices]
+
+    def compute_moment_energies(self):
+        """utils/moment_energy_corrections.py:101-150: residuals of the moment
+        space from U^dagger exp(i dt H) U |ref> / dt, and the MP- and EN-
+        denominator corrected energies."""
+        if self._moment_dt is None:
+            self._moment_dt = 0.001
+        eiH, _ = trotterize(self._qb_ham, factor=self._moment_dt * (0.0 + 1.0j),
+                            trotter_number=self._trotter_number)
+        U = self.ansatz_circuit()
+        qc = Computer(self._nqb)
+        qc.apply_circuit(self._Uprep)
+        qc.apply_circuit(U)
+        qc.apply_circuit(eiH)
+        qc.apply_circuit(U.adjoint())
+        coeffs = qc.get_coeff_array()
+        res = [coeffs[I] / self._moment_dt for I in self._mmcc_excitation_indices]
+        E = self._curr_energy
+        self._E_mmcc_mp.append(E + sum(np.real(np.conj(r) * r / d)
+                                       for r, d in zip(res, self._mpdenom)))
+        self._E_mmcc_en.append(E + sum(np.real(np.conj(r) * r / (E - en))
+                                       for r, en in zip(res, self._epstein_nesbet)))
 
     def _check_optimizer(self, optimizer):
         if optimizer.lower() != "jacobi" and optimizer.lower() not in self._SCIPY_SOLVERS:
@@ -853,6 +912,37 @@ class UCCNPQE(_UCCBase):
         self._Egs = Ek
 
 
+def _sector_excitations(alg, max_rank, irrep):
+    """(basis index, occupied, unoccupied, tau - tau^dagger) for every
+    determinant of the reference's (N_alpha, N_beta) sector and irrep, other
+    than the reference, of excitation rank <= max_rank, in basis-index order
+    (spqe.py:186-240, utils/moment_energy_corrections.py:42-90)."""
+    ref = alg._ref
+    nq = alg._nqb
+    ref_idx = ref_to_basis_idx(ref)
+    nalpha = sum(ref[0::2])
+    nbeta = sum(ref[1::2])
+    irreps = getattr(alg._sys, "orb_irreps_to_int", None) or [0] * (nq // 2 + 1)
+    out = []
+    for I in range(1 << nq):
+        occ = [q for q in range(nq) if I >> q & 1]
+        if sum(1 for q in occ if q % 2 == 0) != nalpha or sum(1 for q in occ if q % 2) != nbeta:
+            continue
+        if find_irrep(irreps, occ) != irrep:
+            continue
+        excit = ref_idx ^ I
+        if excit == 0 or bin(excit).count("1") // 2 > max_rank:
+            continue
+        occ_idx = [q for q in range(nq) if excit >> q & 1 and ref[q] == 1]
+        unocc_idx = [q for q in range(nq) if excit >> q & 1 and ref[q] == 0]
+        sq_op = SQOperator()
+        sq_op.add(+1.0, unocc_idx, occ_idx)
+        sq_op.add(-1.0, occ_idx[::-1], unocc_idx[::-1])
+        sq_op.simplify()
+        out.append((I, occ_idx, unocc_idx, sq_op))
+    return out
+
+
 class SPQE(UCCNPQE):
     """Selected PQE (ucc/spqe.py:24-605): grow the ansatz from the residuals of
     every determinant of the reference's particle-number sector, then solve the
@@ -907,6 +997,8 @@ class SPQE(UCCNPQE):
                 self._nbody_counts.append(0)
         self._build_determinant_pool(max_excit_rank)
         self.build_orb_energies()
+        if self._max_moment_rank:
+            self.construct_moment_space()
         self._spqe_iter = 1
         while not self._stop_macro:
             self.update_ansatz()
@@ -914,6 +1006,8 @@ class SPQE(UCCNPQE):
                 break
             self.fill_excited_dets()
             self.solve()
+            if self._max_moment_rank:
+                self.compute_moment_energies()
             self._spqe_iter += 1
         self._Egs = self._energies[-1]
         return self._Egs
@@ -923,7 +1017,6 @@ class SPQE(UCCNPQE):
         sector and irrep, up to max_excit_rank-fold excitations, in basis-index
         order (spqe.py:159-240): tau - tau^dagger with the determinant's
         creators and annihilators in ascending order."""
-        ref_idx = ref_to_basis_idx(self._ref)
         nalpha = sum(self._ref[0::2])
         nbeta = sum(self._ref[1::2])
         if max_excit_rank is None:
@@ -933,25 +1026,10 @@ class SPQE(UCCNPQE):
         elif max_excit_rank > nalpha + nbeta:
             max_excit_rank = nalpha + nbeta
         self._pool_type = max_excit_rank
-        irreps = getattr(self._sys, "orb_irreps_to_int", None) or [0] * (self._nqb // 2 + 1)
         self._pool_obj = SQOpPool()
         self._coeff_idx_to_pool_idx = {}
         self._indices_of_zeroable_residuals_for_pool = set()
-        for I in range(1 << self._nqb):
-            occ = [q for q in range(self._nqb) if I >> q & 1]
-            if sum(1 for q in occ if q % 2 == 0) != nalpha or sum(1 for q in occ if q % 2) != nbeta:
-                continue
-            if find_irrep(irreps, occ) != self._irrep:
-                continue
-            excit = ref_idx ^ I
-            if excit == 0 or bin(excit).count("1") // 2 > max_excit_rank:
-                continue
-            occ_idx = [q for q in range(self._nqb) if excit >> q & 1 and self._ref[q] == 1]
-            unocc_idx = [q for q in range(self._nqb) if excit >> q & 1 and self._ref[q] == 0]
-            sq_op = SQOperator()
-            sq_op.add(+1.0, unocc_idx, occ_idx)
-            sq_op.add(-1.0, occ_idx[::-1], unocc_idx[::-1])
-            sq_op.simplify()
+        for I, _, _, sq_op in _sector_excitations(self, max_excit_rank, self._irrep):
             self._coeff_idx_to_pool_idx[I] = len(self._pool_obj)
             self._indices_of_zeroable_residuals_for_pool.add(I)
             self._pool_obj.add_term(0.0, sq_op)

@@ -452,6 +452,17 @@ def spqe_fixture(qf, tests_dir, norb, seed, out):
     res.update({"rand_egs": alg.get_gs_energy(), "rand_energies": np.array(alg._energies),
                 "rand_nparams": np.array(alg._n_classical_params_lst),
                 "rand_tops": np.array(alg._tops), "rand_npool": len(alg._pool_obj)})
+    # moment energy corrections (utils/moment_energy_corrections.py) on H4:
+    # UCCNPQE with the SD pool and SPQE, moments up to quadruples
+    alg = qf.UCCNPQE(mol, max_moment_rank=4, moment_dt=0.001)
+    alg.run(pool_type="SD", opt_thresh=1.0e-7, opt_maxiter=60)
+    res.update({"mmcc_pqe_egs": alg.get_gs_energy(), "mmcc_pqe_mp": np.array(alg._E_mmcc_mp),
+                "mmcc_pqe_en": np.array(alg._E_mmcc_en),
+                "mmcc_pqe_en_diag": np.real(np.array(alg._epstein_nesbet)),
+                "mmcc_pqe_mpdenom": np.array(alg._mpdenom)})
+    alg = qf.SPQE(mol, max_moment_rank=4, moment_dt=0.001)
+    alg.run(spqe_maxiter=20, spqe_thresh=1.0e-2, opt_thresh=1.0e-5, dt=0.0001)
+    res.update({"mmcc_spqe_mp": np.array(alg._E_mmcc_mp), "mmcc_spqe_en": np.array(alg._E_mmcc_en)})
     np.savez_compressed(out, norb=norb, seed=seed, **res)
     print(f"{out}: H4 SPQE E = {res['h4_egs']} ({len(res['h4_energies'])} macro-iterations, "
           f"params {res['h4_nparams']}); random E = {res['rand_egs']}, params {res['rand_nparams']}")

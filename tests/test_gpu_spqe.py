@@ -42,3 +42,9 @@ def test_sampled_spqe_on_device_matches_oracle_sampler(cuda, monkeypatch):
     host = run_sampled(ucc, "percall")
     assert list(dev._tops) == list(host._tops)
     assert np.max(np.abs(np.array(dev._energies) - np.array(host._energies))) < 1e-10
+
+
+def test_moment_corrections_on_device(cuda):
+    from qforte_b200 import ucc
+    from test_spqe_host import check_moments
+    check_moments(ucc, "fused", strict=False)

@@ -170,3 +170,28 @@ def test_sampled_spqe_host_run(host_ucc):
     alg = run_sampled(host_ucc, "percall")
     assert len(alg._energies) >= 1 and len(set(alg._tops)) == len(alg._tops)
     assert alg._n_classical_params_lst == sorted(alg._n_classical_params_lst)
+
+
+def check_moments(ucc, engine, strict=True):
+    """Moment energy corrections (utils/moment_energy_corrections.py) on H4:
+    UCCNPQE with the SD pool and SPQE, moments up to quadruples, against the
+    reference's runs: denominators 1e-12, energies 1e-10 (SPQE's where its
+    selection order matches the reference's, see the module docstring)."""
+    d = golden("spqe_norb3_seed11.npz")
+    a = ucc.UCCNPQE(h4_system(), max_moment_rank=4, moment_dt=0.001, engine=engine)
+    a.run(pool_type="SD", opt_thresh=1.0e-7, opt_maxiter=60)
+    assert abs(a.get_gs_energy() - float(d["mmcc_pqe_egs"])) < E_TOL
+    assert np.max(np.abs(np.array(a._mpdenom) - d["mmcc_pqe_mpdenom"])) < 1e-12
+    assert np.max(np.abs(np.real(a._epstein_nesbet) - d["mmcc_pqe_en_diag"])) < 1e-12
+    for ours, key in ((a._E_mmcc_mp, "mmcc_pqe_mp"), (a._E_mmcc_en, "mmcc_pqe_en")):
+        assert np.max(np.abs(np.array(ours) - d[key])) < E_TOL, key
+    b = ucc.SPQE(h4_system(), max_moment_rank=4, moment_dt=0.001, engine=engine)
+    b.run(spqe_maxiter=20, spqe_thresh=1.0e-2, opt_thresh=1.0e-5, dt=0.0001)
+    for ours, key in ((b._E_mmcc_mp, "mmcc_spqe_mp"), (b._E_mmcc_en, "mmcc_spqe_en")):
+        assert len(ours) == len(d[key]), key
+        if strict:
+            assert np.max(np.abs(np.array(ours) - d[key])) < E_TOL, key
+
+
+def test_moment_corrections_match_reference(host_ucc):
+    check_moments(host_ucc, "percall")
