@@ -923,11 +923,14 @@ def _sector_excitations(alg, max_rank, irrep):
     nalpha = sum(ref[0::2])
     nbeta = sum(ref[1::2])
     irreps = getattr(alg._sys, "orb_irreps_to_int", None) or [0] * (nq // 2 + 1)
+    # the sector's determinants (alpha strings x beta strings) in basis-index
+    # order: the reference scans all 2^n indices for them
+    from itertools import combinations
+    alpha_strings = [sum(1 << q for q in c) for c in combinations(range(0, nq, 2), nalpha)]
+    beta_strings = [sum(1 << q for q in c) for c in combinations(range(1, nq, 2), nbeta)]
     out = []
-    for I in range(1 << nq):
+    for I in sorted(a | b for a in alpha_strings for b in beta_strings):
         occ = [q for q in range(nq) if I >> q & 1]
-        if sum(1 for q in occ if q % 2 == 0) != nalpha or sum(1 for q in occ if q % 2) != nbeta:
-            continue
         if find_irrep(irreps, occ) != irrep:
             continue
         excit = ref_idx ^ I

@@ -195,3 +195,36 @@ def check_moments(ucc, engine, strict=True):
 
 def test_moment_corrections_match_reference(host_ucc):
     check_moments(host_ucc, "percall")
+
+
+def test_sector_enumeration_equals_the_full_scan():
+    """The determinant pool from alpha x beta strings equals the reference's
+    scan over every basis index (spqe.py:186-240) with its filters."""
+    import qforte_b200 as qb
+    from qforte_b200.ucc import _sector_excitations
+
+    class Alg:
+        pass
+
+    for ref, irreps in (([1, 1, 1, 0, 0, 0, 0, 0], [0, 1, 0, 1]),
+                        ([1, 1, 1, 1, 0, 0, 0, 0, 0, 0], [0, 0, 0, 0, 0])):
+        alg = Alg()
+        alg._ref, alg._nqb = ref, len(ref)
+        alg._sys = qb.Molecule()
+        alg._sys.orb_irreps_to_int = irreps
+        nq = len(ref)
+        ref_idx = sum(b << q for q, b in enumerate(ref))
+        for rank, irrep in ((nq, 0), (2, 0), (3, 1)):
+            want = []
+            for I in range(1 << nq):
+                occ = [q for q in range(nq) if I >> q & 1]
+                if (sum(1 for q in occ if q % 2 == 0) != sum(ref[0::2])
+                        or sum(1 for q in occ if q % 2) != sum(ref[1::2])):
+                    continue
+                if qb.find_irrep(irreps, occ) != irrep:
+                    continue
+                ex = ref_idx ^ I
+                if ex and bin(ex).count("1") // 2 <= rank:
+                    want.append(I)
+            got = [I for I, _, _, _ in _sector_excitations(alg, rank, irrep)]
+            assert got == want, (ref, rank, irrep)
