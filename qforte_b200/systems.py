@@ -20,7 +20,7 @@ import numpy as np
 
 from .sq_operator import SQOperator
 
-__all__ = ["Molecule", "random_integrals", "random_molecule", "sq_hamiltonian",
+__all__ = ["Molecule", "create_TFIM", "random_integrals", "random_molecule", "sq_hamiltonian",
            "create_external_mol", "system_factory", "hf_reference"]
 
 
@@ -136,9 +136,30 @@ def create_external_mol(**kwargs):
     return mol
 
 
+def create_TFIM(n, h, J):
+    """1D transverse-field Ising model with open boundaries
+    (adapters/model_adapters.py:5-31): H = -h sum_i Z_i - J sum_i X_i X_{i+1},
+    reference |0...0>."""
+    from .qubit_operator import QubitOperator
+    from .utils import build_circuit
+    tfim = Molecule()
+    tfim.hamiltonian = QubitOperator()
+    terms = [(-h, f"Z_{i}") for i in range(n)] + [(-J, f"X_{i} X_{i + 1}") for i in range(n - 1)]
+    for coeff, op_str in terms:
+        tfim.hamiltonian.add(coeff, build_circuit(op_str))
+    tfim.hf_reference = [0] * n
+    return tfim
+
+
 def system_factory(system_type="molecule", build_type="external", **kwargs):
+    """system/system_factory.py:5-57: molecules from external integrals (or,
+    here, seeded random integrals; psi4 is not available) and the TFIM model."""
+    if system_type == "model":
+        if build_type != "TFIM":
+            raise TypeError(f"build type {build_type} not supported, supported types are: TFIM")
+        return create_TFIM(**kwargs)
     if system_type != "molecule":
-        raise TypeError("system type not supported, supported types are 'molecule'.")
+        raise TypeError("system type not supported, supported types are 'molecule' and 'model'.")
     if build_type == "external":
         return create_external_mol(**kwargs)
     if build_type == "random":

@@ -168,3 +168,20 @@ def test_compact_excitation_circuits_match_reference(pool_type, qe):
     assert tg == z[f"{key}_target"].tolist() and ct == z[f"{key}_control"].tolist()
     assert pr == z[f"{key}_param"].tolist()
     assert U.get_num_cnots() == int(z[f"{key}_cnots"])
+
+
+def test_tfim_model_matches_reference(ref_qforte):
+    """system_factory(system_type="model", build_type="TFIM") builds the
+    reference's transverse-field Ising Hamiltonian (adapters/model_adapters.py:
+    5-31): same terms in the same order, same reference determinant."""
+    import qforte_b200 as qb
+    from qforte.adapters.model_adapters import create_TFIM
+    for n, h, J in ((4, 1.0, 0.5), (7, 0.3, -1.2)):
+        ours = qb.system_factory(system_type="model", build_type="TFIM", n=n, h=h, J=J)
+        ref = create_TFIM(n, h, J)
+        assert ours.hf_reference == ref.hf_reference
+        a = [(complex(c), [(g.gate_id(), g.target()) for g in circ.gates()])
+             for c, circ in ours.hamiltonian.terms()]
+        b = [(complex(c), [(g.gate_id(), g.target()) for g in circ.gates()])
+             for c, circ in ref.hamiltonian.terms()]
+        assert a == b
