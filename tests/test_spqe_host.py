@@ -228,3 +228,26 @@ def test_sector_enumeration_equals_the_full_scan():
                     want.append(I)
             got = [I for I, _, _, _ in _sector_excitations(alg, rank, irrep)]
             assert got == want, (ref, rank, irrep)
+
+
+def test_driver_argument_errors_match_the_reference(host_ucc, monkeypatch):
+    """The exceptions the reference's drivers raise for bad arguments:
+    QITE expansion types (ite/qite.py:214-254), SPQE's max_excit_rank
+    (spqe.py:172-185), MRSQK's reference generator (qkd/mrsqk.py:176-190)."""
+    import qforte_b200 as qb
+    from qforte_b200 import krylov, qite
+    monkeypatch.setattr(qite, "Computer", HostComputer)
+    mol, _ = random_problem(2, 11)
+    with pytest.raises(ValueError):
+        qite.QITE(mol).run(expansion_type="SDX")
+    big = qb.system_factory(system_type="model", build_type="TFIM", n=7, h=1.0, J=1.0)
+    with pytest.raises(ValueError):
+        qite.QITE(big).run(expansion_type="complete_qubit")
+    with pytest.raises(TypeError):
+        host_ucc.SPQE(mol, engine="percall").run(max_excit_rank=0)
+    with pytest.raises(TypeError):
+        host_ucc.SPQE(mol, engine="percall").run(max_excit_rank=1.5)
+    with pytest.raises(ValueError):
+        krylov.MRSQK(mol).run(reference_generator="ACI")
+    with pytest.raises(TypeError):
+        qb.system_factory(system_type="lattice")
