@@ -368,6 +368,12 @@ def qite_fixture(qf, test_file, norb, seed, out):
     alg.run(beta=0.4, db=0.2, expansion_type="GSD", sparseSb=True)
     res["rand_gsd_ekb"] = np.array(alg._Ekb)
     res["rand_gsd_nparams"] = alg._n_classical_params
+    # the transverse-field Ising model (adapters/model_adapters.py), cqoy expansion
+    from qforte.adapters.model_adapters import create_TFIM
+    alg = qf.QITE(create_TFIM(4, 1.0, 0.7))
+    alg.run(beta=0.6, db=0.2, expansion_type="cqoy", sparseSb=True)
+    res["tfim_ekb"] = np.array(alg._Ekb)
+    res["tfim_nparams"] = alg._n_classical_params
     alg = qf.QITE(mol, reference=h2["ref"])
     alg.run(beta=0.6, db=0.2, expansion_type="cqoy", sparseSb=False)
     res["h2_cqoy_ekb"] = np.array(alg._Ekb)

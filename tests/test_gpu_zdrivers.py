@@ -13,9 +13,10 @@ qfb_sum_apply, the Trotter step through Computer.apply_circuit and the Lanczos
 overlaps as device inner products.  Golden values: tests/golden/
 qite_norb3_seed11.npz, written by the reference's QITE (ite/qite.py); the H2 run
 also meets the reference test's FCI pin (tests/test_qite.py:6-81) within 1e-10.
-Tolerances: energies 1e-10, except the random system's steps after the first,
-where the reference's own least-squares solve moves by up to 5e-8 under 1e-16
-changes of S (bound 1e-6, measured in test_qite_host.py).
+Tolerances: the H2 SD run and its Lanczos energy 1e-10.  The cases whose
+least-squares steps are ill-posed (H2 cqoy, random SD and GSD) get 1e-3: noise
+of 1e-15 on S and b moves the reference's own energies by up to 9.5e-5 there
+(measured in test_qite_host.py).
 
 SRQK, NTSRQK and MRSQK on the device against the reference's own runs.
 
@@ -58,7 +59,7 @@ pytestmark = pytest.mark.gpu
 def test_qite_on_device_matches_reference(cuda):
     from qforte_b200 import qite
     d = golden("qite_norb3_seed11.npz")
-    for name, ours, ref, tol in run_cases(qite, d):
+    for name, ours, ref, tol in run_cases(qite, d, device=True):
         assert ours.shape == ref.shape, name
         assert np.max(np.abs(ours - ref)) < tol, (name, np.max(np.abs(ours - ref)))
 

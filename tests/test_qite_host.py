@@ -127,8 +127,22 @@ def random_system(d):
 ILL_POSED_TOL = 1e-6
 
 
-def run_cases(qite, d):
-    """The fixture's reference runs; returns (name, ours, golden, tolerance)."""
+# Three cases are ill-posed from their first step.  Symmetric noise of 1e-16 on
+# S and b moves the reference's own energies by up to 3.1e-6 (H2 cqoy) and
+# 1.2e-5 (random GSD), and noise of 1e-15 moves them by up to 9.5e-5, 9.8e-6 and
+# 5.2e-6 (random SD).  The counts of operators above x_thresh change too (H2
+# cqoy 127 -> 240, random GSD 377-388).  The H2 SD run and its Lanczos energy
+# move by under 2e-14 at either noise level.  The host replay forms S and b with
+# the reference's arithmetic and reproduces the ill-posed cases exactly.  On
+# the device, whose rounding is its own, they are held to this bound, and
+# their counts are not compared.
+DEVICE_ILL_POSED_TOL = 1e-3
+
+
+def run_cases(qite, d, device=False):
+    """The fixture's reference runs; returns (name, ours, golden, tolerance).
+    ``device``: the state is on the GPU, whose rounding differs from the
+    reference's (bounds of the ill-posed cases as stated above)."""
     out = []
     alg = qite.QITE(h2_system(d))
     alg.run(beta=18.0, do_lanczos=True, lanczos_gap=49)
@@ -138,21 +152,30 @@ def run_cases(qite, d):
     assert abs(alg.get_gs_energy() - float(d["h2_efci"])) < E_TOL
     alg = qite.QITE(h2_system(d))
     alg.run(beta=0.6, db=0.2, expansion_type="cqoy", sparseSb=False)
-    assert alg._n_classical_params == int(d["h2_cqoy_nparams"])
-    out.append(("H2 dense cqoy", np.array(alg._Ekb), d["h2_cqoy_ekb"], E_TOL))
+    if not device:
+        assert alg._n_classical_params == int(d["h2_cqoy_nparams"])
+    out.append(("H2 dense cqoy", np.array(alg._Ekb), d["h2_cqoy_ekb"],
+                DEVICE_ILL_POSED_TOL if device else E_TOL))
     alg = qite.QITE(random_system(d))
     alg.run(beta=0.6, db=0.2, expansion_type="SD", sparseSb=True)
-    assert alg._n_classical_params == int(d["rand_sd_nparams"])
+    assert device or alg._n_classical_params == int(d["rand_sd_nparams"])
     ekb = np.array(alg._Ekb)
-    out.append(("random 6 q sparse SD, first step", ekb[:2], d["rand_sd_ekb"][:2], E_TOL))
-    out.append(("random 6 q sparse SD, later steps", ekb, d["rand_sd_ekb"], ILL_POSED_TOL))
+    if device:
+        out.append(("random 6 q sparse SD", ekb, d["rand_sd_ekb"], DEVICE_ILL_POSED_TOL))
+    else:
+        out.append(("random 6 q sparse SD, first step", ekb[:2], d["rand_sd_ekb"][:2], E_TOL))
+        out.append(("random 6 q sparse SD, later steps", ekb, d["rand_sd_ekb"], ILL_POSED_TOL))
     alg = qite.QITE(random_system(d), trotter_number=2)
     alg.run(beta=0.4, db=0.2, expansion_type="GSD", sparseSb=True)
-    assert alg._n_classical_params == int(d["rand_gsd_nparams"])
     ekb = np.array(alg._Ekb)
-    out.append(("random 6 q GSD, 2 Trotter steps, first step", ekb[:2], d["rand_gsd_ekb"][:2],
-                E_TOL))
-    out.append(("random 6 q GSD, 2 Trotter steps", ekb, d["rand_gsd_ekb"], ILL_POSED_TOL))
+    if device:
+        out.append(("random 6 q GSD, 2 Trotter steps", ekb, d["rand_gsd_ekb"],
+                    DEVICE_ILL_POSED_TOL))
+    else:
+        assert alg._n_classical_params == int(d["rand_gsd_nparams"])
+        out.append(("random 6 q GSD, 2 Trotter steps, first step", ekb[:2],
+                    d["rand_gsd_ekb"][:2], E_TOL))
+        out.append(("random 6 q GSD, 2 Trotter steps", ekb, d["rand_gsd_ekb"], ILL_POSED_TOL))
     return out
 
 
@@ -161,6 +184,21 @@ def test_qite_host_replay_matches_reference(host_qite):
     for name, ours, ref, tol in run_cases(host_qite, d):
         assert ours.shape == ref.shape, name
         assert np.max(np.abs(ours - ref)) < tol, (name, np.max(np.abs(ours - ref)))
+
+
+def test_qite_tfim_host_replay_matches_reference(host_qite):
+    """QITE on the 4-site transverse-field Ising model with the cqoy expansion.
+    Its least-squares steps are so ill-posed that symmetric noise of 1e-16 on S
+    moves the reference's own energies by up to 1.3e-4.  So the case is pinned
+    only here, where the replay forms S with the reference's arithmetic and
+    reproduces its energies bit for bit; the device's rounding would not."""
+    import qforte_b200 as qb
+    d = golden("qite_norb3_seed11.npz")
+    alg = host_qite.QITE(qb.system_factory(system_type="model", build_type="TFIM", n=4,
+                                           h=1.0, J=0.7))
+    alg.run(beta=0.6, db=0.2, expansion_type="cqoy", sparseSb=True)
+    assert alg._n_classical_params == int(d["tfim_nparams"])
+    assert np.max(np.abs(np.array(alg._Ekb) - d["tfim_ekb"])) < E_TOL
 
 
 def test_S_products_equal_dense_overlaps(host_qite):
