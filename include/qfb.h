@@ -73,6 +73,12 @@ QFB_API int qfb_set_stream(void *stream);
 QFB_API int qfb_sync(void);
 /* Count of kernels this library launched in this process (evidence counter). */
 QFB_API int qfb_launch_count(uint64_t *out);
+/* How long a gate tile waits for its bulk load copies before it gives up,
+ * flags the failure and leaves its tile unwritten (reported as QFB_ETIMEDOUT
+ * by the next qfb_sync or state download).  Default 2 s; at most 60 s; 0
+ * gives up without waiting, which lets a test exercise that path with no
+ * fault.  No counterpart in the reference (its CPU loops never wait). */
+QFB_API int qfb_set_tile_wait_limit(uint64_t ns);
 
 /* ---- states: Computer::Computer / copy ctor / reset / null_state ----------
  * computer.cc:28-54, computer.h:28.  nbatch > 1 holds nbatch independent

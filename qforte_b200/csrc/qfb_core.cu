@@ -882,13 +882,23 @@ static int check_device_waits() {
     QFB_CUDA(cudaMemcpyToSymbolAsync(qfbt::g_tile_wait_err, &zero, sizeof(int), 0,
                                      cudaMemcpyHostToDevice, t_stream));
     QFB_CUDA(cudaStreamSynchronize(t_stream));
-    return fail(QFB_ETIMEDOUT, "a gate tile's bulk copies did not complete within 2 s; "
-                               "the state is not valid");
+    return fail(QFB_ETIMEDOUT, "a gate tile's bulk copies did not complete within the wait "
+                               "limit; the state is not valid");
 }
 
 int qfb_sync(void) {
     QFB_CUDA(cudaStreamSynchronize(t_stream));
     return check_device_waits();
+}
+
+int qfb_set_tile_wait_limit(uint64_t ns) {
+    if (ns > 60000000000ull)
+        return fail(QFB_EINVAL, "qfb_set_tile_wait_limit: %llu ns is above the 60 s bound",
+                    (unsigned long long)ns);
+    QFB_CUDA(cudaMemcpyToSymbolAsync(qfbt::g_tile_wait_limit_ns, &ns, sizeof(ns), 0,
+                                     cudaMemcpyHostToDevice, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
 }
 
 int qfb_launch_count(uint64_t *out) {

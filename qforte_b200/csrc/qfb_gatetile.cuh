@@ -378,6 +378,13 @@ static __device__ int g_tile_wait_err = 0;
 
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 
+// How long a tile waits for its load copies before it gives up (default
+// kWaitLimitNs; 0: give up without waiting, so a test can make the wait run
+// out without any fault).  Only the first wait reads it: the wait that keeps
+// the copies in flight from landing after the CTA exits always allows
+// kWaitLimitNs.
+static __device__ uint64_t g_tile_wait_limit_ns = kWaitLimitNs;
+
 // One CTA per tile (blockIdx.x: tile position over the qubits outside Q;
 // blockIdx.y: batch slot); 2^(b-R) threads, 2^R amplitudes each.
 template <int R>
@@ -406,10 +413,11 @@ __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
     const uint64_t *ch = chunks + run.ch0;
     for (int c = tid; c < nch; c += nth)
         bulk_g2s(smem_u32(tile + tpad((uint32_t)c << 3)), s + __ldg(&ch[c]), 128u, bar_a);
-    if (!mbar_wait_bounded(bar_a, 0, kWaitLimitNs)) {
-        // the copies never completed: flag it, give them a second bounded
-        // wait so none lands after this CTA's shared memory is released, and
-        // leave the tile unwritten
+    const uint64_t limit = g_tile_wait_limit_ns;
+    if (limit == 0 || !mbar_wait_bounded(bar_a, 0, limit)) {
+        // the copies did not complete in time: flag it, give them a second
+        // bounded wait so none lands after this CTA's shared memory is
+        // released, and leave the tile unwritten
         if (tid == 0) atomicExch(&g_tile_wait_err, 1);
         mbar_wait_bounded(bar_a, 0, kWaitLimitNs);
         return;

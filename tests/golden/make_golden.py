@@ -3,7 +3,9 @@
 Run in a container that holds the reference sources (read where they lie) and
 its compiled module (``make -C oracle ref``):
 
-    python tests/golden/make_golden.py [--ref-src /root/reference/src/qforte]
+    python tests/golden/make_golden.py [--ref-src DIR] [--only FAMILY]
+
+DIR defaults to $QFORTE_REF_SRC, else /root/reference/src/qforte.
 
 Every output comes from the reference's own code path -- its C++ ``Computer``,
 ``SQOperator.jw_transform``, ``SQOpPool`` and its Python UCC drivers -- on
@@ -515,10 +517,125 @@ def mrsqk_fixture(qf, test_file, norb, seed, out):
           f"{res['rand_sa_egs']}, single-reference E = {res['rand_egs']}")
 
 
+def oppl_fixture(qf, norb, seed, out):
+    """Computer.direct_oppl_exp_val / direct_idxd_oppl_exp_val (computer.cc:773-806)
+    on the commutator pool of UCCVQE.fill_commutator_pool (uccvqeabc.py:85-89):
+    every [H, A_k] of the GSD pool at a seeded 3-operator dUCC state, and an
+    indexed subset in a scrambled order."""
+    h, g = random_integrals(norb, seed)
+    H = ref_sq_ham(qf, h, g).jw_transform()
+    ref = hf_reference(norb, norb)
+    rng = np.random.default_rng(3000 + seed)
+    alg = make_alg(qf, H, ref, "GSD")
+    P = len(alg._pool_obj)
+    tops = [int(t) for t in rng.choice(P, 3, replace=False)]
+    amps = rng.uniform(-0.2, 0.2, 3)
+    alg._tops, alg._tamps = tops, list(amps)
+    comm = alg._pool_obj.get_qubit_op_pool()
+    comm.join_as_commutator(H)
+    qc = qf.Computer(2 * norb)
+    qc.apply_circuit(alg.build_Uvqc(list(amps)))
+    psi = np.array(qc.get_coeff_vec())
+    vals = np.array(qc.direct_oppl_exp_val(comm))
+    idxs = [int(i) for i in rng.permutation(P)[:P // 3]]
+    ivals = np.array(qc.direct_idxd_oppl_exp_val(comm, idxs))
+    np.savez_compressed(out, norb=norb, seed=seed, tops=np.array(tops), amps=amps, psi=psi,
+                        oppl=vals, idxs=np.array(idxs), idxd_oppl=ivals)
+    print(f"{out}: {P} commutators, max |<[H,A]>| = {np.max(np.abs(vals)):.3e}")
+
+
+def bench_ucc_fixture(qf, norb, seed, batch, rows, out):
+    """The default benchmark's problem: dUCCSD energy (AnsatzAlgorithm.energy_feval,
+    algorithm.py:458-474) and adjoint gradient (UCCVQE.measure_gradient,
+    uccvqeabc.py:122-251) of the listed rows of the benchmark's parameter matrix,
+    default_rng(seed + 1).uniform(-0.1, 0.1, (batch, M))."""
+    h, g = random_integrals(norb, seed)
+    H = ref_sq_ham(qf, h, g).jw_transform()
+    ref = hf_reference(norb, norb)
+    alg = make_alg(qf, H, ref, "SD")
+    M = len(alg._pool_obj)
+    P = np.random.default_rng(seed + 1).uniform(-0.1, 0.1, (batch, M))
+    alg._tops = list(range(M))
+    E, G = [], []
+    for r in rows:
+        alg._tamps = list(P[r])
+        E.append(alg.energy_feval(list(P[r])))
+        G.append(np.array(alg.measure_gradient(list(P[r]))))
+    np.savez_compressed(out, norb=norb, seed=seed, batch=batch, rows=np.array(rows),
+                        nterms=len(H.terms()), energies=np.array(E), grads=np.array(G))
+    print(f"{out}: rows {rows}: E = {E}, |g|max = {[float(np.max(np.abs(x))) for x in G]}")
+
+
+def grad_fixture(qf, norb, seed, out):
+    """Adjoint dUCCSD gradient at 2 norb qubits (UCCVQE.measure_gradient) at row
+    0 of default_rng(seed + norb).uniform(-0.1, 0.1, (B, M)), the amplitudes
+    the differentiation workload starts from, with its energy."""
+    h, g = random_integrals(norb, seed)
+    H = ref_sq_ham(qf, h, g).jw_transform()
+    ref = hf_reference(norb, norb)
+    alg = make_alg(qf, H, ref, "SD")
+    M = len(alg._pool_obj)
+    amps = np.random.default_rng(seed + norb).uniform(-0.1, 0.1, (1, M))[0]
+    alg._tops = list(range(M))
+    alg._tamps = list(amps)
+    E = alg.energy_feval(list(amps))
+    G = np.array(alg.measure_gradient(list(amps)))
+    np.savez_compressed(out, norb=norb, seed=seed, nterms=len(H.terms()), amps=amps,
+                        energy=E, grad=G)
+    print(f"{out}: {M} parameters, E = {E:.12f}, |g|max = {np.max(np.abs(G)):.3e}")
+
+
+def adapt_fixture(qf, norb, seed, out):
+    """ADAPT pool gradients 2 Re <H psi|A_k psi> (UCCVQE.measure_gradient3,
+    uccvqeabc.py:253-283) of the whole GSD pool at the 12-operator dUCC state
+    of the pool-gradient workload: operators rng.choice(P, 12) and amplitudes
+    U(-0.1, 0.1) from default_rng(seed + 7)."""
+    h, g = random_integrals(norb, seed)
+    H = ref_sq_ham(qf, h, g).jw_transform()
+    ref = hf_reference(norb, norb)
+    alg = make_alg(qf, H, ref, "GSD")
+    P = len(alg._pool_obj)
+    rng = np.random.default_rng(seed + 7)
+    tops = [int(v) for v in rng.choice(P, 12, replace=False)]
+    amps = rng.uniform(-0.1, 0.1, 12)
+    alg._tops, alg._tamps = tops, list(amps)
+    G = np.array(alg.measure_gradient3())
+    np.savez_compressed(out, norb=norb, seed=seed, tops=np.array(tops), amps=amps,
+                        pool_grads=G)
+    print(f"{out}: {P} pool gradients, |g|max = {np.max(np.abs(G)):.3e}")
+
+
+def sweep_fixture(qf, n, layers, seed, out):
+    """The gate-application sweep (Computer.apply_circuit, computer.cc:93-114) of
+    qforte_b200.workloads.layered_random_circuit(n, layers, seed) from |0...0>:
+    the state's norm, 4,096 amplitudes at seeded indices, <Z_k> for every qubit
+    and the probability mass of each value of the top 8 qubits."""
+    from qforte_b200.workloads import layered_random_circuit
+    _, spec = layered_random_circuit(n, layers, seed)
+    circ = qf.Circuit()
+    for k, t, c, p in spec:
+        circ.add(qf.gate(k, t, c, p))
+    qc = qf.Computer(n)
+    qc.apply_circuit(circ)
+    psi = np.array(qc.get_coeff_vec())
+    del qc
+    prob = psi.real ** 2 + psi.imag ** 2
+    idx = np.sort(np.random.default_rng(seed + 500).choice(1 << n, 4096, replace=False))
+    zk = np.array([prob.reshape(-1, 2, 1 << k)[:, 0, :].sum() -
+                   prob.reshape(-1, 2, 1 << k)[:, 1, :].sum() for k in range(n)])
+    top = prob.reshape(256, -1).sum(axis=1)
+    np.savez_compressed(out, n=n, layers=layers, seed=seed, ngates=len(spec),
+                        norm=np.sqrt(prob.sum()), idx=idx, amps=psi[idx], z=zk, top8=top)
+    print(f"{out}: {len(spec)} gates on {n} qubits, norm - 1 = {np.sqrt(prob.sum()) - 1:.2e}")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-src", default="/root/reference/src/qforte")
-    ap.add_argument("--only", default=None, help="one fixture family (pqe, compact, qite, srqk, spqe, mrsqk)")
+    ap.add_argument("--ref-src", default=os.environ.get("QFORTE_REF_SRC",
+                                                        "/root/reference/src/qforte"))
+    ap.add_argument("--only", default=None,
+                    help="one fixture family (pqe, compact, qite, srqk, spqe, mrsqk, oppl, "
+                         "bench16, grad20, adapt20, sweep20, sweep24)")
     a = ap.parse_args()
     qf = O.load_reference(a.ref_src)
     tests_dir = os.path.join(os.path.dirname(a.ref_src.rstrip("/")), "..", "tests")
@@ -538,6 +655,18 @@ def main():
     if a.only in ("mrsqk", None):
         mrsqk_fixture(qf, os.path.join(tests_dir, "test_fast_qk.py"), 3, 11,
                       os.path.join(HERE, "mrsqk_norb3_seed11.npz"))
+    if a.only in ("oppl", None):
+        oppl_fixture(qf, 4, 11, os.path.join(HERE, "oppl_norb4_seed11.npz"))
+    # the benchmarked configurations themselves (minutes to an hour each on one core)
+    if a.only == "bench16":
+        bench_ucc_fixture(qf, 8, 11, 256, (0, 255), os.path.join(HERE, "bench_ucc16_seed11.npz"))
+    if a.only == "grad20":
+        grad_fixture(qf, 10, 11, os.path.join(HERE, "grad_ucc20_seed11.npz"))
+    if a.only == "adapt20":
+        adapt_fixture(qf, 10, 11, os.path.join(HERE, "adapt_gsd20_seed11.npz"))
+    for n in (20, 24, 28):
+        if a.only == f"sweep{n}":
+            sweep_fixture(qf, n, 100, 11 + n, os.path.join(HERE, f"sweep{n}_seed{11 + n}.npz"))
     if a.only is not None:
         return
     ucc_fixture(qf, 4, 11, os.path.join(HERE, "ucc_norb4_seed11.npz"))

@@ -346,6 +346,44 @@ def test_gate_windows_match_oracle(cuda, gate_tiles, tile, low, n, ngates, seed)
     assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
 
 
+def test_gate_tile_wait_that_runs_out_reports_and_leaves_state(cuda, gate_tiles):
+    """The tile kernel's bounded wait for its bulk load copies, made to run out
+    with no fault: with the wait limit at 0 every tile gives up at once, flags
+    it and leaves its tile unwritten.  The next download reports
+    QFB_ETIMEDOUT (RuntimeError), the state is exactly as before, and with the
+    limit restored the same circuit gives the oracle's state."""
+    from qforte_b200._lib import QFB_ETIMEDOUT, check, lib
+    from qforte_b200.device import gate_plan
+    gate_tiles(0, 3)
+    n = 12
+    rng = np.random.default_rng(21)
+    circ, ora = qb.Circuit(), []
+    for _ in range(60):  # gates on qubits 0-5 only: one tile run, no one-gate pass
+        k, t = ONE[rng.integers(len(ONE))], int(rng.integers(6))
+        p = float(rng.uniform(0, 4 * math.pi))
+        circ.add(qb.gate(k, t, t, p))
+        ora.append(O.make_gate(k, t, t, p))
+    runs, single, _ = gate_plan(circ.gates(), n)
+    assert runs >= 1 and single == 0
+    psi0 = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    psi0 /= np.linalg.norm(psi0)
+    qc = qb.Computer(n)
+    qc.set_coeff_vec(psi0)
+    check(lib().qfb_set_tile_wait_limit(0), "qfb_set_tile_wait_limit")
+    try:
+        with pytest.raises(RuntimeError, match=f"qfb status {QFB_ETIMEDOUT}"):
+            qc.apply_circuit(circ)
+            qc.get_coeff_array()
+    finally:
+        check(lib().qfb_set_tile_wait_limit(2_000_000_000), "qfb_set_tile_wait_limit")
+    assert np.array_equal(qc.get_coeff_array(), psi0)
+    qc.apply_circuit(circ)
+    st = O.State(n, psi0.copy())
+    st.apply_gates(ora)
+    assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
+    assert lib().qfb_set_tile_wait_limit(61_000_000_000) != 0
+
+
 @pytest.mark.parametrize("n", [7, 16])
 def test_layered_sweep_circuit_matches_oracle(cuda, gate_tiles, n):
     """The gate-sweep workload (random layers of 1-qubit gates and pairings)."""

@@ -64,6 +64,75 @@ def test_qite_on_device_matches_reference(cuda):
         assert np.max(np.abs(ours - ref)) < tol, (name, np.max(np.abs(ours - ref)))
 
 
+def _dense_apply(terms, psi):
+    """sum_k c_k P(x_k, z_k) psi with P(x, z)|i> = i^{|x & z|} (-1)^{|i & z|} |i ^ x>."""
+    idx = np.arange(psi.size, dtype=np.uint64)
+    out = np.zeros_like(psi)
+    for c, x, z in terms:
+        x, z = np.uint64(x), np.uint64(z)
+        sign = 1 - 2 * (np.bitwise_count(idx & z).astype(np.int64) & 1)
+        out[idx ^ x] += complex(c) * (1j ** int(np.bitwise_count(x & z))) * sign * psi
+    return out
+
+
+S_B_TOL = 1e-12
+
+
+def test_qite_S_and_b_on_device_match_dense_forms(cuda, monkeypatch):
+    """Every S and b the device forms during the ill-posed QITE runs (H2 cqoy,
+    random SD, random GSD at two Trotter steps) equals the dense host form from
+    the same device state: S_IJ = Re <sigma_I psi|sigma_J psi> and b_I =
+    Re(-i c_I <psi|sigma_I H psi>) / sqrt(1 - 2 db E) (ite/qite.py:256-326).
+    Forming them is well-posed even where the least-squares solve after them is
+    not, so they are held to 1e-12 (relative to the largest |b|); the energy of
+    every step is held to the dense <psi|H|psi> of the device state at 1e-12."""
+    from qforte_b200 import qite
+    from test_qite_host import h2_system, random_system
+    d = golden("qite_norb3_seed11.npz")
+    dev_S, dev_b = qite.qite_S, qite.qite_b
+    seen = {"S": 0, "b": 0, "worst": 0.0}
+
+    def terms(op):
+        return op._pauli_terms(applied=True)
+
+    def rec_S(qc, sig_ops):
+        S = dev_S(qc, sig_ops)
+        psi = qc.get_coeff_array()
+        vecs = [_dense_apply(terms(op), psi) for op in sig_ops]
+        want = np.array([[1.0 if i == j else np.real(np.vdot(vi, vj))
+                          for j, vj in enumerate(vecs)] for i, vi in enumerate(vecs)])
+        err = float(np.max(np.abs(S - want))) if len(sig_ops) else 0.0
+        assert err < S_B_TOL, ("S", err)
+        seen["S"] += 1
+        seen["worst"] = max(seen["worst"], err)
+        return S
+
+    def rec_b(qc, hamiltonian, sig_ops, sig_coeffs, db, energy):
+        b = dev_b(qc, hamiltonian, sig_ops, sig_coeffs, db, energy)
+        psi = qc.get_coeff_array()
+        hpsi = _dense_apply(terms(hamiltonian), psi)
+        pre = -1.0j / np.sqrt(1 - 2 * db * energy)
+        want = np.array([np.real(pre * complex(c) * np.vdot(psi, _dense_apply(terms(op), hpsi)))
+                         for op, c in zip(sig_ops, sig_coeffs)])
+        err = float(np.max(np.abs(b - want)) / max(1.0, np.max(np.abs(want))))
+        assert err < S_B_TOL, ("b", err)
+        e_dense = float(np.real(np.vdot(psi, hpsi)))
+        assert abs(energy - e_dense) < S_B_TOL, ("E", energy, e_dense)
+        seen["b"] += 1
+        seen["worst"] = max(seen["worst"], err)
+        return b
+
+    monkeypatch.setattr(qite, "qite_S", rec_S)
+    monkeypatch.setattr(qite, "qite_b", rec_b)
+    qite.QITE(h2_system(d)).run(beta=0.6, db=0.2, expansion_type="cqoy", sparseSb=False)
+    qite.QITE(random_system(d)).run(beta=0.6, db=0.2, expansion_type="SD", sparseSb=True)
+    qite.QITE(random_system(d), trotter_number=2).run(beta=0.4, db=0.2, expansion_type="GSD",
+                                                     sparseSb=True)
+    # one S and one b per imaginary-time step of the three runs
+    steps = sum(len(d[k]) - 1 for k in ("h2_cqoy_ekb", "rand_sd_ekb", "rand_gsd_ekb"))
+    assert seen["S"] == steps and seen["b"] == steps, (seen, steps)
+
+
 def test_segmented_expvals_split_across_calls(cuda):
     """Matrix elements split over several qfb_sum_expval calls equal one call's."""
     import qforte_b200 as qb
