@@ -131,6 +131,14 @@ QFB_API int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates);
  * each fix R mixing qubits.  No counterpart in the reference; set by the
  * autotuner. */
 QFB_API int qfb_gates_config(int tile_bits, int low_bits);
+/* Dense blocks on the FP64 tensor cores, process-wide: k = 5 or 6 makes
+ * qfb_apply_gates fuse each run of gates on at most k qubits into one 2^k x 2^k
+ * unitary (the product of the gates as Computer::apply_gate applies them,
+ * computer.cc:340-751) and apply it in one pass with mma.sync FP64; 0 (the
+ * default) keeps the register-blocked tile runs.  States of fewer than 10
+ * qubits always take the tile runs.  Replaces dense runs of apply_1qubit_gate
+ * / apply_2qubit_gate (computer.cc:340-425, :458-751); set by the autotuner. */
+QFB_API int qfb_gates_dense(int k);
 /* Register bits R per thread of the gate tiles, process-wide (0: the default
  * of 3; always clamped so a tile has at most 256 threads and at least 4).  No
  * counterpart in the reference; set by the autotuner. */

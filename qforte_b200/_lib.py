@@ -45,6 +45,7 @@ SIGNATURES = {
     "qfb_sync": (ctypes.c_int, []),
     "qfb_launch_count": (ctypes.c_int, [_vp]),
     "qfb_set_tile_wait_limit": (ctypes.c_int, [_u64]),
+    "qfb_gates_dense": (ctypes.c_int, [ctypes.c_int]),
     "qfb_state_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp]),
     "qfb_state_destroy": (ctypes.c_int, [c_state]),
     "qfb_state_info": (ctypes.c_int, [c_state, _vp, _vp]),

@@ -25,7 +25,10 @@ from .device import gate_plan, gates_config
 __all__ = ["tune_gates", "tune_evaluator", "apply_cached", "cache_path",
            "GATE_CANDIDATES", "WINDOW_CANDIDATES"]
 
-GATE_CANDIDATES = ((10, 3, 3), (10, 4, 3), (11, 3, 3), (11, 4, 3), (9, 3, 3), (12, 3, 4))
+# (tile_bits, low_bits, reg_bits, dense): register-blocked tiles, and dense
+# 5- and 6-qubit blocks on the FP64 tensor cores
+GATE_CANDIDATES = ((10, 3, 3, 0), (10, 4, 3, 0), (11, 3, 3, 0), (11, 4, 3, 0), (9, 3, 3, 0),
+                   (12, 3, 4, 0), (0, 3, 0, 5), (0, 3, 0, 6))
 WINDOW_CANDIDATES = ((12, 11, 3), (11, 11, 3), (13, 11, 3), (12, 10, 3), (12, 12, 3),
                      (12, 11, 4))
 
@@ -75,17 +78,20 @@ def gate_key(nqubit):
 
 def tune_gates(circuit, nqubit, candidates=GATE_CANDIDATES, reps=2, store=True):
     """Time ``circuit`` on a fresh ``nqubit`` state under each (tile_bits,
-    low_bits, reg_bits); set and return the fastest with every timing (ms)."""
+    low_bits, reg_bits, dense); set and return the fastest with every timing
+    (ms)."""
     from .computer import Computer
     qc = Computer(int(nqubit))
     timings = {}
-    for tile, low, regs in candidates:
-        if tile > nqubit and (tile, low, regs) != tuple(candidates[0]):
+    for cand in candidates:
+        tile, low, regs, dense = (tuple(cand) + (0,))[:4]
+        first = tuple(cand) == tuple(candidates[0])
+        if not first and (tile > nqubit or (dense and nqubit < 10)):
             continue
-        gates_config(tile, low, regs)
+        gates_config(tile, low, regs, dense)
         runs, singles, _ = gate_plan(circuit.gates(), nqubit)
         ms = _time(lambda: qc.apply_circuit(circuit), reps)
-        timings[f"{tile},{low},{regs}"] = {"ms": ms, "passes": runs + singles}
+        timings[f"{tile},{low},{regs},{dense}"] = {"ms": ms, "passes": runs + singles}
     best = min(timings, key=lambda k: timings[k]["ms"])
     shape = tuple(int(v) for v in best.split(","))
     gates_config(*shape)

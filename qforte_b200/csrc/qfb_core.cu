@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "qfb_common.cuh"
+#include "qfb_dense.cuh"
 #include "qfb_gatetile.cuh"
 
 namespace qfb {
@@ -830,6 +831,164 @@ void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, Til
     run.b = b;
 }
 
+// ---------------------------------------------------------------------------
+// Dense blocks (FP64 tensor cores): runs of gates on at most K qubits fused
+// into one 2^K x 2^K unitary each.
+// ---------------------------------------------------------------------------
+
+int g_gate_dense = 0;  // 0: off; 5 or 6: runs of gates become dense K-qubit blocks
+
+// A gate (tile coordinates) on one vector of 2^K amplitudes, as k_gate2 /
+// k_gate4 apply it (the case analysis of computer.cc:340-751).
+void wgate_apply_host(const WGate &w, double2 *v, int K) {
+    auto mul = [](double2 a, double2 b) {
+        return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    };
+    auto add = [](double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); };
+    const uint32_t R = 1u << K, tb = 1u << w.t;
+    if (w.kind == K_GEN) {
+        const uint32_t cb = 1u << w.c;
+        for (uint32_t i = 0; i < R; ++i) {
+            if (i & (tb | cb)) continue;
+            const uint32_t idx[4] = {i, i | tb, i | cb, i | cb | tb};
+            double2 x[4], y[4];
+            for (int j = 0; j < 4; ++j) x[j] = v[idx[j]];
+            for (int r = 0; r < 4; ++r) {
+                double2 acc = make_double2(0.0, 0.0);
+                for (int j = 0; j < 4; ++j)
+                    if (w.nz & (1u << (4 * r + j))) acc = add(acc, mul(w.m[4 * r + j], x[j]));
+                y[r] = acc;
+            }
+            for (int r = 0; r < 4; ++r) v[idx[r]] = y[r];
+        }
+        return;
+    }
+    const uint32_t cb = w.c < 0 ? 0u : (1u << w.c);
+    for (uint32_t i = 0; i < R; ++i) {
+        if ((i & tb) || (i & cb) != cb) continue;
+        const uint32_t i1 = i | tb;
+        const double2 x0 = v[i], x1 = v[i1];
+        switch (w.kind) {
+            case K_DENSE:
+                v[i] = add(mul(w.m[0], x0), mul(w.m[1], x1));
+                v[i1] = add(mul(w.m[2], x0), mul(w.m[3], x1));
+                break;
+            case K_DIAG:
+                if (w.diag_set & 1) v[i] = mul(w.m[0], x0);
+                if (w.diag_set & 2) v[i1] = mul(w.m[3], x1);
+                break;
+            case K_SWAP:
+                v[i] = x1;
+                v[i1] = x0;
+                break;
+            default:
+                v[i] = mul(w.m[1], x1);
+                v[i1] = mul(w.m[2], x0);
+                break;
+        }
+    }
+}
+
+// The run's unitary, appended to `out` as a real plane then an imaginary
+// plane, row-major (row r, column s: the amplitude of block index r that
+// block index s becomes): each gate applied in order to every column of the
+// identity.
+void dense_unitary(const WGate *g, int ng, int K, std::vector<double> &out) {
+    const size_t R = (size_t)1 << K;
+    std::vector<double2> col(R);
+    const size_t o = out.size();
+    out.resize(o + 2 * R * R);
+    for (size_t s = 0; s < R; ++s) {
+        std::fill(col.begin(), col.end(), make_double2(0.0, 0.0));
+        col[s] = make_double2(1.0, 0.0);
+        for (int i = 0; i < ng; ++i) wgate_apply_host(g[i], col.data(), K);
+        for (size_t r = 0; r < R; ++r) {
+            out[o + r * R + s] = col[r].x;
+            out[o + R * R + r * R + s] = col[r].y;
+        }
+    }
+}
+
+// The dense pass of a window on block qubits S (|S| = K): tiles over S and
+// the lowest 10 - K other qubits.
+qfbd::DRun dense_run(uint64_t smask, int n) {
+    uint64_t q = smask;
+    for (int b = 0; b < n && __builtin_popcountll(q) < qfbd::kTileBits; ++b) q |= 1ull << b;
+    qfbd::DRun r{};
+    r.qmask = q;
+    uint32_t k = 0;
+    for (uint64_t m = q; m; m &= m - 1, ++k)
+        if (smask & (m & (~m + 1ull))) r.sbits |= 1u << k;
+    r.ntiles = (1ull << n) >> qfbd::kTileBits;
+    return r;
+}
+
+// Resident CTAs of the dense kernel for block size K, times the SMs.
+int dense_grid(int K, unsigned &grid) {
+    static std::once_flag once;
+    static int per_sm[2] = {0, 0};
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm[0], qfbd::k_dense_block<5>, qfbd::Shape<5>::THREADS,
+            2 * sizeof(double2) * qfbd::Shape<5>::BUF);
+        if (err == cudaSuccess)
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm[1], qfbd::k_dense_block<6>, qfbd::Shape<6>::THREADS,
+                2 * sizeof(double2) * qfbd::Shape<6>::BUF);
+    });
+    if (err != cudaSuccess) return cuda_fail(err, "dense block occupancy");
+    grid = (unsigned)std::max(1, per_sm[K - 5]) * (unsigned)sm_count();
+    return QFB_OK;
+}
+
+// Apply a gate list with dense blocks: windows of at most K qubits (the
+// greedy scan of plan_gate_windows, no forced low qubits) fused into one
+// unitary each; a window of one gate takes its own one-gate pass.
+int apply_gates_dense(qfb_state s, const std::vector<HGate> &hg, int K) {
+    const int n = s->nqubit;
+    std::vector<GatePlanWin> wins;
+    std::vector<WGate> wg;
+    plan_gate_windows(hg, n, K, 0, wins, wg);
+    std::vector<double> us;
+    for (const GatePlanWin &pw : wins)
+        if (pw.single < 0) dense_unitary(wg.data() + pw.w.g0, pw.w.ng, K, us);
+    void *buf = nullptr;
+    if (!us.empty()) {
+        int rc = dev_alloc(&buf, sizeof(double) * us.size());
+        if (rc) return rc;
+        QFB_CUDA(cudaMemcpyAsync(buf, us.data(), sizeof(double) * us.size(),
+                                 cudaMemcpyHostToDevice, t_stream));
+    }
+    unsigned cap = 0;
+    int rc = dense_grid(K, cap);
+    const size_t per_u = (size_t)2 << (2 * K);
+    size_t ui = 0;
+    for (size_t i = 0; i < wins.size() && rc == QFB_OK; ++i) {
+        const GatePlanWin &pw = wins[i];
+        if (pw.single >= 0) {
+            rc = launch_single(s, hg[pw.single]);
+            continue;
+        }
+        const qfbd::DRun run = dense_run(pw.w.qmask, n);
+        const double *U = (const double *)buf + per_u * ui++;
+        const uint64_t total = run.ntiles * (uint64_t)s->nbatch;
+        const unsigned grid = (unsigned)std::min<uint64_t>(total, cap);
+        if (K == 5) {
+            qfbd::k_dense_block<5><<<grid, qfbd::Shape<5>::THREADS,
+                                     2 * sizeof(double2) * qfbd::Shape<5>::BUF, t_stream>>>(
+                s->d, s->nbasis, s->nbatch, run, U);
+        } else {
+            qfbd::k_dense_block<6><<<grid, qfbd::Shape<6>::THREADS,
+                                     2 * sizeof(double2) * qfbd::Shape<6>::BUF, t_stream>>>(
+                s->d, s->nbasis, s->nbatch, run, U);
+        }
+        rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
+    }
+    if (buf) dev_free(buf);
+    return rc;
+}
+
 // Runs of a gate list and the phases of each run.
 void plan_gate_tiles(const std::vector<HGate> &hg, int n, int b, int L,
                      std::vector<GatePlanWin> &wins, TilePlan &tp, std::vector<qfbt::TRun> &runs) {
@@ -1077,6 +1236,13 @@ int qfb_gates_config(int tile_bits, int low_bits) {
     return QFB_OK;
 }
 
+int qfb_gates_dense(int k) {
+    if (k != 0 && k != 5 && k != 6)
+        return fail(QFB_EINVAL, "qfb_gates_dense: k = %d is not 0, 5 or 6", k);
+    g_gate_dense = k;
+    return QFB_OK;
+}
+
 int qfb_gates_regs(int reg_bits) {
     if (reg_bits < 0 || reg_bits > qfbt::kMaxRegBits)
         return fail(QFB_EINVAL, "qfb_gates_regs: reg_bits = %d outside [0, %d]", reg_bits,
@@ -1108,13 +1274,17 @@ int qfb_gates_plan(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t *w
     int64_t nw = 0, ns = 0;
     double bytes = 0.0;
     int b = 0, L = 0;
-    if (!gate_tile_shape(nqubit, b, L) || ngates == 1) {
+    const bool dense = g_gate_dense > 0 && nqubit >= qfbd::kTileBits && ngates > 1;
+    if (!dense && (!gate_tile_shape(nqubit, b, L) || ngates == 1)) {
         for (const HGate &h : hg) bytes += single_bytes(h);
         ns = ngates;
     } else {
         std::vector<GatePlanWin> wins;
         std::vector<WGate> wg;
-        plan_gate_windows(hg, nqubit, b, L, wins, wg);
+        if (dense)
+            plan_gate_windows(hg, nqubit, g_gate_dense, 0, wins, wg);
+        else
+            plan_gate_windows(hg, nqubit, b, L, wins, wg);
         for (const GatePlanWin &pw : wins) {
             if (pw.single >= 0) {
                 ++ns;
@@ -1173,6 +1343,8 @@ int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates) {
     std::vector<HGate> hg((size_t)ngates);
     for (int64_t k = 0; k < ngates; ++k) hg[k] = classify_gate(gates[k]);
     const int n = s->nqubit;
+    if (g_gate_dense > 0 && n >= qfbd::kTileBits && ngates > 1)
+        return apply_gates_dense(s, hg, g_gate_dense);
     int b = 0, L = 0;
     if (!gate_tile_shape(n, b, L) || ngates == 1) {
         for (const HGate &h : hg) {

@@ -74,3 +74,25 @@ def test_every_gate_is_planned_once(tile, low, n):
     assert ops + s <= len(gates)
     assert (w == 0) == (phases == 0)
     assert w <= phases
+
+
+def test_dense_block_planning():
+    """Dense mode: runs on at most k qubits (one pass each, however many gates
+    they hold); states under 10 qubits keep the tile runs; k is 0, 5 or 6."""
+    circ, spec = layered_random_circuit(24, 20, 2)
+    gates_config(0, 3, 0, 6)
+    w6, s6, b6 = gate_plan(circ.gates(), 24)
+    assert w6 > 0 and w6 + s6 < len(spec)
+    gates_config(0, 3, 0, 5)
+    w5, s5, _ = gate_plan(circ.gates(), 24)
+    assert w5 + s5 >= w6 + s6
+    deep = [qb.gate("H", q, q) for q in (1, 4, 7, 11, 14)] * 40
+    deep += [qb.gate("cX", 4, 11), qb.gate("SWAP", 1, 14), qb.gate("cZ", 7, 4)] * 20
+    assert gate_plan(deep, 15)[:2] == (1, 0)
+    small = circ.gates()[:40]
+    small = [g for g in small if g.target() < 8 and g.control() < 8]
+    tiles_dense = gate_plan(small, 8)
+    gates_config(0, 3, 0, 0)
+    assert tiles_dense == gate_plan(small, 8)
+    with pytest.raises(ValueError):
+        gates_config(0, 3, 0, 7)

@@ -92,8 +92,8 @@ def _sweep_cases():
     out = []
     for n in (20, 24, 28):
         if os.path.exists(os.path.join(GOLDEN, f"sweep{n}_seed{11 + n}.npz")):
-            for tile in (0, -1):
-                out.append((n, tile))
+            for tile, dense in ((0, 0), (-1, 0), (0, 5), (0, 6)):
+                out.append((n, tile, dense))
     return out
 
 
@@ -101,18 +101,19 @@ def _sweep_cases():
 def restore_gates_config():
     from qforte_b200.device import gates_config
     yield gates_config
-    gates_config(0, 3, 0)
+    gates_config(0, 3, 0, 0)
 
 
-@pytest.mark.parametrize("n,tile", _sweep_cases())
-def test_gate_sweep_matches_reference(cuda, restore_gates_config, n, tile):
+@pytest.mark.parametrize("n,tile,dense", _sweep_cases())
+def test_gate_sweep_matches_reference(cuda, restore_gates_config, n, tile, dense):
     """Config: the 100-layer random gate sweep on the register-blocked tile
-    path (tile 0) and on one pass per gate (tile -1): sampled amplitudes at
-    1e-12, the norm, <Z_k> of every qubit and the mass of each value of the
-    top 8 qubits against the reference's state."""
+    path (tile 0), on one pass per gate (tile -1) and in dense 5- and 6-qubit
+    blocks on the FP64 tensor cores: sampled amplitudes at 1e-12, the norm,
+    <Z_k> of every qubit and the mass of each value of the top 8 qubits
+    against the reference's state."""
     from qforte_b200.workloads import layered_random_circuit
     z = golden(f"sweep{n}_seed{11 + n}.npz")
-    restore_gates_config(tile, 3, 0)
+    restore_gates_config(tile, 3, 0, dense)
     circ, spec = layered_random_circuit(n, int(z["layers"]), int(z["seed"]))
     assert len(spec) == int(z["ngates"])
     qc = qb.Computer(n)

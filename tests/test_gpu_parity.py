@@ -346,6 +346,95 @@ def test_gate_windows_match_oracle(cuda, gate_tiles, tile, low, n, ngates, seed)
     assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
 
 
+@pytest.fixture
+def dense_blocks():
+    """Sets dense K-qubit blocks (FP64 tensor cores) and restores the default."""
+    from qforte_b200.device import gates_config
+    yield lambda k: gates_config(0, 3, 0, k)
+    gates_config(0, 3, 0, 0)
+
+
+def _random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return v / np.linalg.norm(v)
+
+
+@pytest.mark.parametrize("k", [5, 6])
+@pytest.mark.parametrize("n,ngates,seed", [(10, 300, 31), (13, 250, 32), (16, 200, 33)])
+def test_dense_blocks_match_oracle(cuda, dense_blocks, k, n, ngates, seed):
+    """Runs of every gate kind fused into dense 2^k x 2^k unitaries and
+    applied with FP64 mma.sync, from a random state, against the oracle's
+    gate-by-gate application."""
+    from qforte_b200.device import gate_plan
+    circ, ora = _rand_circuit(n, ngates, seed)
+    psi0 = _random_state(n, seed)
+    dense_blocks(k)
+    runs, singles, _ = gate_plan(circ.gates(), n)
+    assert runs > 0
+    qc = qb.Computer(n)
+    qc.set_coeff_vec(psi0)
+    qc.apply_circuit(circ)
+    st = O.State(n, psi0.copy())
+    st.apply_gates(ora)
+    assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
+
+
+@pytest.mark.parametrize("k", [5, 6])
+def test_dense_block_of_a_deep_run_on_few_qubits(cuda, dense_blocks, k):
+    """400 gates on 5 scattered qubits of 15 become one dense pass."""
+    from qforte_b200.device import gate_plan
+    n, qs = 15, [1, 4, 7, 11, 14]
+    rng = np.random.default_rng(40 + k)
+    circ, ora = qb.Circuit(), []
+    for _ in range(400):
+        if rng.random() < 0.5:
+            kk, t = ONE[rng.integers(len(ONE))], int(rng.choice(qs))
+            c = t
+        else:
+            kk = TWO[rng.integers(len(TWO))]
+            t, c = (int(v) for v in rng.choice(qs, 2, replace=False))
+        p = float(rng.uniform(0, 4 * math.pi))
+        circ.add(qb.gate(kk, t, c, p))
+        ora.append(O.make_gate(kk, t, c, p))
+    psi0 = _random_state(n, 44)
+    dense_blocks(k)
+    assert gate_plan(circ.gates(), n)[:2] == (1, 0)
+    qc = qb.Computer(n)
+    qc.set_coeff_vec(psi0)
+    qc.apply_circuit(circ)
+    st = O.State(n, psi0.copy())
+    st.apply_gates(ora)
+    assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
+
+
+def test_dense_blocks_on_a_batch_of_states(cuda, dense_blocks):
+    """Every slot of a batched state gets the same dense passes."""
+    import ctypes
+    from qforte_b200._lib import check, lib, ptr
+    from qforte_b200.device import pack_gates
+    n = 12
+    circ, ora = _rand_circuit(n, 150, 35)
+    L = lib()
+    h = ctypes.c_void_p()
+    check(L.qfb_state_create(n, 3, ctypes.byref(h)))
+    try:
+        psis = [_random_state(n, 50 + b) for b in range(3)]
+        for b, v in enumerate(psis):
+            check(L.qfb_state_upload(h, b, ptr(v), 1 << n))
+        arr = pack_gates(circ.gates())
+        dense_blocks(5)
+        check(L.qfb_apply_gates(h, arr.ctypes.data, len(arr)), "qfb_apply_gates")
+        for b, v in enumerate(psis):
+            out = np.zeros(1 << n, dtype=np.complex128)
+            check(L.qfb_state_download(h, b, ptr(out), 1 << n))
+            st = O.State(n, v.copy())
+            st.apply_gates(ora)
+            assert np.max(np.abs(out - st.psi)) < AMP_TOL
+    finally:
+        L.qfb_state_destroy(h)
+
+
 def test_gate_tile_wait_that_runs_out_reports_and_leaves_state(cuda, gate_tiles):
     """The tile kernel's bounded wait for its bulk load copies, made to run out
     with no fault: with the wait limit at 0 every tile gives up at once, flags
