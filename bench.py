@@ -35,6 +35,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "UCC energy+grad evals/s"
+
+# The compact-sector kernels of the default workload (16 qubits, 256 sets), from
+# one ncu capture of that workload (--set full --clock-control none,
+# -k regex:k_sector_(forward|h|sweep), 3 launches): DRAM bytes read + written
+# per launch, and the L1 / shared-memory pipe and issue activity that bind them.
+NCU_SECTOR_UCC16_B256 = {
+    "k_sector_forward": {"dram_bytes": 1.497e6, "l1_shared_pipe_pct": 50.7, "issue_active_pct": 39.8,
+                         "warps_active_pct": 42.9},
+    "k_sector_h": {"dram_bytes": 31.35e6, "l1_shared_pipe_pct": 88.6, "issue_active_pct": 34.6,
+                   "warps_active_pct": 49.9},
+    "k_sector_sweep": {"dram_bytes": 21.58e6, "l1_shared_pipe_pct": 47.8, "issue_active_pct": 35.5,
+                       "warps_active_pct": 21.7},
+}
 UNIT = "evals/s"
 
 
@@ -48,6 +61,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the gate-sweep, Pauli-exponential and serving numbers of the "
+                         "default run")
     ap.add_argument("--full-space", action="store_true",
                     help="keep full-space states (no compact sector evaluator)")
     ap.add_argument("--workload", default="ucc",
@@ -180,11 +196,26 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(a, mol, pool, amps_row, steps=2):
-    """The compiled reference on a bounded sample (seconds per evaluation)."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def cpu_baseline(a, mol, pool, rows, rounds=1):
+    """The compiled reference (serial shipped build) on a bounded sample of the
+    workload, one evaluation per host core at once (the batch's evaluations
+    are independent).  Each worker times U(t) in full, H on a tenth of its
+    terms and 12 reverse-sweep steps, scaled to one whole evaluation."""
     from oracle import oracle as O
     from qforte_b200.pauli import letters
-    qf = O.load_reference_engine()
+    O.load_reference_engine()  # fail here, in the parent, if it is not built
 
     def terms(qo):
         return [(complex(c), letters(*circ._pauli_masks()[:2])) for c, circ in qo.terms()]
@@ -201,19 +232,25 @@ def cpu_baseline(a, mol, pool, amps_row, steps=2):
         kf.append(terms(q))
     ht = terms(mol.hamiltonian)
     h_sample = max(1, len(ht) // 10)
-    m_sample = 24
-    per = []
-    for _ in range(steps):
-        t, parts = O.ref_eval_sample(qf, 2 * a.norb, mol.hf_reference, kf, kg, list(amps_row), ht,
-                                     h_sample, m_sample)
-        per.append(t)
-    t = statistics.median(per)
-    return {"value": 1.0 / t, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"per evaluation: U(t) as gates in full, apply_operator(H) on {h_sample} of "
-                      f"{len(ht)} terms scaled x{len(ht) / h_sample:.1f} (twice: energy and "
-                      f"sigma), {m_sample} of {len(kf)} reverse-sweep steps scaled; median of "
-                      f"{steps}; serial shipped build (USE_OpenMP off)",
-            "seconds_per_eval": t, "parts": parts}
+    m_sample = 12
+    workers = max(1, min(O.host_cores(), 128))
+    per, walls, parts = [], [], None
+    for _ in range(max(1, rounds)):
+        rate, t, wall, parts = O.ref_eval_parallel(2 * a.norb, mol.hf_reference, kf, kg, rows, ht,
+                                                   h_sample, m_sample, workers)
+        per += t
+        walls.append(wall)
+    t_eval = statistics.median(per)
+    return {"value": workers / t_eval, "unit": UNIT, "cores": workers, "kind": "reference",
+            "sample": f"per evaluation: U(t) as gates in full, apply_operator(H) on {h_sample} "
+                      f"of {len(ht)} terms scaled x{len(ht) / h_sample:.1f} (twice: energy and "
+                      f"sigma), {m_sample} of {len(kf)} reverse-sweep steps scaled; one "
+                      f"evaluation per core on {workers} cores at once, {max(1, rounds)} "
+                      "round(s), median seconds per evaluation; serial shipped build "
+                      "(USE_OpenMP off) in each worker",
+            "extrapolated": True, "cpu_model": cpu_model(),
+            "seconds_per_eval": t_eval, "sample_wall_s": statistics.median(walls),
+            "parts": parts[0] if parts else None}
 
 
 def run_reference(a, rank, world):
@@ -229,13 +266,21 @@ def run_reference(a, rank, world):
     except Exception as e:
         print(json.dumps({"impl": "reference", "unavailable": f"reference module not built: {e}"}))
         return None
-    cb = cpu_baseline(a, mol, pool, P[0], steps=max(1, a.steps))
+    # each step is one bounded sample round on every host core; the rounds of
+    # the whole run stay within a few minutes
+    rounds = max(1, min(a.steps, 8))
+    cb = cpu_baseline(a, mol, pool, P, rounds=rounds)
     v = cb["value"]
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": 1000.0 * a.batch / v, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": rounds,
+            "warmup": 0, "ms_per_step": 1000.0 * cb["sample_wall_s"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex128 states)",
+            "data": "synthetic",
             "config": workload_config(a, len(mol.hamiltonian), len(pool)), "impl": "reference",
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                "extrapolated", "cpu_model")},
+            "timing": "ms_per_step is the wall time of one sample round (one sampled "
+                      "evaluation per core); value extrapolates the sampled parts of each "
+                      "evaluation to the whole evaluation",
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "gpu_launches": 0}
     print(json.dumps(line))
@@ -256,7 +301,7 @@ def gate_cpu_baseline(n, spec, seconds=12.0):
     return t, ngates
 
 
-def run_gates(a, rank, world, local):
+def run_gates(a, rank, world, local, emit=True):
     """Gate sweep: layered random circuits applied with Computer.apply_circuit."""
     import torch
     import qforte_b200 as qb
@@ -331,14 +376,15 @@ def run_gates(a, rank, world, local):
                                     "seconds_per_gate": t}
         except Exception as e:
             line["cpu_baseline"] = {"unavailable": str(e)}
-    print(json.dumps(line))
+    if emit:
+        print(json.dumps(line))
     return line
 
 
 PEXP_METRIC = "Pauli-exponential pass GB/s"
 
 
-def run_pexp(a, local):
+def run_pexp(a, local, emit=True, ducc_part=True):
     """Pauli-exponential passes on one n-qubit state (default 28 qubits, 4 GiB).
 
     * ``strings``: exp(i phi P) for random Pauli strings with distinct x-masks,
@@ -403,6 +449,11 @@ def run_pexp(a, local):
     check(L.qfb_state_get_amp(h, 0, 0, out), "qfb_state_get_amp")
     roundtrip_err = abs(complex(out[0], out[1]) - 1.0)
     gbs = K * 32.0 * N / (ms_s * 1e-3) / 1e9
+    if not ducc_part:
+        check(L.qfb_state_destroy(h), "destroy")
+        return {"pass_gbs": gbs, "frac_of_hbm": gbs / peak, "peak": peak, "peak_source": src,
+                "nqubit": n, "strings": K, "ms_per_program": ms_s,
+                "gpu_launches": int(launches), "roundtrip_abs_err": roundtrip_err}
 
     # dUCC ansatz program of the (n/2)-orbital half-filled problem
     norb = n // 2
@@ -442,7 +493,8 @@ def run_pexp(a, local):
                          "avg_launch_ms": ms_s / max(1, launches), "traffic": None},
             "roundtrip_abs_err": roundtrip_err, "ducc": ducc,
             "gpu_launches": int(launches), "clocks": ck}
-    print(json.dumps(line))
+    if emit:
+        print(json.dumps(line))
     return line
 
 
@@ -868,6 +920,87 @@ def run_serve(a, local):
     return line
 
 
+def serve_saturating(a, local, rate=8000.0, duration=1.0, norbs=(5, 6, 7, 8)):
+    """Serving at an arrival rate far above what one-request-at-a-time can
+    take: a Poisson stream of mixed energy / energy+gradient requests of the
+    10-16-qubit dUCCSD problems, served with continuous batching and packing,
+    against the same trace served one request at a time (batch 1, one
+    stream) over its first requests."""
+    import torch
+    from qforte_b200.serving import Server
+    from qforte_b200.ucc import DUCC
+    torch.cuda.set_device(local)
+    problems = {}
+    for norb in norbs:
+        mol, pool = problem(norb, a.seed + norb)
+        problems[f"norb{norb}"] = DUCC(mol.hamiltonian, pool, list(range(len(pool))),
+                                       mol.hf_reference)
+    t = argparse.Namespace(seed=a.seed, rate=rate, duration=duration)
+    trace = serve_trace(t, problems)
+    t.seed = a.seed + 1000
+    t.duration = 0.3
+    warm = serve_trace(t, problems)
+
+    def served(max_batch, streams, tr, warm_tr):
+        srv = Server(hbm_budget=a.budget_gb * 1e9, max_batch=max_batch, streams=streams,
+                     device=local)
+        for k, d in problems.items():
+            srv.register(k, d)
+        with srv:
+            replay(srv, warm_tr)
+            srv.reset_stats()
+            res, wall = replay(srv, tr)
+            st = srv.stats()
+        return st, len(res), wall
+
+    st, n, wall = served(256, 4, trace, warm)
+    nseq = min(len(trace), 400)
+    st1, n1, wall1 = served(1, 1, trace[:nseq], warm[:64])
+    return {"workload": f"Poisson arrivals at {rate:.0f}/s for {duration} s, dUCCSD problems of "
+                        f"{norbs[0]}..{norbs[-1]} orbitals (half filling, SD pool), half energy "
+                        "and half energy+gradient requests",
+            "requests": n, "served_requests_per_s": n / wall,
+            "served_latency_ms": st.get("latency_ms"),
+            "served_batches": st.get("batches"), "served_mean_batch_rows": st.get("mean_batch_rows"),
+            "one_at_a_time": {"requests": n1, "requests_per_s": n1 / wall1,
+                              "latency_ms": st1.get("latency_ms"),
+                              "sample": "the first requests of the same trace, batch 1, one "
+                                        "stream"},
+            "served_vs_one_at_a_time": (n / wall) / (n1 / wall1)}
+
+
+def secondary(a, local):
+    """The metric's other numbers, timed in the same process after the
+    headline: gate-sweep passes at 28 qubits (register-blocked tile runs and
+    one pass per gate), Pauli-exponential passes at 28 qubits, and serving
+    latency at a saturating arrival rate."""
+    from qforte_b200.device import gates_config
+    out = {}
+    g = argparse.Namespace(**vars(a))
+    g.nqubits, g.steps, g.warmup, g.no_cpu_baseline, g.autotune = "28", 1, 1, True, False
+    try:
+        g.tile, g.layers = 0, 100
+        tile = run_gates(g, 0, 1, local, emit=False)
+        g.tile, g.layers = -1, 20
+        one = run_gates(g, 0, 1, local, emit=False)
+    finally:
+        gates_config(0, 3, 0)
+    for name, ln in (("tile_runs", tile), ("one_pass_per_gate", one)):
+        r = ln["sweep"][-1]
+        out[f"gates28_{name}"] = {"layers": g.layers if name != "tile_runs" else 100,
+                                  "gates": r["gates"], "passes": r["passes"],
+                                  "ms_per_circuit": r["ms_per_circuit"], "pass_gbs": r["pass_gbs"],
+                                  "frac_of_hbm": r["frac_of_hbm"],
+                                  "effective_gate_gbs": r["effective_gate_gbs"],
+                                  "gpu_launches": r["gpu_launches"]}
+    p = argparse.Namespace(**vars(a))
+    p.pexp_n, p.pexp_strings, p.steps, p.warmup = 28, 64, 3, 1
+    out["pauli_exp28"] = run_pexp(p, local, emit=False, ducc_part=False)
+    out["serving"] = serve_saturating(a, local)
+    out["peak_gbs"], out["peak_source"] = peaks()
+    return out
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1077,18 +1210,23 @@ def main():
         roof["h_row_entries"] = ev.h_rows
     if compact:
         roof["real_states"] = ev.real_states
+        roof["bound"] = "l1/shared"
         roof["bound_note"] = ("states live in shared memory, so HBM carries only the save "
-                              "buffer and the step lists: the forward and sweep kernels are "
-                              "latency bound (one barrier per step record; L1 / shared pipe "
-                              "47-50% of peak), the H kernel L1 / shared-pipe bound (88%), per "
-                              "profiles/k_sector_kernels_ucc16_b256.md")
+                              "buffer and the step lists; frac is the HBM fraction, the binding "
+                              "unit is the L1 / shared-memory pipe (ncu figures in "
+                              "binding_unit)")
+        ncu = NCU_SECTOR_UCC16_B256.get(kernel)
+        if ncu is not None and a.norb == 8 and a.batch == 256:
+            roof["traffic"] = ncu["dram_bytes"]
+            roof["binding_unit"] = dict(ncu)
         if dom in l2_stream:
             roof["l2_stream_bytes_per_launch"] = l2_stream[dom]
             roof["l2_stream_gbs"] = l2_stream[dom] / (avg_ms / 1000.0) / 1e9
 
+    dtype = "f64 (real sector states; complex128 API)" if compact and ev.real_states else "c128"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": max(a.warmup, 3), "ms_per_step": ms_all, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
             "config": workload_config(a, len(mol.hamiltonian), M),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(P.nbytes),
                     "d2h_bytes_per_step": int(hE.numel() * 8 + hG.numel() * 8)},
@@ -1098,11 +1236,14 @@ def main():
         line["batched_vs_plain"] = value / plain["value"]
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
-            cb = cpu_baseline(a, mol, pool, P[0])
-            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            cb = cpu_baseline(a, mol, pool, P)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                       "extrapolated", "cpu_model")}
             line["cpu_baseline"]["parts_s"] = cb["parts"]
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0 and world == 1 and not a.no_secondary:
+        line["secondary"] = secondary(a, local)
     if rank == 0:
         print(json.dumps(line))
     del ev, eng

@@ -586,6 +586,45 @@ def ref_eval_sample(qf, nqubit, ref, kops_fwd, kops_grad, amps, hterms, h_sample
     return t_u + 2.0 * t_h + t_sweep, {"t_U": t_u, "t_H": t_h, "t_sweep": t_sweep}
 
 
+def _ref_eval_worker(args):
+    """One spawned worker of ref_eval_parallel: imports the compiled reference
+    itself and times one sample evaluation."""
+    nqubit, ref, kops_fwd, kops_grad, amps, hterms, h_sample, m_sample = args
+    qf = load_reference_engine()
+    return ref_eval_sample(qf, nqubit, ref, kops_fwd, kops_grad, amps, hterms, h_sample,
+                           m_sample)
+
+
+def host_cores():
+    """The host threads this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        return os.cpu_count() or 1
+
+
+def ref_eval_parallel(nqubit, ref, kops_fwd, kops_grad, rows, hterms, h_sample, m_sample,
+                      workers):
+    """ref_eval_sample on ``workers`` host cores at once: the evaluations of a
+    batch are independent, so the shipped serial build runs one per core, in
+    processes started with ``spawn`` (safe after CUDA was initialised in the
+    parent).  Worker w evaluates ``rows[w % len(rows)]``.  Returns (evaluations
+    per second of all workers together, per-worker seconds per evaluation,
+    wall seconds of the sample, per-worker parts)."""
+    import multiprocessing as mp
+    import time
+
+    args = [(nqubit, list(ref), kops_fwd, kops_grad, list(map(float, rows[w % len(rows)])),
+             hterms, h_sample, m_sample) for w in range(workers)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(workers) as pool:
+        out = pool.map(_ref_eval_worker, args, chunksize=1)
+    wall = time.perf_counter() - t0
+    per = [t for t, _ in out]
+    return sum(1.0 / t for t in per), per, wall, [p for _, p in out]
+
+
 def ref_gate_sample(qf, nqubit, spec, ngates):
     """Seconds per gate of the compiled reference's Computer.apply_circuit
     (computer.cc:93-114) on the first ``ngates`` gates of ``spec`` [(kind,
