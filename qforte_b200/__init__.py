@@ -18,8 +18,8 @@ from .qubit_basis import QubitBasis
 from .computer import (Computer, add_gate_to_computer, inner_product,
                        prepare_computer_from_circuit, prepare_computer_from_gates)
 from .utils import (build_circuit, build_operator, build_refprep, compact_excitation_circuit,
-                    exponentiate_pauli_string, integer_to_ref, ref_string, smart_print, trotterize,
-                    trotterize_w_cRz)
+                    exponentiate_pauli_string, integer_to_ref, local_timer, ref_string, smart_print,
+                    trotterize, trotterize_w_cRz)
 from .systems import Molecule, create_external_mol, random_molecule, system_factory
 from .ucc import ADAPTVQE, SPQE, UCCNPQE, UCCNVQE
 from .qite import QITE

@@ -339,3 +339,19 @@ def build_eq_dets(open_shell_ref):
             if temp not in found:
                 found.append(temp)
     return [r for r in found if correct_spin(r, abs_spin)]
+
+
+class local_timer:
+    """Wall-clock seconds since construction or the last reset (timer.h:6-19,
+    bound as qforte.local_timer)."""
+
+    def __init__(self):
+        import time
+        self._now = time.perf_counter
+        self._t0 = self._now()
+
+    def reset(self):
+        self._t0 = self._now()
+
+    def get(self):
+        return self._now() - self._t0
