@@ -91,6 +91,9 @@ def parse():
                     help="gate sweep: lowest qubits every tile keeps")
     ap.add_argument("--reg-bits", type=int, default=0,
                     help="gate sweep: register bits per thread of a tile (0: default)")
+    ap.add_argument("--dense", type=int, default=0,
+                    help="gate sweep: fuse runs into dense 5- or 6-qubit blocks on the FP64 "
+                         "tensor cores (0: tile runs)")
     ap.add_argument("--autotune", action="store_true",
                     help="gate sweep: pick the tile shape per qubit count with the autotuner")
     return ap.parse_args()
@@ -309,7 +312,7 @@ def run_gates(a, rank, world, local, emit=True):
     from qforte_b200.device import gate_phases, gate_plan, gates_config
     from qforte_b200.workloads import layered_random_circuit
     torch.cuda.set_device(local)
-    gates_config(a.tile, a.low_bits, a.reg_bits)
+    gates_config(a.tile, a.low_bits, a.reg_bits, getattr(a, "dense", 0))
     peak, src = peaks()
     ns = [int(v) for v in a.nqubits.split(",") if v]
     rows = []
@@ -356,9 +359,13 @@ def run_gates(a, rank, world, local, emit=True):
             "config": {"workload": f"layered random circuits, {a.layers} layers, "
                                    f"{','.join(map(str, ns))} qubits, from |0...0>",
                        "tile_bits": a.tile, "low_bits": a.low_bits, "reg_bits": a.reg_bits,
+                       "dense_block_qubits": getattr(a, "dense", 0),
                        "l2": "state larger than L2 from 23 qubits"},
             "sweep": rows,
-            "roofline": {"bound": "hbm", "kernel": "k_gate_tile", "achieved": last["pass_gbs"],
+            "roofline": {"bound": "hbm",
+                         "kernel": ("k_dense_block" if getattr(a, "dense", 0) else
+                                    "k_gate2 / k_gate4" if a.tile == -1 else "k_gate_tile"),
+                         "achieved": last["pass_gbs"],
                          "peak": peak, "peak_source": src, "unit": "GB/s",
                          "frac": last["pass_gbs"] / peak, "traffic": None},
             "gpu_launches": last["gpu_launches"], "clocks": ck}
@@ -920,12 +927,13 @@ def run_serve(a, local):
     return line
 
 
-def serve_saturating(a, local, rate=8000.0, duration=1.0, norbs=(5, 6, 7, 8)):
-    """Serving at an arrival rate far above what one-request-at-a-time can
+def serve_saturating(a, local, rate=100000.0, duration=0.3, norbs=(5, 6, 7, 8)):
+    """Serving at an arrival rate far above what one request at a time can
     take: a Poisson stream of mixed energy / energy+gradient requests of the
-    10-16-qubit dUCCSD problems, served with continuous batching and packing,
-    against the same trace served one request at a time (batch 1, one
-    stream) over its first requests."""
+    10-16-qubit dUCCSD problems, served with packed launches (every problem's
+    requests together, ucc.Pack), against the same trace served one request at
+    a time (each problem's own evaluator, batch 1, one stream, no packing) over
+    its first requests."""
     import torch
     from qforte_b200.serving import Server
     from qforte_b200.ucc import DUCC
@@ -941,9 +949,9 @@ def serve_saturating(a, local, rate=8000.0, duration=1.0, norbs=(5, 6, 7, 8)):
     t.duration = 0.3
     warm = serve_trace(t, problems)
 
-    def served(max_batch, streams, tr, warm_tr):
+    def served(max_batch, streams, tr, warm_tr, pack):
         srv = Server(hbm_budget=a.budget_gb * 1e9, max_batch=max_batch, streams=streams,
-                     device=local)
+                     device=local, pack=pack)
         for k, d in problems.items():
             srv.register(k, d)
         with srv:
@@ -953,9 +961,9 @@ def serve_saturating(a, local, rate=8000.0, duration=1.0, norbs=(5, 6, 7, 8)):
             st = srv.stats()
         return st, len(res), wall
 
-    st, n, wall = served(256, 4, trace, warm)
+    st, n, wall = served(256, 4, trace, warm, True)
     nseq = min(len(trace), 400)
-    st1, n1, wall1 = served(1, 1, trace[:nseq], warm[:64])
+    st1, n1, wall1 = served(1, 1, trace[:nseq], warm[:64], False)
     return {"workload": f"Poisson arrivals at {rate:.0f}/s for {duration} s, dUCCSD problems of "
                         f"{norbs[0]}..{norbs[-1]} orbitals (half filling, SD pool), half energy "
                         "and half energy+gradient requests",
@@ -964,8 +972,8 @@ def serve_saturating(a, local, rate=8000.0, duration=1.0, norbs=(5, 6, 7, 8)):
             "served_batches": st.get("batches"), "served_mean_batch_rows": st.get("mean_batch_rows"),
             "one_at_a_time": {"requests": n1, "requests_per_s": n1 / wall1,
                               "latency_ms": st1.get("latency_ms"),
-                              "sample": "the first requests of the same trace, batch 1, one "
-                                        "stream"},
+                              "sample": "the first requests of the same trace, each problem's "
+                                        "own evaluator, batch 1, one stream, no packing"},
             "served_vs_one_at_a_time": (n / wall) / (n1 / wall1)}
 
 

@@ -320,6 +320,36 @@ QFB_API int qfb_ucc_eval(qfb_ucc u, const double *params, double *energy, double
 QFB_API int qfb_ucc_profile(qfb_ucc u, int with_grad, int reps, double *stage_ms,
                             int64_t *stage_launches);
 
+/* ---- packed evaluations of several problems (serving) ---------------------
+ * A pack gathers the compact-sector evaluators of several dUCC problems (each
+ * qfb_ucc_path == 2: states of up to ~16 qubits held in shared memory, all
+ * with the same state storage, qfb_ucc_real_states) so that parameter sets of
+ * different problems run in ONE launch: item i evaluates params[i][0..nparam)
+ * of member items[i].member, energy into energy[i] and, when items[i].grad is
+ * set, the adjoint gradient into grad[i][0..nparam) (row stride maxparam).
+ * One CTA per item runs the whole evaluation in shared memory: the forward
+ * program, sigma = H psi, the energy, the reverse sweep and the per-parameter
+ * sums (energy_feval / measure_gradient, algorithm.py:458-474,
+ * uccvqeabc.py:122-251).  The members must outlive the pack.  No counterpart
+ * in the reference (its Computer evaluates one problem per call). */
+typedef struct qfb_pack_s *qfb_pack;
+QFB_API int qfb_pack_create(const qfb_ucc *members, int nmembers, int capacity, qfb_pack *out);
+QFB_API int qfb_pack_destroy(qfb_pack p);
+QFB_API int qfb_pack_info(qfb_pack p, int32_t *capacity, int32_t *maxparam, uint64_t *bytes);
+/* Device blocks: items [capacity][2] int32 (member, grad), params and grad
+ * [capacity][maxparam], energy [capacity]. */
+QFB_API int qfb_pack_buffers(qfb_pack p, int32_t **items, double **params, double **energy,
+                             double **grad);
+/* Enqueue the first nitems items of the device blocks on the calling thread's
+ * stream (an item naming no member gets a NaN energy). */
+QFB_API int qfb_pack_launch(qfb_pack p, int nitems);
+/* Host arrays in and out, synchronising: member[i], with_grad[i] (may be
+ * NULL: energies only), params [nitems][maxparam], energy [nitems], grad
+ * [nitems][maxparam] (may be NULL when no item asks for a gradient). */
+QFB_API int qfb_pack_run(qfb_pack p, const int32_t *member, const int32_t *with_grad, int nitems,
+                         const double *params, double *energy, double *grad);
+
+
 #ifdef __cplusplus
 }
 #endif

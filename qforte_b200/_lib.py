@@ -46,6 +46,12 @@ SIGNATURES = {
     "qfb_launch_count": (ctypes.c_int, [_vp]),
     "qfb_set_tile_wait_limit": (ctypes.c_int, [_u64]),
     "qfb_gates_dense": (ctypes.c_int, [ctypes.c_int]),
+    "qfb_pack_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "qfb_pack_destroy": (ctypes.c_int, [_vp]),
+    "qfb_pack_info": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "qfb_pack_buffers": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "qfb_pack_launch": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "qfb_pack_run": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
     "qfb_state_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp]),
     "qfb_state_destroy": (ctypes.c_int, [c_state]),
     "qfb_state_info": (ctypes.c_int, [c_state, _vp, _vp]),

@@ -2706,6 +2706,7 @@ struct qfb_ucc_s {
     const double2 *rphase = nullptr;  // [nres]
     qfbs::PStream rstream{};          // compact: forward pair lists in reverse order
     std::shared_ptr<PairPlanDev> pairs;  // compact: the plan's pair lists in use
+    int64_t nprows = 1;                  // rows of the gradient partials (gradient steps)
 };
 
 // Whether every pattern of every record of a stream has real coefficients.
@@ -3231,6 +3232,9 @@ static cudaError_t sector_smem_attr_v() {
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, m);
     if (err == cudaSuccess)
         err = cudaFuncSetAttribute(qfbs::k_sector_pool<V>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(qfbs::k_sector_pack<V>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, m);
     return err;
 }
@@ -3784,6 +3788,7 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
     u->vpart = (double2 *)(base + o_vp);
     u->gpart = (double2 *)(base + o_gp);
     u->psteps = (int2 *)(base + o_ps);
+    u->nprows = (int64_t)nsteps;
     u->nsec = compact ? (int64_t)splan.nsec : (int64_t)sector.size();
     u->SL.save = (double2 *)(base + o_save);
     u->h_epart = (double *)(base + o_hep);
@@ -4218,6 +4223,177 @@ int qfb_ucc_profile(qfb_ucc u, int with_grad, int reps, double *stage_ms,
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// packed evaluations: parameter sets of several problems in one launch
+// ===========================================================================
+
+struct qfb_pack_s {
+    int nmem = 0, cap = 0, maxparam = 1, max_rows = 1, sreal = 0;
+    size_t smem = 0, bytes = 0;
+    void *blob = nullptr;
+    qfbs::PackMember *d_mem = nullptr;
+    int2 *items = nullptr;
+    double *params = nullptr, *energy = nullptr, *grad = nullptr;
+    double2 *partial = nullptr;
+};
+
+extern "C" int qfb_pack_create(const qfb_ucc *members, int nmembers, int capacity, qfb_pack *out) {
+    if (!out) return fail(QFB_EINVAL, "qfb_pack_create: null output");
+    *out = nullptr;
+    if (!members || nmembers < 1 || capacity < 1 || capacity > 65535)
+        return fail(QFB_EINVAL, "qfb_pack_create: need members and a capacity in [1, 65535]");
+    int rc = sector_smem_attr();
+    if (rc) return rc;
+    auto p = std::make_unique<qfb_pack_s>();
+    p->nmem = nmembers;
+    p->cap = capacity;
+    std::vector<qfbs::PackMember> hm((size_t)nmembers);
+    for (int k = 0; k < nmembers; ++k) {
+        const qfb_ucc u = members[k];
+        if (!u) return fail(QFB_EINVAL, "qfb_pack_create: member %d is null", k);
+        if (!u->compact || u->gsec)
+            return fail(QFB_EINVAL,
+                        "qfb_pack_create: member %d does not keep its states in shared memory "
+                        "(only compact-sector evaluators of up to ~16 qubits can be packed)", k);
+        if (u->nparam > 0 && !u->grad)
+            return fail(QFB_EINVAL, "qfb_pack_create: member %d has no gradient program", k);
+        if (k == 0) p->sreal = u->sreal;
+        if (u->sreal != p->sreal)
+            return fail(QFB_EINVAL, "qfb_pack_create: members mix real and complex state storage");
+        const qfbs::SLaunch &L = u->SL;
+        const size_t es = u->sreal ? sizeof(qfbs::PSmem<double>) : sizeof(qfbs::PSmem<double2>);
+        const size_t need = qfbs::sector_smem_states(2, (size_t)L.nsec, u->sreal) +
+                            es * (size_t)std::max(L.fwd.n, L.sweep.n);
+        if (need > kSectorSmemMax)
+            return fail(QFB_EINVAL, "qfb_pack_create: member %d needs %zu bytes of shared memory",
+                        k, need);
+        p->smem = std::max(p->smem, need);
+        p->maxparam = std::max(p->maxparam, u->nparam);
+        p->max_rows = std::max(p->max_rows, (int)u->nprows);
+        qfbs::PackMember &m = hm[(size_t)k];
+        m.nsec = L.nsec;
+        m.ref_i = L.ref_i;
+        m.nparam = u->nparam;
+        m.pad = 0;
+        m.fwd = L.fwd;
+        m.sweep = L.sweep;
+        m.rowptr = L.rowptr;
+        m.col = L.col;
+        m.val_r = L.val_r;
+        m.val_c = L.val_c;
+        m.psteps = u->psteps;
+    }
+    const size_t C = (size_t)capacity, MP = (size_t)p->maxparam;
+    const size_t nw = qfbs::kPackThreads / 32;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_mem = take(sizeof(qfbs::PackMember) * (size_t)nmembers);
+    const size_t o_it = take(sizeof(int2) * C), o_par = take(sizeof(double) * C * MP);
+    const size_t o_en = take(sizeof(double) * C), o_gr = take(sizeof(double) * C * MP);
+    const size_t o_pt = take(sizeof(double2) * C * (size_t)p->max_rows * nw);
+    rc = dev_alloc(&p->blob, off);
+    if (rc) return rc;
+    p->bytes = off;
+    char *base = (char *)p->blob;
+    p->d_mem = (qfbs::PackMember *)(base + o_mem);
+    p->items = (int2 *)(base + o_it);
+    p->params = (double *)(base + o_par);
+    p->energy = (double *)(base + o_en);
+    p->grad = (double *)(base + o_gr);
+    p->partial = (double2 *)(base + o_pt);
+    cudaError_t e = cudaMemsetAsync(p->blob, 0, off, t_stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p->d_mem, hm.data(), sizeof(qfbs::PackMember) * hm.size(),
+                            cudaMemcpyHostToDevice, t_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t_stream);
+    if (e != cudaSuccess) {
+        dev_free(p->blob);
+        return cuda_fail(e, "qfb_pack_create");
+    }
+    *out = p.release();
+    return QFB_OK;
+}
+
+extern "C" int qfb_pack_destroy(qfb_pack p) {
+    if (!p) return QFB_OK;
+    dev_free(p->blob);
+    delete p;
+    return QFB_OK;
+}
+
+extern "C" int qfb_pack_info(qfb_pack p, int32_t *capacity, int32_t *maxparam, uint64_t *bytes) {
+    if (!p) return fail(QFB_EINVAL, "qfb_pack_info: null pack");
+    if (capacity) *capacity = p->cap;
+    if (maxparam) *maxparam = p->maxparam;
+    if (bytes) *bytes = p->bytes;
+    return QFB_OK;
+}
+
+extern "C" int qfb_pack_buffers(qfb_pack p, int32_t **items, double **params, double **energy,
+                                double **grad) {
+    if (!p) return fail(QFB_EINVAL, "qfb_pack_buffers: null pack");
+    if (items) *items = (int32_t *)p->items;
+    if (params) *params = p->params;
+    if (energy) *energy = p->energy;
+    if (grad) *grad = p->grad;
+    return QFB_OK;
+}
+
+extern "C" int qfb_pack_launch(qfb_pack p, int nitems) {
+    if (!p) return fail(QFB_EINVAL, "qfb_pack_launch: null pack");
+    if (nitems < 0 || nitems > p->cap)
+        return fail(QFB_EINVAL, "qfb_pack_launch: %d items for a capacity of %d", nitems, p->cap);
+    if (nitems == 0) return QFB_OK;
+    if (p->sreal)
+        qfbs::k_sector_pack<double><<<nitems, qfbs::kPackThreads, p->smem, t_stream>>>(
+            p->d_mem, p->items, p->maxparam, p->params, p->energy, p->grad, p->partial, p->max_rows,
+            p->nmem);
+    else
+        qfbs::k_sector_pack<double2><<<nitems, qfbs::kPackThreads, p->smem, t_stream>>>(
+            p->d_mem, p->items, p->maxparam, p->params, p->energy, p->grad, p->partial, p->max_rows,
+            p->nmem);
+    QFB_LAUNCHED();
+    return QFB_OK;
+}
+
+extern "C" int qfb_pack_run(qfb_pack p, const int32_t *member, const int32_t *with_grad, int nitems,
+                            const double *params, double *energy, double *grad) {
+    if (!p) return fail(QFB_EINVAL, "qfb_pack_run: null pack");
+    if (nitems < 0 || nitems > p->cap)
+        return fail(QFB_EINVAL, "qfb_pack_run: %d items for a capacity of %d", nitems, p->cap);
+    if (nitems == 0) return QFB_OK;
+    if (!member || !params || !energy)
+        return fail(QFB_EINVAL, "qfb_pack_run: null argument");
+    std::vector<int2> it((size_t)nitems);
+    bool any_grad = false;
+    for (int i = 0; i < nitems; ++i) {
+        if (member[i] < 0 || member[i] >= p->nmem)
+            return fail(QFB_EINVAL, "qfb_pack_run: item %d names member %d of %d", i, member[i],
+                        p->nmem);
+        it[(size_t)i] = make_int2(member[i], with_grad && with_grad[i] ? 1 : 0);
+        any_grad = any_grad || it[(size_t)i].y;
+    }
+    if (any_grad && !grad) return fail(QFB_EINVAL, "qfb_pack_run: gradients asked for, no buffer");
+    const size_t MP = (size_t)p->maxparam;
+    QFB_CUDA(cudaMemcpyAsync(p->items, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice,
+                             t_stream));
+    QFB_CUDA(cudaMemcpyAsync(p->params, params, sizeof(double) * MP * nitems,
+                             cudaMemcpyHostToDevice, t_stream));
+    int rc = qfb_pack_launch(p, nitems);
+    if (rc) return rc;
+    QFB_CUDA(cudaMemcpyAsync(energy, p->energy, sizeof(double) * nitems, cudaMemcpyDeviceToHost,
+                             t_stream));
+    if (grad)
+        QFB_CUDA(cudaMemcpyAsync(grad, p->grad, sizeof(double) * MP * nitems,
+                                 cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
 
 // ===========================================================================
 // expectation values without device allocation

@@ -354,12 +354,12 @@ __device__ __forceinline__ V p_step(const PStream &S, const PSmem<V> &rec, const
 }
 
 // The warp partials of the inner products of records a and b (b < 0: none):
-// one per warp and record at partial[row][CTA][warp], zero from warps that
-// hold no pair of the record, two records reduced together where both have
-// one.
+// one per warp and record at partial[row][slot][warp] (nslot slots), zero
+// from warps that hold no pair of the record, two records reduced together
+// where both have one.
 template <class V>
 __device__ __forceinline__ void p_partials(const PSmem<V> *s_pr, int a, V acca, int b, V accb,
-                                           double2 *partial) {
+                                           double2 *partial, int nslot, int slot) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const PHead ha = s_pr[a].h;
     const bool ipa = ha.fl & R_IP;
@@ -372,7 +372,7 @@ __device__ __forceinline__ void p_partials(const PSmem<V> *s_pr, int a, V acca, 
     if (!ipa && !ipb) return;
     const bool ida = 32 * warp >= ha.np, idb = 32 * warp >= hb.np;  // warp holds no pair
     auto put = [&](const PHead &h, V x) {
-        partial[((size_t)h.row * gridDim.x + blockIdx.x) * nw + warp] = v_as2(x);
+        partial[((size_t)h.row * nslot + slot) * nw + warp] = v_as2(x);
     };
     if (ipa && ipb && !ida && !idb) {
         const V k = p_sum2(acca, accb);
@@ -397,7 +397,7 @@ __device__ __forceinline__ void p_partials(const PSmem<V> *s_pr, int a, V acca, 
 // L2.  SWEEP: the inner products of records (r, r + 1) are reduced together.
 template <bool SWEEP, class V>
 __device__ __forceinline__ void p_run(const PStream &S, const PSmem<V> *s_pr, V *v, V *w,
-                                      double2 *partial) {
+                                      double2 *partial, int nslot, int slot) {
     constexpr int KP = pair_slots<V>();
     constexpr int RING = SWEEP ? kSweepRing : 4;
     const int n = S.n;
@@ -410,12 +410,12 @@ __device__ __forceinline__ void p_run(const PStream &S, const PSmem<V> *s_pr, V 
         const V a0 = p_step<SWEEP, V, KP>(S, s_pr[r], w0, v, w);
         __syncthreads();
         if (r + 1 >= n) {
-            if (SWEEP) p_partials(s_pr, r, a0, -1, a0, partial);
+            if (SWEEP) p_partials(s_pr, r, a0, -1, a0, partial, nslot, slot);
             break;
         }
         if (r + RING < n) p_words(S, s_pr[r + RING].h, w0);
         const V a1 = p_step<SWEEP, V, KP>(S, s_pr[r + 1], w1, v, w);
-        if (SWEEP) p_partials(s_pr, r, a0, r + 1, a1, partial);
+        if (SWEEP) p_partials(s_pr, r, a0, r + 1, a1, partial, nslot, slot);
         __syncthreads();
         if (RING == 2) {
             if (r + 3 < n) p_words(S, s_pr[r + 3].h, w1);
@@ -426,12 +426,12 @@ __device__ __forceinline__ void p_run(const PStream &S, const PSmem<V> *s_pr, V 
         const V a2 = p_step<SWEEP, V, KP>(S, s_pr[r + 2], w2, v, w);
         __syncthreads();
         if (r + 3 >= n) {
-            if (SWEEP) p_partials(s_pr, r + 2, a2, -1, a2, partial);
+            if (SWEEP) p_partials(s_pr, r + 2, a2, -1, a2, partial, nslot, slot);
             break;
         }
         if (r + 6 < n) p_words(S, s_pr[r + 6].h, w2);
         const V a3 = p_step<SWEEP, V, KP>(S, s_pr[r + 3], w3, v, w);
-        if (SWEEP) p_partials(s_pr, r + 2, a2, r + 3, a3, partial);
+        if (SWEEP) p_partials(s_pr, r + 2, a2, r + 3, a3, partial, nslot, slot);
         __syncthreads();
     }
 }
@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(kStepThreads, 1024 / kStepThreads) k_sector_fo
     for (int i = tid; i < L.nsec; i += nth) psi[i] = i == L.ref_i ? v_one_of<V>() : v_zero(V());
     p_angles(L.fwd, par, 1, s_pr);
     __syncthreads();
-    p_run<false, V>(L.fwd, s_pr, psi, (V *)nullptr, nullptr);
+    p_run<false, V>(L.fwd, s_pr, psi, (V *)nullptr, nullptr, 1, 0);
     V *sv = reinterpret_cast<V *>(L.save) + (size_t)b * 2 * L.nsec;
     for (int i = tid; i < L.nsec; i += nth) sv[i] = psi[i];
 }
@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1024 / kSweepThreads) k_sector_
     for (int i = tid; i < 2 * L.nsec; i += nth) psi[i] = sv[i];
     p_angles(L.sweep, par, -1, s_pr);
     __syncthreads();
-    p_run<true, V>(L.sweep, s_pr, psi, sig, L.partial);
+    p_run<true, V>(L.sweep, s_pr, psi, sig, L.partial, gridDim.x, blockIdx.x);
 }
 
 // PQE residuals on the compact states: sigma of slot blockIdx.x from the save
@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(kStepThreads, 1024 / kStepThreads) k_sector_re
     for (int i = tid; i < L.nsec; i += nth) sig[i] = sv[i];
     p_angles(R, par, -1, s_pr);
     __syncthreads();
-    p_run<false, V>(R, s_pr, sig, (V *)nullptr, nullptr);
+    p_run<false, V>(R, s_pr, sig, (V *)nullptr, nullptr, 1, 0);
     for (int k = tid; k < nres; k += nth) {
         const int64_t i = idx[k];
         double r = 0.0;
@@ -664,6 +664,104 @@ __global__ void __launch_bounds__(512, 2) k_sector_pool(SLaunch L, PStream P) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc = v_add(acc, v_shfl_down(acc, o));
         if ((tid & 31) == 0) L.partial[((size_t)h.row * gridDim.y + b) * nw + (tid >> 5)] = v_as2(acc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Packed evaluations of several problems in one launch
+// ---------------------------------------------------------------------------
+
+// One problem of a packed launch: the compact evaluator data of one dUCC
+// problem (its sector, forward and sweep pair lists, H rows on the sector and
+// the sweep record rows of each parameter).
+struct PackMember {
+    int nsec, ref_i, nparam, pad;
+    PStream fwd, sweep;
+    const int32_t *rowptr;
+    const uint32_t *col;
+    const double *val_r;   // real H (val_c == nullptr) ...
+    const double2 *val_c;  // ... or complex
+    const int2 *psteps;    // per parameter: its rows of the sweep partials
+};
+
+constexpr int kPackThreads = 256;
+
+// sigma = H psi on one CTA's state (a warp per row, the lanes over the row's
+// entries) and this CTA's energy <psi|H|psi>, summed in a fixed order.
+template <class V>
+__device__ __forceinline__ double p_hpsi(const PackMember &m, const V *psi, V *sig, double *s_red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double en = 0.0;
+    for (int i = warp; i < m.nsec; i += nw) {
+        V acc = v_zero(V());
+        const int e1 = m.rowptr[i + 1];
+        for (int e = m.rowptr[i] + lane; e < e1; e += 32) {
+            const V x = psi[__ldg(&m.col[e])];
+            if constexpr (sizeof(V) == sizeof(double2)) {
+                if (m.val_c) acc = v_add(acc, v_mul(__ldg(&m.val_c[e]), x));
+                else v_acc(acc, __ldg(&m.val_r[e]), x);
+            } else {
+                v_acc(acc, __ldg(&m.val_r[e]), x);
+            }
+        }
+        acc = p_sum1(acc);
+        if (lane == 0) {
+            sig[i] = acc;
+            en += v_cj(psi[i], acc).x;
+        }
+    }
+    if (lane == 0) s_red[warp] = en;
+    __syncthreads();
+    double t = 0.0;
+    for (int k = 0; k < nw; ++k) t += s_red[k];
+    return t;
+}
+
+// CTA x evaluates item x: parameter set params[x][0 .. nparam) of problem
+// items[x].x, with its gradient when items[x].y != 0.  Energy into energy[x],
+// gradient into grad[x][0 .. nparam); partial[x] holds the sweep's warp
+// partials ([max_rows][warps] per item).  The whole evaluation stays in
+// this CTA's shared memory: psi = U(t)|ref> (forward pair lists), sigma = H psi
+// from the H rows, the energy, the reverse sweep and the per-parameter sums,
+// so one launch serves parameter sets of different problems side by side.
+template <class V>
+__global__ void __launch_bounds__(kPackThreads, 2) k_sector_pack(
+    const PackMember *__restrict__ members, const int2 *__restrict__ items, int maxparam,
+    const double *__restrict__ params, double *__restrict__ energy, double *__restrict__ grad,
+    double2 *__restrict__ partial, int max_rows, int nmem) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    __shared__ double s_red[kPackThreads / 32];
+    const int2 it = items[blockIdx.x];
+    if ((unsigned)it.x >= (unsigned)nmem) {  // no such problem: NaN energy, nothing else
+        if (threadIdx.x == 0) energy[blockIdx.x] = __longlong_as_double(0x7ff8000000000000ll);
+        return;
+    }
+    const PackMember m = members[it.x];
+    const int tid = threadIdx.x, nth = blockDim.x, nw = nth >> 5;
+    V *psi = reinterpret_cast<V *>(s_raw), *sig = psi + m.nsec;
+    PSmem<V> *s_pr = reinterpret_cast<PSmem<V> *>(s_raw + ((sizeof(V) * 2 * m.nsec + 15) & ~(size_t)15));
+    const double *par = params + (size_t)blockIdx.x * maxparam;
+    for (int i = tid; i < m.nsec; i += nth) psi[i] = i == m.ref_i ? v_one_of<V>() : v_zero(V());
+    p_angles(m.fwd, par, 1, s_pr);
+    __syncthreads();
+    p_run<false, V>(m.fwd, s_pr, psi, (V *)nullptr, nullptr, 1, 0);
+    __syncthreads();
+    const double e = p_hpsi<V>(m, psi, sig, s_red);
+    if (tid == 0) energy[blockIdx.x] = e;
+    if (!it.y || m.nparam == 0) return;
+    __syncthreads();  // every thread is done with the forward angles and sigma
+    p_angles(m.sweep, par, -1, s_pr);
+    __syncthreads();
+    double2 *pp = partial + (size_t)blockIdx.x * max_rows * nw;
+    p_run<true, V>(m.sweep, s_pr, psi, sig, pp, 1, 0);
+    __syncthreads();  // this CTA's partials are visible to all its threads
+    double *g = grad + (size_t)blockIdx.x * maxparam;
+    for (int mu = tid; mu < m.nparam; mu += nth) {
+        const int2 r = m.psteps[mu];
+        double acc = 0.0;
+        for (int s = r.x; s < r.y; ++s)
+            for (int c = 0; c < nw; ++c) acc += pp[(size_t)s * nw + c].x;
+        g[mu] = 2.0 * acc;
     }
 }
 

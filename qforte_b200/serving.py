@@ -5,10 +5,15 @@ evaluations of their current amplitudes; each driver's problem (Hamiltonian,
 compiled Pauli-exponential programs) is registered once and stays on the
 device.  One serving thread owns the loop:
 
-* **continuous batching** - requests of one problem and kind that are waiting
-  when a CUDA stream frees up go out together as one graph-captured evaluator
-  run (a batch of parameter rows, padded to a power of two); requests that
-  arrive while others are on the GPU join the next batch of their problem;
+* **packing** - requests of every problem small enough for the compact
+  shared-memory evaluator (up to ~16 qubits), energy and energy+gradient
+  alike, go out together in ONE launch (``ucc.Pack``: one CTA per request,
+  whatever its problem), so a mix of small problems shares launches instead
+  of each problem waiting for its own;
+* **continuous batching** - requests of a larger problem and kind that are
+  waiting when a CUDA stream frees up go out together as one graph-captured
+  evaluator run (a batch of parameter rows, padded to a power of two);
+  requests that arrive while others are on the GPU join the next launch;
 * **overlap** - up to ``streams`` batches (of different problems or of the
   same one) are in flight at once, each on its own stream with its own
   evaluator, so their kernels share the device;
@@ -35,7 +40,7 @@ from concurrent.futures import Future
 import numpy as np
 
 from ._lib import check, lib
-from .ucc import DUCC, Evaluator
+from .ucc import DUCC, Evaluator, Pack
 
 __all__ = ["Server"]
 
@@ -66,8 +71,22 @@ class _Slot:
         self.last_used = time.perf_counter()
 
 
+class _PackSlot:
+    """A Pack with its pinned host buffers (one launch at a time)."""
+
+    def __init__(self, pack):
+        import torch
+        self.pack = pack
+        C, MP = pack.capacity, pack.maxparam
+        self.h_items = torch.zeros((C, 2), dtype=torch.int32).pin_memory()
+        self.h_par = torch.zeros((C, MP), dtype=torch.float64).pin_memory()
+        self.h_en = torch.empty(C, dtype=torch.float64).pin_memory()
+        self.h_gr = torch.empty((C, MP), dtype=torch.float64).pin_memory()
+        self.d_items, self.d_par, self.d_en, self.d_gr = pack.tensors()
+
+
 class _Batch:
-    __slots__ = ("slot", "reqs", "stream", "event", "mode", "key", "t_launch")
+    __slots__ = ("slot", "reqs", "stream", "event", "mode", "key", "t_launch", "pack")
 
 
 class Server:
@@ -77,11 +96,16 @@ class Server:
     bounds the rows of one run; ``streams`` bounds the batches in flight.
     """
 
-    def __init__(self, hbm_budget=150e9, max_batch=256, streams=4, device=0):
+    def __init__(self, hbm_budget=150e9, max_batch=256, streams=4, device=0, pack=True):
         self.hbm_budget = float(hbm_budget)
         self.max_batch = int(max_batch)
         self.nstreams = int(streams)
         self.device = int(device)
+        self.pack = bool(pack)
+        self._pack_of = {}      # key -> (group, member index) for packed problems
+        self._pack_free = []    # per group: idle _PackSlot objects
+        self._pack_bytes = 0    # device bytes the packs hold
+        self._repack = queue.SimpleQueue()  # registrations waiting for the packs to be rebuilt
         self._problems = {}
         self._inbox = queue.SimpleQueue()
         self._waiting = collections.OrderedDict()  # (key, mode) -> deque of _Req
@@ -103,10 +127,20 @@ class Server:
 
     # ---- problems ----------------------------------------------------------
     def register(self, key, ducc):
-        """Make a compiled problem (a qforte_b200.ucc.DUCC) servable."""
+        """Make a compiled problem (a qforte_b200.ucc.DUCC) servable.  With
+        packing on, a problem that fits the compact shared-memory evaluator
+        joins the packs: on a running server the call returns once the loop
+        has rebuilt them (between launches), so every request of the problem
+        takes the packed path."""
         if key in self._problems:
             raise ValueError(f"problem {key!r} already registered")
         self._problems[key] = ducc
+        if self.pack and self._thread is not None and self._thread.is_alive():
+            done = threading.Event()
+            self._repack.put(done)
+            while not done.wait(0.05):
+                if self._error is not None:
+                    raise RuntimeError(f"server failed: {self._error}")
 
     def register_problem(self, key, hamiltonian, pool, tops, ref, pool_type=None):
         self.register(key, DUCC(hamiltonian, pool, tops, ref, pool_type))
@@ -179,15 +213,105 @@ class Server:
                                  "mean": float(lat.mean()), "max": float(lat.max())}
         return out
 
+    # ---- packing -------------------------------------------------------------
+    def _build_packs(self):
+        """One pack group per state storage (real / complex) over the
+        registered problems that take the compact shared-memory path, with a
+        pack per stream; their device bytes count against the budget."""
+        self._live_bytes -= self._pack_bytes
+        self._pack_bytes = 0
+        self._pack_free, self._pack_of = [], {}
+        if not self.pack:
+            return
+        groups = {}
+        for key, ducc in list(self._problems.items()):
+            ev = ducc.evaluator(1)
+            if ev.path == 2:
+                groups.setdefault(ev.real_states, []).append(key)
+        for keys in groups.values():
+            g = len(self._pack_free)
+            slots = []
+            for _ in range(self.nstreams):
+                pk = Pack([self._problems[k] for k in keys], capacity=self.max_batch)
+                # the members' evaluators are shared by the group's packs
+                need = pk.pack_bytes if slots else pk.device_bytes
+                if self._live_bytes + need > self.hbm_budget:
+                    break
+                self._live_bytes += need
+                self._pack_bytes += need
+                slots.append(_PackSlot(pk))
+            if not slots:
+                continue
+            self._pack_free.append(slots)
+            for i, k in enumerate(keys):
+                self._pack_of[k] = (g, i)
+        self._peak_bytes = max(self._peak_bytes, self._live_bytes)
+
+    def _launch_packs(self):
+        """One packed launch per pack group with waiting requests and a free
+        pack and stream: the group's oldest requests first, energy and
+        gradient requests of every problem together."""
+        import torch
+        n = 0
+        for g, free in enumerate(self._pack_free):
+            if not free or not self._free_streams:
+                continue
+            queues = [(k, dq) for k, dq in self._waiting.items() if k[0] in self._pack_of
+                      and self._pack_of[k[0]][0] == g]
+            if not queues:
+                continue
+            queues.sort(key=lambda kv: kv[1][0].t_submit)
+            ps = free.pop()
+            cap = ps.pack.capacity
+            reqs = []
+            for k, dq in queues:
+                while dq and len(reqs) < cap:
+                    reqs.append(dq.popleft())
+                if not dq:
+                    del self._waiting[k]
+                if len(reqs) == cap:
+                    break
+            items, par = ps.h_items.numpy(), ps.h_par.numpy()
+            for i, r in enumerate(reqs):
+                items[i, 0] = self._pack_of[r.key][1]
+                items[i, 1] = r.mode
+                par[i, :r.params.shape[0]] = r.params
+            m = len(reqs)
+            stream = self._free_streams.pop()
+            with torch.cuda.stream(stream):
+                check(lib().qfb_set_stream(stream.cuda_stream), "qfb_set_stream")
+                ps.d_items[:m].copy_(ps.h_items[:m], non_blocking=True)
+                ps.d_par[:m].copy_(ps.h_par[:m], non_blocking=True)
+                ps.pack.launch(m)
+                ps.h_en[:m].copy_(ps.d_en[:m], non_blocking=True)
+                if any(r.mode for r in reqs):
+                    ps.h_gr[:m].copy_(ps.d_gr[:m], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+            b = _Batch()
+            b.slot, b.reqs, b.stream, b.event, b.mode, b.key = None, reqs, stream, ev, -1, g
+            b.pack = ps
+            b.t_launch = time.perf_counter()
+            self._inflight.append(b)
+            self._batches += 1
+            self._rows += m
+            n += 1
+        return n
+
     # ---- the loop ----------------------------------------------------------
     def _loop(self):
         import torch
         try:
             torch.cuda.set_device(self.device)
             self._free_streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
+            self._build_packs()
             while True:
                 got = self._drain()
                 done = self._complete()
+                if not self._repack.empty() and not any(b.pack for b in self._inflight):
+                    self._build_packs()  # problems registered while running
+                    while not self._repack.empty():
+                        self._repack.get().set()
                 launched = self._launch()
                 if self._stop.is_set() and not self._inflight and not self._waiting \
                         and self._inbox.empty():
@@ -241,6 +365,22 @@ class Server:
         for b in self._inflight:
             if not b.event.query():
                 still.append(b)
+                continue
+            if b.pack is not None:
+                ps = b.pack
+                en, gr = ps.h_en.numpy(), ps.h_gr.numpy()
+                now = time.perf_counter()
+                for i, r in enumerate(b.reqs):
+                    g = gr[i, :r.params.shape[0]].copy() if r.mode else None
+                    r.future.set_result((float(en[i]), g))
+                    with self._lock:
+                        self._lat.append(now - r.t_submit)
+                        self._done += 1
+                with self._lock:
+                    self._t_last = now
+                self._pack_free[b.key].append(ps)
+                self._free_streams.append(b.stream)
+                n += 1
                 continue
             s = b.slot
             en = s.h_en.numpy()
@@ -297,15 +437,21 @@ class Server:
         for lst in self._idle.values():
             lst.clear()
         self._idle.clear()
+        self._pack_free = []
+        self._pack_of = {}
+        self._pack_bytes = 0
         self._live_bytes = 0
+        while not self._repack.empty():
+            self._repack.get().set()
 
     def _launch(self):
         import torch
-        n = 0
+        n = self._launch_packs()
         blocked_oldest = False
         while self._free_streams and self._waiting:
             # the problem whose oldest request has waited longest goes first
-            order = sorted(self._waiting.items(), key=lambda kv: kv[1][0].t_submit)
+            order = sorted(((k, dq) for k, dq in self._waiting.items() if k[0] not in self._pack_of),
+                           key=lambda kv: kv[1][0].t_submit)
             started = False
             for (key, mode), dq in order:
                 ducc = self._problems[key]
@@ -347,6 +493,7 @@ class Server:
             ev.record(stream)
         b = _Batch()
         b.slot, b.reqs, b.stream, b.event, b.mode, b.key = slot, reqs, stream, ev, mode, key
+        b.pack = None
         b.t_launch = time.perf_counter()
         self._inflight.append(b)
         self._batches += 1

@@ -41,8 +41,8 @@ from .sq_op_pool import SQOpPool, find_irrep
 from .sq_operator import SQOperator
 from .utils import build_refprep, compact_excitation_circuit, ref_to_basis_idx, trotterize
 
-__all__ = ["DUCC", "Evaluator", "evaluator_config", "UCCNVQE", "ADAPTVQE", "UCCNPQE", "SPQE",
-           "ansatz_strings", "gradient_strings"]
+__all__ = ["DUCC", "Evaluator", "Pack", "evaluator_config", "UCCNVQE", "ADAPTVQE", "UCCNPQE",
+           "SPQE", "ansatz_strings", "gradient_strings"]
 
 
 def evaluator_config(compact=True):
@@ -211,6 +211,84 @@ class Evaluator:
         try:
             if self.h:
                 lib().qfb_ucc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class Pack:
+    """Parameter sets of several dUCC problems evaluated in one launch
+    (qfb_pack_*): every problem must take the compact shared-memory path
+    (``Evaluator.path == 2``: up to ~16 qubits) with the same state storage.
+    Item i of a run evaluates ``params[i]`` of problem ``members[i]`` (an index
+    into ``duccs``), with its gradient when asked; one CTA per item."""
+
+    def __init__(self, duccs, capacity=256):
+        self.duccs = list(duccs)
+        self._evs = [d.evaluator(1) for d in self.duccs]  # members: kept alive with the pack
+        arr = (ctypes.c_void_p * len(self._evs))(*[ev.h.value for ev in self._evs])
+        h = ctypes.c_void_p()
+        check(lib().qfb_pack_create(arr, len(self._evs), int(capacity), ctypes.byref(h)),
+              "qfb_pack_create")
+        self.h = h
+        cap, mp, nb = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_uint64()
+        check(lib().qfb_pack_info(h, ctypes.byref(cap), ctypes.byref(mp), ctypes.byref(nb)))
+        self.capacity, self.maxparam, self.pack_bytes = cap.value, mp.value, nb.value
+        pi, pp, pe, pg = (ctypes.c_void_p() for _ in range(4))
+        check(lib().qfb_pack_buffers(h, ctypes.byref(pi), ctypes.byref(pp), ctypes.byref(pe),
+                                     ctypes.byref(pg)))
+        self._addr = (pi.value, pp.value, pe.value, pg.value)
+
+    @property
+    def device_bytes(self):
+        """Device memory of the pack and of its member evaluators."""
+        return self.pack_bytes + sum(ev.device_bytes for ev in self._evs)
+
+    def run(self, members, params, with_grad=True):
+        """Energies [n] and gradients (a list of per-item arrays, None where not
+        asked) of items (members[i], params[i])."""
+        n = len(members)
+        m = np.ascontiguousarray(members, dtype=np.int32)
+        wg = np.broadcast_to(np.asarray(with_grad, dtype=np.int32), (n,)).copy()
+        P = np.zeros((max(n, 1), self.maxparam))
+        for i, (k, p) in enumerate(zip(m, params)):
+            p = np.asarray(p, dtype=np.float64).reshape(-1)
+            if not 0 <= k < len(self.duccs) or p.shape[0] != self.duccs[k].nparam:
+                raise ValueError(f"item {i}: member {k} with {p.shape[0]} parameters")
+            P[i, :p.shape[0]] = p
+        e = np.empty(max(n, 1))
+        g = np.empty((max(n, 1), self.maxparam))
+        check(lib().qfb_pack_run(self.h, ptr(m), ptr(wg), n, ptr(P), ptr(e), ptr(g)),
+              "qfb_pack_run")
+        grads = [g[i, :self.duccs[k].nparam].copy() if wg[i] else None for i, k in enumerate(m)]
+        return e[:n].copy(), grads
+
+    def tensors(self):
+        """(items int32 [capacity, 2], params, energy, grad) as torch CUDA views
+        of the device blocks, for callers that stage copies on their own
+        streams and enqueue ``launch``."""
+        import torch
+
+        def view(addr, shape, typestr):
+            class _I:
+                __cuda_array_interface__ = {"shape": shape, "typestr": typestr,
+                                            "data": (int(addr), False), "version": 2}
+            return torch.as_tensor(_I(), device="cuda")
+
+        ai, ap, ae, ag = self._addr
+        C, MP = self.capacity, self.maxparam
+        return (view(ai, (C, 2), "<i4"), view(ap, (C, MP), "<f8"), view(ae, (C,), "<f8"),
+                view(ag, (C, MP), "<f8"))
+
+    def launch(self, nitems):
+        """Enqueue the first ``nitems`` items of the device blocks on the
+        library's stream."""
+        check(lib().qfb_pack_launch(self.h, int(nitems)), "qfb_pack_launch")
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().qfb_pack_destroy(self.h)
                 self.h = None
         except Exception:
             pass
