@@ -419,7 +419,11 @@ def measure_gradient3(nqubit, ref, kops, amps, hterms, pool_kops):
 # --------------------------------------------------------------------------
 
 
-def load_reference(ref_src="/root/reference/src/qforte"):
+# The reference's Python sources: $QFORTE_REF_SRC, else the build container's copy.
+REF_SRC_DEFAULT = os.environ.get("QFORTE_REF_SRC", "/root/reference/src/qforte")
+
+
+def load_reference(ref_src=REF_SRC_DEFAULT):
     """Import the reference package with its compiled module from oracle/_ref.
 
     The package's Python sources are used where they lie; its extension
