@@ -94,6 +94,8 @@ def parse():
     ap.add_argument("--dense", type=int, default=0,
                     help="gate sweep: fuse runs into dense 5- or 6-qubit blocks on the FP64 "
                          "tensor cores (0: tile runs)")
+    ap.add_argument("--complex64", action="store_true",
+                    help="gate sweep: the complex64 throughput variant (FP32 arithmetic)")
     ap.add_argument("--autotune", action="store_true",
                     help="gate sweep: pick the tile shape per qubit count with the autotuner")
     return ap.parse_args()
@@ -325,7 +327,10 @@ def run_gates(a, rank, world, local, emit=True):
             tuned, _ = tune_gates(circ, n, reps=1, store=False)
         nw, nsingle, pass_bytes = gate_plan(circ.gates(), n)
         nphase, _ = gate_phases(circ.gates(), n)
-        qc = qb.Computer(n)
+        c64 = getattr(a, "complex64", False)
+        if c64:
+            pass_bytes /= 2.0  # 8-byte amplitudes
+        qc = qb.ComputerC64(n) if c64 else qb.Computer(n)
         for _ in range(max(a.warmup, 3) if n < 28 else 1):
             qc.apply_circuit(circ)
         steps = a.steps if n < 28 else 1
@@ -347,14 +352,16 @@ def run_gates(a, rank, world, local, emit=True):
                      "register_phases": nphase, "one_gate_passes": nsingle,
                      "ms_per_circuit": ms, "pass_gbs": gbs,
                      "frac_of_hbm": gbs / peak,
-                     "effective_gate_gbs": len(spec) * 32.0 * 2 ** n / (ms * 1e-3) / 1e9,
+                     "effective_gate_gbs": len(spec) * (16.0 if c64 else 32.0) * 2 ** n /
+                                           (ms * 1e-3) / 1e9,
                      "gpu_launches": launches,
                      "tile": list(tuned) if tuned else a.tile})
         del qc
     last = rows[-1]
     line = {"metric": GATE_METRIC, "value": last["pass_gbs"], "unit": "GB/s", "n_gpus": 1,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": last["ms_per_circuit"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 (throughput only)" if getattr(a, "complex64", False) else "c128",
             "data": "synthetic",
             "config": {"workload": f"layered random circuits, {a.layers} layers, "
                                    f"{','.join(map(str, ns))} qubits, from |0...0>",
@@ -980,8 +987,9 @@ def serve_saturating(a, local, rate=100000.0, duration=0.3, norbs=(5, 6, 7, 8)):
 def secondary(a, local):
     """The metric's other numbers, timed in the same process after the
     headline: gate-sweep passes at 28 qubits (register-blocked tile runs and
-    one pass per gate), Pauli-exponential passes at 28 qubits, and serving
-    latency at a saturating arrival rate."""
+    one pass per gate) and at 32 qubits (tile runs, one 64 GiB state),
+    Pauli-exponential passes at 28 qubits, and serving latency at a
+    saturating arrival rate."""
     from qforte_b200.device import gates_config
     out = {}
     g = argparse.Namespace(**vars(a))
@@ -993,9 +1001,20 @@ def secondary(a, local):
         one = run_gates(g, 0, 1, local, emit=False)
     finally:
         gates_config(0, 3, 0)
+    try:
+        g.tile, g.layers, g.nqubits = 0, 10, "32"
+        big = run_gates(g, 0, 1, local, emit=False)
+    finally:
+        gates_config(0, 3, 0)
+    r = big["sweep"][-1]
+    out["gates32_tile_runs"] = {"layers": 10, "gates": r["gates"], "passes": r["passes"],
+                                "ms_per_circuit": r["ms_per_circuit"], "pass_gbs": r["pass_gbs"],
+                                "frac_of_hbm": r["frac_of_hbm"],
+                                "effective_gate_gbs": r["effective_gate_gbs"],
+                                "state_bytes": 16 << 32}
     for name, ln in (("tile_runs", tile), ("one_pass_per_gate", one)):
         r = ln["sweep"][-1]
-        out[f"gates28_{name}"] = {"layers": g.layers if name != "tile_runs" else 100,
+        out[f"gates28_{name}"] = {"layers": 20 if name != "tile_runs" else 100,
                                   "gates": r["gates"], "passes": r["passes"],
                                   "ms_per_circuit": r["ms_per_circuit"], "pass_gbs": r["pass_gbs"],
                                   "frac_of_hbm": r["frac_of_hbm"],

@@ -131,6 +131,22 @@ QFB_API int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates);
  * each fix R mixing qubits.  No counterpart in the reference; set by the
  * autotuner. */
 QFB_API int qfb_gates_config(int tile_bits, int low_bits);
+/* ---- complex64 states: throughput only -------------------------------------
+ * A state of 2^n complex64 amplitudes (interleaved float re, im) for the
+ * complex64 variant of the gate sweep.  Gates are applied as for complex128
+ * states (the same planning, register-blocked tile runs and one-gate passes)
+ * with FP32 arithmetic; never used for parity with the reference, whose
+ * Computer is complex128 only.  No counterpart in the reference. */
+typedef struct qfb_state_c64_s *qfb_state_c64;
+QFB_API int qfb_c64_create(int nqubit, qfb_state_c64 *out); /* |0...0> */
+QFB_API int qfb_c64_destroy(qfb_state_c64 s);
+QFB_API int qfb_c64_reset(qfb_state_c64 s);
+QFB_API int qfb_c64_upload(qfb_state_c64 s, const float *host, uint64_t n);
+QFB_API int qfb_c64_download(qfb_state_c64 s, float *host, uint64_t n);
+QFB_API int qfb_c64_apply_gates(qfb_state_c64 s, const qfb_gate *gates, int64_t ngates);
+/* sum of |amplitude|^2, accumulated in FP64 */
+QFB_API int qfb_c64_norm2(qfb_state_c64 s, double *out);
+
 /* Dense blocks on the FP64 tensor cores, process-wide: k = 5 or 6 makes
  * qfb_apply_gates fuse each run of gates on at most k qubits into one 2^k x 2^k
  * unitary (the product of the gates as Computer::apply_gate applies them,

@@ -15,7 +15,7 @@ from .qubit_operator import QubitOperator
 from .sq_operator import SQOperator
 from .sq_op_pool import QubitOpPool, SQOpPool, find_irrep
 from .qubit_basis import QubitBasis
-from .computer import (Computer, add_gate_to_computer, inner_product,
+from .computer import (Computer, ComputerC64, add_gate_to_computer, inner_product,
                        prepare_computer_from_circuit, prepare_computer_from_gates)
 from .utils import (build_circuit, build_operator, build_refprep, compact_excitation_circuit,
                     exponentiate_pauli_string, integer_to_ref, local_timer, ref_string, smart_print,

@@ -46,6 +46,13 @@ SIGNATURES = {
     "qfb_launch_count": (ctypes.c_int, [_vp]),
     "qfb_set_tile_wait_limit": (ctypes.c_int, [_u64]),
     "qfb_gates_dense": (ctypes.c_int, [ctypes.c_int]),
+    "qfb_c64_create": (ctypes.c_int, [ctypes.c_int, _vp]),
+    "qfb_c64_destroy": (ctypes.c_int, [_vp]),
+    "qfb_c64_reset": (ctypes.c_int, [_vp]),
+    "qfb_c64_upload": (ctypes.c_int, [_vp, _vp, _u64]),
+    "qfb_c64_download": (ctypes.c_int, [_vp, _vp, _u64]),
+    "qfb_c64_apply_gates": (ctypes.c_int, [_vp, _vp, _i64]),
+    "qfb_c64_norm2": (ctypes.c_int, [_vp, _vp]),
     "qfb_pack_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
     "qfb_pack_destroy": (ctypes.c_int, [_vp]),
     "qfb_pack_info": (ctypes.c_int, [_vp, _vp, _vp, _vp]),

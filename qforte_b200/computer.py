@@ -30,7 +30,7 @@ from .pauli import ipow_mul
 from .qubit_basis import QubitBasis
 from .qubit_operator import QubitOperator, to_string
 
-__all__ = ["Computer", "inner_product", "prepare_computer_from_circuit",
+__all__ = ["Computer", "ComputerC64", "inner_product", "prepare_computer_from_circuit",
            "prepare_computer_from_gates", "add_gate_to_computer", "set_sampling_seed"]
 
 
@@ -475,3 +475,53 @@ def add_gate_to_computer(gate, computer):
     qc = Computer(computer)
     qc.apply_gate(gate)
     return qc
+
+
+class ComputerC64:
+    """A complex64 state for gate-sweep throughput (qfb_c64_*): the gate path
+    of Computer.apply_circuit with FP32 arithmetic and half the bytes per
+    amplitude.  Not a drop-in for the reference's Computer (complex128 only)
+    and never used where results are compared with it."""
+
+    def __init__(self, nqubits):
+        self._n = int(nqubits)
+        h = ctypes.c_void_p()
+        check(lib().qfb_c64_create(self._n, ctypes.byref(h)), "qfb_c64_create")
+        self._h = h
+
+    def get_nqubit(self):
+        return self._n
+
+    def reset(self):
+        check(lib().qfb_c64_reset(self._h), "qfb_c64_reset")
+
+    def set_coeff_vec(self, c_vec):
+        v = np.ascontiguousarray(c_vec, dtype=np.complex64)
+        if v.shape != (1 << self._n,):
+            raise ValueError(f"expected {1 << self._n} amplitudes, got {v.shape}")
+        check(lib().qfb_c64_upload(self._h, ptr(v), v.size), "qfb_c64_upload")
+
+    def get_coeff_array(self):
+        out = np.empty(1 << self._n, dtype=np.complex64)
+        check(lib().qfb_c64_download(self._h, ptr(out), out.size), "qfb_c64_download")
+        return out
+
+    def apply_circuit(self, qc):
+        """The circuit's gates (gates beyond the state raise ValueError)."""
+        arr = pack_gates(qc.gates())
+        check(lib().qfb_c64_apply_gates(self._h, arr.ctypes.data if len(arr) else None, len(arr)),
+              "qfb_c64_apply_gates")
+
+    def norm2(self):
+        out = ctypes.c_double()
+        check(lib().qfb_c64_norm2(self._h, ctypes.byref(out)), "qfb_c64_norm2")
+        return out.value
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().qfb_c64_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+

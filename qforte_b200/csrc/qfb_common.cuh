@@ -72,6 +72,30 @@ __device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
 __device__ __forceinline__ double2 c_add(double2 a, double2 b) {
     return make_double2(a.x + b.x, a.y + b.y);
 }
+// complex64 amplitudes (the throughput-only variant of the gate kernels)
+__device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+
+// An amplitude type's scalar, its constructor and the conversion of a
+// complex128 matrix entry to it (identities for complex128).
+template <class A>
+struct AmpT;
+template <>
+struct AmpT<double2> {
+    using S = double;
+    __device__ __forceinline__ static double2 make(double re, double im) { return make_double2(re, im); }
+    __device__ __forceinline__ static double2 cvt(double2 v) { return v; }
+};
+template <>
+struct AmpT<float2> {
+    using S = float;
+    __device__ __forceinline__ static float2 make(float re, float im) { return make_float2(re, im); }
+    __device__ __forceinline__ static float2 cvt(double2 v) {
+        return make_float2((float)v.x, (float)v.y);
+    }
+};
 // conj(a) * b
 __device__ __forceinline__ double2 c_cjmul(double2 a, double2 b) {
     return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);

@@ -20,6 +20,7 @@
 #include <cstdarg>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -117,8 +118,11 @@ struct Gate4 {  // generic 2-qubit matrix
     double2 m[16];
 };
 
-__global__ void k_gate2(double2 *__restrict__ psi, uint64_t nbasis, Gate2 g) {
-    double2 *s = psi + (uint64_t)blockIdx.y * nbasis;
+template <class A = double2>
+__global__ void k_gate2(A *__restrict__ psi, uint64_t nbasis, Gate2 g) {
+    A *s = psi + (uint64_t)blockIdx.y * nbasis;
+    const A ga = AmpT<A>::cvt(g.a), gb = AmpT<A>::cvt(g.b), gc = AmpT<A>::cvt(g.cc),
+            gd = AmpT<A>::cvt(g.d);
     const uint64_t tbit = 1ull << g.t;
     const uint64_t npair = (g.c < 0) ? (nbasis >> 1) : (nbasis >> 2);
     const int lo = (g.c < 0) ? g.t : min(g.t, g.c);
@@ -130,26 +134,27 @@ __global__ void k_gate2(double2 *__restrict__ psi, uint64_t nbasis, Gate2 g) {
         if (hi >= 0) i0 = insert0(i0, hi) | cbit;
         const uint64_t i1 = i0 | tbit;
         if (g.kind == K_DENSE) {
-            const double2 x0 = s[i0], x1 = s[i1];
-            s[i0] = c_add(c_mul(g.a, x0), c_mul(g.b, x1));
-            s[i1] = c_add(c_mul(g.cc, x0), c_mul(g.d, x1));
+            const A x0 = s[i0], x1 = s[i1];
+            s[i0] = c_add(c_mul(ga, x0), c_mul(gb, x1));
+            s[i1] = c_add(c_mul(gc, x0), c_mul(gd, x1));
         } else if (g.kind == K_DIAG) {
-            if (g.diag_set & 1) s[i0] = c_mul(g.a, s[i0]);
-            if (g.diag_set & 2) s[i1] = c_mul(g.d, s[i1]);
+            if (g.diag_set & 1) s[i0] = c_mul(ga, s[i0]);
+            if (g.diag_set & 2) s[i1] = c_mul(gd, s[i1]);
         } else if (g.kind == K_SWAP) {
-            const double2 x0 = s[i0], x1 = s[i1];
+            const A x0 = s[i0], x1 = s[i1];
             s[i0] = x1;
             s[i1] = x0;
         } else {
-            const double2 x0 = s[i0], x1 = s[i1];
-            s[i0] = c_mul(g.b, x1);
-            s[i1] = c_mul(g.cc, x0);
+            const A x0 = s[i0], x1 = s[i1];
+            s[i0] = c_mul(gb, x1);
+            s[i1] = c_mul(gc, x0);
         }
     }
 }
 
-__global__ void k_gate4(double2 *__restrict__ psi, uint64_t nbasis, Gate4 g) {
-    double2 *s = psi + (uint64_t)blockIdx.y * nbasis;
+template <class A = double2>
+__global__ void k_gate4(A *__restrict__ psi, uint64_t nbasis, Gate4 g) {
+    A *s = psi + (uint64_t)blockIdx.y * nbasis;
     const uint64_t tbit = 1ull << g.t, cbit = 1ull << g.c;
     const int lo = min(g.t, g.c), hi = max(g.t, g.c);
     const uint64_t nquad = nbasis >> 2;
@@ -161,15 +166,16 @@ __global__ void k_gate4(double2 *__restrict__ psi, uint64_t nbasis, Gate4 g) {
         idx[1] = base | tbit;
         idx[2] = base | cbit;
         idx[3] = base | cbit | tbit;
-        double2 x[4], y[4];
+        A x[4], y[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) x[j] = s[idx[j]];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            double2 acc = make_double2(0.0, 0.0);
+            A acc = AmpT<A>::make(0, 0);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (g.nz & (1u << (4 * i + j))) acc = c_add(acc, c_mul(g.m[4 * i + j], x[j]));
+                if (g.nz & (1u << (4 * i + j)))
+                    acc = c_add(acc, c_mul(AmpT<A>::cvt(g.m[4 * i + j]), x[j]));
             y[i] = acc;
         }
 #pragma unroll
@@ -477,19 +483,22 @@ HGate classify_gate(const qfb_gate &g) {
     return h;
 }
 
-// One full-state pass for one gate.
-int launch_single(qfb_state s, const HGate &h) {
+// One full-state pass for one gate, on nbatch states of nbasis amplitudes.
+template <class A>
+int launch_single_t(A *d, uint64_t nbasis, int nbatch, const HGate &h) {
     const dim3 block(256);
     if (h.form == 0) {
-        const uint64_t n = (h.g2.c < 0) ? (s->nbasis >> 1) : (s->nbasis >> 2);
-        k_gate2<<<dim3(grid_for(n, 256), s->nbatch), block, 0, t_stream>>>(s->d, s->nbasis, h.g2);
+        const uint64_t n = (h.g2.c < 0) ? (nbasis >> 1) : (nbasis >> 2);
+        k_gate2<A><<<dim3(grid_for(n, 256), nbatch), block, 0, t_stream>>>(d, nbasis, h.g2);
     } else {
-        k_gate4<<<dim3(grid_for(s->nbasis >> 2, 256), s->nbatch), block, 0, t_stream>>>(
-            s->d, s->nbasis, h.g4);
+        k_gate4<A><<<dim3(grid_for(nbasis >> 2, 256), nbatch), block, 0, t_stream>>>(d, nbasis,
+                                                                                      h.g4);
     }
     QFB_LAUNCHED();
     return QFB_OK;
 }
+
+int launch_single(qfb_state s, const HGate &h) { return launch_single_t(s->d, s->nbasis, s->nbatch, h); }
 
 constexpr int kGateTileDefault = 10;  // 2^10 amplitudes = 18 KB of shared memory per tile
 constexpr int kGateTileMax = 12;
@@ -523,15 +532,17 @@ int gate_tile_smem() {
     static cudaError_t err = cudaSuccess;
     std::call_once(once, [] {
         auto bytes = [](int b) { return (int)(sizeof(double2) * qfbt::tpad_size(b) + 16); };
-        err = cudaFuncSetAttribute(qfbt::k_gate_tile<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   bytes(10));
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(qfbt::k_gate_tile<3>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes(11));
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(qfbt::k_gate_tile<4>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       bytes(kGateTileMax));
+        auto bytes8 = [](int b) { return (int)(sizeof(float2) * qfbt::tpad8_size(b) + 16); };
+        auto attr = [&](const void *f, int n) {
+            if (err == cudaSuccess)
+                err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, n);
+        };
+        attr((const void *)qfbt::k_gate_tile<2>, bytes(10));
+        attr((const void *)qfbt::k_gate_tile<3>, bytes(11));
+        attr((const void *)qfbt::k_gate_tile<4>, bytes(kGateTileMax));
+        attr((const void *)qfbt::k_gate_tile<2, float2>, bytes8(10));
+        attr((const void *)qfbt::k_gate_tile<3, float2>, bytes8(11));
+        attr((const void *)qfbt::k_gate_tile<4, float2>, bytes8(kGateTileMax));
     });
     return err == cudaSuccess ? QFB_OK : cuda_fail(err, "gate tile shared memory");
 }
@@ -653,7 +664,10 @@ bool is_swap4(const WGate &g) {
 // fit in the phase's R register bits together with those already chosen; a
 // gate that cannot join blocks its bits for the rest of the scan, so only
 // gates on disjoint qubits change order.
-void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, TilePlan &tp) {
+// c64: shared offsets in the complex64 tile layout (qfbt::tpad8).
+void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, TilePlan &tp,
+                      bool c64 = false) {
+    auto toff = [c64](uint32_t l) { return c64 ? qfbt::tpad8(l) : qfbt::tpad(l); };
     std::vector<uint32_t> mix((size_t)ng), qm((size_t)ng);
     for (int i = 0; i < ng; ++i) {
         const WGate &w = g[i];
@@ -728,14 +742,14 @@ void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, Til
             uint32_t l = 0;
             for (int p = 0; p < b; ++p)
                 if (pos[p] >= 0 && (k >> pos[p] & 1)) l |= 1u << p;
-            ph.roff[k] = qfbt::tpad(l);
+            ph.roff[k] = toff(l);
         }
         ph.th0 = (int)tp.threads.size();
         for (uint32_t tid = 0; tid < (1u << (b - R)); ++tid) {
             uint32_t tl = 0;
             for (size_t j = 0; j < tb.size(); ++j)
                 if (tid >> j & 1u) tl |= 1u << tb[j];
-            tp.threads.push_back(tl | (qfbt::tpad(tl) << 16));
+            tp.threads.push_back(tl | (toff(tl) << 16));
         }
         ph.o0 = (int)tp.ops.size();
         auto swap2 = [](double2 &x, double2 &y) {
@@ -822,7 +836,7 @@ void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, Til
             uint32_t l = 0;
             for (int p = 0; p < b; ++p)
                 if (pos[p] >= 0 && (((k >> pos[p]) & 1) ^ flip[p])) l |= 1u << p;
-            ph.soff[k] = qfbt::tpad(l);
+            ph.soff[k] = toff(l);
         }
         ph.no = (int)tp.ops.size() - ph.o0;
         tp.ph.push_back(ph);
@@ -991,7 +1005,8 @@ int apply_gates_dense(qfb_state s, const std::vector<HGate> &hg, int K) {
 
 // Runs of a gate list and the phases of each run.
 void plan_gate_tiles(const std::vector<HGate> &hg, int n, int b, int L,
-                     std::vector<GatePlanWin> &wins, TilePlan &tp, std::vector<qfbt::TRun> &runs) {
+                     std::vector<GatePlanWin> &wins, TilePlan &tp, std::vector<qfbt::TRun> &runs,
+                     bool c64 = false) {
     std::vector<WGate> wg;
     plan_gate_windows(hg, n, b, L, wins, wg);
     runs.assign(wins.size(), qfbt::TRun{});
@@ -1003,8 +1018,107 @@ void plan_gate_tiles(const std::vector<HGate> &hg, int n, int b, int L,
         r.ch0 = (int)tp.chunks.size();
         for (uint64_t c = 0; c < (1ull << (pw.w.b - 3)); ++c)
             tp.chunks.push_back(deposit_host(c, pw.w.qmask & ~7ull));
-        plan_tile_phases(wg.data() + pw.w.g0, pw.w.ng, pw.w.b, tile_reg_bits(pw.w.b), r, tp);
+        plan_tile_phases(wg.data() + pw.w.g0, pw.w.ng, pw.w.b, tile_reg_bits(pw.w.b), r, tp, c64);
     }
+}
+
+// Bounds-check and classify a gate list for an nqubit state.
+int classify_gates(const qfb_gate *gates, int64_t ngates, int nqubit, const char *fn,
+                   std::vector<HGate> &hg) {
+    if (ngates < 0 || (ngates > 0 && !gates)) return fail(QFB_EINVAL, "%s: bad gate array", fn);
+    for (int64_t k = 0; k < ngates; ++k) {
+        const qfb_gate &g = gates[k];
+        if (g.target < 0 || g.target >= nqubit || g.control < 0 || g.control >= nqubit)
+            return fail(QFB_EINVAL, "%s: gate %lld acts on qubit (%d, %d) of a %d-qubit state", fn,
+                        (long long)k, g.target, g.control, nqubit);
+    }
+    hg.resize((size_t)ngates);
+    for (int64_t k = 0; k < ngates; ++k) hg[(size_t)k] = classify_gate(gates[k]);
+    return QFB_OK;
+}
+
+// Apply classified gates to nbatch states of 2^n amplitudes of A (double2, or
+// float2 for the complex64 variant): register-blocked tile runs, one pass per
+// gate where a gate joins no run (or the tile shape says so).
+template <class A>
+int apply_gates_tiles(A *d, int n, int nbatch, const std::vector<HGate> &hg) {
+    const uint64_t nbasis = 1ull << n;
+    int b = 0, L = 0;
+    if (!gate_tile_shape(n, b, L) || hg.size() == 1) {
+        for (const HGate &h : hg) {
+            const int rc = launch_single_t(d, nbasis, nbatch, h);
+            if (rc) return rc;
+        }
+        return QFB_OK;
+    }
+    constexpr bool c64 = sizeof(A) == sizeof(float2);
+    std::vector<GatePlanWin> wins;
+    TilePlan tp;
+    std::vector<qfbt::TRun> runs;
+    plan_gate_tiles(hg, n, b, L, wins, tp, runs, c64);
+    // one upload of phases, ops and 4x4 matrices
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t bp = al(sizeof(qfbt::TPhase) * tp.ph.size());
+    const size_t bo = al(sizeof(qfbt::TOp) * tp.ops.size());
+    const size_t bm = al(sizeof(double2) * tp.m4.size());
+    const size_t bc = al(sizeof(uint64_t) * tp.chunks.size());
+    const size_t bt = sizeof(uint32_t) * tp.threads.size();
+    void *buf = nullptr;
+    if (!tp.ph.empty()) {
+        std::vector<unsigned char> host(bp + bo + bm + bc + bt);
+        auto put = [&](size_t off, const void *src, size_t sz) {
+            if (sz) std::memcpy(host.data() + off, src, sz);
+        };
+        put(0, tp.ph.data(), sizeof(qfbt::TPhase) * tp.ph.size());
+        put(bp, tp.ops.data(), sizeof(qfbt::TOp) * tp.ops.size());
+        put(bp + bo, tp.m4.data(), sizeof(double2) * tp.m4.size());
+        put(bp + bo + bm, tp.chunks.data(), sizeof(uint64_t) * tp.chunks.size());
+        put(bp + bo + bm + bc, tp.threads.data(), bt);
+        int rc = dev_alloc(&buf, host.size());
+        if (rc) return rc;
+        QFB_CUDA(cudaMemcpyAsync(buf, host.data(), host.size(), cudaMemcpyHostToDevice, t_stream));
+    }
+    unsigned char *ub = (unsigned char *)buf;
+    const qfbt::TPhase *d_ph = (const qfbt::TPhase *)ub;
+    const qfbt::TOp *d_ops = (const qfbt::TOp *)(ub + bp);
+    const double2 *d_m4 = (const double2 *)(ub + bp + bo);
+    const uint64_t *d_ch = (const uint64_t *)(ub + bp + bo + bm);
+    const uint32_t *d_th = (const uint32_t *)(ub + bp + bo + bm + bc);
+    int rc = gate_tile_smem();
+    for (size_t i = 0; i < wins.size() && rc == QFB_OK; ++i) {
+        const GatePlanWin &pw = wins[i];
+        if (pw.single >= 0) {
+            rc = launch_single_t(d, nbasis, nbatch, hg[pw.single]);
+            continue;
+        }
+        const int tb = pw.w.b, R = tile_reg_bits(tb);
+        const size_t smem = sizeof(A) * qfbt::tpad_size_of<A>(tb) + 16;
+        const dim3 grid((unsigned)(nbasis >> tb), nbatch), block(1u << (tb - R));
+        if (R == 2)
+            qfbt::k_gate_tile<2, A><<<grid, block, smem, t_stream>>>(d, nbasis, runs[i], d_ph, d_ops,
+                                                                     d_m4, d_ch, d_th);
+        else if (R == 3)
+            qfbt::k_gate_tile<3, A><<<grid, block, smem, t_stream>>>(d, nbasis, runs[i], d_ph, d_ops,
+                                                                     d_m4, d_ch, d_th);
+        else
+            qfbt::k_gate_tile<4, A><<<grid, block, smem, t_stream>>>(d, nbasis, runs[i], d_ph, d_ops,
+                                                                     d_m4, d_ch, d_th);
+        rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
+    }
+    dev_free(buf);
+    return rc;
+}
+
+// Sum of |amplitude|^2 of a complex64 state, accumulated in FP64.
+__global__ void k_norm2_c64(const float2 *__restrict__ psi, uint64_t n, double2 *__restrict__ part) {
+    double acc = 0.0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float2 v = psi[i];
+        acc += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    const double2 t = block_sum(make_double2(acc, 0.0));
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
 }  // namespace
@@ -1330,83 +1444,112 @@ int qfb_gates_phases(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t 
 
 int qfb_apply_gates(qfb_state s, const qfb_gate *gates, int64_t ngates) {
     if (!s) return fail(QFB_EINVAL, "qfb_apply_gates: null state");
-    if (ngates < 0 || (ngates > 0 && !gates))
-        return fail(QFB_EINVAL, "qfb_apply_gates: bad gate array");
-    for (int64_t k = 0; k < ngates; ++k) {
-        const qfb_gate &g = gates[k];
-        if (g.target < 0 || g.target >= s->nqubit || g.control < 0 || g.control >= s->nqubit)
-            return fail(QFB_EINVAL,
-                        "qfb_apply_gates: gate %lld acts on qubit (%d, %d) of a %d-qubit state",
-                        (long long)k, g.target, g.control, s->nqubit);
-    }
-    if (ngates == 0) return QFB_OK;
-    std::vector<HGate> hg((size_t)ngates);
-    for (int64_t k = 0; k < ngates; ++k) hg[k] = classify_gate(gates[k]);
+    std::vector<HGate> hg;
+    int rc = classify_gates(gates, ngates, s->nqubit, "qfb_apply_gates", hg);
+    if (rc || ngates == 0) return rc;
     const int n = s->nqubit;
     if (g_gate_dense > 0 && n >= qfbd::kTileBits && ngates > 1)
         return apply_gates_dense(s, hg, g_gate_dense);
-    int b = 0, L = 0;
-    if (!gate_tile_shape(n, b, L) || ngates == 1) {
-        for (const HGate &h : hg) {
-            const int rc = launch_single(s, h);
-            if (rc) return rc;
-        }
-        return QFB_OK;
+    return apply_gates_tiles<double2>(s->d, n, s->nbatch, hg);
+}
+
+// ---- complex64 states: the throughput-only variant of the gate path ---------
+
+struct qfb_state_c64_s {
+    int nqubit;
+    uint64_t nbasis;
+    float2 *d;
+};
+
+int qfb_c64_create(int nqubit, qfb_state_c64 *out) {
+    if (!out) return fail(QFB_EINVAL, "qfb_c64_create: null output");
+    *out = nullptr;
+    if (nqubit < 1 || nqubit > 40)
+        return fail(QFB_EINVAL, "qfb_c64_create: nqubit = %d outside [1, 40]", nqubit);
+    auto s = std::make_unique<qfb_state_c64_s>();
+    s->nqubit = nqubit;
+    s->nbasis = 1ull << nqubit;
+    s->d = nullptr;
+    int rc = dev_alloc((void **)&s->d, s->nbasis * sizeof(float2));
+    if (rc) return rc;
+    qfb_state_c64 h = s.release();
+    rc = qfb_c64_reset(h);
+    if (rc) {
+        qfb_c64_destroy(h);
+        return rc;
     }
-    std::vector<GatePlanWin> wins;
-    TilePlan tp;
-    std::vector<qfbt::TRun> runs;
-    plan_gate_tiles(hg, n, b, L, wins, tp, runs);
-    // one upload of phases, ops and 4x4 matrices
-    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t bp = al(sizeof(qfbt::TPhase) * tp.ph.size());
-    const size_t bo = al(sizeof(qfbt::TOp) * tp.ops.size());
-    const size_t bm = al(sizeof(double2) * tp.m4.size());
-    const size_t bc = al(sizeof(uint64_t) * tp.chunks.size());
-    const size_t bt = sizeof(uint32_t) * tp.threads.size();
+    *out = h;
+    return QFB_OK;
+}
+
+int qfb_c64_destroy(qfb_state_c64 s) {
+    if (!s) return QFB_OK;
+    dev_free(s->d);
+    delete s;
+    return QFB_OK;
+}
+
+int qfb_c64_reset(qfb_state_c64 s) {
+    if (!s) return fail(QFB_EINVAL, "qfb_c64_reset: null state");
+    static const float one[2] = {1.0f, 0.0f};
+    QFB_CUDA(cudaMemsetAsync(s->d, 0, s->nbasis * sizeof(float2), t_stream));
+    QFB_CUDA(cudaMemcpyAsync(s->d, one, sizeof(float2), cudaMemcpyHostToDevice, t_stream));
+    return QFB_OK;
+}
+
+int qfb_c64_upload(qfb_state_c64 s, const float *host, uint64_t n) {
+    if (!s || !host) return fail(QFB_EINVAL, "qfb_c64_upload: null argument");
+    if (n != s->nbasis)
+        return fail(QFB_EINVAL, "qfb_c64_upload: %llu amplitudes for a state of %llu",
+                    (unsigned long long)n, (unsigned long long)s->nbasis);
+    QFB_CUDA(cudaMemcpyAsync(s->d, host, n * sizeof(float2), cudaMemcpyHostToDevice, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return QFB_OK;
+}
+
+int qfb_c64_download(qfb_state_c64 s, float *host, uint64_t n) {
+    if (!s || !host) return fail(QFB_EINVAL, "qfb_c64_download: null argument");
+    if (n != s->nbasis)
+        return fail(QFB_EINVAL, "qfb_c64_download: buffer of %llu for a state of %llu",
+                    (unsigned long long)n, (unsigned long long)s->nbasis);
+    QFB_CUDA(cudaMemcpyAsync(host, s->d, n * sizeof(float2), cudaMemcpyDeviceToHost, t_stream));
+    QFB_CUDA(cudaStreamSynchronize(t_stream));
+    return check_device_waits();
+}
+
+int qfb_c64_apply_gates(qfb_state_c64 s, const qfb_gate *gates, int64_t ngates) {
+    if (!s) return fail(QFB_EINVAL, "qfb_c64_apply_gates: null state");
+    std::vector<HGate> hg;
+    int rc = classify_gates(gates, ngates, s->nqubit, "qfb_c64_apply_gates", hg);
+    if (rc || ngates == 0) return rc;
+    return apply_gates_tiles<float2>(s->d, s->nqubit, 1, hg);
+}
+
+int qfb_c64_norm2(qfb_state_c64 s, double *out) {
+    if (!s || !out) return fail(QFB_EINVAL, "qfb_c64_norm2: null argument");
+    const unsigned nblk = grid_for(s->nbasis, 256, 2);
     void *buf = nullptr;
-    if (!tp.ph.empty()) {
-        std::vector<unsigned char> host(bp + bo + bm + bc + bt);
-        auto put = [&](size_t off, const void *src, size_t n) {
-            if (n) std::memcpy(host.data() + off, src, n);
-        };
-        put(0, tp.ph.data(), sizeof(qfbt::TPhase) * tp.ph.size());
-        put(bp, tp.ops.data(), sizeof(qfbt::TOp) * tp.ops.size());
-        put(bp + bo, tp.m4.data(), sizeof(double2) * tp.m4.size());
-        put(bp + bo + bm, tp.chunks.data(), sizeof(uint64_t) * tp.chunks.size());
-        put(bp + bo + bm + bc, tp.threads.data(), bt);
-        int rc = dev_alloc(&buf, host.size());
-        if (rc) return rc;
-        QFB_CUDA(cudaMemcpyAsync(buf, host.data(), host.size(), cudaMemcpyHostToDevice, t_stream));
-    }
-    unsigned char *ub = (unsigned char *)buf;
-    const qfbt::TPhase *d_ph = (const qfbt::TPhase *)ub;
-    const qfbt::TOp *d_ops = (const qfbt::TOp *)(ub + bp);
-    const double2 *d_m4 = (const double2 *)(ub + bp + bo);
-    const uint64_t *d_ch = (const uint64_t *)(ub + bp + bo + bm);
-    const uint32_t *d_th = (const uint32_t *)(ub + bp + bo + bm + bc);
-    int rc = gate_tile_smem();
-    for (size_t i = 0; i < wins.size() && rc == QFB_OK; ++i) {
-        const GatePlanWin &pw = wins[i];
-        if (pw.single >= 0) {
-            rc = launch_single(s, hg[pw.single]);
-            continue;
-        }
-        const int tb = pw.w.b, R = tile_reg_bits(tb);
-        const size_t smem = sizeof(double2) * qfbt::tpad_size(tb) + 16;
-        const dim3 grid((unsigned)(s->nbasis >> tb), s->nbatch), block(1u << (tb - R));
-        if (R == 2)
-            qfbt::k_gate_tile<2><<<grid, block, smem, t_stream>>>(s->d, s->nbasis, runs[i], d_ph,
-                                                                  d_ops, d_m4, d_ch, d_th);
-        else if (R == 3)
-            qfbt::k_gate_tile<3><<<grid, block, smem, t_stream>>>(s->d, s->nbasis, runs[i], d_ph,
-                                                                  d_ops, d_m4, d_ch, d_th);
-        else
-            qfbt::k_gate_tile<4><<<grid, block, smem, t_stream>>>(s->d, s->nbasis, runs[i], d_ph,
-                                                                  d_ops, d_m4, d_ch, d_th);
+    int rc = dev_alloc(&buf, sizeof(double2) * ((size_t)nblk + 1));
+    if (rc) return rc;
+    double2 *part = (double2 *)buf, *res = part + nblk;
+    k_norm2_c64<<<nblk, 256, 0, t_stream>>>(s->d, s->nbasis, part);
+    rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
+    if (rc == QFB_OK) {
+        k_rows_sum<<<1, 256, 0, t_stream>>>(part, nblk, res);
         rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
     }
+    double2 h = make_double2(0.0, 0.0);
+    if (rc == QFB_OK) {
+        const cudaError_t e = cudaMemcpyAsync(&h, res, sizeof(double2), cudaMemcpyDeviceToHost,
+                                              t_stream);
+        rc = e == cudaSuccess ? QFB_OK : cuda_fail(e, "qfb_c64_norm2");
+    }
+    if (rc == QFB_OK) {
+        const cudaError_t e = cudaStreamSynchronize(t_stream);
+        rc = e == cudaSuccess ? QFB_OK : cuda_fail(e, "qfb_c64_norm2");
+    }
     dev_free(buf);
+    if (rc == QFB_OK) *out = h.x;
     return rc;
 }
 

@@ -93,6 +93,12 @@ __host__ __device__ __forceinline__ uint32_t tpad(uint32_t l) {
 // Elements (16 bytes) a padded tile of 2^b amplitudes occupies.
 __host__ __device__ __forceinline__ uint32_t tpad_size(int b) { return tpad((1u << b) - 1u) + 1u; }
 
+// The same layout for 8-byte (complex64) elements: two elements of padding
+// where complex128 has one, so every 8-element chunk still starts on a
+// 16-byte boundary (the bulk copies need it) and stays contiguous.
+__host__ __device__ __forceinline__ uint32_t tpad8(uint32_t l) { return 2u * tpad(l) - l; }
+__host__ __device__ __forceinline__ uint32_t tpad8_size(int b) { return tpad8((1u << b) - 1u) + 2u; }
+
 // ---- PTX helpers: mbarrier and bulk copies ---------------------------------
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -166,9 +172,8 @@ __device__ __forceinline__ void fence_async_smem() {
 
 // f(x0, x1) on every pair (k, k | 2^T) of registers with k & cm == cv (a
 // control on register bits, uniform across the CTA; cm = 0: every pair).
-template <int R, int T, class F>
-__device__ __forceinline__ void for_pairs(double2 (&v)[1 << R], uint32_t cm, uint32_t cv,
-                                          const F &f) {
+template <int R, int T, class F, class A>
+__device__ __forceinline__ void for_pairs(A (&v)[1 << R], uint32_t cm, uint32_t cv, const F &f) {
     if constexpr (T < R) {
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) {
@@ -178,41 +183,46 @@ __device__ __forceinline__ void for_pairs(double2 (&v)[1 << R], uint32_t cm, uin
     }
 }
 
+template <class A>
 struct FDense {  // complex 2x2
-    double2 a, b, c, d;
-    __device__ __forceinline__ void operator()(double2 &x0, double2 &x1) const {
-        const double2 y0 = c_add(c_mul(a, x0), c_mul(b, x1));
+    A a, b, c, d;
+    __device__ __forceinline__ void operator()(A &x0, A &x1) const {
+        const A y0 = c_add(c_mul(a, x0), c_mul(b, x1));
         x1 = c_add(c_mul(c, x0), c_mul(d, x1));
         x0 = y0;
     }
 };
+template <class A>
 struct FReal {  // real 2x2
-    double a, b, c, d;
-    __device__ __forceinline__ void operator()(double2 &x0, double2 &x1) const {
-        const double2 y0 = make_double2(a * x0.x + b * x1.x, a * x0.y + b * x1.y);
-        x1 = make_double2(c * x0.x + d * x1.x, c * x0.y + d * x1.y);
+    typename AmpT<A>::S a, b, c, d;
+    __device__ __forceinline__ void operator()(A &x0, A &x1) const {
+        const A y0 = AmpT<A>::make(a * x0.x + b * x1.x, a * x0.y + b * x1.y);
+        x1 = AmpT<A>::make(c * x0.x + d * x1.x, c * x0.y + d * x1.y);
         x0 = y0;
     }
 };
+template <class A>
 struct FRxi {  // a, d real; b = i bi, c = i ci
-    double a, bi, ci, d;
-    __device__ __forceinline__ void operator()(double2 &x0, double2 &x1) const {
-        const double2 y0 = make_double2(a * x0.x - bi * x1.y, a * x0.y + bi * x1.x);
-        x1 = make_double2(d * x1.x - ci * x0.y, d * x1.y + ci * x0.x);
+    typename AmpT<A>::S a, bi, ci, d;
+    __device__ __forceinline__ void operator()(A &x0, A &x1) const {
+        const A y0 = AmpT<A>::make(a * x0.x - bi * x1.y, a * x0.y + bi * x1.x);
+        x1 = AmpT<A>::make(d * x1.x - ci * x0.y, d * x1.y + ci * x0.x);
         x0 = y0;
     }
 };
 struct FPswap {
-    __device__ __forceinline__ void operator()(double2 &x0, double2 &x1) const {
-        const double2 t = x0;
+    template <class A>
+    __device__ __forceinline__ void operator()(A &x0, A &x1) const {
+        const A t = x0;
         x0 = x1;
         x1 = t;
     }
 };
+template <class A>
 struct FAnti {
-    double2 b, c;
-    __device__ __forceinline__ void operator()(double2 &x0, double2 &x1) const {
-        const double2 t = x0;
+    A b, c;
+    __device__ __forceinline__ void operator()(A &x0, A &x1) const {
+        const A t = x0;
         x0 = c_mul(b, x1);
         x1 = c_mul(c, t);
     }
@@ -220,9 +230,8 @@ struct FAnti {
 
 // diagonal on register bit T: a where the bit is 0 (DS & 1), d where it is 1
 // (DS & 2), on the registers with k & cm == cv
-template <int R, int T, int DS>
-__device__ __forceinline__ void ap_diag(double2 (&v)[1 << R], uint32_t cm, uint32_t cv, double2 a,
-                                        double2 d) {
+template <int R, int T, int DS, class A>
+__device__ __forceinline__ void ap_diag(A (&v)[1 << R], uint32_t cm, uint32_t cv, A a, A d) {
     if constexpr (T < R) {
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) {
@@ -237,8 +246,8 @@ __device__ __forceinline__ void ap_diag(double2 (&v)[1 << R], uint32_t cm, uint3
 }
 
 // one factor on the registers with k & cm == cv
-template <int R>
-__device__ __forceinline__ void ap_scale(double2 (&v)[1 << R], uint32_t cm, uint32_t cv, double2 f) {
+template <int R, class A>
+__device__ __forceinline__ void ap_scale(A (&v)[1 << R], uint32_t cm, uint32_t cv, A f) {
 #pragma unroll
     for (int k = 0; k < (1 << R); ++k)
         if (((uint32_t)k & cm) == cv) v[k] = c_mul(f, v[k]);
@@ -255,18 +264,20 @@ __device__ __forceinline__ double2 ld_entry(const double2 *p) {
 // Matrix index (bit C << 1) | bit T; each output is the sum over the inputs
 // in column order.  The host zeroes the entries the reference skips (|m| <=
 // 1e-16, computer.cc:721-750), so their products add exact zeros.
-template <int R, int T, int C>
-__device__ __forceinline__ void ap_gen4(double2 (&v)[1 << R], const double2 *__restrict__ m) {
+template <int R, int T, int C, class A>
+__device__ __forceinline__ void ap_gen4(A (&v)[1 << R], const double2 *__restrict__ m) {
     if constexpr (T < R && C < R && T != C) {
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) {
             if (k & ((1 << T) | (1 << C))) continue;
             const int i0 = k, i1 = k | (1 << T), i2 = k | (1 << C), i3 = k | (1 << T) | (1 << C);
-            double2 y[4];
+            A y[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const double2 m0 = ld_entry(m + 4 * i), m1 = ld_entry(m + 4 * i + 1),
-                              m2 = ld_entry(m + 4 * i + 2), m3 = ld_entry(m + 4 * i + 3);
+                const A m0 = AmpT<A>::cvt(ld_entry(m + 4 * i)),
+                        m1 = AmpT<A>::cvt(ld_entry(m + 4 * i + 1)),
+                        m2 = AmpT<A>::cvt(ld_entry(m + 4 * i + 2)),
+                        m3 = AmpT<A>::cvt(ld_entry(m + 4 * i + 3));
                 y[i] = c_add(c_add(c_add(c_mul(m0, v[i0]), c_mul(m1, v[i1])), c_mul(m2, v[i2])),
                              c_mul(m3, v[i3]));
             }
@@ -279,14 +290,14 @@ __device__ __forceinline__ void ap_gen4(double2 (&v)[1 << R], const double2 *__r
 }
 
 // SWAP of register bits T and C
-template <int R, int T, int C>
-__device__ __forceinline__ void ap_bswap(double2 (&v)[1 << R]) {
+template <int R, int T, int C, class A>
+__device__ __forceinline__ void ap_bswap(A (&v)[1 << R]) {
     if constexpr (T < R && C < R && T != C) {
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) {
             if ((k & (1 << T)) && !(k & (1 << C))) {
                 const int k2 = k ^ (1 << T) ^ (1 << C);
-                const double2 x = v[k];
+                const A x = v[k];
                 v[k] = v[k2];
                 v[k2] = x;
             }
@@ -298,9 +309,11 @@ __device__ __forceinline__ void ap_bswap(double2 (&v)[1 << R]) {
 #define QFBT_T4(B, X) X(B + 0, 0) X(B + 1, 1) X(B + 2, 2) X(B + 3, 3)
 #define QFBT_TT16(B, X) X(B + 0, 0, 0) X(B + 1, 0, 1) X(B + 2, 0, 2) X(B + 3, 0, 3) X(B + 4, 1, 0) X(B + 5, 1, 1) X(B + 6, 1, 2) X(B + 7, 1, 3) X(B + 8, 2, 0) X(B + 9, 2, 1) X(B + 10, 2, 2) X(B + 11, 2, 3) X(B + 12, 3, 0) X(B + 13, 3, 1) X(B + 14, 3, 2) X(B + 15, 3, 3)
 
-template <int R>
-__device__ __forceinline__ void apply_op(double2 (&v)[1 << R], const TOp *__restrict__ op, uint32_t tl,
+template <int R, class A>
+__device__ __forceinline__ void apply_op(A (&v)[1 << R], const TOp *__restrict__ op, uint32_t tl,
                                          const double2 *__restrict__ m4) {
+    using S = typename AmpT<A>::S;
+    auto cv_ = [](double2 z) { return AmpT<A>::cvt(z); };
     const uint4 hdr = __ldg(reinterpret_cast<const uint4 *>(op));
     if ((tl & hdr.y) != hdr.y) return;  // a control on one of the thread's bits is 0
     const uint32_t cm = hdr.w & 0xffu, cv = (hdr.w >> 16) & 0xffu;
@@ -308,46 +321,46 @@ __device__ __forceinline__ void apply_op(double2 (&v)[1 << R], const TOp *__rest
 #define X(N, T)                                                                            \
     case N:                                                                                \
         for_pairs<R, T>(v, cm, cv,                                                         \
-                        FDense{__ldg(&op->m[0]), __ldg(&op->m[1]), __ldg(&op->m[2]),       \
-                               __ldg(&op->m[3])});                                         \
+                        FDense<A>{cv_(__ldg(&op->m[0])), cv_(__ldg(&op->m[1])),            \
+                                  cv_(__ldg(&op->m[2])), cv_(__ldg(&op->m[3]))});          \
         break;
         QFBT_T4(0, X)
 #undef X
 #define X(N, T)                                                                            \
     case N:                                                                                \
         for_pairs<R, T>(v, cm, cv,                                                         \
-                        FReal{__ldg(&op->m[0].x), __ldg(&op->m[1].x), __ldg(&op->m[2].x),  \
-                              __ldg(&op->m[3].x)});                                        \
+                        FReal<A>{(S)__ldg(&op->m[0].x), (S)__ldg(&op->m[1].x),             \
+                                 (S)__ldg(&op->m[2].x), (S)__ldg(&op->m[3].x)});           \
         break;
         QFBT_T4(4, X)
 #undef X
 #define X(N, T)                                                                            \
     case N:                                                                                \
         for_pairs<R, T>(v, cm, cv,                                                         \
-                        FRxi{__ldg(&op->m[0].x), __ldg(&op->m[1].y), __ldg(&op->m[2].y),   \
-                             __ldg(&op->m[3].x)});                                         \
+                        FRxi<A>{(S)__ldg(&op->m[0].x), (S)__ldg(&op->m[1].y),              \
+                                (S)__ldg(&op->m[2].y), (S)__ldg(&op->m[3].x)});            \
         break;
         QFBT_T4(8, X)
 #undef X
 #define X(N, T) case N: for_pairs<R, T>(v, cm, cv, FPswap{}); break;
         QFBT_T4(12, X)
 #undef X
-#define X(N, T) case N: for_pairs<R, T>(v, cm, cv, FAnti{__ldg(&op->m[1]), __ldg(&op->m[2])}); break;
+#define X(N, T) case N: for_pairs<R, T>(v, cm, cv, FAnti<A>{cv_(__ldg(&op->m[1])), cv_(__ldg(&op->m[2]))}); break;
         QFBT_T4(16, X)
 #undef X
-#define X(N, T) case N: ap_diag<R, T, 1>(v, cm, cv, __ldg(&op->m[0]), __ldg(&op->m[3])); break;
+#define X(N, T) case N: ap_diag<R, T, 1>(v, cm, cv, cv_(__ldg(&op->m[0])), cv_(__ldg(&op->m[3]))); break;
         QFBT_T4(20, X)
 #undef X
-#define X(N, T) case N: ap_diag<R, T, 2>(v, cm, cv, __ldg(&op->m[0]), __ldg(&op->m[3])); break;
+#define X(N, T) case N: ap_diag<R, T, 2>(v, cm, cv, cv_(__ldg(&op->m[0])), cv_(__ldg(&op->m[3]))); break;
         QFBT_T4(24, X)
 #undef X
-#define X(N, T) case N: ap_diag<R, T, 3>(v, cm, cv, __ldg(&op->m[0]), __ldg(&op->m[3])); break;
+#define X(N, T) case N: ap_diag<R, T, 3>(v, cm, cv, cv_(__ldg(&op->m[0])), cv_(__ldg(&op->m[3]))); break;
         QFBT_T4(28, X)
 #undef X
         case OPC_DIAG_THREAD: {
             // the diagonal bit is one of this thread's bits: one factor for all registers
             const bool one = (tl & hdr.z) != 0;
-            if ((hdr.w >> 8) & (one ? 2u : 1u)) ap_scale<R>(v, cm, cv, __ldg(&op->m[one ? 3 : 0]));
+            if ((hdr.w >> 8) & (one ? 2u : 1u)) ap_scale<R>(v, cm, cv, cv_(__ldg(&op->m[one ? 3 : 0])));
             break;
         }
 #define X(N, T, C) case N: ap_gen4<R, T, C>(v, m4 + (int)hdr.w); break;
@@ -385,18 +398,32 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 // kWaitLimitNs.
 static __device__ uint64_t g_tile_wait_limit_ns = kWaitLimitNs;
 
+// Offsets in the padded tile for amplitudes of A (the host's tables use the
+// same function).
+template <class A>
+__host__ __device__ __forceinline__ uint32_t tpad_of(uint32_t l) {
+    return sizeof(A) == 16 ? tpad(l) : tpad8(l);
+}
+template <class A>
+__host__ __device__ __forceinline__ uint32_t tpad_size_of(int b) {
+    return sizeof(A) == 16 ? tpad_size(b) : tpad8_size(b);
+}
+
 // One CTA per tile (blockIdx.x: tile position over the qubits outside Q;
-// blockIdx.y: batch slot); 2^(b-R) threads, 2^R amplitudes each.
-template <int R>
+// blockIdx.y: batch slot); 2^(b-R) threads, 2^R amplitudes each.  A: double2
+// (complex128) or float2 (the complex64 throughput variant, arithmetic in
+// FP32); a chunk is 8 amplitudes either way (128 or 64 bytes).
+template <int R, class A = double2>
 __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
-    k_gate_tile(double2 *__restrict__ psi, uint64_t nbasis, TRun run,
+    k_gate_tile(A *__restrict__ psi, uint64_t nbasis, TRun run,
                 const TPhase *__restrict__ phases, const TOp *__restrict__ ops,
                 const double2 *__restrict__ m4, const uint64_t *__restrict__ chunks,
                 const uint32_t *__restrict__ threads) {
     extern __shared__ __align__(128) unsigned char t_smem[];
-    double2 *tile = reinterpret_cast<double2 *>(t_smem);
+    constexpr uint32_t kChunk = 8u * sizeof(A);
+    A *tile = reinterpret_cast<A *>(t_smem);
     const int b = run.b;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(tile + tpad_size(b));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(tile + tpad_size_of<A>(b));
     const uint32_t bar_a = smem_u32(bar);
     const int tid = threadIdx.x, nth = blockDim.x;
     const int nch = 1 << (b - 3);
@@ -404,15 +431,15 @@ __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
 
     if (tid == 0) {
         mbar_init(bar_a, 1);
-        mbar_expect_tx(bar_a, (uint32_t)nch * 128u);
+        mbar_expect_tx(bar_a, (uint32_t)nch * kChunk);
         // tile origin: blockIdx.x's bits on the qubits outside Q, plus the slot
         s_base = (uint64_t)blockIdx.y * nbasis + spread_around(blockIdx.x, run.qmask);
     }
     __syncthreads();
-    double2 *s = psi + s_base;
+    A *s = psi + s_base;
     const uint64_t *ch = chunks + run.ch0;
     for (int c = tid; c < nch; c += nth)
-        bulk_g2s(smem_u32(tile + tpad((uint32_t)c << 3)), s + __ldg(&ch[c]), 128u, bar_a);
+        bulk_g2s(smem_u32(tile + tpad_of<A>((uint32_t)c << 3)), s + __ldg(&ch[c]), kChunk, bar_a);
     const uint64_t limit = g_tile_wait_limit_ns;
     if (limit == 0 || !mbar_wait_bounded(bar_a, 0, limit)) {
         // the copies did not complete in time: flag it, give them a second
@@ -427,13 +454,13 @@ __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
         const TPhase *ph = phases + run.p0 + p;
         const uint32_t tw = __ldg(&threads[__ldg(&ph->th0) + tid]);
         const uint32_t tl = tw & 0xffffu;
-        const double2 *t0 = tile + (tw >> 16);
-        double2 v[1 << R];
+        const A *t0 = tile + (tw >> 16);
+        A v[1 << R];
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) v[k] = t0[__ldg(&ph->roff[k])];
         const int o0 = __ldg(&ph->o0), o1 = o0 + __ldg(&ph->no);
-        for (int o = o0; o < o1; ++o) apply_op<R>(v, ops + o, tl, m4);
-        double2 *t1 = tile + (tw >> 16);
+        for (int o = o0; o < o1; ++o) apply_op<R, A>(v, ops + o, tl, m4);
+        A *t1 = tile + (tw >> 16);
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) t1[__ldg(&ph->soff[k])] = v[k];
         if (p + 1 < run.np) __syncthreads();
@@ -441,7 +468,7 @@ __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
     fence_async_smem();
     __syncthreads();
     for (int c = tid; c < nch; c += nth)
-        bulk_s2g(s + __ldg(&ch[c]), smem_u32(tile + tpad((uint32_t)c << 3)), 128u);
+        bulk_s2g(s + __ldg(&ch[c]), smem_u32(tile + tpad_of<A>((uint32_t)c << 3)), kChunk);
     bulk_commit_and_wait();
 }
 

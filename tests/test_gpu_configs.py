@@ -152,3 +152,34 @@ def test_operator_pool_expectation_values_match_reference(cuda):
     assert np.max(np.abs(ivals - z["idxd_oppl"])) < E_TOL
     # the state is left as it was (the reference restores coeff_, computer.cc:796-803)
     assert np.max(np.abs(qc.get_coeff_array() - z["psi"])) < AMP_TOL
+
+
+def test_gate_sweep_32_qubits_norm_and_inverse(cuda, restore_gates_config):
+    """Config: the gate sweep at its largest size, one 32-qubit complex128
+    state (64 GiB) worked in place.  Neither the oracle nor the reference can
+    hold it (the reference needs 40 bytes an amplitude and overflows 32-bit
+    loop counters there, computer.cc:637-643), so the checks are
+    size-independent: after 10 layers the norm is 1 within 1e-12, and the
+    adjoint circuit returns |0...0> within 1e-12, on the tile runs and on
+    dense 5-qubit blocks."""
+    import torch
+    from qforte_b200.workloads import layered_random_circuit
+    free, _ = torch.cuda.mem_get_info()
+    if free < 70 * 2 ** 30:
+        pytest.skip("needs 64 GiB of free device memory")
+    n = 32
+    circ, spec = layered_random_circuit(n, 10, 43)
+    inv = circ.adjoint()
+    qc = qb.Computer(n)
+    try:
+        for tile, dense in ((0, 0), (0, 5)):
+            restore_gates_config(tile, 3, 0, dense)
+            qc.reset()
+            qc.apply_circuit(circ)
+            assert abs(qb.inner_product(qc, qc) - 1.0) < AMP_TOL
+            assert abs(qc.coeff(0)) < 1.0
+            qc.apply_circuit(inv)
+            assert abs(qc.coeff(0) - 1.0) < AMP_TOL
+            assert abs(qb.inner_product(qc, qc) - 1.0) < AMP_TOL
+    finally:
+        del qc

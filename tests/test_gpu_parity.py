@@ -751,3 +751,29 @@ def test_multi_pattern_steps_on_the_compact_path(cuda, case):
     g_o = O.measure_gradient(10, mol.hf_reference, kf, P[1], hterms,
                              kops_grad=kops_gradient(pool2, tops))
     assert abs(E[1] - E_o) < E_TOL and np.max(np.abs(G[1] - g_o)) < G_TOL
+
+
+@pytest.mark.parametrize("tile,low", [(0, 3), (-1, 4), (12, 3)])
+@pytest.mark.parametrize("n,ngates,seed", [(5, 300, 61), (13, 250, 62), (18, 200, 63)])
+def test_complex64_gates_track_complex128(cuda, gate_tiles, tile, low, n, ngates, seed):
+    """The complex64 throughput variant of the gate path (tile runs and one
+    pass per gate, FP32 arithmetic) against the oracle's complex128 state:
+    within FP32 rounding (3e-6 max-abs after a few hundred gates), norm 1
+    within 1e-5.  Never used for parity with the reference."""
+    from qforte_b200.computer import ComputerC64
+    gate_tiles(tile, low)
+    circ, ora = _rand_circuit(n, ngates, seed)
+    psi0 = _random_state(n, seed)
+    qc = ComputerC64(n)
+    qc.set_coeff_vec(psi0)
+    qc.apply_circuit(circ)
+    st = O.State(n, psi0.copy())
+    st.apply_gates(ora)
+    got = qc.get_coeff_array()
+    assert got.dtype == np.complex64
+    assert np.max(np.abs(got.astype(np.complex128) - st.psi)) < 3e-6
+    assert abs(qc.norm2() - 1.0) < 1e-5
+    qc.reset()
+    assert qc.get_coeff_array()[0] == 1 and abs(qc.norm2() - 1.0) == 0
+    with pytest.raises(ValueError):
+        qc.apply_circuit(qb.build_circuit(f"X_{n}"))
