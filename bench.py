@@ -8,10 +8,13 @@ Workload (one step): 256 parameter sets of the 16-qubit dUCCSD problem
 adjoint gradient.  Metric: evaluations per second (whole job).
 
 * ``value``    device-timed (CUDA events, max over ranks): parameters already in
-               HBM, one graph-captured run per step.
+               HBM, one graph-captured run per step; consecutive steps alternate
+               between two evaluators on two streams (``--streams``), so one
+               step's kernels use the SMs the other leaves idle.
 * ``e2e``      the same through the public API with host buffers: the step's
                parameters copied from pinned host memory and its energies and
-               gradients read back, inside the timed region.
+               gradients read back, inside the timed region (a step's copies
+               overlap the other stream's kernels).
 * ``roofline`` the dominant kernel, timed stage by stage with CUDA events.
 * ``cpu_baseline`` the compiled reference (``oracle/_ref``) on a bounded sample
                of the same workload, on this host's cores (rank 0, N = 1 only).
@@ -60,6 +63,9 @@ def parse():
     ap.add_argument("--norb", type=int, default=8)
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--streams", type=int, default=2,
+                    help="default workload: consecutive steps alternate between this many "
+                         "evaluators, each on its own stream, so their kernels and copies overlap")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the gate-sweep, Pauli-exponential and serving numbers of the "
@@ -141,7 +147,8 @@ def workload_config(a, nterms, nparam):
             "nqubit": 2 * a.norb, "batch": a.batch, "nparam": nparam, "hamiltonian_terms": nterms,
             "l2": f"inputs larger than L2: {2 * a.batch} states x {16 << (2 * a.norb)} B "
                   "resident per step",
-            "parallelism": f"replicas x{a.gpus}"}
+            "parallelism": f"replicas x{a.gpus}",
+            "streams": f"consecutive steps on {max(1, a.streams)} evaluator(s), one stream each"}
 
 
 class Clocks:
@@ -1087,11 +1094,37 @@ def main():
         from qforte_b200.ucc import evaluator_config
         evaluator_config(False)
     eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
-    ev = eng.evaluator(a.batch)
     P = replica_parameters(a.seed, rank, a.batch, M)
-    d_params, d_energy, d_grad = ev.tensors()
-    d_params.copy_(torch.from_numpy(P))
+    # consecutive steps alternate between S evaluators, each on its own stream
+    S = max(1, a.streams)
+    evs = [eng.evaluator(a.batch)]
+    for _ in range(1, S):
+        from qforte_b200.ucc import Evaluator
+        evs.append(Evaluator(eng, a.batch))
+    ev = evs[0]
     stream = torch.cuda.current_stream()
+    streams = [stream] + [torch.cuda.Stream() for _ in range(1, S)]
+    bufs = [e.tensors() for e in evs]
+    for b in bufs:
+        b[0].copy_(torch.from_numpy(P))
+    d_params, d_energy, d_grad = bufs[0]
+
+    def on(k):
+        """Make stream k the library's stream (torch's current one too)."""
+        _lib.check(_lib.lib().qfb_set_stream(_lib.ctypes.c_void_p(streams[k].cuda_stream)))
+        return torch.cuda.stream(streams[k])
+
+    def fork(ev0):
+        # every stream starts after the timed region's opening event
+        for st in streams[1:]:
+            st.wait_event(ev0)
+
+    def join(ev1):
+        for st in streams[1:]:
+            e = torch.cuda.Event()
+            e.record(st)
+            stream.wait_event(e)
+        ev1.record(stream)
 
     def barrier():
         if world > 1:
@@ -1099,7 +1132,9 @@ def main():
 
     # ---- device-resident throughput ----------------------------------------
     for _ in range(max(a.warmup, 3)):
-        ev.run(True)
+        for k in range(S):
+            with on(k):
+                evs[k].run(True)
     torch.cuda.synchronize()
     clocks = Clocks(local)
     barrier()
@@ -1108,9 +1143,11 @@ def main():
     l0 = _lib.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(a.steps):
-        ev.run(True)
-    e1.record(stream)
+    fork(e0)
+    for i in range(a.steps):
+        with on(i % S):
+            evs[i % S].run(True)
+    join(e1)
     torch.cuda.synchronize()
     launches = _lib.launch_count() - l0
     ms = e0.elapsed_time(e1) / a.steps
@@ -1119,7 +1156,9 @@ def main():
     import time as _time
     t_end = _time.perf_counter() + max(0.0, 0.8 - a.steps * ms / 1000.0)
     while _time.perf_counter() < t_end:
-        ev.run(True)
+        for k in range(S):
+            with on(k):
+                evs[k].run(True)
         torch.cuda.synchronize()
     barrier()
     ck = clocks.stop()
@@ -1129,26 +1168,43 @@ def main():
     value = whole_job_rate(world, a.batch, ms_all)
 
     # ---- end to end through the public API with host buffers ---------------
+    # every step copies its parameters from pinned host memory and reads its
+    # energies and gradients back; with S streams a step's copies overlap the
+    # other streams' kernels, and a stream's host buffers are reused only
+    # after its previous step's read-back completed
     hP = torch.from_numpy(P).pin_memory()
-    hE = torch.empty(a.batch, dtype=torch.float64).pin_memory()
-    hG = torch.empty((a.batch, M), dtype=torch.float64).pin_memory()
-    for _ in range(2):
-        ev.eval(P, True)
+    hE = [torch.empty(a.batch, dtype=torch.float64).pin_memory() for _ in range(S)]
+    hG = [torch.empty((a.batch, M), dtype=torch.float64).pin_memory() for _ in range(S)]
+    done = [None] * S
+    for k in range(S):
+        with on(k):
+            evs[k].eval(P, True)
     barrier()
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(a.steps):
-        d_params.copy_(hP, non_blocking=True)
-        ev.run(True)
-        hE.copy_(d_energy, non_blocking=True)
-        hG.copy_(d_grad, non_blocking=True)
-        stream.synchronize()
-    e1.record(stream)
+    fork(e0)
+    for i in range(a.steps):
+        k = i % S
+        if done[k] is not None:
+            done[k].synchronize()  # the host holds step i - S's results
+        with on(k):
+            bufs[k][0].copy_(hP, non_blocking=True)
+            evs[k].run(True)
+            hE[k].copy_(bufs[k][1], non_blocking=True)
+            hG[k].copy_(bufs[k][2], non_blocking=True)
+            done[k] = torch.cuda.Event()
+            done[k].record(streams[k])
+    for d in done:
+        if d is not None:
+            d.synchronize()
+    join(e1)
     torch.cuda.synchronize()
+    _lib.check(_lib.lib().qfb_set_stream(_lib.ctypes.c_void_p(stream.cuda_stream)))
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / a.steps, world, "cuda")
     e2e = whole_job_rate(world, a.batch, ms_e2e)
     # the numbers coming back are the evaluator's
-    assert np.all(np.isfinite(hE.numpy())) and np.all(np.isfinite(hG.numpy()))
+    for k in range(S):
+        assert np.all(np.isfinite(hE[k].numpy())) and np.all(np.isfinite(hG[k].numpy()))
 
     # ---- the plain per-call GPU path: the reference's drivers call for call --
     plain = None
@@ -1256,7 +1312,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
             "config": workload_config(a, len(mol.hamiltonian), M),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(P.nbytes),
-                    "d2h_bytes_per_step": int(hE.numel() * 8 + hG.numel() * 8)},
+                    "d2h_bytes_per_step": int(hE[0].numel() * 8 + hG[0].numel() * 8)},
             "roofline": roof, "gpu_launches": int(launches), "clocks": ck}
     if plain is not None:
         line["plain_per_call"] = plain
