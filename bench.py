@@ -1228,6 +1228,7 @@ def main():
                            "applied, direct_op_exp_val, then the reverse sweep of "
                            "measure_gradient with Computer copies, apply_operator and "
                            "get_coeff_vec readbacks)",
+                 "wall_s": t_p,
                  "energy_abs_diff": abs(E_p - float(e_b[0])),
                  "gradient_max_abs_diff": float(np.max(np.abs(np.asarray(g_p) - g_b[0])))}
 
@@ -1315,8 +1316,29 @@ def main():
                     "d2h_bytes_per_step": int(hE[0].numel() * 8 + hG[0].numel() * 8)},
             "roofline": roof, "gpu_launches": int(launches), "clocks": ck}
     if plain is not None:
+        # the same evaluation through the per-call C ABI with the host work
+        # hoisted (state preparation, H psi, one device gradient call): the
+        # plain path's device time, beside the Python drivers' wall time above
+        import time
+        eng.energy_grad_percall(P[0])
+        torch.cuda.synchronize()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        c0.record(stream)
+        E_c, g_c = eng.energy_grad_percall(P[0])
+        c1.record(stream)
+        torch.cuda.synchronize()
+        t_c = time.perf_counter() - t0
         line["plain_per_call"] = plain
         line["batched_vs_plain"] = value / plain["value"]
+        line["per_call_cabi"] = {"value": 1000.0 / c0.elapsed_time(c1), "unit": UNIT,
+                                 "device_ms": c0.elapsed_time(c1), "wall_s": t_c,
+                                 "sample": "one energy + gradient of parameter row 0, full-space "
+                                           "states, through the per-call C ABI (reference prep, "
+                                           "U(t), H psi, <psi|H psi>, one device gradient call)",
+                                 "energy_abs_diff": abs(E_c - float(e_b[0])),
+                                 "gradient_max_abs_diff": float(np.max(np.abs(g_c - g_b[0])))}
+        line["batched_vs_per_call_cabi"] = value / line["per_call_cabi"]["value"]
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             cb = cpu_baseline(a, mol, pool, P)
