@@ -941,7 +941,7 @@ def run_serve(a, local):
     return line
 
 
-def serve_saturating(a, local, rate=100000.0, duration=0.3, norbs=(5, 6, 7, 8)):
+def serve_saturating(a, local, rate=50000.0, duration=0.4, norbs=(5, 6, 7, 8)):
     """Serving at an arrival rate far above what one request at a time can
     take: a Poisson stream of mixed energy / energy+gradient requests of the
     10-16-qubit dUCCSD problems, served with packed launches (every problem's
