@@ -16,7 +16,9 @@ device.  One serving thread owns the loop:
   requests that arrive while others are on the GPU join the next launch;
 * **overlap** - up to ``streams`` batches (of different problems or of the
   same one) are in flight at once, each on its own stream with its own
-  evaluator, so their kernels share the device;
+  evaluator, so their kernels share the device; at most one of them belongs
+  to a problem of ``heavy_qubits`` or more, so long evaluations never slow
+  each other down;
 * **admission against an HBM budget** - every evaluator's device bytes are
   counted; a batch is admitted only when its evaluator fits in the budget
   (idle evaluators are released oldest first to make room), otherwise its
@@ -96,12 +98,17 @@ class Server:
     bounds the rows of one run; ``streams`` bounds the batches in flight.
     """
 
-    def __init__(self, hbm_budget=150e9, max_batch=256, streams=4, device=0, pack=True):
+    def __init__(self, hbm_budget=150e9, max_batch=256, streams=4, device=0, pack=True,
+                 heavy_qubits=22):
         self.hbm_budget = float(hbm_budget)
         self.max_batch = int(max_batch)
         self.nstreams = int(streams)
         self.device = int(device)
         self.pack = bool(pack)
+        # problems of at least this many qubits take tens of milliseconds a
+        # batch: at most one such batch runs at a time, so two never share the
+        # GPU and stretch each other's latency, while smaller work overlaps it
+        self.heavy_qubits = int(heavy_qubits)
         self._pack_of = {}      # key -> (group, member index) for packed problems
         self._pack_free = []    # per group: idle _PackSlot objects
         self._pack_bytes = 0    # device bytes the packs hold
@@ -452,9 +459,13 @@ class Server:
             # the problem whose oldest request has waited longest goes first
             order = sorted(((k, dq) for k, dq in self._waiting.items() if k[0] not in self._pack_of),
                            key=lambda kv: kv[1][0].t_submit)
+            heavy_busy = any(b.pack is None and self._problems[b.key].nqubit >= self.heavy_qubits
+                             for b in self._inflight)
             started = False
             for (key, mode), dq in order:
                 ducc = self._problems[key]
+                if heavy_busy and ducc.nqubit >= self.heavy_qubits:
+                    continue
                 take = min(len(dq), self._bucket_cap(ducc))
                 bucket = 1 << int(math.ceil(math.log2(take))) if take > 1 else 1
                 # while the oldest problem waits for memory, others may only
