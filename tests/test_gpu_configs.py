@@ -11,8 +11,9 @@ and oppl).  Tolerances as everywhere: amplitudes 1e-12 max-abs, energies
   through torch.autograd;
 * every ADAPT pool gradient of the 20-qubit GSD pool (7,020 operators) in one
   launch, against the reference's measure_gradient3 (uccvqeabc.py:253-283);
-* the 100-layer gate sweep at 20 and 24 qubits on the tile path and on one
-  pass per gate, against the reference's apply_circuit (computer.cc:93-114);
+* the 100-layer gate sweep at 20, 24 and 28 qubits on the tile path, on one
+  pass per gate and in dense 5- and 6-qubit blocks, against the reference's
+  apply_circuit (computer.cc:93-114); 32 qubits by norm and inverse;
 * direct_oppl_exp_val / direct_idxd_oppl_exp_val (computer.cc:773-806).
 """
 
