@@ -691,17 +691,37 @@ constexpr int kPackThreads = 256;
 template <class V>
 __device__ __forceinline__ double p_hpsi(const PackMember &m, const V *psi, V *sig, double *s_red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int U = 4;  // row entries in flight per lane
     double en = 0.0;
     for (int i = warp; i < m.nsec; i += nw) {
         V acc = v_zero(V());
         const int e1 = m.rowptr[i + 1];
-        for (int e = m.rowptr[i] + lane; e < e1; e += 32) {
-            const V x = psi[__ldg(&m.col[e])];
-            if constexpr (sizeof(V) == sizeof(double2)) {
-                if (m.val_c) acc = v_add(acc, v_mul(__ldg(&m.val_c[e]), x));
-                else v_acc(acc, __ldg(&m.val_r[e]), x);
-            } else {
-                v_acc(acc, __ldg(&m.val_r[e]), x);
+        for (int e0 = m.rowptr[i] + lane; e0 < e1; e0 += 32 * U) {
+            uint32_t c[U];
+            double fr[U];
+            double2 fc[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + 32 * u;
+                const bool in = e < e1;
+                c[u] = in ? __ldg(&m.col[e]) : 0u;
+                if (sizeof(V) == sizeof(double2) && m.val_c) {
+                    fc[u] = in ? __ldg(&m.val_c[e]) : make_double2(0.0, 0.0);
+                    fr[u] = 0.0;
+                } else {
+                    fr[u] = in ? __ldg(&m.val_r[e]) : 0.0;
+                    fc[u] = make_double2(0.0, 0.0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const V x = psi[c[u]];
+                if constexpr (sizeof(V) == sizeof(double2)) {
+                    if (m.val_c) acc = v_add(acc, v_mul(fc[u], x));
+                    else v_acc(acc, fr[u], x);
+                } else {
+                    v_acc(acc, fr[u], x);
+                }
             }
         }
         acc = p_sum1(acc);
