@@ -72,6 +72,9 @@ def parse():
                          "default run")
     ap.add_argument("--full-space", action="store_true",
                     help="keep full-space states (no compact sector evaluator)")
+    ap.add_argument("--one-set", action="store_true",
+                    help="one parameter set per CTA in the compact forward program "
+                         "(default: two real sets per CTA)")
     ap.add_argument("--workload", default="ucc",
                     choices=["ucc", "gates", "grad", "adapt", "serve", "pexp", "pqe", "sample"],
                     help="ucc: batched dUCCSD energy+gradient (default); gates: the gate sweep; "
@@ -100,6 +103,9 @@ def parse():
     ap.add_argument("--dense", type=int, default=0,
                     help="gate sweep: fuse runs into dense 5- or 6-qubit blocks on the FP64 "
                          "tensor cores (0: tile runs)")
+    ap.add_argument("--fused-phases", action="store_true",
+                    help="gate sweep: apply each tile phase as fused block matrices instead of "
+                         "its gates one by one")
     ap.add_argument("--complex64", action="store_true",
                     help="gate sweep: the complex64 throughput variant (FP32 arithmetic)")
     ap.add_argument("--autotune", action="store_true",
@@ -321,7 +327,8 @@ def run_gates(a, rank, world, local, emit=True):
     from qforte_b200.device import gate_phases, gate_plan, gates_config
     from qforte_b200.workloads import layered_random_circuit
     torch.cuda.set_device(local)
-    gates_config(a.tile, a.low_bits, a.reg_bits, getattr(a, "dense", 0))
+    gates_config(a.tile, a.low_bits, a.reg_bits, getattr(a, "dense", 0),
+                 getattr(a, "fused_phases", False))
     peak, src = peaks()
     ns = [int(v) for v in a.nqubits.split(",") if v]
     rows = []
@@ -374,6 +381,7 @@ def run_gates(a, rank, world, local, emit=True):
                                    f"{','.join(map(str, ns))} qubits, from |0...0>",
                        "tile_bits": a.tile, "low_bits": a.low_bits, "reg_bits": a.reg_bits,
                        "dense_block_qubits": getattr(a, "dense", 0),
+                       "phase_form": "fused" if getattr(a, "fused_phases", False) else "ops",
                        "l2": "state larger than L2 from 23 qubits"},
             "sweep": rows,
             "roofline": {"bound": "hbm",
@@ -1089,9 +1097,9 @@ def main():
     mol, pool = problem(a.norb, a.seed)
     tops = list(range(len(pool)))
     M = len(tops)
-    if a.full_space:
+    if a.full_space or a.one_set:
         from qforte_b200.ucc import evaluator_config
-        evaluator_config(False)
+        evaluator_config(False if a.full_space else "one-set")
     eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference)
     P = replica_parameters(a.seed, rank, a.batch, M)
     # consecutive steps alternate between S evaluators, each on its own stream

@@ -159,6 +159,13 @@ QFB_API int qfb_gates_dense(int k);
  * of 3; always clamped so a tile has at most 256 threads and at least 4).  No
  * counterpart in the reference; set by the autotuner. */
 QFB_API int qfb_gates_regs(int reg_bits);
+/* Form of the tile phases, process-wide: 1 applies each phase of at most 3
+ * register bits as a few block-diagonal 2^R x 2^R matrices (the product of
+ * its gates, one per assignment of the thread bits its controls test) and one
+ * factor per thread; 0 (the default) applies the phase's gates one by one.
+ * Both give the result of the gates in list order (up to rounding of the
+ * fused products).  No counterpart in the reference; set by the autotuner. */
+QFB_API int qfb_gates_fused(int on);
 /* Host only: how qfb_apply_gates would apply these gates to one nqubit state
  * under the current tile shape: the number of tile runs, of one-gate passes,
  * and the bytes those passes read and write (a run 32 * 2^n; a one-gate pass
@@ -269,6 +276,11 @@ QFB_API int qfb_ucc_path(qfb_ucc u, int32_t *path);
 /* 1 when the evaluator's compact states are stored as real doubles (see
  * qfb_ucc_config), else 0.  No counterpart in the reference. */
 QFB_API int qfb_ucc_real_states(qfb_ucc u, int32_t *real);
+/* Parameter sets one CTA of the compact shared-memory forward program holds:
+ * 2 with real states (two sets in one 16-byte slot per amplitude), 1
+ * otherwise, 0 off the compact shared-memory path.  No counterpart in the
+ * reference. */
+QFB_API int qfb_ucc_sets_per_cta(qfb_ucc u, int32_t *sets);
 /* Entries of the H rows the compact path streams for each parameter set (0
  * on the other paths).  No counterpart in the reference. */
 QFB_API int qfb_ucc_rows(qfb_ucc u, int64_t *nnz);
@@ -277,7 +289,8 @@ QFB_API int qfb_ucc_rows(qfb_ucc u, int64_t *nnz);
  * global memory), only the global-memory one (2), only the global-memory one
  * with sigma formed from the grouped terms instead of stored H rows (3; the
  * rows are over 24 GB beyond ~24 qubits, where this happens by itself), 1
- * or 2 with complex state storage (4, 5), or neither (0).  Otherwise a
+ * or 2 with complex state storage (4, 5), 1 with one real parameter set per
+ * CTA in the shared-memory forward program instead of two (6), or neither (0).  Otherwise a
  * compact evaluator whose H and step coefficients are all real keeps psi and
  * sigma as real doubles (half the memory and traffic).  No counterpart in the
  * reference. */

@@ -46,6 +46,7 @@ SIGNATURES = {
     "qfb_launch_count": (ctypes.c_int, [_vp]),
     "qfb_set_tile_wait_limit": (ctypes.c_int, [_u64]),
     "qfb_gates_dense": (ctypes.c_int, [ctypes.c_int]),
+    "qfb_ucc_sets_per_cta": (ctypes.c_int, [_vp, _vp]),
     "qfb_c64_create": (ctypes.c_int, [ctypes.c_int, _vp]),
     "qfb_c64_destroy": (ctypes.c_int, [_vp]),
     "qfb_c64_reset": (ctypes.c_int, [_vp]),
@@ -77,6 +78,7 @@ SIGNATURES = {
     "qfb_gates_plan": (ctypes.c_int, [_vp, _i64, ctypes.c_int, _vp, _vp, _vp]),
     "qfb_gates_phases": (ctypes.c_int, [_vp, _i64, ctypes.c_int, _vp, _vp]),
     "qfb_gates_regs": (ctypes.c_int, [ctypes.c_int]),
+    "qfb_gates_fused": (ctypes.c_int, [ctypes.c_int]),
     "qfb_scale": (ctypes.c_int, [c_state, QfbComplex]),
     "qfb_vdot": (ctypes.c_int, [c_state, c_state, _vp]),
     "qfb_axpy": (ctypes.c_int, [c_state, QfbComplex, c_state]),

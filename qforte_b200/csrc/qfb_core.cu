@@ -506,6 +506,7 @@ int g_gate_tile_bits = 0;  // 0: kGateTileDefault; -1: one pass per gate
 int g_gate_low_bits = 3;
 
 int g_gate_reg_bits = 0;  // 0: default
+int g_gate_fused = 0;     // 1: phases of R <= 3 register bits in the fused form
 
 // Register bits R of a tile of b qubits: 2^(b-R) threads (<= 256) hold 2^R
 // amplitudes each.  Default 3 (8 amplitudes, 80 registers a thread, three
@@ -543,6 +544,10 @@ int gate_tile_smem() {
         attr((const void *)qfbt::k_gate_tile<2, float2>, bytes8(10));
         attr((const void *)qfbt::k_gate_tile<3, float2>, bytes8(11));
         attr((const void *)qfbt::k_gate_tile<4, float2>, bytes8(kGateTileMax));
+        attr((const void *)qfbt::k_gate_tile<2, double2, true>, bytes(10));
+        attr((const void *)qfbt::k_gate_tile<3, double2, true>, bytes(11));
+        attr((const void *)qfbt::k_gate_tile<2, float2, true>, bytes8(10));
+        attr((const void *)qfbt::k_gate_tile<3, float2, true>, bytes8(11));
     });
     return err == cudaSuccess ? QFB_OK : cuda_fail(err, "gate tile shared memory");
 }
@@ -639,6 +644,8 @@ struct TilePlan {
     std::vector<double2> m4;
     std::vector<uint64_t> chunks;   // per run: global offset of each 8-amplitude chunk
     std::vector<uint32_t> threads;  // per phase: tl | tpad(tl) << 16 of each thread
+    std::vector<qfbt::TSeg> segs;   // fused form: segments of the phases
+    std::vector<double2> fm;        // fused form: segment matrices, per-thread factors
 };
 
 // The bits of v, lowest first, placed on the set bits of m.
@@ -658,6 +665,155 @@ bool is_swap4(const WGate &g) {
     return true;
 }
 
+// ---- the fused form of a phase ----------------------------------------------
+
+inline double2 cmul_h(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+inline double2 cadd_h(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+// One op of a phase on the 2^R registers of the thread with tile bits tl,
+// exactly as qfbt::apply_op applies it.
+void top_apply_host(const qfbt::TOp &o, const double2 *m4, uint32_t tl, int R, double2 *v) {
+    if ((tl & o.tctl) != o.tctl) return;
+    const uint32_t NR = 1u << R, cm = o.aux & 0xffu, cv = (o.aux >> 16) & 0xffu;
+    const uint32_t opc = o.opc;
+    if (opc < qfbt::OPC_DIAG) {
+        const uint32_t kind = opc / 4, tb = 1u << (opc % 4);
+        for (uint32_t k = 0; k < NR; ++k) {
+            if ((k & tb) || (k & cm) != cv) continue;
+            const double2 x0 = v[k], x1 = v[k | tb];
+            if (kind == qfbt::OP_PSWAP) {
+                v[k] = x1;
+                v[k | tb] = x0;
+            } else if (kind == qfbt::OP_ANTI) {
+                v[k] = cmul_h(o.m[1], x1);
+                v[k | tb] = cmul_h(o.m[2], x0);
+            } else {
+                v[k] = cadd_h(cmul_h(o.m[0], x0), cmul_h(o.m[1], x1));
+                v[k | tb] = cadd_h(cmul_h(o.m[2], x0), cmul_h(o.m[3], x1));
+            }
+        }
+    } else if (opc < qfbt::OPC_DIAG_THREAD) {
+        const uint32_t dset = (opc - qfbt::OPC_DIAG) / 4 + 1, tb = 1u << ((opc - qfbt::OPC_DIAG) % 4);
+        for (uint32_t k = 0; k < NR; ++k) {
+            if ((k & cm) != cv) continue;
+            if (k & tb) {
+                if (dset & 2u) v[k] = cmul_h(o.m[3], v[k]);
+            } else if (dset & 1u) {
+                v[k] = cmul_h(o.m[0], v[k]);
+            }
+        }
+    } else if (opc == qfbt::OPC_DIAG_THREAD) {
+        const bool one = (tl & o.tbit) != 0;
+        if (!(((o.aux >> 8) & 3u) & (one ? 2u : 1u))) return;
+        const double2 f = o.m[one ? 3 : 0];
+        for (uint32_t k = 0; k < NR; ++k)
+            if ((k & cm) == cv) v[k] = cmul_h(f, v[k]);
+    } else if (opc < qfbt::OPC_BSWAP) {
+        const uint32_t tb = 1u << ((opc - qfbt::OPC_GEN4) / 4), cb = 1u << ((opc - qfbt::OPC_GEN4) % 4);
+        const double2 *m = m4 + o.aux;
+        for (uint32_t k = 0; k < NR; ++k) {
+            if (k & (tb | cb)) continue;
+            const uint32_t idx[4] = {k, k | tb, k | cb, k | tb | cb};
+            double2 y[4];
+            for (int i = 0; i < 4; ++i) {
+                double2 acc = make_double2(0.0, 0.0);
+                for (int j = 0; j < 4; ++j) acc = cadd_h(acc, cmul_h(m[4 * i + j], v[idx[j]]));
+                y[i] = acc;
+            }
+            for (int i = 0; i < 4; ++i) v[idx[i]] = y[i];
+        }
+    } else {
+        const uint32_t tb = 1u << ((opc - qfbt::OPC_BSWAP) / 4), cb = 1u << ((opc - qfbt::OPC_BSWAP) % 4);
+        for (uint32_t k = 0; k < NR; ++k)
+            if ((k & tb) && !(k & cb)) std::swap(v[k], v[k ^ tb ^ cb]);
+    }
+}
+
+// The fused form of phase ph (its ops already in tp.ops): segments of
+// consecutive ops with at most kMaxVarBits variant bits, and the per-thread
+// product of the factors that depend on thread bits alone.
+void fuse_phase(TilePlan &tp, qfbt::TPhase &ph, int R, int b) {
+    const uint32_t NR = 1u << R, nth = 1u << (b - R);
+    ph.s0 = (int)tp.segs.size();
+    ph.sc = -1;
+    std::vector<int> run_ops;
+    std::vector<double2> fac(nth, make_double2(1.0, 0.0));
+    bool any_fac = false;
+    std::vector<double2> col(NR), mat;
+    auto flush = [&](uint32_t D) {
+        if (run_ops.empty()) return;
+        std::vector<int> dbits;
+        for (int p = 0; p < 16; ++p)
+            if (D >> p & 1u) dbits.push_back(p);
+        const uint32_t nvar = 1u << dbits.size();
+        // every variant's full matrix, then the mixing mask over all of them
+        mat.assign((size_t)nvar * NR * NR, make_double2(0.0, 0.0));
+        uint32_t mm = 0;
+        for (uint32_t x = 0; x < nvar; ++x) {
+            uint32_t tl = 0;
+            for (size_t j = 0; j < dbits.size(); ++j)
+                if (x >> j & 1u) tl |= 1u << dbits[j];
+            for (uint32_t c = 0; c < NR; ++c) {
+                std::fill(col.begin(), col.end(), make_double2(0.0, 0.0));
+                col[c] = make_double2(1.0, 0.0);
+                for (int oi : run_ops) top_apply_host(tp.ops[oi], tp.m4.data(), tl, R, col.data());
+                for (uint32_t r = 0; r < NR; ++r) {
+                    mat[((size_t)x * NR + r) * NR + c] = col[r];
+                    if (col[r].x != 0.0 || col[r].y != 0.0) mm |= r ^ c;
+                }
+            }
+        }
+        const uint32_t Dm = 1u << __builtin_popcount(mm);
+        qfbt::TSeg sg{};
+        sg.m0 = (uint32_t)tp.fm.size();
+        sg.mm = mm;
+        sg.nd = (uint32_t)dbits.size();
+        for (size_t j = 0; j < dbits.size(); ++j) sg.dsel |= (uint32_t)dbits[j] << (4 * j);
+        for (uint32_t x = 0; x < nvar; ++x)
+            for (uint32_t k = 0; k < NR; ++k) {  // groups in ascending order of k's other bits
+                if (k & mm) continue;
+                for (uint32_t i = 0; i < Dm; ++i)
+                    for (uint32_t j = 0; j < Dm; ++j) {
+                        const uint32_t r = k | (uint32_t)deposit_host(i, mm),
+                                       c = k | (uint32_t)deposit_host(j, mm);
+                        tp.fm.push_back(mat[((size_t)x * NR + r) * NR + c]);
+                    }
+            }
+        tp.segs.push_back(sg);
+        run_ops.clear();
+    };
+    uint32_t D = 0;
+    for (int oi = ph.o0; oi < ph.o0 + ph.no; ++oi) {
+        const qfbt::TOp &o = tp.ops[oi];
+        const uint32_t cm = o.aux & 0xffu;
+        if (o.opc == qfbt::OPC_DIAG_THREAD && cm == 0) {  // a factor of thread bits alone
+            for (uint32_t t = 0; t < nth; ++t) {
+                double2 one = make_double2(1.0, 0.0);
+                const uint32_t tl = tp.threads[ph.th0 + t] & 0xffffu;
+                top_apply_host(o, tp.m4.data(), tl, 0, &one);
+                fac[t] = cmul_h(one, fac[t]);
+            }
+            any_fac = true;
+            continue;
+        }
+        uint32_t need = o.tctl | (o.opc == qfbt::OPC_DIAG_THREAD ? o.tbit : 0u);
+        if (__builtin_popcount(D | need) > qfbt::kMaxVarBits) {
+            flush(D);
+            D = 0;
+        }
+        D |= need;
+        run_ops.push_back(oi);
+    }
+    flush(D);
+    ph.ns = (int)tp.segs.size() - ph.s0;
+    if (any_fac) {
+        ph.sc = (int)tp.fm.size();
+        tp.fm.insert(tp.fm.end(), fac.begin(), fac.end());
+    }
+}
+
 // Split a run's gates (tile coordinates) into phases of R register bits.
 // Scanning the unplaced gates in order, a gate joins the current phase when
 // no earlier unplaced gate shares one of its tile bits and its mixing bits
@@ -665,8 +821,9 @@ bool is_swap4(const WGate &g) {
 // gate that cannot join blocks its bits for the rest of the scan, so only
 // gates on disjoint qubits change order.
 // c64: shared offsets in the complex64 tile layout (qfbt::tpad8).
+// fused: also the phases' fused form (R <= kMaxFusedRegBits).
 void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, TilePlan &tp,
-                      bool c64 = false) {
+                      bool c64 = false, bool fused = false) {
     auto toff = [c64](uint32_t l) { return c64 ? qfbt::tpad8(l) : qfbt::tpad(l); };
     std::vector<uint32_t> mix((size_t)ng), qm((size_t)ng);
     for (int i = 0; i < ng; ++i) {
@@ -839,6 +996,7 @@ void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, Til
             ph.soff[k] = toff(l);
         }
         ph.no = (int)tp.ops.size() - ph.o0;
+        if (fused && R <= qfbt::kMaxFusedRegBits) fuse_phase(tp, ph, R, b);
         tp.ph.push_back(ph);
     }
     run.np = (int)tp.ph.size() - run.p0;
@@ -1006,7 +1164,7 @@ int apply_gates_dense(qfb_state s, const std::vector<HGate> &hg, int K) {
 // Runs of a gate list and the phases of each run.
 void plan_gate_tiles(const std::vector<HGate> &hg, int n, int b, int L,
                      std::vector<GatePlanWin> &wins, TilePlan &tp, std::vector<qfbt::TRun> &runs,
-                     bool c64 = false) {
+                     bool c64 = false, bool fused = false) {
     std::vector<WGate> wg;
     plan_gate_windows(hg, n, b, L, wins, wg);
     runs.assign(wins.size(), qfbt::TRun{});
@@ -1018,7 +1176,8 @@ void plan_gate_tiles(const std::vector<HGate> &hg, int n, int b, int L,
         r.ch0 = (int)tp.chunks.size();
         for (uint64_t c = 0; c < (1ull << (pw.w.b - 3)); ++c)
             tp.chunks.push_back(deposit_host(c, pw.w.qmask & ~7ull));
-        plan_tile_phases(wg.data() + pw.w.g0, pw.w.ng, pw.w.b, tile_reg_bits(pw.w.b), r, tp, c64);
+        plan_tile_phases(wg.data() + pw.w.g0, pw.w.ng, pw.w.b, tile_reg_bits(pw.w.b), r, tp, c64,
+                         fused);
     }
 }
 
@@ -1055,17 +1214,21 @@ int apply_gates_tiles(A *d, int n, int nbatch, const std::vector<HGate> &hg) {
     std::vector<GatePlanWin> wins;
     TilePlan tp;
     std::vector<qfbt::TRun> runs;
-    plan_gate_tiles(hg, n, b, L, wins, tp, runs, c64);
-    // one upload of phases, ops and 4x4 matrices
+    const bool fused = g_gate_fused != 0;
+    plan_gate_tiles(hg, n, b, L, wins, tp, runs, c64, fused);
+    // one upload of phases, ops, 4x4 matrices, chunk and thread tables and
+    // the fused form
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t bp = al(sizeof(qfbt::TPhase) * tp.ph.size());
     const size_t bo = al(sizeof(qfbt::TOp) * tp.ops.size());
     const size_t bm = al(sizeof(double2) * tp.m4.size());
     const size_t bc = al(sizeof(uint64_t) * tp.chunks.size());
-    const size_t bt = sizeof(uint32_t) * tp.threads.size();
+    const size_t bt = al(sizeof(uint32_t) * tp.threads.size());
+    const size_t bs = al(sizeof(qfbt::TSeg) * tp.segs.size());
+    const size_t bf = sizeof(double2) * tp.fm.size();
     void *buf = nullptr;
     if (!tp.ph.empty()) {
-        std::vector<unsigned char> host(bp + bo + bm + bc + bt);
+        std::vector<unsigned char> host(bp + bo + bm + bc + bt + bs + bf);
         auto put = [&](size_t off, const void *src, size_t sz) {
             if (sz) std::memcpy(host.data() + off, src, sz);
         };
@@ -1073,7 +1236,9 @@ int apply_gates_tiles(A *d, int n, int nbatch, const std::vector<HGate> &hg) {
         put(bp, tp.ops.data(), sizeof(qfbt::TOp) * tp.ops.size());
         put(bp + bo, tp.m4.data(), sizeof(double2) * tp.m4.size());
         put(bp + bo + bm, tp.chunks.data(), sizeof(uint64_t) * tp.chunks.size());
-        put(bp + bo + bm + bc, tp.threads.data(), bt);
+        put(bp + bo + bm + bc, tp.threads.data(), sizeof(uint32_t) * tp.threads.size());
+        put(bp + bo + bm + bc + bt, tp.segs.data(), sizeof(qfbt::TSeg) * tp.segs.size());
+        put(bp + bo + bm + bc + bt + bs, tp.fm.data(), bf);
         int rc = dev_alloc(&buf, host.size());
         if (rc) return rc;
         QFB_CUDA(cudaMemcpyAsync(buf, host.data(), host.size(), cudaMemcpyHostToDevice, t_stream));
@@ -1084,6 +1249,8 @@ int apply_gates_tiles(A *d, int n, int nbatch, const std::vector<HGate> &hg) {
     const double2 *d_m4 = (const double2 *)(ub + bp + bo);
     const uint64_t *d_ch = (const uint64_t *)(ub + bp + bo + bm);
     const uint32_t *d_th = (const uint32_t *)(ub + bp + bo + bm + bc);
+    const qfbt::TSeg *d_sg = (const qfbt::TSeg *)(ub + bp + bo + bm + bc + bt);
+    const double2 *d_fm = (const double2 *)(ub + bp + bo + bm + bc + bt + bs);
     int rc = gate_tile_smem();
     for (size_t i = 0; i < wins.size() && rc == QFB_OK; ++i) {
         const GatePlanWin &pw = wins[i];
@@ -1094,15 +1261,20 @@ int apply_gates_tiles(A *d, int n, int nbatch, const std::vector<HGate> &hg) {
         const int tb = pw.w.b, R = tile_reg_bits(tb);
         const size_t smem = sizeof(A) * qfbt::tpad_size_of<A>(tb) + 16;
         const dim3 grid((unsigned)(nbasis >> tb), nbatch), block(1u << (tb - R));
-        if (R == 2)
-            qfbt::k_gate_tile<2, A><<<grid, block, smem, t_stream>>>(d, nbasis, runs[i], d_ph, d_ops,
-                                                                     d_m4, d_ch, d_th);
+#define QFB_TILE(RR, FF)                                                                        \
+    qfbt::k_gate_tile<RR, A, FF><<<grid, block, smem, t_stream>>>(d, nbasis, runs[i], d_ph, d_ops, \
+                                                                  d_m4, d_ch, d_th, d_sg, d_fm)
+        if (R == 2 && fused)
+            QFB_TILE(2, true);
+        else if (R == 2)
+            QFB_TILE(2, false);
+        else if (R == 3 && fused)
+            QFB_TILE(3, true);
         else if (R == 3)
-            qfbt::k_gate_tile<3, A><<<grid, block, smem, t_stream>>>(d, nbasis, runs[i], d_ph, d_ops,
-                                                                     d_m4, d_ch, d_th);
+            QFB_TILE(3, false);
         else
-            qfbt::k_gate_tile<4, A><<<grid, block, smem, t_stream>>>(d, nbasis, runs[i], d_ph, d_ops,
-                                                                     d_m4, d_ch, d_th);
+            QFB_TILE(4, false);
+#undef QFB_TILE
         rc = [&]() -> int { QFB_LAUNCHED(); return QFB_OK; }();
     }
     dev_free(buf);
@@ -1354,6 +1526,12 @@ int qfb_gates_dense(int k) {
     if (k != 0 && k != 5 && k != 6)
         return fail(QFB_EINVAL, "qfb_gates_dense: k = %d is not 0, 5 or 6", k);
     g_gate_dense = k;
+    return QFB_OK;
+}
+
+int qfb_gates_fused(int on) {
+    if (on != 0 && on != 1) return fail(QFB_EINVAL, "qfb_gates_fused: %d is not 0 or 1", on);
+    g_gate_fused = on;
     return QFB_OK;
 }
 

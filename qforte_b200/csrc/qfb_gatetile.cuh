@@ -71,8 +71,39 @@ struct TPhase {
     int32_t o0, no;                   // ops of this phase
     int32_t th0;                      // this phase's entries of the thread table
     int32_t pad;
+    int32_t s0, ns;                   // fused form: segments of this phase
+    int32_t sc;                       // fused form: per-thread factor table (-1: none)
+    int32_t pad2;
 };
-static_assert(sizeof(TPhase) == 144, "TPhase layout");
+static_assert(sizeof(TPhase) == 160, "TPhase layout");
+
+// The fused form of a phase (runs with R <= kMaxFusedRegBits): its ops, in
+// order, become a few segments, each one block-diagonal 2^R x 2^R matrix on
+// the thread's registers, plus one factor per thread.
+//  * The matrix of a segment depends on the thread only through its variant
+//    bits (the tile bits of the thread part that its ops test: controls on
+//    thread bits, the bit of a diagonal on a thread bit that is also
+//    controlled by register bits), at most kMaxVarBits of them; the host
+//    builds one matrix per assignment of those bits.
+//  * Its mixing mask mm holds the register bits the matrix mixes (the bits of
+//    i ^ j over its nonzero entries i, j): registers that differ only outside
+//    mm never mix, so the matrix is 2^R / D blocks of D x D (D = 2^|mm|), for
+//    the groups of registers with equal bits outside mm, in ascending order.
+//  * Diagonal factors that depend on thread bits alone (a diagonal on a
+//    thread bit, controlled by thread bits or not at all) scale all 2^R
+//    registers of a thread alike and commute with everything else in the
+//    phase: their product, per thread, is one table entry.
+// Variant index: bit j is tile bit (dsel >> 4j) & 15 of the thread; matrix of
+// variant x at m0 + x * 2^R * D, block g at + g * D * D, row-major.
+constexpr int kMaxFusedRegBits = 3;
+constexpr int kMaxVarBits = 4;
+struct TSeg {
+    uint32_t m0;    // first entry of this segment's matrices
+    uint32_t dsel;  // variant bits: tile bit positions, 4 bits each
+    uint32_t mm;    // mixing mask on the register bits
+    uint32_t nd;    // number of variant bits
+};
+static_assert(sizeof(TSeg) == 16, "TSeg layout");
 // thread table entry of thread tid in a phase: tl | tpad(tl) << 16, with tl
 // the thread's tile bits (the phase's non-register bits set from tid)
 
@@ -374,6 +405,90 @@ __device__ __forceinline__ void apply_op(A (&v)[1 << R], const TOp *__restrict__
     }
 }
 
+// ---- the fused form ---------------------------------------------------------
+
+// The bits of j placed on the set bits of MM, lowest first (compile time).
+template <int MM>
+__host__ __device__ constexpr int dep_c(int j) {
+    int r = 0, b = 0;
+    for (int p = 0; p < 8; ++p)
+        if ((MM >> p) & 1) {
+            if ((j >> b) & 1) r |= 1 << p;
+            ++b;
+        }
+    return r;
+}
+
+// Index of register group k (k's bits outside MM, packed; compile time).
+template <int R, int MM>
+__host__ __device__ constexpr int grp_c(int k) {
+    int r = 0, b = 0;
+    for (int p = 0; p < R; ++p)
+        if (!((MM >> p) & 1)) {
+            if ((k >> p) & 1) r |= 1 << b;
+            ++b;
+        }
+    return r;
+}
+
+template <int MM>
+__host__ __device__ constexpr int popc_c() {
+    int c = 0;
+    for (int p = 0; p < 8; ++p) c += (MM >> p) & 1;
+    return c;
+}
+
+// acc + m x (complex)
+template <class A>
+__device__ __forceinline__ A c_fma(A m, A x, A acc) {
+    acc.x = fma(m.x, x.x, acc.x);
+    acc.y = fma(m.x, x.y, acc.y);
+    acc.x = fma(-m.y, x.y, acc.x);
+    acc.y = fma(m.y, x.x, acc.y);
+    return acc;
+}
+
+// The segment matrix (blocks of D x D on the mixing bits MM) on the registers.
+template <int R, int MM, class A>
+__device__ __forceinline__ void ap_fused(A (&v)[1 << R], const double2 *__restrict__ m) {
+    if constexpr (MM < (1 << R)) {
+        constexpr int D = 1 << popc_c<MM>();
+#pragma unroll
+        for (int k = 0; k < (1 << R); ++k) {
+            if (k & MM) continue;
+            const double2 *mg = m + grp_c<R, MM>(k) * D * D;
+            A y[D];
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                A acc = c_mul(AmpT<A>::cvt(ld_entry(mg + i * D)), v[k | dep_c<MM>(0)]);
+#pragma unroll
+                for (int j = 1; j < D; ++j)
+                    acc = c_fma(AmpT<A>::cvt(ld_entry(mg + i * D + j)), v[k | dep_c<MM>(j)], acc);
+                y[i] = acc;
+            }
+#pragma unroll
+            for (int i = 0; i < D; ++i) v[k | dep_c<MM>(i)] = y[i];
+        }
+    }
+}
+
+// One segment of a fused phase on the thread with tile bits tl.
+template <int R, class A>
+__device__ __forceinline__ void apply_seg(A (&v)[1 << R], const TSeg *__restrict__ sg, uint32_t tl,
+                                          const double2 *__restrict__ fm) {
+    const uint4 h = __ldg(reinterpret_cast<const uint4 *>(sg));
+    uint32_t var = 0;
+    for (uint32_t j = 0; j < h.w; ++j) var |= ((tl >> ((h.y >> (4 * j)) & 15u)) & 1u) << j;
+    const double2 *m = fm + h.x + (size_t)var * ((1u << R) << __popc(h.z));
+    switch (h.z) {
+#define X(N) case N: ap_fused<R, N>(v, m); break;
+        X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7)
+#undef X
+        default:
+            break;
+    }
+}
+
 // v with a zero bit inserted at every set bit of m (ascending): the bits of
 // v placed on the complement of m.
 __device__ __forceinline__ uint64_t spread_around(uint64_t v, uint64_t m) {
@@ -413,12 +528,15 @@ __host__ __device__ __forceinline__ uint32_t tpad_size_of(int b) {
 // blockIdx.y: batch slot); 2^(b-R) threads, 2^R amplitudes each.  A: double2
 // (complex128) or float2 (the complex64 throughput variant, arithmetic in
 // FP32); a chunk is 8 amplitudes either way (128 or 64 bytes).
-template <int R, class A = double2>
+// F: the phases' fused form (segments and per-thread factors in segs / fm)
+// instead of their op lists.
+template <int R, class A = double2, bool F = false>
 __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
     k_gate_tile(A *__restrict__ psi, uint64_t nbasis, TRun run,
                 const TPhase *__restrict__ phases, const TOp *__restrict__ ops,
                 const double2 *__restrict__ m4, const uint64_t *__restrict__ chunks,
-                const uint32_t *__restrict__ threads) {
+                const uint32_t *__restrict__ threads, const TSeg *__restrict__ segs,
+                const double2 *__restrict__ fm) {
     extern __shared__ __align__(128) unsigned char t_smem[];
     constexpr uint32_t kChunk = 8u * sizeof(A);
     A *tile = reinterpret_cast<A *>(t_smem);
@@ -458,8 +576,18 @@ __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
         A v[1 << R];
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) v[k] = t0[__ldg(&ph->roff[k])];
-        const int o0 = __ldg(&ph->o0), o1 = o0 + __ldg(&ph->no);
-        for (int o = o0; o < o1; ++o) apply_op<R, A>(v, ops + o, tl, m4);
+        if constexpr (F && R <= kMaxFusedRegBits) {
+            const int s0 = __ldg(&ph->s0), s1 = s0 + __ldg(&ph->ns), sc = __ldg(&ph->sc);
+            for (int si = s0; si < s1; ++si) apply_seg<R, A>(v, segs + si, tl, fm);
+            if (sc >= 0) {
+                const A f = AmpT<A>::cvt(__ldg(fm + sc + tid));
+#pragma unroll
+                for (int k = 0; k < (1 << R); ++k) v[k] = c_mul(f, v[k]);
+            }
+        } else {
+            const int o0 = __ldg(&ph->o0), o1 = o0 + __ldg(&ph->no);
+            for (int o = o0; o < o1; ++o) apply_op<R, A>(v, ops + o, tl, m4);
+        }
         A *t1 = tile + (tw >> 16);
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) t1[__ldg(&ph->soff[k])] = v[k];

@@ -2707,6 +2707,11 @@ struct qfb_ucc_s {
     qfbs::PStream rstream{};          // compact: forward pair lists in reverse order
     std::shared_ptr<PairPlanDev> pairs;  // compact: the plan's pair lists in use
     int64_t nprows = 1;                  // rows of the gradient partials (gradient steps)
+    // compact, real states: two parameter sets per CTA in the forward kernel
+    // (k_sector_forward_pr), with pair lists ordered for 16-byte slots
+    int paired = 0;
+    std::shared_ptr<PairPlanDev> pairs16b;
+    qfbs::SLaunch SLp{};
 };
 
 // Whether every pattern of every record of a stream has real coefficients.
@@ -3161,6 +3166,15 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
         if (rc) return rc;
         u->pairs = pairs;
         u->bytes += pairs->bytes;
+        // two real sets per CTA in the forward program where its shared memory fits
+        const size_t fwd_b = ((16 * (size_t)sp.nsec + 15) & ~(size_t)15) +
+                             sizeof(qfbs::PSmemPR) * (size_t)pairs->fwd.n;
+        if (u->sreal && g_ucc_compact != 6 && u->nbatch >= 2 && fwd_b <= kSectorSmemMax) {
+            rc = pair_plan(sp, 8, &u->pairs16b);
+            if (rc) return rc;
+            if (u->pairs16b != pairs) u->bytes += u->pairs16b->bytes;
+            u->paired = 1;
+        }
     }
     u->splan = plan;
     u->rows = rows;
@@ -3203,6 +3217,10 @@ static int sector_attach(qfb_ucc u, qfb_sum_s *ham, const std::shared_ptr<Sector
     L.params = u->params;
     L.energy = u->energy;
     L.partial = u->gpart;
+    if (u->paired) {
+        u->SLp = L;
+        u->SLp.fwd = u->pairs16b->fwd;
+    }
     return QFB_OK;
 }
 
@@ -3236,6 +3254,11 @@ static cudaError_t sector_smem_attr_v() {
     if (err == cudaSuccess)
         err = cudaFuncSetAttribute(qfbs::k_sector_pack<V>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    if constexpr (sizeof(V) == sizeof(double)) {
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(qfbs::k_sector_forward_pr,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+    }
     return err;
 }
 
@@ -3256,6 +3279,17 @@ static int ucc_stage_compact_v(qfb_ucc u, int stage, int with_grad) {
     const bool real = sizeof(V) == sizeof(double);
     switch (stage) {
         case 1:
+            if constexpr (sizeof(V) == sizeof(double)) {
+                if (u->paired) {
+                    const qfbs::SLaunch &LP = u->SLp;
+                    qfbs::k_sector_forward_pr<<<(u->nbatch + 1) / 2, qfbs::kStepThreads,
+                                                ((16 * n + 15) & ~(size_t)15) +
+                                                    sizeof(qfbs::PSmemPR) * (size_t)LP.fwd.n,
+                                                t_stream>>>(LP, u->nbatch);
+                    QFB_LAUNCHED();
+                    break;
+                }
+            }
             qfbs::k_sector_forward<V><<<u->nbatch, qfbs::kStepThreads,
                                         qfbs::sector_smem_states(1, n, real) +
                                             sizeof(qfbs::PSmem<V>) * (size_t)L.fwd.n,
@@ -3709,7 +3743,7 @@ static int ucc_create_impl(qfb_prog fprog, qfb_prog gprog, qfb_prog uprog, qfb_s
             fprog->sector_plans[key] = r;
             return r;
         };
-        if (g_ucc_compact == 1 || g_ucc_compact == 4) {  // 2, 3: global memory only (3: sigma without stored rows)
+        if (g_ucc_compact == 1 || g_ucc_compact == 4 || g_ucc_compact == 6) {  // 2, 3: global memory only (3: sigma without stored rows)
             plan = get_plan(true);
             compact = plan != nullptr;
         }
@@ -3858,7 +3892,7 @@ int qfb_ucc_tiles(int fwd_bits, int grad_bits, int low_bits) {
 }
 
 int qfb_ucc_config(int compact) {
-    if (compact < 0 || compact > 5) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
+    if (compact < 0 || compact > 6) return fail(QFB_EINVAL, "qfb_ucc_config: compact = %d", compact);
     g_ucc_compact = compact;
     return QFB_OK;
 }
@@ -3866,6 +3900,12 @@ int qfb_ucc_config(int compact) {
 int qfb_ucc_real_states(qfb_ucc u, int32_t *real) {
     if (!u || !real) return fail(QFB_EINVAL, "qfb_ucc_real_states: null argument");
     *real = u->sreal | u->greal;
+    return QFB_OK;
+}
+
+int qfb_ucc_sets_per_cta(qfb_ucc u, int32_t *sets) {
+    if (!u || !sets) return fail(QFB_EINVAL, "qfb_ucc_sets_per_cta: null argument");
+    *sets = u->compact ? (u->paired ? 2 : 1) : 0;
     return QFB_OK;
 }
 

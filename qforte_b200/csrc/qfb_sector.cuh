@@ -668,6 +668,122 @@ __global__ void __launch_bounds__(512, 2) k_sector_pool(SLaunch L, PStream P) {
 }
 
 // ---------------------------------------------------------------------------
+// Two real parameter sets per CTA (forward program)
+// ---------------------------------------------------------------------------
+// With real states, sets 2g and 2g + 1 share one CTA of the forward program:
+// amplitude slot i holds both sets' values as one double2 (.x set 2g, .y set
+// 2g + 1), so every pair word, record header, shared-memory load / store and
+// barrier serves both sets, while each set keeps its own angle (cos / sin per
+// set in the record).  The arithmetic on each set is that of k_sector_forward.
+// (The reverse sweep stays one set per CTA: paired, its shared memory of two
+// states for two sets leaves half the warps per set to hide latency, and it
+// ran slower at 256 sets on 148 SMs.)
+
+struct PSmemPR {
+    PHead h;
+    double2 c, s;   // cos / sin of the record's angle: .x first set, .y second
+    double gn, hn;  // single-pattern records: the coefficients
+};
+static_assert(sizeof(PSmemPR) == 80, "PSmemPR layout");
+
+__device__ __forceinline__ void p_angles_pr(const PStream &S, const double *parA, const double *parB,
+                                            int sign, PSmemPR *s_pr) {
+    for (int r = threadIdx.x; r < S.n; r += blockDim.x) {
+        const PHead h = p_head(S.hd + r);
+        double sa, ca, sb, cb;
+        sincos((double)sign * h.gamma * parA[h.param], &sa, &ca);
+        sincos((double)sign * h.gamma * parB[h.param], &sb, &cb);
+        double gn, hn;
+        p_coef(S, h, gn, hn);
+        s_pr[r].h = h;
+        s_pr[r].c = make_double2(ca, cb);
+        s_pr[r].s = make_double2(sa, sb);
+        s_pr[r].gn = gn;
+        s_pr[r].hn = hn;
+    }
+}
+
+// One pair of a forward record on both sets (p_pair's rotation per set).
+__device__ __forceinline__ void pr_pair(uint32_t pw, double2 c, double2 s, double gn, double hn,
+                                        double2 *v) {
+    constexpr uint32_t M = (1u << kPairIdxBits) - 1u;
+    const int i0 = (int)(pw & M), i1 = (int)((pw >> kPairIdxBits) & M);
+    const bool neg = (pw >> (2 * kPairIdxBits)) & 1u;
+    const double2 a0 = v[i0], a1 = v[i1];
+    const double sx = neg ? -s.x : s.x, sy = neg ? -s.y : s.y;
+    v[i0] = make_double2(c.x * a0.x + sx * (hn * a1.x), c.y * a0.y + sy * (hn * a1.y));
+    v[i1] = make_double2(c.x * a1.x + sx * (gn * a0.x), c.y * a1.y + sy * (gn * a0.y));
+}
+
+template <int KP>
+__device__ __forceinline__ void pr_record(const PStream &S, const PSmemPR &rec, const uint32_t (&pw)[KP],
+                                          double2 *v) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const PHead &h = rec.h;
+    const bool one = (h.fl >> 8) == 1;
+    double gn = rec.gn, hn = rec.hn;
+    auto run = [&](uint32_t p) {
+        if (!one) p_ldcoef(S, h.c0 + (int)(p >> (2 * kPairIdxBits + 1)), gn, hn);
+        pr_pair(p, rec.c, rec.s, gn, hn, v);
+    };
+#pragma unroll
+    for (int j = 0; j < KP; ++j)
+        if (tid + j * nth < h.np) run(pw[j]);
+    for (int k = tid + KP * nth; k < h.np; k += nth) run(__ldg(S.pair + h.p0 + k));
+}
+
+// p_run's forward program for two real sets: the same ring of four
+// prefetched sets of pair words, one barrier per record.
+__device__ __forceinline__ void pr_run(const PStream &S, const PSmemPR *s_pr, double2 *v) {
+    constexpr int KP = 2;
+    const int n = S.n;
+    uint32_t w0[KP], w1[KP], w2[KP], w3[KP];
+    if (n > 0) p_words(S, s_pr[0].h, w0);
+    if (n > 1) p_words(S, s_pr[1].h, w1);
+    if (n > 2) p_words(S, s_pr[2].h, w2);
+    for (int r = 0; r < n; r += 4) {
+        if (r + 3 < n) p_words(S, s_pr[r + 3].h, w3);
+        pr_record<KP>(S, s_pr[r], w0, v);
+        __syncthreads();
+        if (r + 1 >= n) break;
+        if (r + 4 < n) p_words(S, s_pr[r + 4].h, w0);
+        pr_record<KP>(S, s_pr[r + 1], w1, v);
+        __syncthreads();
+        if (r + 2 >= n) break;
+        if (r + 5 < n) p_words(S, s_pr[r + 5].h, w1);
+        pr_record<KP>(S, s_pr[r + 2], w2, v);
+        __syncthreads();
+        if (r + 3 >= n) break;
+        if (r + 6 < n) p_words(S, s_pr[r + 6].h, w2);
+        pr_record<KP>(S, s_pr[r + 3], w3, v);
+        __syncthreads();
+    }
+}
+
+// Forward program of sets 2g, 2g + 1 (g = blockIdx.x; a last odd set runs
+// alone, its twin a copy that is not saved); psi of both into the save buffer.
+__global__ void __launch_bounds__(kStepThreads, 1) k_sector_forward_pr(SLaunch L, int nbatch) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    double2 *psi = reinterpret_cast<double2 *>(s_raw);
+    PSmemPR *s_pr = reinterpret_cast<PSmemPR *>(s_raw + ((16 * (size_t)L.nsec + 15) & ~(size_t)15));
+    const int b0 = 2 * blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    const bool two = b0 + 1 < nbatch;
+    const double *parA = L.params + (size_t)b0 * L.nparam;
+    const double *parB = two ? parA + L.nparam : parA;
+    for (int i = tid; i < L.nsec; i += nth)
+        psi[i] = i == L.ref_i ? make_double2(1.0, 1.0) : make_double2(0.0, 0.0);
+    p_angles_pr(L.fwd, parA, parB, 1, s_pr);
+    __syncthreads();
+    pr_run(L.fwd, s_pr, psi);
+    double *sv = reinterpret_cast<double *>(L.save) + (size_t)b0 * 2 * L.nsec;
+    for (int i = tid; i < L.nsec; i += nth) {
+        const double2 x = psi[i];
+        sv[i] = x.x;
+        if (two) sv[2 * (size_t)L.nsec + i] = x.y;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Packed evaluations of several problems in one launch
 // ---------------------------------------------------------------------------
 

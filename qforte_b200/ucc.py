@@ -48,11 +48,12 @@ __all__ = ["DUCC", "Evaluator", "Pack", "evaluator_config", "UCCNVQE", "ADAPTVQE
 def evaluator_config(compact=True):
     """Process-wide: let evaluators created from now on use the compact
     sector paths (True, the default; real states where every coefficient is
-    real), the same with complex state storage ("complex"), only the
+    real, two parameter sets per CTA in the forward program), the same with
+    one set per CTA ("one-set"), with complex state storage ("complex"), only the
     global-memory one ("global"; "global-complex" with complex storage), or
     keep full-space states (False)."""
-    mode = {"global": 2, "global-no-rows": 3, "complex": 4, "global-complex": 5}.get(
-        compact, 1 if compact else 0)
+    mode = {"global": 2, "global-no-rows": 3, "complex": 4, "global-complex": 5,
+            "one-set": 6}.get(compact, 1 if compact else 0)
     check(lib().qfb_ucc_config(mode), "qfb_ucc_config")
 
 
@@ -98,6 +99,14 @@ class Evaluator:
         n = ctypes.c_int32()
         check(lib().qfb_ucc_real_states(self.h, ctypes.byref(n)), "qfb_ucc_real_states")
         return bool(n.value)
+
+    @property
+    def sets_per_cta(self):
+        """Parameter sets a CTA of the compact forward program holds (2: two
+        real sets per 16-byte slot; 0: not the compact shared path)."""
+        n = ctypes.c_int32()
+        check(lib().qfb_ucc_sets_per_cta(self.h, ctypes.byref(n)), "qfb_ucc_sets_per_cta")
+        return n.value
 
     @property
     def h_rows(self):

@@ -346,6 +346,65 @@ def test_gate_windows_match_oracle(cuda, gate_tiles, tile, low, n, ngates, seed)
     assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
 
 
+def _control_heavy_circuit(n, seed):
+    """Gates whose controls and diagonals sit on many qubits at once: runs of
+    cX / cRz / cV on one target controlled by every other qubit (more thread
+    bits per phase than one segment holds), cZ / cR between two high qubits
+    (factors of the thread's bits alone), cR controlled by a low qubit on a
+    high target, SWAPs and X (relabelings), between random gates."""
+    rng = np.random.default_rng(seed)
+    circ, ora = qb.Circuit(), []
+
+    def add(k, t, c, p=0.0):
+        circ.add(qb.gate(k, t, c, p))
+        ora.append(O.make_gate(k, t, c, p))
+
+    for rep in range(6):
+        t = int(rng.integers(3))
+        for c in range(n):
+            if c != t:
+                add(["cX", "cRz", "cV"][c % 3], t, c, float(rng.uniform(0, 6.3)))
+        for _ in range(4):
+            a, b = (int(v) for v in rng.choice(range(3, n), 2, replace=False))
+            add(["cZ", "cR"][rep % 2], a, b, float(rng.uniform(0, 6.3)))
+        add("cR", int(rng.integers(3, n)), int(rng.integers(3)), float(rng.uniform(0, 6.3)))
+        add("SWAP", 0, 1)
+        add("X", 2, 2)
+        q = int(rng.integers(n))
+        add("T", q, q)
+        c2, o2 = _rand_circuit(n, 40, seed + rep)
+        for g in c2.gates():
+            circ.add(g)
+        ora.extend(o2)
+    return circ, ora
+
+
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("regs", [2, 3])
+@pytest.mark.parametrize("n,kind,seed", [(10, "random", 41), (12, "controls", 42),
+                                         (13, "random", 43), (14, "controls", 44)])
+def test_fused_phases_match_oracle(cuda, fused, regs, n, kind, seed):
+    """Tile phases in their fused form (block matrices per variant of the
+    thread bits the controls test, per-thread factors) and gate by gate, with
+    2 and 3 register bits, from a random state, against the oracle's
+    gate-by-gate application."""
+    from qforte_b200.device import gates_config
+    circ, ora = (_rand_circuit(n, 400, seed) if kind == "random"
+                 else _control_heavy_circuit(n, seed))
+    psi0 = _random_state(n, seed)
+    gates_config(0, 3, regs, 0, fused)
+    try:
+        qc = qb.Computer(n)
+        qc.set_coeff_vec(psi0)
+        qc.apply_circuit(circ)
+        got = qc.get_coeff_array()
+    finally:
+        gates_config()
+    st = O.State(n, psi0.copy())
+    st.apply_gates(ora)
+    assert np.max(np.abs(got - st.psi)) < AMP_TOL
+
+
 @pytest.fixture
 def dense_blocks():
     """Sets dense K-qubit blocks (FP64 tensor cores) and restores the default."""
@@ -777,3 +836,38 @@ def test_complex64_gates_track_complex128(cuda, gate_tiles, tile, low, n, ngates
     assert qc.get_coeff_array()[0] == 1 and abs(qc.norm2() - 1.0) == 0
     with pytest.raises(ValueError):
         qc.apply_circuit(qb.build_circuit(f"X_{n}"))
+
+
+@pytest.mark.parametrize("norb,seed,pool_type,B", [(4, 11, "SD", 5), (6, 3, "SD", 2),
+                                                   (5, 9, "GSD", 7), (8, 2, "SD", 6)])
+def test_two_sets_per_cta_match_one_set(cuda, norb, seed, pool_type, B):
+    """Real compact states: the forward program with two parameter sets per
+    CTA (one 16-byte slot per amplitude, each set with its own angles; an odd
+    batch's last CTA holds one set) gives each set's one-set-per-CTA energies
+    and gradients, also when the sweep runs alone on the saved states after an
+    energy-only run (mode 2)."""
+    import torch
+    from qforte_b200.ucc import evaluator_config
+    mol, pool = random_problem(norb, seed, pool_type)
+    tops = list(range(0, len(pool), 1 if len(pool) < 400 else 3))
+    P = np.random.default_rng(norb + B).uniform(-0.1, 0.1, (B, len(tops)))
+    eng = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference, pool_type=pool_type)
+    ev = eng.evaluator(B)
+    assert ev.path == 2 and ev.real_states and ev.sets_per_cta == 2
+    E, G = ev.eval(P, True)
+    evaluator_config("one-set")
+    try:
+        eng1 = DUCC(mol.hamiltonian, pool, tops, mol.hf_reference, pool_type=pool_type)
+        ev1 = eng1.evaluator(B)
+        assert ev1.sets_per_cta == 1
+        E1, G1 = ev1.eval(P, True)
+    finally:
+        evaluator_config(True)
+    assert np.max(np.abs(E - E1)) < 1e-12 and np.max(np.abs(G - G1)) < 1e-11
+    # energy-only run, then the sweep alone on the saved states
+    d_par, d_en, d_gr = ev.tensors()
+    d_par.copy_(torch.from_numpy(P))
+    ev.run(0)
+    ev.run(2)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(d_gr.cpu().numpy() - G1)) < 1e-11
