@@ -103,9 +103,9 @@ def parse():
     ap.add_argument("--dense", type=int, default=0,
                     help="gate sweep: fuse runs into dense 5- or 6-qubit blocks on the FP64 "
                          "tensor cores (0: tile runs)")
-    ap.add_argument("--fused-phases", action="store_true",
-                    help="gate sweep: apply each tile phase as fused block matrices instead of "
-                         "its gates one by one")
+    ap.add_argument("--phase-form", choices=["auto", "fused", "ops"], default="auto",
+                    help="gate sweep: tile phases as fused 8 x 8 matrices on the FP64 tensor "
+                         "cores, gate by gate, or fused for states larger than L2 (default)")
     ap.add_argument("--complex64", action="store_true",
                     help="gate sweep: the complex64 throughput variant (FP32 arithmetic)")
     ap.add_argument("--autotune", action="store_true",
@@ -328,7 +328,7 @@ def run_gates(a, rank, world, local, emit=True):
     from qforte_b200.workloads import layered_random_circuit
     torch.cuda.set_device(local)
     gates_config(a.tile, a.low_bits, a.reg_bits, getattr(a, "dense", 0),
-                 getattr(a, "fused_phases", False))
+                 {"auto": None, "fused": True, "ops": False}[getattr(a, "phase_form", "auto")])
     peak, src = peaks()
     ns = [int(v) for v in a.nqubits.split(",") if v]
     rows = []
@@ -381,7 +381,7 @@ def run_gates(a, rank, world, local, emit=True):
                                    f"{','.join(map(str, ns))} qubits, from |0...0>",
                        "tile_bits": a.tile, "low_bits": a.low_bits, "reg_bits": a.reg_bits,
                        "dense_block_qubits": getattr(a, "dense", 0),
-                       "phase_form": "fused" if getattr(a, "fused_phases", False) else "ops",
+                       "phase_form": getattr(a, "phase_form", "auto"),
                        "l2": "state larger than L2 from 23 qubits"},
             "sweep": rows,
             "roofline": {"bound": "hbm",

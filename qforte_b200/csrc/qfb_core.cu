@@ -506,7 +506,12 @@ int g_gate_tile_bits = 0;  // 0: kGateTileDefault; -1: one pass per gate
 int g_gate_low_bits = 3;
 
 int g_gate_reg_bits = 0;  // 0: default
-int g_gate_fused = 0;     // 1: phases of R <= 3 register bits in the fused form
+// Form of the tile phases: 0 gate by gate; 1 fused (8 x 8 matrices on the
+// FP64 tensor cores) where it applies; 2 (default) fused for states of at
+// least kFusedMinBytes (larger than L2: below it the gate-by-gate form is
+// faster, the tile traffic being L2-resident).
+int g_gate_fused = 2;
+constexpr uint64_t kFusedMinBytes = 1ull << 27;
 
 // Register bits R of a tile of b qubits: 2^(b-R) threads (<= 256) hold 2^R
 // amplitudes each.  Default 3 (8 amplitudes, 80 registers a thread, three
@@ -528,6 +533,13 @@ bool gate_tile_shape(int n, int &b, int &L) {
     return true;
 }
 
+// Shared memory of the fused-form tile kernel: the tile and barrier word
+// (`plain` bytes), aligned to 16, then two staging buffers.
+inline int fused_bytes(int plain) {
+    return ((plain + 15) & ~15) + 2 * qfbt::kStage * (int)sizeof(double2) +
+           2 * (1 << qfbt::kMaxThreadBits) * (int)sizeof(uint32_t);
+}
+
 int gate_tile_smem() {
     static std::once_flag once;
     static cudaError_t err = cudaSuccess;
@@ -544,10 +556,7 @@ int gate_tile_smem() {
         attr((const void *)qfbt::k_gate_tile<2, float2>, bytes8(10));
         attr((const void *)qfbt::k_gate_tile<3, float2>, bytes8(11));
         attr((const void *)qfbt::k_gate_tile<4, float2>, bytes8(kGateTileMax));
-        attr((const void *)qfbt::k_gate_tile<2, double2, true>, bytes(10));
-        attr((const void *)qfbt::k_gate_tile<3, double2, true>, bytes(11));
-        attr((const void *)qfbt::k_gate_tile<2, float2, true>, bytes8(10));
-        attr((const void *)qfbt::k_gate_tile<3, float2, true>, bytes8(11));
+        attr((const void *)qfbt::k_gate_tile<3, double2, true>, fused_bytes(bytes(11)));
     });
     return err == cudaSuccess ? QFB_OK : cuda_fail(err, "gate tile shared memory");
 }
@@ -731,26 +740,52 @@ void top_apply_host(const qfbt::TOp &o, const double2 *m4, uint32_t tl, int R, d
     }
 }
 
-// The fused form of phase ph (its ops already in tp.ops): segments of
-// consecutive ops with at most kMaxVarBits variant bits, and the per-thread
-// product of the factors that depend on thread bits alone.
-void fuse_phase(TilePlan &tp, qfbt::TPhase &ph, int R, int b) {
-    const uint32_t NR = 1u << R, nth = 1u << (b - R);
-    ph.s0 = (int)tp.segs.size();
-    ph.sc = -1;
+// The fused form of phase ph (R = 3, complex128, 2^(b-3) >= 32 threads; its
+// ops already in tp.ops), appended to tp.ph: segments of consecutive ops with
+// at most kMaxVarBits variant bits, each an 8 x 8 matrix per variant in
+// A-fragment order, and the per-vector product of the factors that depend on
+// thread bits alone.  Consecutive segments share a phase while the union of
+// their variant bits fits in the vector-index bits above the three lowest
+// (n-block and warp bits) and their matrices in one staging buffer (kStage
+// entries); otherwise the phase is split into phases on the same registers,
+// each with its own thread table: all but the last store to the load
+// offsets, the next loads them again.
+void fuse_phase(TilePlan &tp, const qfbt::TPhase &ph, int b) {
+    constexpr int R = 3;
+    constexpr uint32_t NR = 8;
+    const uint32_t nth = 1u << (b - R);
+    const int nvb = b - R - 3;  // vector-index bits above the n-block columns
+    // the register bits' tile bits (loads): register position j <-> roff[1 << j]
+    int rbit[R];
+    uint32_t S = 0;
+    for (int j = 0; j < R; ++j) {
+        rbit[j] = 0;
+        for (int p = 0; p < b; ++p)
+            if (qfbt::tpad(1u << p) == ph.roff[1 << j]) rbit[j] = p;
+        S |= 1u << rbit[j];
+    }
+    const uint32_t T = ((1u << b) - 1u) & ~S;  // thread bits
     std::vector<int> run_ops;
-    std::vector<double2> fac(nth, make_double2(1.0, 0.0));
-    bool any_fac = false;
+    std::vector<qfbt::TOp> fac_ops;
     std::vector<double2> col(NR), mat;
+    struct Seg {
+        uint32_t D;  // variant bits
+        qfbt::TSeg h;
+    };
+    std::vector<Seg> segs;
+    std::vector<double2> mats;
     auto flush = [&](uint32_t D) {
         if (run_ops.empty()) return;
         std::vector<int> dbits;
         for (int p = 0; p < 16; ++p)
             if (D >> p & 1u) dbits.push_back(p);
         const uint32_t nvar = 1u << dbits.size();
-        // every variant's full matrix, then the mixing mask over all of them
-        mat.assign((size_t)nvar * NR * NR, make_double2(0.0, 0.0));
-        uint32_t mm = 0;
+        Seg sg{};
+        sg.D = D;
+        sg.h.m0 = (uint32_t)mats.size();
+        sg.h.nd = (uint32_t)dbits.size();
+        for (size_t j = 0; j < dbits.size(); ++j) sg.h.dsel |= (uint32_t)dbits[j] << (4 * j);
+        mat.assign((size_t)NR * NR, make_double2(0.0, 0.0));
         for (uint32_t x = 0; x < nvar; ++x) {
             uint32_t tl = 0;
             for (size_t j = 0; j < dbits.size(); ++j)
@@ -760,45 +795,25 @@ void fuse_phase(TilePlan &tp, qfbt::TPhase &ph, int R, int b) {
                 col[c] = make_double2(1.0, 0.0);
                 for (int oi : run_ops) top_apply_host(tp.ops[oi], tp.m4.data(), tl, R, col.data());
                 for (uint32_t r = 0; r < NR; ++r) {
-                    mat[((size_t)x * NR + r) * NR + c] = col[r];
-                    if (col[r].x != 0.0 || col[r].y != 0.0) mm |= r ^ c;
+                    mat[r * NR + c] = col[r];
+                    if (col[r].x != 0.0 || col[r].y != 0.0) sg.h.mm |= r ^ c;
                 }
             }
+            for (uint32_t kb = 0; kb < 2; ++kb)
+                for (uint32_t lane = 0; lane < 32; ++lane)
+                    mats.push_back(mat[(lane >> 2) * NR + 4 * kb + (lane & 3)]);
         }
-        const uint32_t Dm = 1u << __builtin_popcount(mm);
-        qfbt::TSeg sg{};
-        sg.m0 = (uint32_t)tp.fm.size();
-        sg.mm = mm;
-        sg.nd = (uint32_t)dbits.size();
-        for (size_t j = 0; j < dbits.size(); ++j) sg.dsel |= (uint32_t)dbits[j] << (4 * j);
-        for (uint32_t x = 0; x < nvar; ++x)
-            for (uint32_t k = 0; k < NR; ++k) {  // groups in ascending order of k's other bits
-                if (k & mm) continue;
-                for (uint32_t i = 0; i < Dm; ++i)
-                    for (uint32_t j = 0; j < Dm; ++j) {
-                        const uint32_t r = k | (uint32_t)deposit_host(i, mm),
-                                       c = k | (uint32_t)deposit_host(j, mm);
-                        tp.fm.push_back(mat[((size_t)x * NR + r) * NR + c]);
-                    }
-            }
-        tp.segs.push_back(sg);
+        segs.push_back(sg);
         run_ops.clear();
     };
     uint32_t D = 0;
     for (int oi = ph.o0; oi < ph.o0 + ph.no; ++oi) {
         const qfbt::TOp &o = tp.ops[oi];
-        const uint32_t cm = o.aux & 0xffu;
-        if (o.opc == qfbt::OPC_DIAG_THREAD && cm == 0) {  // a factor of thread bits alone
-            for (uint32_t t = 0; t < nth; ++t) {
-                double2 one = make_double2(1.0, 0.0);
-                const uint32_t tl = tp.threads[ph.th0 + t] & 0xffffu;
-                top_apply_host(o, tp.m4.data(), tl, 0, &one);
-                fac[t] = cmul_h(one, fac[t]);
-            }
-            any_fac = true;
+        if (o.opc == qfbt::OPC_DIAG_THREAD && (o.aux & 0xffu) == 0) {  // thread bits alone
+            fac_ops.push_back(o);
             continue;
         }
-        uint32_t need = o.tctl | (o.opc == qfbt::OPC_DIAG_THREAD ? o.tbit : 0u);
+        const uint32_t need = o.tctl | (o.opc == qfbt::OPC_DIAG_THREAD ? o.tbit : 0u);
         if (__builtin_popcount(D | need) > qfbt::kMaxVarBits) {
             flush(D);
             D = 0;
@@ -807,11 +822,81 @@ void fuse_phase(TilePlan &tp, qfbt::TPhase &ph, int R, int b) {
         run_ops.push_back(oi);
     }
     flush(D);
-    ph.ns = (int)tp.segs.size() - ph.s0;
-    if (any_fac) {
-        ph.sc = (int)tp.fm.size();
-        tp.fm.insert(tp.fm.end(), fac.begin(), fac.end());
-    }
+    // thread table of a phase with variant bits Dv: vector-index bits 0-2 from
+    // the other thread bits, chosen by residue class (tile bit mod 3) so the
+    // quarter-warp accesses of the B and D fragments spread over the banks;
+    // then Dv; then the rest
+    auto table = [&](uint32_t Dv) {
+        const int c0 = rbit[0] % 3, c1 = rbit[1] % 3, c2 = 3 - c0 - c1;
+        const int want[3] = {c2 >= 0 && c2 < 3 && c2 != c0 && c2 != c1 ? c2 : -1, c1, c2};
+        uint32_t free_bits = T & ~Dv;
+        std::vector<int> tb;
+        for (int w : want) {
+            int pick = -1;
+            for (int p = 0; p < b && pick < 0; ++p)
+                if ((free_bits >> p & 1u) && (w < 0 || p % 3 == w)) pick = p;
+            for (int p = 0; p < b && pick < 0; ++p)
+                if (free_bits >> p & 1u) pick = p;
+            tb.push_back(pick);
+            free_bits &= ~(1u << pick);
+        }
+        for (int p = 0; p < b; ++p)
+            if (Dv >> p & 1u) tb.push_back(p);
+        for (int p = 0; p < b; ++p)
+            if (free_bits >> p & 1u) tb.push_back(p);
+        const int th0 = (int)tp.threads.size();
+        for (uint32_t t = 0; t < nth; ++t) {
+            uint32_t tl = 0;
+            for (size_t j = 0; j < tb.size(); ++j)
+                if (t >> j & 1u) tl |= 1u << tb[j];
+            tp.threads.push_back(tl | (qfbt::tpad(tl) << 16));
+        }
+        return th0;
+    };
+    // group the segments into phases
+    size_t i = 0;
+    bool first = true;
+    do {
+        qfbt::TPhase q = ph;
+        uint32_t Dv = 0;
+        size_t j = i;
+        const uint32_t base = i < segs.size() ? segs[i].h.m0 : 0u;
+        while (j < segs.size()) {
+            const uint32_t end = j + 1 < segs.size() ? segs[j + 1].h.m0 : (uint32_t)mats.size();
+            if (j > i && (end - base > (uint32_t)qfbt::kStage ||
+                          __builtin_popcount(Dv | segs[j].D) > nvb))
+                break;
+            Dv |= segs[j].D;
+            ++j;
+        }
+        q.th0 = table(Dv);
+        q.s0 = (int)tp.segs.size();
+        q.m0 = (int)tp.fm.size();
+        for (size_t k = i; k < j; ++k) {
+            qfbt::TSeg h = segs[k].h;
+            h.m0 = (uint32_t)q.m0 + (h.m0 - base);
+            tp.segs.push_back(h);
+        }
+        const uint32_t end = j < segs.size() ? segs[j].h.m0 : (uint32_t)mats.size();
+        tp.fm.insert(tp.fm.end(), mats.begin() + base, mats.begin() + end);
+        q.ns = (int)(j - i);
+        q.nm = (int)(end - base);
+        q.sc = -1;
+        if (first && !fac_ops.empty()) {
+            q.sc = (int)tp.fm.size();
+            for (uint32_t t = 0; t < nth; ++t) {
+                double2 f = make_double2(1.0, 0.0);
+                const uint32_t tl = tp.threads[q.th0 + t] & 0xffffu;
+                for (const qfbt::TOp &o : fac_ops) top_apply_host(o, tp.m4.data(), tl, 0, &f);
+                tp.fm.push_back(f);
+            }
+        }
+        if (j < segs.size())  // more segments follow on the same registers
+            std::memcpy(q.soff, q.roff, sizeof(q.roff));
+        tp.ph.push_back(q);
+        i = j;
+        first = false;
+    } while (i < segs.size());
 }
 
 // Split a run's gates (tile coordinates) into phases of R register bits.
@@ -821,7 +906,8 @@ void fuse_phase(TilePlan &tp, qfbt::TPhase &ph, int R, int b) {
 // gate that cannot join blocks its bits for the rest of the scan, so only
 // gates on disjoint qubits change order.
 // c64: shared offsets in the complex64 tile layout (qfbt::tpad8).
-// fused: also the phases' fused form (R <= kMaxFusedRegBits).
+// fused: the phases' fused form where it applies (R = 3, complex128, at
+// least 32 threads).
 void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, TilePlan &tp,
                       bool c64 = false, bool fused = false) {
     auto toff = [c64](uint32_t l) { return c64 ? qfbt::tpad8(l) : qfbt::tpad(l); };
@@ -996,8 +1082,10 @@ void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, Til
             ph.soff[k] = toff(l);
         }
         ph.no = (int)tp.ops.size() - ph.o0;
-        if (fused && R <= qfbt::kMaxFusedRegBits) fuse_phase(tp, ph, R, b);
-        tp.ph.push_back(ph);
+        if (fused && R == 3 && b - R >= 5 && !c64)
+            fuse_phase(tp, ph, b);
+        else
+            tp.ph.push_back(ph);
     }
     run.np = (int)tp.ph.size() - run.p0;
     run.b = b;
@@ -1214,7 +1302,8 @@ int apply_gates_tiles(A *d, int n, int nbatch, const std::vector<HGate> &hg) {
     std::vector<GatePlanWin> wins;
     TilePlan tp;
     std::vector<qfbt::TRun> runs;
-    const bool fused = g_gate_fused != 0;
+    const bool fused = g_gate_fused == 1 ||
+                       (g_gate_fused == 2 && sizeof(double2) * nbasis * (uint64_t)nbatch >= kFusedMinBytes);
     plan_gate_tiles(hg, n, b, L, wins, tp, runs, c64, fused);
     // one upload of phases, ops, 4x4 matrices, chunk and thread tables and
     // the fused form
@@ -1259,16 +1348,16 @@ int apply_gates_tiles(A *d, int n, int nbatch, const std::vector<HGate> &hg) {
             continue;
         }
         const int tb = pw.w.b, R = tile_reg_bits(tb);
-        const size_t smem = sizeof(A) * qfbt::tpad_size_of<A>(tb) + 16;
+        const size_t smem0 = sizeof(A) * qfbt::tpad_size_of<A>(tb) + 16;
+        const bool fz = fused && R == 3 && tb - R >= 5 && !c64;
+        const size_t smem = fz ? (size_t)fused_bytes((int)smem0) : smem0;
         const dim3 grid((unsigned)(nbasis >> tb), nbatch), block(1u << (tb - R));
 #define QFB_TILE(RR, FF)                                                                        \
     qfbt::k_gate_tile<RR, A, FF><<<grid, block, smem, t_stream>>>(d, nbasis, runs[i], d_ph, d_ops, \
                                                                   d_m4, d_ch, d_th, d_sg, d_fm)
-        if (R == 2 && fused)
-            QFB_TILE(2, true);
-        else if (R == 2)
+        if (R == 2)
             QFB_TILE(2, false);
-        else if (R == 3 && fused)
+        else if (R == 3 && fz)
             QFB_TILE(3, true);
         else if (R == 3)
             QFB_TILE(3, false);
@@ -1529,9 +1618,9 @@ int qfb_gates_dense(int k) {
     return QFB_OK;
 }
 
-int qfb_gates_fused(int on) {
-    if (on != 0 && on != 1) return fail(QFB_EINVAL, "qfb_gates_fused: %d is not 0 or 1", on);
-    g_gate_fused = on;
+int qfb_gates_fused(int mode) {
+    if (mode < 0 || mode > 2) return fail(QFB_EINVAL, "qfb_gates_fused: %d is not 0, 1 or 2", mode);
+    g_gate_fused = mode;
     return QFB_OK;
 }
 

@@ -70,37 +70,46 @@ struct TPhase {
     uint32_t soff[1 << kMaxRegBits];  // store: the same after the phase's relabelings
     int32_t o0, no;                   // ops of this phase
     int32_t th0;                      // this phase's entries of the thread table
-    int32_t pad;
+    int32_t nm;                       // fused form: matrix entries of its segments
     int32_t s0, ns;                   // fused form: segments of this phase
     int32_t sc;                       // fused form: per-thread factor table (-1: none)
-    int32_t pad2;
+    int32_t m0;                       // fused form: first matrix entry of its segments
 };
 static_assert(sizeof(TPhase) == 160, "TPhase layout");
 
-// The fused form of a phase (runs with R <= kMaxFusedRegBits): its ops, in
-// order, become a few segments, each one block-diagonal 2^R x 2^R matrix on
-// the thread's registers, plus one factor per thread.
-//  * The matrix of a segment depends on the thread only through its variant
+// The fused form of a phase (complex128 tiles with R = 3 and at least 32
+// threads): the phase's ops, in order, become a few segments, each one 8 x 8
+// matrix on the 8 register amplitudes, applied on the FP64 tensor cores.
+//  * Vector t of the phase (the 8 amplitudes at tile offsets base(t) +
+//    roff[k], base from entry t of the thread table) is processed by warp
+//    t / 32 as column t % 8 of n-block (t / 8) % 4: per n-block the warp
+//    computes Y = M X with mma.sync.m8n8k4 FP64 (k-blocks of registers 0-3
+//    and 4-7; real and imaginary parts as four real products), B fragments
+//    read straight from the tile, D fragments stored straight back.
+//  * The matrix of a segment depends on the vector only through its variant
 //    bits (the tile bits of the thread part that its ops test: controls on
 //    thread bits, the bit of a diagonal on a thread bit that is also
 //    controlled by register bits), at most kMaxVarBits of them; the host
-//    builds one matrix per assignment of those bits.
-//  * Its mixing mask mm holds the register bits the matrix mixes (the bits of
-//    i ^ j over its nonzero entries i, j): registers that differ only outside
-//    mm never mix, so the matrix is 2^R / D blocks of D x D (D = 2^|mm|), for
-//    the groups of registers with equal bits outside mm, in ascending order.
+//    builds one matrix per assignment of those bits and orders the thread
+//    table so that the phase's variant bits are vector-index bits 3 and up:
+//    all 8 columns of an n-block share one matrix.
 //  * Diagonal factors that depend on thread bits alone (a diagonal on a
-//    thread bit, controlled by thread bits or not at all) scale all 2^R
-//    registers of a thread alike and commute with everything else in the
-//    phase: their product, per thread, is one table entry.
-// Variant index: bit j is tile bit (dsel >> 4j) & 15 of the thread; matrix of
-// variant x at m0 + x * 2^R * D, block g at + g * D * D, row-major.
-constexpr int kMaxFusedRegBits = 3;
-constexpr int kMaxVarBits = 4;
+//    thread bit, controlled by thread bits or not at all) scale all 8
+//    amplitudes of a vector alike and commute with everything else in the
+//    phase: their product, per vector, is one table entry (applied on load).
+// Variant index: bit j is tile bit (dsel >> 4j) & 15 of the vector; matrix of
+// variant x at m0 + 64 x, in A-fragment order: entry 32 kb + lane holds
+// (Re, Im) of M[lane / 4][4 kb + lane % 4].
+// A phase's matrices (at most kStage entries; the host splits a phase that
+// would hold more into phases on the same registers) and its thread table
+// are copied into one of two shared-memory buffers before the barrier that
+// precedes the phase.
+constexpr int kMaxVarBits = 3;
+constexpr int kStage = 512;  // double2 entries per staging buffer (8 KB)
 struct TSeg {
     uint32_t m0;    // first entry of this segment's matrices
     uint32_t dsel;  // variant bits: tile bit positions, 4 bits each
-    uint32_t mm;    // mixing mask on the register bits
+    uint32_t mm;    // register bits the matrix mixes (host statistics)
     uint32_t nd;    // number of variant bits
 };
 static_assert(sizeof(TSeg) == 16, "TSeg layout");
@@ -195,6 +204,13 @@ __device__ __forceinline__ void bulk_commit_and_wait() {
 __device__ __forceinline__ void fence_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+
+// 16-byte asynchronous global -> shared copy (L2 only) and its group waits.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // ---- gate arithmetic on the registers --------------------------------------
 // Register positions are template parameters, so every register index below
@@ -407,85 +423,108 @@ __device__ __forceinline__ void apply_op(A (&v)[1 << R], const TOp *__restrict__
 
 // ---- the fused form ---------------------------------------------------------
 
-// The bits of j placed on the set bits of MM, lowest first (compile time).
-template <int MM>
-__host__ __device__ constexpr int dep_c(int j) {
-    int r = 0, b = 0;
-    for (int p = 0; p < 8; ++p)
-        if ((MM >> p) & 1) {
-            if ((j >> b) & 1) r |= 1 << p;
-            ++b;
-        }
-    return r;
+// D += A B on one 8x8x4 FP64 block (register operands only).
+__device__ __forceinline__ void tmma(double &d0, double &d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
 }
 
-// Index of register group k (k's bits outside MM, packed; compile time).
-template <int R, int MM>
-__host__ __device__ constexpr int grp_c(int k) {
-    int r = 0, b = 0;
-    for (int p = 0; p < R; ++p)
-        if (!((MM >> p) & 1)) {
-            if ((k >> p) & 1) r |= 1 << b;
-            ++b;
-        }
-    return r;
-}
-
-template <int MM>
-__host__ __device__ constexpr int popc_c() {
-    int c = 0;
-    for (int p = 0; p < 8; ++p) c += (MM >> p) & 1;
-    return c;
-}
-
-// acc + m x (complex)
-template <class A>
-__device__ __forceinline__ A c_fma(A m, A x, A acc) {
-    acc.x = fma(m.x, x.x, acc.x);
-    acc.y = fma(m.x, x.y, acc.y);
-    acc.x = fma(-m.y, x.y, acc.x);
-    acc.y = fma(m.y, x.x, acc.y);
-    return acc;
-}
-
-// The segment matrix (blocks of D x D on the mixing bits MM) on the registers.
-template <int R, int MM, class A>
-__device__ __forceinline__ void ap_fused(A (&v)[1 << R], const double2 *__restrict__ m) {
-    if constexpr (MM < (1 << R)) {
-        constexpr int D = 1 << popc_c<MM>();
-#pragma unroll
-        for (int k = 0; k < (1 << R); ++k) {
-            if (k & MM) continue;
-            const double2 *mg = m + grp_c<R, MM>(k) * D * D;
-            A y[D];
-#pragma unroll
-            for (int i = 0; i < D; ++i) {
-                A acc = c_mul(AmpT<A>::cvt(ld_entry(mg + i * D)), v[k | dep_c<MM>(0)]);
-#pragma unroll
-                for (int j = 1; j < D; ++j)
-                    acc = c_fma(AmpT<A>::cvt(ld_entry(mg + i * D + j)), v[k | dep_c<MM>(j)], acc);
-                y[i] = acc;
-            }
-#pragma unroll
-            for (int i = 0; i < D; ++i) v[k | dep_c<MM>(i)] = y[i];
-        }
-    }
-}
-
-// One segment of a fused phase on the thread with tile bits tl.
-template <int R, class A>
-__device__ __forceinline__ void apply_seg(A (&v)[1 << R], const TSeg *__restrict__ sg, uint32_t tl,
-                                          const double2 *__restrict__ fm) {
-    const uint4 h = __ldg(reinterpret_cast<const uint4 *>(sg));
+// Variant of a vector with tile bits tl for a segment with header h.
+__device__ __forceinline__ uint32_t seg_variant(uint32_t tl, const uint4 &h) {
     uint32_t var = 0;
     for (uint32_t j = 0; j < h.w; ++j) var |= ((tl >> ((h.y >> (4 * j)) & 15u)) & 1u) << j;
-    const double2 *m = fm + h.x + (size_t)var * ((1u << R) << __popc(h.z));
-    switch (h.z) {
-#define X(N) case N: ap_fused<R, N>(v, m); break;
-        X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7)
-#undef X
-        default:
-            break;
+    return var;
+}
+
+// One fused phase on this warp's 32 vectors: its segments in order (each
+// reads the vectors at roff and writes them back, the last one at soff).
+__device__ __forceinline__ void fused_phase(const TPhase *__restrict__ ph, const TSeg *__restrict__ segs,
+                                            const double2 *__restrict__ fm, const double2 *sm,
+                                            const uint32_t *thr, double2 *tile) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+    const int s0 = __ldg(&ph->s0), ns = __ldg(&ph->ns), sc = __ldg(&ph->sc);
+    const uint32_t m0 = (uint32_t)__ldg(&ph->m0);
+    const uint32_t ri0 = __ldg(&ph->roff[q]), ri1 = __ldg(&ph->roff[4 + q]);
+    const uint32_t ro_mid = __ldg(&ph->roff[g]), ro_last = __ldg(&ph->soff[g]);
+    if (ns == 0) {  // relabelings only: each thread moves its own vector
+        const uint32_t base = thr[threadIdx.x] >> 16;
+        double2 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = tile[base + __ldg(&ph->roff[k])];
+        if (sc >= 0) {
+            const double2 f = __ldg(fm + sc + threadIdx.x);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = c_mul(f, v[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) tile[base + __ldg(&ph->soff[k])] = v[k];
+        return;
+    }
+    for (int si = 0; si < ns; ++si) {
+        const uint4 h = __ldg(reinterpret_cast<const uint4 *>(segs + s0 + si));
+        const uint32_t ro = si + 1 == ns ? ro_last : ro_mid;
+        const bool scale = si == 0 && sc >= 0;
+        const double2 *mseg = sm + (h.x - m0);
+        double2 a0[2], a1[2];
+        // two n-blocks at a time: all their B loads, then 16 mma in four
+        // independent chains, then their D stores (n-blocks hold disjoint
+        // vectors, so the loads may all precede the stores)
+#pragma unroll
+        for (int np = 0; np < 4; np += 2) {
+            double2 x0[2], x1[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int tv = warp * 32 + (np + u) * 8;  // first vector of the n-block
+                if (np + u == 0 || h.w != 0) {
+                    const double2 *mv = mseg + 64u * seg_variant(thr[tv] & 0xffffu, h);
+                    a0[u] = mv[lane];
+                    a1[u] = mv[32 + lane];
+                } else {
+                    a0[u] = a0[0];
+                    a1[u] = a1[0];
+                }
+                // B fragments: registers 4 kb + q of vector tv + g
+                const uint32_t bb = thr[tv + g] >> 16;
+                x0[u] = tile[bb + ri0];
+                x1[u] = tile[bb + ri1];
+                if (scale) {
+                    const double2 f = __ldg(fm + sc + tv + g);
+                    x0[u] = c_mul(f, x0[u]);
+                    x1[u] = c_mul(f, x1[u]);
+                }
+            }
+            double dr[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, di[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                tmma(dr[u][0], dr[u][1], a0[u].x, x0[u].x);
+                tmma(di[u][0], di[u][1], a0[u].x, x0[u].y);
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                tmma(dr[u][0], dr[u][1], a0[u].y, -x0[u].y);
+                tmma(di[u][0], di[u][1], a0[u].y, x0[u].x);
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                tmma(dr[u][0], dr[u][1], a1[u].x, x1[u].x);
+                tmma(di[u][0], di[u][1], a1[u].x, x1[u].y);
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                tmma(dr[u][0], dr[u][1], a1[u].y, -x1[u].y);
+                tmma(di[u][0], di[u][1], a1[u].y, x1[u].x);
+            }
+            // D fragments: register g of vectors tv + 2q and tv + 2q + 1 (every
+            // lane's B loads completed before the warp-wide mma)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int tv = warp * 32 + (np + u) * 8;
+                tile[(thr[tv + 2 * q] >> 16) + ro] = make_double2(dr[u][0], di[u][0]);
+                tile[(thr[tv + 2 * q + 1] >> 16) + ro] = make_double2(dr[u][1], di[u][1]);
+            }
+        }
+        if (si + 1 < ns) __syncwarp();  // the next segment reads what this one wrote
     }
 }
 
@@ -546,16 +585,55 @@ __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
     const int tid = threadIdx.x, nth = blockDim.x;
     const int nch = 1 << (b - 3);
     __shared__ uint64_t s_base;
+    // fused form: two staging buffers (kStage matrix entries, then the
+    // phase's thread table) after the barrier word
+    constexpr bool kF = F && R == 3 && sizeof(A) == sizeof(double2);
+    double2 *sbuf = reinterpret_cast<double2 *>(
+        t_smem + ((sizeof(A) * tpad_size_of<A>(b) + 16 + 15) & ~(size_t)15));
+    uint32_t *sthr = reinterpret_cast<uint32_t *>(sbuf + 2 * kStage);
+    auto stage = [&](int p) {
+        if constexpr (kF) {
+            const TPhase *q = phases + run.p0 + p;
+            const int nm = __ldg(&q->nm), m0 = __ldg(&q->m0);
+            double2 *dst = sbuf + (p & 1) * kStage;
+            for (int i = tid; i < nm; i += nth) dst[i] = __ldg(fm + m0 + i);
+            sthr[(p & 1) * (1 << kMaxThreadBits) + tid] = __ldg(&threads[__ldg(&q->th0) + tid]);
+        }
+    };
 
     if (tid == 0) {
-        mbar_init(bar_a, 1);
-        mbar_expect_tx(bar_a, (uint32_t)nch * kChunk);
+        if constexpr (!kF) {
+            mbar_init(bar_a, 1);
+            mbar_expect_tx(bar_a, (uint32_t)nch * kChunk);
+        }
         // tile origin: blockIdx.x's bits on the qubits outside Q, plus the slot
         s_base = (uint64_t)blockIdx.y * nbasis + spread_around(blockIdx.x, run.qmask);
     }
     __syncthreads();
     A *s = psi + s_base;
     const uint64_t *ch = chunks + run.ch0;
+    if constexpr (kF) {
+        // 16-byte asynchronous copies, eight consecutive threads per chunk
+        for (int i = tid; i < 8 * nch; i += nth) {
+            const int c = i >> 3, e = i & 7;
+            cp_async16(smem_u32(tile + tpad((uint32_t)c << 3) + e), s + __ldg(&ch[c]) + e);
+        }
+        cp_async_commit();
+        if (run.np > 0) stage(0);
+        cp_async_wait_all();
+        __syncthreads();  // the tile, phase 0's matrices and thread table
+        for (int p = 0; p < run.np; ++p) {
+            fused_phase(phases + run.p0 + p, segs, fm, sbuf + (p & 1) * kStage,
+                        sthr + (p & 1) * (1 << kMaxThreadBits), reinterpret_cast<double2 *>(tile));
+            if (p + 1 < run.np) stage(p + 1);
+            __syncthreads();
+        }
+        for (int i = tid; i < 8 * nch; i += nth) {
+            const int c = i >> 3, e = i & 7;
+            s[__ldg(&ch[c]) + e] = tile[tpad((uint32_t)c << 3) + e];
+        }
+        return;
+    }
     for (int c = tid; c < nch; c += nth)
         bulk_g2s(smem_u32(tile + tpad_of<A>((uint32_t)c << 3)), s + __ldg(&ch[c]), kChunk, bar_a);
     const uint64_t limit = g_tile_wait_limit_ns;
@@ -572,25 +650,14 @@ __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
         const TPhase *ph = phases + run.p0 + p;
         const uint32_t tw = __ldg(&threads[__ldg(&ph->th0) + tid]);
         const uint32_t tl = tw & 0xffffu;
-        const A *t0 = tile + (tw >> 16);
+        A *t0 = tile + (tw >> 16);
         A v[1 << R];
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) v[k] = t0[__ldg(&ph->roff[k])];
-        if constexpr (F && R <= kMaxFusedRegBits) {
-            const int s0 = __ldg(&ph->s0), s1 = s0 + __ldg(&ph->ns), sc = __ldg(&ph->sc);
-            for (int si = s0; si < s1; ++si) apply_seg<R, A>(v, segs + si, tl, fm);
-            if (sc >= 0) {
-                const A f = AmpT<A>::cvt(__ldg(fm + sc + tid));
+        const int o0 = __ldg(&ph->o0), o1 = o0 + __ldg(&ph->no);
+        for (int o = o0; o < o1; ++o) apply_op<R, A>(v, ops + o, tl, m4);
 #pragma unroll
-                for (int k = 0; k < (1 << R); ++k) v[k] = c_mul(f, v[k]);
-            }
-        } else {
-            const int o0 = __ldg(&ph->o0), o1 = o0 + __ldg(&ph->no);
-            for (int o = o0; o < o1; ++o) apply_op<R, A>(v, ops + o, tl, m4);
-        }
-        A *t1 = tile + (tw >> 16);
-#pragma unroll
-        for (int k = 0; k < (1 << R); ++k) t1[__ldg(&ph->soff[k])] = v[k];
+        for (int k = 0; k < (1 << R); ++k) t0[__ldg(&ph->soff[k])] = v[k];
         if (p + 1 < run.np) __syncthreads();
     }
     fence_async_smem();

@@ -185,14 +185,15 @@ def gate_phases(gates, nqubit):
     return p.value, o.value
 
 
-def gates_config(tile_bits=0, low_bits=3, reg_bits=0, dense=0, fused=False):
+def gates_config(tile_bits=0, low_bits=3, reg_bits=0, dense=0, fused=None):
     """Process-wide shape of gate runs: tile_bits 0 (default) or 4-12 for
     register-blocked shared-memory tiles, -1 for one pass per gate; reg_bits 0
     for the default register bits per thread; dense 5 or 6 to fuse runs on at
     most that many qubits into dense unitaries applied on the FP64 tensor
-    cores instead (states of 10 qubits and more); fused True to apply each
-    tile phase as fused block matrices instead of its gates one by one."""
+    cores instead (states of 10 qubits and more); fused True / False to apply
+    each tile phase as fused 8 x 8 matrices on the FP64 tensor cores / its
+    gates one by one (None: fused for states larger than L2)."""
     check(lib().qfb_gates_config(int(tile_bits), int(low_bits)), "qfb_gates_config")
     check(lib().qfb_gates_regs(int(reg_bits)), "qfb_gates_regs")
     check(lib().qfb_gates_dense(int(dense)), "qfb_gates_dense")
-    check(lib().qfb_gates_fused(1 if fused else 0), "qfb_gates_fused")
+    check(lib().qfb_gates_fused(2 if fused is None else 1 if fused else 0), "qfb_gates_fused")

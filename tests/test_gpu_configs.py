@@ -94,7 +94,9 @@ def _sweep_cases():
     for n in (20, 24, 28):
         if os.path.exists(os.path.join(GOLDEN, f"sweep{n}_seed{11 + n}.npz")):
             for tile, dense in ((0, 0), (-1, 0), (0, 5), (0, 6)):
-                out.append((n, tile, dense))
+                out.append((n, tile, dense, None))
+            out.append((n, 0, 0, False))  # tile phases gate by gate at every size
+            out.append((n, 0, 0, True))   # tile phases fused at every size
     return out
 
 
@@ -105,16 +107,17 @@ def restore_gates_config():
     gates_config(0, 3, 0, 0)
 
 
-@pytest.mark.parametrize("n,tile,dense", _sweep_cases())
-def test_gate_sweep_matches_reference(cuda, restore_gates_config, n, tile, dense):
+@pytest.mark.parametrize("n,tile,dense,fused", _sweep_cases())
+def test_gate_sweep_matches_reference(cuda, restore_gates_config, n, tile, dense, fused):
     """Config: the 100-layer random gate sweep on the register-blocked tile
-    path (tile 0), on one pass per gate (tile -1) and in dense 5- and 6-qubit
-    blocks on the FP64 tensor cores: sampled amplitudes at 1e-12, the norm,
-    <Z_k> of every qubit and the mass of each value of the top 8 qubits
-    against the reference's state."""
+    path (tile 0; its phases in the default form, gate by gate, and fused into
+    8 x 8 matrices on the FP64 tensor cores), on one pass per gate (tile -1)
+    and in dense 5- and 6-qubit blocks on the FP64 tensor cores: sampled
+    amplitudes at 1e-12, the norm, <Z_k> of every qubit and the mass of each
+    value of the top 8 qubits against the reference's state."""
     from qforte_b200.workloads import layered_random_circuit
     z = golden(f"sweep{n}_seed{11 + n}.npz")
-    restore_gates_config(tile, 3, 0, dense)
+    restore_gates_config(tile, 3, 0, dense, fused)
     circ, spec = layered_random_circuit(n, int(z["layers"]), int(z["seed"]))
     assert len(spec) == int(z["ngates"])
     qc = qb.Computer(n)
@@ -161,8 +164,8 @@ def test_gate_sweep_32_qubits_norm_and_inverse(cuda, restore_gates_config):
     hold it (the reference needs 40 bytes an amplitude and overflows 32-bit
     loop counters there, computer.cc:637-643), so the checks are
     size-independent: after 10 layers the norm is 1 within 1e-12, and the
-    adjoint circuit returns |0...0> within 1e-12, on the tile runs and on
-    dense 5-qubit blocks."""
+    adjoint circuit returns |0...0> within 1e-12, on the tile runs (phases
+    fused and gate by gate) and on dense 5-qubit blocks."""
     import torch
     from qforte_b200.workloads import layered_random_circuit
     free, _ = torch.cuda.mem_get_info()
@@ -173,8 +176,8 @@ def test_gate_sweep_32_qubits_norm_and_inverse(cuda, restore_gates_config):
     inv = circ.adjoint()
     qc = qb.Computer(n)
     try:
-        for tile, dense in ((0, 0), (0, 5)):
-            restore_gates_config(tile, 3, 0, dense)
+        for tile, dense, fused in ((0, 0, None), (0, 0, False), (0, 5, None)):
+            restore_gates_config(tile, 3, 0, dense, fused)
             qc.reset()
             qc.apply_circuit(circ)
             assert abs(qb.inner_product(qc, qc) - 1.0) < AMP_TOL

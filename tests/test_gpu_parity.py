@@ -495,8 +495,9 @@ def test_dense_blocks_on_a_batch_of_states(cuda, dense_blocks):
 
 
 def test_gate_tile_wait_that_runs_out_reports_and_leaves_state(cuda, gate_tiles):
-    """The tile kernel's bounded wait for its bulk load copies, made to run out
-    with no fault: with the wait limit at 0 every tile gives up at once, flags
+    """The tile kernel's bounded wait for its bulk load copies (the gate-by-gate
+    phase form, which states smaller than L2 take), made to run out with no
+    fault: with the wait limit at 0 every tile gives up at once, flags
     it and leaves its tile unwritten.  The next download reports
     QFB_ETIMEDOUT (RuntimeError), the state is exactly as before, and with the
     limit restored the same circuit gives the oracle's state."""
