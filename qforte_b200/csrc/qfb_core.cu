@@ -534,10 +534,9 @@ bool gate_tile_shape(int n, int &b, int &L) {
 }
 
 // Shared memory of the fused-form tile kernel: the tile and barrier word
-// (`plain` bytes), aligned to 16, then two staging buffers.
+// (`plain` bytes), aligned to 16, then two thread-table buffers.
 inline int fused_bytes(int plain) {
-    return ((plain + 15) & ~15) + 2 * qfbt::kStage * (int)sizeof(double2) +
-           2 * (1 << qfbt::kMaxThreadBits) * (int)sizeof(uint32_t);
+    return ((plain + 15) & ~15) + 2 * (1 << qfbt::kMaxThreadBits) * (int)sizeof(uint32_t);
 }
 
 int gate_tile_smem() {
@@ -802,6 +801,7 @@ void fuse_phase(TilePlan &tp, const qfbt::TPhase &ph, int b) {
             for (uint32_t kb = 0; kb < 2; ++kb)
                 for (uint32_t lane = 0; lane < 32; ++lane)
                     mats.push_back(mat[(lane >> 2) * NR + 4 * kb + (lane & 3)]);
+
         }
         segs.push_back(sg);
         run_ops.clear();

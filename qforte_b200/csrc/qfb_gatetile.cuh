@@ -100,12 +100,14 @@ static_assert(sizeof(TPhase) == 160, "TPhase layout");
 // Variant index: bit j is tile bit (dsel >> 4j) & 15 of the vector; matrix of
 // variant x at m0 + 64 x, in A-fragment order: entry 32 kb + lane holds
 // (Re, Im) of M[lane / 4][4 kb + lane % 4].
-// A phase's matrices (at most kStage entries; the host splits a phase that
-// would hold more into phases on the same registers) and its thread table
-// are copied into one of two shared-memory buffers before the barrier that
-// precedes the phase.
+// A warp reads its A fragments straight from the matrix pool (each lane its
+// own entry: one coalesced 512-byte load per fragment, L1-resident across the
+// tiles of a run); a phase's thread table is copied into one of two
+// shared-memory buffers before the barrier that precedes the phase.  The host
+// splits a phase whose segments hold more than kStage matrix entries into
+// phases on the same registers.
 constexpr int kMaxVarBits = 3;
-constexpr int kStage = 512;  // double2 entries per staging buffer (8 KB)
+constexpr int kStage = 512;  // matrix entries of one phase
 struct TSeg {
     uint32_t m0;    // first entry of this segment's matrices
     uint32_t dsel;  // variant bits: tile bit positions, 4 bits each
@@ -440,32 +442,31 @@ __device__ __forceinline__ uint32_t seg_variant(uint32_t tl, const uint4 &h) {
 // One fused phase on this warp's 32 vectors: its segments in order (each
 // reads the vectors at roff and writes them back, the last one at soff).
 __device__ __forceinline__ void fused_phase(const TPhase *__restrict__ ph, const TSeg *__restrict__ segs,
-                                            const double2 *__restrict__ fm, const double2 *sm,
-                                            const uint32_t *thr, double2 *tile) {
+                                            const double2 *__restrict__ fm, const uint32_t *thr,
+                                            double2 *tile) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
     const int s0 = __ldg(&ph->s0), ns = __ldg(&ph->ns), sc = __ldg(&ph->sc);
-    const uint32_t m0 = (uint32_t)__ldg(&ph->m0);
-    const uint32_t ri0 = __ldg(&ph->roff[q]), ri1 = __ldg(&ph->roff[4 + q]);
-    const uint32_t ro_mid = __ldg(&ph->roff[g]), ro_last = __ldg(&ph->soff[g]);
     if (ns == 0) {  // relabelings only: each thread moves its own vector
-        const uint32_t base = thr[threadIdx.x] >> 16;
+        double2 *t0 = tile + (thr[threadIdx.x] >> 16);
         double2 v[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = tile[base + __ldg(&ph->roff[k])];
+        for (int k = 0; k < 8; ++k) v[k] = t0[__ldg(&ph->roff[k])];
         if (sc >= 0) {
             const double2 f = __ldg(fm + sc + threadIdx.x);
 #pragma unroll
             for (int k = 0; k < 8; ++k) v[k] = c_mul(f, v[k]);
         }
 #pragma unroll
-        for (int k = 0; k < 8; ++k) tile[base + __ldg(&ph->soff[k])] = v[k];
+        for (int k = 0; k < 8; ++k) t0[__ldg(&ph->soff[k])] = v[k];
         return;
     }
+    const uint32_t ri0 = __ldg(&ph->roff[q]), ri1 = __ldg(&ph->roff[4 + q]);
+    const uint32_t ro_mid = __ldg(&ph->roff[g]), ro_last = __ldg(&ph->soff[g]);
     for (int si = 0; si < ns; ++si) {
         const uint4 h = __ldg(reinterpret_cast<const uint4 *>(segs + s0 + si));
         const uint32_t ro = si + 1 == ns ? ro_last : ro_mid;
         const bool scale = si == 0 && sc >= 0;
-        const double2 *mseg = sm + (h.x - m0);
+        const double2 *mseg = fm + h.x;
         double2 a0[2], a1[2];
         // two n-blocks at a time: all their B loads, then 16 mma in four
         // independent chains, then their D stores (n-blocks hold disjoint
@@ -478,8 +479,8 @@ __device__ __forceinline__ void fused_phase(const TPhase *__restrict__ ph, const
                 const int tv = warp * 32 + (np + u) * 8;  // first vector of the n-block
                 if (np + u == 0 || h.w != 0) {
                     const double2 *mv = mseg + 64u * seg_variant(thr[tv] & 0xffffu, h);
-                    a0[u] = mv[lane];
-                    a1[u] = mv[32 + lane];
+                    a0[u] = __ldg(mv + lane);
+                    a1[u] = __ldg(mv + 32 + lane);
                 } else {
                     a0[u] = a0[0];
                     a1[u] = a1[0];
@@ -570,7 +571,7 @@ __host__ __device__ __forceinline__ uint32_t tpad_size_of(int b) {
 // F: the phases' fused form (segments and per-thread factors in segs / fm)
 // instead of their op lists.
 template <int R, class A = double2, bool F = false>
-__global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
+__global__ void __launch_bounds__(256, F ? 4 : R == 4 ? 1 : 3)
     k_gate_tile(A *__restrict__ psi, uint64_t nbasis, TRun run,
                 const TPhase *__restrict__ phases, const TOp *__restrict__ ops,
                 const double2 *__restrict__ m4, const uint64_t *__restrict__ chunks,
@@ -585,20 +586,14 @@ __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
     const int tid = threadIdx.x, nth = blockDim.x;
     const int nch = 1 << (b - 3);
     __shared__ uint64_t s_base;
-    // fused form: two staging buffers (kStage matrix entries, then the
-    // phase's thread table) after the barrier word
+    // fused form: two buffers of a phase's thread table after the barrier word
     constexpr bool kF = F && R == 3 && sizeof(A) == sizeof(double2);
-    double2 *sbuf = reinterpret_cast<double2 *>(
+    uint32_t *sthr = reinterpret_cast<uint32_t *>(
         t_smem + ((sizeof(A) * tpad_size_of<A>(b) + 16 + 15) & ~(size_t)15));
-    uint32_t *sthr = reinterpret_cast<uint32_t *>(sbuf + 2 * kStage);
     auto stage = [&](int p) {
-        if constexpr (kF) {
-            const TPhase *q = phases + run.p0 + p;
-            const int nm = __ldg(&q->nm), m0 = __ldg(&q->m0);
-            double2 *dst = sbuf + (p & 1) * kStage;
-            for (int i = tid; i < nm; i += nth) dst[i] = __ldg(fm + m0 + i);
-            sthr[(p & 1) * (1 << kMaxThreadBits) + tid] = __ldg(&threads[__ldg(&q->th0) + tid]);
-        }
+        if constexpr (kF)
+            sthr[(p & 1) * (1 << kMaxThreadBits) + tid] =
+                __ldg(&threads[__ldg(&phases[run.p0 + p].th0) + tid]);
     };
 
     if (tid == 0) {
@@ -621,10 +616,10 @@ __global__ void __launch_bounds__(256, R == 4 ? 1 : 3)
         cp_async_commit();
         if (run.np > 0) stage(0);
         cp_async_wait_all();
-        __syncthreads();  // the tile, phase 0's matrices and thread table
+        __syncthreads();  // the tile and phase 0's thread table
         for (int p = 0; p < run.np; ++p) {
-            fused_phase(phases + run.p0 + p, segs, fm, sbuf + (p & 1) * kStage,
-                        sthr + (p & 1) * (1 << kMaxThreadBits), reinterpret_cast<double2 *>(tile));
+            fused_phase(phases + run.p0 + p, segs, fm, sthr + (p & 1) * (1 << kMaxThreadBits),
+                        reinterpret_cast<double2 *>(tile));
             if (p + 1 < run.np) stage(p + 1);
             __syncthreads();
         }
