@@ -33,7 +33,7 @@ class Trace:
     """A loaded trace with this package's objects built on demand."""
 
     def __init__(self, z):
-        self.z = z
+        self.z = z if isinstance(z, dict) else {k: z[k] for k in z.files}  # read each array once
         self.labels = [str(s) for s in z["labels"]]
         self._circ, self._op = {}, {}
 
@@ -85,6 +85,7 @@ def replay(z, make, check, inner=None, limit=None):
     make(src_computer) builds a Computer; inner(a, b) is the module-level
     inner product.  Returns the number of calls made."""
     tr = Trace(z)
+    z = tr.z
     comps = {}
     res, rp = z["res"], z["res_ptr"]
     calls = z["calls"] if limit is None else z["calls"][:limit]

@@ -7,9 +7,8 @@ Computer, with its results.  Replayed call for call on the oracle's host state
 with this package's Gate, Circuit and QubitOperator, every result must equal
 the reference's (energies and expectation values 1e-12, state projections
 1e-12), and the last energy the reference's FCI value within the tolerance its
-test states.  The ADAPT trace (19,126 calls) is replayed here up to its first
-2,500 calls, which keeps this CPU test short; the device replay
-(test_gpu_dropin_replay.py) runs both traces in full.
+test states.  The same traces run on the device Computer in
+test_gpu_dropin_replay.py.
 """
 
 import collections
@@ -24,8 +23,8 @@ from tests.conftest import golden
 TOL = 1e-12
 
 
-@pytest.mark.parametrize("name,limit", [("uccnvqe_he", None), ("adaptvqe_h4", 2500)])
-def test_reference_driver_trace_on_the_oracle(name, limit):
+@pytest.mark.parametrize("name", ["uccnvqe_he", "adaptvqe_h4"])
+def test_reference_driver_trace_on_the_oracle(name):
     z = golden(f"dropin_trace_{name}.npz")
     err = collections.defaultdict(float)
     energies = []
@@ -36,10 +35,9 @@ def test_reference_driver_trace_on_the_oracle(name, limit):
         if call == "direct_op_exp_val":
             energies.append(got[0])
 
-    n = replay(z, lambda a: DropinComputer(a), check, inner=lambda a, b: a.s.dot(b.s), limit=limit)
-    assert n == (len(z["calls"]) if limit is None else limit) and energies
+    n = replay(z, lambda a: DropinComputer(a), check, inner=lambda a, b: a.s.dot(b.s))
+    assert n == len(z["calls"]) and energies
     for call, e in err.items():
         assert e < TOL, (call, e)
-    if limit is None:
-        assert abs(energies[-1].real - float(z["e_fci"])) < float(z["tol"])
-        assert abs(energies[-1].real - float(z["energy"])) < TOL
+    assert abs(energies[-1].real - float(z["e_fci"])) < float(z["tol"])
+    assert abs(energies[-1].real - float(z["energy"])) < TOL

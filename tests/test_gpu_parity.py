@@ -467,11 +467,14 @@ def test_dense_block_of_a_deep_run_on_few_qubits(cuda, dense_blocks, k):
     assert np.max(np.abs(qc.get_coeff_array() - st.psi)) < AMP_TOL
 
 
-def test_dense_blocks_on_a_batch_of_states(cuda, dense_blocks):
-    """Every slot of a batched state gets the same dense passes."""
+@pytest.mark.parametrize("form", ["dense5", "fused", "ops"])
+def test_gate_runs_on_a_batch_of_states(cuda, form):
+    """Every slot of a batched state gets the same passes: dense 5-qubit
+    blocks, and tile runs with their phases fused (FP64 tensor cores) or gate
+    by gate."""
     import ctypes
     from qforte_b200._lib import check, lib, ptr
-    from qforte_b200.device import pack_gates
+    from qforte_b200.device import gates_config, pack_gates
     n = 12
     circ, ora = _rand_circuit(n, 150, 35)
     L = lib()
@@ -482,8 +485,12 @@ def test_dense_blocks_on_a_batch_of_states(cuda, dense_blocks):
         for b, v in enumerate(psis):
             check(L.qfb_state_upload(h, b, ptr(v), 1 << n))
         arr = pack_gates(circ.gates())
-        dense_blocks(5)
-        check(L.qfb_apply_gates(h, arr.ctypes.data, len(arr)), "qfb_apply_gates")
+        gates_config(0, 3, 0, 5 if form == "dense5" else 0,
+                     None if form == "dense5" else form == "fused")
+        try:
+            check(L.qfb_apply_gates(h, arr.ctypes.data, len(arr)), "qfb_apply_gates")
+        finally:
+            gates_config()
         for b, v in enumerate(psis):
             out = np.zeros(1 << n, dtype=np.complex128)
             check(L.qfb_state_download(h, b, ptr(out), 1 << n))
