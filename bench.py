@@ -8,9 +8,11 @@ Workload (one step): 256 parameter sets of the 16-qubit dUCCSD problem
 adjoint gradient.  Metric: evaluations per second (whole job).
 
 * ``value``    device-timed (CUDA events, max over ranks): parameters already in
-               HBM, one graph-captured run per step; consecutive steps alternate
-               between two evaluators on two streams (``--streams``), so one
-               step's kernels use the SMs the other leaves idle.
+               HBM, one graph-captured run per step; consecutive steps rotate
+               over four evaluators on four streams (``--streams``), so one
+               step's kernels use the SMs the others leave idle (the forward
+               program fills 128 SMs of 148, the sweep's latency-bound CTAs
+               leave issue slots free).
 * ``e2e``      the same through the public API with host buffers: the step's
                parameters copied from pinned host memory and its energies and
                gradients read back, inside the timed region (a step's copies
@@ -63,7 +65,7 @@ def parse():
     ap.add_argument("--norb", type=int, default=8)
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--seed", type=int, default=11)
-    ap.add_argument("--streams", type=int, default=2,
+    ap.add_argument("--streams", type=int, default=4,
                     help="default workload: consecutive steps alternate between this many "
                          "evaluators, each on its own stream, so their kernels and copies overlap")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -159,12 +159,13 @@ QFB_API int qfb_gates_dense(int k);
  * of 3; always clamped so a tile has at most 256 threads and at least 4).  No
  * counterpart in the reference; set by the autotuner. */
 QFB_API int qfb_gates_regs(int reg_bits);
-/* Form of the tile phases of complex128 states, process-wide: 1 applies each
- * phase (of 3 register bits, in tiles of 256 amplitudes and more) as a few
- * 8 x 8 matrices on the FP64 tensor cores (mma.sync), the product of its
- * gates, one per assignment of the thread bits its controls test, and one
- * factor per amplitude vector; 0 applies the phase's gates one by one; 2 (the
- * default) is 1 for states of 128 MiB and more (larger than L2) and 0 below.
+/* Form of the tile phases, process-wide: 1 applies each phase (of 3 register
+ * bits, in tiles of 256 amplitudes and more) as a few 8 x 8 matrices on the
+ * FP64 tensor cores (mma.sync), the product of its gates, one per assignment
+ * of the thread bits its controls test, and one factor per amplitude vector
+ * (complex64 states widened to FP64 for the products); 0 applies the phase's
+ * gates one by one; 2 (the default) is 1 for states of 128 MiB and more
+ * (larger than L2) and 0 below.
  * Both forms give the result of the gates in list order (up to the rounding
  * of the fused products).  No counterpart in the reference; set by the
  * autotuner. */

@@ -87,6 +87,7 @@ struct AmpT<double2> {
     using S = double;
     __device__ __forceinline__ static double2 make(double re, double im) { return make_double2(re, im); }
     __device__ __forceinline__ static double2 cvt(double2 v) { return v; }
+    __device__ __forceinline__ static double2 wide(double2 v) { return v; }
 };
 template <>
 struct AmpT<float2> {
@@ -95,6 +96,7 @@ struct AmpT<float2> {
     __device__ __forceinline__ static float2 cvt(double2 v) {
         return make_float2((float)v.x, (float)v.y);
     }
+    __device__ __forceinline__ static double2 wide(float2 v) { return make_double2(v.x, v.y); }
 };
 // conj(a) * b
 __device__ __forceinline__ double2 c_cjmul(double2 a, double2 b) {

@@ -556,6 +556,7 @@ int gate_tile_smem() {
         attr((const void *)qfbt::k_gate_tile<3, float2>, bytes8(11));
         attr((const void *)qfbt::k_gate_tile<4, float2>, bytes8(kGateTileMax));
         attr((const void *)qfbt::k_gate_tile<3, double2, true>, fused_bytes(bytes(11)));
+        attr((const void *)qfbt::k_gate_tile<3, float2, true>, fused_bytes(bytes8(11)));
     });
     return err == cudaSuccess ? QFB_OK : cuda_fail(err, "gate tile shared memory");
 }
@@ -739,7 +740,7 @@ void top_apply_host(const qfbt::TOp &o, const double2 *m4, uint32_t tl, int R, d
     }
 }
 
-// The fused form of phase ph (R = 3, complex128, 2^(b-3) >= 32 threads; its
+// The fused form of phase ph (R = 3, 2^(b-3) >= 32 threads; its
 // ops already in tp.ops), appended to tp.ph: segments of consecutive ops with
 // at most kMaxVarBits variant bits, each an 8 x 8 matrix per variant in
 // A-fragment order, and the per-vector product of the factors that depend on
@@ -749,8 +750,9 @@ void top_apply_host(const qfbt::TOp &o, const double2 *m4, uint32_t tl, int R, d
 // entries); otherwise the phase is split into phases on the same registers,
 // each with its own thread table: all but the last store to the load
 // offsets, the next loads them again.
-void fuse_phase(TilePlan &tp, const qfbt::TPhase &ph, int b) {
+void fuse_phase(TilePlan &tp, const qfbt::TPhase &ph, int b, bool c64) {
     constexpr int R = 3;
+    auto toff = [c64](uint32_t l) { return c64 ? qfbt::tpad8(l) : qfbt::tpad(l); };
     constexpr uint32_t NR = 8;
     const uint32_t nth = 1u << (b - R);
     const int nvb = b - R - 3;  // vector-index bits above the n-block columns
@@ -760,7 +762,7 @@ void fuse_phase(TilePlan &tp, const qfbt::TPhase &ph, int b) {
     for (int j = 0; j < R; ++j) {
         rbit[j] = 0;
         for (int p = 0; p < b; ++p)
-            if (qfbt::tpad(1u << p) == ph.roff[1 << j]) rbit[j] = p;
+            if (toff(1u << p) == ph.roff[1 << j]) rbit[j] = p;
         S |= 1u << rbit[j];
     }
     const uint32_t T = ((1u << b) - 1u) & ~S;  // thread bits
@@ -849,7 +851,7 @@ void fuse_phase(TilePlan &tp, const qfbt::TPhase &ph, int b) {
             uint32_t tl = 0;
             for (size_t j = 0; j < tb.size(); ++j)
                 if (t >> j & 1u) tl |= 1u << tb[j];
-            tp.threads.push_back(tl | (qfbt::tpad(tl) << 16));
+            tp.threads.push_back(tl | (toff(tl) << 16));
         }
         return th0;
     };
@@ -906,8 +908,8 @@ void fuse_phase(TilePlan &tp, const qfbt::TPhase &ph, int b) {
 // gate that cannot join blocks its bits for the rest of the scan, so only
 // gates on disjoint qubits change order.
 // c64: shared offsets in the complex64 tile layout (qfbt::tpad8).
-// fused: the phases' fused form where it applies (R = 3, complex128, at
-// least 32 threads).
+// fused: the phases' fused form where it applies (R = 3, at least 32
+// threads).
 void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, TilePlan &tp,
                       bool c64 = false, bool fused = false) {
     auto toff = [c64](uint32_t l) { return c64 ? qfbt::tpad8(l) : qfbt::tpad(l); };
@@ -1082,8 +1084,8 @@ void plan_tile_phases(const WGate *g, int ng, int b, int R, qfbt::TRun &run, Til
             ph.soff[k] = toff(l);
         }
         ph.no = (int)tp.ops.size() - ph.o0;
-        if (fused && R == 3 && b - R >= 5 && !c64)
-            fuse_phase(tp, ph, b);
+        if (fused && R == 3 && b - R >= 5)
+            fuse_phase(tp, ph, b, c64);
         else
             tp.ph.push_back(ph);
     }
@@ -1303,7 +1305,7 @@ int apply_gates_tiles(A *d, int n, int nbatch, const std::vector<HGate> &hg) {
     TilePlan tp;
     std::vector<qfbt::TRun> runs;
     const bool fused = g_gate_fused == 1 ||
-                       (g_gate_fused == 2 && sizeof(double2) * nbasis * (uint64_t)nbatch >= kFusedMinBytes);
+                       (g_gate_fused == 2 && sizeof(A) * nbasis * (uint64_t)nbatch >= kFusedMinBytes);
     plan_gate_tiles(hg, n, b, L, wins, tp, runs, c64, fused);
     // one upload of phases, ops, 4x4 matrices, chunk and thread tables and
     // the fused form
@@ -1349,7 +1351,7 @@ int apply_gates_tiles(A *d, int n, int nbatch, const std::vector<HGate> &hg) {
         }
         const int tb = pw.w.b, R = tile_reg_bits(tb);
         const size_t smem0 = sizeof(A) * qfbt::tpad_size_of<A>(tb) + 16;
-        const bool fz = fused && R == 3 && tb - R >= 5 && !c64;
+        const bool fz = fused && R == 3 && tb - R >= 5;
         const size_t smem = fz ? (size_t)fused_bytes((int)smem0) : smem0;
         const dim3 grid((unsigned)(nbasis >> tb), nbatch), block(1u << (tb - R));
 #define QFB_TILE(RR, FF)                                                                        \

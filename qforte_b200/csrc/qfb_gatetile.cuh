@@ -77,9 +77,10 @@ struct TPhase {
 };
 static_assert(sizeof(TPhase) == 160, "TPhase layout");
 
-// The fused form of a phase (complex128 tiles with R = 3 and at least 32
-// threads): the phase's ops, in order, become a few segments, each one 8 x 8
-// matrix on the 8 register amplitudes, applied on the FP64 tensor cores.
+// The fused form of a phase (tiles with R = 3 and at least 32 threads; the
+// products in FP64 also for complex64 tiles): the phase's ops, in order,
+// become a few segments, each one 8 x 8 matrix on the 8 register amplitudes,
+// applied on the FP64 tensor cores.
 //  * Vector t of the phase (the 8 amplitudes at tile offsets base(t) +
 //    roff[k], base from entry t of the thread table) is processed by warp
 //    t / 32 as column t % 8 of n-block (t / 8) % 4: per n-block the warp
@@ -440,21 +441,23 @@ __device__ __forceinline__ uint32_t seg_variant(uint32_t tl, const uint4 &h) {
 }
 
 // One fused phase on this warp's 32 vectors: its segments in order (each
-// reads the vectors at roff and writes them back, the last one at soff).
+// reads the vectors at roff and writes them back, the last one at soff).  A:
+// the tile's amplitudes (complex128, or complex64 widened to FP64 for the
+// products and rounded back on store).
+template <class A>
 __device__ __forceinline__ void fused_phase(const TPhase *__restrict__ ph, const TSeg *__restrict__ segs,
-                                            const double2 *__restrict__ fm, const uint32_t *thr,
-                                            double2 *tile) {
+                                            const double2 *__restrict__ fm, const uint32_t *thr, A *tile) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
     const int s0 = __ldg(&ph->s0), ns = __ldg(&ph->ns), sc = __ldg(&ph->sc);
     if (ns == 0) {  // relabelings only: each thread moves its own vector
-        double2 *t0 = tile + (thr[threadIdx.x] >> 16);
-        double2 v[8];
+        A *t0 = tile + (thr[threadIdx.x] >> 16);
+        A v[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) v[k] = t0[__ldg(&ph->roff[k])];
         if (sc >= 0) {
             const double2 f = __ldg(fm + sc + threadIdx.x);
 #pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = c_mul(f, v[k]);
+            for (int k = 0; k < 8; ++k) v[k] = AmpT<A>::cvt(c_mul(f, AmpT<A>::wide(v[k])));
         }
 #pragma unroll
         for (int k = 0; k < 8; ++k) t0[__ldg(&ph->soff[k])] = v[k];
@@ -487,8 +490,8 @@ __device__ __forceinline__ void fused_phase(const TPhase *__restrict__ ph, const
                 }
                 // B fragments: registers 4 kb + q of vector tv + g
                 const uint32_t bb = thr[tv + g] >> 16;
-                x0[u] = tile[bb + ri0];
-                x1[u] = tile[bb + ri1];
+                x0[u] = AmpT<A>::wide(tile[bb + ri0]);
+                x1[u] = AmpT<A>::wide(tile[bb + ri1]);
                 if (scale) {
                     const double2 f = __ldg(fm + sc + tv + g);
                     x0[u] = c_mul(f, x0[u]);
@@ -521,8 +524,8 @@ __device__ __forceinline__ void fused_phase(const TPhase *__restrict__ ph, const
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
                 const int tv = warp * 32 + (np + u) * 8;
-                tile[(thr[tv + 2 * q] >> 16) + ro] = make_double2(dr[u][0], di[u][0]);
-                tile[(thr[tv + 2 * q + 1] >> 16) + ro] = make_double2(dr[u][1], di[u][1]);
+                tile[(thr[tv + 2 * q] >> 16) + ro] = AmpT<A>::cvt(make_double2(dr[u][0], di[u][0]));
+                tile[(thr[tv + 2 * q + 1] >> 16) + ro] = AmpT<A>::cvt(make_double2(dr[u][1], di[u][1]));
             }
         }
         if (si + 1 < ns) __syncwarp();  // the next segment reads what this one wrote
@@ -587,7 +590,7 @@ __global__ void __launch_bounds__(256, F ? 4 : R == 4 ? 1 : 3)
     const int nch = 1 << (b - 3);
     __shared__ uint64_t s_base;
     // fused form: two buffers of a phase's thread table after the barrier word
-    constexpr bool kF = F && R == 3 && sizeof(A) == sizeof(double2);
+    constexpr bool kF = F && R == 3;
     uint32_t *sthr = reinterpret_cast<uint32_t *>(
         t_smem + ((sizeof(A) * tpad_size_of<A>(b) + 16 + 15) & ~(size_t)15));
     auto stage = [&](int p) {
@@ -608,24 +611,27 @@ __global__ void __launch_bounds__(256, F ? 4 : R == 4 ? 1 : 3)
     A *s = psi + s_base;
     const uint64_t *ch = chunks + run.ch0;
     if constexpr (kF) {
-        // 16-byte asynchronous copies, eight consecutive threads per chunk
-        for (int i = tid; i < 8 * nch; i += nth) {
-            const int c = i >> 3, e = i & 7;
-            cp_async16(smem_u32(tile + tpad((uint32_t)c << 3) + e), s + __ldg(&ch[c]) + e);
+        // 16-byte asynchronous copies, PPC consecutive threads per chunk
+        constexpr int PPC = (int)kChunk / 16;
+        for (int i = tid; i < PPC * nch; i += nth) {
+            const int c = i / PPC, e = i % PPC;
+            cp_async16(smem_u32(reinterpret_cast<unsigned char *>(tile + tpad_of<A>((uint32_t)c << 3)) + 16 * e),
+                       reinterpret_cast<const unsigned char *>(s + __ldg(&ch[c])) + 16 * e);
         }
         cp_async_commit();
         if (run.np > 0) stage(0);
         cp_async_wait_all();
         __syncthreads();  // the tile and phase 0's thread table
         for (int p = 0; p < run.np; ++p) {
-            fused_phase(phases + run.p0 + p, segs, fm, sthr + (p & 1) * (1 << kMaxThreadBits),
-                        reinterpret_cast<double2 *>(tile));
+            fused_phase<A>(phases + run.p0 + p, segs, fm, sthr + (p & 1) * (1 << kMaxThreadBits), tile);
             if (p + 1 < run.np) stage(p + 1);
             __syncthreads();
         }
-        for (int i = tid; i < 8 * nch; i += nth) {
-            const int c = i >> 3, e = i & 7;
-            s[__ldg(&ch[c]) + e] = tile[tpad((uint32_t)c << 3) + e];
+        for (int i = tid; i < PPC * nch; i += nth) {
+            const int c = i / PPC, e = i % PPC;
+            *reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(s + __ldg(&ch[c])) + 16 * e) =
+                *reinterpret_cast<const uint4 *>(
+                    reinterpret_cast<const unsigned char *>(tile + tpad_of<A>((uint32_t)c << 3)) + 16 * e);
         }
         return;
     }

@@ -846,6 +846,29 @@ def test_complex64_gates_track_complex128(cuda, gate_tiles, tile, low, n, ngates
         qc.apply_circuit(qb.build_circuit(f"X_{n}"))
 
 
+@pytest.mark.parametrize("n,kind,seed", [(10, "random", 71), (13, "controls", 72), (16, "random", 73)])
+def test_complex64_fused_phases_track_complex128(cuda, n, kind, seed):
+    """The complex64 variant with its tile phases fused (products in FP64 on
+    the tensor cores, amplitudes rounded to FP32 at each phase's store)
+    against the oracle's complex128 state: within FP32 rounding (3e-6)."""
+    from qforte_b200.computer import ComputerC64
+    from qforte_b200.device import gates_config
+    circ, ora = (_rand_circuit(n, 300, seed) if kind == "random"
+                 else _control_heavy_circuit(n, seed))
+    psi0 = _random_state(n, seed)
+    gates_config(0, 3, 0, 0, True)
+    try:
+        qc = ComputerC64(n)
+        qc.set_coeff_vec(psi0)
+        qc.apply_circuit(circ)
+        got = qc.get_coeff_array()
+    finally:
+        gates_config()
+    st = O.State(n, psi0.copy())
+    st.apply_gates(ora)
+    assert np.max(np.abs(got.astype(np.complex128) - st.psi)) < 3e-6
+
+
 @pytest.mark.parametrize("norb,seed,pool_type,B", [(4, 11, "SD", 5), (6, 3, "SD", 2),
                                                    (5, 9, "GSD", 7), (8, 2, "SD", 6)])
 def test_two_sets_per_cta_match_one_set(cuda, norb, seed, pool_type, B):
