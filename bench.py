@@ -59,7 +59,9 @@ UNIT = "evals/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 40 for the default workload, whose steps "
+                         "rotate over --streams evaluators, else 5)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--norb", type=int, default=8)
@@ -112,7 +114,10 @@ def parse():
                     help="gate sweep: the complex64 throughput variant (FP32 arithmetic)")
     ap.add_argument("--autotune", action="store_true",
                     help="gate sweep: pick the tile shape per qubit count with the autotuner")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.steps is None:
+        a.steps = 40 if a.workload == "ucc" else 5
+    return a
 
 
 def problem(norb, seed):
