@@ -37,6 +37,59 @@ __all__ = ["Computer", "ComputerC64", "inner_product", "prepare_computer_from_ci
 _SEED = [int.from_bytes(__import__("os").urandom(8), "little")]
 
 
+# ---- objects of the reference's own module (duck typing) -------------------
+# The entry points below also take the reference's pybind Gate, Circuit,
+# QubitOperator and QubitOpPool (bindings.cc:193-218 and the classes around
+# them): a gate is rebuilt from gate_id(), target(), control() and
+# parameter() by make_gate, the same construction as the reference's
+# (make_gate.cc:18-235); circuits, operators and pools from gates() and
+# terms().  So a caller may keep the reference's object model and swap in
+# this Computer alone.
+
+
+def _as_gate(g):
+    if isinstance(g, Gate):
+        return g
+    p = g.parameter() if g.has_parameter() else None
+    # the adjoint of a parameter-free gate that is not its own inverse is
+    # labelled adj(label) (gate.cc:172-177): rebuild the gate, then take it
+    label, depth = g.gate_id(), 0
+    while label.startswith("adj(") and label.endswith(")"):
+        label, depth = label[4:-1], depth + 1
+    out = make_gate(label, g.target(), g.control(), 0.0 if p is None else float(p))
+    for _ in range(depth):
+        out = out.adjoint()
+    return out
+
+
+def _as_circuit(c):
+    if isinstance(c, Circuit):
+        return c
+    out = Circuit()
+    for g in c.gates():
+        out.add(_as_gate(g))
+    return out
+
+
+def _as_operator(qo):
+    if isinstance(qo, QubitOperator):
+        return qo
+    out = QubitOperator()
+    for coeff, circ in qo.terms():
+        out.add(complex(coeff), _as_circuit(circ))
+    return out
+
+
+def _as_pool(pool):
+    from .sq_op_pool import QubitOpPool
+    if isinstance(pool, QubitOpPool):
+        return pool
+    out = QubitOpPool()
+    for coeff, op in pool.terms():
+        out.add(complex(coeff), _as_operator(op))
+    return out
+
+
 def set_sampling_seed(seed):
     """Start the process-wide seed sequence of Computer's measurement draws
     (the reference's draws are unseeded; equal seeds here give equal draws)."""
@@ -208,6 +261,7 @@ class Computer:
             raise ValueError(f"circuit acts on qubit {nq - 1} of a {self._n}-qubit Computer")
 
     def apply_circuit(self, qc):
+        qc = _as_circuit(qc)
         plan = _plan_for(qc)
         self._check_qubits(plan.nqubit_needed)
         one = np.ones(1)
@@ -220,6 +274,7 @@ class Computer:
     apply_circuit_safe = apply_circuit
 
     def apply_gate(self, qg):
+        qg = _as_gate(qg)
         self._check_qubits(max(qg.target(), qg.control()) + 1)
         arr = pack_gates([qg])
         check(lib().qfb_apply_gates(self._h, ptr(arr), 1), "apply_gate")
@@ -231,6 +286,7 @@ class Computer:
 
     # ---- operators (computer.cc:80-91, :753-848) ---------------------------
     def apply_operator(self, qo):
+        qo = _as_operator(qo)
         pt = qo._pauli_terms(applied=True)
         if pt is not None:
             ds = sum_from_terms(pt)
@@ -270,6 +326,7 @@ class Computer:
         return out
 
     def direct_op_exp_val(self, qo):
+        qo = _as_operator(qo)
         pt = qo._pauli_terms(applied=True)
         if pt is not None:
             return complex(self._expval_terms(pt)[0])
@@ -278,9 +335,11 @@ class Computer:
         return inner_product(self, tmp)
 
     def direct_oppl_exp_val(self, qopl):
+        qopl = _as_pool(qopl)
         return self._pool_expvals(qopl, range(len(qopl)))
 
     def direct_idxd_oppl_exp_val(self, qopl, idxs):
+        qopl = _as_pool(qopl)
         return self._pool_expvals(qopl, list(idxs))
 
     def _pool_expvals(self, qopl, idxs):
@@ -298,6 +357,7 @@ class Computer:
         return [complex(vals[k]) * pool[i][0] for k, i in enumerate(idxs)]
 
     def direct_oppl_exp_val_w_mults(self, qopl, mults):
+        qopl = _as_pool(qopl)
         pool = qopl.terms()
         terms, seg = [], []
         for k, (pc, op) in enumerate(pool):
@@ -322,6 +382,7 @@ class Computer:
         return out
 
     def direct_circ_exp_val(self, qc):
+        qc = _as_circuit(qc)
         m = qc._applied_pauli_masks()
         if m is not None:
             x, z, e = m
@@ -331,6 +392,7 @@ class Computer:
         return inner_product(self, tmp)
 
     def direct_pauli_circ_exp_val(self, qc):
+        qc = _as_circuit(qc)
         xs, ys, zs = [], [], []
         for g in qc.gates():
             lab = g.gate_id()
@@ -366,6 +428,7 @@ class Computer:
         return complex(self._expval_terms([(c, X, zeff)])[0])
 
     def direct_gate_exp_val(self, qg):
+        qg = _as_gate(qg)
         self.apply_gate(qg)
         return 0j
 
@@ -384,6 +447,7 @@ class Computer:
         return tmp
 
     def perfect_measure_circuit(self, qc):
+        qc = _as_circuit(qc)
         zm = 0
         for g in qc.gates():
             zm ^= 1 << g.target()
@@ -404,6 +468,7 @@ class Computer:
     def measure_circuit(self, qc, n_measurements):
         """computer.cc:135-183: rotate X / Y measured qubits to Z on a copy,
         draw basis states, return the product of the measured qubits' +-1."""
+        qc = _as_circuit(qc)
         tmp = self._rotated_copy(qc)
         idx = tmp.sample(n_measurements)
         del tmp
@@ -418,6 +483,7 @@ class Computer:
 
     def measure_readouts(self, qc, n_measurements):
         """computer.cc:213-259: the measured qubits' bits of each draw."""
+        qc = _as_circuit(qc)
         tmp = self._rotated_copy(qc)
         idx = tmp.sample(n_measurements)
         del tmp
@@ -508,6 +574,7 @@ class ComputerC64:
 
     def apply_circuit(self, qc):
         """The circuit's gates (gates beyond the state raise ValueError)."""
+        qc = _as_circuit(qc)
         arr = pack_gates(qc.gates())
         check(lib().qfb_c64_apply_gates(self._h, arr.ctypes.data if len(arr) else None, len(arr)),
               "qfb_c64_apply_gates")

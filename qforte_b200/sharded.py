@@ -169,7 +169,9 @@ class ShardedComputer:
 
     def apply_gates(self, gates):
         from .circuit import Circuit
+        from .computer import _as_gate
         from .gate import Gate
+        gates = [_as_gate(g) for g in gates]
         run = []
 
         def flush():

@@ -1,4 +1,5 @@
-"""The reference's own drivers' engine calls, replayed on the device Computer.
+"""The reference's own drivers' engine calls, replayed on the device Computer,
+and the reference's own objects handed to it.
 
 tests/golden/dropin_trace_*.npz record every Computer call the reference's
 UCCNVQE (He/cc-pVDZ, its tests/test_uccsd.py:13-29) and ADAPTVQE (H4/STO-6G,
@@ -45,3 +46,34 @@ def test_reference_driver_trace_on_the_device(cuda, name):
         assert e < TOL, (call, e)
     assert abs(energies[-1].real - float(z["e_fci"])) < float(z["tol"])
     assert abs(energies[-1].real - float(z["energy"])) < TOL
+
+
+def test_reference_objects_on_the_device(cuda):
+    """The reference's compiled Gate / Circuit / QubitOperator / QubitOpPool
+    passed straight to the device Computer (rebuilt by duck typing at each
+    entry point): states, expectation values and pool expectation values equal
+    the reference Computer's on the same objects (1e-12)."""
+    from test_foreign_objects import reference_circuit, reference_engine, reference_operator
+    qf = reference_engine()
+    n = 9
+    for seed in range(3):
+        rc = reference_circuit(qf, n, 200, 10 + seed)
+        ref = qf.Computer(n)
+        ref.apply_circuit(rc)
+        qc = qb.Computer(n)
+        qc.apply_circuit(rc)
+        assert np.max(np.abs(qc.get_coeff_array() - np.array(ref.get_coeff_vec()))) < TOL
+        g = qf.gate("cRz", 3, 1, 0.7)
+        ref.apply_gate(g)
+        qc.apply_gate(g)
+        assert np.max(np.abs(qc.get_coeff_array() - np.array(ref.get_coeff_vec()))) < TOL
+        qo = reference_operator(qf, n, 40, seed)
+        assert abs(qc.direct_op_exp_val(qo) - ref.direct_op_exp_val(qo)) < TOL
+        pool = qf.QubitOpPool()
+        for k in range(4):
+            pool.add(complex(0.5 + k, -0.25 * k), reference_operator(qf, n, 10, 100 * seed + k))
+        assert np.max(np.abs(np.array(qc.direct_oppl_exp_val(pool)) -
+                             np.array(ref.direct_oppl_exp_val(pool)))) < TOL
+        ref.apply_operator(qo)
+        qc.apply_operator(qo)
+        assert np.max(np.abs(qc.get_coeff_array() - np.array(ref.get_coeff_vec()))) < 1e-11
