@@ -170,6 +170,15 @@ QFB_API int qfb_gates_regs(int reg_bits);
  * of the fused products).  No counterpart in the reference; set by the
  * autotuner. */
 QFB_API int qfb_gates_fused(int mode);
+/* Host only: the fused form of the tile runs qfb_apply_gates would apply to
+ * one nqubit state (complex64 != 0: a complex64 state) under the current tile
+ * shape, each phase checked as the device reads it (thread tables: every
+ * thread-bit assignment once, offsets in the tile; segments: variant bits on
+ * thread bits, shared by the 8 vectors of each n-block; matrices in range).
+ * Returns QFB_EINVAL on a failed check; else the fused phases, their
+ * segments and matrix entries.  No counterpart in the reference. */
+QFB_API int qfb_gates_fused_plan(const qfb_gate *gates, int64_t ngates, int nqubit, int complex64,
+                                 int64_t *phases, int64_t *segments, int64_t *entries);
 /* Host only: how qfb_apply_gates would apply these gates to one nqubit state
  * under the current tile shape: the number of tile runs, of one-gate passes,
  * and the bytes those passes read and write (a run 32 * 2^n; a one-gate pass

@@ -79,6 +79,7 @@ SIGNATURES = {
     "qfb_gates_phases": (ctypes.c_int, [_vp, _i64, ctypes.c_int, _vp, _vp]),
     "qfb_gates_regs": (ctypes.c_int, [ctypes.c_int]),
     "qfb_gates_fused": (ctypes.c_int, [ctypes.c_int]),
+    "qfb_gates_fused_plan": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "qfb_scale": (ctypes.c_int, [c_state, QfbComplex]),
     "qfb_vdot": (ctypes.c_int, [c_state, c_state, _vp]),
     "qfb_axpy": (ctypes.c_int, [c_state, QfbComplex, c_state]),

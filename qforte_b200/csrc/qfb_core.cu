@@ -756,6 +756,8 @@ void fuse_phase(TilePlan &tp, const qfbt::TPhase &ph, int b, bool c64) {
     constexpr uint32_t NR = 8;
     const uint32_t nth = 1u << (b - R);
     const int nvb = b - R - 3;  // vector-index bits above the n-block columns
+    // a segment's variant bits must all fit there (8-qubit tiles have 2)
+    const int maxv = std::min(qfbt::kMaxVarBits, nvb);
     // the register bits' tile bits (loads): register position j <-> roff[1 << j]
     int rbit[R];
     uint32_t S = 0;
@@ -816,7 +818,7 @@ void fuse_phase(TilePlan &tp, const qfbt::TPhase &ph, int b, bool c64) {
             continue;
         }
         const uint32_t need = o.tctl | (o.opc == qfbt::OPC_DIAG_THREAD ? o.tbit : 0u);
-        if (__builtin_popcount(D | need) > qfbt::kMaxVarBits) {
+        if (__builtin_popcount(D | need) > maxv) {
             flush(D);
             D = 0;
         }
@@ -1708,6 +1710,74 @@ int qfb_gates_phases(const qfb_gate *gates, int64_t ngates, int nqubit, int64_t 
     }
     if (phases) *phases = np;
     if (ops) *ops = no;
+    return QFB_OK;
+}
+
+int qfb_gates_fused_plan(const qfb_gate *gates, int64_t ngates, int nqubit, int complex64,
+                         int64_t *phases, int64_t *segments, int64_t *entries) {
+    if (ngates < 0 || (ngates > 0 && !gates) || nqubit < 1 || nqubit > 40)
+        return fail(QFB_EINVAL, "qfb_gates_fused_plan: bad arguments");
+    std::vector<HGate> hg((size_t)ngates);
+    for (int64_t k = 0; k < ngates; ++k) {
+        const qfb_gate &g = gates[k];
+        if (g.target < 0 || g.target >= nqubit || g.control < 0 || g.control >= nqubit)
+            return fail(QFB_EINVAL, "qfb_gates_fused_plan: gate %lld acts beyond qubit %d",
+                        (long long)k, nqubit);
+        hg[k] = classify_gate(g);
+    }
+    int b = 0, L = 0;
+    int64_t np = 0, ns = 0, ne = 0;
+    const bool c64 = complex64 != 0;
+    auto toff = [c64](uint32_t l) { return c64 ? qfbt::tpad8(l) : qfbt::tpad(l); };
+    if (gate_tile_shape(nqubit, b, L) && ngates > 1) {
+        std::vector<GatePlanWin> wins;
+        TilePlan tp;
+        std::vector<qfbt::TRun> runs;
+        plan_gate_tiles(hg, nqubit, b, L, wins, tp, runs, c64, true);
+        for (size_t w = 0; w < wins.size(); ++w) {
+            if (wins[w].single >= 0) continue;
+            const qfbt::TRun &r = runs[w];
+            const int R = tile_reg_bits(r.b);
+            if (!(R == 3 && r.b - R >= 5)) continue;  // this run keeps the gate-by-gate form
+            const uint32_t nth = 1u << (r.b - R), all = (1u << r.b) - 1u;
+            for (int p = r.p0; p < r.p0 + r.np; ++p) {
+                const qfbt::TPhase &ph = tp.ph[(size_t)p];
+                uint32_t S = 0;  // the register bits
+                for (int k = 1; k < 8; k <<= 1)
+                    for (int q = 0; q < r.b; ++q)
+                        if (toff(1u << q) == ph.roff[k]) S |= 1u << q;
+                // the thread table: a permutation of the thread-bit assignments
+                std::vector<char> seen((size_t)1 << r.b, 0);
+                for (uint32_t t = 0; t < nth; ++t) {
+                    const uint32_t e = tp.threads[(size_t)ph.th0 + t], tl = e & 0xffffu;
+                    if ((tl & ~(all & ~S)) || (e >> 16) != toff(tl) || seen[tl])
+                        return fail(QFB_EINVAL, "qfb_gates_fused_plan: bad thread table (phase %d)", p);
+                    seen[tl] = 1;
+                }
+                if (ph.nm > qfbt::kStage || ph.m0 < 0 || (size_t)ph.m0 + (size_t)ph.nm > tp.fm.size() ||
+                    (ph.sc >= 0 && (size_t)ph.sc + nth > tp.fm.size()))
+                    return fail(QFB_EINVAL, "qfb_gates_fused_plan: matrices out of range (phase %d)", p);
+                for (int s = ph.s0; s < ph.s0 + ph.ns; ++s) {
+                    const qfbt::TSeg &sg = tp.segs[(size_t)s];
+                    uint32_t vm = 0;
+                    for (uint32_t j = 0; j < sg.nd; ++j) vm |= 1u << ((sg.dsel >> (4 * j)) & 15u);
+                    if ((vm & ~(all & ~S)) || sg.nd > (uint32_t)qfbt::kMaxVarBits ||
+                        (int64_t)sg.m0 < ph.m0 || (size_t)sg.m0 + 64u * (1u << sg.nd) > (size_t)ph.m0 + ph.nm)
+                        return fail(QFB_EINVAL, "qfb_gates_fused_plan: bad segment %d", s);
+                    // the 8 vectors of an n-block share the variant bits
+                    for (uint32_t t = 0; t < nth; ++t)
+                        if (((tp.threads[(size_t)ph.th0 + t] ^ tp.threads[(size_t)ph.th0 + (t & ~7u)]) & vm) != 0)
+                            return fail(QFB_EINVAL, "qfb_gates_fused_plan: variant splits an n-block (segment %d)", s);
+                }
+                ++np;
+                ns += ph.ns;
+                ne += ph.nm;
+            }
+        }
+    }
+    if (phases) *phases = np;
+    if (segments) *segments = ns;
+    if (entries) *entries = ne;
     return QFB_OK;
 }
 

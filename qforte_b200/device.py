@@ -185,6 +185,19 @@ def gate_phases(gates, nqubit):
     return p.value, o.value
 
 
+def gate_fused_plan(gates, nqubit, complex64=False):
+    """(phases, segments, matrix entries) of the fused form of the tile runs
+    of ``gates`` on one ``nqubit`` state under the current tile shape, every
+    phase checked as the device reads it (ValueError on a failed check); host
+    only."""
+    arr = pack_gates(gates)
+    p, s, e = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    check(lib().qfb_gates_fused_plan(arr.ctypes.data if len(arr) else None, len(arr), int(nqubit),
+                                     1 if complex64 else 0, ctypes.byref(p), ctypes.byref(s),
+                                     ctypes.byref(e)), "qfb_gates_fused_plan")
+    return p.value, s.value, e.value
+
+
 def gates_config(tile_bits=0, low_bits=3, reg_bits=0, dense=0, fused=None):
     """Process-wide shape of gate runs: tile_bits 0 (default) or 4-12 for
     register-blocked shared-memory tiles, -1 for one pass per gate; reg_bits 0

@@ -96,3 +96,26 @@ def test_dense_block_planning():
     assert tiles_dense == gate_plan(small, 8)
     with pytest.raises(ValueError):
         gates_config(0, 3, 0, 7)
+
+
+@pytest.mark.parametrize("tile,low", [(8, 3), (9, 4), (10, 3), (11, 3), (11, 6)])
+@pytest.mark.parametrize("complex64", [False, True])
+def test_fused_plans_are_consistent(tile, low, complex64):
+    """The fused form of the tile phases, planned on the host for tiles of 8
+    to 11 qubits (1 to 8 warps of amplitude vectors), random, control-heavy
+    and layered circuits: every thread table a permutation of the thread-bit
+    assignments with offsets inside the tile, every segment's variant bits on
+    thread bits and shared by the 8 vectors of each n-block (as the tensor-core
+    products need), every matrix inside the phase's range."""
+    from test_gpu_parity import _control_heavy_circuit, _rand_circuit
+    from qforte_b200.device import gate_fused_plan, gates_config
+    from qforte_b200.workloads import layered_random_circuit
+    gates_config(tile, low)
+    try:
+        for n, seed in ((12, 1), (14, 2), (16, 3)):
+            for circ in (_rand_circuit(n, 400, seed)[0], _control_heavy_circuit(n, seed)[0],
+                         layered_random_circuit(n, 10, seed)[0]):
+                phases, segments, entries = gate_fused_plan(circ.gates(), n, complex64)
+                assert phases > 0 and segments > 0 and entries >= 64 * segments
+    finally:
+        gates_config()

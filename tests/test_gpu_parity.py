@@ -405,6 +405,29 @@ def test_fused_phases_match_oracle(cuda, fused, regs, n, kind, seed):
     assert np.max(np.abs(got - st.psi)) < AMP_TOL
 
 
+@pytest.mark.parametrize("tile,low", [(8, 3), (9, 4), (11, 3), (11, 6)])
+@pytest.mark.parametrize("n,kind,seed", [(12, "random", 45), (14, "controls", 46)])
+def test_fused_phases_every_tile_shape(cuda, tile, low, n, kind, seed):
+    """Fused tile phases in tiles of 8, 9 and 11 qubits (1, 2 and 8 warps of
+    amplitude vectors) and with 3 to 6 low qubits kept, from a random state,
+    against the oracle's gate-by-gate application."""
+    from qforte_b200.device import gates_config
+    circ, ora = (_rand_circuit(n, 400, seed) if kind == "random"
+                 else _control_heavy_circuit(n, seed))
+    psi0 = _random_state(n, seed)
+    gates_config(tile, low, 0, 0, True)
+    try:
+        qc = qb.Computer(n)
+        qc.set_coeff_vec(psi0)
+        qc.apply_circuit(circ)
+        got = qc.get_coeff_array()
+    finally:
+        gates_config()
+    st = O.State(n, psi0.copy())
+    st.apply_gates(ora)
+    assert np.max(np.abs(got - st.psi)) < AMP_TOL
+
+
 @pytest.fixture
 def dense_blocks():
     """Sets dense K-qubit blocks (FP64 tensor cores) and restores the default."""
