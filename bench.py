@@ -2,6 +2,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+(K defaults to 40 for the default workload, 5 for the others; W to 3.)
+
 Workload (one step): 256 parameter sets of the 16-qubit dUCCSD problem
 (8 spatial orbitals, 8 electrons, 360 SD parameters, seeded random integrals,
 5,793 Hamiltonian terms); each evaluation is the energy <U^dag H U> and its full
