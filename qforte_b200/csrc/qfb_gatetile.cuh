@@ -633,39 +633,39 @@ __global__ void __launch_bounds__(256, F ? 4 : R == 4 ? 1 : 3)
                 *reinterpret_cast<const uint4 *>(
                     reinterpret_cast<const unsigned char *>(tile + tpad_of<A>((uint32_t)c << 3)) + 16 * e);
         }
-        return;
-    }
-    for (int c = tid; c < nch; c += nth)
-        bulk_g2s(smem_u32(tile + tpad_of<A>((uint32_t)c << 3)), s + __ldg(&ch[c]), kChunk, bar_a);
-    const uint64_t limit = g_tile_wait_limit_ns;
-    if (limit == 0 || !mbar_wait_bounded(bar_a, 0, limit)) {
-        // the copies did not complete in time: flag it, give them a second
-        // bounded wait so none lands after this CTA's shared memory is
-        // released, and leave the tile unwritten
-        if (tid == 0) atomicExch(&g_tile_wait_err, 1);
-        mbar_wait_bounded(bar_a, 0, kWaitLimitNs);
-        return;
-    }
+    } else {
+        for (int c = tid; c < nch; c += nth)
+            bulk_g2s(smem_u32(tile + tpad_of<A>((uint32_t)c << 3)), s + __ldg(&ch[c]), kChunk, bar_a);
+        const uint64_t limit = g_tile_wait_limit_ns;
+        if (limit == 0 || !mbar_wait_bounded(bar_a, 0, limit)) {
+            // the copies did not complete in time: flag it, give them a second
+            // bounded wait so none lands after this CTA's shared memory is
+            // released, and leave the tile unwritten
+            if (tid == 0) atomicExch(&g_tile_wait_err, 1);
+            mbar_wait_bounded(bar_a, 0, kWaitLimitNs);
+            return;
+        }
 
-    for (int p = 0; p < run.np; ++p) {
-        const TPhase *ph = phases + run.p0 + p;
-        const uint32_t tw = __ldg(&threads[__ldg(&ph->th0) + tid]);
-        const uint32_t tl = tw & 0xffffu;
-        A *t0 = tile + (tw >> 16);
-        A v[1 << R];
+        for (int p = 0; p < run.np; ++p) {
+            const TPhase *ph = phases + run.p0 + p;
+            const uint32_t tw = __ldg(&threads[__ldg(&ph->th0) + tid]);
+            const uint32_t tl = tw & 0xffffu;
+            A *t0 = tile + (tw >> 16);
+            A v[1 << R];
 #pragma unroll
-        for (int k = 0; k < (1 << R); ++k) v[k] = t0[__ldg(&ph->roff[k])];
-        const int o0 = __ldg(&ph->o0), o1 = o0 + __ldg(&ph->no);
-        for (int o = o0; o < o1; ++o) apply_op<R, A>(v, ops + o, tl, m4);
+            for (int k = 0; k < (1 << R); ++k) v[k] = t0[__ldg(&ph->roff[k])];
+            const int o0 = __ldg(&ph->o0), o1 = o0 + __ldg(&ph->no);
+            for (int o = o0; o < o1; ++o) apply_op<R, A>(v, ops + o, tl, m4);
 #pragma unroll
-        for (int k = 0; k < (1 << R); ++k) t0[__ldg(&ph->soff[k])] = v[k];
-        if (p + 1 < run.np) __syncthreads();
+            for (int k = 0; k < (1 << R); ++k) t0[__ldg(&ph->soff[k])] = v[k];
+            if (p + 1 < run.np) __syncthreads();
+        }
+        fence_async_smem();
+        __syncthreads();
+        for (int c = tid; c < nch; c += nth)
+            bulk_s2g(s + __ldg(&ch[c]), smem_u32(tile + tpad_of<A>((uint32_t)c << 3)), kChunk);
+        bulk_commit_and_wait();
     }
-    fence_async_smem();
-    __syncthreads();
-    for (int c = tid; c < nch; c += nth)
-        bulk_s2g(s + __ldg(&ch[c]), smem_u32(tile + tpad_of<A>((uint32_t)c << 3)), kChunk);
-    bulk_commit_and_wait();
 }
 
 }  // namespace qfbt
